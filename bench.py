@@ -1,0 +1,366 @@
+"""Benchmark of the NPB CG inverse-power-iteration hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step"): the NPB class-B solve, n=75000, nonzer=13, shift=60,
+rcond=0.1, seed 314159265 -- 75 outer steps x (25 CG iterations + residual)
+in FP64, as the reference times it (GMAP/NPB-GPU CUDA/CG/cg.cu:491-522).
+The CSR (13.7 M entries, 166 MB) is larger than the 126 MB L2, so no L2
+flush is needed between steps.
+
+Metric: SpMV-equivalent HBM GB/s = (SpMV algorithmic bytes x SpMVs per solve)
+/ solve time, next to time-to-zeta (the solve's wall time with zeta within
+1e-10 of the reference verification value).
+
+Multi-GPU (torchrun, one rank per GPU): the single system does not shard, so
+each rank solves its own replica (weak scaling, no data-path collective);
+value = all ranks' bytes / the slowest rank's time.
+
+`--impl reference` times the reference's own CPU code (oracle/_ref, the
+reference cg.cu compiled as is: serial, it has no threading) on the same
+metric, rank 0 only.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "npb-gpu_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "SpMV HBM GB/s; time-to-zeta (rel err≤1e-10), learned/mixed vs plain CG"
+CLASS = "B"
+CGITMAX = 25
+CPU_SAMPLE_STEPS = 20     # outer steps in the bounded CPU baseline sample
+REF_STEP_OUTER = 4        # outer steps per reference-arm step
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def spmv_bytes(n, nnz):
+    """FP64 CSR SpMV: 12 B/entry (value + int32 index), row pointers, p once, q once."""
+    return 12 * nnz + 4 * (n + 1) + 8 * n + 8 * n
+
+
+def outer_step_bytes(n, nnz, cgitmax=CGITMAX):
+    """Algorithmic bytes of one outer-step kernel: per CG iteration the SpMV
+    stream plus the fused vector work (p.q, z/r update with r.r, p update:
+    12 nnz + 4(n+1) + 96 n), the residual SpMV with x.z, z.z (12 nnz +
+    4(n+1) + 48 n) and the start of conj_grad (40 n)."""
+    it = 12 * nnz + 4 * (n + 1) + 96 * n
+    res = 12 * nnz + 4 * (n + 1) + 48 * n
+    return cgitmax * it + res + 40 * n
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while timing."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.index)],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        busy = [v for v in sm if mx and v >= 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def physical_index(local_rank):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v.strip() for v in vis.split(",")]
+        if local_rank < len(ids) and ids[local_rank].isdigit():
+            return int(ids[local_rank])
+    return local_rank
+
+
+def load_traffic():
+    """Per-launch DRAM bytes of the outer-step kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic_per_launch.txt")
+    out = {}
+    if os.path.exists(path):
+        for line in open(path):
+            parts = line.split()
+            if len(parts) >= 3 and not line.startswith("#"):
+                try:
+                    out[(parts[0], parts[1])] = float(parts[2])
+                except ValueError:
+                    pass
+    return out
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ CPU arms
+def cpu_reference_run(outer_steps, repeats=1):
+    """Times the reference's own serial CPU conj_grad loop (oracle/_ref)."""
+    from oracle_py import RefLib
+    ref = RefLib(os.path.join(ROOT, "oracle", "_ref", f"libref_{CLASS}.so"))
+    nnz = ref.makea(copy_out=False)
+    times = []
+    for _ in range(repeats):
+        times.append(ref.power(outer_steps)["seconds"])
+    return ref.n, nnz, times
+
+
+def cpu_openmp_run(rowstr, colidx, a, shift, outer_steps, threads):
+    from oracle_py import Oracle
+    o = Oracle(os.path.join(ROOT, "oracle", "liboracle.so"))
+    return o.power_iterate(rowstr, colidx, a, shift, outer_steps, threads=threads)["seconds"]
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    c = CLASSES[CLASS]
+    n, nnz, times = cpu_reference_run(REF_STEP_OUTER, repeats=args.warmup + args.steps)
+    timed = times[args.warmup:]
+    per_step_bytes = REF_STEP_OUTER * (CGITMAX + 1) * spmv_bytes(n, nnz)
+    total = sum(timed)
+    value = per_step_bytes * len(timed) / total / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / len(timed), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference makea, seed 314159265)",
+        "config": {"workload": f"NPB class {CLASS}: n={c['n']} nonzer={c['nonzer']} "
+                               f"shift={c['shift']} rcond=0.1; each step {REF_STEP_OUTER} outer "
+                               f"x (25 CG + residual) FP64 of the 75-step solve",
+                   "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": 1, "kind": "reference",
+                         "sample": f"{REF_STEP_OUTER} outer steps of class {CLASS} per step, "
+                                   "reference cg.cu conj_grad compiled as is (serial)"},
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------- our arm
+CLASSES = None
+
+
+def our_arm(args, rank, world, local_rank):
+    import torch
+    import npbcg
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    else:
+        torch.cuda.set_device(local_rank)
+    device = local_rank
+
+    c = npbcg.CLASSES[CLASS]
+    n, niter, shift = c["n"], c["niter"], c["shift"]
+    rs, ci, a = npbcg.makea(n, c["nonzer"], npbcg.RCOND, shift)
+    nnz = len(a)
+    lib = npbcg.lib()
+
+    # pinned host copies for the end-to-end leg
+    def pinned(arr):
+        p = ctypes.c_void_p()
+        npbcg._check(lib.cgb_host_alloc(ctypes.byref(p), arr.nbytes))
+        buf = (ctypes.c_char * arr.nbytes).from_address(p.value)
+        out = np.frombuffer(buf, dtype=arr.dtype)
+        out[:] = arr
+        return out, p
+
+    h_rs, p_rs = pinned(rs)
+    h_ci, p_ci = pinned(ci)
+    h_a, p_a = pinned(a)
+
+    sess = npbcg.Session(h_rs, h_ci, h_a, device=device)
+    solve_bytes = niter * (CGITMAX + 1) * spmv_bytes(n, nnz)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def reduce_max(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(max(args.warmup, 3)):
+        out = sess.power_iterate(niter, shift)
+
+    # ---- device-resident timed region
+    sampler = ClockSampler(physical_index(local_rank))
+    barrier()
+    sampler.start()
+    dev_ms = []
+    for _ in range(args.steps):
+        out = sess.power_iterate(niter, shift)
+        dev_ms.append(out["device_ms"])
+    barrier()
+    clocks = sampler.stop()
+    total_ms = reduce_max(sum(dev_ms))
+    zeta = float(out["zeta"][-1])
+    zeta_err = abs(zeta - c["zeta"]) / c["zeta"]
+    value = world * args.steps * solve_bytes / (total_ms / 1e3) / 1e9
+    ms_per_step = total_ms / args.steps
+
+    # ---- end to end through the C ABI: H2D of the CSR from pinned memory,
+    # the solve, D2H of the traces and of x, every step
+    h2d = 4 * (n + 1) + 12 * nnz
+    d2h = niter * (8 + 8 + 4) + 8 * n
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sess.upload(h_rs, h_ci, h_a)
+        e2e_out = sess.power_iterate(niter, shift, want_x=True)
+    barrier()
+    e2e_s = reduce_max(time.perf_counter() - t0)
+    e2e_value = world * args.steps * solve_bytes / e2e_s / 1e9
+
+    # ---- roofline of the dominant kernel (the outer-step kernel)
+    per_launch_ms = ms_per_step / niter
+    bytes_launch = outer_step_bytes(n, nnz)
+    achieved = bytes_launch / (per_launch_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = load_traffic().get(("outer_step_fp64", f"class{CLASS}"))
+    kernel_ms, gap_ms = sess.time_outer_steps(niter, shift)
+    spmv_ms = sess.time_spmv(50)
+    spmv_gbs = spmv_bytes(n, nnz) / (spmv_ms / 1e3) / 1e9
+
+    line = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (the reference makea generator, seed 314159265)",
+            "config": {
+                "workload": f"NPB class {CLASS}: n={n} nonzer={c['nonzer']} shift={shift} "
+                            f"rcond=0.1 nnz={nnz}; {niter} outer x ({CGITMAX} CG + residual) FP64, "
+                            "one persistent cooperative kernel per outer step, CUDA graph per solve",
+                "l2": "inputs larger than L2 (CSR 166 MB > 126 MB L2), no flush",
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            },
+            "time_to_zeta_s": ms_per_step / 1e3,
+            "zeta": zeta, "zeta_rel_err": zeta_err,
+            "spmv_standalone": {"ms": spmv_ms, "gbs": spmv_gbs,
+                                "frac_of_peak": spmv_gbs / peak},
+            "outer_step_kernel_ms": kernel_ms, "graph_gap_ms_per_step": gap_ms,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "outer_step_fp64", "peak_source": peak_kind},
+            "clocks": clocks,
+            "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": args.steps * (niter + 1),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            nref, nnz_ref, times = cpu_reference_run(CPU_SAMPLE_STEPS)
+            sample_bytes = CPU_SAMPLE_STEPS * (CGITMAX + 1) * spmv_bytes(nref, nnz_ref)
+            ser = sample_bytes / times[0] / 1e9
+            threads = os.cpu_count() or 1
+            omp_s = cpu_openmp_run(rs, ci, a, shift, CPU_SAMPLE_STEPS, threads)
+            line["cpu_baseline"] = {
+                "value": ser, "unit": "GB/s", "cores": 1, "kind": "reference",
+                "sample": f"{CPU_SAMPLE_STEPS} of {niter} outer steps of class {CLASS}, the "
+                          "reference's serial conj_grad loop (oracle/_ref)",
+                "seconds": times[0],
+                "openmp_port": {"value": sample_bytes / omp_s / 1e9, "unit": "GB/s",
+                                "cores": threads, "kind": "port", "seconds": omp_s},
+            }
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    sess.close()
+    for p in (p_rs, p_ci, p_a):
+        lib.cgb_host_free(p)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    global CLASSES
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    import npbcg
+    CLASSES = npbcg.CLASSES
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    local_rank = env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+    return our_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,163 @@
+/*
+ * cgb.h -- C ABI of libcgb.so, a B200 (sm_100a) implementation of the NPB CG
+ * benchmark's hot path: the makea matrix generator and the inverse power
+ * iteration around conj_grad, from GMAP/NPB-GPU CUDA/CG/cg.cu.
+ *
+ * Conventions
+ *   - Every entry point returns an int status (CGB_OK == 0).  Nothing here
+ *     calls exit(); the reference does (cg.cu:1670-1674, :1748-1751, :1424-1426).
+ *     cgb_last_error() gives a one-line description of the last failure on
+ *     the calling thread.
+ *   - Matrices use the reference's CSR layout: 0-based int32 rowstr[n+1] and
+ *     colidx[nnz], FP64 a[nnz], columns sorted and unique within each row
+ *     (cg.cu:1763-1784).
+ *   - Vectors passed to the conj_grad-compatible call hold at least n+1
+ *     doubles, as the reference's do (cg.cu:105-122, NA+2 entries).
+ *   - A session is bound to one CUDA device and one stream; it is not
+ *     re-entrant: one thread at a time per session.
+ *   - There is no CPU fallback.  Without a usable sm_100 device the solver
+ *     entry points fail with CGB_ERR_NO_DEVICE.  cgb_makea and the option
+ *     helpers are host code and work without a GPU.
+ */
+#ifndef CGB_H
+#define CGB_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define CGB_OK 0
+#define CGB_ERR_INVALID 1     /* bad argument (sizes, seed, null pointer, mode) */
+#define CGB_ERR_NOMEM 2       /* host or device allocation failed */
+#define CGB_ERR_CAPACITY 3    /* caller's output arrays too small (*nnz_out has the need) */
+#define CGB_ERR_CUDA 4        /* a CUDA runtime call failed */
+#define CGB_ERR_TIMEOUT 5     /* a device-side wait hit its limit; the session stays usable */
+#define CGB_ERR_NO_DEVICE 6   /* no CUDA device, or not compute capability 10.x */
+#define CGB_ERR_STATE 7       /* call not valid in the session's current state */
+#define CGB_ERR_NUMERIC 8     /* non-finite value met (NaN/Inf in A or a breakdown) */
+#define CGB_ERR_BAD_MATRIX 9  /* CSR fails validation (rowstr not monotone, col out of range) */
+
+const char *cgb_status_string(int status);
+const char *cgb_last_error(void);
+/* Library version as 10000*major + 100*minor + patch. */
+int cgb_version(void);
+
+/* ------------------------------------------------------------- generator */
+/* Capacity the reference allocates for the CSR arrays: NZ = n*(nonzer+1)^2
+ * (cg.cu:81).  Always >= the nnz cgb_makea produces. */
+long long cgb_nz_bound(int n, int nonzer);
+
+/* Replaces makea() (cg.cu:1303-1368) with sparse() (cg.cu:1611-1785) and the
+ * LCG seeding of main() (cg.cu:404-408): the generator's state starts at
+ * `seed` (314159265.0 for every NPB class), one draw is discarded, then n
+ * sparse vectors are drawn and their scaled outer products summed into A,
+ * with (rcond - shift) added to the diagonal.  Output is bit-identical to the
+ * reference for any odd seed in (1, 2^46).
+ *   rowstr: n+1 ints; colidx, a: nz_capacity entries each.
+ *   *nnz_out receives the stored-entry count (also on CGB_ERR_CAPACITY).
+ * The reference's firstrow/lastrow/firstcol/lastcol arguments are always the
+ * full range (cg.cu:367-370) and its arow/acol/aelt/iv workspaces are
+ * internal here.  Host code; needs no GPU. */
+int cgb_makea(int n, int nonzer, double rcond, double shift, double seed, int *rowstr,
+              int *colidx, double *a, long long nz_capacity, long long *nnz_out);
+
+/* --------------------------------------------------------------- session */
+typedef struct cgb_session cgb_session;
+
+typedef struct cgb_options {
+    int device;               /* CUDA device ordinal (reference: GPU_DEVICE, gpu.config:1) */
+    int lanes_per_row;        /* SpMV lanes per row: 0 = autotuned, else 2, 4, 8, 16 or 32 */
+    int block_threads;        /* threads per CTA of the persistent kernels: 0 = 512 */
+    long long wait_limit_ns;  /* limit of every device-side wait (grid barrier): 0 = 2 s */
+    int use_graph;            /* 1 (default): outer loop replayed as one CUDA graph */
+    int keep_fp32_copy;       /* 1 (default): also hold FP32 values for the mixed mode */
+} cgb_options;
+
+void cgb_default_options(cgb_options *opts);
+
+/* Uploads the CSR (host pointers) and sets the session up (the part of the
+ * reference's setup_gpu that matters, cg.cu:1390-1603).  The matrix is
+ * validated first.  `opts` may be NULL for the defaults. */
+int cgb_create(int n, const int *rowstr, const int *colidx, const double *a,
+               const cgb_options *opts, cgb_session **out);
+
+/* Replaces the session's matrix values/structure with another CSR of the
+ * same order n from host memory (an H2D copy; same validation). */
+int cgb_upload(cgb_session *s, const int *rowstr, const int *colidx, const double *a);
+
+int cgb_destroy(cgb_session *s);
+
+/* Same call surface as the reference conj_grad (cg.cu:225-233, :653-801), on
+ * host pointers: 25 CG iterations on A z = x from z = 0, then
+ * rnorm = ||x - A z||.  On return z, p, q, r hold what the reference leaves
+ * there (r = A z).  If colidx/rowstr/a differ from the arrays the session was
+ * created or last uploaded with, they are uploaded first (n is the
+ * session's).  Vectors: n+1 doubles (entry n copied as the reference sets it). */
+int cgb_conj_grad(cgb_session *s, const int *colidx, const int *rowstr, const double *x,
+                  double *z, const double *a, double *p, double *q, double *r, double *rnorm);
+
+/* ------------------------------------------------------- power iteration */
+#define CGB_MODE_FP64 0         /* reference algorithm: fixed cgitmax FP64 CG steps */
+#define CGB_MODE_FP64_TOL 1     /* FP64 CG stopped at relative residual tol */
+#define CGB_MODE_MIXED 2        /* FP32 SpMV inside FP64 iterative refinement */
+#define CGB_MODE_MIXED_LEARNED 3 /* MIXED + learned preconditioner M = G^T G */
+
+typedef struct cgb_solve_params {
+    int niter;          /* outer steps (reference NITER, setparams.cpp:751-785) */
+    double shift;       /* zeta = shift + 1/(x.z) (cg.cu:513) */
+    int mode;           /* CGB_MODE_* */
+    int cgitmax;        /* inner iterations: exact count in FP64 mode (25 = reference),
+                           the cap in the tolerance modes */
+    double tol;         /* tolerance modes: stop when ||r|| <= tol * ||x|| */
+    int refresh_every;  /* MIXED*: replace r by x - A z in FP64 every k steps (10) */
+    int warm_start;     /* tolerance modes: start from z0 = x/(zeta_prev - shift) */
+} cgb_solve_params;
+
+void cgb_default_solve_params(cgb_solve_params *p);
+
+typedef struct cgb_solve_result {
+    double zeta;          /* final zeta */
+    double rnorm;         /* final ||x - A z|| (FP64) */
+    double device_ms;     /* device time of the whole outer loop (CUDA events) */
+    int total_inner;      /* inner iterations summed over the outer steps */
+    int fallbacks;        /* outer steps that fell back to plain FP64 CG */
+} cgb_solve_result;
+
+/* The reference's timed region (cg.cu:491-522): x = 1, then niter times
+ * { z = conj_grad(x); zeta = shift + 1/(x.z); x = z/||z|| }.  Each trace
+ * (nullable) gets niter entries: zeta, rnorm, inner iterations.  x_out
+ * (nullable) receives the final x (n doubles).  res may be NULL. */
+int cgb_power_iterate(cgb_session *s, const cgb_solve_params *params, double *zeta_trace,
+                      double *rnorm_trace, int *iters_trace, double *x_out,
+                      cgb_solve_result *res);
+
+/* ---------------------------------------------------------- diagnostics */
+/* Time `reps` launches of the standalone FP64 SpMV (q = A p with the p.q
+ * reduction fused, the operation of kernel three + four, cg.cu:937-1004) and
+ * return the mean device milliseconds per launch. */
+int cgb_time_spmv(cgb_session *s, int reps, int fp32, double *ms_per_launch);
+
+/* Per-launch device times of one FP64 outer step kernel, and the gap the
+ * graph adds per outer step: runs `niter` steps with events between the
+ * kernels.  Outputs are means in milliseconds. */
+int cgb_time_outer_steps(cgb_session *s, int niter, double shift, double *kernel_ms,
+                         double *graph_gap_ms);
+
+/* Grid barrier time-out self-test: runs a 2-CTA kernel whose second CTA never
+ * arrives, with a wait limit of `limit_ns`, and reports the status the host
+ * reads back (CGB_ERR_TIMEOUT expected).  The session stays usable. */
+int cgb_selftest_wait_timeout(cgb_session *s, long long limit_ns, int *device_status);
+
+/* Host memory that the device copies at full speed (cudaHostAlloc). */
+int cgb_host_alloc(void **ptr, long long bytes);
+int cgb_host_free(void *ptr);
+
+/* Device count and properties, for drivers and tests. */
+int cgb_device_info(int device, int *sm_count, int *cc_major, int *cc_minor,
+                    long long *global_mem_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CGB_H */

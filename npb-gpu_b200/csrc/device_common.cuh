@@ -1,0 +1,163 @@
+// device_common.cuh -- device building blocks shared by the CG kernels:
+// bounded grid barrier, deterministic block/grid reductions, streaming loads.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cgb {
+
+// Device status word values (first failure wins; 0 = none).
+constexpr int kDevOk = 0;
+constexpr int kDevTimeout = 1;    // a grid-barrier wait ran past its limit
+constexpr int kDevNonFinite = 2;  // a reduction produced NaN/Inf
+constexpr int kDevBadShape = 3;   // launch shape does not match the session
+
+// State of the grid barrier.  count and gen sit on separate 128-byte lines.
+struct GridBarrier {
+    unsigned int *count;  // CTAs arrived in the current generation
+    unsigned int *gen;    // generation; bumped by the last arriver
+    int *status;          // device status word
+    long long limit_ns;   // wait limit per barrier
+};
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned atom_add_acq_rel_u32(unsigned *p, unsigned v)
+{
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;"
+                 : "=r"(old)
+                 : "l"(p), "r"(v)
+                 : "memory");
+    return old;
+}
+
+__device__ __forceinline__ int ld_relaxed_i32(const int *p)
+{
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void raise_status(int *status, int code)
+{
+    atomicCAS(status, kDevOk, code);
+}
+
+// Grid-wide barrier for a co-resident (cooperative) grid.  Thread 0 of each
+// CTA arrives with an acq_rel atomic; the last arriver resets the count and
+// releases the next generation; the others poll the generation with acquire
+// loads, which also makes every write issued before the barrier by any CTA
+// visible after it.  Every wait is bounded: past `limit_ns`, or as soon as
+// another CTA has raised the status word, the barrier records kDevTimeout
+// (first failure wins) and returns false; the caller then leaves the kernel.
+// The host resets count/gen after a failed launch.
+__device__ __forceinline__ bool grid_barrier(const GridBarrier &gb)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned g = ld_acquire_u32(gb.gen);
+        __threadfence();
+        const unsigned arrived = atom_add_acq_rel_u32(gb.count, 1u);
+        if (arrived == gridDim.x - 1) {
+            atomicExch(gb.count, 0u);
+            st_release_u32(gb.gen, g + 1u);
+        } else {
+            const unsigned long long t0 = global_ns();
+            unsigned spins = 0;
+            while (ld_acquire_u32(gb.gen) == g) {
+                if (((++spins) & 63u) == 0u) {
+                    if (ld_relaxed_i32(gb.status) != kDevOk) {
+                        ok = 0;
+                        break;
+                    }
+                    if ((long long)(global_ns() - t0) > gb.limit_ns) {
+                        raise_status(gb.status, kDevTimeout);
+                        ok = 0;
+                        break;
+                    }
+                }
+            }
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+template <int W>
+__device__ __forceinline__ double group_sum(double v, unsigned mask)
+{
+#pragma unroll
+    for (int off = W / 2; off > 0; off >>= 1) v += __shfl_xor_sync(mask, v, off);
+    return v;
+}
+
+template <int W>
+__device__ __forceinline__ float group_sum_f(float v, unsigned mask)
+{
+#pragma unroll
+    for (int off = W / 2; off > 0; off >>= 1) v += __shfl_xor_sync(mask, v, off);
+    return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v) { return group_sum<32>(v, 0xffffffffu); }
+
+// Sum of `v` over the CTA, valid in thread 0.  `scratch` holds >= 32 doubles.
+// Fixed shuffle/smem order: deterministic for a given launch shape.
+__device__ __forceinline__ double block_sum(double v, double *scratch)
+{
+    v = warp_sum(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) scratch[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (w == 0) {
+        s = (l < int(blockDim.x >> 5)) ? scratch[l] : 0.0;
+        s = warp_sum(s);
+    }
+    return s;
+}
+
+// Sum of the `nparts` per-CTA partials at `part`, computed identically by
+// every CTA (same order), returned to all threads through `bcast`.  Reads go
+// to L2 (ld.cg): the partials were written by other SMs during this launch.
+__device__ __forceinline__ double all_partials(const double *part, int nparts, double *bcast)
+{
+    if (threadIdx.x < 32) {
+        double s = 0.0;
+        for (int i = threadIdx.x; i < nparts; i += 32) s += __ldcg(part + i);
+        s = warp_sum(s);
+        if (threadIdx.x == 0) *bcast = s;
+    }
+    __syncthreads();
+    return *bcast;
+}
+
+// Streaming (evict-first) loads for data read once per pass: the matrix.
+__device__ __forceinline__ double2 ld_stream(const double2 *p) { return __ldcs(p); }
+__device__ __forceinline__ int2 ld_stream(const int2 *p) { return __ldcs(p); }
+__device__ __forceinline__ float2 ld_stream(const float2 *p) { return __ldcs(p); }
+
+}  // namespace cgb

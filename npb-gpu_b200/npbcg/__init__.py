@@ -1,0 +1,266 @@
+"""npbcg -- Python binding of libcgb.so, the B200 CG inverse-power-iteration library.
+
+Mirrors the reference's CG call surface (GMAP/NPB-GPU CUDA/CG/cg.cu):
+
+* ``makea(n, nonzer, rcond, shift, seed)`` -> ``(rowstr, colidx, a)``, the
+  reference makea()+sparse() (cg.cu:1303-1368, :1611-1785) seeded as main()
+  does (cg.cu:404-408);
+* ``Session(rowstr, colidx, a)`` holds the matrix on the GPU (setup_gpu,
+  cg.cu:1390-1603);
+* ``Session.conj_grad(x)`` -> ``(z, p, q, r, rnorm)``, the reference
+  conj_grad (cg.cu:653-801);
+* ``Session.power_iterate(niter, shift, ...)`` runs the timed outer loop
+  (cg.cu:491-522) and returns the zeta / rnorm traces.
+
+Errors raise ``CgbError`` carrying the library's status code and message;
+there is no CPU fallback: without libcgb.so or a usable sm_100 GPU the
+solver calls raise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libcgb.so")
+
+# status codes (include/cgb.h)
+OK = 0
+ERR_INVALID = 1
+ERR_NOMEM = 2
+ERR_CAPACITY = 3
+ERR_CUDA = 4
+ERR_TIMEOUT = 5
+ERR_NO_DEVICE = 6
+ERR_STATE = 7
+ERR_NUMERIC = 8
+ERR_BAD_MATRIX = 9
+
+MODE_FP64 = 0
+MODE_FP64_TOL = 1
+MODE_MIXED = 2
+MODE_MIXED_LEARNED = 3
+
+# NPB classes (setparams.cpp:751-785) and their verification zetas (cg.cu:373-396)
+CLASSES = {
+    "S": dict(n=1400, nonzer=7, niter=15, shift=10.0, zeta=8.5971775078648),
+    "W": dict(n=7000, nonzer=8, niter=15, shift=12.0, zeta=10.362595087124),
+    "A": dict(n=14000, nonzer=11, niter=15, shift=20.0, zeta=17.130235054029),
+    "B": dict(n=75000, nonzer=13, niter=75, shift=60.0, zeta=22.712745482631),
+    "C": dict(n=150000, nonzer=15, niter=75, shift=110.0, zeta=28.973605592845),
+}
+RCOND = 0.1
+SEED = 314159265.0
+VERIFY_EPSILON = 1.0e-10
+
+
+class CgbError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("lanes_per_row", ctypes.c_int),
+                ("block_threads", ctypes.c_int), ("wait_limit_ns", ctypes.c_longlong),
+                ("use_graph", ctypes.c_int), ("keep_fp32_copy", ctypes.c_int)]
+
+
+class SolveParams(ctypes.Structure):
+    _fields_ = [("niter", ctypes.c_int), ("shift", ctypes.c_double), ("mode", ctypes.c_int),
+                ("cgitmax", ctypes.c_int), ("tol", ctypes.c_double),
+                ("refresh_every", ctypes.c_int), ("warm_start", ctypes.c_int)]
+
+
+class SolveResult(ctypes.Structure):
+    _fields_ = [("zeta", ctypes.c_double), ("rnorm", ctypes.c_double),
+                ("device_ms", ctypes.c_double), ("total_inner", ctypes.c_int),
+                ("fallbacks", ctypes.c_int)]
+
+
+_I32 = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_F64 = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_lib = None
+
+# every symbol include/cgb.h declares, with its ctypes signature
+_SIGNATURES = {
+    "cgb_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "cgb_last_error": (ctypes.c_char_p, []),
+    "cgb_version": (ctypes.c_int, []),
+    "cgb_nz_bound": (ctypes.c_longlong, [ctypes.c_int, ctypes.c_int]),
+    "cgb_makea": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_double, _I32, _I32, _F64, ctypes.c_longlong,
+                                 ctypes.POINTER(ctypes.c_longlong)]),
+    "cgb_default_options": (None, [ctypes.POINTER(Options)]),
+    "cgb_create": (ctypes.c_int, [ctypes.c_int, _I32, _I32, _F64, ctypes.POINTER(Options),
+                                  ctypes.POINTER(ctypes.c_void_p)]),
+    "cgb_upload": (ctypes.c_int, [ctypes.c_void_p, _I32, _I32, _F64]),
+    "cgb_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "cgb_conj_grad": (ctypes.c_int, [ctypes.c_void_p, _I32, _I32, _F64, _F64, _F64, _F64, _F64,
+                                     _F64, ctypes.POINTER(ctypes.c_double)]),
+    "cgb_default_solve_params": (None, [ctypes.POINTER(SolveParams)]),
+    "cgb_power_iterate": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SolveParams),
+                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.POINTER(SolveResult)]),
+    "cgb_time_spmv": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_double)]),
+    "cgb_time_outer_steps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
+                                            ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_double)]),
+    "cgb_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong,
+                                                 ctypes.POINTER(ctypes.c_int)]),
+    "cgb_host_alloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_longlong]),
+    "cgb_host_free": (ctypes.c_int, [ctypes.c_void_p]),
+    "cgb_device_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_longlong)]),
+}
+
+
+def lib():
+    """Load libcgb.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise CgbError(ERR_STATE, f"{LIB_PATH} is missing: run npb-gpu_b200/build.py")
+        handle = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def _check(status):
+    if status != OK:
+        msg = lib().cgb_last_error().decode(errors="replace")
+        raise CgbError(status, msg or lib().cgb_status_string(status).decode())
+
+
+def _ptr(arr):
+    return None if arr is None else arr.ctypes.data_as(ctypes.c_void_p)
+
+
+def nz_bound(n, nonzer):
+    return int(lib().cgb_nz_bound(n, nonzer))
+
+
+def makea(n, nonzer, rcond=RCOND, shift=10.0, seed=SEED):
+    """The reference matrix: returns (rowstr int32[n+1], colidx int32[nnz], a float64[nnz])."""
+    cap = nz_bound(n, nonzer)
+    rowstr = np.zeros(n + 1, np.int32)
+    colidx = np.zeros(max(cap, 1), np.int32)
+    a = np.zeros(max(cap, 1), np.float64)
+    nnz = ctypes.c_longlong(0)
+    _check(lib().cgb_makea(n, nonzer, rcond, shift, seed, rowstr, colidx, a, cap,
+                           ctypes.byref(nnz)))
+    k = nnz.value
+    return rowstr, colidx[:k].copy(), a[:k].copy()
+
+
+def device_info(device=0):
+    sm, ma, mi, mem = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+    _check(lib().cgb_device_info(device, ctypes.byref(sm), ctypes.byref(ma), ctypes.byref(mi),
+                                 ctypes.byref(mem)))
+    return dict(sm_count=sm.value, cc=(ma.value, mi.value), global_mem=mem.value)
+
+
+def default_options(**kw):
+    o = Options()
+    lib().cgb_default_options(ctypes.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Session:
+    """A matrix resident on one GPU (the reference's setup_gpu state)."""
+
+    def __init__(self, rowstr, colidx, a, **options):
+        self.n = int(len(rowstr) - 1)
+        self._keep = (np.ascontiguousarray(rowstr, np.int32),
+                      np.ascontiguousarray(colidx, np.int32),
+                      np.ascontiguousarray(a, np.float64))
+        opts = default_options(**options)
+        h = ctypes.c_void_p()
+        _check(lib().cgb_create(self.n, *self._keep, ctypes.byref(opts), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cgb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def upload(self, rowstr, colidx, a):
+        self._keep = (np.ascontiguousarray(rowstr, np.int32),
+                      np.ascontiguousarray(colidx, np.int32),
+                      np.ascontiguousarray(a, np.float64))
+        _check(lib().cgb_upload(self._h, *self._keep))
+
+    def conj_grad(self, x):
+        """One reference conj_grad from z = 0; returns (z, p, q, r, rnorm), n+1 entries each."""
+        n = self.n
+        xv = np.ones(n + 1, np.float64)
+        xv[: min(len(x), n + 1)] = np.asarray(x, np.float64)[: n + 1]
+        z, p, q, r = (np.zeros(n + 1) for _ in range(4))
+        rn = ctypes.c_double()
+        rowstr, colidx, a = self._keep
+        _check(lib().cgb_conj_grad(self._h, colidx, rowstr, xv, z, a, p, q, r, ctypes.byref(rn)))
+        return z, p, q, r, rn.value
+
+    def power_iterate(self, niter, shift, mode=MODE_FP64, cgitmax=25, tol=1e-12,
+                      refresh_every=10, warm_start=False, want_x=False):
+        """The outer loop of cg.cu:500-520; returns a dict with traces and timings."""
+        P = SolveParams()
+        lib().cgb_default_solve_params(ctypes.byref(P))
+        P.niter, P.shift, P.mode, P.cgitmax = niter, shift, mode, cgitmax
+        P.tol, P.refresh_every, P.warm_start = tol, refresh_every, int(bool(warm_start))
+        zt, rt = np.zeros(niter), np.zeros(niter)
+        it = np.zeros(niter, np.int32)
+        x = np.zeros(self.n) if want_x else None
+        res = SolveResult()
+        _check(lib().cgb_power_iterate(self._h, ctypes.byref(P), _ptr(zt), _ptr(rt), _ptr(it),
+                                       _ptr(x), ctypes.byref(res)))
+        out = dict(zeta=zt, rnorm=rt, iters=it, device_ms=res.device_ms,
+                   total_inner=res.total_inner, fallbacks=res.fallbacks)
+        if want_x:
+            out["x"] = x
+        return out
+
+    def time_spmv(self, reps=50, fp32=False):
+        ms = ctypes.c_double()
+        _check(lib().cgb_time_spmv(self._h, reps, int(fp32), ctypes.byref(ms)))
+        return ms.value
+
+    def time_outer_steps(self, niter, shift):
+        k, g = ctypes.c_double(), ctypes.c_double()
+        _check(lib().cgb_time_outer_steps(self._h, niter, shift, ctypes.byref(k), ctypes.byref(g)))
+        return k.value, g.value
+
+    def selftest_wait_timeout(self, limit_ns):
+        """Returns (status, device_status) of the bounded-wait self-test."""
+        dev = ctypes.c_int()
+        st = lib().cgb_selftest_wait_timeout(self._h, limit_ns, ctypes.byref(dev))
+        return st, dev.value
+
+
+def spmv_bytes_fp64(n, nnz):
+    """Algorithmic bytes of one FP64 CSR SpMV: values + indices + row pointers + p + q."""
+    return 12 * nnz + 4 * (n + 1) + 8 * n + 8 * n
+
+
+def spmv_bytes_fp32(n, nnz):
+    return 8 * nnz + 4 * (n + 1) + 4 * n + 4 * n

@@ -1,0 +1,125 @@
+"""ctypes handle on the CPU oracle (oracle/liboracle.so) and the reference
+libraries (oracle/_ref/libref_<class>.so).  Test infrastructure only."""
+import ctypes
+import os
+
+import numpy as np
+
+I32 = np.ctypeslib.ndpointer(np.int32, flags="C")
+F64 = np.ctypeslib.ndpointer(np.float64, flags="C")
+
+
+class Oracle:
+    def __init__(self, path):
+        lib = ctypes.CDLL(path)
+        lib.orc_randlc.restype = ctypes.c_double
+        lib.orc_randlc.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.c_double]
+        lib.orc_nz_bound.restype = ctypes.c_longlong
+        lib.orc_nz_bound.argtypes = [ctypes.c_int, ctypes.c_int]
+        lib.orc_makea.restype = ctypes.c_int
+        lib.orc_makea.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, I32, I32, F64, ctypes.c_longlong,
+                                  ctypes.POINTER(ctypes.c_longlong)]
+        lib.orc_csr_hash.restype = ctypes.c_uint64
+        lib.orc_csr_hash.argtypes = [ctypes.c_int, I32, I32, F64]
+        lib.orc_spmv.restype = None
+        lib.orc_spmv.argtypes = [ctypes.c_int, I32, I32, F64, F64, F64]
+        lib.orc_conj_grad.restype = None
+        lib.orc_conj_grad.argtypes = [ctypes.c_int, I32, I32, F64, F64, F64, F64, F64, F64,
+                                      ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        lib.orc_power_iterate.restype = ctypes.c_int
+        lib.orc_power_iterate.argtypes = [ctypes.c_int, I32, I32, F64, ctypes.c_double,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.POINTER(ctypes.c_double)]
+        lib.orc_max_threads.restype = ctypes.c_int
+        self.lib = lib
+
+    def makea(self, n, nonzer, rcond, shift, seed=314159265.0):
+        cap = self.lib.orc_nz_bound(n, nonzer)
+        rs = np.zeros(n + 1, np.int32)
+        ci = np.zeros(cap, np.int32)
+        a = np.zeros(cap)
+        nnz = ctypes.c_longlong()
+        rc = self.lib.orc_makea(n, nonzer, rcond, shift, seed, rs, ci, a, cap, ctypes.byref(nnz))
+        if rc != 0:
+            raise RuntimeError(f"orc_makea failed: {rc}")
+        k = nnz.value
+        return rs, ci[:k].copy(), a[:k].copy()
+
+    def csr_hash(self, rowstr, colidx, a):
+        n = len(rowstr) - 1
+        return "%016x" % self.lib.orc_csr_hash(n, np.ascontiguousarray(rowstr, np.int32),
+                                                np.ascontiguousarray(colidx, np.int32),
+                                                np.ascontiguousarray(a, np.float64))
+
+    def spmv(self, rowstr, colidx, a, x):
+        n = len(rowstr) - 1
+        y = np.zeros(n)
+        self.lib.orc_spmv(n, rowstr, colidx, a, np.ascontiguousarray(x, np.float64), y)
+        return y
+
+    def conj_grad(self, rowstr, colidx, a, x, cgitmax=25):
+        n = len(rowstr) - 1
+        xv = np.ones(n + 2)
+        xv[:n] = x[:n]
+        z, p, q, r = (np.zeros(n + 2) for _ in range(4))
+        rn = ctypes.c_double()
+        self.lib.orc_conj_grad(n, rowstr, colidx, a, xv, z, p, q, r, cgitmax, ctypes.byref(rn))
+        return z[: n + 1], p[: n + 1], q[: n + 1], r[: n + 1], rn.value
+
+    def power_iterate(self, rowstr, colidx, a, shift, niter, cgitmax=25, threads=1):
+        n = len(rowstr) - 1
+        zt, rt, x = np.zeros(niter), np.zeros(niter), np.zeros(n)
+        secs = ctypes.c_double()
+        rc = self.lib.orc_power_iterate(n, rowstr, colidx, a, shift, niter, cgitmax, threads,
+                                        zt.ctypes.data, rt.ctypes.data, x.ctypes.data,
+                                        ctypes.byref(secs))
+        if rc != 0:
+            raise RuntimeError(f"orc_power_iterate failed: {rc}")
+        return dict(zeta=zt, rnorm=rt, x=x, seconds=secs.value)
+
+
+class RefLib:
+    """The reference's own CG code for one NPB class (oracle/_ref)."""
+
+    def __init__(self, path):
+        lib = ctypes.CDLL(path)
+        lib.ref_info.argtypes = [ctypes.POINTER(ctypes.c_int)] * 3 + [
+            ctypes.POINTER(ctypes.c_double)] * 2 + [ctypes.POINTER(ctypes.c_longlong)]
+        lib.ref_makea.argtypes = [ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                                  ctypes.c_void_p]
+        lib.ref_makea.restype = ctypes.c_int
+        lib.ref_power.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        lib.ref_power.restype = ctypes.c_double
+        lib.ref_conj_grad.argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_void_p]
+        lib.ref_conj_grad.restype = ctypes.c_int
+        na, nz, ni = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        sh, rc, bound = ctypes.c_double(), ctypes.c_double(), ctypes.c_longlong()
+        lib.ref_info(ctypes.byref(na), ctypes.byref(nz), ctypes.byref(ni), ctypes.byref(sh),
+                     ctypes.byref(rc), ctypes.byref(bound))
+        self.n, self.nonzer, self.niter = na.value, nz.value, ni.value
+        self.shift, self.rcond, self.nz_bound = sh.value, rc.value, bound.value
+        self.lib = lib
+
+    def makea(self, seed=314159265.0, copy_out=True):
+        if not copy_out:
+            return self.lib.ref_makea(seed, None, None, None)
+        rs = np.zeros(self.n + 1, np.int32)
+        ci = np.zeros(self.nz_bound, np.int32)
+        a = np.zeros(self.nz_bound)
+        nnz = self.lib.ref_makea(seed, rs.ctypes.data, ci.ctypes.data, a.ctypes.data)
+        return rs, ci[:nnz].copy(), a[:nnz].copy()
+
+    def power(self, niter):
+        zt, rt = np.zeros(niter), np.zeros(niter)
+        secs = self.lib.ref_power(niter, zt.ctypes.data, rt.ctypes.data)
+        return dict(zeta=zt, rnorm=rt, seconds=secs)
+
+    def conj_grad(self, x):
+        n = self.n
+        z, r, p, q = (np.zeros(n) for _ in range(4))
+        rn = np.zeros(1)
+        self.lib.ref_conj_grad(np.ascontiguousarray(x, np.float64).ctypes.data, z.ctypes.data,
+                               r.ctypes.data, p.ctypes.data, q.ctypes.data, rn.ctypes.data)
+        return z, p, q, r, float(rn[0])

@@ -1,0 +1,183 @@
+"""GPU parity of the FP64 CG path through the C ABI (libcgb.so).
+
+Compared with the reference's own outputs (tests/golden, oracle/_ref) and
+the CPU oracle.  Tolerances:
+  * zeta: relative 1e-10, the reference's verification epsilon (cg.cu:534-537);
+  * rnorm: absolute 1e-10 * ||x|| (rnorm itself is roundoff, ~1e-13);
+  * vectors after one conj_grad: relative 1e-12 of the vector norm (the GPU
+    sums in a different order and with FMA).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ref_lib_path
+
+pytestmark = pytest.mark.gpu
+
+PARAMS = {"S": (1400, 7, 15, 10.0), "W": (7000, 8, 15, 12.0), "A": (14000, 11, 15, 20.0),
+          "B": (75000, 13, 75, 60.0), "C": (150000, 15, 75, 110.0)}
+VERIFY = {"S": 8.5971775078648, "W": 10.362595087124, "A": 17.130235054029,
+          "B": 22.712745482631, "C": 28.973605592845}
+
+
+def session_for(cgb, cls, seed=314159265.0, **opts):
+    n, nonzer, niter, shift = PARAMS[cls]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift, seed)
+    return cgb.Session(rs, ci, a, **opts), (rs, ci, a)
+
+
+def test_device_is_b200_class(cgb):
+    info = cgb.device_info(0)
+    assert info["cc"][0] == 10
+    assert info["sm_count"] >= 100
+
+
+def test_conj_grad_matches_reference_fixture(cgb):
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "conj_grad_S.npz"))
+    s, (rs, ci, a) = session_for(cgb, "S")
+    n = PARAMS["S"][0]
+    z, p, q, r, rn = s.conj_grad(np.ones(n))
+    for name, got in (("z", z), ("p", p), ("q", q), ("r", r)):
+        want = g[name]
+        err = np.linalg.norm(got[:n] - want) / np.linalg.norm(want)
+        assert err <= 1e-12, (name, err)
+    assert abs(rn - g["rnorm"][0]) <= 1e-10
+    # entry n, as the reference leaves it (cg.cu:670-675)
+    assert z[n] == 0.0 and q[n] == 0.0 and r[n] == 1.0 and p[n] == 1.0
+
+
+@pytest.mark.parametrize("cls", ["S", "W", "A", "B"])
+def test_power_iterate_matches_reference(cgb, golden, cls):
+    n, nonzer, niter, shift = PARAMS[cls]
+    e = golden[cls]["seeds"]["314159265.0"]
+    s, _ = session_for(cgb, cls)
+    out = s.power_iterate(niter, shift)
+    zeta = out["zeta"]
+    ref_zeta = np.array(e["zeta"])
+    assert np.max(np.abs(zeta - ref_zeta) / np.abs(ref_zeta)) <= 1e-10
+    assert np.max(np.abs(out["rnorm"] - np.array(e["rnorm"]))) <= 1e-10
+    assert abs(zeta[-1] - VERIFY[cls]) / VERIFY[cls] <= 1e-10
+    assert np.all(out["iters"] == 25)
+    assert out["device_ms"] > 0
+
+
+@pytest.mark.slow
+def test_power_iterate_class_c(cgb):
+    n, nonzer, niter, shift = PARAMS["C"]
+    s, _ = session_for(cgb, "C")
+    out = s.power_iterate(niter, shift)
+    assert abs(out["zeta"][-1] - VERIFY["C"]) / VERIFY["C"] <= 1e-10
+
+
+def test_other_seeds_match_reference(cgb, golden):
+    for cls in ("S", "A"):
+        n, nonzer, niter, shift = PARAMS[cls]
+        for key, e in golden[cls]["seeds"].items():
+            s, _ = session_for(cgb, cls, seed=e["seed"])
+            out = s.power_iterate(niter, shift)
+            ref = np.array(e["zeta"])
+            assert np.max(np.abs(out["zeta"] - ref) / np.abs(ref)) <= 1e-10
+
+
+@pytest.mark.parametrize("lpr", [2, 4, 8, 16, 32])
+def test_lane_counts_agree(cgb, golden, lpr):
+    n, nonzer, niter, shift = PARAMS["W"]
+    s, _ = session_for(cgb, "W", lanes_per_row=lpr)
+    out = s.power_iterate(niter, shift)
+    ref = np.array(golden["W"]["seeds"]["314159265.0"]["zeta"])
+    assert np.max(np.abs(out["zeta"] - ref) / np.abs(ref)) <= 1e-10
+
+
+def test_graph_and_direct_launch_agree_bitwise(cgb):
+    n, nonzer, niter, shift = PARAMS["S"]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    g = cgb.Session(rs, ci, a, use_graph=1).power_iterate(niter, shift, want_x=True)
+    d = cgb.Session(rs, ci, a, use_graph=0).power_iterate(niter, shift, want_x=True)
+    assert np.array_equal(g["zeta"], d["zeta"])
+    assert np.array_equal(g["x"], d["x"])
+
+
+def test_repeatable_bitwise(cgb):
+    s, _ = session_for(cgb, "A")
+    n, nonzer, niter, shift = PARAMS["A"]
+    a1 = s.power_iterate(niter, shift, want_x=True)
+    a2 = s.power_iterate(niter, shift, want_x=True)
+    assert np.array_equal(a1["zeta"], a2["zeta"]) and np.array_equal(a1["x"], a2["x"])
+
+
+def test_conj_grad_against_reference_library(cgb, oracle):
+    path = ref_lib_path("S")
+    if not os.path.exists(path):
+        pytest.skip("oracle/_ref not built")
+    from oracle_py import RefLib
+    ref = RefLib(path)
+    n = ref.n
+    rs, ci, a = ref.makea(123456789.0)
+    s = cgb.Session(rs, ci, a)
+    x = np.cos(np.arange(n) * 0.37) + 1.5
+    zr, pr, qr, rr, rnr = ref.conj_grad(x)
+    z, p, q, r, rn = s.conj_grad(x)
+    assert np.linalg.norm(z[:n] - zr) <= 1e-12 * np.linalg.norm(zr)
+    assert np.linalg.norm(r[:n] - rr) <= 1e-12 * np.linalg.norm(rr)
+    assert abs(rn - rnr) <= 1e-10 * np.linalg.norm(x)
+
+
+def test_conj_grad_reuploads_changed_matrix(cgb, oracle):
+    n, nonzer, _, shift = PARAMS["S"]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    s = cgb.Session(rs, ci, a)
+    rs2, ci2, a2 = cgb.makea(n, nonzer, 0.1, shift, 271828183.0)
+    s.upload(rs2, ci2, a2)
+    z, *_ , rn = s.conj_grad(np.ones(n))
+    zo, *_ = oracle.conj_grad(rs2, ci2, a2, np.ones(n))
+    assert np.linalg.norm(z[:n] - zo[:n]) <= 1e-12 * np.linalg.norm(zo[:n])
+
+
+def test_tolerance_mode_reaches_reference_zeta(cgb, golden):
+    n, nonzer, niter, shift = PARAMS["A"]
+    s, _ = session_for(cgb, "A")
+    for warm in (False, True):
+        out = s.power_iterate(niter, shift, mode=cgb.MODE_FP64_TOL, tol=1e-12, cgitmax=60,
+                              warm_start=warm)
+        assert abs(out["zeta"][-1] - VERIFY["A"]) / VERIFY["A"] <= 1e-10
+        assert out["total_inner"] < 25 * niter
+
+
+def test_tiny_and_ragged_systems(cgb, oracle):
+    """Edge shapes: fewer rows than CTAs, rows of very uneven length."""
+    for n, nonzer, shift in ((40, 3, 2.0), (300, 2, 3.0), (1500, 20, 30.0)):
+        rs, ci, a = cgb.makea(n, nonzer, 0.1, shift, 271828183.0)
+        s = cgb.Session(rs, ci, a)
+        out = s.power_iterate(5, shift)
+        ref = oracle.power_iterate(rs, ci, a, shift, 5)
+        assert np.max(np.abs(out["zeta"] - ref["zeta"]) / np.abs(ref["zeta"])) <= 1e-10
+
+
+def test_empty_rows_handled(cgb):
+    """A CSR with empty rows (the generator never makes one) still solves."""
+    import scipy.sparse as sp
+    n = 64
+    d = -np.linspace(2.0, 3.0, n)
+    d[::7] = -1.0
+    A = sp.diags(d).tocsr()
+    rs, ci, a = A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data
+    s = cgb.Session(rs, ci, a)
+    z, p, q, r, rn = s.conj_grad(np.ones(n))
+    assert np.allclose(z[:n], 1.0 / d, rtol=1e-14)
+
+
+def test_wait_timeout_selftest_leaves_session_usable(cgb):
+    s, _ = session_for(cgb, "S")
+    st, dev = s.selftest_wait_timeout(50_000_000)  # 50 ms limit on a wait nobody ends
+    assert st == cgb.ERR_TIMEOUT and dev == 1
+    n, nonzer, niter, shift = PARAMS["S"]
+    out = s.power_iterate(niter, shift)
+    assert abs(out["zeta"][-1] - VERIFY["S"]) / VERIFY["S"] <= 1e-10
+
+
+def test_spmv_timer_runs(cgb):
+    s, _ = session_for(cgb, "A")
+    ms = s.time_spmv(5)
+    assert 0 < ms < 50
