@@ -20,6 +20,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["session.cu"]
 CPP_SOURCES = ["makea.cpp"]
 LIB = os.path.join(LIBDIR, "libcgb.so")
+BINDIR = os.path.join(HERE, "bin")
+DRIVER = os.path.join(BINDIR, "cg")
 
 
 def nvcc():
@@ -77,6 +79,12 @@ def build(verbose=False, ptxas_info=False, force=False):
     if force or sources_newer(LIB, objs):
         run([nvcc(), "-shared", "-o", LIB, *objs, *ARCH, "-cudart", "static",
              "-Xcompiler", "-pthread", "-lpthread"], verbose)
+    # the NPB-style command-line driver, linked against libcgb.so
+    os.makedirs(BINDIR, exist_ok=True)
+    main_src = os.path.join(CSRC, "cg_main.cpp")
+    if force or sources_newer(DRIVER, [main_src, LIB] + headers):
+        run([nvcc(), "-O2", "-std=c++17", "-o", DRIVER, main_src, "-L" + LIBDIR, "-lcgb",
+             "-Xlinker", "-rpath=$ORIGIN/../lib"], verbose)
     return LIB
 
 

@@ -1,0 +1,205 @@
+// cg_main.cpp -- `cg`, a drop-in for the reference benchmark binary cg.<CLASS>
+// (GMAP/NPB-GPU CUDA/CG/cg.cu main(), :337-645) on top of libcgb's C ABI.
+//
+//   cg S|W|A|B|C            an NPB class (setparams.cpp:751-785 parameters)
+//   cg U --n N --nonzer K --niter I --shift S [--seed X]   custom sizes
+//   options: --mode fp64|tol|mixed|learned  --tol T  --cgitmax M  --warm
+//            --device D  --json (one JSON result line instead of the report)
+//
+// Like the reference it generates the matrix (makea), runs the timed inverse
+// power iteration, prints the per-iteration "||r||  zeta" lines in the
+// reference format (cg.cu:515-516), verifies zeta against the class's value
+// at relative 1e-10 (cg.cu:534-552), and reports time and Mop/s with the
+// reference's operation count (cg.cu:553-561).  The timed region is the
+// device time of the outer loop; matrix generation and upload are outside
+// it, as in the reference (cg.cu:490-522).
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cgb.h"
+
+namespace {
+
+struct ClassParams {
+    char name;
+    int n, nonzer, niter;
+    double shift, zeta_verify;
+};
+
+// NPB CG classes and verification zetas (cg.cu:373-396).
+const ClassParams kClasses[] = {
+    {'S', 1400, 7, 15, 10.0, 8.5971775078648},
+    {'W', 7000, 8, 15, 12.0, 10.362595087124},
+    {'A', 14000, 11, 15, 20.0, 17.130235054029},
+    {'B', 75000, 13, 75, 60.0, 22.712745482631},
+    {'C', 150000, 15, 75, 110.0, 28.973605592845},
+    {'D', 1500000, 21, 100, 500.0, 52.514532105794},
+};
+
+int fail(int st, const char *what)
+{
+    std::fprintf(stderr, "cg: %s failed: %s (%s)\n", what, cgb_status_string(st), cgb_last_error());
+    return 1;
+}
+
+void usage()
+{
+    std::fprintf(stderr,
+                 "usage: cg S|W|A|B|C|D | cg U --n N --nonzer K --niter I --shift S [--seed X]\n"
+                 "          [--mode fp64|tol|mixed|learned] [--tol T] [--cgitmax M] [--warm]\n"
+                 "          [--device D] [--json]\n");
+}
+
+}  // namespace
+
+int main(int argc, char **argv)
+{
+    if (argc < 2) {
+        usage();
+        return 2;
+    }
+    ClassParams P{'U', 0, 0, 0, 0.0, 0.0};
+    const char cls = argv[1][0];
+    bool known = false;
+    for (const auto &c : kClasses)
+        if (c.name == cls) {
+            P = c;
+            known = true;
+        }
+    if (!known && cls != 'U') {
+        usage();
+        return 2;
+    }
+    double seed = 314159265.0, tol = 1e-12;
+    int mode = CGB_MODE_FP64, cgitmax = 25, device = 0, warm = 0, json = 0;
+    for (int i = 2; i < argc; i++) {
+        const std::string a = argv[i];
+        auto next = [&](void) -> const char * {
+            if (i + 1 >= argc) {
+                usage();
+                std::exit(2);
+            }
+            return argv[++i];
+        };
+        if (a == "--n") P.n = std::atoi(next());
+        else if (a == "--nonzer") P.nonzer = std::atoi(next());
+        else if (a == "--niter") P.niter = std::atoi(next());
+        else if (a == "--shift") P.shift = std::atof(next());
+        else if (a == "--seed") seed = std::atof(next());
+        else if (a == "--tol") tol = std::atof(next());
+        else if (a == "--cgitmax") cgitmax = std::atoi(next());
+        else if (a == "--device") device = std::atoi(next());
+        else if (a == "--warm") warm = 1;
+        else if (a == "--json") json = 1;
+        else if (a == "--mode") {
+            const std::string m = next();
+            if (m == "fp64") mode = CGB_MODE_FP64;
+            else if (m == "tol") mode = CGB_MODE_FP64_TOL;
+            else if (m == "mixed") mode = CGB_MODE_MIXED;
+            else if (m == "learned") mode = CGB_MODE_MIXED_LEARNED;
+            else {
+                usage();
+                return 2;
+            }
+        } else {
+            usage();
+            return 2;
+        }
+    }
+    if (P.n < 2 || P.nonzer < 1 || P.niter < 1) {
+        usage();
+        return 2;
+    }
+    // a custom size or another seed has no verification value (cg.cu:548-551)
+    const bool verify = known && seed == 314159265.0;
+
+    const long long cap = cgb_nz_bound(P.n, P.nonzer);
+    std::vector<int> rowstr(P.n + 1), colidx(cap);
+    std::vector<double> a(cap);
+    long long nnz = 0;
+    int st = cgb_makea(P.n, P.nonzer, 0.1, P.shift, seed, rowstr.data(), colidx.data(), a.data(),
+                       cap, &nnz);
+    if (st) return fail(st, "makea");
+
+    cgb_options opt;
+    cgb_default_options(&opt);
+    opt.device = device;
+    cgb_session *s = nullptr;
+    st = cgb_create(P.n, rowstr.data(), colidx.data(), a.data(), &opt, &s);
+    if (st) return fail(st, "create");
+
+    cgb_solve_params sp;
+    cgb_default_solve_params(&sp);
+    sp.niter = P.niter;
+    sp.shift = P.shift;
+    sp.mode = mode;
+    sp.cgitmax = cgitmax;
+    sp.tol = tol;
+    sp.warm_start = warm;
+    // one untimed solve first, as the reference does one untimed iteration (cg.cu:453-482)
+    cgb_solve_result res;
+    st = cgb_power_iterate(s, &sp, nullptr, nullptr, nullptr, nullptr, &res);
+    if (st) return fail(st, "power_iterate (warm-up)");
+    std::vector<double> zeta(P.niter), rnorm(P.niter);
+    std::vector<int> iters(P.niter);
+    st = cgb_power_iterate(s, &sp, zeta.data(), rnorm.data(), iters.data(), nullptr, &res);
+    if (st) return fail(st, "power_iterate");
+    cgb_destroy(s);
+
+    const double t = res.device_ms / 1e3;
+    const double nz1 = double(P.nonzer) * (P.nonzer + 1);
+    const double mops =
+        t > 0 ? 2.0 * P.niter * P.n * (3.0 + nz1 + 25.0 * (5.0 + nz1) + 3.0) / t / 1e6 : 0.0;
+    const double err = verify ? std::fabs(res.zeta - P.zeta_verify) / P.zeta_verify : -1.0;
+    const bool ok = verify && err <= 1.0e-10;
+
+    if (json) {
+        std::printf("{\"class\": \"%c\", \"n\": %d, \"nonzer\": %d, \"niter\": %d, \"shift\": %.17g, "
+                    "\"nnz\": %lld, \"mode\": %d, \"zeta\": %.17g, \"rnorm\": %.17g, "
+                    "\"seconds\": %.9g, \"mops\": %.6g, \"inner_total\": %d, \"verified\": %s, "
+                    "\"rel_err\": %.6g}\n",
+                    P.name, P.n, P.nonzer, P.niter, P.shift, nnz, mode, res.zeta, res.rnorm, t,
+                    mops, res.total_inner, verify ? (ok ? "true" : "false") : "null", err);
+        return verify && !ok ? 1 : 0;
+    }
+    std::printf("\n\n NAS Parallel Benchmarks 4.1 - CG Benchmark (B200 sm_100a build)\n\n");
+    std::printf(" Size: %11d\n", P.n);
+    std::printf(" Iterations: %5d\n", P.niter);
+    std::printf("\n   iteration           ||r||                 zeta\n");
+    for (int it = 0; it < P.niter; it++)
+        std::printf("    %5d       %20.14e%20.13e\n", it + 1, rnorm[it], zeta[it]);
+    std::printf(" Benchmark completed\n");
+    if (verify) {
+        if (ok) {
+            std::printf(" VERIFICATION SUCCESSFUL\n");
+            std::printf(" Zeta is    %20.13e\n", res.zeta);
+            std::printf(" Error is   %20.13e\n", err);
+        } else {
+            std::printf(" VERIFICATION FAILED\n");
+            std::printf(" Zeta                %20.13e\n", res.zeta);
+            std::printf(" The correct zeta is %20.13e\n", P.zeta_verify);
+        }
+    } else {
+        std::printf(" Problem size unknown\n");
+        std::printf(" NO VERIFICATION PERFORMED\n");
+    }
+    static const char *mode_names[] = {"FP64 fixed", "FP64 tolerance", "FP32 SpMV + FP64 refinement",
+                                       "mixed + learned preconditioner"};
+    std::printf("\n\n CG Benchmark Completed\n");
+    std::printf(" class_npb       =                        %c\n", P.name);
+    std::printf(" Size            =             %12d\n", P.n);
+    std::printf(" Iterations      =             %12d\n", P.niter);
+    std::printf(" Time in seconds =             %12.6f\n", t);
+    std::printf(" Mop/s total     =             %12.2f\n", mops);
+    std::printf(" Operation type  = %24s\n", "floating point");
+    if (!verify) std::printf(" Verification    =            NOT PERFORMED\n");
+    else std::printf(" Verification    =             %12s\n", ok ? "SUCCESSFUL" : "UNSUCCESSFUL");
+    std::printf(" Mode            = %s\n", mode_names[mode & 3]);
+    std::printf(" Inner CG steps  =             %12d\n", res.total_inner);
+    std::printf(" Nonzeros        =             %12lld\n", nnz);
+    return verify && !ok ? 1 : 0;
+}

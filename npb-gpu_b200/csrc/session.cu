@@ -249,6 +249,11 @@ int upload_matrix(cgb_session *s, const int *rowstr, const int *colidx, const do
     const double mean = double(nnz) / double(s->n);
     s->lpr = s->opts.lanes_per_row > 0 ? s->opts.lanes_per_row : lanes_for_mean(mean);
     s->kernel = outer_kernel_for(s->lpr);
+    // these kernels keep almost nothing in shared memory: give L1 the most
+    // room for the gathered vector
+    CUDA_TRY(cudaFuncSetAttribute(s->kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 0));
+    CUDA_TRY(cudaFuncSetAttribute(spmv_kernel_for(s->lpr),
+                                  cudaFuncAttributePreferredSharedMemoryCarveout, 0));
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s->kernel, s->block, 0));
     if (per_sm < 1) return set_error(CGB_ERR_CUDA, "outer kernel cannot be resident");

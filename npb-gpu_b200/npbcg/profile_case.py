@@ -1,0 +1,55 @@
+"""Small, fixed workloads for profiling and tuning runs of libcgb.
+
+    python npb-gpu_b200/npbcg/profile_case.py --cls B --what spmv --reps 3
+    python npb-gpu_b200/npbcg/profile_case.py --cls B --what solve --niter 2
+    python npb-gpu_b200/npbcg/profile_case.py --cls B --what sweep
+
+`spmv` launches the standalone FP64 SpMV+dot kernel `reps` times (after one
+warm-up launch); `solve` runs one power iteration of `niter` outer steps;
+`sweep` prints SpMV timings for every lanes-per-row choice.  Each prints one
+JSON line.
+"""
+import argparse
+import json
+import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+import npbcg  # noqa: E402
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--cls", default="B", choices=sorted(npbcg.CLASSES))
+    ap.add_argument("--what", default="spmv", choices=["spmv", "solve", "sweep"])
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--niter", type=int, default=2)
+    ap.add_argument("--lanes", type=int, default=0)
+    ap.add_argument("--fp32", action="store_true")
+    a = ap.parse_args()
+    c = npbcg.CLASSES[a.cls]
+    rs, ci, av = npbcg.makea(c["n"], c["nonzer"], npbcg.RCOND, c["shift"])
+    n, nnz = c["n"], len(av)
+    out = {"cls": a.cls, "n": n, "nnz": nnz, "what": a.what}
+    if a.what == "sweep":
+        rows = []
+        for lanes in (4, 8, 16, 32):
+            with npbcg.Session(rs, ci, av, lanes_per_row=lanes) as s:
+                ms = s.time_spmv(50, fp32=a.fp32)
+            b = (npbcg.spmv_bytes_fp32 if a.fp32 else npbcg.spmv_bytes_fp64)(n, nnz)
+            rows.append({"lanes": lanes, "ms": ms, "gbs": b / ms / 1e6})
+        out["sweep"] = rows
+    else:
+        with npbcg.Session(rs, ci, av, lanes_per_row=a.lanes) as s:
+            if a.what == "spmv":
+                ms = s.time_spmv(a.reps, fp32=a.fp32)
+                b = (npbcg.spmv_bytes_fp32 if a.fp32 else npbcg.spmv_bytes_fp64)(n, nnz)
+                out.update(ms=ms, gbs=b / ms / 1e6)
+            else:
+                r = s.power_iterate(a.niter, c["shift"])
+                out.update(device_ms=r["device_ms"], zeta=float(r["zeta"][-1]))
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()
