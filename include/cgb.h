@@ -72,6 +72,9 @@ typedef struct cgb_options {
     long long wait_limit_ns;  /* limit of every device-side wait (grid barrier): 0 = 2 s */
     int use_graph;            /* 1 (default): outer loop replayed as one CUDA graph */
     int keep_fp32_copy;       /* 1 (default): also hold FP32 values for the mixed mode */
+    int spmv_kernel;          /* 0 = autotuned, 1 = row kernel (vector read through L1/L2),
+                                 2 = column-tiled kernel (vector staged in shared memory) */
+    int rows_in_flight;       /* tiled kernel: rows per lane group in flight, 0 = autotuned */
 } cgb_options;
 
 void cgb_default_options(cgb_options *opts);
@@ -143,6 +146,12 @@ int cgb_time_spmv(cgb_session *s, int reps, int fp32, double *ms_per_launch);
  * kernels.  Outputs are means in milliseconds. */
 int cgb_time_outer_steps(cgb_session *s, int niter, double shift, double *kernel_ms,
                          double *graph_gap_ms);
+
+/* The kernel configuration the session's autotuner chose: kind 1 = row,
+ * 2 = column-tiled; lanes per row, rows in flight, grid, block, dynamic
+ * shared memory bytes.  Any output may be NULL. */
+int cgb_plan_info(cgb_session *s, int *kind, int *lanes_per_row, int *rows_in_flight, int *grid,
+                  int *block, long long *smem_bytes);
 
 /* Grid barrier time-out self-test: runs a 2-CTA kernel whose second CTA never
  * arrives, with a wait limit of `limit_ns`, and reports the status the host

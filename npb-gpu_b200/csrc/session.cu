@@ -54,26 +54,44 @@ cudaError_t dev_alloc(T **p, size_t count)
 using OuterKernel = void (*)(OuterArgs);
 using SpmvKernel = void (*)(SpmvArgs);
 
-OuterKernel outer_kernel_for(int lpr)
-{
-    switch (lpr) {
-    case 2: return outer_step_fp64<2>;
-    case 4: return outer_step_fp64<4>;
-    case 8: return outer_step_fp64<8>;
-    case 16: return outer_step_fp64<16>;
-    default: return outer_step_fp64<32>;
-    }
-}
+constexpr int kKindRow = 1;
+constexpr int kKindTiled = 2;
+constexpr int kTileWidth = 12288;          // doubles per staged column block (96 KB)
+constexpr size_t kSmemLimit = 227 * 1024;  // opt-in shared memory per CTA on sm_100
 
-SpmvKernel spmv_kernel_for(int lpr)
+// A launch configuration of the persistent kernels.
+struct Plan {
+    int kind = 0;        // kKindRow / kKindTiled
+    int lpr = 32;        // lanes per row
+    int rows = 1;        // rows in flight per lane group (tiled)
+    OuterKernel outer = nullptr;
+    SpmvKernel spmv = nullptr;
+    int block = 512;
+    int grid = 0;
+    size_t smem = 0;
+    int max_rows = 0;    // tiled: row accumulator capacity
+};
+
+bool kernels_for(int kind, int lpr, int rows, OuterKernel *outer, SpmvKernel *spmv)
 {
-    switch (lpr) {
-    case 2: return spmv_dot_fp64<2>;
-    case 4: return spmv_dot_fp64<4>;
-    case 8: return spmv_dot_fp64<8>;
-    case 16: return spmv_dot_fp64<16>;
-    default: return spmv_dot_fp64<32>;
+    if (kind == kKindRow) {
+        switch (lpr) {
+        case 2: *outer = outer_step_fp64<2>; *spmv = spmv_dot_fp64<2>; return true;
+        case 4: *outer = outer_step_fp64<4>; *spmv = spmv_dot_fp64<4>; return true;
+        case 8: *outer = outer_step_fp64<8>; *spmv = spmv_dot_fp64<8>; return true;
+        case 16: *outer = outer_step_fp64<16>; *spmv = spmv_dot_fp64<16>; return true;
+        case 32: *outer = outer_step_fp64<32>; *spmv = spmv_dot_fp64<32>; return true;
+        default: return false;
+        }
     }
+    if (kind == kKindTiled) {
+        if (lpr == 4 && rows == 2) { *outer = outer_step_fp64_tiled<4, 2>; *spmv = spmv_dot_fp64_tiled<4, 2>; return true; }
+        if (lpr == 8 && rows == 1) { *outer = outer_step_fp64_tiled<8, 1>; *spmv = spmv_dot_fp64_tiled<8, 1>; return true; }
+        if (lpr == 8 && rows == 2) { *outer = outer_step_fp64_tiled<8, 2>; *spmv = spmv_dot_fp64_tiled<8, 2>; return true; }
+        if (lpr == 16 && rows == 1) { *outer = outer_step_fp64_tiled<16, 1>; *spmv = spmv_dot_fp64_tiled<16, 1>; return true; }
+        return false;
+    }
+    return false;
 }
 
 // Lanes per row from the mean row length: enough lanes that each covers a
@@ -152,10 +170,13 @@ struct cgb_session {
     int trace_cap = 0;
     double *d_dot = nullptr;
 
-    int lpr = 32;
-    int block = 512;
-    int grid = 0;
-    OuterKernel kernel = nullptr;
+    Plan plan;
+    int *d_seg = nullptr;        // tiled: (nblk+1) x seg_stride segment offsets
+    int seg_stride = 0;
+    int nblk = 0;
+    bool sorted = false;         // columns ascending within every row
+    int *d_flag = nullptr;       // device scratch flag (unsorted rows)
+    std::vector<int> h_rowstr_copy;
 
     const int *h_rowstr = nullptr;
     const int *h_colidx = nullptr;
@@ -201,6 +222,8 @@ void release(cgb_session *s)
     cudaFree(s->d_split);
     cudaFree(s->d_trace);
     cudaFree(s->d_dot);
+    cudaFree(s->d_seg);
+    cudaFree(s->d_flag);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -224,6 +247,214 @@ void make_split(int n, const int *rowstr, int grid, std::vector<int> &split)
     split[grid] = n;
 }
 
+OuterArgs outer_args(cgb_session *s)
+{
+    OuterArgs A{};
+    A.n = s->n;
+    A.rowstr = s->d_rowstr;
+    A.colidx = s->d_colidx;
+    A.a = s->d_a;
+    A.x = s->x();
+    A.z = s->z();
+    A.p = s->p();
+    A.q = s->q();
+    A.r = s->r();
+    A.row_split = s->d_split;
+    A.part = s->d_part;
+    A.gpad = s->gpad;
+    A.gb.count = s->count();
+    A.gb.gen = s->gen();
+    A.gb.status = s->d_status;
+    A.gb.limit_ns = s->opts.wait_limit_ns > 0 ? s->opts.wait_limit_ns : kDefaultWaitNs;
+    A.tile.seg = s->d_seg;
+    A.tile.seg_stride = s->seg_stride;
+    A.tile.nblk = s->nblk;
+    A.tile.width = kTileWidth;
+    A.tile.max_rows = s->plan.max_rows;
+    A.trace = s->d_trace;
+    return A;
+}
+
+cudaError_t launch_outer(cgb_session *s, const OuterArgs &A)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(s->plan.grid);
+    cfg.blockDim = dim3(s->plan.block);
+    cfg.dynamicSmemBytes = s->plan.smem;
+    cfg.stream = s->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, s->plan.outer, A);
+}
+
+// Segment table of the column tiling, built on the device from the uploaded
+// CSR (build_segments); also reports whether every row has ascending
+// columns, which the tiled kernels need.
+int build_tiling(cgb_session *s)
+{
+    const int n = s->n;
+    s->nblk = (n + kTileWidth - 1) / kTileWidth;
+    s->seg_stride = (n + 31) & ~31;
+    const size_t count = size_t(s->nblk + 1) * s->seg_stride;
+    cudaFree(s->d_seg);
+    s->d_seg = nullptr;
+    if (dev_alloc(&s->d_seg, count) != cudaSuccess)
+        return set_error(CGB_ERR_NOMEM, "segment table allocation failed");
+    CUDA_TRY(cudaMemsetAsync(s->d_flag, 0, sizeof(int), s->stream));
+    build_segments<<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
+        s->d_rowstr, s->d_colidx, n, s->nblk, kTileWidth, s->d_seg, s->seg_stride, s->d_flag);
+    CUDA_TRY(cudaGetLastError());
+    int unsorted = 0;
+    CUDA_TRY(cudaMemcpyAsync(&unsorted, s->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->sorted = (unsorted == 0);
+    if (!s->sorted) {
+        cudaFree(s->d_seg);
+        s->d_seg = nullptr;
+        s->nblk = 0;
+    }
+    return CGB_OK;
+}
+
+// Fills `pl` for (kind, lpr, rows): kernels, occupancy-sized cooperative grid,
+// shared memory.  Returns false when the configuration cannot run here.
+bool make_plan(cgb_session *s, int kind, int lpr, int rows, Plan *pl)
+{
+    Plan P;
+    P.kind = kind;
+    P.lpr = lpr;
+    P.rows = rows;
+    if (!kernels_for(kind, lpr, rows, &P.outer, &P.spmv)) return false;
+    if (kind == kKindRow) {
+        P.block = s->opts.block_threads ? s->opts.block_threads : 512;
+        P.smem = 0;
+        // almost nothing lives in shared memory: give L1 the room
+        if (cudaFuncSetAttribute(P.outer, cudaFuncAttributePreferredSharedMemoryCarveout, 0) ||
+            cudaFuncSetAttribute(P.spmv, cudaFuncAttributePreferredSharedMemoryCarveout, 0))
+            return false;
+    } else {
+        if (!s->sorted || s->d_seg == nullptr) return false;
+        P.block = 1024;
+        // rows per CTA with one CTA per SM, balanced as make_split does
+        const int grid = std::min(s->prop.multiProcessorCount, s->n);
+        std::vector<int> split;
+        make_split(s->n, s->h_rowstr_copy.data(), grid, split);
+        int mr = 0;
+        for (int c = 0; c < grid; c++) mr = std::max(mr, split[c + 1] - split[c]);
+        P.max_rows = (mr + 31) & ~31;
+        P.smem = tiled_smem_bytes(kTileWidth, P.max_rows);
+        if (P.smem > kSmemLimit) return false;
+        if (cudaFuncSetAttribute(P.outer, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)) ||
+            cudaFuncSetAttribute(P.spmv, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)))
+            return false;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, P.outer, P.block, P.smem) != cudaSuccess ||
+        per_sm < 1)
+        return false;
+    per_sm = std::min(per_sm, kind == kKindTiled ? 1 : 4);
+    P.grid = std::max(1, std::min(per_sm * s->prop.multiProcessorCount, s->n));
+    if (P.grid > s->gpad) return false;
+    *pl = P;
+    return true;
+}
+
+// Makes `pl` the session's plan: uploads its row split.
+int apply_plan(cgb_session *s, const Plan &pl)
+{
+    std::vector<int> split;
+    make_split(s->n, s->h_rowstr_copy.data(), pl.grid, split);
+    CUDA_TRY(cudaMemcpy(s->d_split, split.data(), sizeof(int) * (pl.grid + 1), cudaMemcpyHostToDevice));
+    s->plan = pl;
+    drop_graph(s);
+    return CGB_OK;
+}
+
+SpmvArgs spmv_args(cgb_session *s)
+{
+    SpmvArgs S{};
+    S.A = outer_args(s);
+    S.ticket = s->ticket();
+    S.dot = s->d_dot;
+    return S;
+}
+
+// Mean device ms of `reps` standalone SpMV launches under the current plan.
+int time_plan_spmv(cgb_session *s, int reps, double *ms_out)
+{
+    SpmvArgs S = spmv_args(s);
+    const Plan &P = s->plan;
+    fill_ones<<<s->prop.multiProcessorCount, 256, 0, s->stream>>>(s->p(), s->n + 1);
+    for (int i = 0; i < 2; i++) P.spmv<<<P.grid, P.block, P.smem, s->stream>>>(S);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(s->ev0, s->stream));
+    for (int i = 0; i < reps; i++) P.spmv<<<P.grid, P.block, P.smem, s->stream>>>(S);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(s->ev1, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    *ms_out = double(ms) / reps;
+    int st = 0;
+    CUDA_TRY(cudaMemcpy(&st, s->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st != kDevOk) {
+        CUDA_TRY(cudaMemset(s->d_status, 0, sizeof(int)));
+        return set_error(CGB_ERR_TIMEOUT, "SpMV wait failed (status %d)", st);
+    }
+    return CGB_OK;
+}
+
+// Picks the plan: the one the options force, else the fastest standalone
+// SpMV among the candidates (the session's autotuner).
+int choose_plan(cgb_session *s)
+{
+    const cgb_options &o = s->opts;
+    const double mean = double(s->nnz) / double(s->n);
+    std::vector<Plan> cands;
+    auto add = [&](int kind, int lpr, int rows) {
+        Plan p;
+        if (make_plan(s, kind, lpr, rows, &p)) cands.push_back(p);
+    };
+    const int want_kind = o.spmv_kernel;
+    if (want_kind == 0 || want_kind == kKindRow) {
+        if (o.lanes_per_row > 0) add(kKindRow, o.lanes_per_row, 1);
+        else {
+            const int l = lanes_for_mean(mean);
+            add(kKindRow, l, 1);
+            if (want_kind == 0 && l > 2) add(kKindRow, l / 2, 1);
+        }
+    }
+    if ((want_kind == 0 || want_kind == kKindTiled) && s->sorted && s->n >= 2 * kTileWidth) {
+        if (o.lanes_per_row > 0) {
+            add(kKindTiled, o.lanes_per_row, o.rows_in_flight > 0 ? o.rows_in_flight : 1);
+        } else {
+            add(kKindTiled, 4, 2);
+            add(kKindTiled, 8, 2);
+            add(kKindTiled, 8, 1);
+            add(kKindTiled, 16, 1);
+        }
+    }
+    if (cands.empty()) return set_error(CGB_ERR_INVALID, "no kernel configuration fits these options");
+    if (cands.size() == 1) return apply_plan(s, cands[0]);
+    double best = 1e30;
+    int bi = 0;
+    for (size_t i = 0; i < cands.size(); i++) {
+        int st = apply_plan(s, cands[i]);
+        if (st) return st;
+        double ms = 0.0;
+        st = time_plan_spmv(s, 10, &ms);
+        if (st) return st;
+        if (ms < best) {
+            best = ms;
+            bi = int(i);
+        }
+    }
+    return apply_plan(s, cands[bi]);
+}
+
 int upload_matrix(cgb_session *s, const int *rowstr, const int *colidx, const double *a)
 {
     const long long nnz = rowstr[s->n];
@@ -245,71 +476,31 @@ int upload_matrix(cgb_session *s, const int *rowstr, const int *colidx, const do
     CUDA_TRY(cudaMemcpyAsync(s->d_a, a, sizeof(double) * nnz, cudaMemcpyHostToDevice, s->stream));
     CUDA_TRY(cudaMemsetAsync(s->d_colidx + nnz, 0, sizeof(int) * kPad, s->stream));
     CUDA_TRY(cudaMemsetAsync(s->d_a + nnz, 0, sizeof(double) * kPad, s->stream));
-
-    const double mean = double(nnz) / double(s->n);
-    s->lpr = s->opts.lanes_per_row > 0 ? s->opts.lanes_per_row : lanes_for_mean(mean);
-    s->kernel = outer_kernel_for(s->lpr);
-    // these kernels keep almost nothing in shared memory: give L1 the most
-    // room for the gathered vector
-    CUDA_TRY(cudaFuncSetAttribute(s->kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 0));
-    CUDA_TRY(cudaFuncSetAttribute(spmv_kernel_for(s->lpr),
-                                  cudaFuncAttributePreferredSharedMemoryCarveout, 0));
-    int per_sm = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s->kernel, s->block, 0));
-    if (per_sm < 1) return set_error(CGB_ERR_CUDA, "outer kernel cannot be resident");
-    per_sm = std::min(per_sm, 4);
-    s->grid = per_sm * s->prop.multiProcessorCount;
-    // tiny systems: no more CTAs than rows
-    s->grid = std::max(1, std::min(s->grid, s->n));
-    if (s->grid > s->gpad) return set_error(CGB_ERR_STATE, "grid %d exceeds partial capacity", s->grid);
-    std::vector<int> split;
-    make_split(s->n, rowstr, s->grid, split);
-    CUDA_TRY(cudaMemcpyAsync(s->d_split, split.data(), sizeof(int) * (s->grid + 1),
-                             cudaMemcpyHostToDevice, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     s->h_rowstr = rowstr;
     s->h_colidx = colidx;
     s->h_a = a;
-    drop_graph(s);
-    return CGB_OK;
-}
-
-OuterArgs outer_args(cgb_session *s)
-{
-    OuterArgs A{};
-    A.n = s->n;
-    A.rowstr = s->d_rowstr;
-    A.colidx = s->d_colidx;
-    A.a = s->d_a;
-    A.x = s->x();
-    A.z = s->z();
-    A.p = s->p();
-    A.q = s->q();
-    A.r = s->r();
-    A.row_split = s->d_split;
-    A.part = s->d_part;
-    A.gpad = s->gpad;
-    A.gb.count = s->count();
-    A.gb.gen = s->gen();
-    A.gb.status = s->d_status;
-    A.gb.limit_ns = s->opts.wait_limit_ns > 0 ? s->opts.wait_limit_ns : kDefaultWaitNs;
-    A.trace = s->d_trace;
-    return A;
-}
-
-cudaError_t launch_outer(cgb_session *s, const OuterArgs &A)
-{
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3(s->grid);
-    cfg.blockDim = dim3(s->block);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = s->stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, s->kernel, A);
+    // same row pointers as before (e.g. the same matrix uploaded again): the
+    // row split and tuned plan still hold; only the segment table is rebuilt
+    const bool same_rows = s->plan.outer != nullptr &&
+                           s->h_rowstr_copy.size() == size_t(s->n) + 1 &&
+                           std::equal(rowstr, rowstr + s->n + 1, s->h_rowstr_copy.begin());
+    s->h_rowstr_copy.assign(rowstr, rowstr + s->n + 1);
+    const bool was_tiled = s->plan.kind == kKindTiled;
+    s->sorted = false;
+    cudaFree(s->d_seg);
+    s->d_seg = nullptr;
+    s->nblk = 0;
+    if (s->n >= 2 * kTileWidth) {
+        int st = build_tiling(s);
+        if (st) return st;
+    }
+    if (same_rows && (!was_tiled || s->sorted)) {
+        drop_graph(s);
+        return CGB_OK;
+    }
+    s->plan = Plan();
+    return choose_plan(s);
 }
 
 int ensure_trace(cgb_session *s, int niter)
@@ -425,6 +616,8 @@ void cgb_default_options(cgb_options *o)
     o->wait_limit_ns = 0;
     o->use_graph = 1;
     o->keep_fp32_copy = 1;
+    o->spmv_kernel = 0;
+    o->rows_in_flight = 0;
 }
 
 void cgb_default_solve_params(cgb_solve_params *p)
@@ -470,6 +663,10 @@ int cgb_create(int n, const int *rowstr, const int *colidx, const double *a,
         return set_error(CGB_ERR_INVALID, "lanes_per_row must be 0, 2, 4, 8, 16 or 32");
     if (o.block_threads != 0 && o.block_threads != 256 && o.block_threads != 512)
         return set_error(CGB_ERR_INVALID, "block_threads must be 0, 256 or 512");
+    if (o.spmv_kernel < 0 || o.spmv_kernel > 2)
+        return set_error(CGB_ERR_INVALID, "spmv_kernel must be 0 (auto), 1 (row) or 2 (tiled)");
+    if (o.rows_in_flight < 0 || o.rows_in_flight > 2)
+        return set_error(CGB_ERR_INVALID, "rows_in_flight must be 0, 1 or 2");
     cudaDeviceProp prop;
     st = check_device(o.device, &prop);
     if (st) return st;
@@ -481,7 +678,6 @@ int cgb_create(int n, const int *rowstr, const int *colidx, const double *a,
     s->n = n;
     s->opts = o;
     s->prop = prop;
-    s->block = o.block_threads ? o.block_threads : 512;
     s->vstride = (size_t(n) + 2 + 31) & ~size_t(31);
     s->gpad = 4 * prop.multiProcessorCount;
 #define CREATE_TRY(call)                                                                  \
@@ -507,6 +703,7 @@ int cgb_create(int n, const int *rowstr, const int *colidx, const double *a,
     CREATE_TRY(cudaMemset(s->d_status, 0, sizeof(int)));
     CREATE_TRY(dev_alloc(&s->d_split, size_t(s->gpad) + 1));
     CREATE_TRY(dev_alloc(&s->d_dot, 1));
+    CREATE_TRY(dev_alloc(&s->d_flag, 1));
 #undef CREATE_TRY
     st = ensure_trace(s, 128);
     if (st == CGB_OK) st = upload_matrix(s, rowstr, colidx, a);
@@ -646,29 +843,19 @@ int cgb_time_spmv(cgb_session *s, int reps, int fp32, double *ms_per_launch)
     if (!s || reps < 1 || !ms_per_launch) return set_error(CGB_ERR_INVALID, "bad arguments");
     if (fp32) return set_error(CGB_ERR_INVALID, "FP32 SpMV is not available in this build");
     CUDA_TRY(cudaSetDevice(s->device));
-    SpmvArgs S{};
-    S.n = s->n;
-    S.rowstr = s->d_rowstr;
-    S.colidx = s->d_colidx;
-    S.a = s->d_a;
-    S.p = s->p();
-    S.q = s->q();
-    S.row_split = s->d_split;
-    S.part = s->d_part;
-    S.ticket = s->ticket();
-    S.dot = s->d_dot;
-    SpmvKernel k = spmv_kernel_for(s->lpr);
-    fill_ones<<<s->prop.multiProcessorCount, 256, 0, s->stream>>>(s->p(), s->n + 1);
-    k<<<s->grid, s->block, 0, s->stream>>>(S);  // warm-up
-    CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaEventRecord(s->ev0, s->stream));
-    for (int i = 0; i < reps; i++) k<<<s->grid, s->block, 0, s->stream>>>(S);
-    CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaEventRecord(s->ev1, s->stream));
-    CUDA_TRY(cudaStreamSynchronize(s->stream));
-    float ms = 0.f;
-    CUDA_TRY(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
-    *ms_per_launch = double(ms) / reps;
+    return time_plan_spmv(s, reps, ms_per_launch);
+}
+
+int cgb_plan_info(cgb_session *s, int *kind, int *lanes_per_row, int *rows_in_flight, int *grid,
+                  int *block, long long *smem_bytes)
+{
+    if (!s) return set_error(CGB_ERR_INVALID, "session is null");
+    if (kind) *kind = s->plan.kind;
+    if (lanes_per_row) *lanes_per_row = s->plan.lpr;
+    if (rows_in_flight) *rows_in_flight = s->plan.rows;
+    if (grid) *grid = s->plan.grid;
+    if (block) *block = s->plan.block;
+    if (smem_bytes) *smem_bytes = (long long)s->plan.smem;
     return CGB_OK;
 }
 

@@ -63,7 +63,8 @@ class CgbError(RuntimeError):
 class Options(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("lanes_per_row", ctypes.c_int),
                 ("block_threads", ctypes.c_int), ("wait_limit_ns", ctypes.c_longlong),
-                ("use_graph", ctypes.c_int), ("keep_fp32_copy", ctypes.c_int)]
+                ("use_graph", ctypes.c_int), ("keep_fp32_copy", ctypes.c_int),
+                ("spmv_kernel", ctypes.c_int), ("rows_in_flight", ctypes.c_int)]
 
 
 class SolveParams(ctypes.Structure):
@@ -107,6 +108,8 @@ _SIGNATURES = {
     "cgb_time_outer_steps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
                                             ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_double)]),
+    "cgb_plan_info": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int)] * 5 +
+                      [ctypes.POINTER(ctypes.c_longlong)]),
     "cgb_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong,
                                                  ctypes.POINTER(ctypes.c_int)]),
     "cgb_host_alloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_longlong]),
@@ -249,6 +252,15 @@ class Session:
         k, g = ctypes.c_double(), ctypes.c_double()
         _check(lib().cgb_time_outer_steps(self._h, niter, shift, ctypes.byref(k), ctypes.byref(g)))
         return k.value, g.value
+
+    def plan(self):
+        """The kernel configuration chosen for this matrix."""
+        v = [ctypes.c_int() for _ in range(5)]
+        smem = ctypes.c_longlong()
+        _check(lib().cgb_plan_info(self._h, *[ctypes.byref(x) for x in v], ctypes.byref(smem)))
+        kind, lpr, rows, grid, block = (x.value for x in v)
+        return dict(kind={1: "row", 2: "tiled"}.get(kind, kind), lanes_per_row=lpr,
+                    rows_in_flight=rows, grid=grid, block=block, smem=smem.value)
 
     def selftest_wait_timeout(self, limit_ns):
         """Returns (status, device_status) of the bounded-wait self-test."""

@@ -189,3 +189,61 @@ def test_spmv_timer_runs(cgb):
     s, _ = session_for(cgb, "A")
     ms = s.time_spmv(5)
     assert 0 < ms < 50
+
+
+@pytest.mark.parametrize("kind,lpr,rows", [(1, 16, 0), (2, 4, 2), (2, 8, 1), (2, 8, 2), (2, 16, 1)])
+def test_spmv_kernels_agree_class_b(cgb, golden, kind, lpr, rows):
+    """Row and column-tiled SpMV policies reproduce the reference trace."""
+    n, nonzer, niter, shift = PARAMS["B"]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    with cgb.Session(rs, ci, a, spmv_kernel=kind, lanes_per_row=lpr, rows_in_flight=rows) as s:
+        plan = s.plan()
+        assert plan["kind"] == {1: "row", 2: "tiled"}[kind]
+        out = s.power_iterate(niter, shift)
+        z, p, q, r, rn = s.conj_grad(np.ones(n))
+    ref = np.array(golden["B"]["seeds"]["314159265.0"]["zeta"])
+    assert np.max(np.abs(out["zeta"] - ref) / np.abs(ref)) <= 1e-10
+    assert np.max(np.abs(out["rnorm"] - np.array(golden["B"]["seeds"]["314159265.0"]["rnorm"]))) <= 1e-10
+
+
+def test_tiled_spmv_matches_oracle_product(cgb, oracle):
+    """One tiled conj_grad against the oracle's on an unsorted-free random x."""
+    n, nonzer, niter, shift = PARAMS["C"]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    x = 1.0 + 0.5 * np.sin(np.arange(n) * 0.001)
+    with cgb.Session(rs, ci, a, spmv_kernel=2) as s:
+        z, p, q, r, rn = s.conj_grad(x)
+    zo, po, qo, ro, rno = oracle.conj_grad(rs, ci, a, x)
+    assert np.linalg.norm(z[:n] - zo[:n]) <= 1e-12 * np.linalg.norm(zo[:n])
+    assert np.linalg.norm(r[:n] - ro[:n]) <= 1e-12 * np.linalg.norm(ro[:n])
+
+
+def test_tiled_refused_for_small_or_unsorted(cgb):
+    n, nonzer, niter, shift = PARAMS["W"]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    with pytest.raises(cgb.CgbError) as e:
+        cgb.Session(rs, ci, a, spmv_kernel=2)
+    assert e.value.status == cgb.ERR_INVALID
+    # a large CSR with one row's columns out of order: the autotuner must not pick tiled
+    n, nonzer, niter, shift = PARAMS["B"]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    ci = ci.copy()
+    k0 = rs[10]
+    ci[k0], ci[k0 + 1] = ci[k0 + 1], ci[k0]
+    a = a.copy()
+    a[k0], a[k0 + 1] = a[k0 + 1], a[k0]
+    with cgb.Session(rs, ci, a) as s:
+        assert s.plan()["kind"] == "row"
+        out = s.power_iterate(3, shift)
+    ok = cgb.makea(n, nonzer, 0.1, shift)
+    with cgb.Session(*ok) as s2:
+        ref = s2.power_iterate(3, shift)
+    assert np.max(np.abs(out["zeta"] - ref["zeta"]) / np.abs(ref["zeta"])) <= 1e-12
+
+
+def test_autotuned_plan_reported(cgb):
+    n, nonzer, niter, shift = PARAMS["C"]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    with cgb.Session(rs, ci, a) as s:
+        plan = s.plan()
+    assert plan["kind"] in ("row", "tiled") and plan["grid"] >= 148
