@@ -158,6 +158,27 @@ int cgb_plan_info(cgb_session *s, int *kind, int *lanes_per_row, int *rows_in_fl
  * reads back (CGB_ERR_TIMEOUT expected).  The session stays usable. */
 int cgb_selftest_wait_timeout(cgb_session *s, long long limit_ns, int *device_status);
 
+/* conj_grad for callers that cannot allocate GPU memory.  No counterpart in
+ * the reference: it exists for hosts that forbid device allocation on this
+ * path (their device memory is handed out by their own pool, or the loop must
+ * never allocate).  Same computation as cgb_conj_grad (25 CG iterations from
+ * z = 0, then rnorm = ||x - A z||), but every pointer is caller-owned device
+ * memory and the work space (p, q, r, partial sums, barrier words) sits in
+ * one fixed array inside the library; this call allocates nothing.
+ *   d_rowstr n+1, d_colidx / d_a nnz entries (sorted or not), d_x and d_z
+ *   n+1 doubles (entry n as the reference sets it), d_rnorm one double,
+ *   d_status (nullable) one int: 0, or the device status on a failed wait.
+ *   stream: a cudaStream_t (NULL = legacy default stream).  Asynchronous:
+ *   synchronise the stream before reading the outputs.
+ * Limit: n <= 262144 (CGB_ERR_CAPACITY above).  The array (about 6.3 MB) is
+ * held on every GPU that loads the library until exit.  Calls share it:
+ * calls that overlap on the GPU race, so serialise them.  Runs on the
+ * calling thread's current device; the first call on a device looks the
+ * array up there, so make that first call before any stream capture. */
+int cgb_conj_grad_noalloc(int n, long long nnz, const int *d_rowstr, const int *d_colidx,
+                          const double *d_a, const double *d_x, double *d_z, double *d_rnorm,
+                          int *d_status, void *stream);
+
 /* Host memory that the device copies at full speed (cudaHostAlloc). */
 int cgb_host_alloc(void **ptr, long long bytes);
 int cgb_host_free(void *ptr);

@@ -503,7 +503,7 @@ __global__ void __launch_bounds__(1024, 1) outer_step_fp64_tiled(OuterArgs A)
 }
 
 // x = 1 over n+1 entries (cg.cu:485-488).
-__global__ void fill_ones(double *x, int count)
+static __global__ void fill_ones(double *x, int count)
 {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x)
         x[j] = 1.0;
@@ -565,7 +565,7 @@ __global__ void __launch_bounds__(1024, 1) spmv_dot_fp64_tiled(SpmvArgs S)
 // Segment table of the column tiling: seg[b*stride + j] = first entry of row
 // j whose column is >= b*width (b < nblk), seg[nblk*stride + j] = end of row
 // j; *unsorted is set when some row's columns do not ascend.
-__global__ void build_segments(const int *__restrict__ rowstr, const int *__restrict__ colidx,
+static __global__ void build_segments(const int *__restrict__ rowstr, const int *__restrict__ colidx,
                                int n, int nblk, int width, int *seg, int stride, int *unsorted)
 {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
@@ -589,7 +589,7 @@ __global__ void build_segments(const int *__restrict__ rowstr, const int *__rest
 
 // Self-test of the bounded wait: CTA 1 never arrives, so CTA 0's barrier
 // wait runs into its limit and records kDevTimeout.
-__global__ void barrier_timeout_probe(GridBarrier gb)
+static __global__ void barrier_timeout_probe(GridBarrier gb)
 {
     if (blockIdx.x == 1) return;
     (void)grid_barrier(gb);

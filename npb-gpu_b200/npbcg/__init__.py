@@ -112,6 +112,8 @@ _SIGNATURES = {
                       [ctypes.POINTER(ctypes.c_longlong)]),
     "cgb_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong,
                                                  ctypes.POINTER(ctypes.c_int)]),
+    "cgb_conj_grad_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_longlong] +
+                              [ctypes.c_void_p] * 8),
     "cgb_host_alloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_longlong]),
     "cgb_host_free": (ctypes.c_int, [ctypes.c_void_p]),
     "cgb_device_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
