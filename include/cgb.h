@@ -72,9 +72,10 @@ typedef struct cgb_options {
     long long wait_limit_ns;  /* limit of every device-side wait (grid barrier): 0 = 2 s */
     int use_graph;            /* 1 (default): outer loop replayed as one CUDA graph */
     int keep_fp32_copy;       /* 1 (default): also hold FP32 values for the mixed mode */
-    int spmv_kernel;          /* 0 = autotuned, 1 = row kernel (vector read through L1/L2),
-                                 2 = column-tiled kernel (vector staged in shared memory) */
-    int rows_in_flight;       /* tiled kernel: rows per lane group in flight, 0 = autotuned */
+    int spmv_kernel;          /* 0 = autotuned, 1 = row kernel on the CSR (gathered vector read
+                                 through L1/L2), 2 = sliced kernel (a sliced copy of the matrix
+                                 with 16-bit local columns, gathered vector staged in shared
+                                 memory by TMA bulk copies) */
 } cgb_options;
 
 void cgb_default_options(cgb_options *opts);
@@ -125,6 +126,7 @@ typedef struct cgb_solve_result {
     double device_ms;     /* device time of the whole outer loop (CUDA events) */
     int total_inner;      /* inner iterations summed over the outer steps */
     int fallbacks;        /* outer steps that fell back to plain FP64 CG */
+    int refreshes;        /* true-residual replacements (MIXED*) summed over the outer steps */
 } cgb_solve_result;
 
 /* The reference's timed region (cg.cu:491-522): x = 1, then niter times
@@ -136,9 +138,10 @@ int cgb_power_iterate(cgb_session *s, const cgb_solve_params *params, double *ze
                       cgb_solve_result *res);
 
 /* ---------------------------------------------------------- diagnostics */
-/* Time `reps` launches of the standalone FP64 SpMV (q = A p with the p.q
- * reduction fused, the operation of kernel three + four, cg.cu:937-1004) and
- * return the mean device milliseconds per launch. */
+/* Time `reps` launches of the standalone SpMV (q = A p with the p.q
+ * reduction fused, the operation of kernel three + four, cg.cu:937-1004) of
+ * the session's plan, FP64 or (fp32 != 0) the FP32 copy, and return the mean
+ * device milliseconds per launch. */
 int cgb_time_spmv(cgb_session *s, int reps, int fp32, double *ms_per_launch);
 
 /* Per-launch device times of one FP64 outer step kernel, and the gap the
@@ -148,10 +151,11 @@ int cgb_time_outer_steps(cgb_session *s, int niter, double shift, double *kernel
                          double *graph_gap_ms);
 
 /* The kernel configuration the session's autotuner chose: kind 1 = row,
- * 2 = column-tiled; lanes per row, rows in flight, grid, block, dynamic
- * shared memory bytes.  Any output may be NULL. */
-int cgb_plan_info(cgb_session *s, int *kind, int *lanes_per_row, int *rows_in_flight, int *grid,
-                  int *block, long long *smem_bytes);
+ * 2 = sliced; lanes per row (row kind), grid, block, dynamic shared memory
+ * bytes, and the stored entries of the layout the SpMV streams (nnz for the
+ * CSR, nnz plus slice padding for the sliced copy).  Any output may be NULL. */
+int cgb_plan_info(cgb_session *s, int *kind, int *lanes_per_row, int *grid, int *block,
+                  long long *smem_bytes, long long *layout_entries);
 
 /* Grid barrier time-out self-test: runs a 2-CTA kernel whose second CTA never
  * arrives, with a wait limit of `limit_ns`, and reports the status the host

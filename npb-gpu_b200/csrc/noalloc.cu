@@ -152,9 +152,9 @@ extern "C" int cgb_conj_grad_noalloc(int n, long long nnz, const int *d_rowstr, 
 
     OuterArgs A{};
     A.n = n;
-    A.rowstr = d_rowstr;
-    A.colidx = d_colidx;
-    A.a = d_a;
+    A.M.rowstr = d_rowstr;
+    A.M.colidx = d_colidx;
+    A.M.a = d_a;
     A.x = const_cast<double *>(d_x);  // read only: finish = 0 leaves x untouched
     A.z = d_z;
     A.p = vec;

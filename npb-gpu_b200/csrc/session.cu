@@ -1,5 +1,5 @@
 // session.cu -- the C ABI of libcgb: device set-up, the conj_grad-compatible
-// call, the CUDA-graph power iteration and diagnostics.
+// call, the CUDA-graph power iteration, the SpMV autotuner and diagnostics.
 //
 // Reference call surface being replaced (GMAP/NPB-GPU CUDA/CG/cg.cu):
 //   setup_gpu   :1390-1603  device pick, allocation, H2D upload
@@ -42,8 +42,11 @@ int set_error(int status, const char *fmt, ...)
 
 namespace {
 
-constexpr int kPad = 64;              // entries of padding after a / colidx
+constexpr int kPad = 64;                   // entries of padding after matrix arrays
 constexpr long long kDefaultWaitNs = 2000000000LL;
+constexpr size_t kSmemLimit = 227 * 1024;  // opt-in shared memory per CTA on sm_100
+constexpr int kKindRow = 1;
+constexpr int kKindSliced = 2;
 
 template <typename T>
 cudaError_t dev_alloc(T **p, size_t count)
@@ -51,47 +54,38 @@ cudaError_t dev_alloc(T **p, size_t count)
     return cudaMalloc(reinterpret_cast<void **>(p), sizeof(T) * std::max<size_t>(count, 1));
 }
 
+template <typename T>
+void dev_free(T *&p)
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
 using OuterKernel = void (*)(OuterArgs);
 using SpmvKernel = void (*)(SpmvArgs);
 
-constexpr int kKindRow = 1;
-constexpr int kKindTiled = 2;
-constexpr int kTileWidth = 12288;          // doubles per staged column block (96 KB)
-constexpr size_t kSmemLimit = 227 * 1024;  // opt-in shared memory per CTA on sm_100
-
 // A launch configuration of the persistent kernels.
 struct Plan {
-    int kind = 0;        // kKindRow / kKindTiled
-    int lpr = 32;        // lanes per row
-    int rows = 1;        // rows in flight per lane group (tiled)
-    OuterKernel outer = nullptr;
+    int kind = 0;  // kKindRow / kKindSliced
+    int lpr = 0;   // row policy: lanes per row
+    OuterKernel fp64 = nullptr;
+    OuterKernel mixed = nullptr;
     SpmvKernel spmv = nullptr;
     int block = 512;
     int grid = 0;
     size_t smem = 0;
-    int max_rows = 0;    // tiled: row accumulator capacity
 };
 
-bool kernels_for(int kind, int lpr, int rows, OuterKernel *outer, SpmvKernel *spmv)
+bool row_kernels(int lpr, Plan *P)
 {
-    if (kind == kKindRow) {
-        switch (lpr) {
-        case 2: *outer = outer_step_fp64<2>; *spmv = spmv_dot_fp64<2>; return true;
-        case 4: *outer = outer_step_fp64<4>; *spmv = spmv_dot_fp64<4>; return true;
-        case 8: *outer = outer_step_fp64<8>; *spmv = spmv_dot_fp64<8>; return true;
-        case 16: *outer = outer_step_fp64<16>; *spmv = spmv_dot_fp64<16>; return true;
-        case 32: *outer = outer_step_fp64<32>; *spmv = spmv_dot_fp64<32>; return true;
-        default: return false;
-        }
+    switch (lpr) {
+    case 2: P->fp64 = outer_step_fp64<2>; P->mixed = outer_step_mixed<2>; P->spmv = spmv_dot_row<2>; return true;
+    case 4: P->fp64 = outer_step_fp64<4>; P->mixed = outer_step_mixed<4>; P->spmv = spmv_dot_row<4>; return true;
+    case 8: P->fp64 = outer_step_fp64<8>; P->mixed = outer_step_mixed<8>; P->spmv = spmv_dot_row<8>; return true;
+    case 16: P->fp64 = outer_step_fp64<16>; P->mixed = outer_step_mixed<16>; P->spmv = spmv_dot_row<16>; return true;
+    case 32: P->fp64 = outer_step_fp64<32>; P->mixed = outer_step_mixed<32>; P->spmv = spmv_dot_row<32>; return true;
+    default: return false;
     }
-    if (kind == kKindTiled) {
-        if (lpr == 4 && rows == 2) { *outer = outer_step_fp64_tiled<4, 2>; *spmv = spmv_dot_fp64_tiled<4, 2>; return true; }
-        if (lpr == 8 && rows == 1) { *outer = outer_step_fp64_tiled<8, 1>; *spmv = spmv_dot_fp64_tiled<8, 1>; return true; }
-        if (lpr == 8 && rows == 2) { *outer = outer_step_fp64_tiled<8, 2>; *spmv = spmv_dot_fp64_tiled<8, 2>; return true; }
-        if (lpr == 16 && rows == 1) { *outer = outer_step_fp64_tiled<16, 1>; *spmv = spmv_dot_fp64_tiled<16, 1>; return true; }
-        return false;
-    }
-    return false;
 }
 
 // Lanes per row from the mean row length: enough lanes that each covers a
@@ -141,6 +135,23 @@ int validate_csr(int n, const int *rowstr, const int *colidx, const double *a)
     return CGB_OK;
 }
 
+// Row split with balanced (stored entries + a per-row allowance for the
+// vector updates) per CTA.
+void make_split(int n, const int *rowstr, int grid, std::vector<int> &split)
+{
+    split.assign(grid + 1, n);
+    const double per_row = 8.0;
+    const double total = double(rowstr[n]) + per_row * n;
+    int j = 0;
+    split[0] = 0;
+    for (int c = 1; c < grid; c++) {
+        const double target = total * c / grid;
+        while (j < n && double(rowstr[j]) + per_row * j < target) j++;
+        split[c] = j;
+    }
+    split[grid] = n;
+}
+
 }  // namespace
 }  // namespace cgb
 
@@ -156,36 +167,52 @@ struct cgb_session {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
+    // CSR (reference layout) and its FP32 values
     int *d_rowstr = nullptr;
     int *d_colidx = nullptr;
     double *d_a = nullptr;
-    double *d_vec = nullptr;  // x, z, p, q, r: vstride doubles each
+    float *d_a32 = nullptr;
+    // vectors: x, z, p, q, r (vstride doubles each) and p32
+    double *d_vec = nullptr;
+    float *d_p32 = nullptr;
     size_t vstride = 0;
+    // reductions, barrier, status, trace
     double *d_part = nullptr;
     int gpad = 0;
     unsigned *d_sync = nullptr;  // [0] count, [32] gen, [64] ticket (128-byte lines)
     int *d_status = nullptr;
+    int *d_flag = nullptr;
     int *d_split = nullptr;
     StepTrace *d_trace = nullptr;
     int trace_cap = 0;
     double *d_dot = nullptr;
 
-    Plan plan;
-    int *d_seg = nullptr;        // tiled: (nblk+1) x seg_stride segment offsets
+    // sliced layout (built for the sliced plan's row split)
+    int *d_seg = nullptr;
     int seg_stride = 0;
     int nblk = 0;
-    bool sorted = false;         // columns ascending within every row
-    int *d_flag = nullptr;       // device scratch flag (unsorted rows)
-    std::vector<int> h_rowstr_copy;
+    bool sorted = false;
+    int sliced_grid = 0;   // grid the layout was built for (0: none)
+    int sliced_max_rows = 0;
+    int *d_chunk_slice = nullptr;
+    unsigned short *d_srow = nullptr;
+    int *d_slice_width = nullptr;
+    unsigned *d_slice_off = nullptr;
+    double *d_sval = nullptr;
+    float *d_sval32 = nullptr;
+    unsigned short *d_scol = nullptr;
+    long long slice_entries = 0;
 
+    Plan plan;
+    std::vector<int> h_rowstr_copy;
     const int *h_rowstr = nullptr;
     const int *h_colidx = nullptr;
     const double *h_a = nullptr;
 
     // graph of the last power iteration shape
     cudaGraphExec_t graph = nullptr;
-    int g_niter = -1, g_cgitmax = -1, g_fixed = -1, g_warm = -1;
-    double g_shift = 0.0, g_tol = -1.0;
+    cgb_solve_params g_params{};
+    bool g_valid = false;
 
     double *x() { return d_vec; }
     double *z() { return d_vec + vstride; }
@@ -204,7 +231,20 @@ void drop_graph(cgb_session *s)
 {
     if (s->graph) cudaGraphExecDestroy(s->graph);
     s->graph = nullptr;
-    s->g_niter = -1;
+    s->g_valid = false;
+}
+
+void free_sliced(cgb_session *s)
+{
+    dev_free(s->d_chunk_slice);
+    dev_free(s->d_srow);
+    dev_free(s->d_slice_width);
+    dev_free(s->d_slice_off);
+    dev_free(s->d_sval);
+    dev_free(s->d_sval32);
+    dev_free(s->d_scol);
+    s->sliced_grid = 0;
+    s->slice_entries = 0;
 }
 
 void release(cgb_session *s)
@@ -212,53 +252,58 @@ void release(cgb_session *s)
     if (!s) return;
     cudaSetDevice(s->device);
     drop_graph(s);
-    cudaFree(s->d_rowstr);
-    cudaFree(s->d_colidx);
-    cudaFree(s->d_a);
-    cudaFree(s->d_vec);
-    cudaFree(s->d_part);
-    cudaFree(s->d_sync);
-    cudaFree(s->d_status);
-    cudaFree(s->d_split);
-    cudaFree(s->d_trace);
-    cudaFree(s->d_dot);
-    cudaFree(s->d_seg);
-    cudaFree(s->d_flag);
+    free_sliced(s);
+    dev_free(s->d_rowstr);
+    dev_free(s->d_colidx);
+    dev_free(s->d_a);
+    dev_free(s->d_a32);
+    dev_free(s->d_vec);
+    dev_free(s->d_p32);
+    dev_free(s->d_part);
+    dev_free(s->d_sync);
+    dev_free(s->d_status);
+    dev_free(s->d_flag);
+    dev_free(s->d_split);
+    dev_free(s->d_trace);
+    dev_free(s->d_dot);
+    dev_free(s->d_seg);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
 
-// Row split with balanced (stored entries + a per-row allowance for the
-// vector updates) per CTA.
-void make_split(int n, const int *rowstr, int grid, std::vector<int> &split)
+MatrixView matrix_view(cgb_session *s)
 {
-    split.assign(grid + 1, n);
-    const double per_row = 8.0;
-    const double total = double(rowstr[n]) + per_row * n;
-    int j = 0;
-    split[0] = 0;
-    for (int c = 1; c < grid; c++) {
-        const double target = total * c / grid;
-        while (j < n && double(rowstr[j]) + per_row * j < target) j++;
-        split[c] = j;
-    }
-    split[grid] = n;
+    MatrixView M{};
+    M.rowstr = s->d_rowstr;
+    M.colidx = s->d_colidx;
+    M.a = s->d_a;
+    M.a32 = s->d_a32;
+    M.sval = s->d_sval;
+    M.sval32 = s->d_sval32;
+    M.scol = s->d_scol;
+    M.srow = s->d_srow;
+    M.slice_off = s->d_slice_off;
+    M.slice_width = s->d_slice_width;
+    M.chunk_slice = s->d_chunk_slice;
+    M.nblk = s->nblk;
+    M.width = kSliceWidth;
+    M.max_rows = s->sliced_max_rows;
+    return M;
 }
 
 OuterArgs outer_args(cgb_session *s)
 {
     OuterArgs A{};
     A.n = s->n;
-    A.rowstr = s->d_rowstr;
-    A.colidx = s->d_colidx;
-    A.a = s->d_a;
+    A.M = matrix_view(s);
     A.x = s->x();
     A.z = s->z();
     A.p = s->p();
     A.q = s->q();
     A.r = s->r();
+    A.p32 = s->d_p32;
     A.row_split = s->d_split;
     A.part = s->d_part;
     A.gpad = s->gpad;
@@ -266,16 +311,12 @@ OuterArgs outer_args(cgb_session *s)
     A.gb.gen = s->gen();
     A.gb.status = s->d_status;
     A.gb.limit_ns = s->opts.wait_limit_ns > 0 ? s->opts.wait_limit_ns : kDefaultWaitNs;
-    A.tile.seg = s->d_seg;
-    A.tile.seg_stride = s->seg_stride;
-    A.tile.nblk = s->nblk;
-    A.tile.width = kTileWidth;
-    A.tile.max_rows = s->plan.max_rows;
+    A.refresh_every = 10;
     A.trace = s->d_trace;
     return A;
 }
 
-cudaError_t launch_outer(cgb_session *s, const OuterArgs &A)
+cudaError_t launch_outer(cgb_session *s, OuterKernel k, const OuterArgs &A)
 {
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(s->plan.grid);
@@ -287,75 +328,130 @@ cudaError_t launch_outer(cgb_session *s, const OuterArgs &A)
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, s->plan.outer, A);
+    return cudaLaunchKernelEx(&cfg, k, A);
 }
 
-// Segment table of the column tiling, built on the device from the uploaded
-// CSR (build_segments); also reports whether every row has ascending
-// columns, which the tiled kernels need.
-int build_tiling(cgb_session *s)
+// Segment table of the column blocking, built on the device; also finds
+// whether every row has ascending columns (the sliced layout needs it).
+int build_segments_table(cgb_session *s)
 {
     const int n = s->n;
-    s->nblk = (n + kTileWidth - 1) / kTileWidth;
+    s->nblk = (n + kSliceWidth - 1) / kSliceWidth;
     s->seg_stride = (n + 31) & ~31;
     const size_t count = size_t(s->nblk + 1) * s->seg_stride;
-    cudaFree(s->d_seg);
-    s->d_seg = nullptr;
+    dev_free(s->d_seg);
     if (dev_alloc(&s->d_seg, count) != cudaSuccess)
         return set_error(CGB_ERR_NOMEM, "segment table allocation failed");
     CUDA_TRY(cudaMemsetAsync(s->d_flag, 0, sizeof(int), s->stream));
     build_segments<<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
-        s->d_rowstr, s->d_colidx, n, s->nblk, kTileWidth, s->d_seg, s->seg_stride, s->d_flag);
+        s->d_rowstr, s->d_colidx, n, s->nblk, kSliceWidth, s->d_seg, s->seg_stride, s->d_flag);
     CUDA_TRY(cudaGetLastError());
     int unsorted = 0;
     CUDA_TRY(cudaMemcpyAsync(&unsorted, s->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     s->sorted = (unsorted == 0);
     if (!s->sorted) {
-        cudaFree(s->d_seg);
-        s->d_seg = nullptr;
+        dev_free(s->d_seg);
         s->nblk = 0;
     }
     return CGB_OK;
 }
 
-// Fills `pl` for (kind, lpr, rows): kernels, occupancy-sized cooperative grid,
+// The sliced copy of the matrix for a row split over `grid` CTAs (one per SM).
+int build_sliced(cgb_session *s, int grid)
+{
+    free_sliced(s);
+    std::vector<int> split;
+    make_split(s->n, s->h_rowstr_copy.data(), grid, split);
+    int max_rows = 0;
+    std::vector<int> chunk_slice(size_t(grid) * s->nblk + 1, 0);
+    int total = 0;
+    for (int c = 0; c < grid; c++) {
+        const int rows = split[c + 1] - split[c];
+        max_rows = std::max(max_rows, rows);
+        for (int b = 0; b < s->nblk; b++) {
+            chunk_slice[size_t(c) * s->nblk + b] = total;
+            total += (rows + 31) / 32;
+        }
+    }
+    chunk_slice[size_t(grid) * s->nblk] = total;
+    s->sliced_max_rows = (max_rows + 31) & ~31;
+    if (s->sliced_max_rows >= 0xffff || sliced_smem_bytes(s->sliced_max_rows) > kSmemLimit)
+        return set_error(CGB_ERR_STATE, "sliced layout: %d rows per CTA exceed shared memory", max_rows);
+    const int nchunks = grid * s->nblk;
+    if (dev_alloc(&s->d_chunk_slice, chunk_slice.size()) || dev_alloc(&s->d_srow, size_t(total) * 32) ||
+        dev_alloc(&s->d_slice_width, size_t(total)) || dev_alloc(&s->d_slice_off, size_t(total) + 1))
+        return set_error(CGB_ERR_NOMEM, "sliced layout: metadata allocation failed");
+    CUDA_TRY(cudaMemcpy(s->d_split, split.data(), sizeof(int) * (grid + 1), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->d_chunk_slice, chunk_slice.data(), sizeof(int) * chunk_slice.size(),
+                        cudaMemcpyHostToDevice));
+    slice_sort_rows<<<nchunks, 256, 0, s->stream>>>(s->d_seg, s->seg_stride, s->nblk, s->d_split,
+                                                   s->d_chunk_slice, s->d_srow, s->d_slice_width);
+    CUDA_TRY(cudaGetLastError());
+    slice_offsets<<<1, 1024, 0, s->stream>>>(s->d_slice_width, total, s->d_slice_off);
+    CUDA_TRY(cudaGetLastError());
+    unsigned entries = 0;
+    CUDA_TRY(cudaMemcpyAsync(&entries, s->d_slice_off + total, sizeof(unsigned),
+                             cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->slice_entries = entries;
+    if (dev_alloc(&s->d_sval, size_t(entries) + kPad) || dev_alloc(&s->d_scol, size_t(entries) + kPad) ||
+        (s->opts.keep_fp32_copy && dev_alloc(&s->d_sval32, size_t(entries) + kPad)))
+        return set_error(CGB_ERR_NOMEM, "sliced layout: %u entries do not fit", entries);
+    slice_fill<<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
+        s->d_seg, s->seg_stride, s->nblk, kSliceWidth, s->d_split, s->d_chunk_slice, nchunks,
+        s->d_colidx, s->d_a, s->d_srow, s->d_slice_width, s->d_slice_off, total, s->d_sval,
+        s->d_sval32, s->d_scol);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->sliced_grid = grid;
+    return CGB_OK;
+}
+
+// Fills `pl` for (kind, lpr): kernels, occupancy-sized cooperative grid,
 // shared memory.  Returns false when the configuration cannot run here.
-bool make_plan(cgb_session *s, int kind, int lpr, int rows, Plan *pl)
+bool make_plan(cgb_session *s, int kind, int lpr, Plan *pl)
 {
     Plan P;
     P.kind = kind;
     P.lpr = lpr;
-    P.rows = rows;
-    if (!kernels_for(kind, lpr, rows, &P.outer, &P.spmv)) return false;
     if (kind == kKindRow) {
+        if (!row_kernels(lpr, &P)) return false;
         P.block = s->opts.block_threads ? s->opts.block_threads : 512;
         P.smem = 0;
         // almost nothing lives in shared memory: give L1 the room
-        if (cudaFuncSetAttribute(P.outer, cudaFuncAttributePreferredSharedMemoryCarveout, 0) ||
-            cudaFuncSetAttribute(P.spmv, cudaFuncAttributePreferredSharedMemoryCarveout, 0))
+        for (OuterKernel k : {P.fp64, P.mixed})
+            if (cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 0)) return false;
+        if (cudaFuncSetAttribute(P.spmv, cudaFuncAttributePreferredSharedMemoryCarveout, 0)) return false;
+    } else if (kind == kKindSliced) {
+        // 32-bit slice offsets: keep the padded copy well below 2^32 entries
+        if (!s->sorted || s->d_seg == nullptr || s->n < 2 * kSliceWidth || s->nnz > (1LL << 30))
+            return false;
+        P.fp64 = outer_step_fp64_sliced;
+        P.mixed = outer_step_mixed_sliced;
+        P.spmv = spmv_dot_sliced;
+        P.block = 1024;
+        const int grid = std::min(s->prop.multiProcessorCount, s->n);
+        if (s->sliced_grid != grid && build_sliced(s, grid) != CGB_OK) return false;
+        P.smem = sliced_smem_bytes(s->sliced_max_rows);
+        for (OuterKernel k : {P.fp64, P.mixed})
+            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)))
+                return false;
+        if (cudaFuncSetAttribute(P.spmv, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)))
             return false;
     } else {
-        if (!s->sorted || s->d_seg == nullptr) return false;
-        P.block = 1024;
-        // rows per CTA with one CTA per SM, balanced as make_split does
-        const int grid = std::min(s->prop.multiProcessorCount, s->n);
-        std::vector<int> split;
-        make_split(s->n, s->h_rowstr_copy.data(), grid, split);
-        int mr = 0;
-        for (int c = 0; c < grid; c++) mr = std::max(mr, split[c + 1] - split[c]);
-        P.max_rows = (mr + 31) & ~31;
-        P.smem = tiled_smem_bytes(kTileWidth, P.max_rows);
-        if (P.smem > kSmemLimit) return false;
-        if (cudaFuncSetAttribute(P.outer, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)) ||
-            cudaFuncSetAttribute(P.spmv, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)))
-            return false;
+        return false;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, P.outer, P.block, P.smem) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, P.fp64, P.block, P.smem) != cudaSuccess ||
         per_sm < 1)
         return false;
-    per_sm = std::min(per_sm, kind == kKindTiled ? 1 : 4);
+    int per_sm_mixed = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_mixed, P.mixed, P.block, P.smem) !=
+            cudaSuccess ||
+        per_sm_mixed < 1)
+        return false;
+    per_sm = std::min({per_sm, per_sm_mixed, kind == kKindSliced ? 1 : 4});
     P.grid = std::max(1, std::min(per_sm * s->prop.multiProcessorCount, s->n));
     if (P.grid > s->gpad) return false;
     *pl = P;
@@ -373,21 +469,26 @@ int apply_plan(cgb_session *s, const Plan &pl)
     return CGB_OK;
 }
 
-SpmvArgs spmv_args(cgb_session *s)
+SpmvArgs spmv_args(cgb_session *s, int fp32)
 {
     SpmvArgs S{};
     S.A = outer_args(s);
     S.ticket = s->ticket();
     S.dot = s->d_dot;
+    S.fp32 = fp32;
     return S;
 }
 
 // Mean device ms of `reps` standalone SpMV launches under the current plan.
-int time_plan_spmv(cgb_session *s, int reps, double *ms_out)
+int time_plan_spmv(cgb_session *s, int reps, int fp32, double *ms_out)
 {
-    SpmvArgs S = spmv_args(s);
+    if (fp32 && !s->d_a32) return set_error(CGB_ERR_STATE, "no FP32 copy (keep_fp32_copy = 0)");
+    SpmvArgs S = spmv_args(s, fp32);
     const Plan &P = s->plan;
     fill_ones<<<s->prop.multiProcessorCount, 256, 0, s->stream>>>(s->p(), s->n + 1);
+    if (fp32) {
+        to_fp32<<<s->prop.multiProcessorCount, 256, 0, s->stream>>>(s->p(), s->d_p32, s->n + 1);
+    }
     for (int i = 0; i < 2; i++) P.spmv<<<P.grid, P.block, P.smem, s->stream>>>(S);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaEventRecord(s->ev0, s->stream));
@@ -408,35 +509,26 @@ int time_plan_spmv(cgb_session *s, int reps, double *ms_out)
 }
 
 // Picks the plan: the one the options force, else the fastest standalone
-// SpMV among the candidates (the session's autotuner).
+// FP64 SpMV among the candidates (the session's autotuner).
 int choose_plan(cgb_session *s)
 {
     const cgb_options &o = s->opts;
     const double mean = double(s->nnz) / double(s->n);
     std::vector<Plan> cands;
-    auto add = [&](int kind, int lpr, int rows) {
+    auto add = [&](int kind, int lpr) {
         Plan p;
-        if (make_plan(s, kind, lpr, rows, &p)) cands.push_back(p);
+        if (make_plan(s, kind, lpr, &p)) cands.push_back(p);
     };
-    const int want_kind = o.spmv_kernel;
-    if (want_kind == 0 || want_kind == kKindRow) {
-        if (o.lanes_per_row > 0) add(kKindRow, o.lanes_per_row, 1);
+    const int want = o.spmv_kernel;
+    if (want == 0 || want == kKindRow) {
+        if (o.lanes_per_row > 0) add(kKindRow, o.lanes_per_row);
         else {
             const int l = lanes_for_mean(mean);
-            add(kKindRow, l, 1);
-            if (want_kind == 0 && l > 2) add(kKindRow, l / 2, 1);
+            add(kKindRow, l);
+            if (want == 0 && l > 2) add(kKindRow, l / 2);
         }
     }
-    if ((want_kind == 0 || want_kind == kKindTiled) && s->sorted && s->n >= 2 * kTileWidth) {
-        if (o.lanes_per_row > 0) {
-            add(kKindTiled, o.lanes_per_row, o.rows_in_flight > 0 ? o.rows_in_flight : 1);
-        } else {
-            add(kKindTiled, 4, 2);
-            add(kKindTiled, 8, 2);
-            add(kKindTiled, 8, 1);
-            add(kKindTiled, 16, 1);
-        }
-    }
+    if (want == 0 || want == kKindSliced) add(kKindSliced, 0);
     if (cands.empty()) return set_error(CGB_ERR_INVALID, "no kernel configuration fits these options");
     if (cands.size() == 1) return apply_plan(s, cands[0]);
     double best = 1e30;
@@ -445,7 +537,7 @@ int choose_plan(cgb_session *s)
         int st = apply_plan(s, cands[i]);
         if (st) return st;
         double ms = 0.0;
-        st = time_plan_spmv(s, 10, &ms);
+        st = time_plan_spmv(s, 10, 0, &ms);
         if (st) return st;
         if (ms < best) {
             best = ms;
@@ -459,12 +551,12 @@ int upload_matrix(cgb_session *s, const int *rowstr, const int *colidx, const do
 {
     const long long nnz = rowstr[s->n];
     if (nnz > s->nnz_cap) {
-        cudaFree(s->d_colidx);
-        cudaFree(s->d_a);
-        s->d_colidx = nullptr;
-        s->d_a = nullptr;
+        dev_free(s->d_colidx);
+        dev_free(s->d_a);
+        dev_free(s->d_a32);
         if (dev_alloc(&s->d_colidx, nnz + kPad) != cudaSuccess ||
-            dev_alloc(&s->d_a, nnz + kPad) != cudaSuccess)
+            dev_alloc(&s->d_a, nnz + kPad) != cudaSuccess ||
+            (s->opts.keep_fp32_copy && dev_alloc(&s->d_a32, nnz + kPad) != cudaSuccess))
             return set_error(CGB_ERR_NOMEM, "device allocation of %lld entries failed", nnz);
         s->nnz_cap = nnz;
     }
@@ -476,26 +568,31 @@ int upload_matrix(cgb_session *s, const int *rowstr, const int *colidx, const do
     CUDA_TRY(cudaMemcpyAsync(s->d_a, a, sizeof(double) * nnz, cudaMemcpyHostToDevice, s->stream));
     CUDA_TRY(cudaMemsetAsync(s->d_colidx + nnz, 0, sizeof(int) * kPad, s->stream));
     CUDA_TRY(cudaMemsetAsync(s->d_a + nnz, 0, sizeof(double) * kPad, s->stream));
+    if (s->d_a32) {
+        to_fp32<<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(s->d_a, s->d_a32, nnz + kPad);
+        CUDA_TRY(cudaGetLastError());
+    }
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     s->h_rowstr = rowstr;
     s->h_colidx = colidx;
     s->h_a = a;
     // same row pointers as before (e.g. the same matrix uploaded again): the
-    // row split and tuned plan still hold; only the segment table is rebuilt
-    const bool same_rows = s->plan.outer != nullptr &&
+    // row split and tuned plan still hold; the column tables are rebuilt
+    const bool same_rows = s->plan.fp64 != nullptr &&
                            s->h_rowstr_copy.size() == size_t(s->n) + 1 &&
                            std::equal(rowstr, rowstr + s->n + 1, s->h_rowstr_copy.begin());
     s->h_rowstr_copy.assign(rowstr, rowstr + s->n + 1);
-    const bool was_tiled = s->plan.kind == kKindTiled;
+    const int kept_kind = s->plan.kind;
+    const int kept_grid = s->sliced_grid;
+    free_sliced(s);
+    dev_free(s->d_seg);
     s->sorted = false;
-    cudaFree(s->d_seg);
-    s->d_seg = nullptr;
     s->nblk = 0;
-    if (s->n >= 2 * kTileWidth) {
-        int st = build_tiling(s);
+    if (s->n >= 2 * kSliceWidth) {
+        int st = build_segments_table(s);
         if (st) return st;
     }
-    if (same_rows && (!was_tiled || s->sorted)) {
+    if (same_rows && (kept_kind == kKindRow || (s->sorted && build_sliced(s, kept_grid) == CGB_OK))) {
         drop_graph(s);
         return CGB_OK;
     }
@@ -506,8 +603,7 @@ int upload_matrix(cgb_session *s, const int *rowstr, const int *colidx, const do
 int ensure_trace(cgb_session *s, int niter)
 {
     if (niter <= s->trace_cap) return CGB_OK;
-    cudaFree(s->d_trace);
-    s->d_trace = nullptr;
+    dev_free(s->d_trace);
     if (dev_alloc(&s->d_trace, size_t(niter)) != cudaSuccess)
         return set_error(CGB_ERR_NOMEM, "trace allocation failed");
     s->trace_cap = niter;
@@ -525,11 +621,13 @@ int collect_status(cgb_session *s)
     CUDA_TRY(cudaMemset(s->d_sync, 0, sizeof(unsigned) * 96));
     CUDA_TRY(cudaMemset(s->d_status, 0, sizeof(int)));
     if (st == kDevTimeout)
-        return set_error(CGB_ERR_TIMEOUT, "a grid barrier wait hit its %lld ns limit",
+        return set_error(CGB_ERR_TIMEOUT, "a device wait hit its %lld ns limit",
                          (long long)(s->opts.wait_limit_ns > 0 ? s->opts.wait_limit_ns : kDefaultWaitNs));
     if (st == kDevNonFinite) return set_error(CGB_ERR_NUMERIC, "non-finite zeta or residual");
     return set_error(CGB_ERR_CUDA, "device status %d", st);
 }
+
+bool is_mixed(int mode) { return mode == CGB_MODE_MIXED; }
 
 // Enqueues one power iteration (x = 1, then niter outer-step kernels) on the
 // session stream.
@@ -547,25 +645,35 @@ cudaError_t enqueue_power(cgb_session *s, const cgb_solve_params &P)
     A.fixed = (P.mode == CGB_MODE_FP64) ? 1 : 0;
     A.tol = P.tol;
     A.warm = P.warm_start;
+    A.refresh_every = P.refresh_every > 0 ? P.refresh_every : 10;
     A.finish = 1;
+    const OuterKernel k = is_mixed(P.mode) ? s->plan.mixed : s->plan.fp64;
     for (int it = 0; it < P.niter; it++) {
         A.step = it;
-        e = launch_outer(s, A);
+        e = launch_outer(s, k, A);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
 }
 
-int check_params(const cgb_solve_params &P)
+int check_params(cgb_session *s, const cgb_solve_params &P)
 {
     if (P.niter < 1) return set_error(CGB_ERR_INVALID, "niter must be >= 1");
     if (P.cgitmax < 0) return set_error(CGB_ERR_INVALID, "cgitmax must be >= 0");
     if (!std::isfinite(P.shift)) return set_error(CGB_ERR_INVALID, "shift must be finite");
-    if (P.mode != CGB_MODE_FP64 && P.mode != CGB_MODE_FP64_TOL)
+    if (P.mode != CGB_MODE_FP64 && P.mode != CGB_MODE_FP64_TOL && P.mode != CGB_MODE_MIXED)
         return set_error(CGB_ERR_INVALID, "mode %d is not available in this build", P.mode);
     if (P.mode != CGB_MODE_FP64 && !(P.tol > 0.0))
         return set_error(CGB_ERR_INVALID, "tolerance modes need tol > 0");
+    if (is_mixed(P.mode) && !s->d_a32)
+        return set_error(CGB_ERR_STATE, "mixed mode needs the FP32 copy (keep_fp32_copy = 1)");
     return CGB_OK;
+}
+
+bool same_params(const cgb_solve_params &a, const cgb_solve_params &b)
+{
+    return a.niter == b.niter && a.shift == b.shift && a.mode == b.mode && a.cgitmax == b.cgitmax &&
+           a.tol == b.tol && a.refresh_every == b.refresh_every && a.warm_start == b.warm_start;
 }
 
 }  // namespace
@@ -593,7 +701,7 @@ const char *cgb_status_string(int status)
 
 const char *cgb_last_error(void) { return cgb::g_last_error; }
 
-int cgb_version(void) { return 10000 * 0 + 100 * 1 + 0; }
+int cgb_version(void) { return 10000 * 0 + 100 * 2 + 0; }
 
 long long cgb_nz_bound(int n, int nonzer)
 {
@@ -617,7 +725,6 @@ void cgb_default_options(cgb_options *o)
     o->use_graph = 1;
     o->keep_fp32_copy = 1;
     o->spmv_kernel = 0;
-    o->rows_in_flight = 0;
 }
 
 void cgb_default_solve_params(cgb_solve_params *p)
@@ -664,9 +771,7 @@ int cgb_create(int n, const int *rowstr, const int *colidx, const double *a,
     if (o.block_threads != 0 && o.block_threads != 256 && o.block_threads != 512)
         return set_error(CGB_ERR_INVALID, "block_threads must be 0, 256 or 512");
     if (o.spmv_kernel < 0 || o.spmv_kernel > 2)
-        return set_error(CGB_ERR_INVALID, "spmv_kernel must be 0 (auto), 1 (row) or 2 (tiled)");
-    if (o.rows_in_flight < 0 || o.rows_in_flight > 2)
-        return set_error(CGB_ERR_INVALID, "rows_in_flight must be 0, 1 or 2");
+        return set_error(CGB_ERR_INVALID, "spmv_kernel must be 0 (auto), 1 (row) or 2 (sliced)");
     cudaDeviceProp prop;
     st = check_device(o.device, &prop);
     if (st) return st;
@@ -678,7 +783,7 @@ int cgb_create(int n, const int *rowstr, const int *colidx, const double *a,
     s->n = n;
     s->opts = o;
     s->prop = prop;
-    s->vstride = (size_t(n) + 2 + 31) & ~size_t(31);
+    s->vstride = (size_t(n) + 8 + 31) & ~size_t(31);
     s->gpad = 4 * prop.multiProcessorCount;
 #define CREATE_TRY(call)                                                                  \
     do {                                                                                  \
@@ -696,14 +801,16 @@ int cgb_create(int n, const int *rowstr, const int *colidx, const double *a,
     CREATE_TRY(dev_alloc(&s->d_rowstr, size_t(n) + 1));
     CREATE_TRY(dev_alloc(&s->d_vec, 5 * s->vstride));
     CREATE_TRY(cudaMemset(s->d_vec, 0, sizeof(double) * 5 * s->vstride));
+    CREATE_TRY(dev_alloc(&s->d_p32, s->vstride));
+    CREATE_TRY(cudaMemset(s->d_p32, 0, sizeof(float) * s->vstride));
     CREATE_TRY(dev_alloc(&s->d_part, size_t(kSlotCount) * s->gpad));
     CREATE_TRY(dev_alloc(&s->d_sync, 96));
     CREATE_TRY(cudaMemset(s->d_sync, 0, sizeof(unsigned) * 96));
     CREATE_TRY(dev_alloc(&s->d_status, 1));
     CREATE_TRY(cudaMemset(s->d_status, 0, sizeof(int)));
+    CREATE_TRY(dev_alloc(&s->d_flag, 1));
     CREATE_TRY(dev_alloc(&s->d_split, size_t(s->gpad) + 1));
     CREATE_TRY(dev_alloc(&s->d_dot, 1));
-    CREATE_TRY(dev_alloc(&s->d_flag, 1));
 #undef CREATE_TRY
     st = ensure_trace(s, 128);
     if (st == CGB_OK) st = upload_matrix(s, rowstr, colidx, a);
@@ -751,7 +858,7 @@ int cgb_conj_grad(cgb_session *s, const int *colidx, const int *rowstr, const do
     A.warm = 0;
     A.step = 0;
     A.finish = 0;
-    CUDA_TRY(launch_outer(s, A));
+    CUDA_TRY(launch_outer(s, s->plan.fp64, A));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     int st = collect_status(s);
     if (st) return st;
@@ -771,17 +878,13 @@ int cgb_power_iterate(cgb_session *s, const cgb_solve_params *params, double *ze
 {
     if (!s || !params) return set_error(CGB_ERR_INVALID, "null session or params");
     const cgb_solve_params P = *params;
-    int st = check_params(P);
+    int st = check_params(s, P);
     if (st) return st;
     CUDA_TRY(cudaSetDevice(s->device));
     st = ensure_trace(s, P.niter);
     if (st) return st;
-    const int fixed = P.mode == CGB_MODE_FP64 ? 1 : 0;
     if (s->opts.use_graph) {
-        const bool same = s->graph && s->g_niter == P.niter && s->g_cgitmax == P.cgitmax &&
-                          s->g_fixed == fixed && s->g_warm == P.warm_start &&
-                          s->g_shift == P.shift && s->g_tol == P.tol;
-        if (!same) {
+        if (!(s->g_valid && same_params(s->g_params, P))) {
             drop_graph(s);
             cudaGraph_t g = nullptr;
             CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
@@ -798,12 +901,8 @@ int cgb_power_iterate(cgb_session *s, const cgb_solve_params *params, double *ze
                 s->graph = nullptr;
                 return set_error(CGB_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
             }
-            s->g_niter = P.niter;
-            s->g_cgitmax = P.cgitmax;
-            s->g_fixed = fixed;
-            s->g_warm = P.warm_start;
-            s->g_shift = P.shift;
-            s->g_tol = P.tol;
+            s->g_params = P;
+            s->g_valid = true;
         }
         CUDA_TRY(cudaEventRecord(s->ev0, s->stream));
         CUDA_TRY(cudaGraphLaunch(s->graph, s->stream));
@@ -820,12 +919,13 @@ int cgb_power_iterate(cgb_session *s, const cgb_solve_params *params, double *ze
     CUDA_TRY(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     std::vector<StepTrace> tr(P.niter);
     CUDA_TRY(cudaMemcpy(tr.data(), s->d_trace, sizeof(StepTrace) * P.niter, cudaMemcpyDeviceToHost));
-    int total_inner = 0;
+    int total_inner = 0, refreshes = 0;
     for (int i = 0; i < P.niter; i++) {
         if (zeta_trace) zeta_trace[i] = tr[i].zeta;
         if (rnorm_trace) rnorm_trace[i] = tr[i].rnorm;
         if (iters_trace) iters_trace[i] = int(tr[i].inner);
         total_inner += int(tr[i].inner);
+        refreshes += int(tr[i].refresh);
     }
     if (x_out) CUDA_TRY(cudaMemcpy(x_out, s->x(), sizeof(double) * s->n, cudaMemcpyDeviceToHost));
     if (res) {
@@ -834,6 +934,7 @@ int cgb_power_iterate(cgb_session *s, const cgb_solve_params *params, double *ze
         res->device_ms = ms;
         res->total_inner = total_inner;
         res->fallbacks = 0;
+        res->refreshes = refreshes;
     }
     return CGB_OK;
 }
@@ -841,21 +942,20 @@ int cgb_power_iterate(cgb_session *s, const cgb_solve_params *params, double *ze
 int cgb_time_spmv(cgb_session *s, int reps, int fp32, double *ms_per_launch)
 {
     if (!s || reps < 1 || !ms_per_launch) return set_error(CGB_ERR_INVALID, "bad arguments");
-    if (fp32) return set_error(CGB_ERR_INVALID, "FP32 SpMV is not available in this build");
     CUDA_TRY(cudaSetDevice(s->device));
-    return time_plan_spmv(s, reps, ms_per_launch);
+    return time_plan_spmv(s, reps, fp32 ? 1 : 0, ms_per_launch);
 }
 
-int cgb_plan_info(cgb_session *s, int *kind, int *lanes_per_row, int *rows_in_flight, int *grid,
-                  int *block, long long *smem_bytes)
+int cgb_plan_info(cgb_session *s, int *kind, int *lanes_per_row, int *grid, int *block,
+                  long long *smem_bytes, long long *layout_entries)
 {
     if (!s) return set_error(CGB_ERR_INVALID, "session is null");
     if (kind) *kind = s->plan.kind;
     if (lanes_per_row) *lanes_per_row = s->plan.lpr;
-    if (rows_in_flight) *rows_in_flight = s->plan.rows;
     if (grid) *grid = s->plan.grid;
     if (block) *block = s->plan.block;
     if (smem_bytes) *smem_bytes = (long long)s->plan.smem;
+    if (layout_entries) *layout_entries = s->plan.kind == kKindSliced ? s->slice_entries : s->nnz;
     return CGB_OK;
 }
 
@@ -879,7 +979,7 @@ int cgb_time_outer_steps(cgb_session *s, int niter, double shift, double *kernel
     for (int it = 0; it < niter; it++) {
         CUDA_TRY(cudaEventRecord(ev[it], s->stream));
         A.step = it;
-        CUDA_TRY(launch_outer(s, A));
+        CUDA_TRY(launch_outer(s, s->plan.fp64, A));
     }
     CUDA_TRY(cudaEventRecord(ev[niter], s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));

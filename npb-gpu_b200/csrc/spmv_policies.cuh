@@ -1,0 +1,354 @@
+// spmv_policies.cuh -- the two SpMV policies of the persistent CG kernels.
+//
+// Both compute out[j] = (A v)[j] for the rows [row0, row1) the CTA owns and
+// return this thread's share of dotv . out (FP64).  They are generic in the
+// value type VT: double for the FP64 solver (the reference's precision,
+// cg.cu:691-697), float for the FP32 SpMV of the mixed-precision solver
+// (matrix values and gathered vector in FP32, FP32 accumulation per row).
+//
+//   RowSpmv<LPR>   CSR as the reference stores it; LPR lanes per row, each
+//                  lane two consecutive entries per chunk (one 16/8-byte load
+//                  of values, one 8-byte load of indices, from an even start,
+//                  masked to the row), four chunks in flight; the gathered
+//                  vector is read through L1/L2.
+//   SlicedSpmv     a sliced copy of the matrix built on the device (see
+//                  slices.cuh): per CTA and per column block of W columns,
+//                  the CTA's rows sorted by length and packed 32 to a slice,
+//                  stored column-major (entry k of the slice's lane i at
+//                  offset + 32 k + i) with 16-bit local columns.  The block
+//                  of v is staged in shared memory by TMA bulk copies
+//                  (cp.async.bulk + mbarrier) into a 2-slot ring; warps walk
+//                  the blocks independently and the last warp done with a
+//                  block refills its slot with block b+2, so no CTA-wide
+//                  barrier sits between blocks.  Gathers are shared-memory
+//                  loads; each row accumulates in registers, then into one of
+//                  two shared accumulators (by block parity: blocks b and b+1
+//                  may run at once, b+2 only after all of b), summed at the
+//                  end -- deterministic.
+#pragma once
+
+#include "device_common.cuh"
+
+namespace cgb {
+
+template <typename VT>
+struct Pair;
+template <>
+struct Pair<double> {
+    using T = double2;
+};
+template <>
+struct Pair<float> {
+    using T = float2;
+};
+
+__device__ __forceinline__ double fma_vt(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float fma_vt(float a, float b, float c) { return fmaf(a, b, c); }
+
+template <int W, typename VT>
+__device__ __forceinline__ VT group_sum_vt(VT v, unsigned mask)
+{
+#pragma unroll
+    for (int off = W / 2; off > 0; off >>= 1) v += __shfl_xor_sync(mask, v, off);
+    return v;
+}
+
+// Matrix in both layouts, both precisions (unused members may be null).
+struct MatrixView {
+    const int *__restrict__ rowstr;
+    const int *__restrict__ colidx;
+    const double *__restrict__ a;      // FP64 values (CSR order)
+    const float *__restrict__ a32;     // FP32 values (CSR order), mixed mode
+    // sliced layout
+    const double *__restrict__ sval;   // FP64 values, slice order
+    const float *__restrict__ sval32;  // FP32 values, slice order
+    const unsigned short *__restrict__ scol;  // column - b*W
+    const unsigned short *__restrict__ srow;  // local row per (slice, lane); 0xffff = none
+    const unsigned *__restrict__ slice_off;   // first entry of each slice
+    const int *__restrict__ slice_width;      // steps of each slice
+    const int *__restrict__ chunk_slice;      // (c*nblk + b) -> first slice
+    int nblk;                                 // column blocks
+    int width;                                // columns per block
+    int max_rows;                             // shared accumulator capacity
+};
+
+template <typename VT>
+__device__ __forceinline__ const VT *csr_values(const MatrixView &M);
+template <>
+__device__ __forceinline__ const double *csr_values<double>(const MatrixView &M) { return M.a; }
+template <>
+__device__ __forceinline__ const float *csr_values<float>(const MatrixView &M) { return M.a32; }
+template <typename VT>
+__device__ __forceinline__ const VT *slice_values(const MatrixView &M);
+template <>
+__device__ __forceinline__ const double *slice_values<double>(const MatrixView &M) { return M.sval; }
+template <>
+__device__ __forceinline__ const float *slice_values<float>(const MatrixView &M) { return M.sval32; }
+
+// ------------------------------------------------------------ row policy
+template <int LPR, typename VT>
+__device__ __forceinline__ double spmv_rows(const MatrixView &M, const VT *v, double *out, int row0,
+                                            int row1, const double *dotv)
+{
+    using P2 = typename Pair<VT>::T;
+    constexpr int kStep = 2 * LPR;
+    constexpr int kUnroll = 4;
+    const VT *__restrict__ a = csr_values<VT>(M);
+    const int lane = threadIdx.x % LPR;
+    const int grp = threadIdx.x / LPR;
+    const int ngrp = blockDim.x / LPR;
+    const unsigned mask =
+        LPR == 32 ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) & ~(LPR - 1)));
+    double dacc = 0.0;
+    for (int row = row0 + grp; row < row1; row += ngrp) {
+        const int k0 = __ldg(M.rowstr + row);
+        const int k1 = __ldg(M.rowstr + row + 1);
+        VT s = VT(0);
+        for (int k = (k0 & ~1) + 2 * lane; k < k1; k += kUnroll * kStep) {
+            P2 av[kUnroll];
+            int2 cv[kUnroll];
+#pragma unroll
+            for (int u = 0; u < kUnroll; u++) {
+                const int kk = k + u * kStep;
+                if (kk < k1) {
+                    av[u] = __ldcs(reinterpret_cast<const P2 *>(a + kk));
+                    cv[u] = __ldcs(reinterpret_cast<const int2 *>(M.colidx + kk));
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kUnroll; u++) {
+                const int kk = k + u * kStep;
+                if (kk < k1) {
+                    if (kk >= k0) s = fma_vt(av[u].x, v[cv[u].x], s);
+                    if (kk + 1 < k1) s = fma_vt(av[u].y, v[cv[u].y], s);
+                }
+            }
+        }
+        s = group_sum_vt<LPR>(s, mask);
+        if (lane == 0) {
+            const double t = double(s);
+            out[row] = t;
+            if (dotv) dacc = fma(dotv[row], t, dacc);
+        }
+    }
+    return dacc;
+}
+
+template <int LPR>
+struct RowSpmv {
+    int row0, row1;
+    __device__ void setup(const MatrixView &, int r0, int r1)
+    {
+        row0 = r0;
+        row1 = r1;
+    }
+    template <typename VT>
+    __device__ __forceinline__ double apply(const MatrixView &M, const VT *v, double *out,
+                                            const double *dotv, int, long long, int *, bool &ok)
+    {
+        ok = true;
+        return spmv_rows<LPR, VT>(M, v, out, row0, row1, dotv);
+    }
+};
+
+// ---------------------------------------------------------- sliced policy
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+                 : "memory");
+}
+
+// Orders this thread's earlier generic-proxy accesses (and those it has
+// observed) before its later async-proxy (TMA) accesses.
+__device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async;" ::: "memory");
+}
+
+// 1-D bulk copy global -> shared completing on `bar`; issued by one thread.
+// src, dst 16-byte aligned, bytes a multiple of 16.  Never multicast.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes,
+                                          uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Bounded wait for phase `parity` of `bar`; gives up after limit_ns or when
+// *abort is set by another warp of the CTA.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, long long limit_ns,
+                                          volatile int *abort)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try_wait(bar, parity)) {
+        if (abort && *abort) return false;
+        if ((long long)(global_ns() - t0) > limit_ns) return false;
+    }
+    return true;
+}
+
+// Bytes of one staging slot and dynamic shared memory of SlicedSpmv.
+constexpr int kSliceWidth = 12288;  // columns per block
+constexpr unsigned kSlotBytes = kSliceWidth * 8u;
+__host__ __device__ inline size_t sliced_smem_bytes(int max_rows)
+{
+    return 2 * size_t(kSlotBytes) + 2 * size_t(max_rows) * sizeof(double) + 128;
+}
+
+struct SlicedSpmv {
+    int row0, row1, chunk0;  // chunk0 = blockIdx.x * nblk
+    unsigned char *buf;      // 2 slots
+    double *acc0, *acc1;     // max_rows each
+    uint64_t *bars;          // 2 "full" barriers
+    int *cnt;                // 2 per-slot completion counters
+    int *abort;
+    unsigned parity;         // bit i: next phase parity of slot i
+
+    __device__ void setup(const MatrixView &M, int r0, int r1)
+    {
+        extern __shared__ __align__(128) unsigned char sliced_smem[];
+        row0 = r0;
+        row1 = r1;
+        chunk0 = blockIdx.x * M.nblk;
+        buf = sliced_smem;
+        acc0 = reinterpret_cast<double *>(sliced_smem + 2 * size_t(kSlotBytes));
+        acc1 = acc0 + M.max_rows;
+        bars = reinterpret_cast<uint64_t *>(acc1 + M.max_rows);
+        cnt = reinterpret_cast<int *>(bars + 2);
+        abort = cnt + 2;
+        parity = 0;
+        if (threadIdx.x == 0) {
+            mbar_init(&bars[0], 1);
+            mbar_init(&bars[1], 1);
+            cnt[0] = cnt[1] = 0;
+            *abort = 0;
+        }
+        __syncthreads();
+    }
+
+    template <typename VT>
+    __device__ __forceinline__ void issue(const MatrixView &M, const VT *v, int n, int b, int slot)
+    {
+        const int cols = min(M.width, n - b * M.width);
+        const unsigned bytes = (unsigned(cols) * unsigned(sizeof(VT)) + 15u) & ~15u;
+        bulk_load(buf + size_t(slot) * kSlotBytes, v + size_t(b) * M.width, bytes, &bars[slot]);
+    }
+
+    template <typename VT>
+    __device__ __forceinline__ double apply(const MatrixView &M, const VT *v, double *out,
+                                            const double *dotv, int n, long long limit_ns,
+                                            int *status, bool &ok)
+    {
+        constexpr int kU = 8;  // slice steps in flight per lane
+        const VT *__restrict__ vals = slice_values<VT>(M);
+        const int lane = threadIdx.x & 31;
+        const int warp = threadIdx.x >> 5;
+        const int nwarps = blockDim.x >> 5;
+        const int nrows = row1 - row0;
+        for (int i = threadIdx.x; i < nrows; i += blockDim.x) {
+            acc0[i] = 0.0;
+            acc1[i] = 0.0;
+        }
+        if (threadIdx.x == 0) {
+            fence_proxy_async();  // v was written by generic stores before the grid barrier
+            issue(M, v, n, 0, 0);
+            if (M.nblk > 1) issue(M, v, n, 1, 1);
+        }
+        __syncthreads();
+        bool failed = false;
+        for (int b = 0; b < M.nblk && !failed; b++) {
+            const int slot = b & 1;
+            if (!mbar_wait(&bars[slot], (parity >> slot) & 1u, limit_ns, abort)) {
+                failed = true;
+                *abort = 1;
+                break;
+            }
+            parity ^= 1u << slot;
+            const VT *pv = reinterpret_cast<const VT *>(buf + size_t(slot) * kSlotBytes);
+            double *accb = (b & 1) ? acc1 : acc0;
+            const int s0 = __ldg(M.chunk_slice + chunk0 + b);
+            const int s1 = __ldg(M.chunk_slice + chunk0 + b + 1);
+            // rotate the warp -> slice assignment from block to block so the
+            // widest slices do not always land on the same warps
+            const int rot = (b * 7) % nwarps;
+            for (int s = s0 + (warp + rot) % nwarps; s < s1; s += nwarps) {
+                const unsigned off = __ldg(M.slice_off + s) + lane;
+                const int w = __ldg(M.slice_width + s);
+                const unsigned short row = __ldg(M.srow + size_t(s) * 32 + lane);
+                VT sum = VT(0);
+                for (int k = 0; k < w; k += kU) {
+                    VT av[kU];
+                    unsigned short cv[kU];
+#pragma unroll
+                    for (int u = 0; u < kU; u++) {
+                        if (k + u < w) {
+                            av[u] = __ldcs(vals + off + 32u * unsigned(k + u));
+                            cv[u] = __ldcs(M.scol + off + 32u * unsigned(k + u));
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kU; u++)
+                        if (k + u < w) sum = fma_vt(av[u], pv[cv[u]], sum);
+                }
+                if (row != 0xffffu) accb[row] += double(sum);
+            }
+            __syncwarp();
+            if (lane == 0) {
+                __threadfence_block();
+                if (atomicAdd(&cnt[slot], 1) == nwarps - 1) {
+                    cnt[slot] = 0;
+                    if (b + 2 < M.nblk) {
+                        fence_proxy_async();  // all warps' reads of the slot before the refill
+                        issue(M, v, n, b + 2, slot);
+                    }
+                }
+            }
+        }
+        if (__syncthreads_or(failed)) {
+            ok = false;
+            if (threadIdx.x == 0) {
+                raise_status(status, kDevTimeout);
+                // let issued copies land before the CTA leaves (a completed
+                // phase returns at once)
+                (void)mbar_wait(&bars[0], (parity & 1u), limit_ns, nullptr);
+                (void)mbar_wait(&bars[1], (parity >> 1) & 1u, limit_ns, nullptr);
+            }
+            __syncthreads();
+            return 0.0;
+        }
+        double dacc = 0.0;
+        for (int i = threadIdx.x; i < nrows; i += blockDim.x) {
+            const double t = acc0[i] + acc1[i];
+            out[row0 + i] = t;
+            if (dotv) dacc = fma(dotv[row0 + i], t, dacc);
+        }
+        ok = true;
+        return dacc;
+    }
+};
+
+}  // namespace cgb

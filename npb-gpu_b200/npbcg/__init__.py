@@ -64,7 +64,7 @@ class Options(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("lanes_per_row", ctypes.c_int),
                 ("block_threads", ctypes.c_int), ("wait_limit_ns", ctypes.c_longlong),
                 ("use_graph", ctypes.c_int), ("keep_fp32_copy", ctypes.c_int),
-                ("spmv_kernel", ctypes.c_int), ("rows_in_flight", ctypes.c_int)]
+                ("spmv_kernel", ctypes.c_int)]
 
 
 class SolveParams(ctypes.Structure):
@@ -76,7 +76,7 @@ class SolveParams(ctypes.Structure):
 class SolveResult(ctypes.Structure):
     _fields_ = [("zeta", ctypes.c_double), ("rnorm", ctypes.c_double),
                 ("device_ms", ctypes.c_double), ("total_inner", ctypes.c_int),
-                ("fallbacks", ctypes.c_int)]
+                ("fallbacks", ctypes.c_int), ("refreshes", ctypes.c_int)]
 
 
 _I32 = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
@@ -108,8 +108,8 @@ _SIGNATURES = {
     "cgb_time_outer_steps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
                                             ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_double)]),
-    "cgb_plan_info": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int)] * 5 +
-                      [ctypes.POINTER(ctypes.c_longlong)]),
+    "cgb_plan_info": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int)] * 4 +
+                      [ctypes.POINTER(ctypes.c_longlong)] * 2),
     "cgb_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong,
                                                  ctypes.POINTER(ctypes.c_int)]),
     "cgb_conj_grad_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_longlong] +
@@ -240,7 +240,8 @@ class Session:
         _check(lib().cgb_power_iterate(self._h, ctypes.byref(P), _ptr(zt), _ptr(rt), _ptr(it),
                                        _ptr(x), ctypes.byref(res)))
         out = dict(zeta=zt, rnorm=rt, iters=it, device_ms=res.device_ms,
-                   total_inner=res.total_inner, fallbacks=res.fallbacks)
+                   total_inner=res.total_inner, fallbacks=res.fallbacks,
+                   refreshes=res.refreshes)
         if want_x:
             out["x"] = x
         return out
@@ -257,12 +258,13 @@ class Session:
 
     def plan(self):
         """The kernel configuration chosen for this matrix."""
-        v = [ctypes.c_int() for _ in range(5)]
-        smem = ctypes.c_longlong()
-        _check(lib().cgb_plan_info(self._h, *[ctypes.byref(x) for x in v], ctypes.byref(smem)))
-        kind, lpr, rows, grid, block = (x.value for x in v)
-        return dict(kind={1: "row", 2: "tiled"}.get(kind, kind), lanes_per_row=lpr,
-                    rows_in_flight=rows, grid=grid, block=block, smem=smem.value)
+        v = [ctypes.c_int() for _ in range(4)]
+        smem, entries = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(lib().cgb_plan_info(self._h, *[ctypes.byref(x) for x in v], ctypes.byref(smem),
+                                   ctypes.byref(entries)))
+        kind, lpr, grid, block = (x.value for x in v)
+        return dict(kind={1: "row", 2: "sliced"}.get(kind, kind), lanes_per_row=lpr, grid=grid,
+                    block=block, smem=smem.value, layout_entries=entries.value)
 
     def selftest_wait_timeout(self, limit_ns):
         """Returns (status, device_status) of the bounded-wait self-test."""

@@ -25,8 +25,7 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--niter", type=int, default=2)
     ap.add_argument("--lanes", type=int, default=0)
-    ap.add_argument("--kind", type=int, default=0, help="0 auto, 1 row, 2 column-tiled")
-    ap.add_argument("--rows", type=int, default=0, help="tiled: rows in flight per group")
+    ap.add_argument("--kind", type=int, default=0, help="0 auto, 1 row, 2 sliced")
     ap.add_argument("--fp32", action="store_true")
     a = ap.parse_args()
     c = npbcg.CLASSES[a.cls]
@@ -35,24 +34,24 @@ def main():
     out = {"cls": a.cls, "n": n, "nnz": nnz, "what": a.what}
     if a.what == "sweep":
         rows = []
-        configs = [(1, l, 0) for l in (8, 16, 32)] + [(2, 4, 2), (2, 8, 1), (2, 8, 2), (2, 16, 1)]
-        for kind, lanes, rif in configs:
-            try:
-                with npbcg.Session(rs, ci, av, spmv_kernel=kind, lanes_per_row=lanes,
-                                   rows_in_flight=rif) as s:
-                    ms = s.time_spmv(50, fp32=a.fp32)
-            except npbcg.CgbError as e:
-                rows.append({"kind": kind, "lanes": lanes, "rows": rif, "error": str(e)})
-                continue
-            b = (npbcg.spmv_bytes_fp32 if a.fp32 else npbcg.spmv_bytes_fp64)(n, nnz)
-            rows.append({"kind": kind, "lanes": lanes, "rows": rif, "ms": ms,
-                         "gbs": b / ms / 1e6})
+        configs = [(1, l) for l in (8, 16, 32)] + [(2, 0)]
+        for kind, lanes in configs:
+            for fp32 in (False, True):
+                try:
+                    with npbcg.Session(rs, ci, av, spmv_kernel=kind, lanes_per_row=lanes) as s:
+                        ms = s.time_spmv(50, fp32=fp32)
+                        entries = s.plan()["layout_entries"]
+                except npbcg.CgbError as e:
+                    rows.append({"kind": kind, "lanes": lanes, "fp32": fp32, "error": str(e)})
+                    continue
+                b = (npbcg.spmv_bytes_fp32 if fp32 else npbcg.spmv_bytes_fp64)(n, nnz)
+                rows.append({"kind": kind, "lanes": lanes, "fp32": fp32, "ms": ms,
+                             "gbs": b / ms / 1e6, "layout_entries": entries})
         with npbcg.Session(rs, ci, av) as s:
             out["autotuned"] = s.plan()
         out["sweep"] = rows
     else:
-        with npbcg.Session(rs, ci, av, lanes_per_row=a.lanes, spmv_kernel=a.kind,
-                           rows_in_flight=a.rows) as s:
+        with npbcg.Session(rs, ci, av, lanes_per_row=a.lanes, spmv_kernel=a.kind) as s:
             out["plan"] = s.plan()
             if a.what == "spmv":
                 ms = s.time_spmv(a.reps, fp32=a.fp32)
