@@ -105,7 +105,8 @@ int cgb_conj_grad(cgb_session *s, const int *colidx, const int *rowstr, const do
 #define CGB_MODE_FP64 0         /* reference algorithm: fixed cgitmax FP64 CG steps */
 #define CGB_MODE_FP64_TOL 1     /* FP64 CG stopped at relative residual tol */
 #define CGB_MODE_MIXED 2        /* FP32 SpMV inside FP64 iterative refinement */
-#define CGB_MODE_MIXED_LEARNED 3 /* MIXED + learned preconditioner M = G^T G */
+#define CGB_MODE_MIXED_LEARNED 3 /* MIXED, preconditioned by M = F^T F (cgb_set_preconditioner),
+                                   falling back to plain CG when it stalls */
 
 typedef struct cgb_solve_params {
     int niter;          /* outer steps (reference NITER, setparams.cpp:751-785) */
@@ -114,8 +115,9 @@ typedef struct cgb_solve_params {
     int cgitmax;        /* inner iterations: exact count in FP64 mode (25 = reference),
                            the cap in the tolerance modes */
     double tol;         /* tolerance modes: stop when ||r|| <= tol * ||x|| */
-    int refresh_every;  /* MIXED*: replace r by x - A z in FP64 every k steps (10) */
-    int warm_start;     /* tolerance modes: start from z0 = x/(zeta_prev - shift) */
+    int refresh_every;  /* MIXED*: replace r by x - A z in FP64 (and restart) at least every
+                           k steps (10); also when the recursive residual fell 1e-6 since the
+                           last replacement, and before accepting convergence */
 } cgb_solve_params;
 
 void cgb_default_solve_params(cgb_solve_params *p);
@@ -136,6 +138,52 @@ typedef struct cgb_solve_result {
 int cgb_power_iterate(cgb_session *s, const cgb_solve_params *params, double *zeta_trace,
                       double *rnorm_trace, int *iters_trace, double *x_out,
                       cgb_solve_result *res);
+
+/* Installs the preconditioner of CGB_MODE_MIXED_LEARNED: the factor F of
+ * M = F^T F, which approximates (-A)^-1 (A is negative definite; the solver
+ * runs CG on -A).  F is lower triangular in CSR (n+1 row pointers, columns
+ * <= row, every row holding a positive diagonal), FP64 values stored FP32 on
+ * the device.  The learned factor is G diag(-A)^-1/2 with G from
+ * cgb_gnn_infer; F = diag(-A)^-1/2 is Jacobi.  No counterpart in the
+ * reference. */
+int cgb_set_preconditioner(cgb_session *s, const int *fptr, const int *fcol, const double *fval);
+
+/* --------------------------------------------- learned preconditioner */
+/* A message-passing network over the sparsity graph of A (3 layers, width 32,
+ * FP32 weights) that emits G on A's lower pattern, g_ii > 0, so M = G^T G is
+ * SPD; it is trained to make diag(-A)^-1/2 M diag(-A)^-1/2 approximate
+ * (-A)^-1 on residual vectors.  Forward, backward (training) and inference
+ * run on the GPU.  No counterpart in the reference. */
+typedef struct cgb_gnn cgb_gnn;
+typedef struct cgb_gnn_graph cgb_gnn_graph;
+
+int cgb_gnn_param_count(void);
+/* New model with deterministic initial weights from `seed`. */
+int cgb_gnn_create(int device, unsigned seed, cgb_gnn **out);
+int cgb_gnn_destroy(cgb_gnn *m);
+int cgb_gnn_get_params(cgb_gnn *m, float *out, int count);
+/* Loads weights (and resets the optimiser state). */
+int cgb_gnn_set_params(cgb_gnn *m, const float *in, int count);
+/* A matrix (the generator's CSR, negative diagonal) prepared for the model. */
+int cgb_gnn_graph_create(cgb_gnn *m, int n, const int *rowstr, const int *colidx, const double *a,
+                         cgb_gnn_graph **out);
+int cgb_gnn_graph_destroy(cgb_gnn_graph *g);
+/* n, strict-lower entry count, diag(-A)^-1/2 (n doubles); outputs nullable. */
+int cgb_gnn_graph_info(cgb_gnn_graph *g, int *n, long long *nnz_low, double *dscale_out);
+/* Loss and gradient (cgb_gnn_param_count floats) on 32 probe vectors: the
+ * caller's (`probes`, n x 32 row-major) or, when NULL, generated from `seed`:
+ * normal vectors, or with cg_steps > 0 the residuals after cg_steps batched
+ * CG steps on them (residual histories).  Outputs nullable. */
+int cgb_gnn_loss_grad(cgb_gnn *m, cgb_gnn_graph *g, const float *probes, unsigned seed,
+                      int cg_steps, float *loss, float *grad);
+/* One Adam step on generated probes; *loss (nullable) is the step's loss. */
+int cgb_gnn_train_step(cgb_gnn *m, cgb_gnn_graph *g, unsigned seed, int cg_steps, float lr,
+                       float *loss);
+/* G for the graph: strict lower values (graph order: rows ascending, then
+ * the CSR order of the row) and the diagonal; outputs nullable. */
+int cgb_gnn_infer(cgb_gnn *m, cgb_gnn_graph *g, float *goff, float *gdiag);
+/* Infers G and installs F = G diag(-A)^-1/2 as the session's preconditioner. */
+int cgb_gnn_attach(cgb_gnn *m, cgb_gnn_graph *g, cgb_session *s);
 
 /* ---------------------------------------------------------- diagnostics */
 /* Time `reps` launches of the standalone SpMV (q = A p with the p.q

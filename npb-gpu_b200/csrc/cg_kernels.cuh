@@ -19,7 +19,7 @@
 // Bodies:
 //   outer_step_body        FP64 CG: the reference algorithm (fixed cgitmax
 //                          steps from z = 0) or stopped at a relative
-//                          residual, optionally warm-started;
+//                          residual;
 //   outer_step_mixed_body  FP32 SpMV (values and search vector in FP32,
 //                          FP32 row sums) inside FP64 CG: dot products,
 //                          alpha/beta, the z/r/p updates, zeta and a
@@ -49,7 +49,10 @@ struct OuterArgs {
     int n;
     MatrixView M;
     double *x, *z, *p, *q, *r;
-    float *p32;                         // FP32 search vector (mixed mode)
+    float *p32;                         // FP32 search vector (mixed modes)
+    float *r32;                         // FP32 residual (preconditioned mode)
+    double *y;                          // preconditioned residual (preconditioned mode)
+    MatrixView F, FT;                   // preconditioner factor F (lower) and F^T, FP32
     const int *__restrict__ row_split;  // gridDim.x + 1 entries
     double *part;                       // kSlotCount * gpad
     int gpad;
@@ -58,8 +61,7 @@ struct OuterArgs {
     int cgitmax;        // fixed mode: exact count; tolerance modes: cap
     int fixed;          // 1: reference semantics (no tolerance test, z0 = 0)
     double tol;         // tolerance modes: stop when ||r|| <= tol * ||x||
-    int warm;           // tolerance modes: z0 = x / (zeta_prev - shift) when step > 0
-    int refresh_every;  // mixed mode: replace r by x - A z every k steps
+    int refresh_every;  // mixed mode: replace r by x - A z at least every k steps
     int step;           // outer step index (trace slot)
     int finish;         // 1: zeta + x update (power iteration); 0: conj_grad only
     StepTrace *trace;
@@ -94,70 +96,48 @@ __device__ __forceinline__ double spmv(Spmv &sp, const OuterArgs &A, const VT *v
     return sp.template apply<VT>(A.M, v, out, dotv, A.n, A.gb.limit_ns, A.gb.status, ok);
 }
 
-// Start of a solve (shared by both bodies): z0 = 0 (r0 = x) or, warm,
-// z0 = x / (zeta_prev - shift) and r0 = x - A z0 in FP64; p0 = r0; the
-// mixed body also fills p32.  Leaves partials of r.r and x.x.
+// Start of a solve (shared by the bodies): z0 = 0, r0 = x, p0 = r0 (the
+// mixed body also fills p32); leaves the partial of r.r = x.x.  (CG's first
+// iterate from z0 = 0 is already the best multiple of x, the Galerkin
+// solution on span{x}, so no other starting guess built from x saves work.)
 template <class Spmv>
-__device__ __forceinline__ bool start_solve(Spmv &sp, const OuterArgs &A, int row0, int row1,
-                                            int vend, bool warm, bool fill32, double *scratch)
+__device__ __forceinline__ void start_solve(const OuterArgs &A, int row0, int vend, bool fill32,
+                                            double *scratch)
 {
-    double acc = 0.0, accx = 0.0;
-    if (!warm) {
-        for (int j = row0 + threadIdx.x; j < vend; j += blockDim.x) {
-            const double xv = A.x[j];
-            A.q[j] = 0.0;
-            A.z[j] = 0.0;
-            A.r[j] = xv;
-            A.p[j] = xv;
-            if (fill32) A.p32[j] = float(xv);
-            if (j < A.n) acc = fma(xv, xv, acc);
-        }
-        put_partial(A, kSlotRho, acc, scratch);
-        put_partial(A, kSlotXX, acc, scratch);
-        return true;
-    }
-    const double mu = 1.0 / (A.trace[A.step - 1].zeta - A.shift);
-    for (int j = row0 + threadIdx.x; j < vend; j += blockDim.x) {
-        A.q[j] = 0.0;
-        A.z[j] = (j < A.n) ? mu * A.x[j] : 0.0;
-    }
-    if (!grid_barrier(A.gb)) return false;
-    bool ok = true;
-    spmv<Spmv, double>(sp, A, A.z, A.r, nullptr, ok);  // r = A z0
-    if (!ok) return false;
-    __syncthreads();
+    double acc = 0.0;
     for (int j = row0 + threadIdx.x; j < vend; j += blockDim.x) {
         const double xv = A.x[j];
-        const double rv = (j < A.n) ? xv - A.r[j] : xv;
-        A.r[j] = rv;
-        A.p[j] = rv;
-        if (fill32) A.p32[j] = float(rv);
-        if (j < A.n) {
-            acc = fma(rv, rv, acc);
-            accx = fma(xv, xv, accx);
-        }
+        A.q[j] = 0.0;
+        A.z[j] = 0.0;
+        A.r[j] = xv;
+        A.p[j] = xv;
+        if (fill32) A.p32[j] = float(xv);
+        if (j < A.n) acc = fma(xv, xv, acc);
     }
     put_partial(A, kSlotRho, acc, scratch);
-    put_partial(A, kSlotXX, accx, scratch);
-    return true;
 }
 
 // End of a solve (shared): r = A z (FP64), rnorm = ||x - r|| (cg.cu:777-800),
 // x.z and z.z (cg.cu:508-511), zeta, the trace record and, when finishing
 // an outer step, x = z / ||z|| (cg.cu:517-519).
+// When `r_true` the caller's r already holds x - A z computed in FP64 (a
+// true-residual replacement right before), so the residual SpMV is skipped
+// and r is left as the residual instead of A z.
 template <class Spmv>
 __device__ __forceinline__ void end_solve(Spmv &sp, const OuterArgs &A, int row0, int row1, int it,
-                                          double rho, int refreshes, double *scratch,
+                                          double rho, int refreshes, bool r_true, double *scratch,
                                           double *bcast)
 {
-    bool ok = true;
-    spmv<Spmv, double>(sp, A, A.z, A.r, nullptr, ok);
-    if (!ok) return;
-    __syncthreads();
+    if (!r_true) {
+        bool ok = true;
+        spmv<Spmv, double>(sp, A, A.z, A.r, nullptr, ok);
+        if (!ok) return;
+        __syncthreads();
+    }
     double res = 0.0, xz = 0.0, zz = 0.0;
     for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) {
         const double xv = A.x[j], zv = A.z[j];
-        const double dv = xv - A.r[j];
+        const double dv = r_true ? A.r[j] : xv - A.r[j];
         res = fma(dv, dv, res);
         xz = fma(xv, zv, xz);
         zz = fma(zv, zv, zz);
@@ -200,12 +180,10 @@ __device__ __forceinline__ void outer_step_body(const OuterArgs &A)
     // the reference initialises n+1 vector entries (cg.cu:670-675); the
     // last CTA also owns entry n, which never enters a dot product
     const int vend = (blockIdx.x == gridDim.x - 1) ? row1 + 1 : row1;
-    const bool warm = (!A.fixed) && A.warm && A.step > 0;
-    if (!start_solve(sp, A, row0, row1, vend, warm, false, scratch)) return;
+    start_solve<Spmv>(A, row0, vend, false, scratch);
     CGB_BARRIER_OR_RETURN(A);
     double rho = get_total(A, kSlotRho, &bcast[0]);
-    const double xx = get_total(A, kSlotXX, &bcast[1]);
-    const double stop2 = A.tol * A.tol * xx;
+    const double stop2 = A.tol * A.tol * rho;  // rho = x.x here
 
     // ---- CG iterations (cg.cu:678-768)
     int it = 0;
@@ -236,14 +214,18 @@ __device__ __forceinline__ void outer_step_body(const OuterArgs &A)
             A.p[j] = fma(beta, A.p[j], A.r[j]);
         CGB_BARRIER_OR_RETURN(A);
     }
-    end_solve(sp, A, row0, row1, it, rho, 0, scratch, bcast);
+    end_solve(sp, A, row0, row1, it, rho, 0, false, scratch, bcast);
 }
 
-// Mixed precision: q = A32 p32 in FP32, everything else FP64.  The
-// recursive residual drifts from the true one by the FP32 rounding of each
-// product, so it is replaced by x - A z (FP64 matrix) every refresh_every
-// steps and whenever it claims convergence; the solve stops only on a true
-// residual below tol.
+// Mixed precision: q = A32 p32 in FP32, everything else FP64, as
+// iterative refinement.  The recursive residual drifts from the true one by
+// the FP32 rounding of each product, so r is replaced by x - A z (FP64
+// matrix) and CG restarts from it (p = r) whenever the recursive residual
+// has fallen kDrift2 below its value at the last replacement, after
+// refresh_every steps, or when it claims convergence; the solve stops only
+// on a true residual below tol.
+constexpr double kDrift2 = 1e-12;  // (1e-6)^2: what one FP32-driven cycle can reliably gain
+
 template <class Spmv>
 __device__ __forceinline__ void outer_step_mixed_body(const OuterArgs &A)
 {
@@ -255,26 +237,26 @@ __device__ __forceinline__ void outer_step_mixed_body(const OuterArgs &A)
     sp.setup(A.M, row0, row1);
     bool ok = true;
     const int vend = (blockIdx.x == gridDim.x - 1) ? row1 + 1 : row1;
-    const bool warm = A.warm && A.step > 0;
-    if (!start_solve(sp, A, row0, row1, vend, warm, true, scratch)) return;
+    start_solve<Spmv>(A, row0, vend, true, scratch);
     CGB_BARRIER_OR_RETURN(A);
     double rho = get_total(A, kSlotRho, &bcast[0]);
-    const double xx = get_total(A, kSlotXX, &bcast[1]);
-    const double stop2 = A.tol * A.tol * xx;
+    const double stop2 = A.tol * A.tol * rho;  // rho = x.x here
+    double rho_cycle = rho;                    // rho at the last true residual
 
     int it = 0, since = 0, refreshes = 0;
-    bool fresh = true;  // r is a true residual
+    bool fresh = true;  // r is a true residual (and p = r)
     for (;;) {
         bool refresh = false;
         if (rho <= stop2) {
             if (fresh) break;
             refresh = true;
-        } else if (since >= A.refresh_every && !fresh) {
+        } else if (!fresh && (since >= A.refresh_every || rho <= kDrift2 * rho_cycle)) {
             refresh = true;
         }
         if (!refresh && it >= A.cgitmax) break;
         if (refresh) {
-            // r = x - A z with the FP64 matrix (z is complete: we are past a barrier)
+            // r = x - A z with the FP64 matrix (z is complete: we are past a
+            // barrier), then restart: p = r
             spmv<Spmv, double>(sp, A, A.z, A.r, nullptr, ok);
             CGB_OK_OR_RETURN(ok);
             __syncthreads();
@@ -282,11 +264,14 @@ __device__ __forceinline__ void outer_step_mixed_body(const OuterArgs &A)
             for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) {
                 const double rv = A.x[j] - A.r[j];
                 A.r[j] = rv;
+                A.p[j] = rv;
+                A.p32[j] = float(rv);
                 acc = fma(rv, rv, acc);
             }
             put_partial(A, kSlotRho, acc, scratch);
             CGB_BARRIER_OR_RETURN(A);
             rho = get_total(A, kSlotRho, &bcast[3]);
+            rho_cycle = rho;
             refreshes++;
             since = 0;
             fresh = true;
@@ -321,7 +306,168 @@ __device__ __forceinline__ void outer_step_mixed_body(const OuterArgs &A)
         since++;
         fresh = false;
     }
-    end_solve(sp, A, row0, row1, it, rho, refreshes, scratch, bcast);
+    end_solve(sp, A, row0, row1, it, rho, refreshes, fresh, scratch, bcast);
+}
+
+// Preconditioned mixed precision.  A is negative definite, so CG runs on
+// A' = -A (SPD) with b' = -x, which has the same solution z; the
+// preconditioner is M = F^T F (F lower triangular with a positive diagonal,
+// e.g. the learned factor scaled by diag(A')^-1/2), applied as two FP32
+// sparse products y = F^T (F r).  The refinement structure is the mixed
+// body's (FP32 A-products, FP64 everything else, true-residual replacement
+// with restart).  When the preconditioned iteration stalls -- no halving of
+// |r|^2 in four steps, or a non-positive p.A'p or r.y -- the outer step
+// falls back to unpreconditioned CG (counted in the trace).
+template <int LPRG>
+__device__ __forceinline__ bool apply_prec(const OuterArgs &A, int row0, int row1, bool use,
+                                           double &rho_out, double *scratch, double *bcast)
+{
+    // r32 of every row is complete (caller passed a barrier)
+    double acc = 0.0;
+    if (use) {
+        spmv_rows<LPRG, float>(A.F, A.r32, A.q, row0, row1, nullptr);  // t = F r
+        __syncthreads();
+        for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) A.p32[j] = float(A.q[j]);
+        if (!grid_barrier(A.gb)) return false;
+        spmv_rows<LPRG, float>(A.FT, A.p32, A.y, row0, row1, nullptr);  // y = F^T t
+        __syncthreads();
+        for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) acc = fma(A.r[j], A.y[j], acc);
+    } else {
+        for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) {
+            A.y[j] = A.r[j];
+            acc = fma(A.r[j], A.r[j], acc);
+        }
+    }
+    put_partial(A, kSlotD, acc, scratch);
+    if (!grid_barrier(A.gb)) return false;
+    rho_out = get_total(A, kSlotD, &bcast[2]);
+    return true;
+}
+
+template <class Spmv, int LPRG>
+__device__ __forceinline__ void outer_step_pcg_body(const OuterArgs &A)
+{
+    __shared__ double scratch[32];
+    __shared__ double bcast[8];
+    const int row0 = A.row_split[blockIdx.x];
+    const int row1 = A.row_split[blockIdx.x + 1];
+    Spmv sp;
+    sp.setup(A.M, row0, row1);
+    bool ok = true;
+    const int vend = (blockIdx.x == gridDim.x - 1) ? row1 + 1 : row1;
+    // z0 = 0, r' = b' = -x
+    double acc = 0.0;
+    for (int j = row0 + threadIdx.x; j < vend; j += blockDim.x) {
+        const double xv = A.x[j];
+        A.q[j] = 0.0;
+        A.z[j] = 0.0;
+        A.r[j] = -xv;
+        A.r32[j] = float(-xv);
+        if (j < A.n) acc = fma(xv, xv, acc);
+    }
+    put_partial(A, kSlotRho, acc, scratch);
+    CGB_BARRIER_OR_RETURN(A);
+    double rr = get_total(A, kSlotRho, &bcast[0]);
+    const double stop2 = A.tol * A.tol * rr;
+    double rr_cycle = rr;
+    double hist[4] = {rr, rr, rr, rr};  // |r|^2 of the last four steps
+    bool use_prec = true;
+    int fallbacks = 0;
+    double rho = 0.0;
+    // p = y = M r'
+    if (!apply_prec<LPRG>(A, row0, row1, use_prec, rho, scratch, bcast)) return;
+    for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) {
+        A.p[j] = A.y[j];
+        A.p32[j] = float(A.y[j]);
+    }
+    CGB_BARRIER_OR_RETURN(A);
+
+    int it = 0, since = 0, refreshes = 0;
+    bool fresh = true;
+    for (;;) {
+        bool refresh = false;
+        if (rr <= stop2) {
+            if (fresh) break;
+            refresh = true;
+        } else if (!fresh && (since >= A.refresh_every || rr <= kDrift2 * rr_cycle)) {
+            refresh = true;
+        }
+        if (!refresh && it >= A.cgitmax) break;
+        bool restart = refresh;
+        if (refresh) {
+            // r' = b' - A' z = A z - x (FP64 matrix)
+            spmv<Spmv, double>(sp, A, A.z, A.r, nullptr, ok);
+            CGB_OK_OR_RETURN(ok);
+            __syncthreads();
+            acc = 0.0;
+            for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) {
+                const double rv = A.r[j] - A.x[j];
+                A.r[j] = rv;
+                A.r32[j] = float(rv);
+                acc = fma(rv, rv, acc);
+            }
+            put_partial(A, kSlotRho, acc, scratch);
+            CGB_BARRIER_OR_RETURN(A);
+            rr = get_total(A, kSlotRho, &bcast[3]);
+            rr_cycle = rr;
+            hist[0] = hist[1] = hist[2] = hist[3] = rr;
+            refreshes++;
+            since = 0;
+            fresh = true;
+            if (rr <= stop2) break;
+        } else {
+            // q = A32 p32; p.A'p = -p.q
+            acc = spmv<Spmv, float>(sp, A, A.p32, A.q, A.p, ok);
+            CGB_OK_OR_RETURN(ok);
+            put_partial(A, kSlotD, acc, scratch);
+            CGB_BARRIER_OR_RETURN(A);
+            const double pAp = -get_total(A, kSlotD, &bcast[2]);
+            const double alpha = rho / pAp;
+            acc = 0.0;
+            for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) {
+                A.z[j] = fma(alpha, A.p[j], A.z[j]);
+                const double rv = fma(alpha, A.q[j], A.r[j]);  // r' -= alpha A'p
+                A.r[j] = rv;
+                A.r32[j] = float(rv);
+                acc = fma(rv, rv, acc);
+            }
+            put_partial(A, kSlotRho, acc, scratch);
+            CGB_BARRIER_OR_RETURN(A);
+            rr = get_total(A, kSlotRho, &bcast[3]);
+            it++;
+            since++;
+            fresh = false;
+            // stall: no halving of |r|^2 over four steps, or lost positivity
+            if (use_prec && (!(pAp > 0.0) || (since >= 4 && rr > 0.25 * hist[0]))) {
+                use_prec = false;
+                fallbacks++;
+                restart = true;
+            }
+            hist[0] = hist[1];
+            hist[1] = hist[2];
+            hist[2] = hist[3];
+            hist[3] = rr;
+        }
+        // y = M r', new rho; p = y + beta p (beta = 0 on a restart)
+        double rho_new = 0.0;
+        if (!apply_prec<LPRG>(A, row0, row1, use_prec, rho_new, scratch, bcast)) return;
+        if (use_prec && !(rho_new > 0.0)) {
+            use_prec = false;
+            fallbacks++;
+            restart = true;
+            if (!apply_prec<LPRG>(A, row0, row1, false, rho_new, scratch, bcast)) return;
+        }
+        const double beta = restart ? 0.0 : rho_new / rho;
+        rho = rho_new;
+        for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) {
+            const double pv = fma(beta, A.p[j], A.y[j]);
+            A.p[j] = pv;
+            A.p32[j] = float(pv);
+        }
+        CGB_BARRIER_OR_RETURN(A);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) A.trace[A.step].spare[0] = double(fallbacks);
+    end_solve(sp, A, row0, row1, it, rr, refreshes, fresh, scratch, bcast);
 }
 
 template <int LPR>
@@ -344,6 +490,21 @@ __global__ void __launch_bounds__(512, 2) outer_step_mixed(OuterArgs A)
 static __global__ void __launch_bounds__(1024, 1) outer_step_mixed_sliced(OuterArgs A)
 {
     outer_step_mixed_body<SlicedSpmv>(A);
+}
+
+// lanes per row of the preconditioner products (F has about half of A's
+// entries per row)
+constexpr int kLanesF = 16;
+
+template <int LPR>
+__global__ void __launch_bounds__(512, 2) outer_step_pcg(OuterArgs A)
+{
+    outer_step_pcg_body<RowSpmv<LPR>, kLanesF>(A);
+}
+
+static __global__ void __launch_bounds__(1024, 1) outer_step_pcg_sliced(OuterArgs A)
+{
+    outer_step_pcg_body<SlicedSpmv, kLanesF>(A);
 }
 
 // Standalone q = A p with the p.q reduction fused (the work of reference

@@ -3,7 +3,7 @@
 //
 //   cg S|W|A|B|C            an NPB class (setparams.cpp:751-785 parameters)
 //   cg U --n N --nonzer K --niter I --shift S [--seed X]   custom sizes
-//   options: --mode fp64|tol|mixed|learned  --tol T  --cgitmax M  --warm
+//   options: --mode fp64|tol|mixed|learned  --tol T  --cgitmax M
 //            --device D  --json (one JSON result line instead of the report)
 //
 // Like the reference it generates the matrix (makea), runs the timed inverse
@@ -50,7 +50,7 @@ void usage()
 {
     std::fprintf(stderr,
                  "usage: cg S|W|A|B|C|D | cg U --n N --nonzer K --niter I --shift S [--seed X]\n"
-                 "          [--mode fp64|tol|mixed|learned] [--tol T] [--cgitmax M] [--warm]\n"
+                 "          [--mode fp64|tol|mixed|learned] [--tol T] [--cgitmax M]\n"
                  "          [--device D] [--json]\n");
 }
 
@@ -75,7 +75,7 @@ int main(int argc, char **argv)
         return 2;
     }
     double seed = 314159265.0, tol = 1e-12;
-    int mode = CGB_MODE_FP64, cgitmax = 25, device = 0, warm = 0, json = 0;
+    int mode = CGB_MODE_FP64, cgitmax = 25, device = 0, json = 0;
     for (int i = 2; i < argc; i++) {
         const std::string a = argv[i];
         auto next = [&](void) -> const char * {
@@ -93,7 +93,6 @@ int main(int argc, char **argv)
         else if (a == "--tol") tol = std::atof(next());
         else if (a == "--cgitmax") cgitmax = std::atoi(next());
         else if (a == "--device") device = std::atoi(next());
-        else if (a == "--warm") warm = 1;
         else if (a == "--json") json = 1;
         else if (a == "--mode") {
             const std::string m = next();
@@ -139,7 +138,6 @@ int main(int argc, char **argv)
     sp.mode = mode;
     sp.cgitmax = cgitmax;
     sp.tol = tol;
-    sp.warm_start = warm;
     // one untimed solve first, as the reference does one untimed iteration (cg.cu:453-482)
     cgb_solve_result res;
     st = cgb_power_iterate(s, &sp, nullptr, nullptr, nullptr, nullptr, &res);

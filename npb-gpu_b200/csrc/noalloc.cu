@@ -171,7 +171,6 @@ extern "C" int cgb_conj_grad_noalloc(int n, long long nnz, const int *d_rowstr, 
     A.cgitmax = 25;  // cgitmax of the reference (cg.cu:666)
     A.fixed = 1;
     A.tol = 0.0;
-    A.warm = 0;
     A.step = 0;
     A.finish = 0;
     A.trace = trace;

@@ -70,6 +70,7 @@ struct Plan {
     int lpr = 0;   // row policy: lanes per row
     OuterKernel fp64 = nullptr;
     OuterKernel mixed = nullptr;
+    OuterKernel pcg = nullptr;
     SpmvKernel spmv = nullptr;
     int block = 512;
     int grid = 0;
@@ -79,11 +80,11 @@ struct Plan {
 bool row_kernels(int lpr, Plan *P)
 {
     switch (lpr) {
-    case 2: P->fp64 = outer_step_fp64<2>; P->mixed = outer_step_mixed<2>; P->spmv = spmv_dot_row<2>; return true;
-    case 4: P->fp64 = outer_step_fp64<4>; P->mixed = outer_step_mixed<4>; P->spmv = spmv_dot_row<4>; return true;
-    case 8: P->fp64 = outer_step_fp64<8>; P->mixed = outer_step_mixed<8>; P->spmv = spmv_dot_row<8>; return true;
-    case 16: P->fp64 = outer_step_fp64<16>; P->mixed = outer_step_mixed<16>; P->spmv = spmv_dot_row<16>; return true;
-    case 32: P->fp64 = outer_step_fp64<32>; P->mixed = outer_step_mixed<32>; P->spmv = spmv_dot_row<32>; return true;
+    case 2: P->fp64 = outer_step_fp64<2>; P->mixed = outer_step_mixed<2>; P->pcg = outer_step_pcg<2>; P->spmv = spmv_dot_row<2>; return true;
+    case 4: P->fp64 = outer_step_fp64<4>; P->mixed = outer_step_mixed<4>; P->pcg = outer_step_pcg<4>; P->spmv = spmv_dot_row<4>; return true;
+    case 8: P->fp64 = outer_step_fp64<8>; P->mixed = outer_step_mixed<8>; P->pcg = outer_step_pcg<8>; P->spmv = spmv_dot_row<8>; return true;
+    case 16: P->fp64 = outer_step_fp64<16>; P->mixed = outer_step_mixed<16>; P->pcg = outer_step_pcg<16>; P->spmv = spmv_dot_row<16>; return true;
+    case 32: P->fp64 = outer_step_fp64<32>; P->mixed = outer_step_mixed<32>; P->pcg = outer_step_pcg<32>; P->spmv = spmv_dot_row<32>; return true;
     default: return false;
     }
 }
@@ -175,7 +176,13 @@ struct cgb_session {
     // vectors: x, z, p, q, r (vstride doubles each) and p32
     double *d_vec = nullptr;
     float *d_p32 = nullptr;
+    float *d_r32 = nullptr;
+    double *d_y = nullptr;
     size_t vstride = 0;
+    // preconditioner factor F (lower, CSR) and F^T, FP32 values
+    int *d_f_ptr = nullptr, *d_f_col = nullptr, *d_ft_ptr = nullptr, *d_ft_col = nullptr;
+    float *d_f_val = nullptr, *d_ft_val = nullptr;
+    bool has_prec = false;
     // reductions, barrier, status, trace
     double *d_part = nullptr;
     int gpad = 0;
@@ -259,6 +266,14 @@ void release(cgb_session *s)
     dev_free(s->d_a32);
     dev_free(s->d_vec);
     dev_free(s->d_p32);
+    dev_free(s->d_r32);
+    dev_free(s->d_y);
+    dev_free(s->d_f_ptr);
+    dev_free(s->d_f_col);
+    dev_free(s->d_f_val);
+    dev_free(s->d_ft_ptr);
+    dev_free(s->d_ft_col);
+    dev_free(s->d_ft_val);
     dev_free(s->d_part);
     dev_free(s->d_sync);
     dev_free(s->d_status);
@@ -304,6 +319,14 @@ OuterArgs outer_args(cgb_session *s)
     A.q = s->q();
     A.r = s->r();
     A.p32 = s->d_p32;
+    A.r32 = s->d_r32;
+    A.y = s->d_y;
+    A.F.rowstr = s->d_f_ptr;
+    A.F.colidx = s->d_f_col;
+    A.F.a32 = s->d_f_val;
+    A.FT.rowstr = s->d_ft_ptr;
+    A.FT.colidx = s->d_ft_col;
+    A.FT.a32 = s->d_ft_val;
     A.row_split = s->d_split;
     A.part = s->d_part;
     A.gpad = s->gpad;
@@ -420,7 +443,7 @@ bool make_plan(cgb_session *s, int kind, int lpr, Plan *pl)
         P.block = s->opts.block_threads ? s->opts.block_threads : 512;
         P.smem = 0;
         // almost nothing lives in shared memory: give L1 the room
-        for (OuterKernel k : {P.fp64, P.mixed})
+        for (OuterKernel k : {P.fp64, P.mixed, P.pcg})
             if (cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 0)) return false;
         if (cudaFuncSetAttribute(P.spmv, cudaFuncAttributePreferredSharedMemoryCarveout, 0)) return false;
     } else if (kind == kKindSliced) {
@@ -429,12 +452,13 @@ bool make_plan(cgb_session *s, int kind, int lpr, Plan *pl)
             return false;
         P.fp64 = outer_step_fp64_sliced;
         P.mixed = outer_step_mixed_sliced;
+        P.pcg = outer_step_pcg_sliced;
         P.spmv = spmv_dot_sliced;
         P.block = 1024;
         const int grid = std::min(s->prop.multiProcessorCount, s->n);
         if (s->sliced_grid != grid && build_sliced(s, grid) != CGB_OK) return false;
         P.smem = sliced_smem_bytes(s->sliced_max_rows);
-        for (OuterKernel k : {P.fp64, P.mixed})
+        for (OuterKernel k : {P.fp64, P.mixed, P.pcg})
             if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)))
                 return false;
         if (cudaFuncSetAttribute(P.spmv, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)))
@@ -446,12 +470,14 @@ bool make_plan(cgb_session *s, int kind, int lpr, Plan *pl)
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, P.fp64, P.block, P.smem) != cudaSuccess ||
         per_sm < 1)
         return false;
-    int per_sm_mixed = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_mixed, P.mixed, P.block, P.smem) !=
-            cudaSuccess ||
-        per_sm_mixed < 1)
-        return false;
-    per_sm = std::min({per_sm, per_sm_mixed, kind == kKindSliced ? 1 : 4});
+    for (OuterKernel k : {P.mixed, P.pcg}) {
+        int per = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, P.block, P.smem) != cudaSuccess ||
+            per < 1)
+            return false;
+        per_sm = std::min(per_sm, per);
+    }
+    per_sm = std::min(per_sm, kind == kKindSliced ? 1 : 4);
     P.grid = std::max(1, std::min(per_sm * s->prop.multiProcessorCount, s->n));
     if (P.grid > s->gpad) return false;
     *pl = P;
@@ -627,7 +653,7 @@ int collect_status(cgb_session *s)
     return set_error(CGB_ERR_CUDA, "device status %d", st);
 }
 
-bool is_mixed(int mode) { return mode == CGB_MODE_MIXED; }
+bool is_mixed(int mode) { return mode == CGB_MODE_MIXED || mode == CGB_MODE_MIXED_LEARNED; }
 
 // Enqueues one power iteration (x = 1, then niter outer-step kernels) on the
 // session stream.
@@ -644,10 +670,11 @@ cudaError_t enqueue_power(cgb_session *s, const cgb_solve_params &P)
     A.cgitmax = P.cgitmax;
     A.fixed = (P.mode == CGB_MODE_FP64) ? 1 : 0;
     A.tol = P.tol;
-    A.warm = P.warm_start;
     A.refresh_every = P.refresh_every > 0 ? P.refresh_every : 10;
     A.finish = 1;
-    const OuterKernel k = is_mixed(P.mode) ? s->plan.mixed : s->plan.fp64;
+    const OuterKernel k = P.mode == CGB_MODE_MIXED_LEARNED ? s->plan.pcg
+                          : P.mode == CGB_MODE_MIXED       ? s->plan.mixed
+                                                           : s->plan.fp64;
     for (int it = 0; it < P.niter; it++) {
         A.step = it;
         e = launch_outer(s, k, A);
@@ -661,8 +688,10 @@ int check_params(cgb_session *s, const cgb_solve_params &P)
     if (P.niter < 1) return set_error(CGB_ERR_INVALID, "niter must be >= 1");
     if (P.cgitmax < 0) return set_error(CGB_ERR_INVALID, "cgitmax must be >= 0");
     if (!std::isfinite(P.shift)) return set_error(CGB_ERR_INVALID, "shift must be finite");
-    if (P.mode != CGB_MODE_FP64 && P.mode != CGB_MODE_FP64_TOL && P.mode != CGB_MODE_MIXED)
-        return set_error(CGB_ERR_INVALID, "mode %d is not available in this build", P.mode);
+    if (P.mode < CGB_MODE_FP64 || P.mode > CGB_MODE_MIXED_LEARNED)
+        return set_error(CGB_ERR_INVALID, "unknown mode %d", P.mode);
+    if (P.mode == CGB_MODE_MIXED_LEARNED && !s->has_prec)
+        return set_error(CGB_ERR_STATE, "preconditioned mode needs cgb_set_preconditioner first");
     if (P.mode != CGB_MODE_FP64 && !(P.tol > 0.0))
         return set_error(CGB_ERR_INVALID, "tolerance modes need tol > 0");
     if (is_mixed(P.mode) && !s->d_a32)
@@ -673,7 +702,7 @@ int check_params(cgb_session *s, const cgb_solve_params &P)
 bool same_params(const cgb_solve_params &a, const cgb_solve_params &b)
 {
     return a.niter == b.niter && a.shift == b.shift && a.mode == b.mode && a.cgitmax == b.cgitmax &&
-           a.tol == b.tol && a.refresh_every == b.refresh_every && a.warm_start == b.warm_start;
+           a.tol == b.tol && a.refresh_every == b.refresh_every;
 }
 
 }  // namespace
@@ -736,7 +765,6 @@ void cgb_default_solve_params(cgb_solve_params *p)
     p->cgitmax = 25;
     p->tol = 1e-12;
     p->refresh_every = 10;
-    p->warm_start = 0;
 }
 
 int cgb_device_info(int device, int *sm_count, int *cc_major, int *cc_minor,
@@ -803,6 +831,10 @@ int cgb_create(int n, const int *rowstr, const int *colidx, const double *a,
     CREATE_TRY(cudaMemset(s->d_vec, 0, sizeof(double) * 5 * s->vstride));
     CREATE_TRY(dev_alloc(&s->d_p32, s->vstride));
     CREATE_TRY(cudaMemset(s->d_p32, 0, sizeof(float) * s->vstride));
+    CREATE_TRY(dev_alloc(&s->d_r32, s->vstride));
+    CREATE_TRY(cudaMemset(s->d_r32, 0, sizeof(float) * s->vstride));
+    CREATE_TRY(dev_alloc(&s->d_y, s->vstride));
+    CREATE_TRY(cudaMemset(s->d_y, 0, sizeof(double) * s->vstride));
     CREATE_TRY(dev_alloc(&s->d_part, size_t(kSlotCount) * s->gpad));
     CREATE_TRY(dev_alloc(&s->d_sync, 96));
     CREATE_TRY(cudaMemset(s->d_sync, 0, sizeof(unsigned) * 96));
@@ -855,7 +887,6 @@ int cgb_conj_grad(cgb_session *s, const int *colidx, const int *rowstr, const do
     A.cgitmax = 25;  // cgitmax of the reference (cg.cu:666)
     A.fixed = 1;
     A.tol = 0.0;
-    A.warm = 0;
     A.step = 0;
     A.finish = 0;
     CUDA_TRY(launch_outer(s, s->plan.fp64, A));
@@ -919,8 +950,9 @@ int cgb_power_iterate(cgb_session *s, const cgb_solve_params *params, double *ze
     CUDA_TRY(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     std::vector<StepTrace> tr(P.niter);
     CUDA_TRY(cudaMemcpy(tr.data(), s->d_trace, sizeof(StepTrace) * P.niter, cudaMemcpyDeviceToHost));
-    int total_inner = 0, refreshes = 0;
+    int total_inner = 0, refreshes = 0, fallbacks = 0;
     for (int i = 0; i < P.niter; i++) {
+        if (P.mode == CGB_MODE_MIXED_LEARNED) fallbacks += int(tr[i].spare[0]);
         if (zeta_trace) zeta_trace[i] = tr[i].zeta;
         if (rnorm_trace) rnorm_trace[i] = tr[i].rnorm;
         if (iters_trace) iters_trace[i] = int(tr[i].inner);
@@ -933,9 +965,66 @@ int cgb_power_iterate(cgb_session *s, const cgb_solve_params *params, double *ze
         res->rnorm = tr[P.niter - 1].rnorm;
         res->device_ms = ms;
         res->total_inner = total_inner;
-        res->fallbacks = 0;
+        res->fallbacks = fallbacks;
         res->refreshes = refreshes;
     }
+    return CGB_OK;
+}
+
+int cgb_set_preconditioner(cgb_session *s, const int *fptr, const int *fcol, const double *fval)
+{
+    if (!s || !fptr || !fcol || !fval) return set_error(CGB_ERR_INVALID, "null argument");
+    const int n = s->n;
+    if (fptr[0] != 0) return set_error(CGB_ERR_BAD_MATRIX, "factor: fptr[0] != 0");
+    for (int i = 0; i < n; i++) {
+        if (fptr[i + 1] < fptr[i]) return set_error(CGB_ERR_BAD_MATRIX, "factor: fptr decreases at %d", i);
+        bool diag = false;
+        for (int k = fptr[i]; k < fptr[i + 1]; k++) {
+            if (fcol[k] < 0 || fcol[k] > i)
+                return set_error(CGB_ERR_BAD_MATRIX, "factor: entry (%d, %d) not in the lower triangle", i, fcol[k]);
+            if (!std::isfinite(fval[k])) return set_error(CGB_ERR_NUMERIC, "factor: non-finite value in row %d", i);
+            if (fcol[k] == i) {
+                if (!(fval[k] > 0.0))
+                    return set_error(CGB_ERR_NUMERIC, "factor: diagonal of row %d not positive", i);
+                diag = true;
+            }
+        }
+        if (!diag) return set_error(CGB_ERR_BAD_MATRIX, "factor: row %d has no diagonal", i);
+    }
+    const long long nf = fptr[n];
+    // transpose (rows of F^T = columns of F), rows in ascending order
+    std::vector<int> tptr(n + 1, 0), tcol(nf);
+    std::vector<float> tval(nf), val32(nf);
+    for (long long k = 0; k < nf; k++) tptr[fcol[k] + 1]++;
+    for (int i = 0; i < n; i++) tptr[i + 1] += tptr[i];
+    std::vector<int> cur(tptr.begin(), tptr.end() - 1);
+    for (int i = 0; i < n; i++)
+        for (int k = fptr[i]; k < fptr[i + 1]; k++) {
+            const int at = cur[fcol[k]]++;
+            tcol[at] = i;
+            tval[at] = float(fval[k]);
+            val32[k] = float(fval[k]);
+        }
+    CUDA_TRY(cudaSetDevice(s->device));
+    dev_free(s->d_f_ptr); dev_free(s->d_f_col); dev_free(s->d_f_val);
+    dev_free(s->d_ft_ptr); dev_free(s->d_ft_col); dev_free(s->d_ft_val);
+    s->has_prec = false;
+    if (dev_alloc(&s->d_f_ptr, size_t(n) + 1) || dev_alloc(&s->d_f_col, size_t(nf) + kPad) ||
+        dev_alloc(&s->d_f_val, size_t(nf) + kPad) || dev_alloc(&s->d_ft_ptr, size_t(n) + 1) ||
+        dev_alloc(&s->d_ft_col, size_t(nf) + kPad) || dev_alloc(&s->d_ft_val, size_t(nf) + kPad))
+        return set_error(CGB_ERR_NOMEM, "factor allocation failed");
+    CUDA_TRY(cudaMemset(s->d_f_col, 0, sizeof(int) * (nf + kPad)));
+    CUDA_TRY(cudaMemset(s->d_f_val, 0, sizeof(float) * (nf + kPad)));
+    CUDA_TRY(cudaMemset(s->d_ft_col, 0, sizeof(int) * (nf + kPad)));
+    CUDA_TRY(cudaMemset(s->d_ft_val, 0, sizeof(float) * (nf + kPad)));
+    CUDA_TRY(cudaMemcpy(s->d_f_ptr, fptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->d_f_col, fcol, sizeof(int) * nf, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->d_f_val, val32.data(), sizeof(float) * nf, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->d_ft_ptr, tptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->d_ft_col, tcol.data(), sizeof(int) * nf, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->d_ft_val, tval.data(), sizeof(float) * nf, cudaMemcpyHostToDevice));
+    s->has_prec = true;
+    drop_graph(s);
     return CGB_OK;
 }
 

@@ -70,7 +70,7 @@ class Options(ctypes.Structure):
 class SolveParams(ctypes.Structure):
     _fields_ = [("niter", ctypes.c_int), ("shift", ctypes.c_double), ("mode", ctypes.c_int),
                 ("cgitmax", ctypes.c_int), ("tol", ctypes.c_double),
-                ("refresh_every", ctypes.c_int), ("warm_start", ctypes.c_int)]
+                ("refresh_every", ctypes.c_int)]
 
 
 class SolveResult(ctypes.Structure):
@@ -81,6 +81,7 @@ class SolveResult(ctypes.Structure):
 
 _I32 = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _F64 = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_F32 = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _lib = None
 
 # every symbol include/cgb.h declares, with its ctypes signature
@@ -114,6 +115,26 @@ _SIGNATURES = {
                                                  ctypes.POINTER(ctypes.c_int)]),
     "cgb_conj_grad_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_longlong] +
                               [ctypes.c_void_p] * 8),
+    "cgb_set_preconditioner": (ctypes.c_int, [ctypes.c_void_p, _I32, _I32, _F64]),
+    "cgb_gnn_param_count": (ctypes.c_int, []),
+    "cgb_gnn_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint, ctypes.POINTER(ctypes.c_void_p)]),
+    "cgb_gnn_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "cgb_gnn_get_params": (ctypes.c_int, [ctypes.c_void_p, _F32, ctypes.c_int]),
+    "cgb_gnn_set_params": (ctypes.c_int, [ctypes.c_void_p, _F32, ctypes.c_int]),
+    "cgb_gnn_graph_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _I32, _I32, _F64,
+                                            ctypes.POINTER(ctypes.c_void_p)]),
+    "cgb_gnn_graph_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "cgb_gnn_graph_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_longlong), ctypes.c_void_p]),
+    "cgb_gnn_loss_grad": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_uint, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_float), ctypes.c_void_p]),
+    "cgb_gnn_train_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint,
+                                          ctypes.c_int, ctypes.c_float,
+                                          ctypes.POINTER(ctypes.c_float)]),
+    "cgb_gnn_infer": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_void_p]),
+    "cgb_gnn_attach": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cgb_host_alloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_longlong]),
     "cgb_host_free": (ctypes.c_int, [ctypes.c_void_p]),
     "cgb_device_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
@@ -227,12 +248,12 @@ class Session:
         return z, p, q, r, rn.value
 
     def power_iterate(self, niter, shift, mode=MODE_FP64, cgitmax=25, tol=1e-12,
-                      refresh_every=10, warm_start=False, want_x=False):
+                      refresh_every=10, want_x=False):
         """The outer loop of cg.cu:500-520; returns a dict with traces and timings."""
         P = SolveParams()
         lib().cgb_default_solve_params(ctypes.byref(P))
         P.niter, P.shift, P.mode, P.cgitmax = niter, shift, mode, cgitmax
-        P.tol, P.refresh_every, P.warm_start = tol, refresh_every, int(bool(warm_start))
+        P.tol, P.refresh_every = tol, refresh_every
         zt, rt = np.zeros(niter), np.zeros(niter)
         it = np.zeros(niter, np.int32)
         x = np.zeros(self.n) if want_x else None
@@ -245,6 +266,12 @@ class Session:
         if want_x:
             out["x"] = x
         return out
+
+    def set_preconditioner(self, fptr, fcol, fval):
+        """M = F^T F for the preconditioned mode; F lower CSR with a positive diagonal."""
+        _check(lib().cgb_set_preconditioner(self._h, np.ascontiguousarray(fptr, np.int32),
+                                            np.ascontiguousarray(fcol, np.int32),
+                                            np.ascontiguousarray(fval, np.float64)))
 
     def time_spmv(self, reps=50, fp32=False):
         ms = ctypes.c_double()
@@ -280,3 +307,147 @@ def spmv_bytes_fp64(n, nnz):
 
 def spmv_bytes_fp32(n, nnz):
     return 8 * nnz + 4 * (n + 1) + 4 * n + 4 * n
+
+
+# ------------------------------------------------------------ learned preconditioner
+WEIGHTS_PATH = os.path.join(_HERE, "lp_weights.f32")
+
+
+class GnnGraph:
+    """A matrix prepared for the network (device resident)."""
+
+    def __init__(self, model, rowstr, colidx, a):
+        self.n = int(len(rowstr) - 1)
+        self._model = model
+        h = ctypes.c_void_p()
+        _check(lib().cgb_gnn_graph_create(model._h, self.n, np.ascontiguousarray(rowstr, np.int32),
+                                          np.ascontiguousarray(colidx, np.int32),
+                                          np.ascontiguousarray(a, np.float64), ctypes.byref(h)))
+        self._h = h
+        n_, nl = ctypes.c_int(), ctypes.c_longlong()
+        self.dscale = np.zeros(self.n)
+        _check(lib().cgb_gnn_graph_info(h, ctypes.byref(n_), ctypes.byref(nl), _ptr(self.dscale)))
+        self.nnz_low = nl.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cgb_gnn_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Gnn:
+    """The learned-preconditioner network (weights on one GPU)."""
+
+    def __init__(self, device=0, seed=20241203):
+        h = ctypes.c_void_p()
+        _check(lib().cgb_gnn_create(device, seed, ctypes.byref(h)))
+        self._h = h
+        self.n_params = int(lib().cgb_gnn_param_count())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cgb_gnn_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def params(self):
+        out = np.zeros(self.n_params, np.float32)
+        _check(lib().cgb_gnn_get_params(self._h, out, self.n_params))
+        return out
+
+    @params.setter
+    def params(self, values):
+        v = np.ascontiguousarray(values, np.float32)
+        if v.size != self.n_params:
+            raise CgbError(ERR_INVALID, f"expected {self.n_params} weights, got {v.size}")
+        _check(lib().cgb_gnn_set_params(self._h, v, self.n_params))
+
+    def save(self, path=WEIGHTS_PATH):
+        self.params.astype("<f4").tofile(path)
+
+    def load(self, path=WEIGHTS_PATH):
+        self.params = np.fromfile(path, dtype="<f4")
+
+    def graph(self, rowstr, colidx, a):
+        return GnnGraph(self, rowstr, colidx, a)
+
+    def loss_grad(self, graph, probes=None, seed=0, cg_steps=0):
+        loss = ctypes.c_float()
+        grad = np.zeros(self.n_params, np.float32)
+        pr = None
+        if probes is not None:
+            pr = np.ascontiguousarray(probes, np.float32)
+            if pr.shape != (graph.n, 32):
+                raise CgbError(ERR_INVALID, "probes must be n x 32")
+        _check(lib().cgb_gnn_loss_grad(self._h, graph._h, _ptr(pr), seed, cg_steps,
+                                       ctypes.byref(loss), _ptr(grad)))
+        return float(loss.value), grad
+
+    def train_step(self, graph, seed, cg_steps=0, lr=1e-3):
+        loss = ctypes.c_float()
+        _check(lib().cgb_gnn_train_step(self._h, graph._h, seed, cg_steps, lr, ctypes.byref(loss)))
+        return float(loss.value)
+
+    def infer(self, graph):
+        goff = np.zeros(graph.nnz_low, np.float32)
+        gdiag = np.zeros(graph.n, np.float32)
+        _check(lib().cgb_gnn_infer(self._h, graph._h, _ptr(goff), _ptr(gdiag)))
+        return goff, gdiag
+
+    def attach(self, graph, session):
+        """Installs F = G diag(-A)^-1/2 as the session's preconditioner."""
+        _check(lib().cgb_gnn_attach(self._h, graph._h, session._h))
+
+
+def strict_lower_pattern(rowstr, colidx):
+    """(ptr, col) of the entries with col < row, in CSR order (the graph's order)."""
+    n = len(rowstr) - 1
+    rows = np.repeat(np.arange(n), np.diff(rowstr))
+    keep = colidx < rows
+    ptr = np.zeros(n + 1, np.int64)
+    np.add.at(ptr, rows[keep] + 1, 1)
+    return np.cumsum(ptr).astype(np.int32), colidx[keep].astype(np.int32)
+
+
+def factor_from_g(rowstr, colidx, goff, gdiag, dscale):
+    """F = G diag(dscale) as lower CSR (strict lower entries, then the diagonal)."""
+    n = len(rowstr) - 1
+    lptr, lcol = strict_lower_pattern(rowstr, colidx)
+    cnt = np.diff(lptr) + 1
+    fptr = np.zeros(n + 1, np.int64)
+    fptr[1:] = np.cumsum(cnt)
+    fcol = np.empty(fptr[-1], np.int32)
+    fval = np.empty(fptr[-1], np.float64)
+    lrows = np.repeat(np.arange(n), np.diff(lptr))
+    pos = fptr[lrows] + (np.arange(len(lcol)) - lptr[lrows])
+    fcol[pos] = lcol
+    fval[pos] = goff.astype(np.float64) * dscale[lcol]
+    fcol[fptr[1:] - 1] = np.arange(n)
+    fval[fptr[1:] - 1] = gdiag.astype(np.float64) * dscale
+    return fptr.astype(np.int32), fcol, fval
+
+
+def jacobi_factor(rowstr, colidx, a):
+    """F = diag(-A)^-1/2: M = diag(-A)^-1, the method without the network."""
+    n = len(rowstr) - 1
+    rows = np.repeat(np.arange(n), np.diff(rowstr))
+    d = -a[colidx == rows]
+    return (np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), 1.0 / np.sqrt(d))

@@ -150,11 +150,9 @@ def test_conj_grad_reuploads_changed_matrix(cgb, oracle):
 def test_tolerance_mode_reaches_reference_zeta(cgb, golden):
     n, nonzer, niter, shift = PARAMS["A"]
     s, _ = session_for(cgb, "A")
-    for warm in (False, True):
-        out = s.power_iterate(niter, shift, mode=cgb.MODE_FP64_TOL, tol=1e-12, cgitmax=60,
-                              warm_start=warm)
-        assert abs(out["zeta"][-1] - VERIFY["A"]) / VERIFY["A"] <= 1e-10
-        assert out["total_inner"] < 25 * niter
+    out = s.power_iterate(niter, shift, mode=cgb.MODE_FP64_TOL, tol=1e-12, cgitmax=60)
+    assert abs(out["zeta"][-1] - VERIFY["A"]) / VERIFY["A"] <= 1e-10
+    assert out["total_inner"] < 25 * niter
 
 
 def test_tiny_and_ragged_systems(cgb, oracle):
@@ -279,8 +277,7 @@ def test_mixed_precision_class_c(cgb, golden, kind):
     rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
     ref = golden["C"]["seeds"]["314159265.0"]
     with cgb.Session(rs, ci, a, spmv_kernel=kind) as s:
-        out = s.power_iterate(niter, shift, mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=100,
-                              warm_start=True)
+        out = s.power_iterate(niter, shift, mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=100)
     zeta_ref = np.array(ref["zeta"])
     assert np.max(np.abs(out["zeta"] - zeta_ref) / np.abs(zeta_ref)) <= 1e-10
     assert np.max(np.abs(out["rnorm"] - np.array(ref["rnorm"]))) <= 1e-10
