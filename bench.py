@@ -194,6 +194,56 @@ def reference_arm(args, rank, world):
     return 0
 
 
+# ------------------------------------------------------------ north star
+def north_star_section(npbcg, device):
+    """Class C (n=150000, nonzer=15, shift=110, 75 outer steps): time to zeta
+    of the FP64 reference algorithm on these kernels (fixed 25 CG steps)
+    against the tolerance-stopped FP64, mixed-precision and learned-
+    preconditioned mixed-precision solvers, each judged against the FP64
+    plain zeta of the same GPU run (and the reference verification value)."""
+    c = npbcg.CLASSES["C"]
+    n, niter, shift = c["n"], c["niter"], c["shift"]
+    rs, ci, a = npbcg.makea(n, c["nonzer"], npbcg.RCOND, shift)
+    out = {"workload": f"NPB class C: n={n} nonzer={c['nonzer']} shift={shift}, {niter} outer steps",
+           "tol": 1e-12}
+
+    def timed(s, **kw):
+        s.power_iterate(niter, shift, **kw)          # builds the graph
+        best = None
+        for _ in range(2):
+            r = s.power_iterate(niter, shift, **kw)
+            if best is None or r["device_ms"] < best["device_ms"]:
+                best = r
+        return best
+
+    with npbcg.Session(rs, ci, a, device=device) as s:
+        out["plan"] = s.plan()
+        plain = timed(s)
+        zp = float(plain["zeta"][-1])
+        runs = {"fp64_fixed25": plain,
+                "fp64_tol": timed(s, mode=npbcg.MODE_FP64_TOL, tol=1e-12, cgitmax=100),
+                "mixed": timed(s, mode=npbcg.MODE_MIXED, tol=1e-12, cgitmax=100)}
+        if os.path.exists(npbcg.WEIGHTS_PATH):
+            model = npbcg.Gnn(device=device)
+            model.load()
+            with model.graph(rs, ci, a) as g:
+                model.attach(g, s)
+            runs["mixed_learned"] = timed(s, mode=npbcg.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=100)
+            model.close()
+        for name, r in runs.items():
+            z = float(r["zeta"][-1])
+            out[name] = {"ms": r["device_ms"], "zeta": z,
+                         "zeta_rel_err_vs_fp64_plain": abs(z - zp) / abs(zp),
+                         "zeta_rel_err_vs_verify": abs(z - c["zeta"]) / c["zeta"],
+                         "max_step_zeta_rel_err_vs_fp64_plain":
+                             float(np.max(np.abs(r["zeta"] - plain["zeta"]) / np.abs(plain["zeta"]))),
+                         "inner_iterations": int(r["total_inner"]),
+                         "refreshes": int(r.get("refreshes", 0)),
+                         "fallbacks": int(r.get("fallbacks", 0)),
+                         "speedup_vs_fp64_fixed25": plain["device_ms"] / r["device_ms"]}
+    return out
+
+
 # ------------------------------------------------------------------- our arm
 CLASSES = None
 
@@ -317,6 +367,8 @@ def our_arm(args, rank, world, local_rank):
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": args.steps * (niter + 1),
         }
+        if not args.no_north_star:
+            line["north_star"] = north_star_section(npbcg, device)
         if world == 1 and not args.no_cpu_baseline:
             nref, nnz_ref, times = cpu_reference_run(CPU_SAMPLE_STEPS)
             sample_bytes = CPU_SAMPLE_STEPS * (CGITMAX + 1) * spmv_bytes(nref, nnz_ref)
@@ -350,6 +402,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-north-star", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     import npbcg

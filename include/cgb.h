@@ -151,8 +151,8 @@ int cgb_set_preconditioner(cgb_session *s, const int *fptr, const int *fcol, con
 /* --------------------------------------------- learned preconditioner */
 /* A message-passing network over the sparsity graph of A (3 layers, width 32,
  * FP32 weights) that emits G on A's lower pattern, g_ii > 0, so M = G^T G is
- * SPD; it is trained to make diag(-A)^-1/2 M diag(-A)^-1/2 approximate
- * (-A)^-1 on residual vectors.  Forward, backward (training) and inference
+ * SPD; it is trained to make M / delta approximate (-A)^-1 on residual
+ * vectors (delta = mean of diag(-A)).  Forward, backward (training) and inference
  * run on the GPU.  No counterpart in the reference. */
 typedef struct cgb_gnn cgb_gnn;
 typedef struct cgb_gnn_graph cgb_gnn_graph;
@@ -168,7 +168,8 @@ int cgb_gnn_set_params(cgb_gnn *m, const float *in, int count);
 int cgb_gnn_graph_create(cgb_gnn *m, int n, const int *rowstr, const int *colidx, const double *a,
                          cgb_gnn_graph **out);
 int cgb_gnn_graph_destroy(cgb_gnn_graph *g);
-/* n, strict-lower entry count, diag(-A)^-1/2 (n doubles); outputs nullable. */
+/* n, strict-lower entry count, the per-row factor scale 1/sqrt(delta) (n
+ * doubles); outputs nullable. */
 int cgb_gnn_graph_info(cgb_gnn_graph *g, int *n, long long *nnz_low, double *dscale_out);
 /* Loss and gradient (cgb_gnn_param_count floats) on 32 probe vectors: the
  * caller's (`probes`, n x 32 row-major) or, when NULL, generated from `seed`:
@@ -182,7 +183,7 @@ int cgb_gnn_train_step(cgb_gnn *m, cgb_gnn_graph *g, unsigned seed, int cg_steps
 /* G for the graph: strict lower values (graph order: rows ascending, then
  * the CSR order of the row) and the diagonal; outputs nullable. */
 int cgb_gnn_infer(cgb_gnn *m, cgb_gnn_graph *g, float *goff, float *gdiag);
-/* Infers G and installs F = G diag(-A)^-1/2 as the session's preconditioner. */
+/* Infers G and installs F = G / sqrt(delta) as the session's preconditioner. */
 int cgb_gnn_attach(cgb_gnn *m, cgb_gnn_graph *g, cgb_session *s);
 
 /* ---------------------------------------------------------- diagnostics */

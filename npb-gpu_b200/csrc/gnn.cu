@@ -427,15 +427,17 @@ static void gfree(T *&p)
     p = nullptr;
 }
 
-// One matrix prepared for the network: the scaled matrix Ahat = D^-1/2 (-A)
-// D^-1/2 without its (unit) diagonal, its strict lower pattern and that
-// pattern's transpose, the node features, and the work space of a pass.
+// One matrix prepared for the network: the scaled matrix Ahat = -A / delta
+// (delta = mean of diag(-A)) as its diagonal plus its off-diagonal part, its
+// strict lower pattern and that pattern's transpose, the node features, and
+// the work space of a pass.
 struct cgb_gnn_graph {
     int n = 0;
     long long nnz_off = 0, nnz_low = 0;
-    std::vector<double> dscale;   // D^-1/2 (host, FP64)
+    std::vector<double> dscale;   // 1/sqrt(delta) per row (host, FP64): F = G diag(dscale)
     int *off_ptr = nullptr, *off_col = nullptr;
     float *off_val = nullptr;
+    float *adiag = nullptr;       // diagonal of Ahat
     int *low_ptr = nullptr, *low_col = nullptr;
     float *low_val = nullptr;
     int *up_ptr = nullptr, *up_row = nullptr, *up_map = nullptr;
@@ -473,7 +475,7 @@ void free_graph(cgb_gnn_graph *g)
     gfree(g->off_ptr); gfree(g->off_col); gfree(g->off_val);
     gfree(g->low_ptr); gfree(g->low_col); gfree(g->low_val);
     gfree(g->up_ptr); gfree(g->up_row); gfree(g->up_map);
-    gfree(g->X);
+    gfree(g->X); gfree(g->adiag);
     for (auto &h : g->Hs) gfree(h);
     gfree(g->T); gfree(g->U); gfree(g->goff); gfree(g->gdiag); gfree(g->ud);
     gfree(g->R); gfree(g->Pv); gfree(g->Q); gfree(g->Tg); gfree(g->Ug); gfree(g->W);
@@ -483,8 +485,9 @@ void free_graph(cgb_gnn_graph *g)
 }
 
 // Deterministic initial weights: uniform(-a, a) from a hash of (seed, index),
-// a = 1/sqrt(fan_in); head biases chosen so G starts near the first-order
-// inverse square root of Ahat: g_ii = 1, g_ij = -ahat_ij / 2.
+// a = 1/sqrt(fan_in); head biases chosen so G starts near I - L (L the
+// strict lower part of Ahat), whose G^T G ~ I - (Ahat - I) is the
+// first-order inverse of Ahat: g_ii = 1, g_ij = -ahat_ij.
 void init_params(std::vector<float> &p, unsigned seed)
 {
     p.assign(kNumParams, 0.f);
@@ -503,7 +506,7 @@ void init_params(std::vector<float> &p, unsigned seed)
         p[kOffWe + t] = 0.1f * unif(kOffWe + t, 1.f);
     }
     p[kOffCd] = 0.5413249f;  // softplus^-1(1)
-    p[kOffCe] = -0.5f;
+    p[kOffCe] = -1.0f;
 }
 
 // Forward pass on graph g: Hs[0..3], then G (goff, gdiag).
@@ -527,11 +530,11 @@ int forward(cgb_gnn *m, cgb_gnn_graph *g)
     return CGB_OK;
 }
 
-// Y = Ahat X = X + Aoff X (unit diagonal).
+// Y = Ahat X = diag(Ahat) X + Aoff X.
 void ahat_mm(cgb_gnn *m, cgb_gnn_graph *g, const float *X, float *Y)
 {
     k_spmm<<<grid_rows(m, g->n), 256, 0, m->stream>>>(g->off_ptr, g->off_col, g->off_val, nullptr,
-                                                     nullptr, 1.f, X, Y, g->n);
+                                                     g->adiag, 0.f, X, Y, g->n);
 }
 // Y = G X (lower pattern + diagonal)
 void g_mm(cgb_gnn *m, cgb_gnn_graph *g, const float *X, float *Y)
@@ -730,8 +733,12 @@ int cgb_gnn_graph_create(cgb_gnn *m, int n, const int *rowstr, const int *colidx
     cgb_gnn_graph *g = new (std::nothrow) cgb_gnn_graph;
     if (!g) return set_error(CGB_ERR_NOMEM, "graph allocation failed");
     g->n = n;
-    g->dscale.resize(n);
-    for (int i = 0; i < n; i++) g->dscale[i] = 1.0 / std::sqrt(d[i]);
+    double delta = 0.0;
+    for (int i = 0; i < n; i++) delta += d[i];
+    delta /= n;
+    g->dscale.assign(n, 1.0 / std::sqrt(delta));
+    std::vector<float> adiag(n);
+    for (int i = 0; i < n; i++) adiag[i] = float(d[i] / delta);
     std::vector<int> optr(n + 1, 0), lptr(n + 1, 0), uptr(n + 1, 0);
     for (int i = 0; i < n; i++)
         for (int k = rowstr[i]; k < rowstr[i + 1]; k++) {
@@ -761,7 +768,7 @@ int cgb_gnn_graph_create(cgb_gnn *m, int n, const int *rowstr, const int *colidx
         for (int k = rowstr[i]; k < rowstr[i + 1]; k++) {
             const int j = colidx[k];
             if (j == i) continue;
-            const float v = float(-a[k] * g->dscale[i] * g->dscale[j]);
+            const float v = float(-a[k] / delta);
             ocol[o] = j;
             oval[o++] = v;
             s += std::fabs(v);
@@ -774,7 +781,7 @@ int cgb_gnn_graph_create(cgb_gnn *m, int n, const int *rowstr, const int *colidx
                 l++;
             }
         }
-        X[size_t(i) * kF + 0] = 1.f;
+        X[size_t(i) * kF + 0] = adiag[i];
         X[size_t(i) * kF + 1] = s;
         X[size_t(i) * kF + 2] = t;
         X[size_t(i) * kF + 3] = float(optr[i + 1] - optr[i]);
@@ -792,7 +799,7 @@ int cgb_gnn_graph_create(cgb_gnn *m, int n, const int *rowstr, const int *colidx
               !galloc(&g->up_ptr, n + 1) && !galloc(&g->up_row, g->nnz_low) &&
               !galloc(&g->up_map, g->nnz_low) && !galloc(&g->X, size_t(n) * kF) &&
               !galloc(&g->T, nh) && !galloc(&g->U, nh) && !galloc(&g->goff, g->nnz_low) &&
-              !galloc(&g->gdiag, n) && !galloc(&g->ud, n);
+              !galloc(&g->gdiag, n) && !galloc(&g->ud, n) && !galloc(&g->adiag, n);
     for (auto &h : g->Hs) ok = ok && !galloc(&h, nh);
     if (!ok) {
         free_graph(g);
@@ -807,6 +814,7 @@ int cgb_gnn_graph_create(cgb_gnn *m, int n, const int *rowstr, const int *colidx
     cudaMemcpy(g->up_ptr, uptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice);
     cudaMemcpy(g->up_row, urow.data(), sizeof(int) * g->nnz_low, cudaMemcpyHostToDevice);
     cudaMemcpy(g->up_map, umap.data(), sizeof(int) * g->nnz_low, cudaMemcpyHostToDevice);
+    cudaMemcpy(g->adiag, adiag.data(), sizeof(float) * n, cudaMemcpyHostToDevice);
     cudaError_t e = cudaMemcpy(g->X, X.data(), sizeof(float) * X.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         free_graph(g);
@@ -897,7 +905,7 @@ int cgb_gnn_infer(cgb_gnn *m, cgb_gnn_graph *g, float *goff_host, float *gdiag_h
     return CGB_OK;
 }
 
-// Learned preconditioner into a session: F = G diag(-A)^-1/2 on the lower
+// Learned preconditioner into a session: F = G / sqrt(delta) on the lower
 // pattern of A (strictly lower entries in column order, then the diagonal).
 int cgb_gnn_attach(cgb_gnn *m, cgb_gnn_graph *g, cgb_session *s)
 {

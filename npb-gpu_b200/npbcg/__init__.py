@@ -413,7 +413,7 @@ class Gnn:
         return goff, gdiag
 
     def attach(self, graph, session):
-        """Installs F = G diag(-A)^-1/2 as the session's preconditioner."""
+        """Installs F = G / sqrt(delta) as the session's preconditioner."""
         _check(lib().cgb_gnn_attach(self._h, graph._h, session._h))
 
 
@@ -445,8 +445,13 @@ def factor_from_g(rowstr, colidx, goff, gdiag, dscale):
     return fptr.astype(np.int32), fcol, fval
 
 
+def identity_factor(n):
+    """F = I: the preconditioned solver then is plain CG (the method without the network)."""
+    return np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), np.ones(n)
+
+
 def jacobi_factor(rowstr, colidx, a):
-    """F = diag(-A)^-1/2: M = diag(-A)^-1, the method without the network."""
+    """F = diag(-A)^-1/2: M = diag(-A)^-1 (Jacobi)."""
     n = len(rowstr) - 1
     rows = np.repeat(np.arange(n), np.diff(rowstr))
     d = -a[colidx == rows]

@@ -7,10 +7,12 @@ addition "learned preconditioner"), so it restates the network as the
 library defines it, in NumPy float64:
 
 Matrix scaling.  A (the generator's matrix) is negative definite; the
-network sees the SPD, Jacobi-scaled matrix
-    A' = -A,  D = diag(A'),  Ahat = D^-1/2 A' D^-1/2   (unit diagonal).
+network sees the SPD matrix scaled by one constant
+    A' = -A,  delta = mean(diag(A')),  Ahat = A' / delta
+(a per-row scaling would change the spectrum: for this generator Jacobi
+scaling slows CG down, so the network's starting point G = I stays plain CG).
 
-Inputs per row i (X, 4 columns): [1, s_i, t_i, deg_i / mean_deg] with
+Inputs per row i (X, 4 columns): [ahat_ii, s_i, t_i, deg_i / mean_deg] with
 s_i = sum_{j!=i} |ahat_ij|, t_i = sum_{j!=i} ahat_ij, deg_i the count of
 stored off-diagonal entries.
 
@@ -23,7 +25,7 @@ Output head, on the lower pattern of Ahat (stored (i, j), j <= i):
     g_ii = softplus(H3_i . w_d + c_d)
     g_ij = ahat_ij * (sum_c w_e[c] H3_i[c] H3_j[c] + c_e)     (j < i)
 G is lower triangular with a positive diagonal, so M = G^T G is SPD.  The
-preconditioner of A' is D^-1/2 G^T G D^-1/2.
+preconditioner of A' is G^T G / delta, i.e. F = G / sqrt(delta).
 
 Loss over K probe vectors r_k (columns of R):
     L = (1/K) sum_k || Ahat G^T G r_k - r_k ||^2 / ||r_k||^2
@@ -83,12 +85,14 @@ class Graph:
         d = Ap.diagonal()
         if np.any(d <= 0):
             raise ValueError("diag(-A) must be positive")
-        s = 1.0 / np.sqrt(d)
+        delta = float(np.mean(d))
         self.n = n
-        self.dscale = s
-        self.Ahat = sp.csr_matrix(sp.diags(s) @ Ap @ sp.diags(s))
+        self.delta = delta
+        self.dscale = np.full(n, 1.0 / np.sqrt(delta))
+        self.Ahat = sp.csr_matrix(Ap / delta)
         self.Ahat.sort_indices()
-        self.Aoff = self.Ahat - sp.diags(self.Ahat.diagonal())
+        self.adiag = self.Ahat.diagonal()
+        self.Aoff = self.Ahat - sp.diags(self.adiag)
         self.Aoff.eliminate_zeros()
         low = sp.tril(self.Ahat, k=-1).tocsr()
         low.sort_indices()
@@ -96,7 +100,7 @@ class Graph:
         offdeg = np.diff(self.Aoff.indptr).astype(np.float64)
         mean_deg = max(offdeg.mean(), 1.0)
         absA = abs(self.Aoff)
-        self.X = np.stack([np.ones(n), np.asarray(absA.sum(axis=1)).ravel(),
+        self.X = np.stack([self.adiag, np.asarray(absA.sum(axis=1)).ravel(),
                            np.asarray(self.Aoff.sum(axis=1)).ravel(), offdeg / mean_deg], axis=1)
 
 
@@ -177,6 +181,6 @@ def loss_and_grad(p, g, R):
 
 
 def preconditioner_apply(G, dscale, r):
-    """z = D^-1/2 G^T G D^-1/2 r (the preconditioner of A' = -A)."""
+    """z = F^T F r with F = G diag(dscale) (the preconditioner of A' = -A)."""
     y = dscale * r
     return dscale * (G.T @ (G @ y))

@@ -161,35 +161,44 @@ def test_learned_preconditioner_class_c_unseen_seed(cgb, golden):
     ref = golden["C"]["seeds"]["314159265.0"]
     zr = np.array(ref["zeta"])
     assert np.max(np.abs(out["zeta"] - zr) / np.abs(zr)) <= 1e-10, how
-    assert np.max(np.abs(out["rnorm"] - np.array(ref["rnorm"]))) <= 1e-10
+    # rnorm: absolute 1e-10 * ||x_k|| (x_0 = ones, later x_k has unit norm)
+    xnorm = np.r_[np.sqrt(n), np.ones(niter - 1)]
+    assert np.all(np.abs(out["rnorm"] - np.array(ref["rnorm"])) <= 1e-10 * xnorm)
 
 
 def test_learned_gain_over_method_without_it(cgb):
-    """Ablation on an unseen matrix: the trained network's preconditioner
-    against the same solver without it (Jacobi factor, and no
-    preconditioner): iterations to the same tolerance, and the training
-    objective on fresh probes.  Records the numbers; asserts the trained
-    factor's loss beats Jacobi's."""
+    """Ablation on an unseen matrix: the same preconditioned solver with the
+    trained network's factor against the method without the network (F = I,
+    i.e. plain CG) and Jacobi: inner iterations to the same tolerance and the
+    training objective on fresh probes.  Records the numbers; asserts that
+    training lowered the objective below the untrained network's and below
+    F = I, and that the learned factor does not need more iterations than
+    plain CG."""
     model, how = trained_model(cgb)
     n, nonzer, shift = 14000, 11, 20.0
     rs, ci, a = cgb.makea(n, nonzer, 0.1, shift, 987654321.0)
+    kw = dict(mode=cgb.MODE_MIXED_LEARNED, tol=1e-10, cgitmax=200)
     with cgb.Session(rs, ci, a) as s, model.graph(rs, ci, a) as g:
-        plain = s.power_iterate(15, shift, mode=cgb.MODE_MIXED, tol=1e-10, cgitmax=200)
+        s.set_preconditioner(*cgb.identity_factor(n))
+        plain = s.power_iterate(15, shift, **kw)
         s.set_preconditioner(*cgb.jacobi_factor(rs, ci, a))
-        jac = s.power_iterate(15, shift, mode=cgb.MODE_MIXED_LEARNED, tol=1e-10, cgitmax=200)
+        jac = s.power_iterate(15, shift, **kw)
         model.attach(g, s)
-        lrn = s.power_iterate(15, shift, mode=cgb.MODE_MIXED_LEARNED, tol=1e-10, cgitmax=200)
+        lrn = s.power_iterate(15, shift, **kw)
+        untrained = cgb.Gnn()
         loss_learned, _ = model.loss_grad(g, seed=99, cg_steps=4)
-        untrained = cgb.Gnn(seed=5)
-        # Jacobi in network terms: G = I (c_d = softplus^-1(1), no off-diagonal)
-        p = untrained.params
+        loss_untrained, _ = untrained.loss_grad(g, seed=99, cg_steps=4)
+        ident = cgb.Gnn()
+        p = ident.params
         p[:] = 0.0
-        p[untrained.n_params - 34] = 0.5413249
-        untrained.params = p
-        loss_jacobi, _ = untrained.loss_grad(g, seed=99, cg_steps=4)
-    for r in (plain, jac, lrn):
+        p[ident.n_params - 34] = 0.5413249  # c_d: g_ii = softplus(c_d) = 1, g_ij = 0: G = I
+        ident.params = p
+        loss_identity, _ = ident.loss_grad(g, seed=99, cg_steps=4)
+    for r in (jac, lrn):
         assert abs(r["zeta"][-1] - plain["zeta"][-1]) <= 1e-10 * abs(plain["zeta"][-1])
-    print(f"\nablation ({how}): iterations plain={plain['total_inner']} jacobi={jac['total_inner']} "
-          f"learned={lrn['total_inner']} fallbacks={lrn['fallbacks']}; loss learned={loss_learned:.4g} "
-          f"jacobi={loss_jacobi:.4g}")
-    assert loss_learned < loss_jacobi
+    print(f"\nablation ({how}): inner iterations plain={plain['total_inner']} "
+          f"jacobi={jac['total_inner']} learned={lrn['total_inner']} "
+          f"(fallbacks {lrn['fallbacks']}); loss learned={loss_learned:.4g} "
+          f"untrained={loss_untrained:.4g} identity={loss_identity:.4g}")
+    assert loss_learned < loss_untrained and loss_learned < loss_identity
+    assert lrn["total_inner"] <= plain["total_inner"]
