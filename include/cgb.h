@@ -186,6 +186,43 @@ int cgb_gnn_infer(cgb_gnn *m, cgb_gnn_graph *g, float *goff, float *gdiag);
 /* Infers G and installs F = G / sqrt(delta) as the session's preconditioner. */
 int cgb_gnn_attach(cgb_gnn *m, cgb_gnn_graph *g, cgb_session *s);
 
+/* ------------------------------------------------------------- batches */
+/* Many independent systems of uneven order (n <= 27000 each) solved in one
+ * persistent launch: every CTA takes systems from a device work queue (the
+ * largest first) and runs a system's whole inverse power iteration alone,
+ * its search vector in shared memory.  Lanes per row per system and the
+ * block shape come from cgb_batch_tune (defaults otherwise).  In
+ * CGB_MODE_MIXED a system whose iteration meets p.Ap >= 0 (not negative
+ * definite) or does not converge within cgitmax is solved again with the
+ * FP64 reference algorithm; its status is then 1.  No counterpart in the
+ * reference (it solves one system). */
+typedef struct cgb_batch cgb_batch;
+
+typedef struct cgb_batch_params {
+    int niter;          /* outer steps per system */
+    int mode;           /* CGB_MODE_FP64 (fixed cgitmax steps) or CGB_MODE_MIXED */
+    int cgitmax;        /* inner steps: exact (FP64) or cap (MIXED) */
+    double tol;         /* MIXED: stop when ||x - A z|| <= tol ||x|| */
+    int refresh_every;  /* MIXED: true-residual replacement at least every k steps */
+} cgb_batch_params;
+
+void cgb_default_batch_params(cgb_batch_params *p);
+/* nsys systems: n[s], and rowstr[s] / colidx[s] / a[s] host CSR arrays, shift[s]. */
+int cgb_batch_create(int device, int nsys, const int *n, const int *const *rowstr,
+                     const int *const *colidx, const double *const *a, const double *shift,
+                     cgb_batch **out);
+int cgb_batch_destroy(cgb_batch *b);
+/* Per-system outputs (nsys entries each, nullable): final zeta, rnorm, inner
+ * iterations summed over the outer steps, status (0, or 1 = re-solved in
+ * FP64); *device_ms the launch's device time. */
+int cgb_batch_solve(cgb_batch *b, const cgb_batch_params *params, double *zeta, double *rnorm,
+                    int *iters, int *status, double *device_ms);
+/* Autotuner: times the batch for each candidate block shape and lane policy
+ * (row-length thresholds t0 < t1 < t2 for 8 / 16 / 32 lanes per row, 4 below
+ * t0), keeps the fastest for later solves and reports it. */
+int cgb_batch_tune(cgb_batch *b, const cgb_batch_params *params, int *block, double *t0,
+                   double *t1, double *t2, double *best_ms);
+
 /* ---------------------------------------------------------- diagnostics */
 /* Time `reps` launches of the standalone SpMV (q = A p with the p.q
  * reduction fused, the operation of kernel three + four, cg.cu:937-1004) of

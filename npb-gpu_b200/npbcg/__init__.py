@@ -73,6 +73,11 @@ class SolveParams(ctypes.Structure):
                 ("refresh_every", ctypes.c_int)]
 
 
+class BatchParams(ctypes.Structure):
+    _fields_ = [("niter", ctypes.c_int), ("mode", ctypes.c_int), ("cgitmax", ctypes.c_int),
+                ("tol", ctypes.c_double), ("refresh_every", ctypes.c_int)]
+
+
 class SolveResult(ctypes.Structure):
     _fields_ = [("zeta", ctypes.c_double), ("rnorm", ctypes.c_double),
                 ("device_ms", ctypes.c_double), ("total_inner", ctypes.c_int),
@@ -135,6 +140,16 @@ _SIGNATURES = {
     "cgb_gnn_infer": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_void_p]),
     "cgb_gnn_attach": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "cgb_default_batch_params": (None, [ctypes.POINTER(BatchParams)]),
+    "cgb_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _I32, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_void_p, _F64,
+                                        ctypes.POINTER(ctypes.c_void_p)]),
+    "cgb_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "cgb_batch_solve": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchParams), _F64, _F64,
+                                       _I32, _I32, ctypes.POINTER(ctypes.c_double)]),
+    "cgb_batch_tune": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchParams),
+                                      ctypes.POINTER(ctypes.c_int)] +
+                       [ctypes.POINTER(ctypes.c_double)] * 4),
     "cgb_host_alloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_longlong]),
     "cgb_host_free": (ctypes.c_int, [ctypes.c_void_p]),
     "cgb_device_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
@@ -456,3 +471,92 @@ def jacobi_factor(rowstr, colidx, a):
     rows = np.repeat(np.arange(n), np.diff(rowstr))
     d = -a[colidx == rows]
     return (np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), 1.0 / np.sqrt(d))
+
+
+# ------------------------------------------------------------------------ batches
+def batch_config5(nsys=512, seed=20241203, n_range=(1400, 20000), nonzer_range=(7, 13)):
+    """The batched workload: per system n log-uniform in n_range, nonzer
+    uniform in nonzer_range, shift = 10 + n/1000, rcond 0.1, its own odd LCG
+    seed; all drawn from a fixed host PRNG.  Returns [(n, nonzer, shift, seed)]."""
+    rng = np.random.RandomState(seed)
+    lo, hi = np.log(n_range[0]), np.log(n_range[1])
+    out = []
+    for s in range(nsys):
+        n = int(round(np.exp(rng.uniform(lo, hi))))
+        nonzer = int(rng.randint(nonzer_range[0], nonzer_range[1] + 1))
+        lcg_seed = float(2 * rng.randint(1 << 20, 1 << 40) + 1)
+        out.append((n, nonzer, 10.0 + n / 1000.0, lcg_seed))
+    return out
+
+
+def shard_systems(weights, world):
+    """Greedy split of systems over `world` ranks by weight (largest first to
+    the least loaded rank); returns the system indices of each rank."""
+    order = sorted(range(len(weights)), key=lambda i: -weights[i])
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += weights[i]
+    return [sorted(p) for p in parts]
+
+
+class Batch:
+    """Many independent systems on one GPU (cgb_batch)."""
+
+    def __init__(self, systems, shifts, device=0):
+        """systems: [(rowstr, colidx, a)], shifts: per system."""
+        self.nsys = len(systems)
+        self._keep = [(np.ascontiguousarray(r, np.int32), np.ascontiguousarray(c, np.int32),
+                       np.ascontiguousarray(v, np.float64)) for r, c, v in systems]
+        n = np.array([len(r) - 1 for r, _, _ in self._keep], np.int32)
+        P = ctypes.c_void_p * self.nsys
+        rp = P(*[r.ctypes.data for r, _, _ in self._keep])
+        cp = P(*[c.ctypes.data for _, c, _ in self._keep])
+        ap = P(*[v.ctypes.data for _, _, v in self._keep])
+        self.shifts = np.ascontiguousarray(shifts, np.float64)
+        h = ctypes.c_void_p()
+        _check(lib().cgb_batch_create(device, self.nsys, n, rp, cp, ap, self.shifts, ctypes.byref(h)))
+        self._h = h
+        self.nnz = np.array([len(v) for _, _, v in self._keep], np.int64)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cgb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _params(self, niter, mode, cgitmax, tol, refresh_every):
+        P = BatchParams()
+        lib().cgb_default_batch_params(ctypes.byref(P))
+        P.niter, P.mode, P.cgitmax, P.tol, P.refresh_every = niter, mode, cgitmax, tol, refresh_every
+        return P
+
+    def solve(self, niter=15, mode=MODE_FP64, cgitmax=25, tol=1e-12, refresh_every=10):
+        P = self._params(niter, mode, cgitmax, tol, refresh_every)
+        z, rn = np.zeros(self.nsys), np.zeros(self.nsys)
+        it, st = np.zeros(self.nsys, np.int32), np.zeros(self.nsys, np.int32)
+        ms = ctypes.c_double()
+        _check(lib().cgb_batch_solve(self._h, ctypes.byref(P), z, rn, it, st, ctypes.byref(ms)))
+        return dict(zeta=z, rnorm=rn, iters=it, status=st, device_ms=ms.value)
+
+    def tune(self, niter=1, mode=MODE_FP64, cgitmax=25, tol=1e-12, refresh_every=10):
+        P = self._params(niter, mode, cgitmax, tol, refresh_every)
+        block = ctypes.c_int()
+        t = [ctypes.c_double() for _ in range(4)]
+        _check(lib().cgb_batch_tune(self._h, ctypes.byref(P), ctypes.byref(block),
+                                    *[ctypes.byref(x) for x in t]))
+        return dict(block=block.value, thresholds=(t[0].value, t[1].value, t[2].value),
+                    best_ms=t[3].value)

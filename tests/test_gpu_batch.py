@@ -1,0 +1,86 @@
+"""GPU tests of the batched persistent solver (cgb_batch).
+
+FP64 mode is the reference algorithm, so each system must match the
+single-system session (and the CPU oracle) to zeta relative 1e-10.  MIXED
+mode is judged against the FP64 mode of the same batch: zeta relative 1e-10
+where that judge has converged (its final rnorm <= 1e-10), and a system the
+mixed iteration gives up on (status 1) is re-solved in FP64, bit-identically.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def build(cgb, specs):
+    systems, shifts = [], []
+    for n, nonzer, shift, seed in specs:
+        systems.append(cgb.makea(n, nonzer, 0.1, shift, seed))
+        shifts.append(shift)
+    return systems, np.array(shifts)
+
+
+def test_batch_fp64_matches_single_system_and_oracle(cgb, oracle):
+    specs = [(1400, 7, 10.0, 314159265.0), (2000, 9, 12.0, 271828183.0),
+             (5000, 11, 15.0, 123456789.0), (700, 5, 8.0, 161803399.0),
+             (9000, 13, 19.0, 987654321.0)]
+    systems, shifts = build(cgb, specs)
+    with cgb.Batch(systems, shifts) as b:
+        out = b.solve(niter=15)
+    for (rs, ci, a), sh, z in zip(systems, shifts, out["zeta"]):
+        with cgb.Session(rs, ci, a) as s:
+            ref = s.power_iterate(15, sh)["zeta"][-1]
+        assert abs(z - ref) <= 1e-10 * abs(ref)
+    rs, ci, a = systems[0]
+    o = oracle.power_iterate(rs, ci, a, shifts[0], 15)
+    assert abs(out["zeta"][0] - 8.5971775078648) / 8.5971775078648 <= 1e-10
+    assert abs(out["zeta"][0] - o["zeta"][-1]) <= 1e-10 * abs(o["zeta"][-1])
+    assert np.all(out["status"] == 0) and np.all(out["iters"] == 15 * 25)
+
+
+def test_batch_mixed_against_fp64_judge(cgb):
+    specs = cgb.batch_config5(nsys=48, seed=7, n_range=(1400, 8000))
+    systems, shifts = build(cgb, specs)
+    with cgb.Batch(systems, shifts) as b:
+        judge = b.solve(niter=15)
+        mixed = b.solve(niter=15, mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=200)
+    converged = judge["rnorm"] <= 1e-10
+    assert converged.sum() >= 10
+    rel = np.abs(mixed["zeta"] - judge["zeta"]) / np.abs(judge["zeta"])
+    ok = converged & (mixed["status"] == 0)
+    assert np.all(rel[ok] <= 1e-10), rel[ok].max()
+    fell = mixed["status"] == 1
+    assert np.array_equal(mixed["zeta"][fell], judge["zeta"][fell])
+    assert mixed["iters"][ok].sum() < judge["iters"][ok].sum()
+
+
+def test_batch_indefinite_system_falls_back(cgb):
+    """n=1400, nonzer=13, shift=11.4 is indefinite: the mixed iteration must
+    give up and the system be solved with the reference algorithm."""
+    specs = [(1400, 13, 11.4, 314159265.0), (1400, 7, 11.4, 314159265.0)]
+    systems, shifts = build(cgb, specs)
+    with cgb.Batch(systems, shifts) as b:
+        judge = b.solve(niter=15)
+        mixed = b.solve(niter=15, mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=200)
+    assert mixed["status"][0] == 1
+    assert mixed["zeta"][0] == judge["zeta"][0]
+    assert mixed["status"][1] == 0
+    assert abs(mixed["zeta"][1] - judge["zeta"][1]) <= 1e-10 * abs(judge["zeta"][1])
+
+
+def test_batch_tune_keeps_results(cgb):
+    specs = cgb.batch_config5(nsys=24, seed=11, n_range=(1400, 6000))
+    systems, shifts = build(cgb, specs)
+    with cgb.Batch(systems, shifts) as b:
+        before = b.solve(niter=3)
+        cfg = b.tune(niter=1)
+        after = b.solve(niter=3)
+    assert cfg["block"] in (512, 1024) and cfg["best_ms"] > 0
+    assert np.max(np.abs(after["zeta"] - before["zeta"]) / np.abs(before["zeta"])) <= 1e-12
+
+
+def test_batch_rejects_oversize(cgb):
+    rs = np.zeros(27002, np.int32)
+    with pytest.raises(cgb.CgbError) as e:
+        cgb.Batch([(rs, np.zeros(0, np.int32), np.zeros(0))], [1.0])
+    assert e.value.status == cgb.ERR_CAPACITY
