@@ -244,6 +244,38 @@ def north_star_section(npbcg, device):
     return out
 
 
+# -------------------------------------------------------------- batched
+def batched_section(npbcg, device, nsys=512, niter=15):
+    """512 generator systems (n log-uniform in [1400, 20000], nonzer in 7..13,
+    shift = 10 + n/1000, own seeds) in one persistent launch: the FP64
+    reference algorithm (the judge) and the mixed-precision solver after the
+    autotuner; aggregate solves/s and each system's zeta error against the
+    judge."""
+    specs = npbcg.batch_config5(nsys=nsys)
+    systems = [npbcg.makea(n, nz, npbcg.RCOND, sh, seed) for n, nz, sh, seed in specs]
+    shifts = [sh for _, _, sh, _ in specs]
+    with npbcg.Batch(systems, shifts, device=device) as b:
+        tuned = b.tune(niter=1, mode=npbcg.MODE_MIXED, tol=1e-12, cgitmax=200)
+        judge = b.solve(niter=niter)
+        mixed = b.solve(niter=niter, mode=npbcg.MODE_MIXED, tol=1e-12, cgitmax=200)
+    conv = judge["rnorm"] <= 1e-10
+    rel = np.abs(mixed["zeta"] - judge["zeta"]) / np.abs(judge["zeta"])
+    return {
+        "workload": f"{nsys} systems, n log-uniform in [1400, 20000], nonzer 7..13, "
+                    f"shift 10 + n/1000, {niter} outer steps each",
+        "total_nnz": int(sum(len(s[2]) for s in systems)),
+        "autotuned": tuned,
+        "fp64_judge": {"ms": judge["device_ms"], "solves_per_s": nsys / judge["device_ms"] * 1e3},
+        "mixed": {"ms": mixed["device_ms"], "solves_per_s": nsys / mixed["device_ms"] * 1e3,
+                  "refit_in_fp64": int((mixed["status"] == 1).sum())},
+        "judge_converged_systems": int(conv.sum()),
+        "max_zeta_rel_err_converged": float(rel[conv].max()) if conv.any() else None,
+        "within_1e-10_converged": int((rel[conv] <= 1e-10).sum()),
+        "within_1e-10_all": int((rel <= 1e-10).sum()),
+        "speedup_mixed_vs_fp64": judge["device_ms"] / mixed["device_ms"],
+    }
+
+
 # ------------------------------------------------------------------- our arm
 CLASSES = None
 
@@ -369,6 +401,8 @@ def our_arm(args, rank, world, local_rank):
         }
         if not args.no_north_star:
             line["north_star"] = north_star_section(npbcg, device)
+        if not args.no_batched and world == 1:
+            line["batched"] = batched_section(npbcg, device)
         if world == 1 and not args.no_cpu_baseline:
             nref, nnz_ref, times = cpu_reference_run(CPU_SAMPLE_STEPS)
             sample_bytes = CPU_SAMPLE_STEPS * (CGITMAX + 1) * spmv_bytes(nref, nnz_ref)
@@ -403,6 +437,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-north-star", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     import npbcg
