@@ -362,13 +362,17 @@ def our_arm(args, rank, world, local_rank):
     e2e_s = reduce_max(time.perf_counter() - t0)
     e2e_value = world * args.steps * solve_bytes / e2e_s / 1e9
 
-    # ---- roofline of the dominant kernel (the outer-step kernel)
-    per_launch_ms = ms_per_step / niter
-    bytes_launch = outer_step_bytes(n, nnz)
-    achieved = bytes_launch / (per_launch_ms / 1e3) / 1e9
-    peak, peak_kind = peaks()
-    traffic = load_traffic().get(("outer_step_fp64", f"class{CLASS}"))
+    # ---- roofline of the dominant kernel (the outer-step kernel): its
+    # average launch duration from CUDA events around each launch on the
+    # library's stream, algorithmic bytes per launch from outer_step_bytes
+    plan = sess.plan()
+    kernel = "outer_step_fp64_sliced" if plan["kind"] == "sliced" else \
+        f"outer_step_fp64<{plan['lanes_per_row']}>"
     kernel_ms, gap_ms = sess.time_outer_steps(niter, shift)
+    bytes_launch = outer_step_bytes(n, nnz)
+    achieved = bytes_launch / (kernel_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = load_traffic().get((kernel.split("<")[0], f"class{CLASS}"))
     spmv_ms = sess.time_spmv(50)
     spmv_gbs = spmv_bytes(n, nnz) / (spmv_ms / 1e3) / 1e9
 
@@ -392,8 +396,10 @@ def our_arm(args, rank, world, local_rank):
                                 "frac_of_peak": spmv_gbs / peak},
             "outer_step_kernel_ms": kernel_ms, "graph_gap_ms_per_step": gap_ms,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "outer_step_fp64", "peak_source": peak_kind},
+                         "frac": achieved / peak, "traffic": traffic, "kernel": kernel,
+                         "algorithmic_bytes_per_launch": bytes_launch,
+                         "launch_ms": kernel_ms, "peak_source": peak_kind},
+            "plan": plan,
             "clocks": clocks,
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},

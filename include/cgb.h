@@ -193,8 +193,9 @@ int cgb_gnn_attach(cgb_gnn *m, cgb_gnn_graph *g, cgb_session *s);
  * its search vector in shared memory.  Lanes per row per system and the
  * block shape come from cgb_batch_tune (defaults otherwise).  In
  * CGB_MODE_MIXED a system whose iteration meets p.Ap >= 0 (not negative
- * definite) or does not converge within cgitmax is solved again with the
- * FP64 reference algorithm; its status is then 1.  No counterpart in the
+ * definite), a non-finite residual, or does not converge within cgitmax is
+ * solved again with the FP64 reference algorithm (25 steps, the reference's
+ * cgitmax); its status is then 1.  No counterpart in the
  * reference (it solves one system). */
 typedef struct cgb_batch cgb_batch;
 

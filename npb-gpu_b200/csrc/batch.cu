@@ -16,9 +16,13 @@
 //          and restart (as the single-system mixed solver), stopped at
 //          ||r|| <= tol ||x||.  A system whose iteration shows p.Ap >= 0
 //          (the NPB matrices are negative definite; small orders with large
-//          nonzer are not) or does not converge within cgitmax is solved
-//          again from the start with the fixed FP64 algorithm, so its zeta is
-//          the reference algorithm's; its status says so.
+//          nonzer are not), a non-finite residual, or no convergence within
+//          cgitmax is solved again from the start with the fixed FP64
+//          algorithm at the reference's 25 steps (cg.cu's cgitmax), so its
+//          zeta is the reference algorithm's; its status says so.  (On an
+//          indefinite system an eigenvalue of A near zero can make zeta
+//          sensitive beyond what a 1e-12 residual pins down, so agreement
+//          with the reference needs the reference's own iteration there.)
 // Lanes per row are a per-system choice (the autotuner's, by row length).
 #include <cuda_runtime.h>
 
@@ -36,6 +40,7 @@ namespace cgb {
 namespace batch {
 
 constexpr int kBatchMaxN = 27000;  // rows of the largest system (shared p: 8 bytes a row)
+constexpr int kReferenceCgitmax = 25;  // cg.cu's cgitmax: the FP64 re-solve of a mixed failure
 
 struct SysDesc {
     int n;
@@ -127,8 +132,9 @@ __device__ __forceinline__ double sys_spmv(const BatchArgs &B, const SysDesc &S,
     return dacc;
 }
 
-// One system's power iteration.  Returns false when the mixed iteration
-// met p.Ap >= 0 or did not converge (the caller then runs the fixed mode).
+// One system's power iteration.  Returns false when the mixed iteration met
+// p.Ap >= 0, a non-finite residual, or did not converge (the caller then
+// runs the fixed mode).
 template <int LPR, bool mixed>
 __device__ bool solve_system(const BatchArgs &B, const SysDesc &S, double *p, double *red,
                              int *iters_out, double *zeta_out, double *rnorm_out)
@@ -186,7 +192,7 @@ __device__ bool solve_system(const BatchArgs &B, const SysDesc &S, double *p, do
             const double dpart = mixed ? sys_spmv<LPR, true>(B, S, p, nullptr, q, p)
                                        : sys_spmv<LPR, false>(B, S, p, nullptr, q, p);
             const double d = cta_sum(dpart, red);  // barrier: q complete
-            if (mixed && !(d < 0.0)) return false;  // not negative definite: fall back
+            if (mixed && !(d < 0.0)) return false;  // not negative definite (or NaN): fall back
             const double alpha = rho / d;
             const double rho0 = rho;
             acc = 0.0;
@@ -197,6 +203,7 @@ __device__ bool solve_system(const BatchArgs &B, const SysDesc &S, double *p, do
                 acc = fma(rv, rv, acc);
             }
             rho = cta_sum(acc, red);
+            if (mixed && !(rho < INFINITY)) return false;  // non-finite residual: fall back
             const double beta = rho / rho0;
             for (int j = threadIdx.x; j < n; j += blockDim.x) p[j] = fma(beta, p[j], r[j]);
             __syncthreads();
@@ -425,6 +432,7 @@ int launch(cgb_batch *b, const cgb_batch_params &P, double *ms)
             BT_TRY(cudaMemcpyAsync(b->d_redo, redo.data(), sizeof(int) * redo.size(),
                                    cudaMemcpyHostToDevice, b->stream));
             A.mode = 0;
+            A.cgitmax = kReferenceCgitmax;
             st = launch_list<false>(b, A, b->d_redo, int(redo.size()));
             if (st) return st;
             // the FP64 pass wrote status 0 for these systems; mark them re-solved

@@ -27,6 +27,8 @@
 //                          computed with the FP64 matrix stay in FP64.
 #pragma once
 
+#include <type_traits>
+
 #include "spmv_policies.cuh"
 
 namespace cgb {
@@ -318,18 +320,36 @@ __device__ __forceinline__ void outer_step_mixed_body(const OuterArgs &A)
 // with restart).  When the preconditioned iteration stalls -- no halving of
 // |r|^2 in four steps, or a non-positive p.A'p or r.y -- the outer step
 // falls back to unpreconditioned CG (counted in the trace).
-template <int LPRG>
-__device__ __forceinline__ bool apply_prec(const OuterArgs &A, int row0, int row1, bool use,
-                                           double &rho_out, double *scratch, double *bcast)
+// out = F v (FP32 products, FP64 row results) for the CTA's rows: the
+// sliced policy walks F's own sliced copy (same row split and column
+// blocks as A's); the row policy reads F's CSR with LPRG lanes per row.
+template <class Spmv, int LPRG>
+__device__ __forceinline__ bool factor_product(Spmv &sp, const OuterArgs &A, const MatrixView &F,
+                                               const float *v, double *out, int row0, int row1)
+{
+    if constexpr (std::is_same<Spmv, SlicedSpmv>::value) {
+        bool ok = true;
+        (void)sp.template apply<float>(F, v, out, nullptr, A.n, A.gb.limit_ns, A.gb.status, ok);
+        return ok;
+    } else {
+        spmv_rows<LPRG, float>(F, v, out, row0, row1, nullptr);
+        return true;
+    }
+}
+
+template <class Spmv, int LPRG>
+__device__ __forceinline__ bool apply_prec(Spmv &sp, const OuterArgs &A, int row0, int row1,
+                                           bool use, double &rho_out, double *scratch,
+                                           double *bcast)
 {
     // r32 of every row is complete (caller passed a barrier)
     double acc = 0.0;
     if (use) {
-        spmv_rows<LPRG, float>(A.F, A.r32, A.q, row0, row1, nullptr);  // t = F r
+        if (!factor_product<Spmv, LPRG>(sp, A, A.F, A.r32, A.q, row0, row1)) return false;  // t = F r
         __syncthreads();
         for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) A.p32[j] = float(A.q[j]);
         if (!grid_barrier(A.gb)) return false;
-        spmv_rows<LPRG, float>(A.FT, A.p32, A.y, row0, row1, nullptr);  // y = F^T t
+        if (!factor_product<Spmv, LPRG>(sp, A, A.FT, A.p32, A.y, row0, row1)) return false;  // y = F^T t
         __syncthreads();
         for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) acc = fma(A.r[j], A.y[j], acc);
     } else {
@@ -375,7 +395,7 @@ __device__ __forceinline__ void outer_step_pcg_body(const OuterArgs &A)
     int fallbacks = 0;
     double rho = 0.0;
     // p = y = M r'
-    if (!apply_prec<LPRG>(A, row0, row1, use_prec, rho, scratch, bcast)) return;
+    if (!apply_prec<Spmv, LPRG>(sp, A, row0, row1, use_prec, rho, scratch, bcast)) return;
     for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) {
         A.p[j] = A.y[j];
         A.p32[j] = float(A.y[j]);
@@ -450,12 +470,12 @@ __device__ __forceinline__ void outer_step_pcg_body(const OuterArgs &A)
         }
         // y = M r', new rho; p = y + beta p (beta = 0 on a restart)
         double rho_new = 0.0;
-        if (!apply_prec<LPRG>(A, row0, row1, use_prec, rho_new, scratch, bcast)) return;
+        if (!apply_prec<Spmv, LPRG>(sp, A, row0, row1, use_prec, rho_new, scratch, bcast)) return;
         if (use_prec && !(rho_new > 0.0)) {
             use_prec = false;
             fallbacks++;
             restart = true;
-            if (!apply_prec<LPRG>(A, row0, row1, false, rho_new, scratch, bcast)) return;
+            if (!apply_prec<Spmv, LPRG>(sp, A, row0, row1, false, rho_new, scratch, bcast)) return;
         }
         const double beta = restart ? 0.0 : rho_new / rho;
         rho = rho_new;
@@ -607,7 +627,8 @@ static __global__ void build_segments(const int *__restrict__ rowstr,
 // Sliced layout, step 1 -- one CTA per chunk (CTA c of the solve grid,
 // column block b): order the chunk's rows by descending segment length
 // (counting sort on min(len, 255)), 32 to a slice; srow gets the local row of
-// each (slice, lane), 0xffff for the tail; slice_width the longest segment.
+// each (slice, lane), 0xffff for the tail; slice_width the longest segment,
+// rounded up to even.
 // Placement order within a bin does not matter: each row is summed by one
 // lane in its CSR order wherever it lands.
 static __global__ void slice_sort_rows(const int *__restrict__ seg, int seg_stride, int nblk,
@@ -648,7 +669,7 @@ static __global__ void slice_sort_rows(const int *__restrict__ seg, int seg_stri
             const unsigned short row = dst[t * 32 + l];
             if (row != 0xffffu) w = max(w, hi[row] - lo[row]);
         }
-        slice_width[s0 + t] = w;
+        slice_width[s0 + t] = (w + 1) & ~1;  // whole step pairs
     }
 }
 
@@ -681,16 +702,18 @@ static __global__ void slice_offsets(const int *__restrict__ width, int total, u
     }
 }
 
-// Step 3 -- one warp per slice: copy each lane's row segment, column-major,
-// values and 16-bit local columns; padding steps get value 0, column 0.
-static __global__ void slice_fill(const int *__restrict__ seg, int seg_stride, int nblk, int width,
-                                  const int *__restrict__ row_split,
-                                  const int *__restrict__ chunk_slice, int nchunks,
-                                  const int *__restrict__ colidx, const double *__restrict__ a,
-                                  const unsigned short *__restrict__ srow,
-                                  const int *__restrict__ slice_width,
-                                  const unsigned *__restrict__ slice_off, int total, double *sval,
-                                  float *sval32, unsigned short *scol)
+// Step 3 -- one warp per slice: copy each lane's row segment in step-pair
+// column-major order (entry k of lane i at off + 64 (k/2) + 2 i + k%2),
+// values (from FP64 or FP32 source values; sval or sval32 may be null) and
+// 16-bit local columns; padding steps get value 0, column 0.
+template <typename ST>
+__global__ void slice_fill(const int *__restrict__ seg, int seg_stride, int nblk, int width,
+                           const int *__restrict__ row_split, const int *__restrict__ chunk_slice,
+                           int nchunks, const int *__restrict__ colidx, const ST *__restrict__ a,
+                           const unsigned short *__restrict__ srow,
+                           const int *__restrict__ slice_width,
+                           const unsigned *__restrict__ slice_off, int total, double *sval,
+                           float *sval32, unsigned short *scol)
 {
     const int lane = threadIdx.x & 31;
     for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < total;
@@ -710,19 +733,20 @@ static __global__ void slice_fill(const int *__restrict__ seg, int seg_stride, i
             e1 = seg[size_t(b + 1) * seg_stride + j];
         }
         const int w = slice_width[s];
-        const unsigned off = slice_off[s] + lane;
+        const unsigned off = slice_off[s] + 2u * lane;
         const int base = b * width;
         for (int k = 0; k < w; k++) {
             const int e = e0 + k;
             double v = 0.0;
             int col = 0;
             if (e < e1) {
-                v = a[e];
+                v = double(a[e]);
                 col = colidx[e] - base;
             }
-            sval[off + 32u * k] = v;
-            if (sval32) sval32[off + 32u * k] = float(v);
-            scol[off + 32u * k] = (unsigned short)col;
+            const unsigned at = off + 64u * unsigned(k >> 1) + unsigned(k & 1);
+            if (sval) sval[at] = v;
+            if (sval32) sval32[at] = float(v);
+            scol[at] = (unsigned short)col;
         }
     }
 }

@@ -4,6 +4,8 @@
 //   cg S|W|A|B|C            an NPB class (setparams.cpp:751-785 parameters)
 //   cg U --n N --nonzer K --niter I --shift S [--seed X]   custom sizes
 //   options: --mode fp64|tol|mixed|learned  --tol T  --cgitmax M
+//            --weights FILE (learned mode: network weights, raw FP32; default
+//            the trained weights shipped beside the package, npbcg/lp_weights.f32)
 //            --device D  --json (one JSON result line instead of the report)
 //
 // Like the reference it generates the matrix (makea), runs the timed inverse
@@ -13,6 +15,8 @@
 // reference's operation count (cg.cu:553-561).  The timed region is the
 // device time of the outer loop; matrix generation and upload are outside
 // it, as in the reference (cg.cu:490-522).
+#include <unistd.h>
+
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -51,7 +55,50 @@ void usage()
     std::fprintf(stderr,
                  "usage: cg S|W|A|B|C|D | cg U --n N --nonzer K --niter I --shift S [--seed X]\n"
                  "          [--mode fp64|tol|mixed|learned] [--tol T] [--cgitmax M]\n"
-                 "          [--device D] [--json]\n");
+                 "          [--weights FILE] [--device D] [--json]\n");
+}
+
+// The weights shipped with the package: <dir of this binary>/../npbcg/lp_weights.f32.
+std::string default_weights()
+{
+    char buf[4096];
+    const ssize_t len = readlink("/proc/self/exe", buf, sizeof(buf) - 1);
+    if (len <= 0) return "lp_weights.f32";
+    std::string exe(buf, size_t(len));
+    const size_t slash = exe.rfind('/');
+    const std::string dir = slash == std::string::npos ? "." : exe.substr(0, slash);
+    return dir + "/../npbcg/lp_weights.f32";
+}
+
+// Learned mode: loads the network weights, infers G for this matrix and
+// installs F = G / sqrt(delta) in the session.
+int attach_learned(cgb_session *s, const std::string &path, int device, int n,
+                   const std::vector<int> &rowstr, const std::vector<int> &colidx,
+                   const std::vector<double> &a)
+{
+    const int count = cgb_gnn_param_count();
+    std::vector<float> w(static_cast<size_t>(count));
+    FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f) {
+        std::fprintf(stderr, "cg: cannot open weights %s\n", path.c_str());
+        return 1;
+    }
+    const size_t got = std::fread(w.data(), sizeof(float), w.size(), f);
+    const bool extra = std::fgetc(f) != EOF;
+    std::fclose(f);
+    if (got != w.size() || extra) {
+        std::fprintf(stderr, "cg: %s holds no %d FP32 weights\n", path.c_str(), count);
+        return 1;
+    }
+    cgb_gnn *m = nullptr;
+    cgb_gnn_graph *g = nullptr;
+    int st = cgb_gnn_create(device, 0u, &m);
+    if (!st) st = cgb_gnn_set_params(m, w.data(), count);
+    if (!st) st = cgb_gnn_graph_create(m, n, rowstr.data(), colidx.data(), a.data(), &g);
+    if (!st) st = cgb_gnn_attach(m, g, s);
+    if (g) cgb_gnn_graph_destroy(g);
+    if (m) cgb_gnn_destroy(m);
+    return st ? fail(st, "learned preconditioner") : 0;
 }
 
 }  // namespace
@@ -75,6 +122,7 @@ int main(int argc, char **argv)
         return 2;
     }
     double seed = 314159265.0, tol = 1e-12;
+    std::string weights;
     int mode = CGB_MODE_FP64, cgitmax = 25, device = 0, json = 0;
     for (int i = 2; i < argc; i++) {
         const std::string a = argv[i];
@@ -94,6 +142,7 @@ int main(int argc, char **argv)
         else if (a == "--cgitmax") cgitmax = std::atoi(next());
         else if (a == "--device") device = std::atoi(next());
         else if (a == "--json") json = 1;
+        else if (a == "--weights") weights = next();
         else if (a == "--mode") {
             const std::string m = next();
             if (m == "fp64") mode = CGB_MODE_FP64;
@@ -130,6 +179,12 @@ int main(int argc, char **argv)
     cgb_session *s = nullptr;
     st = cgb_create(P.n, rowstr.data(), colidx.data(), a.data(), &opt, &s);
     if (st) return fail(st, "create");
+    if (mode == CGB_MODE_MIXED_LEARNED &&
+        attach_learned(s, weights.empty() ? default_weights() : weights, device, P.n, rowstr,
+                       colidx, a) != 0) {
+        cgb_destroy(s);
+        return 1;
+    }
 
     cgb_solve_params sp;
     cgb_default_solve_params(&sp);

@@ -557,17 +557,14 @@ void colsum(cgb_gnn *m, const float *a, const float *b, int n, int slot)
 }
 
 // Probes: 32 columns of R.  `cg_steps` = 0: normal random vectors; else the
-// residuals after cg_steps batched CG steps on Ahat started from 31 random
-// right-hand sides and the all-ones one (the benchmark's first x).
+// residuals after cg_steps batched CG steps on Ahat (from z0 = 0) for 32
+// random right-hand sides.
 int make_probes(cgb_gnn *m, cgb_gnn_graph *g, unsigned seed, int cg_steps)
 {
     const int n = g->n;
     const size_t total = size_t(n) * kH;
     k_normal<<<grid_rows(m, n), 256, 0, m->stream>>>(g->R, total, seed);
     if (cg_steps > 0) {
-        // column 0 = ones (overwrite through a tiny copy from a host pattern)
-        std::vector<float> ones_col(1, 1.f);
-        (void)ones_col;
         // R = b (random), r0 = b (z0 = 0), p0 = r0
         GNN_TRY(cudaMemcpyAsync(g->Pv, g->R, total * sizeof(float), cudaMemcpyDeviceToDevice, m->stream));
         float *rho = m->colv + 0 * kH, *pq = m->colv + 1 * kH, *alpha = m->colv + 2 * kH;

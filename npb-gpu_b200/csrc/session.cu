@@ -201,14 +201,13 @@ struct cgb_session {
     bool sorted = false;
     int sliced_grid = 0;   // grid the layout was built for (0: none)
     int sliced_max_rows = 0;
-    int *d_chunk_slice = nullptr;
-    unsigned short *d_srow = nullptr;
-    int *d_slice_width = nullptr;
-    unsigned *d_slice_off = nullptr;
-    double *d_sval = nullptr;
-    float *d_sval32 = nullptr;
-    unsigned short *d_scol = nullptr;
-    long long slice_entries = 0;
+    int *d_chunk_slice = nullptr;  // shared by A, F and F^T (same row split)
+    cgb::SliceSet sa;              // A: FP64 values (+ FP32 copy)
+    cgb::SliceSet sf, sft;         // F and F^T: FP32 values
+    int layout_gen = 0;            // bumped by every build of A's slices
+    int prec_gen = -1;             // layout_gen sf / sft were built for
+    int sliced_grid_pending = 0;   // grid of the layout being built
+    int slice_total = 0;           // slices per matrix (all chunks)
 
     Plan plan;
     std::vector<int> h_rowstr_copy;
@@ -241,17 +240,30 @@ void drop_graph(cgb_session *s)
     s->g_valid = false;
 }
 
+void free_set(SliceSet &t)
+{
+    dev_free(t.srow);
+    dev_free(t.width);
+    dev_free(t.off);
+    dev_free(t.sval);
+    dev_free(t.sval32);
+    dev_free(t.scol);
+    t.entries = 0;
+}
+
+void free_prec_slices(cgb_session *s)
+{
+    free_set(s->sf);
+    free_set(s->sft);
+    s->prec_gen = -1;
+}
+
 void free_sliced(cgb_session *s)
 {
     dev_free(s->d_chunk_slice);
-    dev_free(s->d_srow);
-    dev_free(s->d_slice_width);
-    dev_free(s->d_slice_off);
-    dev_free(s->d_sval);
-    dev_free(s->d_sval32);
-    dev_free(s->d_scol);
+    free_set(s->sa);
+    free_prec_slices(s);
     s->sliced_grid = 0;
-    s->slice_entries = 0;
 }
 
 void release(cgb_session *s)
@@ -288,6 +300,21 @@ void release(cgb_session *s)
     delete s;
 }
 
+// Points the sliced members of M at slice set t (A's row split and blocks).
+void set_slices(cgb_session *s, const SliceSet &t, MatrixView *M)
+{
+    M->sval = t.sval;
+    M->sval32 = t.sval32;
+    M->scol = t.scol;
+    M->srow = t.srow;
+    M->slice_off = t.off;
+    M->slice_width = t.width;
+    M->chunk_slice = s->d_chunk_slice;
+    M->nblk = s->nblk;
+    M->width = kSliceWidth;
+    M->max_rows = s->sliced_max_rows;
+}
+
 MatrixView matrix_view(cgb_session *s)
 {
     MatrixView M{};
@@ -295,16 +322,7 @@ MatrixView matrix_view(cgb_session *s)
     M.colidx = s->d_colidx;
     M.a = s->d_a;
     M.a32 = s->d_a32;
-    M.sval = s->d_sval;
-    M.sval32 = s->d_sval32;
-    M.scol = s->d_scol;
-    M.srow = s->d_srow;
-    M.slice_off = s->d_slice_off;
-    M.slice_width = s->d_slice_width;
-    M.chunk_slice = s->d_chunk_slice;
-    M.nblk = s->nblk;
-    M.width = kSliceWidth;
-    M.max_rows = s->sliced_max_rows;
+    set_slices(s, s->sa, &M);
     return M;
 }
 
@@ -327,6 +345,10 @@ OuterArgs outer_args(cgb_session *s)
     A.FT.rowstr = s->d_ft_ptr;
     A.FT.colidx = s->d_ft_col;
     A.FT.a32 = s->d_ft_val;
+    if (s->prec_gen == s->layout_gen && s->prec_gen >= 0) {
+        set_slices(s, s->sf, &A.F);
+        set_slices(s, s->sft, &A.FT);
+    }
     A.row_split = s->d_split;
     A.part = s->d_part;
     A.gpad = s->gpad;
@@ -380,6 +402,40 @@ int build_segments_table(cgb_session *s)
     return CGB_OK;
 }
 
+// Steps 1-3 of a sliced copy of one matrix over the current row split
+// (d_split and d_chunk_slice on the device, `total` slices): row order per
+// slice, slice offsets, then values (FP64 and/or FP32) and local columns.
+// `seg` is the matrix's segment table.
+template <typename ST>
+int fill_set(cgb_session *s, const int *seg, const int *d_colidx, const ST *vals, int total,
+             bool want64, bool want32, SliceSet *t)
+{
+    const int nchunks = s->sliced_grid_pending * s->nblk;
+    if (dev_alloc(&t->srow, size_t(total) * 32) || dev_alloc(&t->width, size_t(total)) ||
+        dev_alloc(&t->off, size_t(total) + 1))
+        return set_error(CGB_ERR_NOMEM, "sliced layout: metadata allocation failed");
+    slice_sort_rows<<<nchunks, 256, 0, s->stream>>>(seg, s->seg_stride, s->nblk, s->d_split,
+                                                   s->d_chunk_slice, t->srow, t->width);
+    CUDA_TRY(cudaGetLastError());
+    slice_offsets<<<1, 1024, 0, s->stream>>>(t->width, total, t->off);
+    CUDA_TRY(cudaGetLastError());
+    unsigned entries = 0;
+    CUDA_TRY(cudaMemcpyAsync(&entries, t->off + total, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                             s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    t->entries = entries;
+    if ((want64 && dev_alloc(&t->sval, size_t(entries) + kPad)) ||
+        dev_alloc(&t->scol, size_t(entries) + kPad) ||
+        (want32 && dev_alloc(&t->sval32, size_t(entries) + kPad)))
+        return set_error(CGB_ERR_NOMEM, "sliced layout: %u entries do not fit", entries);
+    slice_fill<ST><<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
+        seg, s->seg_stride, s->nblk, kSliceWidth, s->d_split, s->d_chunk_slice, nchunks, d_colidx,
+        vals, t->srow, t->width, t->off, total, t->sval, t->sval32, t->scol);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return CGB_OK;
+}
+
 // The sliced copy of the matrix for a row split over `grid` CTAs (one per SM).
 int build_sliced(cgb_session *s, int grid)
 {
@@ -401,33 +457,61 @@ int build_sliced(cgb_session *s, int grid)
     s->sliced_max_rows = (max_rows + 31) & ~31;
     if (s->sliced_max_rows >= 0xffff || sliced_smem_bytes(s->sliced_max_rows) > kSmemLimit)
         return set_error(CGB_ERR_STATE, "sliced layout: %d rows per CTA exceed shared memory", max_rows);
-    const int nchunks = grid * s->nblk;
-    if (dev_alloc(&s->d_chunk_slice, chunk_slice.size()) || dev_alloc(&s->d_srow, size_t(total) * 32) ||
-        dev_alloc(&s->d_slice_width, size_t(total)) || dev_alloc(&s->d_slice_off, size_t(total) + 1))
+    if (dev_alloc(&s->d_chunk_slice, chunk_slice.size()))
         return set_error(CGB_ERR_NOMEM, "sliced layout: metadata allocation failed");
     CUDA_TRY(cudaMemcpy(s->d_split, split.data(), sizeof(int) * (grid + 1), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(s->d_chunk_slice, chunk_slice.data(), sizeof(int) * chunk_slice.size(),
                         cudaMemcpyHostToDevice));
-    slice_sort_rows<<<nchunks, 256, 0, s->stream>>>(s->d_seg, s->seg_stride, s->nblk, s->d_split,
-                                                   s->d_chunk_slice, s->d_srow, s->d_slice_width);
-    CUDA_TRY(cudaGetLastError());
-    slice_offsets<<<1, 1024, 0, s->stream>>>(s->d_slice_width, total, s->d_slice_off);
-    CUDA_TRY(cudaGetLastError());
-    unsigned entries = 0;
-    CUDA_TRY(cudaMemcpyAsync(&entries, s->d_slice_off + total, sizeof(unsigned),
-                             cudaMemcpyDeviceToHost, s->stream));
-    CUDA_TRY(cudaStreamSynchronize(s->stream));
-    s->slice_entries = entries;
-    if (dev_alloc(&s->d_sval, size_t(entries) + kPad) || dev_alloc(&s->d_scol, size_t(entries) + kPad) ||
-        (s->opts.keep_fp32_copy && dev_alloc(&s->d_sval32, size_t(entries) + kPad)))
-        return set_error(CGB_ERR_NOMEM, "sliced layout: %u entries do not fit", entries);
-    slice_fill<<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
-        s->d_seg, s->seg_stride, s->nblk, kSliceWidth, s->d_split, s->d_chunk_slice, nchunks,
-        s->d_colidx, s->d_a, s->d_srow, s->d_slice_width, s->d_slice_off, total, s->d_sval,
-        s->d_sval32, s->d_scol);
-    CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->sliced_grid_pending = grid;
+    s->slice_total = total;
+    const int st = fill_set<double>(s, s->d_seg, s->d_colidx, s->d_a, total, true,
+                                    s->opts.keep_fp32_copy != 0, &s->sa);
+    if (st) return st;
     s->sliced_grid = grid;
+    s->layout_gen++;
+    return CGB_OK;
+}
+
+// Sliced copies of F and F^T (FP32) over A's row split, built on first use
+// by the preconditioned solver after each change of F or of A's layout.
+// F^T rows ascend by construction; F rows are sorted by the setter.
+int ensure_prec_slices(cgb_session *s)
+{
+    if (s->plan.kind != kKindSliced || !s->has_prec) return CGB_OK;
+    if (s->prec_gen == s->layout_gen) return CGB_OK;
+    free_prec_slices(s);
+    const int n = s->n;
+    const size_t count = size_t(s->nblk + 1) * s->seg_stride;
+    int *seg = nullptr;
+    if (dev_alloc(&seg, count) != cudaSuccess)
+        return set_error(CGB_ERR_NOMEM, "factor segment table allocation failed");
+    int st = CGB_OK;
+    const int *ptrs[2] = {s->d_f_ptr, s->d_ft_ptr};
+    const int *cols[2] = {s->d_f_col, s->d_ft_col};
+    const float *vals[2] = {s->d_f_val, s->d_ft_val};
+    SliceSet *sets[2] = {&s->sf, &s->sft};
+    for (int m = 0; m < 2 && st == CGB_OK; m++) {
+        cudaError_t e = cudaMemsetAsync(s->d_flag, 0, sizeof(int), s->stream);
+        if (e == cudaSuccess) {
+            build_segments<<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
+                ptrs[m], cols[m], n, s->nblk, kSliceWidth, seg, s->seg_stride, s->d_flag);
+            e = cudaGetLastError();
+        }
+        int unsorted = 0;
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&unsorted, s->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess) st = set_error(CGB_ERR_CUDA, "factor segments: %s", cudaGetErrorString(e));
+        else if (unsorted) st = set_error(CGB_ERR_STATE, "factor rows not in ascending column order");
+        else st = fill_set<float>(s, seg, cols[m], vals[m], s->slice_total, false, true, sets[m]);
+    }
+    dev_free(seg);
+    if (st) {
+        free_prec_slices(s);
+        return st;
+    }
+    s->prec_gen = s->layout_gen;
+    drop_graph(s);
     return CGB_OK;
 }
 
@@ -675,6 +759,9 @@ cudaError_t enqueue_power(cgb_session *s, const cgb_solve_params &P)
     const OuterKernel k = P.mode == CGB_MODE_MIXED_LEARNED ? s->plan.pcg
                           : P.mode == CGB_MODE_MIXED       ? s->plan.mixed
                                                            : s->plan.fp64;
+    // the sliced preconditioned kernel reads F / F^T slices (ensure_prec_slices)
+    if (P.mode == CGB_MODE_MIXED_LEARNED && s->plan.kind == kKindSliced && A.F.srow == nullptr)
+        return cudaErrorInvalidValue;
     for (int it = 0; it < P.niter; it++) {
         A.step = it;
         e = launch_outer(s, k, A);
@@ -914,6 +1001,10 @@ int cgb_power_iterate(cgb_session *s, const cgb_solve_params *params, double *ze
     CUDA_TRY(cudaSetDevice(s->device));
     st = ensure_trace(s, P.niter);
     if (st) return st;
+    if (P.mode == CGB_MODE_MIXED_LEARNED) {
+        st = ensure_prec_slices(s);
+        if (st) return st;
+    }
     if (s->opts.use_graph) {
         if (!(s->g_valid && same_params(s->g_params, P))) {
             drop_graph(s);
@@ -991,21 +1082,46 @@ int cgb_set_preconditioner(cgb_session *s, const int *fptr, const int *fcol, con
         }
         if (!diag) return set_error(CGB_ERR_BAD_MATRIX, "factor: row %d has no diagonal", i);
     }
-    const long long nf = fptr[n];
+    // F with each row in ascending column order, repeated columns summed
+    // (the sliced products need ascending rows); values rounded to FP32
+    std::vector<int> optr(n + 1, 0), ocol;
+    std::vector<float> val32;
+    ocol.reserve(size_t(fptr[n]));
+    val32.reserve(size_t(fptr[n]));
+    std::vector<std::pair<int, double>> row;
+    for (int i = 0; i < n; i++) {
+        row.clear();
+        for (int k = fptr[i]; k < fptr[i + 1]; k++) row.emplace_back(fcol[k], fval[k]);
+        std::stable_sort(row.begin(), row.end(),
+                         [](const std::pair<int, double> &a, const std::pair<int, double> &b) {
+                             return a.first < b.first;
+                         });
+        for (size_t k = 0; k < row.size(); k++) {
+            if (k > 0 && row[k].first == row[k - 1].first) {
+                row[k].second += row[k - 1].second;
+                ocol.pop_back();
+                val32.pop_back();
+            }
+            ocol.push_back(row[k].first);
+            val32.push_back(float(row[k].second));
+        }
+        optr[i + 1] = int(ocol.size());
+    }
+    const long long nf = optr[n];
     // transpose (rows of F^T = columns of F), rows in ascending order
     std::vector<int> tptr(n + 1, 0), tcol(nf);
-    std::vector<float> tval(nf), val32(nf);
-    for (long long k = 0; k < nf; k++) tptr[fcol[k] + 1]++;
+    std::vector<float> tval(nf);
+    for (long long k = 0; k < nf; k++) tptr[ocol[k] + 1]++;
     for (int i = 0; i < n; i++) tptr[i + 1] += tptr[i];
     std::vector<int> cur(tptr.begin(), tptr.end() - 1);
     for (int i = 0; i < n; i++)
-        for (int k = fptr[i]; k < fptr[i + 1]; k++) {
-            const int at = cur[fcol[k]]++;
+        for (int k = optr[i]; k < optr[i + 1]; k++) {
+            const int at = cur[ocol[k]]++;
             tcol[at] = i;
-            tval[at] = float(fval[k]);
-            val32[k] = float(fval[k]);
+            tval[at] = val32[k];
         }
     CUDA_TRY(cudaSetDevice(s->device));
+    free_prec_slices(s);
     dev_free(s->d_f_ptr); dev_free(s->d_f_col); dev_free(s->d_f_val);
     dev_free(s->d_ft_ptr); dev_free(s->d_ft_col); dev_free(s->d_ft_val);
     s->has_prec = false;
@@ -1017,8 +1133,8 @@ int cgb_set_preconditioner(cgb_session *s, const int *fptr, const int *fcol, con
     CUDA_TRY(cudaMemset(s->d_f_val, 0, sizeof(float) * (nf + kPad)));
     CUDA_TRY(cudaMemset(s->d_ft_col, 0, sizeof(int) * (nf + kPad)));
     CUDA_TRY(cudaMemset(s->d_ft_val, 0, sizeof(float) * (nf + kPad)));
-    CUDA_TRY(cudaMemcpy(s->d_f_ptr, fptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(s->d_f_col, fcol, sizeof(int) * nf, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->d_f_ptr, optr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->d_f_col, ocol.data(), sizeof(int) * nf, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(s->d_f_val, val32.data(), sizeof(float) * nf, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(s->d_ft_ptr, tptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(s->d_ft_col, tcol.data(), sizeof(int) * nf, cudaMemcpyHostToDevice));
@@ -1044,7 +1160,7 @@ int cgb_plan_info(cgb_session *s, int *kind, int *lanes_per_row, int *grid, int 
     if (grid) *grid = s->plan.grid;
     if (block) *block = s->plan.block;
     if (smem_bytes) *smem_bytes = (long long)s->plan.smem;
-    if (layout_entries) *layout_entries = s->plan.kind == kKindSliced ? s->slice_entries : s->nnz;
+    if (layout_entries) *layout_entries = s->plan.kind == kKindSliced ? s->sa.entries : s->nnz;
     return CGB_OK;
 }
 

@@ -14,8 +14,11 @@
 //   SlicedSpmv     a sliced copy of the matrix built on the device (see
 //                  slices.cuh): per CTA and per column block of W columns,
 //                  the CTA's rows sorted by length and packed 32 to a slice,
-//                  stored column-major (entry k of the slice's lane i at
-//                  offset + 32 k + i) with 16-bit local columns.  The block
+//                  stored column-major by step pairs (entry k of the slice's
+//                  lane i at offset + 64 (k/2) + 2 i + k%2, widths rounded up
+//                  to even) with 16-bit local columns, so a lane reads two
+//                  steps per load: one 16/8-byte value pair and one 4-byte
+//                  column pair.  The block
 //                  of v is staged in shared memory by TMA bulk copies
 //                  (cp.async.bulk + mbarrier) into a 2-slot ring; warps walk
 //                  the blocks independently and the last warp done with a
@@ -52,6 +55,18 @@ __device__ __forceinline__ VT group_sum_vt(VT v, unsigned mask)
     for (int off = W / 2; off > 0; off >>= 1) v += __shfl_xor_sync(mask, v, off);
     return v;
 }
+
+// Device arrays of one sliced copy (host-side bookkeeping; any pointer may
+// be null when that precision is not kept).
+struct SliceSet {
+    unsigned short *srow = nullptr;   // local row per (slice, lane)
+    int *width = nullptr;             // steps per slice (even)
+    unsigned *off = nullptr;          // first entry per slice, + total
+    double *sval = nullptr;           // FP64 values
+    float *sval32 = nullptr;          // FP32 values
+    unsigned short *scol = nullptr;   // local columns
+    long long entries = 0;            // padded entries
+};
 
 // Matrix in both layouts, both precisions (unused members may be null).
 struct MatrixView {
@@ -263,7 +278,8 @@ struct SlicedSpmv {
                                             const double *dotv, int n, long long limit_ns,
                                             int *status, bool &ok)
     {
-        constexpr int kU = 8;  // slice steps in flight per lane
+        using P2 = typename Pair<VT>::T;
+        constexpr int kU = sizeof(VT) == 8 ? 4 : 6;  // step pairs in flight per lane (measured best)
         const VT *__restrict__ vals = slice_values<VT>(M);
         const int lane = threadIdx.x & 31;
         const int warp = threadIdx.x >> 5;
@@ -296,23 +312,28 @@ struct SlicedSpmv {
             // widest slices do not always land on the same warps
             const int rot = (b * 7) % nwarps;
             for (int s = s0 + (warp + rot) % nwarps; s < s1; s += nwarps) {
-                const unsigned off = __ldg(M.slice_off + s) + lane;
-                const int w = __ldg(M.slice_width + s);
+                const unsigned off = __ldg(M.slice_off + s) + 2u * lane;
+                const int wp = __ldg(M.slice_width + s) >> 1;
                 const unsigned short row = __ldg(M.srow + size_t(s) * 32 + lane);
                 VT sum = VT(0);
-                for (int k = 0; k < w; k += kU) {
-                    VT av[kU];
-                    unsigned short cv[kU];
+                for (int m = 0; m < wp; m += kU) {
+                    P2 av[kU];
+                    ushort2 cv[kU];
 #pragma unroll
                     for (int u = 0; u < kU; u++) {
-                        if (k + u < w) {
-                            av[u] = __ldcs(vals + off + 32u * unsigned(k + u));
-                            cv[u] = __ldcs(M.scol + off + 32u * unsigned(k + u));
+                        if (m + u < wp) {
+                            const unsigned e = off + 64u * unsigned(m + u);
+                            av[u] = __ldcs(reinterpret_cast<const P2 *>(vals + e));
+                            cv[u] = __ldcs(reinterpret_cast<const ushort2 *>(M.scol + e));
                         }
                     }
 #pragma unroll
-                    for (int u = 0; u < kU; u++)
-                        if (k + u < w) sum = fma_vt(av[u], pv[cv[u]], sum);
+                    for (int u = 0; u < kU; u++) {
+                        if (m + u < wp) {
+                            sum = fma_vt(av[u].x, pv[cv[u].x], sum);
+                            sum = fma_vt(av[u].y, pv[cv[u].y], sum);
+                        }
+                    }
                 }
                 if (row != 0xffffu) accb[row] += double(sum);
             }

@@ -4,7 +4,8 @@ FP64 mode is the reference algorithm, so each system must match the
 single-system session (and the CPU oracle) to zeta relative 1e-10.  MIXED
 mode is judged against the FP64 mode of the same batch: zeta relative 1e-10
 where that judge has converged (its final rnorm <= 1e-10), and a system the
-mixed iteration gives up on (status 1) is re-solved in FP64, bit-identically.
+mixed iteration gives up on (status 1) is re-solved with the FP64 reference
+algorithm, bit-identically.
 """
 import numpy as np
 import pytest
@@ -55,8 +56,9 @@ def test_batch_mixed_against_fp64_judge(cgb):
 
 
 def test_batch_indefinite_system_falls_back(cgb):
-    """n=1400, nonzer=13, shift=11.4 is indefinite: the mixed iteration must
-    give up and the system be solved with the reference algorithm."""
+    """n=1400, nonzer=13, shift=11.4 is symmetric indefinite (eigenvalues
+    from -11.3 to 11.4): the mixed iteration must give up on it and the
+    system be solved with the reference algorithm, bit-identically."""
     specs = [(1400, 13, 11.4, 314159265.0), (1400, 7, 11.4, 314159265.0)]
     systems, shifts = build(cgb, specs)
     with cgb.Batch(systems, shifts) as b:
@@ -68,7 +70,24 @@ def test_batch_indefinite_system_falls_back(cgb):
     assert abs(mixed["zeta"][1] - judge["zeta"][1]) <= 1e-10 * abs(judge["zeta"][1])
 
 
+def test_batch_fallback_is_the_reference_algorithm(cgb):
+    """A cap too small to converge makes every mixed solve give up; each
+    system is then solved again with the FP64 reference algorithm (25 steps
+    whatever the mixed cap), bit-identical to the FP64 mode."""
+    specs = [(1400, 7, 10.0, 314159265.0), (3000, 11, 13.0, 271828183.0),
+             (1400, 13, 11.4, 314159265.0)]
+    systems, shifts = build(cgb, specs)
+    with cgb.Batch(systems, shifts) as b:
+        judge = b.solve(niter=5)
+        mixed = b.solve(niter=5, mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=2)
+    assert np.all(mixed["status"] == 1)
+    assert np.array_equal(mixed["zeta"], judge["zeta"])
+    assert np.array_equal(mixed["iters"], judge["iters"])
+
+
 def test_batch_tune_keeps_results(cgb):
+    """Retuning changes lanes per row and block shape, hence the order of
+    the row sums; converged systems keep zeta to 1e-10."""
     specs = cgb.batch_config5(nsys=24, seed=11, n_range=(1400, 6000))
     systems, shifts = build(cgb, specs)
     with cgb.Batch(systems, shifts) as b:
@@ -76,7 +95,10 @@ def test_batch_tune_keeps_results(cgb):
         cfg = b.tune(niter=1)
         after = b.solve(niter=3)
     assert cfg["block"] in (512, 1024) and cfg["best_ms"] > 0
-    assert np.max(np.abs(after["zeta"] - before["zeta"]) / np.abs(before["zeta"])) <= 1e-12
+    conv = before["rnorm"] <= 1e-10
+    assert conv.sum() >= 12
+    rel = np.abs(after["zeta"] - before["zeta"]) / np.abs(before["zeta"])
+    assert np.all(rel[conv] <= 1e-10), rel[conv].max()
 
 
 def test_batch_rejects_oversize(cgb):

@@ -202,3 +202,47 @@ def test_learned_gain_over_method_without_it(cgb):
           f"untrained={loss_untrained:.4g} identity={loss_identity:.4g}")
     assert loss_learned < loss_untrained and loss_learned < loss_identity
     assert lrn["total_inner"] <= plain["total_inner"]
+
+
+def test_learned_sliced_plan_matches_row_plan(cgb, golden):
+    """Class B with the trained factor under both SpMV policies: the sliced
+    plan applies F and F^T through their own sliced copies, the row plan
+    through CSR rows; both reach the reference zeta trace."""
+    model, how = trained_model(cgb)
+    n, nonzer, niter, shift = PARAMS["B"]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    zr = np.array(golden["B"]["seeds"]["314159265.0"]["zeta"])
+    iters = {}
+    for kind in (1, 2):
+        with cgb.Session(rs, ci, a, spmv_kernel=kind) as s, model.graph(rs, ci, a) as g:
+            assert s.plan()["kind"] == ("row" if kind == 1 else "sliced")
+            model.attach(g, s)
+            out = s.power_iterate(niter, shift, mode=cgb.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=200)
+        assert np.max(np.abs(out["zeta"] - zr) / np.abs(zr)) <= 1e-10, (kind, how)
+        iters[kind] = out["total_inner"]
+    # same mathematics, FP32 sums in another order: iteration counts agree closely
+    assert abs(iters[1] - iters[2]) <= 0.05 * iters[1], iters
+
+
+def test_factor_rows_sorted_and_merged(cgb):
+    """A factor given with unsorted rows and a repeated column equals the
+    sorted, merged one (here Jacobi split into halves around an explicit
+    zero), bit for bit, under the sliced plan."""
+    n, nonzer, niter, shift = PARAMS["B"]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    fp, fc, fv = cgb.jacobi_factor(rs, ci, a)
+    ptr, col, val = [0], [], []
+    for i in range(n):
+        ent = [(i, fv[i] / 2)] + ([(i - 1, 0.0)] if i > 0 else []) + [(i, fv[i] / 2)]
+        for c, v in ent:
+            col.append(c)
+            val.append(v)
+        ptr.append(len(col))
+    kw = dict(mode=cgb.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=200)
+    with cgb.Session(rs, ci, a, spmv_kernel=2) as s:
+        s.set_preconditioner(fp, fc, fv)
+        ref = s.power_iterate(5, shift, **kw)
+        s.set_preconditioner(np.array(ptr, np.int32), np.array(col, np.int32), np.array(val))
+        out = s.power_iterate(5, shift, **kw)
+    assert np.array_equal(out["zeta"], ref["zeta"])
+    assert out["total_inner"] == ref["total_inner"]
