@@ -118,6 +118,11 @@ typedef struct cgb_solve_params {
     int refresh_every;  /* MIXED*: replace r by x - A z in FP64 (and restart) at least every
                            k steps (10); also when the recursive residual fell 1e-6 since the
                            last replacement, and before accepting convergence */
+    int recycle;        /* tolerance modes: start each solve from the Galerkin solution on the
+                           last `recycle` power-iteration iterates (0..4, default 4; 0 = from
+                           z = 0).  The iterates span a Krylov space of A, and A times each
+                           comes from the previous step's residual product, so the start
+                           costs dot products only.  Ignored in CGB_MODE_FP64. */
 } cgb_solve_params;
 
 void cgb_default_solve_params(cgb_solve_params *p);

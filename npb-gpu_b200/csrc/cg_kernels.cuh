@@ -27,15 +27,18 @@
 //                          computed with the FP64 matrix stay in FP64.
 #pragma once
 
-#include <type_traits>
-
 #include "spmv_policies.cuh"
 
 namespace cgb {
 
+// Galerkin start: at most kMaxRecycle previous iterates; the Gram values
+// x_a . A x_b (a <= b) and x_a . x, per CTA.
+constexpr int kMaxRecycle = 4;
+constexpr int kGramValues = kMaxRecycle * (kMaxRecycle + 1) / 2 + kMaxRecycle;
+
 // Partial-sum slots (each holds `gpad` doubles, one per CTA).
 enum Slot { kSlotRho = 0, kSlotD = 1, kSlotXX = 2, kSlotRes = 3, kSlotXZ = 4, kSlotZZ = 5,
-            kSlotCount = 6 };
+            kSlotGram = 6, kSlotCount = kSlotGram + kGramValues };
 
 // Per-step trace record written by CTA 0.
 struct StepTrace {
@@ -67,6 +70,11 @@ struct OuterArgs {
     int step;           // outer step index (trace slot)
     int finish;         // 1: zeta + x update (power iteration); 0: conj_grad only
     StepTrace *trace;
+    // Galerkin start (tolerance modes): ring of the last `recycle` iterates
+    // x_j and A x_j, slot j % recycle, `hstride` doubles a vector
+    double *hx, *hw;
+    size_t hstride;
+    int recycle;        // 0: off; 1..kMaxRecycle
 };
 
 // Writes this CTA's share of a reduction into slot `slot`.
@@ -128,7 +136,7 @@ __device__ __forceinline__ void start_solve(const OuterArgs &A, int row0, int ve
 template <class Spmv>
 __device__ __forceinline__ void end_solve(Spmv &sp, const OuterArgs &A, int row0, int row1, int it,
                                           double rho, int refreshes, bool r_true, double *scratch,
-                                          double *bcast)
+                                          double *bcast, double rsign = 1.0)
 {
     if (!r_true) {
         bool ok = true;
@@ -164,8 +172,255 @@ __device__ __forceinline__ void end_solve(Spmv &sp, const OuterArgs &A, int row0
     }
     if (A.finish) {
         const double norm = 1.0 / sqrt(t2);
-        for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) A.x[j] = norm * A.z[j];
+        if (A.recycle > 0 && !A.fixed) {
+            // the next iterate and A times it, for the next step's Galerkin
+            // start: A x' = norm A z, with A z = r (SpMV above) or, when r
+            // is the true residual rsign (x - A z), A z = x - rsign r
+            const size_t slot = size_t((A.step + 1) % A.recycle) * A.hstride;
+            for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) {
+                const double az = r_true ? A.x[j] - rsign * A.r[j] : A.r[j];
+                const double xn = norm * A.z[j];
+                A.hx[slot + j] = xn;
+                A.hw[slot + j] = norm * az;
+                A.x[j] = xn;
+            }
+        } else {
+            for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) A.x[j] = norm * A.z[j];
+        }
     }
+}
+
+// ---------------------------------------------------------- Galerkin start
+// Iterates of the power iteration span a Krylov space of A: x_{j+1} is
+// A^-1 x_j scaled, so A x_{j+1} is x_j scaled.  At outer step k the ring
+// holds x_j and A x_j for j = k, ..., k-v+1 (v = min(k, recycle); A x_j
+// came from the end-of-step product A z at no extra cost).  The start
+// vector z0 is the Galerkin solution of A z = x on their span:
+//   (V^T A V) y = V^T x,   z0 = V y,   A z0 = W y   (W = A V),
+// which for v = 1 is CG's first iterate from z = 0 and for larger v
+// removes the slowly converging eigen-directions the previous solves met.
+// The v x v system is solved by every CTA identically (Cholesky of -V^T A V,
+// SPD for negative definite A; a direction whose pivot falls below tau
+// times the first is left out, tau raised until the coefficients stay
+// small so that W y is accurate to ~1e-14 of x).
+
+// What the Galerkin start reads and writes (passed by value to the outlined
+// function, so the kernel's argument block is not copied to local memory).
+struct GalerkinArgs {
+    const double *hx, *hw;
+    size_t hstride;
+    int recycle, step;
+    const double *x;
+    double *z, *q;
+    double *part;
+    int gpad;
+    GridBarrier gb;
+};
+
+__device__ __forceinline__ GalerkinArgs galerkin_args(const OuterArgs &A)
+{
+    GalerkinArgs G;
+    G.hx = A.hx;
+    G.hw = A.hw;
+    G.hstride = A.hstride;
+    G.recycle = A.recycle;
+    G.step = A.step;
+    G.x = A.x;
+    G.z = A.z;
+    G.q = A.q;
+    G.part = A.part;
+    G.gpad = A.gpad;
+    G.gb = A.gb;
+    return G;
+}
+
+// Per-CTA sums of nq per-thread values into slots [slot0, slot0 + nq).
+__device__ __forceinline__ void put_partials_multi(const GalerkinArgs &A, int slot0,
+                                                   const double *vals, int nq)
+{
+    __shared__ double red[32][kGramValues];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+    for (int q = 0; q < kGramValues; q++) {
+        if (q < nq) {
+            const double v = warp_sum(vals[q]);
+            if (l == 0) red[w][q] = v;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < nq) {
+        double t = 0.0;
+        for (int i = 0; i < int(blockDim.x >> 5); i++) t += red[i][threadIdx.x];
+        A.part[size_t(slot0 + threadIdx.x) * A.gpad + blockIdx.x] = t;
+    }
+    __syncthreads();
+}
+
+// Totals of slots [slot0, slot0 + nq) into out[] (shared), the same in
+// every CTA: slot q summed by warp q % nwarps in a fixed order.
+__device__ __forceinline__ void get_totals_multi(const GalerkinArgs &A, int slot0, int nq, double *out)
+{
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int q = w; q < nq; q += nw) {
+        double t = 0.0;
+        for (int i = l; i < int(gridDim.x); i += 32) t += __ldcg(A.part + size_t(slot0 + q) * A.gpad + i);
+        t = warp_sum(t);
+        if (l == 0) out[q] = t;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ int gram_index(int a, int b)  // a <= b < v, packed by b
+{
+    return b * (b + 1) / 2 + a;
+}
+
+// Coefficients y of the Galerkin start from the Gram totals g[] (see
+// galerkin_start); one thread.  Returns the number of directions kept.
+static __device__ __noinline__ int galerkin_solve(const double *g, int v, double *y)
+{
+    double N[kMaxRecycle][kMaxRecycle], c[kMaxRecycle];
+    for (int b = 0; b < v; b++) {
+        for (int a = 0; a <= b; a++) N[a][b] = N[b][a] = -g[gram_index(a, b)];
+        c[b] = g[kMaxRecycle * (kMaxRecycle + 1) / 2 + b];
+    }
+    if (!(N[0][0] > 0.0)) {
+        for (int a = 0; a < v; a++) y[a] = 0.0;
+        return 0;
+    }
+    const double taus[4] = {1e-12, 1e-10, 1e-8, 1e-6};
+    for (int t = 0; t < 5; t++) {
+        // t == 4: the first direction alone
+        const double tau = t < 4 ? taus[t] * N[0][0] : 1e300;
+        double L[kMaxRecycle][kMaxRecycle], u[kMaxRecycle];
+        bool keep[kMaxRecycle];
+        int kept = 0;
+        for (int i = 0; i < v; i++) {
+            double d = N[i][i];
+            for (int k = 0; k < i; k++)
+                if (keep[k]) d -= L[i][k] * L[i][k];
+            keep[i] = (i == 0) || d > tau;
+            if (!keep[i]) continue;
+            kept++;
+            L[i][i] = sqrt(d);
+            for (int j = i + 1; j < v; j++) {
+                double e = N[j][i];
+                for (int k = 0; k < i; k++)
+                    if (keep[k]) e -= L[j][k] * L[i][k];
+                L[j][i] = e / L[i][i];
+            }
+        }
+        // N y = -c on the kept directions
+        for (int i = 0; i < v; i++) {
+            if (!keep[i]) { u[i] = 0.0; continue; }
+            double e = -c[i];
+            for (int k = 0; k < i; k++)
+                if (keep[k]) e -= L[i][k] * u[k];
+            u[i] = e / L[i][i];
+        }
+        for (int i = v - 1; i >= 0; i--) {
+            if (!keep[i]) { y[i] = 0.0; continue; }
+            double e = u[i];
+            for (int j = i + 1; j < v; j++)
+                if (keep[j]) e -= L[j][i] * y[j];
+            y[i] = e / L[i][i];
+        }
+        // growth of the combination in the A-norm: sum |y_a| ||x_a||_A
+        // against ||z0||_A; accept when the cancellation is mild
+        double num = 0.0, zA = 0.0;
+        for (int a = 0; a < v; a++) {
+            num += fabs(y[a]) * sqrt(N[a][a]);
+            for (int b = 0; b < v; b++) zA += y[a] * N[a][b] * y[b];
+        }
+        if (t == 4 || (zA > 0.0 && num <= 100.0 * sqrt(zA) && isfinite(num))) return kept;
+    }
+    return 1;
+}
+
+// z0 and A z0 of the Galerkin start into A.z and A.q (own rows; entry n of
+// the last CTA zero), and x.x into *xx (all CTAs).  v >= 1.  Returns false
+// when a grid barrier failed.
+static __device__ __noinline__ bool galerkin_start(const GalerkinArgs A, int row0, int row1, int vend,
+                                                  int v, double *xx)
+{
+    __shared__ double g_sh[kGramValues];
+    __shared__ double y_sh[kMaxRecycle];
+    const int m = A.recycle;
+    size_t off[kMaxRecycle];
+#pragma unroll
+    for (int a = 0; a < kMaxRecycle; a++) off[a] = size_t(((A.step - a) % m + m) % m) * A.hstride;
+    const int npairs = v * (v + 1) / 2;
+    double vals[kGramValues];
+#pragma unroll
+    for (int q = 0; q < kGramValues; q++) vals[q] = 0.0;
+    for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) {
+        double xa[kMaxRecycle], wa[kMaxRecycle];
+#pragma unroll
+        for (int a = 0; a < kMaxRecycle; a++) {
+            if (a < v) {
+                xa[a] = A.hx[off[a] + j];
+                wa[a] = A.hw[off[a] + j];
+            }
+        }
+        const double xv = A.x[j];
+#pragma unroll
+        for (int b = 0; b < kMaxRecycle; b++) {
+#pragma unroll
+            for (int a = 0; a <= b; a++)
+                if (b < v) vals[gram_index(a, b)] = fma(xa[a], wa[b], vals[gram_index(a, b)]);
+            if (b < v) vals[kMaxRecycle * (kMaxRecycle + 1) / 2 + b] =
+                fma(xa[b], xv, vals[kMaxRecycle * (kMaxRecycle + 1) / 2 + b]);
+        }
+    }
+    // pack: Gram pairs first, then the right-hand sides
+    double packed[kGramValues];
+#pragma unroll
+    for (int q = 0; q < kGramValues; q++) packed[q] = 0.0;
+#pragma unroll
+    for (int q = 0; q < kMaxRecycle * (kMaxRecycle + 1) / 2; q++)
+        if (q < npairs) packed[q] = vals[q];
+#pragma unroll
+    for (int b = 0; b < kMaxRecycle; b++)
+        if (b < v) packed[npairs + b] = vals[kMaxRecycle * (kMaxRecycle + 1) / 2 + b];
+    put_partials_multi(A, kSlotGram, packed, npairs + v);
+    if (!grid_barrier(A.gb)) return false;
+    get_totals_multi(A, kSlotGram, npairs + v, g_sh);
+    if (threadIdx.x == 0) {
+        double g[kGramValues];
+        for (int q = 0; q < kGramValues; q++) g[q] = 0.0;
+        for (int q = 0; q < npairs; q++) g[q] = g_sh[q];
+        for (int b = 0; b < v; b++) g[kMaxRecycle * (kMaxRecycle + 1) / 2 + b] = g_sh[npairs + b];
+        double y[kMaxRecycle];
+        galerkin_solve(g, v, y);
+        for (int a = 0; a < kMaxRecycle; a++) y_sh[a] = a < v ? y[a] : 0.0;
+    }
+    __syncthreads();
+    // x_k is the newest ring entry: x.x = its right-hand-side entry
+    *xx = g_sh[npairs];
+    for (int j = row0 + threadIdx.x; j < vend; j += blockDim.x) {
+        double z0 = 0.0, az = 0.0;
+        if (j < row1) {
+#pragma unroll
+            for (int a = 0; a < kMaxRecycle; a++) {
+                if (a < v) {
+                    z0 = fma(y_sh[a], A.hx[off[a] + j], z0);
+                    az = fma(y_sh[a], A.hw[off[a] + j], az);
+                }
+            }
+        }
+        A.z[j] = z0;
+        A.q[j] = az;
+    }
+    __syncthreads();
+    return true;
+}
+
+// Iterates available for the Galerkin start of this outer step (0: start
+// from z = 0).
+__device__ __forceinline__ int recycle_depth(const OuterArgs &A)
+{
+    if (A.fixed || A.recycle <= 0 || !A.finish) return 0;
+    return A.step < A.recycle ? A.step : A.recycle;
 }
 
 // FP64 CG (reference semantics when A.fixed).
@@ -182,10 +437,26 @@ __device__ __forceinline__ void outer_step_body(const OuterArgs &A)
     // the reference initialises n+1 vector entries (cg.cu:670-675); the
     // last CTA also owns entry n, which never enters a dot product
     const int vend = (blockIdx.x == gridDim.x - 1) ? row1 + 1 : row1;
-    start_solve<Spmv>(A, row0, vend, false, scratch);
+    const int v = recycle_depth(A);
+    double xx = 0.0;
+    if (v > 0) {
+        // tolerance mode: Galerkin start, r0 = x - A z0, p0 = r0
+        if (!galerkin_start(galerkin_args(A), row0, row1, vend, v, &xx)) return;
+        double acc = 0.0;
+        for (int j = row0 + threadIdx.x; j < vend; j += blockDim.x) {
+            const double rv = A.x[j] - A.q[j];
+            A.r[j] = rv;
+            A.p[j] = rv;
+            if (j < A.n) acc = fma(rv, rv, acc);
+        }
+        put_partial(A, kSlotRho, acc, scratch);
+    } else {
+        start_solve<Spmv>(A, row0, vend, false, scratch);
+    }
     CGB_BARRIER_OR_RETURN(A);
     double rho = get_total(A, kSlotRho, &bcast[0]);
-    const double stop2 = A.tol * A.tol * rho;  // rho = x.x here
+    if (v == 0) xx = rho;                     // rho = x.x when z0 = 0
+    const double stop2 = A.tol * A.tol * xx;
 
     // ---- CG iterations (cg.cu:678-768)
     int it = 0;
@@ -239,10 +510,27 @@ __device__ __forceinline__ void outer_step_mixed_body(const OuterArgs &A)
     sp.setup(A.M, row0, row1);
     bool ok = true;
     const int vend = (blockIdx.x == gridDim.x - 1) ? row1 + 1 : row1;
-    start_solve<Spmv>(A, row0, vend, true, scratch);
+    const int v = recycle_depth(A);
+    double xx = 0.0;
+    if (v > 0) {
+        // Galerkin start: r0 = x - A z0 (a true residual), p0 = r0
+        if (!galerkin_start(galerkin_args(A), row0, row1, vend, v, &xx)) return;
+        double acc = 0.0;
+        for (int j = row0 + threadIdx.x; j < vend; j += blockDim.x) {
+            const double rv = A.x[j] - A.q[j];
+            A.r[j] = rv;
+            A.p[j] = rv;
+            A.p32[j] = float(rv);
+            if (j < A.n) acc = fma(rv, rv, acc);
+        }
+        put_partial(A, kSlotRho, acc, scratch);
+    } else {
+        start_solve<Spmv>(A, row0, vend, true, scratch);
+    }
     CGB_BARRIER_OR_RETURN(A);
     double rho = get_total(A, kSlotRho, &bcast[0]);
-    const double stop2 = A.tol * A.tol * rho;  // rho = x.x here
+    if (v == 0) xx = rho;                      // rho = x.x when z0 = 0
+    const double stop2 = A.tol * A.tol * xx;
     double rho_cycle = rho;                    // rho at the last true residual
 
     int it = 0, since = 0, refreshes = 0;
@@ -320,23 +608,15 @@ __device__ __forceinline__ void outer_step_mixed_body(const OuterArgs &A)
 // with restart).  When the preconditioned iteration stalls -- no halving of
 // |r|^2 in four steps, or a non-positive p.A'p or r.y -- the outer step
 // falls back to unpreconditioned CG (counted in the trace).
-// out = F v (FP32 products, FP64 row results) for the CTA's rows: the
-// sliced policy walks F's own sliced copy (same row split and column
-// blocks as A's); the row policy reads F's CSR with LPRG lanes per row.
-template <class Spmv, int LPRG>
-__device__ __forceinline__ bool factor_product(Spmv &sp, const OuterArgs &A, const MatrixView &F,
-                                               const float *v, double *out, int row0, int row1)
-{
-    if constexpr (std::is_same<Spmv, SlicedSpmv>::value) {
-        bool ok = true;
-        (void)sp.template apply<float>(F, v, out, nullptr, A.n, A.gb.limit_ns, A.gb.status, ok);
-        return ok;
-    } else {
-        spmv_rows<LPRG, float>(F, v, out, row0, row1, nullptr);
-        return true;
-    }
-}
-
+// y = M r = F^T (F r) and the partial of r.y, then its total in rho_out.
+//  - sliced policy: F and F^T have their own sliced copies with interleaved
+//    row ownership (CTA c computes rows c, c+G, ...).  F is lower
+//    triangular, so contiguous row ranges would leave the first CTAs almost
+//    idle and the last ones with whole rows (and the reverse for F^T);
+//    interleaving gives every CTA a fair sample of row lengths.  The F^T
+//    product fuses the r.y partial over the rows it computes.
+//  - row policy: CSR rows of F and F^T with LPRG lanes per row over the
+//    CTA's own rows.
 template <class Spmv, int LPRG>
 __device__ __forceinline__ bool apply_prec(Spmv &sp, const OuterArgs &A, int row0, int row1,
                                            bool use, double &rho_out, double *scratch,
@@ -345,13 +625,29 @@ __device__ __forceinline__ bool apply_prec(Spmv &sp, const OuterArgs &A, int row
     // r32 of every row is complete (caller passed a barrier)
     double acc = 0.0;
     if (use) {
-        if (!factor_product<Spmv, LPRG>(sp, A, A.F, A.r32, A.q, row0, row1)) return false;  // t = F r
-        __syncthreads();
-        for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) A.p32[j] = float(A.q[j]);
-        if (!grid_barrier(A.gb)) return false;
-        if (!factor_product<Spmv, LPRG>(sp, A, A.FT, A.p32, A.y, row0, row1)) return false;  // y = F^T t
-        __syncthreads();
-        for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) acc = fma(A.r[j], A.y[j], acc);
+        if constexpr (Spmv::kSliced) {
+            bool ok = true;
+            (void)sp.template apply<float>(A.F, A.r32, A.q, nullptr, A.n, A.gb.limit_ns,
+                                           A.gb.status, ok);  // t = F r (interleaved rows)
+            if (!ok) return false;
+            const int G = gridDim.x, nr = interleaved_rows(A.n, blockIdx.x, G);
+            for (int i = threadIdx.x; i < nr; i += blockDim.x) {
+                const int j = blockIdx.x + G * i;
+                A.p32[j] = float(A.q[j]);
+            }
+            if (!grid_barrier(A.gb)) return false;
+            acc = sp.template apply<float>(A.FT, A.p32, A.y, A.r, A.n, A.gb.limit_ns, A.gb.status,
+                                           ok);  // y = F^T t, r.y
+            if (!ok) return false;
+        } else {
+            spmv_rows<LPRG, float>(A.F, A.r32, A.q, row0, row1, nullptr);  // t = F r
+            __syncthreads();
+            for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) A.p32[j] = float(A.q[j]);
+            if (!grid_barrier(A.gb)) return false;
+            spmv_rows<LPRG, float>(A.FT, A.p32, A.y, row0, row1, nullptr);  // y = F^T t
+            __syncthreads();
+            for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) acc = fma(A.r[j], A.y[j], acc);
+        }
     } else {
         for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) {
             A.y[j] = A.r[j];
@@ -375,20 +671,34 @@ __device__ __forceinline__ void outer_step_pcg_body(const OuterArgs &A)
     sp.setup(A.M, row0, row1);
     bool ok = true;
     const int vend = (blockIdx.x == gridDim.x - 1) ? row1 + 1 : row1;
-    // z0 = 0, r' = b' = -x
+    const int v = recycle_depth(A);
+    double xx = 0.0;
     double acc = 0.0;
-    for (int j = row0 + threadIdx.x; j < vend; j += blockDim.x) {
-        const double xv = A.x[j];
-        A.q[j] = 0.0;
-        A.z[j] = 0.0;
-        A.r[j] = -xv;
-        A.r32[j] = float(-xv);
-        if (j < A.n) acc = fma(xv, xv, acc);
+    if (v > 0) {
+        // Galerkin start: r' = b' - A' z0 = A z0 - x
+        if (!galerkin_start(galerkin_args(A), row0, row1, vend, v, &xx)) return;
+        for (int j = row0 + threadIdx.x; j < vend; j += blockDim.x) {
+            const double rv = A.q[j] - A.x[j];
+            A.r[j] = rv;
+            A.r32[j] = float(rv);
+            if (j < A.n) acc = fma(rv, rv, acc);
+        }
+    } else {
+        // z0 = 0, r' = b' = -x
+        for (int j = row0 + threadIdx.x; j < vend; j += blockDim.x) {
+            const double xv = A.x[j];
+            A.q[j] = 0.0;
+            A.z[j] = 0.0;
+            A.r[j] = -xv;
+            A.r32[j] = float(-xv);
+            if (j < A.n) acc = fma(xv, xv, acc);
+        }
     }
     put_partial(A, kSlotRho, acc, scratch);
     CGB_BARRIER_OR_RETURN(A);
     double rr = get_total(A, kSlotRho, &bcast[0]);
-    const double stop2 = A.tol * A.tol * rr;
+    if (v == 0) xx = rr;
+    const double stop2 = A.tol * A.tol * xx;
     double rr_cycle = rr;
     double hist[4] = {rr, rr, rr, rr};  // |r|^2 of the last four steps
     bool use_prec = true;
@@ -487,8 +797,16 @@ __device__ __forceinline__ void outer_step_pcg_body(const OuterArgs &A)
         CGB_BARRIER_OR_RETURN(A);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) A.trace[A.step].spare[0] = double(fallbacks);
-    end_solve(sp, A, row0, row1, it, rr, refreshes, fresh, scratch, bcast);
+    end_solve(sp, A, row0, row1, it, rr, refreshes, fresh, scratch, bcast, -1.0);
 }
+
+// Block shapes of the sliced kernels (one CTA per SM).  The mixed and
+// preconditioned bodies hold more live state than the FP64 one; with fewer
+// threads each thread may use more registers (65536 / block), so their SpMV
+// loops run without spilling.
+constexpr int kSlicedBlock = 1024;
+constexpr int kSlicedMixedBlock = 768;
+constexpr int kSlicedPcgBlock = 512;
 
 template <int LPR>
 __global__ void __launch_bounds__(512, 2) outer_step_fp64(OuterArgs A)
@@ -496,7 +814,7 @@ __global__ void __launch_bounds__(512, 2) outer_step_fp64(OuterArgs A)
     outer_step_body<RowSpmv<LPR>>(A);
 }
 
-static __global__ void __launch_bounds__(1024, 1) outer_step_fp64_sliced(OuterArgs A)
+static __global__ void __launch_bounds__(kSlicedBlock, 1) outer_step_fp64_sliced(OuterArgs A)
 {
     outer_step_body<SlicedSpmv>(A);
 }
@@ -507,9 +825,9 @@ __global__ void __launch_bounds__(512, 2) outer_step_mixed(OuterArgs A)
     outer_step_mixed_body<RowSpmv<LPR>>(A);
 }
 
-static __global__ void __launch_bounds__(1024, 1) outer_step_mixed_sliced(OuterArgs A)
+static __global__ void __launch_bounds__(kSlicedMixedBlock, 1) outer_step_mixed_sliced(OuterArgs A)
 {
-    outer_step_mixed_body<SlicedSpmv>(A);
+    outer_step_mixed_body<SlicedSpmv768>(A);
 }
 
 // lanes per row of the preconditioner products (F has about half of A's
@@ -522,9 +840,9 @@ __global__ void __launch_bounds__(512, 2) outer_step_pcg(OuterArgs A)
     outer_step_pcg_body<RowSpmv<LPR>, kLanesF>(A);
 }
 
-static __global__ void __launch_bounds__(1024, 1) outer_step_pcg_sliced(OuterArgs A)
+static __global__ void __launch_bounds__(kSlicedPcgBlock, 1) outer_step_pcg_sliced(OuterArgs A)
 {
-    outer_step_pcg_body<SlicedSpmv, kLanesF>(A);
+    outer_step_pcg_body<SlicedSpmv512, kLanesF>(A);
 }
 
 // Standalone q = A p with the p.q reduction fused (the work of reference
@@ -576,7 +894,7 @@ __global__ void __launch_bounds__(512, 2) spmv_dot_row(SpmvArgs S)
     spmv_dot_body<RowSpmv<LPR>>(S);
 }
 
-static __global__ void __launch_bounds__(1024, 1) spmv_dot_sliced(SpmvArgs S)
+static __global__ void __launch_bounds__(kSlicedBlock, 1) spmv_dot_sliced(SpmvArgs S)
 {
     spmv_dot_body<SlicedSpmv>(S);
 }
@@ -631,21 +949,31 @@ static __global__ void build_segments(const int *__restrict__ rowstr,
 // rounded up to even.
 // Placement order within a bin does not matter: each row is summed by one
 // lane in its CSR order wherever it lands.
+// Global row of local row i of CTA c: row_split[c] + i, or (interleaved,
+// grid G) c + G i.
+__device__ __forceinline__ int chunk_row(const int *row_split, int interleave_grid, int c, int i)
+{
+    return interleave_grid ? c + interleave_grid * i : row_split[c] + i;
+}
+
 static __global__ void slice_sort_rows(const int *__restrict__ seg, int seg_stride, int nblk,
-                                       const int *__restrict__ row_split,
-                                       const int *__restrict__ chunk_slice, unsigned short *srow,
-                                       int *slice_width)
+                                       const int *__restrict__ row_split, int interleave_grid,
+                                       int n, const int *__restrict__ chunk_slice,
+                                       unsigned short *srow, int *slice_width)
 {
     __shared__ int hist[256];
     const int c = blockIdx.x / nblk, b = blockIdx.x % nblk;
-    const int r0 = row_split[c], r1 = row_split[c + 1], nrows = r1 - r0;
+    const int nrows = interleave_grid ? interleaved_rows(n, c, interleave_grid)
+                                      : row_split[c + 1] - row_split[c];
     const int s0 = chunk_slice[blockIdx.x], ns = chunk_slice[blockIdx.x + 1] - s0;
-    const int *lo = seg + size_t(b) * seg_stride + r0;
-    const int *hi = seg + size_t(b + 1) * seg_stride + r0;
+    const int *lo = seg + size_t(b) * seg_stride;
+    const int *hi = seg + size_t(b + 1) * seg_stride;
+#define SEG_LEN(i) (hi[chunk_row(row_split, interleave_grid, c, (i))] - \
+                    lo[chunk_row(row_split, interleave_grid, c, (i))])
     for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
     __syncthreads();
     for (int i = threadIdx.x; i < nrows; i += blockDim.x)
-        atomicAdd(&hist[255 - min(hi[i] - lo[i], 255)], 1);
+        atomicAdd(&hist[255 - min(SEG_LEN(i), 255)], 1);
     __syncthreads();
     if (threadIdx.x == 0) {
         int run = 0;
@@ -658,7 +986,7 @@ static __global__ void slice_sort_rows(const int *__restrict__ seg, int seg_stri
     __syncthreads();
     unsigned short *dst = srow + size_t(s0) * 32;
     for (int i = threadIdx.x; i < nrows; i += blockDim.x) {
-        const int pos = atomicAdd(&hist[255 - min(hi[i] - lo[i], 255)], 1);
+        const int pos = atomicAdd(&hist[255 - min(SEG_LEN(i), 255)], 1);
         dst[pos] = (unsigned short)i;
     }
     for (int i = nrows + threadIdx.x; i < ns * 32; i += blockDim.x) dst[i] = 0xffffu;
@@ -667,10 +995,11 @@ static __global__ void slice_sort_rows(const int *__restrict__ seg, int seg_stri
         int w = 0;
         for (int l = 0; l < 32; l++) {
             const unsigned short row = dst[t * 32 + l];
-            if (row != 0xffffu) w = max(w, hi[row] - lo[row]);
+            if (row != 0xffffu) w = max(w, SEG_LEN(row));
         }
         slice_width[s0 + t] = (w + 1) & ~1;  // whole step pairs
     }
+#undef SEG_LEN
 }
 
 // Step 2 -- one CTA: slice_off[s] = 32 * sum_{s' < s} width[s'];
@@ -708,7 +1037,8 @@ static __global__ void slice_offsets(const int *__restrict__ width, int total, u
 // 16-bit local columns; padding steps get value 0, column 0.
 template <typename ST>
 __global__ void slice_fill(const int *__restrict__ seg, int seg_stride, int nblk, int width,
-                           const int *__restrict__ row_split, const int *__restrict__ chunk_slice,
+                           const int *__restrict__ row_split, int interleave_grid,
+                           const int *__restrict__ chunk_slice,
                            int nchunks, const int *__restrict__ colidx, const ST *__restrict__ a,
                            const unsigned short *__restrict__ srow,
                            const int *__restrict__ slice_width,
@@ -728,7 +1058,7 @@ __global__ void slice_fill(const int *__restrict__ seg, int seg_stride, int nblk
         const unsigned short row = srow[size_t(s) * 32 + lane];
         int e0 = 0, e1 = 0;
         if (row != 0xffffu) {
-            const int j = row_split[c] + row;
+            const int j = chunk_row(row_split, interleave_grid, c, row);
             e0 = seg[size_t(b) * seg_stride + j];
             e1 = seg[size_t(b + 1) * seg_stride + j];
         }

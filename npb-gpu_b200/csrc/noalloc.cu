@@ -38,7 +38,8 @@ constexpr int kNoallocMaxGrid = 1024;      // CTAs of the cooperative launch
 constexpr size_t kLine = 256;
 constexpr size_t kHeaderBytes = 4 * kLine;  // barrier count, generation, status, trace
 constexpr size_t kSplitBytes = ((kNoallocMaxGrid + 1) * sizeof(int) + kLine - 1) / kLine * kLine;
-constexpr size_t kPartBytes = size_t(kSlotCount) * kNoallocMaxGrid * sizeof(double);
+// the fixed-count FP64 kernel uses the slots below kSlotGram only
+constexpr size_t kPartBytes = size_t(kSlotGram) * kNoallocMaxGrid * sizeof(double);
 constexpr size_t kVecDoubles = size_t(kNoallocMaxN) + 64;
 constexpr size_t kScratchBytes = kHeaderBytes + kSplitBytes + kPartBytes + 3 * kVecDoubles * sizeof(double);
 

@@ -72,7 +72,9 @@ struct Plan {
     OuterKernel mixed = nullptr;
     OuterKernel pcg = nullptr;
     SpmvKernel spmv = nullptr;
-    int block = 512;
+    int block = 512;        // FP64 outer step and standalone SpMV
+    int block_mixed = 512;  // mixed outer step
+    int block_pcg = 512;    // preconditioned outer step
     int grid = 0;
     size_t smem = 0;
 };
@@ -178,6 +180,7 @@ struct cgb_session {
     float *d_p32 = nullptr;
     float *d_r32 = nullptr;
     double *d_y = nullptr;
+    double *d_hx = nullptr, *d_hw = nullptr;  // Galerkin-start ring: kMaxRecycle vectors each
     size_t vstride = 0;
     // preconditioner factor F (lower, CSR) and F^T, FP32 values
     int *d_f_ptr = nullptr, *d_f_col = nullptr, *d_ft_ptr = nullptr, *d_ft_col = nullptr;
@@ -206,8 +209,6 @@ struct cgb_session {
     cgb::SliceSet sf, sft;         // F and F^T: FP32 values
     int layout_gen = 0;            // bumped by every build of A's slices
     int prec_gen = -1;             // layout_gen sf / sft were built for
-    int sliced_grid_pending = 0;   // grid of the layout being built
-    int slice_total = 0;           // slices per matrix (all chunks)
 
     Plan plan;
     std::vector<int> h_rowstr_copy;
@@ -248,6 +249,8 @@ void free_set(SliceSet &t)
     dev_free(t.sval);
     dev_free(t.sval32);
     dev_free(t.scol);
+    dev_free(t.chunk_slice);
+    t.interleaved = 0;
     t.entries = 0;
 }
 
@@ -280,6 +283,8 @@ void release(cgb_session *s)
     dev_free(s->d_p32);
     dev_free(s->d_r32);
     dev_free(s->d_y);
+    dev_free(s->d_hx);
+    dev_free(s->d_hw);
     dev_free(s->d_f_ptr);
     dev_free(s->d_f_col);
     dev_free(s->d_f_val);
@@ -300,7 +305,8 @@ void release(cgb_session *s)
     delete s;
 }
 
-// Points the sliced members of M at slice set t (A's row split and blocks).
+// Points the sliced members of M at slice set t (A's column blocks; A's
+// row split unless t is interleaved).
 void set_slices(cgb_session *s, const SliceSet &t, MatrixView *M)
 {
     M->sval = t.sval;
@@ -309,10 +315,11 @@ void set_slices(cgb_session *s, const SliceSet &t, MatrixView *M)
     M->srow = t.srow;
     M->slice_off = t.off;
     M->slice_width = t.width;
-    M->chunk_slice = s->d_chunk_slice;
+    M->chunk_slice = t.chunk_slice ? t.chunk_slice : s->d_chunk_slice;
     M->nblk = s->nblk;
     M->width = kSliceWidth;
     M->max_rows = s->sliced_max_rows;
+    M->interleaved = t.interleaved;
 }
 
 MatrixView matrix_view(cgb_session *s)
@@ -358,14 +365,19 @@ OuterArgs outer_args(cgb_session *s)
     A.gb.limit_ns = s->opts.wait_limit_ns > 0 ? s->opts.wait_limit_ns : kDefaultWaitNs;
     A.refresh_every = 10;
     A.trace = s->d_trace;
+    A.hx = s->d_hx;
+    A.hw = s->d_hw;
+    A.hstride = s->vstride;
+    A.recycle = 0;
     return A;
 }
 
 cudaError_t launch_outer(cgb_session *s, OuterKernel k, const OuterArgs &A)
 {
+    const Plan &P = s->plan;
     cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3(s->plan.grid);
-    cfg.blockDim = dim3(s->plan.block);
+    cfg.gridDim = dim3(P.grid);
+    cfg.blockDim = dim3(k == P.mixed ? P.block_mixed : k == P.pcg ? P.block_pcg : P.block);
     cfg.dynamicSmemBytes = s->plan.smem;
     cfg.stream = s->stream;
     cudaLaunchAttribute attr[1];
@@ -402,20 +414,40 @@ int build_segments_table(cgb_session *s)
     return CGB_OK;
 }
 
-// Steps 1-3 of a sliced copy of one matrix over the current row split
-// (d_split and d_chunk_slice on the device, `total` slices): row order per
-// slice, slice offsets, then values (FP64 and/or FP32) and local columns.
-// `seg` is the matrix's segment table.
-template <typename ST>
-int fill_set(cgb_session *s, const int *seg, const int *d_colidx, const ST *vals, int total,
-             bool want64, bool want32, SliceSet *t)
+// Chunk table of a sliced copy: first slice of each (CTA c, block b), 32
+// rows a slice; rows per CTA from `rows_of(c)`.  Returns the slice count.
+template <typename RowsOf>
+int chunk_table(int grid, int nblk, RowsOf rows_of, std::vector<int> &chunk_slice)
 {
-    const int nchunks = s->sliced_grid_pending * s->nblk;
+    chunk_slice.assign(size_t(grid) * nblk + 1, 0);
+    int total = 0;
+    for (int c = 0; c < grid; c++) {
+        const int rows = rows_of(c);
+        for (int b = 0; b < nblk; b++) {
+            chunk_slice[size_t(c) * nblk + b] = total;
+            total += (rows + 31) / 32;
+        }
+    }
+    chunk_slice[size_t(grid) * nblk] = total;
+    return total;
+}
+
+// Steps 1-3 of a sliced copy of one matrix over `grid` CTAs: row order per
+// slice, slice offsets, then values (FP64 and/or FP32) and local columns.
+// `seg` is the matrix's segment table; rows are the CTAs' ranges of d_split
+// or, with `interleave`, every grid-th row.  t->chunk_slice must be set.
+template <typename ST>
+int fill_set(cgb_session *s, int grid, bool interleave, const int *seg, const int *d_colidx,
+             const ST *vals, int total, bool want64, bool want32, SliceSet *t)
+{
+    const int nchunks = grid * s->nblk;
+    const int ig = interleave ? grid : 0;
+    t->interleaved = interleave ? 1 : 0;
     if (dev_alloc(&t->srow, size_t(total) * 32) || dev_alloc(&t->width, size_t(total)) ||
         dev_alloc(&t->off, size_t(total) + 1))
         return set_error(CGB_ERR_NOMEM, "sliced layout: metadata allocation failed");
-    slice_sort_rows<<<nchunks, 256, 0, s->stream>>>(seg, s->seg_stride, s->nblk, s->d_split,
-                                                   s->d_chunk_slice, t->srow, t->width);
+    slice_sort_rows<<<nchunks, 256, 0, s->stream>>>(seg, s->seg_stride, s->nblk, s->d_split, ig,
+                                                   s->n, t->chunk_slice, t->srow, t->width);
     CUDA_TRY(cudaGetLastError());
     slice_offsets<<<1, 1024, 0, s->stream>>>(t->width, total, t->off);
     CUDA_TRY(cudaGetLastError());
@@ -429,8 +461,8 @@ int fill_set(cgb_session *s, const int *seg, const int *d_colidx, const ST *vals
         (want32 && dev_alloc(&t->sval32, size_t(entries) + kPad)))
         return set_error(CGB_ERR_NOMEM, "sliced layout: %u entries do not fit", entries);
     slice_fill<ST><<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
-        seg, s->seg_stride, s->nblk, kSliceWidth, s->d_split, s->d_chunk_slice, nchunks, d_colidx,
-        vals, t->srow, t->width, t->off, total, t->sval, t->sval32, t->scol);
+        seg, s->seg_stride, s->nblk, kSliceWidth, s->d_split, ig, t->chunk_slice, nchunks,
+        d_colidx, vals, t->srow, t->width, t->off, total, t->sval, t->sval32, t->scol);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     return CGB_OK;
@@ -442,18 +474,13 @@ int build_sliced(cgb_session *s, int grid)
     free_sliced(s);
     std::vector<int> split;
     make_split(s->n, s->h_rowstr_copy.data(), grid, split);
-    int max_rows = 0;
-    std::vector<int> chunk_slice(size_t(grid) * s->nblk + 1, 0);
-    int total = 0;
-    for (int c = 0; c < grid; c++) {
-        const int rows = split[c + 1] - split[c];
-        max_rows = std::max(max_rows, rows);
-        for (int b = 0; b < s->nblk; b++) {
-            chunk_slice[size_t(c) * s->nblk + b] = total;
-            total += (rows + 31) / 32;
-        }
-    }
-    chunk_slice[size_t(grid) * s->nblk] = total;
+    std::vector<int> chunk_slice;
+    const int total = chunk_table(grid, s->nblk, [&](int c) { return split[c + 1] - split[c]; },
+                                  chunk_slice);
+    // accumulators: the largest row range, or the interleaved share of the
+    // preconditioner's copies
+    int max_rows = interleaved_rows(s->n, 0, grid);
+    for (int c = 0; c < grid; c++) max_rows = std::max(max_rows, split[c + 1] - split[c]);
     s->sliced_max_rows = (max_rows + 31) & ~31;
     if (s->sliced_max_rows >= 0xffff || sliced_smem_bytes(s->sliced_max_rows) > kSmemLimit)
         return set_error(CGB_ERR_STATE, "sliced layout: %d rows per CTA exceed shared memory", max_rows);
@@ -462,25 +489,33 @@ int build_sliced(cgb_session *s, int grid)
     CUDA_TRY(cudaMemcpy(s->d_split, split.data(), sizeof(int) * (grid + 1), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(s->d_chunk_slice, chunk_slice.data(), sizeof(int) * chunk_slice.size(),
                         cudaMemcpyHostToDevice));
-    s->sliced_grid_pending = grid;
-    s->slice_total = total;
-    const int st = fill_set<double>(s, s->d_seg, s->d_colidx, s->d_a, total, true,
-                                    s->opts.keep_fp32_copy != 0, &s->sa);
+    s->sa.chunk_slice = nullptr;  // the session's table
+    const int st = [&] {
+        SliceSet &t = s->sa;
+        t.chunk_slice = s->d_chunk_slice;
+        const int r = fill_set<double>(s, grid, false, s->d_seg, s->d_colidx, s->d_a, total, true,
+                                       s->opts.keep_fp32_copy != 0, &t);
+        t.chunk_slice = nullptr;
+        return r;
+    }();
     if (st) return st;
     s->sliced_grid = grid;
     s->layout_gen++;
     return CGB_OK;
 }
 
-// Sliced copies of F and F^T (FP32) over A's row split, built on first use
-// by the preconditioned solver after each change of F or of A's layout.
-// F^T rows ascend by construction; F rows are sorted by the setter.
+// Sliced copies of F and F^T (FP32) with interleaved row ownership, built on
+// first use by the preconditioned solver after each change of F or of A's
+// layout.  F^T rows ascend by construction; F rows are sorted by the setter.
 int ensure_prec_slices(cgb_session *s)
 {
     if (s->plan.kind != kKindSliced || !s->has_prec) return CGB_OK;
     if (s->prec_gen == s->layout_gen) return CGB_OK;
     free_prec_slices(s);
-    const int n = s->n;
+    const int n = s->n, grid = s->sliced_grid;
+    std::vector<int> chunk_slice;
+    const int total = chunk_table(grid, s->nblk, [&](int c) { return interleaved_rows(n, c, grid); },
+                                  chunk_slice);
     const size_t count = size_t(s->nblk + 1) * s->seg_stride;
     int *seg = nullptr;
     if (dev_alloc(&seg, count) != cudaSuccess)
@@ -491,7 +526,11 @@ int ensure_prec_slices(cgb_session *s)
     const float *vals[2] = {s->d_f_val, s->d_ft_val};
     SliceSet *sets[2] = {&s->sf, &s->sft};
     for (int m = 0; m < 2 && st == CGB_OK; m++) {
-        cudaError_t e = cudaMemsetAsync(s->d_flag, 0, sizeof(int), s->stream);
+        cudaError_t e = dev_alloc(&sets[m]->chunk_slice, chunk_slice.size());
+        if (e == cudaSuccess)
+            e = cudaMemcpy(sets[m]->chunk_slice, chunk_slice.data(), sizeof(int) * chunk_slice.size(),
+                           cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemsetAsync(s->d_flag, 0, sizeof(int), s->stream);
         if (e == cudaSuccess) {
             build_segments<<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
                 ptrs[m], cols[m], n, s->nblk, kSliceWidth, seg, s->seg_stride, s->d_flag);
@@ -501,9 +540,9 @@ int ensure_prec_slices(cgb_session *s)
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(&unsorted, s->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-        if (e != cudaSuccess) st = set_error(CGB_ERR_CUDA, "factor segments: %s", cudaGetErrorString(e));
+        if (e != cudaSuccess) st = set_error(CGB_ERR_CUDA, "factor slices: %s", cudaGetErrorString(e));
         else if (unsorted) st = set_error(CGB_ERR_STATE, "factor rows not in ascending column order");
-        else st = fill_set<float>(s, seg, cols[m], vals[m], s->slice_total, false, true, sets[m]);
+        else st = fill_set<float>(s, grid, true, seg, cols[m], vals[m], total, false, true, sets[m]);
     }
     dev_free(seg);
     if (st) {
@@ -525,6 +564,7 @@ bool make_plan(cgb_session *s, int kind, int lpr, Plan *pl)
     if (kind == kKindRow) {
         if (!row_kernels(lpr, &P)) return false;
         P.block = s->opts.block_threads ? s->opts.block_threads : 512;
+        P.block_mixed = P.block_pcg = P.block;
         P.smem = 0;
         // almost nothing lives in shared memory: give L1 the room
         for (OuterKernel k : {P.fp64, P.mixed, P.pcg})
@@ -538,7 +578,9 @@ bool make_plan(cgb_session *s, int kind, int lpr, Plan *pl)
         P.mixed = outer_step_mixed_sliced;
         P.pcg = outer_step_pcg_sliced;
         P.spmv = spmv_dot_sliced;
-        P.block = 1024;
+        P.block = kSlicedBlock;
+        P.block_mixed = kSlicedMixedBlock;
+        P.block_pcg = kSlicedPcgBlock;
         const int grid = std::min(s->prop.multiProcessorCount, s->n);
         if (s->sliced_grid != grid && build_sliced(s, grid) != CGB_OK) return false;
         P.smem = sliced_smem_bytes(s->sliced_max_rows);
@@ -554,9 +596,11 @@ bool make_plan(cgb_session *s, int kind, int lpr, Plan *pl)
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, P.fp64, P.block, P.smem) != cudaSuccess ||
         per_sm < 1)
         return false;
-    for (OuterKernel k : {P.mixed, P.pcg}) {
+    const std::pair<OuterKernel, int> others[2] = {{P.mixed, P.block_mixed}, {P.pcg, P.block_pcg}};
+    for (const auto &kb : others) {
         int per = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, P.block, P.smem) != cudaSuccess ||
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kb.first, kb.second, P.smem) !=
+                cudaSuccess ||
             per < 1)
             return false;
         per_sm = std::min(per_sm, per);
@@ -756,6 +800,7 @@ cudaError_t enqueue_power(cgb_session *s, const cgb_solve_params &P)
     A.tol = P.tol;
     A.refresh_every = P.refresh_every > 0 ? P.refresh_every : 10;
     A.finish = 1;
+    A.recycle = P.mode == CGB_MODE_FP64 ? 0 : P.recycle;
     const OuterKernel k = P.mode == CGB_MODE_MIXED_LEARNED ? s->plan.pcg
                           : P.mode == CGB_MODE_MIXED       ? s->plan.mixed
                                                            : s->plan.fp64;
@@ -781,6 +826,8 @@ int check_params(cgb_session *s, const cgb_solve_params &P)
         return set_error(CGB_ERR_STATE, "preconditioned mode needs cgb_set_preconditioner first");
     if (P.mode != CGB_MODE_FP64 && !(P.tol > 0.0))
         return set_error(CGB_ERR_INVALID, "tolerance modes need tol > 0");
+    if (P.recycle < 0 || P.recycle > kMaxRecycle)
+        return set_error(CGB_ERR_INVALID, "recycle must be 0..%d", kMaxRecycle);
     if (is_mixed(P.mode) && !s->d_a32)
         return set_error(CGB_ERR_STATE, "mixed mode needs the FP32 copy (keep_fp32_copy = 1)");
     return CGB_OK;
@@ -789,7 +836,7 @@ int check_params(cgb_session *s, const cgb_solve_params &P)
 bool same_params(const cgb_solve_params &a, const cgb_solve_params &b)
 {
     return a.niter == b.niter && a.shift == b.shift && a.mode == b.mode && a.cgitmax == b.cgitmax &&
-           a.tol == b.tol && a.refresh_every == b.refresh_every;
+           a.tol == b.tol && a.refresh_every == b.refresh_every && a.recycle == b.recycle;
 }
 
 }  // namespace
@@ -852,6 +899,7 @@ void cgb_default_solve_params(cgb_solve_params *p)
     p->cgitmax = 25;
     p->tol = 1e-12;
     p->refresh_every = 10;
+    p->recycle = 4;
 }
 
 int cgb_device_info(int device, int *sm_count, int *cc_major, int *cc_minor,
@@ -922,6 +970,8 @@ int cgb_create(int n, const int *rowstr, const int *colidx, const double *a,
     CREATE_TRY(cudaMemset(s->d_r32, 0, sizeof(float) * s->vstride));
     CREATE_TRY(dev_alloc(&s->d_y, s->vstride));
     CREATE_TRY(cudaMemset(s->d_y, 0, sizeof(double) * s->vstride));
+    CREATE_TRY(dev_alloc(&s->d_hx, kMaxRecycle * s->vstride));
+    CREATE_TRY(dev_alloc(&s->d_hw, kMaxRecycle * s->vstride));
     CREATE_TRY(dev_alloc(&s->d_part, size_t(kSlotCount) * s->gpad));
     CREATE_TRY(dev_alloc(&s->d_sync, 96));
     CREATE_TRY(cudaMemset(s->d_sync, 0, sizeof(unsigned) * 96));

@@ -65,6 +65,8 @@ struct SliceSet {
     double *sval = nullptr;           // FP64 values
     float *sval32 = nullptr;          // FP32 values
     unsigned short *scol = nullptr;   // local columns
+    int *chunk_slice = nullptr;       // own chunk table (null: the session's)
+    int interleaved = 0;              // rows owned round-robin by the CTAs
     long long entries = 0;            // padded entries
 };
 
@@ -85,7 +87,15 @@ struct MatrixView {
     int nblk;                                 // column blocks
     int width;                                // columns per block
     int max_rows;                             // shared accumulator capacity
+    int interleaved;                          // 0: CTA c owns its contiguous row range;
+                                              // 1: CTA c owns rows c, c + G, c + 2G, ...
 };
+
+// Rows of CTA `c` of `grid` under interleaved ownership.
+__host__ __device__ inline int interleaved_rows(int n, int c, int grid)
+{
+    return c < n ? (n - c + grid - 1) / grid : 0;
+}
 
 template <typename VT>
 __device__ __forceinline__ const VT *csr_values(const MatrixView &M);
@@ -151,6 +161,7 @@ __device__ __forceinline__ double spmv_rows(const MatrixView &M, const VT *v, do
 
 template <int LPR>
 struct RowSpmv {
+    static constexpr bool kSliced = false;
     int row0, row1;
     __device__ void setup(const MatrixView &, int r0, int r1)
     {
@@ -226,7 +237,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, long l
     return true;
 }
 
-// Bytes of one staging slot and dynamic shared memory of SlicedSpmv.
+// Bytes of one staging slot and dynamic shared memory of the sliced policy.
 constexpr int kSliceWidth = 12288;  // columns per block
 constexpr unsigned kSlotBytes = kSliceWidth * 8u;
 __host__ __device__ inline size_t sliced_smem_bytes(int max_rows)
@@ -234,7 +245,11 @@ __host__ __device__ inline size_t sliced_smem_bytes(int max_rows)
     return 2 * size_t(kSlotBytes) + 2 * size_t(max_rows) * sizeof(double) + 128;
 }
 
-struct SlicedSpmv {
+// kU64 / kU32: step pairs in flight per lane for FP64 / FP32 values (more
+// for kernels with fewer, register-richer threads).
+template <int kU64, int kU32, bool kOutline = false>
+struct SlicedSpmvT {
+    static constexpr bool kSliced = true;
     int row0, row1, chunk0;  // chunk0 = blockIdx.x * nblk
     unsigned char *buf;      // 2 slots
     double *acc0, *acc1;     // max_rows each
@@ -273,18 +288,40 @@ struct SlicedSpmv {
         bulk_load(buf + size_t(slot) * kSlotBytes, v + size_t(b) * M.width, bytes, &bars[slot]);
     }
 
+    // kOutline: the SpMV is a called function with its own register budget
+    // (for kernels whose solver state would otherwise crowd the SpMV loop).
     template <typename VT>
     __device__ __forceinline__ double apply(const MatrixView &M, const VT *v, double *out,
                                             const double *dotv, int n, long long limit_ns,
                                             int *status, bool &ok)
     {
+        if constexpr (kOutline) return apply_outlined<VT>(M, v, out, dotv, n, limit_ns, status, ok);
+        else return apply_body<VT>(M, v, out, dotv, n, limit_ns, status, ok);
+    }
+
+    template <typename VT>
+    __device__ __noinline__ double apply_outlined(const MatrixView &M, const VT *v, double *out,
+                                                  const double *dotv, int n, long long limit_ns,
+                                                  int *status, bool &ok)
+    {
+        return apply_body<VT>(M, v, out, dotv, n, limit_ns, status, ok);
+    }
+
+    template <typename VT>
+    __device__ __forceinline__ double apply_body(const MatrixView &M, const VT *v, double *out,
+                                                 const double *dotv, int n, long long limit_ns,
+                                                 int *status, bool &ok)
+    {
         using P2 = typename Pair<VT>::T;
-        constexpr int kU = sizeof(VT) == 8 ? 4 : 6;  // step pairs in flight per lane (measured best)
+        constexpr int kU = sizeof(VT) == 8 ? kU64 : kU32;
         const VT *__restrict__ vals = slice_values<VT>(M);
         const int lane = threadIdx.x & 31;
         const int warp = threadIdx.x >> 5;
         const int nwarps = blockDim.x >> 5;
-        const int nrows = row1 - row0;
+        // output rows: the CTA's range, or (interleaved copy) every grid-th row
+        const int base = M.interleaved ? int(blockIdx.x) : row0;
+        const int stride = M.interleaved ? int(gridDim.x) : 1;
+        const int nrows = M.interleaved ? interleaved_rows(n, blockIdx.x, gridDim.x) : row1 - row0;
         for (int i = threadIdx.x; i < nrows; i += blockDim.x) {
             acc0[i] = 0.0;
             acc1[i] = 0.0;
@@ -364,12 +401,19 @@ struct SlicedSpmv {
         double dacc = 0.0;
         for (int i = threadIdx.x; i < nrows; i += blockDim.x) {
             const double t = acc0[i] + acc1[i];
-            out[row0 + i] = t;
-            if (dotv) dacc = fma(dotv[row0 + i], t, dacc);
+            const int row = base + i * stride;
+            out[row] = t;
+            if (dotv) dacc = fma(dotv[row], t, dacc);
         }
         ok = true;
         return dacc;
     }
 };
+
+// 1024-thread kernels (64 registers a thread) and the register-richer
+// 768- and 512-thread kernels; pair counts measured on B200.
+using SlicedSpmv = SlicedSpmvT<4, 6>;
+using SlicedSpmv768 = SlicedSpmvT<4, 6>;
+using SlicedSpmv512 = SlicedSpmvT<4, 6>;
 
 }  // namespace cgb

@@ -70,7 +70,7 @@ class Options(ctypes.Structure):
 class SolveParams(ctypes.Structure):
     _fields_ = [("niter", ctypes.c_int), ("shift", ctypes.c_double), ("mode", ctypes.c_int),
                 ("cgitmax", ctypes.c_int), ("tol", ctypes.c_double),
-                ("refresh_every", ctypes.c_int)]
+                ("refresh_every", ctypes.c_int), ("recycle", ctypes.c_int)]
 
 
 class BatchParams(ctypes.Structure):
@@ -263,12 +263,13 @@ class Session:
         return z, p, q, r, rn.value
 
     def power_iterate(self, niter, shift, mode=MODE_FP64, cgitmax=25, tol=1e-12,
-                      refresh_every=10, want_x=False):
-        """The outer loop of cg.cu:500-520; returns a dict with traces and timings."""
+                      refresh_every=10, want_x=False, recycle=4):
+        """The outer loop of cg.cu:500-520; returns a dict with traces and timings.
+        `recycle`: Galerkin start on that many previous iterates (tolerance modes)."""
         P = SolveParams()
         lib().cgb_default_solve_params(ctypes.byref(P))
         P.niter, P.shift, P.mode, P.cgitmax = niter, shift, mode, cgitmax
-        P.tol, P.refresh_every = tol, refresh_every
+        P.tol, P.refresh_every, P.recycle = tol, refresh_every, recycle
         zt, rt = np.zeros(niter), np.zeros(niter)
         it = np.zeros(niter, np.int32)
         x = np.zeros(self.n) if want_x else None

@@ -304,3 +304,39 @@ def test_fp32_spmv_close_to_fp64(cgb):
         with cgb.Session(rs, ci, a, spmv_kernel=kind) as s:
             assert s.time_spmv(3, fp32=True) > 0
             assert s.time_spmv(3, fp32=False) > 0
+
+
+@pytest.mark.parametrize("mode", ["tol", "mixed"])
+def test_galerkin_start_on_previous_iterates(cgb, golden, mode):
+    """Tolerance modes start each solve from the Galerkin solution on the
+    last 4 power-iteration iterates.  Config: class C (n=150000, nonzer=15,
+    shift=110), 75 outer steps, tol 1e-12.  Against the reference's FP64
+    trace: zeta relative 1e-10 at every step and rnorm absolute 1e-10*||x||,
+    with and without the recycled start; the recycled start needs fewer
+    inner iterations."""
+    n, nonzer, niter, shift = PARAMS["C"]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    ref = golden["C"]["seeds"]["314159265.0"]
+    m = cgb.MODE_FP64_TOL if mode == "tol" else cgb.MODE_MIXED
+    zr, rr = np.array(ref["zeta"]), np.array(ref["rnorm"])
+    xnorm = np.r_[np.sqrt(n), np.ones(niter - 1)]
+    inner = {}
+    with cgb.Session(rs, ci, a) as s:
+        for rec in (0, 4):
+            out = s.power_iterate(niter, shift, mode=m, tol=1e-12, cgitmax=100, recycle=rec)
+            assert np.max(np.abs(out["zeta"] - zr) / np.abs(zr)) <= 1e-10, rec
+            assert np.all(np.abs(out["rnorm"] - rr) <= 1e-10 * xnorm), rec
+            inner[rec] = out["total_inner"]
+    print(f"\n{mode}: inner iterations without / with the recycled start: {inner[0]} / {inner[4]}")
+    assert inner[4] < 0.85 * inner[0], inner
+
+
+def test_recycle_rejects_out_of_range(cgb):
+    n, nonzer, niter, shift = PARAMS["S"]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    with cgb.Session(rs, ci, a) as s:
+        with pytest.raises(cgb.CgbError):
+            s.power_iterate(2, shift, mode=cgb.MODE_FP64_TOL, recycle=5)
+        # the reference mode ignores it
+        out = s.power_iterate(niter, shift, recycle=4)
+    assert abs(out["zeta"][-1] - VERIFY["S"]) / VERIFY["S"] <= 1e-10
