@@ -210,6 +210,7 @@ typedef struct cgb_batch_params {
     int cgitmax;        /* inner steps: exact (FP64) or cap (MIXED) */
     double tol;         /* MIXED: stop when ||x - A z|| <= tol ||x|| */
     int refresh_every;  /* MIXED: true-residual replacement at least every k steps */
+    int recycle;        /* MIXED: Galerkin start on the last `recycle` iterates (0..4, default 4) */
 } cgb_batch_params;
 
 void cgb_default_batch_params(cgb_batch_params *p);

@@ -35,6 +35,7 @@
 
 #include "cgb_internal.h"
 #include "device_common.cuh"
+#include "galerkin.cuh"
 
 namespace cgb {
 namespace batch {
@@ -66,7 +67,41 @@ struct BatchArgs {
     double tol;
     double *zeta, *rnorm;
     int *iters, *status;  // status: 0 = done; 1 = mixed iteration gave up (solved again in FP64)
+    // mixed mode: Galerkin start on the last `recycle` iterates; slot j of
+    // system s at hx/hw + j * hstride + vec_off
+    double *hx, *hw;
+    long long hstride;
+    int recycle;
 };
+
+// CTA sums of nq (<= kGramValues) per-thread values, in a fixed order, into
+// out[] (shared, every thread); four values a round keep the static shared
+// memory small beside the up to 216 KB of p.
+__device__ __forceinline__ void cta_sum_multi(const double *vals, int nq, double *out)
+{
+    constexpr int kRound = 4;
+    __shared__ double red[32][kRound];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+    for (int q0 = 0; q0 < kGramValues; q0 += kRound) {
+        if (q0 < nq) {
+#pragma unroll
+            for (int k = 0; k < kRound; k++) {
+                if (q0 + k < nq && q0 + k < kGramValues) {
+                    const double v = warp_sum(vals[q0 + k < kGramValues ? q0 + k : 0]);
+                    if (l == 0) red[w][k] = v;
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x < kRound && q0 + int(threadIdx.x) < nq) {
+                double t = 0.0;
+                for (int i = 0; i < int(blockDim.x >> 5); i++) t += red[i][threadIdx.x];
+                out[q0 + threadIdx.x] = t;
+            }
+            __syncthreads();
+        }
+    }
+}
 
 __device__ __forceinline__ double cta_sum(double v, double *red)
 {
@@ -147,15 +182,82 @@ __device__ bool solve_system(const BatchArgs &B, const SysDesc &S, double *p, do
     double zeta = 0.0, rnorm = 0.0;
     for (int outer = 0; outer < B.niter; outer++) {
         double acc = 0.0;
-        for (int j = threadIdx.x; j < n; j += blockDim.x) {
-            const double xv = x[j];
-            z[j] = 0.0;
-            r[j] = xv;
-            p[j] = xv;
-            acc = fma(xv, xv, acc);
+        const int m = B.recycle;
+        const int v = (mixed && m > 0) ? min(outer, m) : 0;
+        double xx = 0.0;
+        if (v > 0) {
+            // Galerkin start on x_k .. x_{k-v+1}: z0 = V y, A z0 = W y
+            __shared__ double g_sh[kGramValues];
+            __shared__ double y_sh[kMaxRecycle];
+            long long off[kMaxRecycle];
+#pragma unroll
+            for (int a = 0; a < kMaxRecycle; a++)
+                off[a] = ((outer - a) % m + m) % m * B.hstride + S.vec_off;
+            const int npairs = v * (v + 1) / 2;
+            double vals[kGramValues];
+#pragma unroll
+            for (int q = 0; q < kGramValues; q++) vals[q] = 0.0;
+            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                const double xv = x[j];
+#pragma unroll
+                for (int b = 0; b < kMaxRecycle; b++) {
+                    if (b < v) {
+                        const double xb = B.hx[off[b] + j], wb = B.hw[off[b] + j];
+#pragma unroll
+                        for (int a = 0; a <= b; a++)
+                            vals[gram_index(a, b)] = fma(a == b ? xb : B.hx[off[a] + j], wb,
+                                                         vals[gram_index(a, b)]);
+                        vals[kGramPairs + b] = fma(xb, xv, vals[kGramPairs + b]);
+                    }
+                }
+            }
+            double packed[kGramValues];
+#pragma unroll
+            for (int q = 0; q < kGramValues; q++) packed[q] = 0.0;
+#pragma unroll
+            for (int q = 0; q < kGramPairs; q++)
+                if (q < npairs) packed[q] = vals[q];
+#pragma unroll
+            for (int b = 0; b < kMaxRecycle; b++)
+                if (b < v) packed[npairs + b] = vals[kGramPairs + b];
+            cta_sum_multi(packed, npairs + v, g_sh);
+            if (threadIdx.x == 0) {
+                double g[kGramValues], y[kMaxRecycle];
+                for (int q = 0; q < kGramValues; q++) g[q] = 0.0;
+                for (int q = 0; q < npairs; q++) g[q] = g_sh[q];
+                for (int b = 0; b < v; b++) g[kGramPairs + b] = g_sh[npairs + b];
+                galerkin_solve(g, v, y);
+                for (int a = 0; a < kMaxRecycle; a++) y_sh[a] = a < v ? y[a] : 0.0;
+            }
+            __syncthreads();
+            xx = g_sh[npairs];  // x_k . x_k
+            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                double z0 = 0.0, az = 0.0;
+#pragma unroll
+                for (int a = 0; a < kMaxRecycle; a++) {
+                    if (a < v) {
+                        z0 = fma(y_sh[a], B.hx[off[a] + j], z0);
+                        az = fma(y_sh[a], B.hw[off[a] + j], az);
+                    }
+                }
+                const double rv = x[j] - az;
+                z[j] = z0;
+                r[j] = rv;
+                p[j] = rv;
+                acc = fma(rv, rv, acc);
+            }
+        } else {
+            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                const double xv = x[j];
+                z[j] = 0.0;
+                r[j] = xv;
+                p[j] = xv;
+                acc = fma(xv, xv, acc);
+            }
         }
         double rho = cta_sum(acc, red);  // includes a barrier: p complete
-        const double stop2 = B.tol * B.tol * rho;
+        if (v == 0) xx = rho;
+        const double stop2 = B.tol * B.tol * xx;
         double rho_cycle = rho;
         int it = 0, since = 0;
         bool fresh = true;
@@ -212,8 +314,13 @@ __device__ bool solve_system(const BatchArgs &B, const SysDesc &S, double *p, do
             fresh = false;
         }
         total += it;
-        // rnorm = ||x - A z||, x.z, z.z; z from global memory
-        sys_spmv<LPR, false>(B, S, nullptr, z, q, nullptr);
+        // q = A z (FP64): a product, or from the true residual r = x - A z
+        // the mixed iteration just accepted; rnorm = ||x - A z||, x.z, z.z
+        if (mixed && fresh) {
+            for (int j = threadIdx.x; j < n; j += blockDim.x) q[j] = x[j] - r[j];
+        } else {
+            sys_spmv<LPR, false>(B, S, nullptr, z, q, nullptr);
+        }
         __syncthreads();
         double res = 0.0, xz = 0.0, zz = 0.0;
         for (int j = threadIdx.x; j < n; j += blockDim.x) {
@@ -227,7 +334,18 @@ __device__ bool solve_system(const BatchArgs &B, const SysDesc &S, double *p, do
         const double t2 = cta_sum(zz, red);
         zeta = S.shift + 1.0 / t1;
         const double norm = 1.0 / sqrt(t2);
-        for (int j = threadIdx.x; j < n; j += blockDim.x) x[j] = norm * z[j];
+        if (mixed && m > 0) {
+            // the next iterate and A times it into the ring
+            const long long slot = (outer + 1) % m * B.hstride + S.vec_off;
+            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                const double xn = norm * z[j];
+                B.hx[slot + j] = xn;
+                B.hw[slot + j] = norm * q[j];
+                x[j] = xn;
+            }
+        } else {
+            for (int j = threadIdx.x; j < n; j += blockDim.x) x[j] = norm * z[j];
+        }
         __syncthreads();
     }
     *iters_out = total;
@@ -320,6 +438,8 @@ struct cgb_batch {
     double *d_zeta = nullptr, *d_rnorm = nullptr;
     int *d_iters = nullptr, *d_status = nullptr;
     int *d_redo = nullptr;
+    double *d_hx = nullptr, *d_hw = nullptr;  // Galerkin-start ring, kMaxRecycle x vec_total each
+    long long vec_total = 0;
     int block = 512;
     // lane policy: lanes = 32 if mean >= t2, 16 if >= t1, 8 if >= t0, else 4
     double t0 = 16.0, t1 = 40.0, t2 = 96.0;
@@ -347,6 +467,7 @@ void batch_release(cgb_batch *b)
     bfree(b->d_sys); bfree(b->d_order); bfree(b->d_rowstr); bfree(b->d_colidx); bfree(b->d_a);
     bfree(b->d_a32); bfree(b->d_x); bfree(b->d_z); bfree(b->d_r); bfree(b->d_q);
     bfree(b->d_queue); bfree(b->d_zeta); bfree(b->d_rnorm); bfree(b->d_iters); bfree(b->d_status); bfree(b->d_redo);
+    bfree(b->d_hx); bfree(b->d_hw);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -414,6 +535,10 @@ int launch(cgb_batch *b, const cgb_batch_params &P, double *ms)
     A.rnorm = b->d_rnorm;
     A.iters = b->d_iters;
     A.status = b->d_status;
+    A.hx = b->d_hx;
+    A.hw = b->d_hw;
+    A.hstride = b->vec_total;
+    A.recycle = P.recycle;
     BT_TRY(cudaEventRecord(b->ev0, b->stream));
     int st;
     if (A.mode == 1) {
@@ -433,6 +558,7 @@ int launch(cgb_batch *b, const cgb_batch_params &P, double *ms)
                                    cudaMemcpyHostToDevice, b->stream));
             A.mode = 0;
             A.cgitmax = kReferenceCgitmax;
+            A.recycle = 0;
             st = launch_list<false>(b, A, b->d_redo, int(redo.size()));
             if (st) return st;
             // the FP64 pass wrote status 0 for these systems; mark them re-solved
@@ -466,6 +592,7 @@ void cgb_default_batch_params(cgb_batch_params *p)
     p->cgitmax = 25;
     p->tol = 1e-12;
     p->refresh_every = 10;
+    p->recycle = 4;
 }
 
 int cgb_batch_create(int device, int nsys, const int *n, const int *const *rowstr,
@@ -508,6 +635,7 @@ int cgb_batch_create(int device, int nsys, const int *n, const int *const *rowst
     b->nsys = nsys;
     b->max_n = max_n;
     b->total_nnz = nnz_total;
+    b->vec_total = vec_total;
     b->desc.resize(nsys);
     b->mean_len.resize(nsys);
     long long ro = 0, no = 0, vo = 0;
@@ -538,7 +666,8 @@ int cgb_batch_create(int device, int nsys, const int *n, const int *const *rowst
               !balloc(&b->d_r, vec_total) && !balloc(&b->d_q, vec_total) &&
               !balloc(&b->d_queue, 1) && !balloc(&b->d_zeta, nsys) && !balloc(&b->d_rnorm, nsys) &&
               !balloc(&b->d_iters, nsys) && !balloc(&b->d_status, nsys) &&
-              !balloc(&b->d_redo, nsys);
+              !balloc(&b->d_redo, nsys) && !balloc(&b->d_hx, kMaxRecycle * vec_total) &&
+              !balloc(&b->d_hw, kMaxRecycle * vec_total);
     if (!ok) {
         batch_release(b);
         return set_error(CGB_ERR_NOMEM, "batch device allocation failed");
@@ -579,8 +708,10 @@ int cgb_batch_solve(cgb_batch *b, const cgb_batch_params *params, double *zeta, 
     if (!b || !params) return set_error(CGB_ERR_INVALID, "batch: null argument");
     const cgb_batch_params P = *params;
     if (P.niter < 1 || P.cgitmax < 1 || (P.mode != CGB_MODE_FP64 && P.mode != CGB_MODE_MIXED) ||
-        (P.mode == CGB_MODE_MIXED && !(P.tol > 0.0)))
-        return set_error(CGB_ERR_INVALID, "batch: niter, cgitmax >= 1; mode FP64 or MIXED (tol > 0)");
+        (P.mode == CGB_MODE_MIXED && !(P.tol > 0.0)) || P.recycle < 0 || P.recycle > kMaxRecycle)
+        return set_error(CGB_ERR_INVALID,
+                         "batch: niter, cgitmax >= 1; mode FP64 or MIXED (tol > 0); recycle 0..%d",
+                         kMaxRecycle);
     BT_TRY(cudaSetDevice(b->device));
     double ms = 0.0;
     int st = launch(b, P, &ms);

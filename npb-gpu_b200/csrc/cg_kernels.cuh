@@ -27,14 +27,11 @@
 //                          computed with the FP64 matrix stay in FP64.
 #pragma once
 
+#include "galerkin.cuh"
 #include "spmv_policies.cuh"
 
 namespace cgb {
 
-// Galerkin start: at most kMaxRecycle previous iterates; the Gram values
-// x_a . A x_b (a <= b) and x_a . x, per CTA.
-constexpr int kMaxRecycle = 4;
-constexpr int kGramValues = kMaxRecycle * (kMaxRecycle + 1) / 2 + kMaxRecycle;
 
 // Partial-sum slots (each holds `gpad` doubles, one per CTA).
 enum Slot { kSlotRho = 0, kSlotD = 1, kSlotXX = 2, kSlotRes = 3, kSlotXZ = 4, kSlotZZ = 5,
@@ -235,25 +232,33 @@ __device__ __forceinline__ GalerkinArgs galerkin_args(const OuterArgs &A)
 }
 
 // Per-CTA sums of nq per-thread values into slots [slot0, slot0 + nq).
+// Four values a round keep the static shared memory small (the sliced
+// kernels give nearly all of it to staging).
 __device__ __forceinline__ void put_partials_multi(const GalerkinArgs &A, int slot0,
                                                    const double *vals, int nq)
 {
-    __shared__ double red[32][kGramValues];
+    constexpr int kRound = 4;
+    __shared__ double red[32][kRound];
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
 #pragma unroll
-    for (int q = 0; q < kGramValues; q++) {
-        if (q < nq) {
-            const double v = warp_sum(vals[q]);
-            if (l == 0) red[w][q] = v;
+    for (int q0 = 0; q0 < kGramValues; q0 += kRound) {
+        if (q0 < nq) {
+#pragma unroll
+            for (int k = 0; k < kRound; k++) {
+                if (q0 + k < nq && q0 + k < kGramValues) {
+                    const double v = warp_sum(vals[q0 + k < kGramValues ? q0 + k : 0]);
+                    if (l == 0) red[w][k] = v;
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x < kRound && q0 + int(threadIdx.x) < nq) {
+                double t = 0.0;
+                for (int i = 0; i < int(blockDim.x >> 5); i++) t += red[i][threadIdx.x];
+                A.part[size_t(slot0 + q0 + threadIdx.x) * A.gpad + blockIdx.x] = t;
+            }
+            __syncthreads();
         }
     }
-    __syncthreads();
-    if (threadIdx.x < nq) {
-        double t = 0.0;
-        for (int i = 0; i < int(blockDim.x >> 5); i++) t += red[i][threadIdx.x];
-        A.part[size_t(slot0 + threadIdx.x) * A.gpad + blockIdx.x] = t;
-    }
-    __syncthreads();
 }
 
 // Totals of slots [slot0, slot0 + nq) into out[] (shared), the same in
@@ -268,73 +273,6 @@ __device__ __forceinline__ void get_totals_multi(const GalerkinArgs &A, int slot
         if (l == 0) out[q] = t;
     }
     __syncthreads();
-}
-
-__device__ __forceinline__ int gram_index(int a, int b)  // a <= b < v, packed by b
-{
-    return b * (b + 1) / 2 + a;
-}
-
-// Coefficients y of the Galerkin start from the Gram totals g[] (see
-// galerkin_start); one thread.  Returns the number of directions kept.
-static __device__ __noinline__ int galerkin_solve(const double *g, int v, double *y)
-{
-    double N[kMaxRecycle][kMaxRecycle], c[kMaxRecycle];
-    for (int b = 0; b < v; b++) {
-        for (int a = 0; a <= b; a++) N[a][b] = N[b][a] = -g[gram_index(a, b)];
-        c[b] = g[kMaxRecycle * (kMaxRecycle + 1) / 2 + b];
-    }
-    if (!(N[0][0] > 0.0)) {
-        for (int a = 0; a < v; a++) y[a] = 0.0;
-        return 0;
-    }
-    const double taus[4] = {1e-12, 1e-10, 1e-8, 1e-6};
-    for (int t = 0; t < 5; t++) {
-        // t == 4: the first direction alone
-        const double tau = t < 4 ? taus[t] * N[0][0] : 1e300;
-        double L[kMaxRecycle][kMaxRecycle], u[kMaxRecycle];
-        bool keep[kMaxRecycle];
-        int kept = 0;
-        for (int i = 0; i < v; i++) {
-            double d = N[i][i];
-            for (int k = 0; k < i; k++)
-                if (keep[k]) d -= L[i][k] * L[i][k];
-            keep[i] = (i == 0) || d > tau;
-            if (!keep[i]) continue;
-            kept++;
-            L[i][i] = sqrt(d);
-            for (int j = i + 1; j < v; j++) {
-                double e = N[j][i];
-                for (int k = 0; k < i; k++)
-                    if (keep[k]) e -= L[j][k] * L[i][k];
-                L[j][i] = e / L[i][i];
-            }
-        }
-        // N y = -c on the kept directions
-        for (int i = 0; i < v; i++) {
-            if (!keep[i]) { u[i] = 0.0; continue; }
-            double e = -c[i];
-            for (int k = 0; k < i; k++)
-                if (keep[k]) e -= L[i][k] * u[k];
-            u[i] = e / L[i][i];
-        }
-        for (int i = v - 1; i >= 0; i--) {
-            if (!keep[i]) { y[i] = 0.0; continue; }
-            double e = u[i];
-            for (int j = i + 1; j < v; j++)
-                if (keep[j]) e -= L[j][i] * y[j];
-            y[i] = e / L[i][i];
-        }
-        // growth of the combination in the A-norm: sum |y_a| ||x_a||_A
-        // against ||z0||_A; accept when the cancellation is mild
-        double num = 0.0, zA = 0.0;
-        for (int a = 0; a < v; a++) {
-            num += fabs(y[a]) * sqrt(N[a][a]);
-            for (int b = 0; b < v; b++) zA += y[a] * N[a][b] * y[b];
-        }
-        if (t == 4 || (zA > 0.0 && num <= 100.0 * sqrt(zA) && isfinite(num))) return kept;
-    }
-    return 1;
 }
 
 // z0 and A z0 of the Galerkin start into A.z and A.q (own rows; entry n of
@@ -368,8 +306,8 @@ static __device__ __noinline__ bool galerkin_start(const GalerkinArgs A, int row
 #pragma unroll
             for (int a = 0; a <= b; a++)
                 if (b < v) vals[gram_index(a, b)] = fma(xa[a], wa[b], vals[gram_index(a, b)]);
-            if (b < v) vals[kMaxRecycle * (kMaxRecycle + 1) / 2 + b] =
-                fma(xa[b], xv, vals[kMaxRecycle * (kMaxRecycle + 1) / 2 + b]);
+            if (b < v) vals[kGramPairs + b] =
+                fma(xa[b], xv, vals[kGramPairs + b]);
         }
     }
     // pack: Gram pairs first, then the right-hand sides
@@ -377,11 +315,11 @@ static __device__ __noinline__ bool galerkin_start(const GalerkinArgs A, int row
 #pragma unroll
     for (int q = 0; q < kGramValues; q++) packed[q] = 0.0;
 #pragma unroll
-    for (int q = 0; q < kMaxRecycle * (kMaxRecycle + 1) / 2; q++)
+    for (int q = 0; q < kGramPairs; q++)
         if (q < npairs) packed[q] = vals[q];
 #pragma unroll
     for (int b = 0; b < kMaxRecycle; b++)
-        if (b < v) packed[npairs + b] = vals[kMaxRecycle * (kMaxRecycle + 1) / 2 + b];
+        if (b < v) packed[npairs + b] = vals[kGramPairs + b];
     put_partials_multi(A, kSlotGram, packed, npairs + v);
     if (!grid_barrier(A.gb)) return false;
     get_totals_multi(A, kSlotGram, npairs + v, g_sh);
@@ -389,7 +327,7 @@ static __device__ __noinline__ bool galerkin_start(const GalerkinArgs A, int row
         double g[kGramValues];
         for (int q = 0; q < kGramValues; q++) g[q] = 0.0;
         for (int q = 0; q < npairs; q++) g[q] = g_sh[q];
-        for (int b = 0; b < v; b++) g[kMaxRecycle * (kMaxRecycle + 1) / 2 + b] = g_sh[npairs + b];
+        for (int b = 0; b < v; b++) g[kGramPairs + b] = g_sh[npairs + b];
         double y[kMaxRecycle];
         galerkin_solve(g, v, y);
         for (int a = 0; a < kMaxRecycle; a++) y_sh[a] = a < v ? y[a] : 0.0;
@@ -613,8 +551,11 @@ __device__ __forceinline__ void outer_step_mixed_body(const OuterArgs &A)
 //    row ownership (CTA c computes rows c, c+G, ...).  F is lower
 //    triangular, so contiguous row ranges would leave the first CTAs almost
 //    idle and the last ones with whole rows (and the reverse for F^T);
-//    interleaving gives every CTA a fair sample of row lengths.  The F^T
-//    product fuses the r.y partial over the rows it computes.
+//    interleaving gives every CTA a fair sample of row lengths.  Their
+//    values are stored in BF16 (4 bytes an entry with the 16-bit column;
+//    products and sums in FP32): M = F~^T F~ of the rounded factor is still
+//    SPD and the same operator in every application.  The F^T product fuses
+//    the r.y partial over the rows it computes.
 //  - row policy: CSR rows of F and F^T with LPRG lanes per row over the
 //    CTA's own rows.
 template <class Spmv, int LPRG>
@@ -627,8 +568,9 @@ __device__ __forceinline__ bool apply_prec(Spmv &sp, const OuterArgs &A, int row
     if (use) {
         if constexpr (Spmv::kSliced) {
             bool ok = true;
-            (void)sp.template apply<float>(A.F, A.r32, A.q, nullptr, A.n, A.gb.limit_ns,
-                                           A.gb.status, ok);  // t = F r (interleaved rows)
+            (void)sp.template apply<float, __nv_bfloat16>(A.F, A.r32, A.q, nullptr, A.n,
+                                                          A.gb.limit_ns, A.gb.status,
+                                                          ok);  // t = F r (interleaved rows)
             if (!ok) return false;
             const int G = gridDim.x, nr = interleaved_rows(A.n, blockIdx.x, G);
             for (int i = threadIdx.x; i < nr; i += blockDim.x) {
@@ -636,8 +578,9 @@ __device__ __forceinline__ bool apply_prec(Spmv &sp, const OuterArgs &A, int row
                 A.p32[j] = float(A.q[j]);
             }
             if (!grid_barrier(A.gb)) return false;
-            acc = sp.template apply<float>(A.FT, A.p32, A.y, A.r, A.n, A.gb.limit_ns, A.gb.status,
-                                           ok);  // y = F^T t, r.y
+            acc = sp.template apply<float, __nv_bfloat16>(A.FT, A.p32, A.y, A.r, A.n,
+                                                          A.gb.limit_ns, A.gb.status,
+                                                          ok);  // y = F^T t, r.y
             if (!ok) return false;
         } else {
             spmv_rows<LPRG, float>(A.F, A.r32, A.q, row0, row1, nullptr);  // t = F r
@@ -855,7 +798,9 @@ struct SpmvArgs {
     int fp32;  // 1: q = A32 p32
 };
 
-template <class Spmv>
+// kPrec: 0 = FP64 or FP32 by S.fp32; 1 = FP64 only; 2 = FP32 only (a kernel
+// per precision keeps each one's register allocation to itself).
+template <class Spmv, int kPrec>
 __device__ __forceinline__ void spmv_dot_body(const SpmvArgs &S)
 {
     __shared__ double scratch[32];
@@ -864,8 +809,11 @@ __device__ __forceinline__ void spmv_dot_body(const SpmvArgs &S)
     Spmv sp;
     sp.setup(A.M, A.row_split[blockIdx.x], A.row_split[blockIdx.x + 1]);
     bool ok = true;
-    const double acc = S.fp32 ? spmv<Spmv, float>(sp, A, A.p32, A.q, A.p, ok)
-                              : spmv<Spmv, double>(sp, A, A.p, A.q, A.p, ok);
+    double acc;
+    if constexpr (kPrec == 1) acc = spmv<Spmv, double>(sp, A, A.p, A.q, A.p, ok);
+    else if constexpr (kPrec == 2) acc = spmv<Spmv, float>(sp, A, A.p32, A.q, A.p, ok);
+    else acc = S.fp32 ? spmv<Spmv, float>(sp, A, A.p32, A.q, A.p, ok)
+                      : spmv<Spmv, double>(sp, A, A.p, A.q, A.p, ok);
     if (!ok) return;
     const double s = block_sum(acc, scratch);
     if (threadIdx.x == 0) {
@@ -891,12 +839,17 @@ __device__ __forceinline__ void spmv_dot_body(const SpmvArgs &S)
 template <int LPR>
 __global__ void __launch_bounds__(512, 2) spmv_dot_row(SpmvArgs S)
 {
-    spmv_dot_body<RowSpmv<LPR>>(S);
+    spmv_dot_body<RowSpmv<LPR>, 0>(S);
 }
 
 static __global__ void __launch_bounds__(kSlicedBlock, 1) spmv_dot_sliced(SpmvArgs S)
 {
-    spmv_dot_body<SlicedSpmv>(S);
+    spmv_dot_body<SlicedSpmv, 1>(S);
+}
+
+static __global__ void __launch_bounds__(kSlicedBlock, 1) spmv_dot_sliced32(SpmvArgs S)
+{
+    spmv_dot_body<SlicedSpmv, 2>(S);
 }
 
 // ------------------------------------------------------------- utilities
@@ -1043,7 +996,7 @@ __global__ void slice_fill(const int *__restrict__ seg, int seg_stride, int nblk
                            const unsigned short *__restrict__ srow,
                            const int *__restrict__ slice_width,
                            const unsigned *__restrict__ slice_off, int total, double *sval,
-                           float *sval32, unsigned short *scol)
+                           float *sval32, __nv_bfloat16 *sval16, unsigned short *scol)
 {
     const int lane = threadIdx.x & 31;
     for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < total;
@@ -1076,6 +1029,7 @@ __global__ void slice_fill(const int *__restrict__ seg, int seg_stride, int nblk
             const unsigned at = off + 64u * unsigned(k >> 1) + unsigned(k & 1);
             if (sval) sval[at] = v;
             if (sval32) sval32[at] = float(v);
+            if (sval16) sval16[at] = __float2bfloat16_rn(float(v));
             scol[at] = (unsigned short)col;
         }
     }

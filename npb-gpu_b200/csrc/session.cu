@@ -71,7 +71,8 @@ struct Plan {
     OuterKernel fp64 = nullptr;
     OuterKernel mixed = nullptr;
     OuterKernel pcg = nullptr;
-    SpmvKernel spmv = nullptr;
+    SpmvKernel spmv = nullptr;    // standalone SpMV (FP64; the row kernels also FP32 by flag)
+    SpmvKernel spmv32 = nullptr;  // standalone FP32 SpMV
     int block = 512;        // FP64 outer step and standalone SpMV
     int block_mixed = 512;  // mixed outer step
     int block_pcg = 512;    // preconditioned outer step
@@ -82,11 +83,11 @@ struct Plan {
 bool row_kernels(int lpr, Plan *P)
 {
     switch (lpr) {
-    case 2: P->fp64 = outer_step_fp64<2>; P->mixed = outer_step_mixed<2>; P->pcg = outer_step_pcg<2>; P->spmv = spmv_dot_row<2>; return true;
-    case 4: P->fp64 = outer_step_fp64<4>; P->mixed = outer_step_mixed<4>; P->pcg = outer_step_pcg<4>; P->spmv = spmv_dot_row<4>; return true;
-    case 8: P->fp64 = outer_step_fp64<8>; P->mixed = outer_step_mixed<8>; P->pcg = outer_step_pcg<8>; P->spmv = spmv_dot_row<8>; return true;
-    case 16: P->fp64 = outer_step_fp64<16>; P->mixed = outer_step_mixed<16>; P->pcg = outer_step_pcg<16>; P->spmv = spmv_dot_row<16>; return true;
-    case 32: P->fp64 = outer_step_fp64<32>; P->mixed = outer_step_mixed<32>; P->pcg = outer_step_pcg<32>; P->spmv = spmv_dot_row<32>; return true;
+    case 2: P->fp64 = outer_step_fp64<2>; P->mixed = outer_step_mixed<2>; P->pcg = outer_step_pcg<2>; P->spmv = P->spmv32 = spmv_dot_row<2>; return true;
+    case 4: P->fp64 = outer_step_fp64<4>; P->mixed = outer_step_mixed<4>; P->pcg = outer_step_pcg<4>; P->spmv = P->spmv32 = spmv_dot_row<4>; return true;
+    case 8: P->fp64 = outer_step_fp64<8>; P->mixed = outer_step_mixed<8>; P->pcg = outer_step_pcg<8>; P->spmv = P->spmv32 = spmv_dot_row<8>; return true;
+    case 16: P->fp64 = outer_step_fp64<16>; P->mixed = outer_step_mixed<16>; P->pcg = outer_step_pcg<16>; P->spmv = P->spmv32 = spmv_dot_row<16>; return true;
+    case 32: P->fp64 = outer_step_fp64<32>; P->mixed = outer_step_mixed<32>; P->pcg = outer_step_pcg<32>; P->spmv = P->spmv32 = spmv_dot_row<32>; return true;
     default: return false;
     }
 }
@@ -204,6 +205,7 @@ struct cgb_session {
     bool sorted = false;
     int sliced_grid = 0;   // grid the layout was built for (0: none)
     int sliced_max_rows = 0;
+    int sliced_nacc = 2;           // row accumulators (4 when they fit: FP32 pipeline depth)
     int *d_chunk_slice = nullptr;  // shared by A, F and F^T (same row split)
     cgb::SliceSet sa;              // A: FP64 values (+ FP32 copy)
     cgb::SliceSet sf, sft;         // F and F^T: FP32 values
@@ -248,6 +250,7 @@ void free_set(SliceSet &t)
     dev_free(t.off);
     dev_free(t.sval);
     dev_free(t.sval32);
+    dev_free(t.sval16);
     dev_free(t.scol);
     dev_free(t.chunk_slice);
     t.interleaved = 0;
@@ -311,6 +314,7 @@ void set_slices(cgb_session *s, const SliceSet &t, MatrixView *M)
 {
     M->sval = t.sval;
     M->sval32 = t.sval32;
+    M->sval16 = t.sval16;
     M->scol = t.scol;
     M->srow = t.srow;
     M->slice_off = t.off;
@@ -319,6 +323,7 @@ void set_slices(cgb_session *s, const SliceSet &t, MatrixView *M)
     M->nblk = s->nblk;
     M->width = kSliceWidth;
     M->max_rows = s->sliced_max_rows;
+    M->nacc = s->sliced_nacc;
     M->interleaved = t.interleaved;
 }
 
@@ -438,7 +443,7 @@ int chunk_table(int grid, int nblk, RowsOf rows_of, std::vector<int> &chunk_slic
 // or, with `interleave`, every grid-th row.  t->chunk_slice must be set.
 template <typename ST>
 int fill_set(cgb_session *s, int grid, bool interleave, const int *seg, const int *d_colidx,
-             const ST *vals, int total, bool want64, bool want32, SliceSet *t)
+             const ST *vals, int total, bool want64, bool want32, bool want16, SliceSet *t)
 {
     const int nchunks = grid * s->nblk;
     const int ig = interleave ? grid : 0;
@@ -458,11 +463,12 @@ int fill_set(cgb_session *s, int grid, bool interleave, const int *seg, const in
     t->entries = entries;
     if ((want64 && dev_alloc(&t->sval, size_t(entries) + kPad)) ||
         dev_alloc(&t->scol, size_t(entries) + kPad) ||
-        (want32 && dev_alloc(&t->sval32, size_t(entries) + kPad)))
+        (want32 && dev_alloc(&t->sval32, size_t(entries) + kPad)) ||
+        (want16 && dev_alloc(&t->sval16, size_t(entries) + kPad)))
         return set_error(CGB_ERR_NOMEM, "sliced layout: %u entries do not fit", entries);
     slice_fill<ST><<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
         seg, s->seg_stride, s->nblk, kSliceWidth, s->d_split, ig, t->chunk_slice, nchunks,
-        d_colidx, vals, t->srow, t->width, t->off, total, t->sval, t->sval32, t->scol);
+        d_colidx, vals, t->srow, t->width, t->off, total, t->sval, t->sval32, t->sval16, t->scol);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     return CGB_OK;
@@ -482,7 +488,18 @@ int build_sliced(cgb_session *s, int grid)
     int max_rows = interleaved_rows(s->n, 0, grid);
     for (int c = 0; c < grid; c++) max_rows = std::max(max_rows, split[c + 1] - split[c]);
     s->sliced_max_rows = (max_rows + 31) & ~31;
-    if (s->sliced_max_rows >= 0xffff || sliced_smem_bytes(s->sliced_max_rows) > kSmemLimit)
+    // dynamic shared memory must fit beside the kernels' static arrays
+    size_t static_smem = 0;
+    for (const void *k : {(const void *)outer_step_fp64_sliced, (const void *)outer_step_mixed_sliced,
+                          (const void *)outer_step_pcg_sliced, (const void *)spmv_dot_sliced,
+                          (const void *)spmv_dot_sliced32}) {
+        cudaFuncAttributes fa;
+        CUDA_TRY(cudaFuncGetAttributes(&fa, k));
+        static_smem = std::max(static_smem, size_t(fa.sharedSizeBytes));
+    }
+    const size_t room = kSmemLimit - std::min(kSmemLimit, static_smem);
+    s->sliced_nacc = sliced_smem_bytes(s->sliced_max_rows, kMaxSlots) <= room ? kMaxSlots : 2;
+    if (s->sliced_max_rows >= 0xffff || sliced_smem_bytes(s->sliced_max_rows, 2) > room)
         return set_error(CGB_ERR_STATE, "sliced layout: %d rows per CTA exceed shared memory", max_rows);
     if (dev_alloc(&s->d_chunk_slice, chunk_slice.size()))
         return set_error(CGB_ERR_NOMEM, "sliced layout: metadata allocation failed");
@@ -494,7 +511,7 @@ int build_sliced(cgb_session *s, int grid)
         SliceSet &t = s->sa;
         t.chunk_slice = s->d_chunk_slice;
         const int r = fill_set<double>(s, grid, false, s->d_seg, s->d_colidx, s->d_a, total, true,
-                                       s->opts.keep_fp32_copy != 0, &t);
+                                       s->opts.keep_fp32_copy != 0, false, &t);
         t.chunk_slice = nullptr;
         return r;
     }();
@@ -504,7 +521,7 @@ int build_sliced(cgb_session *s, int grid)
     return CGB_OK;
 }
 
-// Sliced copies of F and F^T (FP32) with interleaved row ownership, built on
+// Sliced copies of F and F^T (BF16 values) with interleaved row ownership, built on
 // first use by the preconditioned solver after each change of F or of A's
 // layout.  F^T rows ascend by construction; F rows are sorted by the setter.
 int ensure_prec_slices(cgb_session *s)
@@ -542,7 +559,8 @@ int ensure_prec_slices(cgb_session *s)
         if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
         if (e != cudaSuccess) st = set_error(CGB_ERR_CUDA, "factor slices: %s", cudaGetErrorString(e));
         else if (unsorted) st = set_error(CGB_ERR_STATE, "factor rows not in ascending column order");
-        else st = fill_set<float>(s, grid, true, seg, cols[m], vals[m], total, false, true, sets[m]);
+        else st = fill_set<float>(s, grid, true, seg, cols[m], vals[m], total, false, false, true,
+                                  sets[m]);
     }
     dev_free(seg);
     if (st) {
@@ -578,17 +596,19 @@ bool make_plan(cgb_session *s, int kind, int lpr, Plan *pl)
         P.mixed = outer_step_mixed_sliced;
         P.pcg = outer_step_pcg_sliced;
         P.spmv = spmv_dot_sliced;
+        P.spmv32 = spmv_dot_sliced32;
         P.block = kSlicedBlock;
         P.block_mixed = kSlicedMixedBlock;
         P.block_pcg = kSlicedPcgBlock;
         const int grid = std::min(s->prop.multiProcessorCount, s->n);
         if (s->sliced_grid != grid && build_sliced(s, grid) != CGB_OK) return false;
-        P.smem = sliced_smem_bytes(s->sliced_max_rows);
+        P.smem = sliced_smem_bytes(s->sliced_max_rows, s->sliced_nacc);
         for (OuterKernel k : {P.fp64, P.mixed, P.pcg})
             if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)))
                 return false;
-        if (cudaFuncSetAttribute(P.spmv, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)))
-            return false;
+        for (SpmvKernel k : {P.spmv, P.spmv32})
+            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)))
+                return false;
     } else {
         return false;
     }
@@ -643,10 +663,11 @@ int time_plan_spmv(cgb_session *s, int reps, int fp32, double *ms_out)
     if (fp32) {
         to_fp32<<<s->prop.multiProcessorCount, 256, 0, s->stream>>>(s->p(), s->d_p32, s->n + 1);
     }
-    for (int i = 0; i < 2; i++) P.spmv<<<P.grid, P.block, P.smem, s->stream>>>(S);
+    const SpmvKernel k = fp32 ? P.spmv32 : P.spmv;
+    for (int i = 0; i < 2; i++) k<<<P.grid, P.block, P.smem, s->stream>>>(S);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaEventRecord(s->ev0, s->stream));
-    for (int i = 0; i < reps; i++) P.spmv<<<P.grid, P.block, P.smem, s->stream>>>(S);
+    for (int i = 0; i < reps; i++) k<<<P.grid, P.block, P.smem, s->stream>>>(S);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaEventRecord(s->ev1, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));

@@ -30,6 +30,8 @@
 //                  end -- deterministic.
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include "device_common.cuh"
 
 namespace cgb {
@@ -44,6 +46,15 @@ template <>
 struct Pair<float> {
     using T = float2;
 };
+template <>
+struct Pair<__nv_bfloat16> {
+    using T = __nv_bfloat162;
+};
+
+// Stored value -> arithmetic type (BF16 values widen exactly to FP32).
+__device__ __forceinline__ double widen(double v) { return v; }
+__device__ __forceinline__ float widen(float v) { return v; }
+__device__ __forceinline__ float widen(__nv_bfloat16 v) { return __bfloat162float(v); }
 
 __device__ __forceinline__ double fma_vt(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float fma_vt(float a, float b, float c) { return fmaf(a, b, c); }
@@ -64,6 +75,7 @@ struct SliceSet {
     unsigned *off = nullptr;          // first entry per slice, + total
     double *sval = nullptr;           // FP64 values
     float *sval32 = nullptr;          // FP32 values
+    __nv_bfloat16 *sval16 = nullptr;  // BF16 values
     unsigned short *scol = nullptr;   // local columns
     int *chunk_slice = nullptr;       // own chunk table (null: the session's)
     int interleaved = 0;              // rows owned round-robin by the CTAs
@@ -79,6 +91,7 @@ struct MatrixView {
     // sliced layout
     const double *__restrict__ sval;   // FP64 values, slice order
     const float *__restrict__ sval32;  // FP32 values, slice order
+    const __nv_bfloat16 *__restrict__ sval16;  // BF16 values, slice order (factor copies)
     const unsigned short *__restrict__ scol;  // column - b*W
     const unsigned short *__restrict__ srow;  // local row per (slice, lane); 0xffff = none
     const unsigned *__restrict__ slice_off;   // first entry of each slice
@@ -89,6 +102,7 @@ struct MatrixView {
     int max_rows;                             // shared accumulator capacity
     int interleaved;                          // 0: CTA c owns its contiguous row range;
                                               // 1: CTA c owns rows c, c + G, c + 2G, ...
+    int nacc;                                 // accumulators in shared memory (2 or 4)
 };
 
 // Rows of CTA `c` of `grid` under interleaved ownership.
@@ -109,6 +123,11 @@ template <>
 __device__ __forceinline__ const double *slice_values<double>(const MatrixView &M) { return M.sval; }
 template <>
 __device__ __forceinline__ const float *slice_values<float>(const MatrixView &M) { return M.sval32; }
+template <>
+__device__ __forceinline__ const __nv_bfloat16 *slice_values<__nv_bfloat16>(const MatrixView &M)
+{
+    return M.sval16;
+}
 
 // ------------------------------------------------------------ row policy
 template <int LPR, typename VT>
@@ -237,24 +256,37 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, long l
     return true;
 }
 
-// Bytes of one staging slot and dynamic shared memory of the sliced policy.
+// Staging and dynamic shared memory of the sliced policy: 192 KB of vector
+// staging (2 slots of 12288 doubles, or up to 4 slots of 12288 floats) and
+// one accumulator of max_rows doubles per slot in use.
 constexpr int kSliceWidth = 12288;  // columns per block
-constexpr unsigned kSlotBytes = kSliceWidth * 8u;
-__host__ __device__ inline size_t sliced_smem_bytes(int max_rows)
+constexpr size_t kStagingBytes = 2 * size_t(12288) * 8;
+constexpr int kMaxSlots = 4;
+__host__ __device__ inline size_t sliced_smem_bytes(int max_rows, int nacc)
 {
-    return 2 * size_t(kSlotBytes) + 2 * size_t(max_rows) * sizeof(double) + 128;
+    return kStagingBytes + size_t(nacc) * size_t(max_rows) * sizeof(double) + 128;
 }
 
 // kU64 / kU32: step pairs in flight per lane for FP64 / FP32 values (more
-// for kernels with fewer, register-richer threads).
+// for kernels with fewer, register-richer threads); BF16 values take twice
+// the FP32 count.
+//
+// Pipeline: a block of the vector is staged by one bulk copy into a slot
+// (S slots: 2 for an FP64 vector, M.nacc for an FP32 one); warps walk the
+// blocks independently and the last warp done with block b refills its slot
+// with block b + S, so warps may spread over S consecutive blocks and each
+// slot has its own row accumulator (summed in a fixed order at the end).
+// With an FP32 vector a warp reads its first slice's metadata of a block
+// before waiting for the block's copy, and the next slice's metadata while
+// it works on the current one.
 template <int kU64, int kU32, bool kOutline = false>
 struct SlicedSpmvT {
     static constexpr bool kSliced = true;
     int row0, row1, chunk0;  // chunk0 = blockIdx.x * nblk
-    unsigned char *buf;      // 2 slots
-    double *acc0, *acc1;     // max_rows each
-    uint64_t *bars;          // 2 "full" barriers
-    int *cnt;                // 2 per-slot completion counters
+    unsigned char *buf;      // kStagingBytes of staging
+    double *acc;             // nacc accumulators of max_rows
+    uint64_t *bars;          // kMaxSlots "full" barriers
+    int *cnt;                // kMaxSlots per-slot completion counters
     int *abort;
     unsigned parity;         // bit i: next phase parity of slot i
 
@@ -265,16 +297,16 @@ struct SlicedSpmvT {
         row1 = r1;
         chunk0 = blockIdx.x * M.nblk;
         buf = sliced_smem;
-        acc0 = reinterpret_cast<double *>(sliced_smem + 2 * size_t(kSlotBytes));
-        acc1 = acc0 + M.max_rows;
-        bars = reinterpret_cast<uint64_t *>(acc1 + M.max_rows);
-        cnt = reinterpret_cast<int *>(bars + 2);
-        abort = cnt + 2;
+        acc = reinterpret_cast<double *>(sliced_smem + kStagingBytes);
+        bars = reinterpret_cast<uint64_t *>(acc + size_t(M.nacc) * M.max_rows);
+        cnt = reinterpret_cast<int *>(bars + kMaxSlots);
+        abort = cnt + kMaxSlots;
         parity = 0;
         if (threadIdx.x == 0) {
-            mbar_init(&bars[0], 1);
-            mbar_init(&bars[1], 1);
-            cnt[0] = cnt[1] = 0;
+            for (int i = 0; i < kMaxSlots; i++) {
+                mbar_init(&bars[i], 1);
+                cnt[i] = 0;
+            }
             *abort = 0;
         }
         __syncthreads();
@@ -285,36 +317,44 @@ struct SlicedSpmvT {
     {
         const int cols = min(M.width, n - b * M.width);
         const unsigned bytes = (unsigned(cols) * unsigned(sizeof(VT)) + 15u) & ~15u;
-        bulk_load(buf + size_t(slot) * kSlotBytes, v + size_t(b) * M.width, bytes, &bars[slot]);
+        bulk_load(buf + size_t(slot) * M.width * sizeof(VT), v + size_t(b) * M.width, bytes,
+                  &bars[slot]);
     }
 
     // kOutline: the SpMV is a called function with its own register budget
     // (for kernels whose solver state would otherwise crowd the SpMV loop).
-    template <typename VT>
+    // VT: the gathered vector and the row sums; ST: the stored values
+    // (VT, or BF16 under an FP32 vector).
+    template <typename VT, typename ST = VT>
     __device__ __forceinline__ double apply(const MatrixView &M, const VT *v, double *out,
                                             const double *dotv, int n, long long limit_ns,
                                             int *status, bool &ok)
     {
-        if constexpr (kOutline) return apply_outlined<VT>(M, v, out, dotv, n, limit_ns, status, ok);
-        else return apply_body<VT>(M, v, out, dotv, n, limit_ns, status, ok);
+        if constexpr (kOutline)
+            return apply_outlined<VT, ST>(M, v, out, dotv, n, limit_ns, status, ok);
+        else return apply_body<VT, ST>(M, v, out, dotv, n, limit_ns, status, ok);
     }
 
-    template <typename VT>
+    template <typename VT, typename ST>
     __device__ __noinline__ double apply_outlined(const MatrixView &M, const VT *v, double *out,
                                                   const double *dotv, int n, long long limit_ns,
                                                   int *status, bool &ok)
     {
-        return apply_body<VT>(M, v, out, dotv, n, limit_ns, status, ok);
+        return apply_body<VT, ST>(M, v, out, dotv, n, limit_ns, status, ok);
     }
 
-    template <typename VT>
+    template <typename VT, typename ST>
     __device__ __forceinline__ double apply_body(const MatrixView &M, const VT *v, double *out,
                                                  const double *dotv, int n, long long limit_ns,
                                                  int *status, bool &ok)
     {
-        using P2 = typename Pair<VT>::T;
-        constexpr int kU = sizeof(VT) == 8 ? kU64 : kU32;
-        const VT *__restrict__ vals = slice_values<VT>(M);
+        using P2 = typename Pair<ST>::T;
+        constexpr int kU = sizeof(ST) == 8 ? kU64 : sizeof(ST) == 4 ? kU32 : 2 * kU32;
+        const ST *__restrict__ vals = slice_values<ST>(M);
+        // slots in use: as many blocks of the vector as the staging holds,
+        // at most one accumulator each
+        const int S = min(M.nacc, int(kStagingBytes / (size_t(M.width) * sizeof(VT))));
+        const size_t slot_bytes = size_t(M.width) * sizeof(VT);
         const int lane = threadIdx.x & 31;
         const int warp = threadIdx.x >> 5;
         const int nwarps = blockDim.x >> 5;
@@ -322,36 +362,23 @@ struct SlicedSpmvT {
         const int base = M.interleaved ? int(blockIdx.x) : row0;
         const int stride = M.interleaved ? int(gridDim.x) : 1;
         const int nrows = M.interleaved ? interleaved_rows(n, blockIdx.x, gridDim.x) : row1 - row0;
-        for (int i = threadIdx.x; i < nrows; i += blockDim.x) {
-            acc0[i] = 0.0;
-            acc1[i] = 0.0;
-        }
+        for (int i = threadIdx.x; i < S * M.max_rows; i += blockDim.x) acc[i] = 0.0;
         if (threadIdx.x == 0) {
             fence_proxy_async();  // v was written by generic stores before the grid barrier
-            issue(M, v, n, 0, 0);
-            if (M.nblk > 1) issue(M, v, n, 1, 1);
+            for (int b = 0; b < S && b < M.nblk; b++) issue(M, v, n, b, b);
         }
         __syncthreads();
         bool failed = false;
         for (int b = 0; b < M.nblk && !failed; b++) {
-            const int slot = b & 1;
-            if (!mbar_wait(&bars[slot], (parity >> slot) & 1u, limit_ns, abort)) {
-                failed = true;
-                *abort = 1;
-                break;
-            }
-            parity ^= 1u << slot;
-            const VT *pv = reinterpret_cast<const VT *>(buf + size_t(slot) * kSlotBytes);
-            double *accb = (b & 1) ? acc1 : acc0;
+            const int slot = b % S;
             const int s0 = __ldg(M.chunk_slice + chunk0 + b);
             const int s1 = __ldg(M.chunk_slice + chunk0 + b + 1);
             // rotate the warp -> slice assignment from block to block so the
             // widest slices do not always land on the same warps
             const int rot = (b * 7) % nwarps;
-            for (int s = s0 + (warp + rot) % nwarps; s < s1; s += nwarps) {
-                const unsigned off = __ldg(M.slice_off + s) + 2u * lane;
-                const int wp = __ldg(M.slice_width + s) >> 1;
-                const unsigned short row = __ldg(M.srow + size_t(s) * 32 + lane);
+            // one slice: lane `lane` of slice entries at off, wp step pairs
+            auto run_slice = [&](unsigned off, int wp, unsigned short row, const VT *pv,
+                                 double *accb) {
                 VT sum = VT(0);
                 for (int m = 0; m < wp; m += kU) {
                     P2 av[kU];
@@ -367,21 +394,69 @@ struct SlicedSpmvT {
 #pragma unroll
                     for (int u = 0; u < kU; u++) {
                         if (m + u < wp) {
-                            sum = fma_vt(av[u].x, pv[cv[u].x], sum);
-                            sum = fma_vt(av[u].y, pv[cv[u].y], sum);
+                            sum = fma_vt(VT(widen(av[u].x)), pv[cv[u].x], sum);
+                            sum = fma_vt(VT(widen(av[u].y)), pv[cv[u].y], sum);
                         }
                     }
                 }
                 if (row != 0xffffu) accb[row] += double(sum);
+            };
+            const VT *pv = reinterpret_cast<const VT *>(buf + size_t(slot) * slot_bytes);
+            double *accb = acc + size_t(slot) * M.max_rows;
+            if constexpr (sizeof(VT) == 8) {
+                // FP64 vector: long slices, the plain walk measures fastest
+                if (!mbar_wait(&bars[slot], (parity >> slot) & 1u, limit_ns, abort)) {
+                    failed = true;
+                    *abort = 1;
+                    break;
+                }
+                parity ^= 1u << slot;
+                for (int s = s0 + (warp + rot) % nwarps; s < s1; s += nwarps)
+                    run_slice(__ldg(M.slice_off + s) + 2u * lane, __ldg(M.slice_width + s) >> 1,
+                              __ldg(M.srow + size_t(s) * 32 + lane), pv, accb);
+            } else {
+                // FP32 vector: the first slice's metadata before the wait,
+                // the next slice's while the current one streams
+                int s = s0 + (warp + rot) % nwarps;
+                unsigned off = 0;
+                int wp = 0;
+                unsigned short row = 0xffffu;
+                if (s < s1) {
+                    off = __ldg(M.slice_off + s) + 2u * lane;
+                    wp = __ldg(M.slice_width + s) >> 1;
+                    row = __ldg(M.srow + size_t(s) * 32 + lane);
+                }
+                if (!mbar_wait(&bars[slot], (parity >> slot) & 1u, limit_ns, abort)) {
+                    failed = true;
+                    *abort = 1;
+                    break;
+                }
+                parity ^= 1u << slot;
+                while (s < s1) {
+                    const int sn = s + nwarps;
+                    unsigned offn = 0;
+                    int wpn = 0;
+                    unsigned short rown = 0xffffu;
+                    if (sn < s1) {
+                        offn = __ldg(M.slice_off + sn) + 2u * lane;
+                        wpn = __ldg(M.slice_width + sn) >> 1;
+                        rown = __ldg(M.srow + size_t(sn) * 32 + lane);
+                    }
+                    run_slice(off, wp, row, pv, accb);
+                    s = sn;
+                    off = offn;
+                    wp = wpn;
+                    row = rown;
+                }
             }
             __syncwarp();
             if (lane == 0) {
                 __threadfence_block();
                 if (atomicAdd(&cnt[slot], 1) == nwarps - 1) {
                     cnt[slot] = 0;
-                    if (b + 2 < M.nblk) {
+                    if (b + S < M.nblk) {
                         fence_proxy_async();  // all warps' reads of the slot before the refill
-                        issue(M, v, n, b + 2, slot);
+                        issue(M, v, n, b + S, slot);
                     }
                 }
             }
@@ -392,15 +467,15 @@ struct SlicedSpmvT {
                 raise_status(status, kDevTimeout);
                 // let issued copies land before the CTA leaves (a completed
                 // phase returns at once)
-                (void)mbar_wait(&bars[0], (parity & 1u), limit_ns, nullptr);
-                (void)mbar_wait(&bars[1], (parity >> 1) & 1u, limit_ns, nullptr);
+                for (int i = 0; i < S; i++) (void)mbar_wait(&bars[i], (parity >> i) & 1u, limit_ns, nullptr);
             }
             __syncthreads();
             return 0.0;
         }
         double dacc = 0.0;
         for (int i = threadIdx.x; i < nrows; i += blockDim.x) {
-            const double t = acc0[i] + acc1[i];
+            double t = acc[i];
+            for (int k = 1; k < S; k++) t += acc[size_t(k) * M.max_rows + i];
             const int row = base + i * stride;
             out[row] = t;
             if (dotv) dacc = fma(dotv[row], t, dacc);

@@ -75,7 +75,8 @@ class SolveParams(ctypes.Structure):
 
 class BatchParams(ctypes.Structure):
     _fields_ = [("niter", ctypes.c_int), ("mode", ctypes.c_int), ("cgitmax", ctypes.c_int),
-                ("tol", ctypes.c_double), ("refresh_every", ctypes.c_int)]
+                ("tol", ctypes.c_double), ("refresh_every", ctypes.c_int),
+                ("recycle", ctypes.c_int)]
 
 
 class SolveResult(ctypes.Structure):
@@ -539,14 +540,17 @@ class Batch:
     def __exit__(self, *exc):
         self.close()
 
-    def _params(self, niter, mode, cgitmax, tol, refresh_every):
+    def _params(self, niter, mode, cgitmax, tol, refresh_every, recycle=4):
         P = BatchParams()
         lib().cgb_default_batch_params(ctypes.byref(P))
         P.niter, P.mode, P.cgitmax, P.tol, P.refresh_every = niter, mode, cgitmax, tol, refresh_every
+        P.recycle = recycle
         return P
 
-    def solve(self, niter=15, mode=MODE_FP64, cgitmax=25, tol=1e-12, refresh_every=10):
-        P = self._params(niter, mode, cgitmax, tol, refresh_every)
+    def solve(self, niter=15, mode=MODE_FP64, cgitmax=25, tol=1e-12, refresh_every=10,
+              recycle=4):
+        """`recycle`: Galerkin start on that many previous iterates (MIXED)."""
+        P = self._params(niter, mode, cgitmax, tol, refresh_every, recycle)
         z, rn = np.zeros(self.nsys), np.zeros(self.nsys)
         it, st = np.zeros(self.nsys, np.int32), np.zeros(self.nsys, np.int32)
         ms = ctypes.c_double()

@@ -85,6 +85,30 @@ def test_batch_fallback_is_the_reference_algorithm(cgb):
     assert np.array_equal(mixed["iters"], judge["iters"])
 
 
+def test_batch_galerkin_start(cgb):
+    """The mixed mode's Galerkin start on previous iterates: the same
+    answers (within 1e-10 of the FP64 judge where it converged) with fewer
+    inner iterations than a start from z = 0."""
+    specs = cgb.batch_config5(nsys=32, seed=5, n_range=(1400, 9000))
+    systems, shifts = build(cgb, specs)
+    with cgb.Batch(systems, shifts) as b:
+        judge = b.solve(niter=15)
+        cold = b.solve(niter=15, mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=200, recycle=0)
+        warm = b.solve(niter=15, mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=200, recycle=4)
+    conv = judge["rnorm"] <= 1e-10
+    for out in (cold, warm):
+        ok = conv & (out["status"] == 0)
+        rel = np.abs(out["zeta"] - judge["zeta"]) / np.abs(judge["zeta"])
+        assert np.all(rel[ok] <= 1e-10), rel[ok].max()
+        fell = out["status"] == 1
+        assert np.array_equal(out["zeta"][fell], judge["zeta"][fell])
+    both = (cold["status"] == 0) & (warm["status"] == 0)
+    assert both.sum() >= 8
+    print(f"\nbatch inner iterations, z0 = 0 / Galerkin start: {cold['iters'][both].sum()} / "
+          f"{warm['iters'][both].sum()}")
+    assert warm["iters"][both].sum() < cold["iters"][both].sum()
+
+
 def test_batch_tune_keeps_results(cgb):
     """Retuning changes lanes per row and block shape, hence the order of
     the row sums; converged systems keep zeta to 1e-10."""

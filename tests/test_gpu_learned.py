@@ -206,8 +206,9 @@ def test_learned_gain_over_method_without_it(cgb):
 
 def test_learned_sliced_plan_matches_row_plan(cgb, golden):
     """Class B with the trained factor under both SpMV policies: the sliced
-    plan applies F and F^T through their own sliced copies, the row plan
-    through CSR rows; both reach the reference zeta trace."""
+    plan applies F and F^T through their own sliced copies (BF16 values,
+    interleaved rows), the row plan through FP32 CSR rows; both reach the
+    reference zeta trace."""
     model, how = trained_model(cgb)
     n, nonzer, niter, shift = PARAMS["B"]
     rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
@@ -220,8 +221,9 @@ def test_learned_sliced_plan_matches_row_plan(cgb, golden):
             out = s.power_iterate(niter, shift, mode=cgb.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=200)
         assert np.max(np.abs(out["zeta"] - zr) / np.abs(zr)) <= 1e-10, (kind, how)
         iters[kind] = out["total_inner"]
-    # same mathematics, FP32 sums in another order: iteration counts agree closely
-    assert abs(iters[1] - iters[2]) <= 0.05 * iters[1], iters
+    # same mathematics (the sliced copies hold F in BF16, the row plan in
+    # FP32): iteration counts agree closely
+    assert abs(iters[1] - iters[2]) <= 0.15 * iters[1], iters
 
 
 def test_factor_rows_sorted_and_merged(cgb):
