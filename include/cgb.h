@@ -62,6 +62,16 @@ long long cgb_nz_bound(int n, int nonzer);
 int cgb_makea(int n, int nonzer, double rcond, double shift, double seed, int *rowstr,
               int *colidx, double *a, long long nz_capacity, long long *nnz_out);
 
+/* cgb_makea with the assembly -- the n*(nonzer+1)^2 outer-product
+ * contributions, their per-row sort and in-order duplicate sums
+ * (sparse(), cg.cu:1611-1785) -- on CUDA device `device`; the vectors
+ * (sprnvc/vecset, one sequential LCG stream) are drawn on the host.  Same
+ * arguments, outputs and bit-identical result as cgb_makea; nonzer <= 31.
+ * CGB_ERR_CAPACITY also when one row has more than 2048 contributions. */
+int cgb_makea_device(int device, int n, int nonzer, double rcond, double shift, double seed,
+                     int *rowstr, int *colidx, double *a, long long nz_capacity,
+                     long long *nnz_out);
+
 /* --------------------------------------------------------------- session */
 typedef struct cgb_session cgb_session;
 

@@ -1,6 +1,8 @@
 // cgb_internal.h -- shared host-side declarations of libcgb.
 #pragma once
 
+#include <vector>
+
 #include "../../include/cgb.h"
 
 namespace cgb {
@@ -15,5 +17,18 @@ bool valid_seed(double seed);
 // Generator (makea.cpp).
 int makea(int n, int nonzer, double rcond, double shift, double seed, int *rowstr, int *colidx,
           double *a, long long cap, long long *nnz_out);
+
+// The n sparse vectors of the generator (sprnvc + vecset, cg.cu:1798-1857):
+// vector i has count[i] <= width entries at 0-based positions pos[i*width +
+// t] with values val[i*width + t]; scale[i] is its geometric weight
+// (cg.cu:1695, :1755).  Shared by the host and the GPU assembly.
+struct GenVectors {
+    int width = 0;                // nonzer + 1
+    std::vector<int> count;
+    std::vector<int> pos;
+    std::vector<double> val;
+    std::vector<double> scale;
+};
+int draw_generator_vectors(int n, int nonzer, double rcond, double seed, GenVectors &v);
 
 }  // namespace cgb

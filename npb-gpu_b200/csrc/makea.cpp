@@ -44,12 +44,7 @@ struct Lcg46 {
     }
 };
 
-struct Vectors {
-    int width = 0;                // nonzer + 1
-    std::vector<int> count;       // entries per vector (arow)
-    std::vector<int> pos;         // 0-based positions, width per vector (acol)
-    std::vector<double> val;      // values (aelt)
-};
+using Vectors = GenVectors;  // count = arow, pos = acol (0-based), val = aelt
 
 // n sparse vectors: nonzer distinct random positions with random values
 // (sprnvc, cg.cu:1798-1833) and position i forced to 0.5 (vecset,
@@ -181,6 +176,28 @@ unsigned worker_count(int n)
 
 }  // namespace
 
+int draw_generator_vectors(int n, int nonzer, double rcond, double seed, GenVectors &v)
+{
+    if (n < 2 || nonzer < 1 || nonzer >= n)
+        return set_error(CGB_ERR_INVALID, "makea: need n >= 2, 1 <= nonzer < n");
+    if (!valid_seed(seed))
+        return set_error(CGB_ERR_INVALID, "makea: seed must be an odd integer in (1, 2^46)");
+    try {
+        draw_vectors(n, nonzer, uint64_t(seed), v);
+        // geometric scale per vector: size *= ratio after each (cg.cu:1695, :1755)
+        v.scale.resize(n);
+        const double ratio = std::pow(rcond, 1.0 / double(n));
+        double size = 1.0;
+        for (int i = 0; i < n; i++) {
+            v.scale[i] = size;
+            size = size * ratio;
+        }
+    } catch (const std::bad_alloc &) {
+        return set_error(CGB_ERR_NOMEM, "makea: host allocation failed");
+    }
+    return CGB_OK;
+}
+
 bool valid_seed(double seed)
 {
     if (!(seed > 1.0) || !(seed < 70368744177664.0)) return false;  // (1, 2^46)
@@ -199,16 +216,9 @@ int makea(int n, int nonzer, double rcond, double shift, double seed, int *rowst
         return set_error(CGB_ERR_INVALID, "makea: rcond must be > 0 and shift finite");
     try {
         Vectors v;
-        draw_vectors(n, nonzer, uint64_t(seed), v);
-
-        // geometric scale per vector: size *= ratio after each (cg.cu:1695, :1755)
-        std::vector<double> scale_of(n);
-        const double ratio = std::pow(rcond, 1.0 / double(n));
-        double size = 1.0;
-        for (int i = 0; i < n; i++) {
-            scale_of[i] = size;
-            size = size * ratio;
-        }
+        const int vst = draw_generator_vectors(n, nonzer, rcond, seed, v);
+        if (vst) return vst;
+        const std::vector<double> &scale_of = v.scale;
 
         // contributions per row (cg.cu:1649-1662) and their offsets
         std::vector<long long> slot(size_t(n) + 1, 0);

@@ -279,7 +279,7 @@ __host__ __device__ inline size_t sliced_smem_bytes(int max_rows, int nacc)
 // With an FP32 vector a warp reads its first slice's metadata of a block
 // before waiting for the block's copy, and the next slice's metadata while
 // it works on the current one.
-template <int kU64, int kU32, bool kOutline = false>
+template <int kU64, int kU32, bool kOutline = false, bool kDual = false>
 struct SlicedSpmvT {
     static constexpr bool kSliced = true;
     int row0, row1, chunk0;  // chunk0 = blockIdx.x * nblk
@@ -414,6 +414,78 @@ struct SlicedSpmvT {
                 for (int s = s0 + (warp + rot) % nwarps; s < s1; s += nwarps)
                     run_slice(__ldg(M.slice_off + s) + 2u * lane, __ldg(M.slice_width + s) >> 1,
                               __ldg(M.srow + size_t(s) * 32 + lane), pv, accb);
+            } else if constexpr (kDual) {
+                // FP32 vector, two slices a warp at once (s and s + nwarps):
+                // short slices put twice the loads in flight per latency
+                auto meta = [&](int t, unsigned &o, int &w, unsigned short &r) {
+                    if (t < s1) {
+                        o = __ldg(M.slice_off + t) + 2u * lane;
+                        w = __ldg(M.slice_width + t) >> 1;
+                        r = __ldg(M.srow + size_t(t) * 32 + lane);
+                    } else {
+                        o = 0;
+                        w = 0;
+                        r = 0xffffu;
+                    }
+                };
+                int s = s0 + (warp + rot) % nwarps;
+                unsigned offA, offB;
+                int wpA, wpB;
+                unsigned short rowA, rowB;
+                meta(s, offA, wpA, rowA);
+                meta(s + nwarps, offB, wpB, rowB);
+                if (!mbar_wait(&bars[slot], (parity >> slot) & 1u, limit_ns, abort)) {
+                    failed = true;
+                    *abort = 1;
+                    break;
+                }
+                parity ^= 1u << slot;
+                while (s < s1) {
+                    const int sn = s + 2 * nwarps;
+                    unsigned offC, offD;
+                    int wpC, wpD;
+                    unsigned short rowC, rowD;
+                    meta(sn, offC, wpC, rowC);
+                    meta(sn + nwarps, offD, wpD, rowD);
+                    VT sa = VT(0), sb = VT(0);
+                    const int wmax = max(wpA, wpB);
+                    for (int m = 0; m < wmax; m += kU) {
+                        P2 aa[kU], ab[kU];
+                        ushort2 ca[kU], cb[kU];
+#pragma unroll
+                        for (int u = 0; u < kU; u++) {
+                            const unsigned step = 64u * unsigned(m + u);
+                            if (m + u < wpA) {
+                                aa[u] = __ldcs(reinterpret_cast<const P2 *>(vals + offA + step));
+                                ca[u] = __ldcs(reinterpret_cast<const ushort2 *>(M.scol + offA + step));
+                            }
+                            if (m + u < wpB) {
+                                ab[u] = __ldcs(reinterpret_cast<const P2 *>(vals + offB + step));
+                                cb[u] = __ldcs(reinterpret_cast<const ushort2 *>(M.scol + offB + step));
+                            }
+                        }
+#pragma unroll
+                        for (int u = 0; u < kU; u++) {
+                            if (m + u < wpA) {
+                                sa = fma_vt(VT(widen(aa[u].x)), pv[ca[u].x], sa);
+                                sa = fma_vt(VT(widen(aa[u].y)), pv[ca[u].y], sa);
+                            }
+                            if (m + u < wpB) {
+                                sb = fma_vt(VT(widen(ab[u].x)), pv[cb[u].x], sb);
+                                sb = fma_vt(VT(widen(ab[u].y)), pv[cb[u].y], sb);
+                            }
+                        }
+                    }
+                    if (rowA != 0xffffu) accb[rowA] += double(sa);
+                    if (rowB != 0xffffu) accb[rowB] += double(sb);
+                    s = sn;
+                    offA = offC;
+                    wpA = wpC;
+                    rowA = rowC;
+                    offB = offD;
+                    wpB = wpD;
+                    rowB = rowD;
+                }
             } else {
                 // FP32 vector: the first slice's metadata before the wait,
                 // the next slice's while the current one streams

@@ -99,6 +99,9 @@ _SIGNATURES = {
     "cgb_makea": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                  ctypes.c_double, _I32, _I32, _F64, ctypes.c_longlong,
                                  ctypes.POINTER(ctypes.c_longlong)]),
+    "cgb_makea_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_double, _I32, _I32, _F64,
+                                        ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]),
     "cgb_default_options": (None, [ctypes.POINTER(Options)]),
     "cgb_create": (ctypes.c_int, [ctypes.c_int, _I32, _I32, _F64, ctypes.POINTER(Options),
                                   ctypes.POINTER(ctypes.c_void_p)]),
@@ -197,6 +200,19 @@ def makea(n, nonzer, rcond=RCOND, shift=10.0, seed=SEED):
     nnz = ctypes.c_longlong(0)
     _check(lib().cgb_makea(n, nonzer, rcond, shift, seed, rowstr, colidx, a, cap,
                            ctypes.byref(nnz)))
+    k = nnz.value
+    return rowstr, colidx[:k].copy(), a[:k].copy()
+
+
+def makea_device(n, nonzer, rcond=RCOND, shift=10.0, seed=SEED, device=0):
+    """makea with the assembly on the GPU (bit-identical to makea)."""
+    cap = nz_bound(n, nonzer)
+    rowstr = np.zeros(n + 1, np.int32)
+    colidx = np.zeros(max(cap, 1), np.int32)
+    a = np.zeros(max(cap, 1), np.float64)
+    nnz = ctypes.c_longlong(0)
+    _check(lib().cgb_makea_device(device, n, nonzer, rcond, shift, seed, rowstr, colidx, a, cap,
+                                  ctypes.byref(nnz)))
     k = nnz.value
     return rowstr, colidx[:k].copy(), a[:k].copy()
 
