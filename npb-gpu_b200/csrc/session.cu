@@ -254,6 +254,7 @@ void free_set(SliceSet &t)
     dev_free(t.scol);
     dev_free(t.chunk_slice);
     t.interleaved = 0;
+    t.block_cols = t.blocks = 0;
     t.entries = 0;
 }
 
@@ -320,8 +321,8 @@ void set_slices(cgb_session *s, const SliceSet &t, MatrixView *M)
     M->slice_off = t.off;
     M->slice_width = t.width;
     M->chunk_slice = t.chunk_slice ? t.chunk_slice : s->d_chunk_slice;
-    M->nblk = s->nblk;
-    M->width = kSliceWidth;
+    M->nblk = t.blocks ? t.blocks : s->nblk;
+    M->width = t.block_cols ? t.block_cols : kSliceWidth;
     M->max_rows = s->sliced_max_rows;
     M->nacc = s->sliced_nacc;
     M->interleaved = t.interleaved;
@@ -445,13 +446,15 @@ template <typename ST>
 int fill_set(cgb_session *s, int grid, bool interleave, const int *seg, const int *d_colidx,
              const ST *vals, int total, bool want64, bool want32, bool want16, SliceSet *t)
 {
-    const int nchunks = grid * s->nblk;
+    const int nblk = t->blocks ? t->blocks : s->nblk;
+    const int bcols = t->block_cols ? t->block_cols : kSliceWidth;
+    const int nchunks = grid * nblk;
     const int ig = interleave ? grid : 0;
     t->interleaved = interleave ? 1 : 0;
     if (dev_alloc(&t->srow, size_t(total) * 32) || dev_alloc(&t->width, size_t(total)) ||
         dev_alloc(&t->off, size_t(total) + 1))
         return set_error(CGB_ERR_NOMEM, "sliced layout: metadata allocation failed");
-    slice_sort_rows<<<nchunks, 256, 0, s->stream>>>(seg, s->seg_stride, s->nblk, s->d_split, ig,
+    slice_sort_rows<<<nchunks, 256, 0, s->stream>>>(seg, s->seg_stride, nblk, s->d_split, ig,
                                                    s->n, t->chunk_slice, t->srow, t->width);
     CUDA_TRY(cudaGetLastError());
     slice_offsets<<<1, 1024, 0, s->stream>>>(t->width, total, t->off);
@@ -467,7 +470,7 @@ int fill_set(cgb_session *s, int grid, bool interleave, const int *seg, const in
         (want16 && dev_alloc(&t->sval16, size_t(entries) + kPad)))
         return set_error(CGB_ERR_NOMEM, "sliced layout: %u entries do not fit", entries);
     slice_fill<ST><<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
-        seg, s->seg_stride, s->nblk, kSliceWidth, s->d_split, ig, t->chunk_slice, nchunks,
+        seg, s->seg_stride, nblk, bcols, s->d_split, ig, t->chunk_slice, nchunks,
         d_colidx, vals, t->srow, t->width, t->off, total, t->sval, t->sval32, t->sval16, t->scol);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(s->stream));
@@ -530,10 +533,13 @@ int ensure_prec_slices(cgb_session *s)
     if (s->prec_gen == s->layout_gen) return CGB_OK;
     free_prec_slices(s);
     const int n = s->n, grid = s->sliced_grid;
+    // wider column blocks than A's: F and F^T hold half of A's entries a
+    // row, so fewer, fuller blocks keep the per-block latency down
+    const int bcols = kFactorBlockCols, blocks = (n + bcols - 1) / bcols;
     std::vector<int> chunk_slice;
-    const int total = chunk_table(grid, s->nblk, [&](int c) { return interleaved_rows(n, c, grid); },
+    const int total = chunk_table(grid, blocks, [&](int c) { return interleaved_rows(n, c, grid); },
                                   chunk_slice);
-    const size_t count = size_t(s->nblk + 1) * s->seg_stride;
+    const size_t count = size_t(blocks + 1) * s->seg_stride;
     int *seg = nullptr;
     if (dev_alloc(&seg, count) != cudaSuccess)
         return set_error(CGB_ERR_NOMEM, "factor segment table allocation failed");
@@ -543,6 +549,8 @@ int ensure_prec_slices(cgb_session *s)
     const float *vals[2] = {s->d_f_val, s->d_ft_val};
     SliceSet *sets[2] = {&s->sf, &s->sft};
     for (int m = 0; m < 2 && st == CGB_OK; m++) {
+        sets[m]->block_cols = bcols;
+        sets[m]->blocks = blocks;
         cudaError_t e = dev_alloc(&sets[m]->chunk_slice, chunk_slice.size());
         if (e == cudaSuccess)
             e = cudaMemcpy(sets[m]->chunk_slice, chunk_slice.data(), sizeof(int) * chunk_slice.size(),
@@ -550,7 +558,7 @@ int ensure_prec_slices(cgb_session *s)
         if (e == cudaSuccess) e = cudaMemsetAsync(s->d_flag, 0, sizeof(int), s->stream);
         if (e == cudaSuccess) {
             build_segments<<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
-                ptrs[m], cols[m], n, s->nblk, kSliceWidth, seg, s->seg_stride, s->d_flag);
+                ptrs[m], cols[m], n, blocks, bcols, seg, s->seg_stride, s->d_flag);
             e = cudaGetLastError();
         }
         int unsorted = 0;

@@ -79,6 +79,7 @@ struct SliceSet {
     unsigned short *scol = nullptr;   // local columns
     int *chunk_slice = nullptr;       // own chunk table (null: the session's)
     int interleaved = 0;              // rows owned round-robin by the CTAs
+    int block_cols = 0, blocks = 0;   // columns per block, blocks (0: the session's)
     long long entries = 0;            // padded entries
 };
 
@@ -260,6 +261,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, long l
 // staging (2 slots of 12288 doubles, or up to 4 slots of 12288 floats) and
 // one accumulator of max_rows doubles per slot in use.
 constexpr int kSliceWidth = 12288;  // columns per block
+constexpr int kFactorBlockCols = 24576;  // columns per block of the preconditioner's copies
 constexpr size_t kStagingBytes = 2 * size_t(12288) * 8;
 constexpr int kMaxSlots = 4;
 __host__ __device__ inline size_t sliced_smem_bytes(int max_rows, int nacc)
@@ -279,10 +281,10 @@ __host__ __device__ inline size_t sliced_smem_bytes(int max_rows, int nacc)
 // With an FP32 vector a warp reads its first slice's metadata of a block
 // before waiting for the block's copy, and the next slice's metadata while
 // it works on the current one.
-template <int kU64, int kU32, bool kOutline = false, bool kDual = false>
+template <int kU64, int kU32, bool kOutline = false>
 struct SlicedSpmvT {
     static constexpr bool kSliced = true;
-    int row0, row1, chunk0;  // chunk0 = blockIdx.x * nblk
+    int row0, row1;
     unsigned char *buf;      // kStagingBytes of staging
     double *acc;             // nacc accumulators of max_rows
     uint64_t *bars;          // kMaxSlots "full" barriers
@@ -295,7 +297,6 @@ struct SlicedSpmvT {
         extern __shared__ __align__(128) unsigned char sliced_smem[];
         row0 = r0;
         row1 = r1;
-        chunk0 = blockIdx.x * M.nblk;
         buf = sliced_smem;
         acc = reinterpret_cast<double *>(sliced_smem + kStagingBytes);
         bars = reinterpret_cast<uint64_t *>(acc + size_t(M.nacc) * M.max_rows);
@@ -355,6 +356,7 @@ struct SlicedSpmvT {
         // at most one accumulator each
         const int S = min(M.nacc, int(kStagingBytes / (size_t(M.width) * sizeof(VT))));
         const size_t slot_bytes = size_t(M.width) * sizeof(VT);
+        const int chunk0 = blockIdx.x * M.nblk;
         const int lane = threadIdx.x & 31;
         const int warp = threadIdx.x >> 5;
         const int nwarps = blockDim.x >> 5;
@@ -371,7 +373,7 @@ struct SlicedSpmvT {
         bool failed = false;
         for (int b = 0; b < M.nblk && !failed; b++) {
             const int slot = b % S;
-            const int s0 = __ldg(M.chunk_slice + chunk0 + b);
+            const int s0 = __ldg(M.chunk_slice + chunk0 + b);  // this matrix's blocks
             const int s1 = __ldg(M.chunk_slice + chunk0 + b + 1);
             // rotate the warp -> slice assignment from block to block so the
             // widest slices do not always land on the same warps
@@ -414,78 +416,6 @@ struct SlicedSpmvT {
                 for (int s = s0 + (warp + rot) % nwarps; s < s1; s += nwarps)
                     run_slice(__ldg(M.slice_off + s) + 2u * lane, __ldg(M.slice_width + s) >> 1,
                               __ldg(M.srow + size_t(s) * 32 + lane), pv, accb);
-            } else if constexpr (kDual) {
-                // FP32 vector, two slices a warp at once (s and s + nwarps):
-                // short slices put twice the loads in flight per latency
-                auto meta = [&](int t, unsigned &o, int &w, unsigned short &r) {
-                    if (t < s1) {
-                        o = __ldg(M.slice_off + t) + 2u * lane;
-                        w = __ldg(M.slice_width + t) >> 1;
-                        r = __ldg(M.srow + size_t(t) * 32 + lane);
-                    } else {
-                        o = 0;
-                        w = 0;
-                        r = 0xffffu;
-                    }
-                };
-                int s = s0 + (warp + rot) % nwarps;
-                unsigned offA, offB;
-                int wpA, wpB;
-                unsigned short rowA, rowB;
-                meta(s, offA, wpA, rowA);
-                meta(s + nwarps, offB, wpB, rowB);
-                if (!mbar_wait(&bars[slot], (parity >> slot) & 1u, limit_ns, abort)) {
-                    failed = true;
-                    *abort = 1;
-                    break;
-                }
-                parity ^= 1u << slot;
-                while (s < s1) {
-                    const int sn = s + 2 * nwarps;
-                    unsigned offC, offD;
-                    int wpC, wpD;
-                    unsigned short rowC, rowD;
-                    meta(sn, offC, wpC, rowC);
-                    meta(sn + nwarps, offD, wpD, rowD);
-                    VT sa = VT(0), sb = VT(0);
-                    const int wmax = max(wpA, wpB);
-                    for (int m = 0; m < wmax; m += kU) {
-                        P2 aa[kU], ab[kU];
-                        ushort2 ca[kU], cb[kU];
-#pragma unroll
-                        for (int u = 0; u < kU; u++) {
-                            const unsigned step = 64u * unsigned(m + u);
-                            if (m + u < wpA) {
-                                aa[u] = __ldcs(reinterpret_cast<const P2 *>(vals + offA + step));
-                                ca[u] = __ldcs(reinterpret_cast<const ushort2 *>(M.scol + offA + step));
-                            }
-                            if (m + u < wpB) {
-                                ab[u] = __ldcs(reinterpret_cast<const P2 *>(vals + offB + step));
-                                cb[u] = __ldcs(reinterpret_cast<const ushort2 *>(M.scol + offB + step));
-                            }
-                        }
-#pragma unroll
-                        for (int u = 0; u < kU; u++) {
-                            if (m + u < wpA) {
-                                sa = fma_vt(VT(widen(aa[u].x)), pv[ca[u].x], sa);
-                                sa = fma_vt(VT(widen(aa[u].y)), pv[ca[u].y], sa);
-                            }
-                            if (m + u < wpB) {
-                                sb = fma_vt(VT(widen(ab[u].x)), pv[cb[u].x], sb);
-                                sb = fma_vt(VT(widen(ab[u].y)), pv[cb[u].y], sb);
-                            }
-                        }
-                    }
-                    if (rowA != 0xffffu) accb[rowA] += double(sa);
-                    if (rowB != 0xffffu) accb[rowB] += double(sb);
-                    s = sn;
-                    offA = offC;
-                    wpA = wpC;
-                    rowA = rowC;
-                    offB = offD;
-                    wpB = wpD;
-                    rowB = rowD;
-                }
             } else {
                 // FP32 vector: the first slice's metadata before the wait,
                 // the next slice's while the current one streams
