@@ -30,62 +30,84 @@ __device__ __forceinline__ int gram_index(int a, int b)  // a <= b < v, packed b
 // W y is accurate to ~1e-14 of x).  Returns the number of directions kept.
 static __device__ __noinline__ int galerkin_solve(const double *g, int v, double *y)
 {
-    double N[kMaxRecycle][kMaxRecycle], c[kMaxRecycle];
-    for (int b = 0; b < v; b++) {
-        for (int a = 0; a <= b; a++) N[a][b] = N[b][a] = -g[gram_index(a, b)];
-        c[b] = g[kGramPairs + b];
+    constexpr int R = kMaxRecycle;
+    // every loop has the fixed trip count R and predicates on v, so the
+    // small arrays stay in registers; a left-out direction has zero L, u, y
+    double N[R][R], c[R];
+#pragma unroll
+    for (int b = 0; b < R; b++) {
+#pragma unroll
+        for (int a = 0; a <= b; a++) {
+            const double e = (b < v) ? -g[gram_index(a, b)] : 0.0;
+            N[a][b] = e;
+            N[b][a] = e;
+        }
+        c[b] = (b < v) ? g[kGramPairs + b] : 0.0;
     }
     if (!(N[0][0] > 0.0)) {
-        for (int a = 0; a < v; a++) y[a] = 0.0;
+#pragma unroll
+        for (int a = 0; a < R; a++)
+            if (a < v) y[a] = 0.0;
         return 0;
     }
     const double taus[4] = {1e-12, 1e-10, 1e-8, 1e-6};
+    double yy[R];
+    int kept = 1;
     for (int t = 0; t < 5; t++) {
         // t == 4: the first direction alone
         const double tau = t < 4 ? taus[t] * N[0][0] : 1e300;
-        double L[kMaxRecycle][kMaxRecycle], u[kMaxRecycle];
-        bool keep[kMaxRecycle];
-        int kept = 0;
-        for (int i = 0; i < v; i++) {
+        double L[R][R], u[R];
+        bool keep[R];
+        kept = 0;
+#pragma unroll
+        for (int i = 0; i < R; i++) {
             double d = N[i][i];
-            for (int k = 0; k < i; k++)
-                if (keep[k]) d -= L[i][k] * L[i][k];
-            keep[i] = (i == 0) || d > tau;
-            if (!keep[i]) continue;
-            kept++;
-            L[i][i] = sqrt(d);
-            for (int j = i + 1; j < v; j++) {
+#pragma unroll
+            for (int k = 0; k < i; k++) d -= L[i][k] * L[i][k];
+            keep[i] = (i < v) && ((i == 0) || d > tau);
+            kept += keep[i] ? 1 : 0;
+            const double lii = keep[i] ? sqrt(d) : 1.0;
+            L[i][i] = keep[i] ? lii : 0.0;
+#pragma unroll
+            for (int j = i + 1; j < R; j++) {
                 double e = N[j][i];
-                for (int k = 0; k < i; k++)
-                    if (keep[k]) e -= L[j][k] * L[i][k];
-                L[j][i] = e / L[i][i];
+#pragma unroll
+                for (int k = 0; k < i; k++) e -= L[j][k] * L[i][k];
+                L[j][i] = keep[i] ? e / lii : 0.0;
             }
+#pragma unroll
+            for (int j = 0; j < i; j++) L[j][i] = 0.0;
         }
         // N y = -c on the kept directions
-        for (int i = 0; i < v; i++) {
-            if (!keep[i]) { u[i] = 0.0; continue; }
+#pragma unroll
+        for (int i = 0; i < R; i++) {
             double e = -c[i];
-            for (int k = 0; k < i; k++)
-                if (keep[k]) e -= L[i][k] * u[k];
-            u[i] = e / L[i][i];
+#pragma unroll
+            for (int k = 0; k < i; k++) e -= L[i][k] * u[k];
+            u[i] = keep[i] ? e / L[i][i] : 0.0;
         }
-        for (int i = v - 1; i >= 0; i--) {
-            if (!keep[i]) { y[i] = 0.0; continue; }
+#pragma unroll
+        for (int i = R - 1; i >= 0; i--) {
             double e = u[i];
-            for (int j = i + 1; j < v; j++)
-                if (keep[j]) e -= L[j][i] * y[j];
-            y[i] = e / L[i][i];
+#pragma unroll
+            for (int j = i + 1; j < R; j++) e -= L[j][i] * yy[j];
+            yy[i] = keep[i] ? e / L[i][i] : 0.0;
         }
         // growth of the combination in the A-norm: sum |y_a| ||x_a||_A
         // against ||z0||_A; accept when the cancellation is mild
         double num = 0.0, zA = 0.0;
-        for (int a = 0; a < v; a++) {
-            num += fabs(y[a]) * sqrt(N[a][a]);
-            for (int b = 0; b < v; b++) zA += y[a] * N[a][b] * y[b];
+#pragma unroll
+        for (int a = 0; a < R; a++) {
+            num += (a < v) ? fabs(yy[a]) * sqrt(N[a][a]) : 0.0;
+#pragma unroll
+            for (int b = 0; b < R; b++) zA += yy[a] * N[a][b] * yy[b];
         }
-        if (t == 4 || (zA > 0.0 && num <= 100.0 * sqrt(zA) && isfinite(num))) return kept;
+        if (t == 4 || (zA > 0.0 && num <= 100.0 * sqrt(zA) && isfinite(num))) break;
     }
-    return 1;
+#pragma unroll
+    for (int a = 0; a < R; a++)
+        if (a < v) y[a] = yy[a];
+    return kept;
 }
 
 }  // namespace cgb

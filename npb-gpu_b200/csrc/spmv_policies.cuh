@@ -266,7 +266,7 @@ constexpr size_t kStagingBytes = 2 * size_t(12288) * 8;
 constexpr int kMaxSlots = 4;
 __host__ __device__ inline size_t sliced_smem_bytes(int max_rows, int nacc)
 {
-    return kStagingBytes + size_t(nacc) * size_t(max_rows) * sizeof(double) + 128;
+    return 128 + kStagingBytes + size_t(nacc) * size_t(max_rows) * sizeof(double);
 }
 
 // kU64 / kU32: step pairs in flight per lane for FP64 / FP32 values (more
@@ -284,31 +284,35 @@ __host__ __device__ inline size_t sliced_smem_bytes(int max_rows, int nacc)
 template <int kU64, int kU32, bool kOutline = false>
 struct SlicedSpmvT {
     static constexpr bool kSliced = true;
+    // Dynamic shared memory: the control words first (fixed offsets), then
+    // the staging, then the accumulators; every address is a constant offset
+    // from the array, so the policy keeps only three registers of state.
+    static constexpr size_t kCtrlBytes = 128;
     int row0, row1;
-    unsigned char *buf;      // kStagingBytes of staging
-    double *acc;             // nacc accumulators of max_rows
-    uint64_t *bars;          // kMaxSlots "full" barriers
-    int *cnt;                // kMaxSlots per-slot completion counters
-    int *abort;
     unsigned parity;         // bit i: next phase parity of slot i
 
-    __device__ void setup(const MatrixView &M, int r0, int r1)
+    __device__ static unsigned char *smem()
     {
         extern __shared__ __align__(128) unsigned char sliced_smem[];
+        return sliced_smem;
+    }
+    __device__ static uint64_t *bars() { return reinterpret_cast<uint64_t *>(smem()); }  // kMaxSlots
+    __device__ static int *cnt() { return reinterpret_cast<int *>(smem() + 8 * kMaxSlots); }
+    __device__ static int *abort_flag() { return cnt() + kMaxSlots; }
+    __device__ static unsigned char *buf() { return smem() + kCtrlBytes; }
+    __device__ static double *acc() { return reinterpret_cast<double *>(smem() + kCtrlBytes + kStagingBytes); }
+
+    __device__ void setup(const MatrixView &, int r0, int r1)
+    {
         row0 = r0;
         row1 = r1;
-        buf = sliced_smem;
-        acc = reinterpret_cast<double *>(sliced_smem + kStagingBytes);
-        bars = reinterpret_cast<uint64_t *>(acc + size_t(M.nacc) * M.max_rows);
-        cnt = reinterpret_cast<int *>(bars + kMaxSlots);
-        abort = cnt + kMaxSlots;
         parity = 0;
         if (threadIdx.x == 0) {
             for (int i = 0; i < kMaxSlots; i++) {
-                mbar_init(&bars[i], 1);
-                cnt[i] = 0;
+                mbar_init(&bars()[i], 1);
+                cnt()[i] = 0;
             }
-            *abort = 0;
+            *abort_flag() = 0;
         }
         __syncthreads();
     }
@@ -318,8 +322,8 @@ struct SlicedSpmvT {
     {
         const int cols = min(M.width, n - b * M.width);
         const unsigned bytes = (unsigned(cols) * unsigned(sizeof(VT)) + 15u) & ~15u;
-        bulk_load(buf + size_t(slot) * M.width * sizeof(VT), v + size_t(b) * M.width, bytes,
-                  &bars[slot]);
+        bulk_load(buf() + size_t(slot) * M.width * sizeof(VT), v + size_t(b) * M.width, bytes,
+                  &bars()[slot]);
     }
 
     // kOutline: the SpMV is a called function with its own register budget
@@ -364,6 +368,10 @@ struct SlicedSpmvT {
         const int base = M.interleaved ? int(blockIdx.x) : row0;
         const int stride = M.interleaved ? int(gridDim.x) : 1;
         const int nrows = M.interleaved ? interleaved_rows(n, blockIdx.x, gridDim.x) : row1 - row0;
+        double *const acc = SlicedSpmvT::acc();
+        uint64_t *const bars = SlicedSpmvT::bars();
+        int *const cnt = SlicedSpmvT::cnt();
+        int *const abort = abort_flag();
         for (int i = threadIdx.x; i < S * M.max_rows; i += blockDim.x) acc[i] = 0.0;
         if (threadIdx.x == 0) {
             fence_proxy_async();  // v was written by generic stores before the grid barrier
@@ -403,7 +411,7 @@ struct SlicedSpmvT {
                 }
                 if (row != 0xffffu) accb[row] += double(sum);
             };
-            const VT *pv = reinterpret_cast<const VT *>(buf + size_t(slot) * slot_bytes);
+            const VT *pv = reinterpret_cast<const VT *>(buf() + size_t(slot) * slot_bytes);
             double *accb = acc + size_t(slot) * M.max_rows;
             if constexpr (sizeof(VT) == 8) {
                 // FP64 vector: long slices, the plain walk measures fastest

@@ -148,16 +148,18 @@ def trained_model(cgb):
     return model, "short run"
 
 
-def test_learned_preconditioner_class_c_unseen_seed(cgb, golden):
+@pytest.mark.parametrize("tol", [1e-12, 1e-11])
+def test_learned_preconditioner_class_c_unseen_seed(cgb, golden, tol):
     """Config: train on other seeds, test at n=150000, nonzer=15, shift=110
     (the NPB seed, never used in training); FP64 plain CG (the reference
-    trace) judges zeta."""
+    trace) judges zeta: relative 1e-10 at every outer step, at the solver
+    tolerances the benchmark reports."""
     model, how = trained_model(cgb)
     n, nonzer, niter, shift = PARAMS["C"]
     rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
     with cgb.Session(rs, ci, a) as s, model.graph(rs, ci, a) as g:
         model.attach(g, s)
-        out = s.power_iterate(niter, shift, mode=cgb.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=200)
+        out = s.power_iterate(niter, shift, mode=cgb.MODE_MIXED_LEARNED, tol=tol, cgitmax=200)
     ref = golden["C"]["seeds"]["314159265.0"]
     zr = np.array(ref["zeta"])
     assert np.max(np.abs(out["zeta"] - zr) / np.abs(zr)) <= 1e-10, how
