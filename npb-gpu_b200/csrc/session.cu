@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "cg_kernels.cuh"
@@ -129,12 +130,39 @@ int validate_csr(int n, const int *rowstr, const int *colidx, const double *a)
         if (rowstr[j + 1] < rowstr[j])
             return set_error(CGB_ERR_BAD_MATRIX, "CSR: rowstr decreases at row %d", j);
     const long long nnz = rowstr[n];
-    for (long long k = 0; k < nnz; k++) {
+    // entries checked in parallel chunks; the first bad entry (lowest index)
+    // is reported, as a serial scan would
+    const long long kChunk = 1 << 20;
+    const long long nchunks = (nnz + kChunk - 1) / kChunk;
+    std::vector<long long> first_bad(size_t(std::max<long long>(nchunks, 1)), -1);
+    auto scan = [&](long long c0, long long c1) {
+        for (long long c = c0; c < c1; c++) {
+            const long long e = std::min(nnz, (c + 1) * kChunk);
+            for (long long k = c * kChunk; k < e; k++)
+                if (colidx[k] < 0 || colidx[k] >= n || !std::isfinite(a[k])) {
+                    first_bad[size_t(c)] = k;
+                    break;
+                }
+        }
+    };
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const long long nt = std::min<long long>(hw, nchunks);
+    if (nt <= 1) {
+        scan(0, nchunks);
+    } else {
+        std::vector<std::thread> pool;
+        for (long long t = 1; t < nt; t++)
+            pool.emplace_back(scan, nchunks * t / nt, nchunks * (t + 1) / nt);
+        scan(0, nchunks / nt);
+        for (auto &th : pool) th.join();
+    }
+    for (long long c = 0; c < nchunks; c++) {
+        const long long k = first_bad[size_t(c)];
+        if (k < 0) continue;
         if (colidx[k] < 0 || colidx[k] >= n)
             return set_error(CGB_ERR_BAD_MATRIX, "CSR: colidx[%lld] = %d outside [0, %d)", k,
                              colidx[k], n);
-        if (!std::isfinite(a[k]))
-            return set_error(CGB_ERR_NUMERIC, "CSR: a[%lld] is not finite", k);
+        return set_error(CGB_ERR_NUMERIC, "CSR: a[%lld] is not finite", k);
     }
     return CGB_OK;
 }

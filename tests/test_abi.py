@@ -69,3 +69,21 @@ def test_no_silent_cpu_fallback(cgb):
     h = ctypes.c_void_p()
     st = cgb.lib().cgb_create(100, rs, ci, a, None, ctypes.byref(h))
     assert st == cgb.ERR_NO_DEVICE
+
+
+def test_validation_reports_first_bad_entry_of_large_csr(cgb):
+    """The entry checks run in parallel chunks; the reported entry is still
+    the first bad one (lowest index), across chunk boundaries."""
+    lib = cgb.lib()
+    n, per_row = 1000, 3000
+    rs = (np.arange(n + 1, dtype=np.int32) * per_row).astype(np.int32)
+    ci = np.tile(np.arange(per_row, dtype=np.int32) % n, n)
+    a = np.ones(n * per_row)
+    ci[2_500_000] = n          # out of range, later chunk
+    a[1_900_000] = np.nan      # not finite, earlier chunk
+    h = ctypes.c_void_p()
+    assert lib.cgb_create(n, rs, ci, a, None, ctypes.byref(h)) == cgb.ERR_NUMERIC
+    assert b"1900000" in lib.cgb_last_error()
+    a[1_900_000] = 1.0
+    assert lib.cgb_create(n, rs, ci, a, None, ctypes.byref(h)) == cgb.ERR_BAD_MATRIX
+    assert b"2500000" in lib.cgb_last_error()
