@@ -743,11 +743,13 @@ __device__ __forceinline__ void outer_step_pcg_body(const OuterArgs &A)
     end_solve(sp, A, row0, row1, it, rr, refreshes, fresh, scratch, bcast, -1.0);
 }
 
-// Block shapes of the sliced kernels (one CTA per SM).  The mixed and
-// preconditioned bodies hold more live state than the FP64 one; with fewer
-// threads each thread may use more registers (65536 / block), so their SpMV
-// loops run without spilling.
-constexpr int kSlicedBlock = 1024;
+// Block shapes of the sliced kernels (one CTA per SM; each thread may use
+// 65536 / block registers).  768 threads (80 registers) let the FP64 walk
+// keep six step pairs a lane in flight without spilling -- at class B, whose
+// column blocks hold short slices, that shortens each warp's chain of
+// dependent loads; the preconditioned body holds the most live state and
+// runs with 512 (128 registers).
+constexpr int kSlicedBlock = 768;
 constexpr int kSlicedMixedBlock = 768;
 constexpr int kSlicedPcgBlock = 512;
 
@@ -770,7 +772,7 @@ __global__ void __launch_bounds__(512, 2) outer_step_mixed(OuterArgs A)
 
 static __global__ void __launch_bounds__(kSlicedMixedBlock, 1) outer_step_mixed_sliced(OuterArgs A)
 {
-    outer_step_mixed_body<SlicedSpmv768>(A);
+    outer_step_mixed_body<SlicedSpmvMixed>(A);
 }
 
 // lanes per row of the preconditioner products (F has about half of A's
@@ -785,7 +787,7 @@ __global__ void __launch_bounds__(512, 2) outer_step_pcg(OuterArgs A)
 
 static __global__ void __launch_bounds__(kSlicedPcgBlock, 1) outer_step_pcg_sliced(OuterArgs A)
 {
-    outer_step_pcg_body<SlicedSpmv512, kLanesF>(A);
+    outer_step_pcg_body<SlicedSpmvPcg, kLanesF>(A);
 }
 
 // Standalone q = A p with the p.q reduction fused (the work of reference

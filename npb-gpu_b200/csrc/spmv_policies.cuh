@@ -495,10 +495,11 @@ struct SlicedSpmvT {
     }
 };
 
-// 1024-thread kernels (64 registers a thread) and the register-richer
-// 768- and 512-thread kernels; pair counts measured on B200.
-using SlicedSpmv = SlicedSpmvT<4, 6>;
-using SlicedSpmv768 = SlicedSpmvT<4, 6>;
-using SlicedSpmv512 = SlicedSpmvT<4, 6>;
+// Per kernel (pair counts and block shapes measured on B200): the FP64
+// outer step and the standalone SpMVs (768 threads, 80 registers), the
+// mixed outer step (768), the preconditioned one (512, 128 registers).
+using SlicedSpmv = SlicedSpmvT<6, 6>;
+using SlicedSpmvMixed = SlicedSpmvT<4, 6>;
+using SlicedSpmvPcg = SlicedSpmvT<4, 6>;
 
 }  // namespace cgb
