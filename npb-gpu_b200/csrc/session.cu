@@ -55,6 +55,20 @@ cudaError_t dev_alloc(T **p, size_t count)
     return cudaMalloc(reinterpret_cast<void **>(p), sizeof(T) * std::max<size_t>(count, 1));
 }
 
+// Grow-only buffer: keeps *p when it already holds `count` elements, so a
+// re-upload of the same structure allocates nothing.
+template <typename T>
+cudaError_t dev_reserve(T **p, size_t *cap, size_t count)
+{
+    if (*p && *cap >= count) return cudaSuccess;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    const cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), sizeof(T) * std::max<size_t>(count, 1));
+    if (e == cudaSuccess) *cap = count;
+    return e;
+}
+
 template <typename T>
 void dev_free(T *&p)
 {
@@ -235,6 +249,7 @@ struct cgb_session {
     int sliced_max_rows = 0;
     int sliced_nacc = 2;           // row accumulators (4 when they fit: FP32 pipeline depth)
     int *d_chunk_slice = nullptr;  // shared by A, F and F^T (same row split)
+    size_t cap_chunk = 0, cap_seg = 0;  // allocated elements of d_chunk_slice, d_seg
     cgb::SliceSet sa;              // A: FP64 values (+ FP32 copy)
     cgb::SliceSet sf, sft;         // F and F^T: FP32 values
     int layout_gen = 0;            // bumped by every build of A's slices
@@ -281,9 +296,7 @@ void free_set(SliceSet &t)
     dev_free(t.sval16);
     dev_free(t.scol);
     dev_free(t.chunk_slice);
-    t.interleaved = 0;
-    t.block_cols = t.blocks = 0;
-    t.entries = 0;
+    t = SliceSet();
 }
 
 void free_prec_slices(cgb_session *s)
@@ -296,7 +309,16 @@ void free_prec_slices(cgb_session *s)
 void free_sliced(cgb_session *s)
 {
     dev_free(s->d_chunk_slice);
+    s->cap_chunk = 0;
     free_set(s->sa);
+    free_prec_slices(s);
+    s->sliced_grid = 0;
+}
+
+// Marks A's sliced copy stale without freeing its buffers (a rebuild of
+// the same size reuses them).
+void invalidate_sliced(cgb_session *s)
+{
     free_prec_slices(s);
     s->sliced_grid = 0;
 }
@@ -430,8 +452,7 @@ int build_segments_table(cgb_session *s)
     s->nblk = (n + kSliceWidth - 1) / kSliceWidth;
     s->seg_stride = (n + 31) & ~31;
     const size_t count = size_t(s->nblk + 1) * s->seg_stride;
-    dev_free(s->d_seg);
-    if (dev_alloc(&s->d_seg, count) != cudaSuccess)
+    if (dev_reserve(&s->d_seg, &s->cap_seg, count) != cudaSuccess)
         return set_error(CGB_ERR_NOMEM, "segment table allocation failed");
     CUDA_TRY(cudaMemsetAsync(s->d_flag, 0, sizeof(int), s->stream));
     build_segments<<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
@@ -441,10 +462,7 @@ int build_segments_table(cgb_session *s)
     CUDA_TRY(cudaMemcpyAsync(&unsorted, s->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     s->sorted = (unsorted == 0);
-    if (!s->sorted) {
-        dev_free(s->d_seg);
-        s->nblk = 0;
-    }
+    if (!s->sorted) s->nblk = 0;
     return CGB_OK;
 }
 
@@ -479,8 +497,9 @@ int fill_set(cgb_session *s, int grid, bool interleave, const int *seg, const in
     const int nchunks = grid * nblk;
     const int ig = interleave ? grid : 0;
     t->interleaved = interleave ? 1 : 0;
-    if (dev_alloc(&t->srow, size_t(total) * 32) || dev_alloc(&t->width, size_t(total)) ||
-        dev_alloc(&t->off, size_t(total) + 1))
+    if (dev_reserve(&t->srow, &t->cap_srow, size_t(total) * 32) ||
+        dev_reserve(&t->width, &t->cap_width, size_t(total)) ||
+        dev_reserve(&t->off, &t->cap_off, size_t(total) + 1))
         return set_error(CGB_ERR_NOMEM, "sliced layout: metadata allocation failed");
     slice_sort_rows<<<nchunks, 256, 0, s->stream>>>(seg, s->seg_stride, nblk, s->d_split, ig,
                                                    s->n, t->chunk_slice, t->srow, t->width);
@@ -492,10 +511,10 @@ int fill_set(cgb_session *s, int grid, bool interleave, const int *seg, const in
                              s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     t->entries = entries;
-    if ((want64 && dev_alloc(&t->sval, size_t(entries) + kPad)) ||
-        dev_alloc(&t->scol, size_t(entries) + kPad) ||
-        (want32 && dev_alloc(&t->sval32, size_t(entries) + kPad)) ||
-        (want16 && dev_alloc(&t->sval16, size_t(entries) + kPad)))
+    if ((want64 && dev_reserve(&t->sval, &t->cap_sval, size_t(entries) + kPad)) ||
+        dev_reserve(&t->scol, &t->cap_scol, size_t(entries) + kPad) ||
+        (want32 && dev_reserve(&t->sval32, &t->cap_sval32, size_t(entries) + kPad)) ||
+        (want16 && dev_reserve(&t->sval16, &t->cap_sval16, size_t(entries) + kPad)))
         return set_error(CGB_ERR_NOMEM, "sliced layout: %u entries do not fit", entries);
     slice_fill<ST><<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
         seg, s->seg_stride, nblk, bcols, s->d_split, ig, t->chunk_slice, nchunks,
@@ -508,7 +527,7 @@ int fill_set(cgb_session *s, int grid, bool interleave, const int *seg, const in
 // The sliced copy of the matrix for a row split over `grid` CTAs (one per SM).
 int build_sliced(cgb_session *s, int grid)
 {
-    free_sliced(s);
+    invalidate_sliced(s);
     std::vector<int> split;
     make_split(s->n, s->h_rowstr_copy.data(), grid, split);
     std::vector<int> chunk_slice;
@@ -532,7 +551,7 @@ int build_sliced(cgb_session *s, int grid)
     s->sliced_nacc = sliced_smem_bytes(s->sliced_max_rows, kMaxSlots) <= room ? kMaxSlots : 2;
     if (s->sliced_max_rows >= 0xffff || sliced_smem_bytes(s->sliced_max_rows, 2) > room)
         return set_error(CGB_ERR_STATE, "sliced layout: %d rows per CTA exceed shared memory", max_rows);
-    if (dev_alloc(&s->d_chunk_slice, chunk_slice.size()))
+    if (dev_reserve(&s->d_chunk_slice, &s->cap_chunk, chunk_slice.size()))
         return set_error(CGB_ERR_NOMEM, "sliced layout: metadata allocation failed");
     CUDA_TRY(cudaMemcpy(s->d_split, split.data(), sizeof(int) * (grid + 1), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(s->d_chunk_slice, chunk_slice.data(), sizeof(int) * chunk_slice.size(),
@@ -795,8 +814,7 @@ int upload_matrix(cgb_session *s, const int *rowstr, const int *colidx, const do
     s->h_rowstr_copy.assign(rowstr, rowstr + s->n + 1);
     const int kept_kind = s->plan.kind;
     const int kept_grid = s->sliced_grid;
-    free_sliced(s);
-    dev_free(s->d_seg);
+    invalidate_sliced(s);
     s->sorted = false;
     s->nblk = 0;
     if (s->n >= 2 * kSliceWidth) {

@@ -81,6 +81,9 @@ struct SliceSet {
     int interleaved = 0;              // rows owned round-robin by the CTAs
     int block_cols = 0, blocks = 0;   // columns per block, blocks (0: the session's)
     long long entries = 0;            // padded entries
+    // allocated capacities (elements): a rebuild reuses buffers that fit
+    size_t cap_srow = 0, cap_width = 0, cap_off = 0, cap_sval = 0, cap_sval32 = 0,
+           cap_sval16 = 0, cap_scol = 0;
 };
 
 // Matrix in both layouts, both precisions (unused members may be null).
