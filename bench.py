@@ -389,8 +389,10 @@ def our_arm(args, rank, world, local_rank):
     # average launch duration from CUDA events around each launch on the
     # library's stream, algorithmic bytes per launch from outer_step_bytes
     plan = sess.plan()
-    kernel = "outer_step_fp64_sliced" if plan["kind"] == "sliced" else \
-        f"outer_step_fp64<{plan['lanes_per_row']}>"
+    if plan["kind"] == "sliced":
+        kernel = "outer_step_fp64_sliced_pf" if plan["l2_prefetch"] else "outer_step_fp64_sliced"
+    else:
+        kernel = f"outer_step_fp64<{plan['lanes_per_row']}>"
     kernel_ms, gap_ms = sess.time_outer_steps(niter, shift)
     bytes_launch = outer_step_bytes(n, nnz)
     achieved = bytes_launch / (kernel_ms / 1e3) / 1e9

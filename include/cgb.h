@@ -85,7 +85,9 @@ typedef struct cgb_options {
     int spmv_kernel;          /* 0 = autotuned, 1 = row kernel on the CSR (gathered vector read
                                  through L1/L2), 2 = sliced kernel (a sliced copy of the matrix
                                  with 16-bit local columns, gathered vector staged in shared
-                                 memory by TMA bulk copies) */
+                                 memory by TMA bulk copies), 3 = sliced with an L2 prefetch
+                                 of each warp's slices of the next column block (0 times
+                                 2 against 3 and keeps the faster) */
 } cgb_options;
 
 void cgb_default_options(cgb_options *opts);
@@ -203,14 +205,16 @@ int cgb_gnn_attach(cgb_gnn *m, cgb_gnn_graph *g, cgb_session *s);
 
 /* ------------------------------------------------------------- batches */
 /* Many independent systems of uneven order (n <= 27000 each) solved in one
- * persistent launch: every CTA takes systems from a device work queue (the
- * largest first) and runs a system's whole inverse power iteration alone,
- * its search vector in shared memory.  Lanes per row per system and the
+ * persistent cooperative launch: every CTA takes work from a device queue
+ * (the largest systems first) and runs a system's whole inverse power
+ * iteration, alone or -- the largest systems -- as one of a team of CTAs
+ * that split its rows, the search vector in each CTA's shared memory.  Lanes per row per system and the
  * block shape come from cgb_batch_tune (defaults otherwise).  In
  * CGB_MODE_MIXED a system whose iteration meets p.Ap >= 0 (not negative
  * definite), a non-finite residual, or does not converge within cgitmax is
- * solved again with the FP64 reference algorithm (25 steps, the reference's
- * cgitmax); its status is then 1.  No counterpart in the
+ * solved again at once, by the same CTA in the same launch, with the FP64
+ * reference algorithm (25 steps, the reference's cgitmax); its status is
+ * then 1 and its outputs are that solve's.  No counterpart in the
  * reference (it solves one system). */
 typedef struct cgb_batch cgb_batch;
 
@@ -236,9 +240,19 @@ int cgb_batch_solve(cgb_batch *b, const cgb_batch_params *params, double *zeta, 
                     int *iters, int *status, double *device_ms);
 /* Autotuner: times the batch for each candidate block shape and lane policy
  * (row-length thresholds t0 < t1 < t2 for 8 / 16 / 32 lanes per row, 4 below
- * t0), keeps the fastest for later solves and reports it. */
+ * t0), then for the best of those each team policy, keeps the fastest for
+ * later solves and reports it (cgb_batch_policy gives the rest). */
 int cgb_batch_tune(cgb_batch *b, const cgb_batch_params *params, int *block, double *t0,
                    double *t1, double *t2, double *best_ms);
+/* The batch's current policy: entries a lane loads ahead (4 or 8), the team
+ * fraction, and how many systems the last launch gave a team of 2, 4 or 8
+ * CTAs (a system gets one while its SpMV work per CTA is above team_frac x
+ * the batch's work per resident CTA; the members split its rows and
+ * exchange the search vector through global memory at each update, with
+ * bounded waits: CGB_ERR_TIMEOUT past 2 s).  Any output may be NULL. */
+int cgb_batch_policy(cgb_batch *b, int *unroll, double *team_frac, int *teams);
+/* Sets the team fraction (0 = every system on one CTA; default 0.5). */
+int cgb_batch_set_team_frac(cgb_batch *b, double team_frac);
 
 /* ---------------------------------------------------------- diagnostics */
 /* Time `reps` launches of the standalone SpMV (q = A p with the p.q
@@ -254,7 +268,9 @@ int cgb_time_outer_steps(cgb_session *s, int niter, double shift, double *kernel
                          double *graph_gap_ms);
 
 /* The kernel configuration the session's autotuner chose: kind 1 = row,
- * 2 = sliced; lanes per row (row kind), grid, block, dynamic shared memory
+ * 2 = sliced, 3 = sliced with the L2 prefetch of each warp's next column
+ * block (the FP64 and FP32 SpMVs of the matrix; not the factor products);
+ * lanes per row (row kind), grid, block, dynamic shared memory
  * bytes, and the stored entries of the layout the SpMV streams (nnz for the
  * CSR, nnz plus slice padding for the sliced copy).  Any output may be NULL. */
 int cgb_plan_info(cgb_session *s, int *kind, int *lanes_per_row, int *grid, int *block,

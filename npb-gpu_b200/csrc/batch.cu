@@ -42,10 +42,16 @@ namespace batch {
 
 constexpr int kBatchMaxN = 27000;  // rows of the largest system (shared p: 8 bytes a row)
 constexpr int kReferenceCgitmax = 25;  // cg.cu's cgitmax: the FP64 re-solve of a mixed failure
+constexpr int kMaxTeam = 8;            // CTAs that may share one system
+constexpr int kTeamValues = 16;        // values one team reduction can carry
+constexpr int kSyncStride = 32;        // words between barrier counters (128-byte lines)
+constexpr long long kTeamWaitNs = 2000000000LL;  // limit of one team-barrier wait
+static_assert(kTeamValues >= kGramValues, "team reductions must carry the Gram values");
 
 struct SysDesc {
     int n;
     int lanes;           // lanes per row (2, 4, 8, 16, 32)
+    int team;            // CTAs that solve the system together (1, 2, 4 or 8)
     long long row_off;   // into rowstr_all (n+1 entries)
     long long nnz_off;   // into colidx_all / a_all
     long long vec_off;   // into the vector arrays (n+8 entries)
@@ -55,7 +61,6 @@ struct SysDesc {
 struct BatchArgs {
     int nsys;
     const SysDesc *__restrict__ sys;
-    const int *__restrict__ order;      // systems, largest first
     const int *__restrict__ rowstr;
     const int *__restrict__ colidx;
     const double *__restrict__ a;
@@ -72,7 +77,72 @@ struct BatchArgs {
     double *hx, *hw;
     long long hstride;
     int recycle;
+    // teams: the search vector's exchange copy (vec_off layout), per system
+    // a barrier (count, gen: kSyncStride words apart, 2 * kSyncStride words a
+    // system) and 2 x kMaxTeam x kTeamValues reduction slots
+    double *pg;
+    unsigned *team_sync;
+    double *team_part;
+    int *dev_status;     // kDevOk, or kDevTimeout once a team wait ran out
 };
+
+// This CTA's part of a system: rows [lo, hi) of `size` members (balanced by
+// stored entries), and the team's barrier and reduction slots.  `par`
+// alternates the slot set between consecutive reductions: a member can be
+// at most one reduction ahead of the slowest, so it never overwrites slots
+// that one still reads.
+struct Team {
+    int id, member, size, lo, hi, par;
+};
+
+// The team's barrier words and reduction slots (computed where used: kept in
+// registers across the CG loop they would crowd it).
+struct TeamMem {
+    unsigned *count, *gen;
+    double *part;
+    int *status;  // the launch's device status word
+};
+
+__device__ __forceinline__ TeamMem team_mem(const BatchArgs &B, int id)
+{
+    TeamMem M;
+    M.count = B.team_sync + size_t(id) * (2 * kSyncStride);
+    M.gen = M.count + kSyncStride;
+    M.part = B.team_part + size_t(id) * (2 * kMaxTeam * kTeamValues);
+    M.status = B.dev_status;
+    return M;
+}
+
+// First row whose rowstr entry is >= target (rowstr ascending, n+1 entries).
+__device__ __forceinline__ int first_row_at(const int *rowstr, int n, long long target)
+{
+    int a = 0, b = n;
+    while (a < b) {
+        const int m = (a + b) >> 1;
+        if (rowstr[m] < target) a = m + 1;
+        else b = m;
+    }
+    return a;
+}
+
+__device__ __forceinline__ Team make_team(const BatchArgs &B, int id, const SysDesc &S, int member)
+{
+    Team T;
+    T.id = id;
+    T.member = member;
+    T.size = S.team;
+    T.par = 0;
+    if (T.size == 1) {
+        T.lo = 0;
+        T.hi = S.n;
+    } else {
+        const int *rowstr = B.rowstr + S.row_off;
+        const long long nnz = rowstr[S.n];
+        T.lo = member == 0 ? 0 : first_row_at(rowstr, S.n, nnz * member / T.size);
+        T.hi = member == T.size - 1 ? S.n : first_row_at(rowstr, S.n, nnz * (member + 1) / T.size);
+    }
+    return T;
+}
 
 // CTA sums of nq (<= kGramValues) per-thread values, in a fixed order, into
 // out[] (shared, every thread); four values a round keep the static shared
@@ -115,31 +185,95 @@ __device__ __forceinline__ double cta_sum(double v, double *red)
     return s;  // every thread, same order
 }
 
-// q[j] = (A v)[j] for all rows of the system with LPR lanes per row; v in
-// shared memory (FP64), products in FP64 or (F32) in FP32 with FP32 row sums;
-// returns this thread's share of sum_j dv[j] q[j] (dv: shared p or null).
-template <int LPR, bool F32>
-__device__ __forceinline__ double sys_spmv(const BatchArgs &B, const SysDesc &S, const double *v_sh,
-                                           const double *v_gl, double *q, const double *dv_sh)
+__device__ __forceinline__ bool team_barrier(const TeamMem &M, const Team &T)
+{
+    return counted_barrier(M.count, M.gen, unsigned(T.size), M.status, kTeamWaitNs);
+}
+
+// Team sum of one value per thread: the CTA sum, then (teams) the members'
+// sums added in member order by every member, so all members hold the same
+// bits and take the same branches.  The barrier inside also publishes every
+// global write the members made before it.  False: a team wait failed.
+__device__ __forceinline__ bool team_sum(const BatchArgs &B, Team &T, double v, double *red,
+                                         double &out)
+{
+    const double s = cta_sum(v, red);
+    if (T.size == 1) {
+        out = s;
+        return true;
+    }
+    const TeamMem M = team_mem(B, T.id);
+    double *slot = M.part + T.par * (kMaxTeam * kTeamValues);
+    if (threadIdx.x == 0) slot[T.member * kTeamValues] = s;
+    T.par ^= 1;
+    if (!team_barrier(M, T)) return false;
+    double t = 0.0;
+    for (int m = 0; m < T.size; m++) t += __ldcg(slot + m * kTeamValues);
+    out = t;
+    return true;
+}
+
+// team_sum of nq values a thread, into out[] (shared).
+__device__ __forceinline__ bool team_sum_multi(const TeamMem &M, Team &T, const double *vals,
+                                               int nq, double *out)
+{
+    cta_sum_multi(vals, nq, out);
+    if (T.size == 1) return true;
+    double *slot = M.part + T.par * (kMaxTeam * kTeamValues);
+    if (int(threadIdx.x) < nq) slot[T.member * kTeamValues + threadIdx.x] = out[threadIdx.x];
+    T.par ^= 1;
+    if (!team_barrier(M, T)) return false;
+    if (int(threadIdx.x) < nq) {
+        double t = 0.0;
+        for (int m = 0; m < T.size; m++) t += __ldcg(slot + m * kTeamValues + threadIdx.x);
+        out[threadIdx.x] = t;
+    }
+    __syncthreads();
+    return true;
+}
+
+// After a team barrier that followed the members' writes of their rows of
+// p to pg: the other members' rows into this CTA's shared copy.
+__device__ __forceinline__ void team_gather_p(const Team &T, const double *pg, double *p, int n)
+{
+    if (T.size == 1) return;
+    for (int j = threadIdx.x; j < T.lo; j += blockDim.x) p[j] = __ldcg(pg + j);
+    for (int j = T.hi + threadIdx.x; j < n; j += blockDim.x) p[j] = __ldcg(pg + j);
+    __syncthreads();
+}
+
+// q[j] = (A v)[j] for rows [lo, hi) of the system with S.lanes lanes per
+// row; v in shared memory (FP64) or, v_gl, global memory (v_gl_shared: a
+// team's vector, read through L2, since other members' rows may have been
+// written since this SM last cached them); products in FP64 or (F32) in FP32 with FP32 row sums; returns this
+// thread's share of sum_j dv[j] q[j] (dv: shared p or null).  The lane count
+// is a run-time value: one instance of the solver serves every system (an
+// instance per lane count inlined under one switch needed 128 registers a
+// thread and spilled; one needs about 84).
+template <bool F32, int kU>
+__device__ __forceinline__ double sys_spmv(const BatchArgs &B, const SysDesc &S, int lo, int hi,
+                                           const double *v_sh, const double *v_gl, double *q,
+                                           const double *dv_sh, bool v_gl_shared = false)
 {
     const int *rowstr = B.rowstr + S.row_off;
     const int *colidx = B.colidx + S.nnz_off;
     const double *a = B.a + S.nnz_off;
     const float *a32 = B.a32 ? B.a32 + S.nnz_off : nullptr;
-    const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
+    const int LPR = S.lanes;
+    const int lane = threadIdx.x & (LPR - 1), grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
     const unsigned mask =
         LPR == 32 ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) & ~(LPR - 1)));
     double dacc = 0.0;
-    for (int row = grp; row < S.n; row += ngrp) {
+    for (int row = lo + grp; row < hi; row += ngrp) {
         const int k0 = rowstr[row], k1 = rowstr[row + 1];
         double s64 = 0.0;
         float s32 = 0.f;
-        for (int k = k0 + lane; k < k1; k += 4 * LPR) {
-            int c[4];
-            double av[4];
-            float af[4];
+        for (int k = k0 + lane; k < k1; k += kU * LPR) {
+            int c[kU];
+            double av[kU];
+            float af[kU];
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < kU; u++) {
                 const int kk = k + u * LPR;
                 if (kk < k1) {
                     c[u] = __ldcs(colidx + kk);
@@ -148,17 +282,18 @@ __device__ __forceinline__ double sys_spmv(const BatchArgs &B, const SysDesc &S,
                 }
             }
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < kU; u++) {
                 if (k + u * LPR < k1) {
-                    const double pv = v_sh ? v_sh[c[u]] : v_gl[c[u]];
+                    const double pv = v_sh ? v_sh[c[u]]
+                                           : (v_gl_shared ? __ldcg(v_gl + c[u]) : v_gl[c[u]]);
                     if (F32) s32 = fmaf(af[u], float(pv), s32);
                     else s64 = fma(av[u], pv, s64);
                 }
             }
         }
         double s;
-        if (F32) s = double(group_sum_f<LPR>(s32, mask));
-        else s = group_sum<LPR>(s64, mask);
+        if (F32) s = double(group_sum_f_rt(s32, mask, LPR));
+        else s = group_sum_rt(s64, mask, LPR);
         if (lane == 0) {
             q[row] = s;
             if (dv_sh) dacc = fma(dv_sh[row], s, dacc);
@@ -167,16 +302,127 @@ __device__ __forceinline__ double sys_spmv(const BatchArgs &B, const SysDesc &S,
     return dacc;
 }
 
-// One system's power iteration.  Returns false when the mixed iteration met
-// p.Ap >= 0, a non-finite residual, or did not converge (the caller then
-// runs the fixed mode).
-template <int LPR, bool mixed>
-__device__ bool solve_system(const BatchArgs &B, const SysDesc &S, double *p, double *red,
-                             int *iters_out, double *zeta_out, double *rnorm_out)
+struct GalerkinIn {
+    const double *hx, *hw;
+    long long hstride, vec_off;
+    const double *x;
+    double *z, *r, *pg, *p;
+    Team T;
+    TeamMem M;
+    int outer, m, v;
+};
+
+struct GalerkinOut {
+    double acc, xx;  // this thread's share of r.r; x_k.x_k
+    int par, ok;     // the team's next slot parity; 0 when a team wait failed
+};
+
+// Galerkin start of a mixed solve on x_k .. x_{k-v+1} (v >= 1) for this
+// CTA's rows: z0 = V y, r = x - W y (A z0 = W y), p = r; the Gram values are
+// team sums, so every member solves the same small system.
+static __device__ __forceinline__ GalerkinOut galerkin_body(GalerkinIn in)
 {
-    const int n = S.n;
+    __shared__ double g_sh[kTeamValues];
+    __shared__ double y_sh[kMaxRecycle];
+    const int lo = in.T.lo, hi = in.T.hi, m = in.m, v = in.v, outer = in.outer;
+    const bool team = in.T.size > 1;
+    GalerkinOut out{0.0, 0.0, in.T.par, 0};
+    long long off[kMaxRecycle];
+#pragma unroll
+    for (int a = 0; a < kMaxRecycle; a++) off[a] = ((outer - a) % m + m) % m * in.hstride + in.vec_off;
+    const int npairs = v * (v + 1) / 2;
+    double vals[kGramValues];
+#pragma unroll
+    for (int q = 0; q < kGramValues; q++) vals[q] = 0.0;
+    for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+        const double xv = in.x[j];
+#pragma unroll
+        for (int b = 0; b < kMaxRecycle; b++) {
+            if (b < v) {
+                const double xb = in.hx[off[b] + j], wb = in.hw[off[b] + j];
+#pragma unroll
+                for (int a = 0; a <= b; a++)
+                    vals[gram_index(a, b)] =
+                        fma(a == b ? xb : in.hx[off[a] + j], wb, vals[gram_index(a, b)]);
+                vals[kGramPairs + b] = fma(xb, xv, vals[kGramPairs + b]);
+            }
+        }
+    }
+    double packed[kGramValues];
+#pragma unroll
+    for (int q = 0; q < kGramValues; q++) packed[q] = 0.0;
+#pragma unroll
+    for (int q = 0; q < kGramPairs; q++)
+        if (q < npairs) packed[q] = vals[q];
+#pragma unroll
+    for (int b = 0; b < kMaxRecycle; b++)
+        if (b < v) packed[npairs + b] = vals[kGramPairs + b];
+    Team T = in.T;
+    if (!team_sum_multi(in.M, T, packed, npairs + v, g_sh)) return out;
+    out.par = T.par;
+    if (threadIdx.x == 0) {
+        double g[kGramValues], y[kMaxRecycle];
+        for (int q = 0; q < kGramValues; q++) g[q] = 0.0;
+        for (int q = 0; q < npairs; q++) g[q] = g_sh[q];
+        for (int b = 0; b < v; b++) g[kGramPairs + b] = g_sh[npairs + b];
+        galerkin_solve(g, v, y);
+        for (int a = 0; a < kMaxRecycle; a++) y_sh[a] = a < v ? y[a] : 0.0;
+    }
+    __syncthreads();
+    out.xx = g_sh[npairs];  // x_k . x_k
+    double acc = 0.0;
+    for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+        double z0 = 0.0, az = 0.0;
+#pragma unroll
+        for (int a = 0; a < kMaxRecycle; a++) {
+            if (a < v) {
+                z0 = fma(y_sh[a], in.hx[off[a] + j], z0);
+                az = fma(y_sh[a], in.hw[off[a] + j], az);
+            }
+        }
+        const double rv = in.x[j] - az;
+        in.z[j] = z0;
+        in.r[j] = rv;
+        in.p[j] = rv;
+        if (team) in.pg[j] = rv;
+        acc = fma(rv, rv, acc);
+    }
+    out.acc = acc;
+    out.ok = 1;
+    return out;
+}
+
+// Out of line for the kernels with teams: it runs once an outer step, and
+// inlined there its arrays crowd the CG loop's registers.
+static __device__ __noinline__ GalerkinOut batch_galerkin(GalerkinIn in)
+{
+    return galerkin_body(in);
+}
+
+constexpr int kSolveOk = 0;
+constexpr int kSolveGaveUp = 1;   // mixed: p.Ap >= 0, a non-finite residual, or no convergence
+constexpr int kSolveAborted = 2;  // a team wait failed (dev_status says why)
+
+// One system's power iteration on this CTA's rows [T.lo, T.hi) (all rows
+// without a team).  Every CTA keeps the whole search vector in shared
+// memory; a team's members exchange their rows of it through pg after each
+// update.  Every branch depends on team sums only, so the members run the
+// same sequence of barriers.  cgitmax: the fixed mode's exact count, the
+// mixed mode's cap.
+template <bool mixed, int kU, bool kTeams>
+__device__ int solve_system(const BatchArgs &B, const SysDesc &S, Team &T, int cgitmax, double *p,
+                            double *red, int *iters_out, double *zeta_out, double *rnorm_out)
+{
+    if (!kTeams) {  // a kernel without teams: the team code folds away
+        T.size = 1;
+        T.lo = 0;
+        T.hi = S.n;
+    }
+    const int n = S.n, lo = T.lo, hi = T.hi;
+    const bool team = kTeams && T.size > 1;
     double *x = B.x + S.vec_off, *z = B.z + S.vec_off, *r = B.r + S.vec_off, *q = B.q + S.vec_off;
-    for (int j = threadIdx.x; j < n; j += blockDim.x) x[j] = 1.0;
+    double *pg = B.pg + S.vec_off;
+    for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) x[j] = 1.0;
     __syncthreads();
     int total = 0;
     double zeta = 0.0, rnorm = 0.0;
@@ -186,76 +432,26 @@ __device__ bool solve_system(const BatchArgs &B, const SysDesc &S, double *p, do
         const int v = (mixed && m > 0) ? min(outer, m) : 0;
         double xx = 0.0;
         if (v > 0) {
-            // Galerkin start on x_k .. x_{k-v+1}: z0 = V y, A z0 = W y
-            __shared__ double g_sh[kGramValues];
-            __shared__ double y_sh[kMaxRecycle];
-            long long off[kMaxRecycle];
-#pragma unroll
-            for (int a = 0; a < kMaxRecycle; a++)
-                off[a] = ((outer - a) % m + m) % m * B.hstride + S.vec_off;
-            const int npairs = v * (v + 1) / 2;
-            double vals[kGramValues];
-#pragma unroll
-            for (int q = 0; q < kGramValues; q++) vals[q] = 0.0;
-            for (int j = threadIdx.x; j < n; j += blockDim.x) {
-                const double xv = x[j];
-#pragma unroll
-                for (int b = 0; b < kMaxRecycle; b++) {
-                    if (b < v) {
-                        const double xb = B.hx[off[b] + j], wb = B.hw[off[b] + j];
-#pragma unroll
-                        for (int a = 0; a <= b; a++)
-                            vals[gram_index(a, b)] = fma(a == b ? xb : B.hx[off[a] + j], wb,
-                                                         vals[gram_index(a, b)]);
-                        vals[kGramPairs + b] = fma(xb, xv, vals[kGramPairs + b]);
-                    }
-                }
-            }
-            double packed[kGramValues];
-#pragma unroll
-            for (int q = 0; q < kGramValues; q++) packed[q] = 0.0;
-#pragma unroll
-            for (int q = 0; q < kGramPairs; q++)
-                if (q < npairs) packed[q] = vals[q];
-#pragma unroll
-            for (int b = 0; b < kMaxRecycle; b++)
-                if (b < v) packed[npairs + b] = vals[kGramPairs + b];
-            cta_sum_multi(packed, npairs + v, g_sh);
-            if (threadIdx.x == 0) {
-                double g[kGramValues], y[kMaxRecycle];
-                for (int q = 0; q < kGramValues; q++) g[q] = 0.0;
-                for (int q = 0; q < npairs; q++) g[q] = g_sh[q];
-                for (int b = 0; b < v; b++) g[kGramPairs + b] = g_sh[npairs + b];
-                galerkin_solve(g, v, y);
-                for (int a = 0; a < kMaxRecycle; a++) y_sh[a] = a < v ? y[a] : 0.0;
-            }
-            __syncthreads();
-            xx = g_sh[npairs];  // x_k . x_k
-            for (int j = threadIdx.x; j < n; j += blockDim.x) {
-                double z0 = 0.0, az = 0.0;
-#pragma unroll
-                for (int a = 0; a < kMaxRecycle; a++) {
-                    if (a < v) {
-                        z0 = fma(y_sh[a], B.hx[off[a] + j], z0);
-                        az = fma(y_sh[a], B.hw[off[a] + j], az);
-                    }
-                }
-                const double rv = x[j] - az;
-                z[j] = z0;
-                r[j] = rv;
-                p[j] = rv;
-                acc = fma(rv, rv, acc);
-            }
+            GalerkinIn in{B.hx, B.hw, B.hstride, S.vec_off, x, z, r, pg, p, T, team_mem(B, T.id),
+                          outer, m, v};
+            const GalerkinOut g = kTeams ? batch_galerkin(in) : galerkin_body(in);
+            if (!g.ok) return kSolveAborted;
+            T.par = g.par;
+            acc = g.acc;
+            xx = g.xx;
         } else {
-            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
                 const double xv = x[j];
                 z[j] = 0.0;
                 r[j] = xv;
                 p[j] = xv;
+                if (team) pg[j] = xv;
                 acc = fma(xv, xv, acc);
             }
         }
-        double rho = cta_sum(acc, red);  // includes a barrier: p complete
+        double rho;
+        if (!team_sum(B, T, acc, red, rho)) return kSolveAborted;  // barrier: p complete
+        team_gather_p(T, pg, p, n);
         if (v == 0) xx = rho;
         const double stop2 = B.tol * B.tol * xx;
         double rho_cycle = rho;
@@ -263,7 +459,7 @@ __device__ bool solve_system(const BatchArgs &B, const SysDesc &S, double *p, do
         bool fresh = true;
         for (;;) {
             if (!mixed) {
-                if (it >= B.cgitmax) break;
+                if (it >= cgitmax) break;
             } else {
                 bool refresh = false;
                 if (rho <= stop2) {
@@ -272,43 +468,56 @@ __device__ bool solve_system(const BatchArgs &B, const SysDesc &S, double *p, do
                 } else if (!fresh && (since >= B.refresh_every || rho <= 1e-12 * rho_cycle)) {
                     refresh = true;
                 }
-                if (!refresh && it >= B.cgitmax) return false;  // not converged: fall back
+                if (!refresh && it >= cgitmax) return kSolveGaveUp;  // not converged
                 if (refresh) {
-                    // r = x - A z (FP64 matrix, z from global memory), restart p = r
-                    sys_spmv<LPR, false>(B, S, nullptr, z, q, nullptr);
+                    // r = x - A z (FP64 matrix; every member's z rows were
+                    // published by the last team sum), restart p = r
+                    sys_spmv<false, kU>(B, S, lo, hi, nullptr, z, q, nullptr, team);
                     __syncthreads();
                     acc = 0.0;
-                    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                    for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
                         const double rv = x[j] - q[j];
                         r[j] = rv;
                         p[j] = rv;
+                        if (team) pg[j] = rv;
                         acc = fma(rv, rv, acc);
                     }
-                    rho = cta_sum(acc, red);
+                    if (!team_sum(B, T, acc, red, rho)) return kSolveAborted;
+                    team_gather_p(T, pg, p, n);
                     rho_cycle = rho;
                     since = 0;
                     fresh = true;
                     continue;
                 }
             }
-            const double dpart = mixed ? sys_spmv<LPR, true>(B, S, p, nullptr, q, p)
-                                       : sys_spmv<LPR, false>(B, S, p, nullptr, q, p);
-            const double d = cta_sum(dpart, red);  // barrier: q complete
-            if (mixed && !(d < 0.0)) return false;  // not negative definite (or NaN): fall back
+            const double dpart = mixed ? sys_spmv<true, kU>(B, S, lo, hi, p, nullptr, q, p)
+                                       : sys_spmv<false, kU>(B, S, lo, hi, p, nullptr, q, p);
+            double d;
+            if (!team_sum(B, T, dpart, red, d)) return kSolveAborted;  // barrier: q complete
+            if (mixed && !(d < 0.0)) return kSolveGaveUp;  // not negative definite (or NaN)
             const double alpha = rho / d;
             const double rho0 = rho;
             acc = 0.0;
-            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
                 z[j] = fma(alpha, p[j], z[j]);
                 const double rv = fma(-alpha, q[j], r[j]);
                 r[j] = rv;
                 acc = fma(rv, rv, acc);
             }
-            rho = cta_sum(acc, red);
-            if (mixed && !(rho < INFINITY)) return false;  // non-finite residual: fall back
+            if (!team_sum(B, T, acc, red, rho)) return kSolveAborted;
+            if (mixed && !(rho < INFINITY)) return kSolveGaveUp;  // non-finite residual
             const double beta = rho / rho0;
-            for (int j = threadIdx.x; j < n; j += blockDim.x) p[j] = fma(beta, p[j], r[j]);
-            __syncthreads();
+            for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+                const double pv = fma(beta, p[j], r[j]);
+                p[j] = pv;
+                if (team) pg[j] = pv;
+            }
+            if (team) {
+                if (!team_barrier(team_mem(B, T.id), T)) return kSolveAborted;
+                team_gather_p(T, pg, p, n);
+            } else {
+                __syncthreads();
+            }
             it++;
             since++;
             fresh = false;
@@ -317,63 +526,84 @@ __device__ bool solve_system(const BatchArgs &B, const SysDesc &S, double *p, do
         // q = A z (FP64): a product, or from the true residual r = x - A z
         // the mixed iteration just accepted; rnorm = ||x - A z||, x.z, z.z
         if (mixed && fresh) {
-            for (int j = threadIdx.x; j < n; j += blockDim.x) q[j] = x[j] - r[j];
+            for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) q[j] = x[j] - r[j];
         } else {
-            sys_spmv<LPR, false>(B, S, nullptr, z, q, nullptr);
+            sys_spmv<false, kU>(B, S, lo, hi, nullptr, z, q, nullptr, team);
         }
         __syncthreads();
         double res = 0.0, xz = 0.0, zz = 0.0;
-        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
             const double xv = x[j], zv = z[j], dv = xv - q[j];
             res = fma(dv, dv, res);
             xz = fma(xv, zv, xz);
             zz = fma(zv, zv, zz);
         }
-        rnorm = sqrt(cta_sum(res, red));
-        const double t1 = cta_sum(xz, red);
-        const double t2 = cta_sum(zz, red);
+        double t0, t1, t2;
+        if (!team_sum(B, T, res, red, t0) || !team_sum(B, T, xz, red, t1) ||
+            !team_sum(B, T, zz, red, t2))
+            return kSolveAborted;
+        rnorm = sqrt(t0);
         zeta = S.shift + 1.0 / t1;
         const double norm = 1.0 / sqrt(t2);
         if (mixed && m > 0) {
             // the next iterate and A times it into the ring
             const long long slot = (outer + 1) % m * B.hstride + S.vec_off;
-            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
                 const double xn = norm * z[j];
                 B.hx[slot + j] = xn;
                 B.hw[slot + j] = norm * q[j];
                 x[j] = xn;
             }
         } else {
-            for (int j = threadIdx.x; j < n; j += blockDim.x) x[j] = norm * z[j];
+            for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) x[j] = norm * z[j];
         }
         __syncthreads();
     }
     *iters_out = total;
     *zeta_out = zeta;
     *rnorm_out = rnorm;
-    return true;
+    return kSolveOk;
 }
 
-// One system; status 1 marks a mixed solve that must be redone in FP64
-// (the host launches the FP64 kernel on those systems next).
-template <int LPR, bool mixed>
-__device__ void run_system(const BatchArgs &B, int id, double *p, double *red)
+// This CTA's share (member `member` of the system's team) of one system.  A
+// mixed solve that gives up (an indefinite system shows p.Ap >= 0 within the
+// first iterations) is redone at once by the same team with the reference
+// algorithm (FP64, exactly the reference's 25 CG iterations an outer step)
+// and marked status 1; its outputs are that solve's alone.  False: a team
+// wait failed and the CTA must stop.
+template <bool mixed, int kU, bool kTeams>
+__device__ bool run_system(const BatchArgs &B, int id, int member, const SysDesc &S, double *p,
+                           double *red)
 {
-    const SysDesc S = B.sys[id];
+    Team T = make_team(B, id, S, member);
     int iters = 0;
     double zeta = 0.0, rnorm = 0.0;
-    const bool ok = solve_system<LPR, mixed>(B, S, p, red, &iters, &zeta, &rnorm);
-    if (threadIdx.x == 0) {
+    int rc = solve_system<mixed, kU, kTeams>(B, S, T, B.cgitmax, p, red, &iters, &zeta, &rnorm);
+    const bool gave_up = mixed && rc == kSolveGaveUp;
+    if (gave_up) {
+        __syncthreads();
+        rc = solve_system<false, kU, kTeams>(B, S, T, kReferenceCgitmax, p, red, &iters, &zeta,
+                                             &rnorm);
+    }
+    if (rc == kSolveAborted) return false;
+    if (threadIdx.x == 0 && member == 0) {
         B.zeta[id] = zeta;
         B.rnorm[id] = rnorm;
         B.iters[id] = iters;
-        B.status[id] = ok ? 0 : 1;
+        B.status[id] = gave_up ? 1 : 0;
     }
+    return true;
 }
 
-// Persistent: CTAs take the next system of `list` (count entries) from the
-// work queue until it is empty.
-template <bool mixed, int kMaxThreads>
+// Persistent over a cooperative (co-resident) grid: CTAs take the next work
+// slot of `list` (count entries; slot = system * kMaxTeam + member, a team's
+// slots adjacent, systems largest first) from the queue until it is empty.
+// A member waits for its team only on slots already handed out or the next
+// ones to be, so every team forms.  kUnroll: entries a lane loads before it
+// uses the first (the loads in flight per SM are threads x kUnroll).
+// kTeams: compiled with the team exchanges (a launch whose systems all run
+// alone takes the instance without them, which needs fewer registers).
+template <bool mixed, int kMaxThreads, int kUnroll, bool kTeams>
 __global__ void __launch_bounds__(kMaxThreads, 1) batch_kernel(BatchArgs B, const int *list, int count)
 {
     extern __shared__ __align__(16) double p_sh[];
@@ -381,18 +611,15 @@ __global__ void __launch_bounds__(kMaxThreads, 1) batch_kernel(BatchArgs B, cons
     __shared__ int s_next;
     for (;;) {
         __syncthreads();
-        if (threadIdx.x == 0) s_next = int(atomicAdd(B.queue, 1u));
+        if (threadIdx.x == 0)
+            s_next = ld_relaxed_i32(B.dev_status) != kDevOk ? count : int(atomicAdd(B.queue, 1u));
         __syncthreads();
         const int k = s_next;
         if (k >= count) break;
-        const int id = list[k];
-        switch (B.sys[id].lanes) {
-        case 2: run_system<2, mixed>(B, id, p_sh, red); break;
-        case 4: run_system<4, mixed>(B, id, p_sh, red); break;
-        case 8: run_system<8, mixed>(B, id, p_sh, red); break;
-        case 16: run_system<16, mixed>(B, id, p_sh, red); break;
-        default: run_system<32, mixed>(B, id, p_sh, red); break;
-        }
+        const int slot = list[k];
+        const int id = slot / kMaxTeam;
+        const SysDesc S = B.sys[id];
+        if (!run_system<mixed, kUnroll, kTeams>(B, id, slot % kMaxTeam, S, p_sh, red)) break;
     }
 }
 
@@ -428,21 +655,31 @@ struct cgb_batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<SysDesc> desc;
     std::vector<double> mean_len;
+    std::vector<long long> nnz;   // stored entries per system
+    std::vector<int> order;       // systems, largest first
+    std::vector<int> slots;       // work list of the last launch (system * kMaxTeam + member)
     SysDesc *d_sys = nullptr;
-    int *d_order = nullptr;
+    int *d_slots = nullptr;
     int *d_rowstr = nullptr, *d_colidx = nullptr;
     double *d_a = nullptr;
     float *d_a32 = nullptr;
-    double *d_x = nullptr, *d_z = nullptr, *d_r = nullptr, *d_q = nullptr;
+    double *d_x = nullptr, *d_z = nullptr, *d_r = nullptr, *d_q = nullptr, *d_pg = nullptr;
     unsigned *d_queue = nullptr;
+    unsigned *d_team_sync = nullptr;
+    double *d_team_part = nullptr;
+    int *d_dev_status = nullptr;
     double *d_zeta = nullptr, *d_rnorm = nullptr;
     int *d_iters = nullptr, *d_status = nullptr;
-    int *d_redo = nullptr;
     double *d_hx = nullptr, *d_hw = nullptr;  // Galerkin-start ring, kMaxRecycle x vec_total each
     long long vec_total = 0;
     int block = 512;
+    int unroll = 4;  // 512-thread shape: 4 or 8 entries a lane in flight (1024 threads: 4)
     // lane policy: lanes = 32 if mean >= t2, 16 if >= t1, 8 if >= t0, else 4
     double t0 = 16.0, t1 = 40.0, t2 = 96.0;
+    // team policy: a system gets 2, 4 or 8 CTAs while its work per CTA is
+    // above team_frac x (the batch's work / the grid's CTAs); 0 = no teams
+    double team_frac = 0.5;
+    int resident = 0;  // CTAs of the last launch's grid (team sizes depend on it)
 };
 
 namespace {
@@ -464,9 +701,10 @@ void batch_release(cgb_batch *b)
 {
     if (!b) return;
     cudaSetDevice(b->device);
-    bfree(b->d_sys); bfree(b->d_order); bfree(b->d_rowstr); bfree(b->d_colidx); bfree(b->d_a);
-    bfree(b->d_a32); bfree(b->d_x); bfree(b->d_z); bfree(b->d_r); bfree(b->d_q);
-    bfree(b->d_queue); bfree(b->d_zeta); bfree(b->d_rnorm); bfree(b->d_iters); bfree(b->d_status); bfree(b->d_redo);
+    bfree(b->d_sys); bfree(b->d_slots); bfree(b->d_rowstr); bfree(b->d_colidx); bfree(b->d_a);
+    bfree(b->d_a32); bfree(b->d_x); bfree(b->d_z); bfree(b->d_r); bfree(b->d_q); bfree(b->d_pg);
+    bfree(b->d_queue); bfree(b->d_team_sync); bfree(b->d_team_part); bfree(b->d_dev_status);
+    bfree(b->d_zeta); bfree(b->d_rnorm); bfree(b->d_iters); bfree(b->d_status);
     bfree(b->d_hx); bfree(b->d_hw);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
@@ -482,41 +720,92 @@ int lanes_by_policy(const cgb_batch *b, double mean)
     return 4;
 }
 
-int apply_lanes(cgb_batch *b)
+// Lanes per row and team size of every system for a grid of `grid` CTAs,
+// and the work list (largest systems first, a team's slots adjacent);
+// uploaded on the batch's stream.  The work of a system is counted as its
+// SpMV bytes (12 a stored entry, 8 a row for p and q).
+int apply_policy(cgb_batch *b, int grid)
 {
-    for (int i = 0; i < b->nsys; i++) b->desc[i].lanes = lanes_by_policy(b, b->mean_len[i]);
-    BT_TRY(cudaMemcpy(b->d_sys, b->desc.data(), sizeof(SysDesc) * b->nsys, cudaMemcpyHostToDevice));
+    b->resident = grid;
+    std::vector<double> work(b->nsys);
+    double total = 0.0;
+    for (int i = 0; i < b->nsys; i++) {
+        work[i] = 12.0 * double(b->nnz[i]) + 16.0 * b->desc[i].n;
+        total += work[i];
+    }
+    const double per_cta = total / std::max(grid, 1);
+    b->slots.clear();
+    for (int i : b->order) {
+        SysDesc &d = b->desc[i];
+        d.lanes = lanes_by_policy(b, b->mean_len[i]);
+        int t = 1;
+        if (b->team_frac > 0.0)
+            while (t < kMaxTeam && 2 * t <= grid && work[i] / t > b->team_frac * per_cta) t *= 2;
+        d.team = t;
+        for (int m = 0; m < t; m++) b->slots.push_back(i * kMaxTeam + m);
+    }
+    BT_TRY(cudaMemcpyAsync(b->d_sys, b->desc.data(), sizeof(SysDesc) * b->nsys,
+                           cudaMemcpyHostToDevice, b->stream));
+    BT_TRY(cudaMemcpyAsync(b->d_slots, b->slots.data(), sizeof(int) * b->slots.size(),
+                           cudaMemcpyHostToDevice, b->stream));
     return CGB_OK;
 }
 
-// The kernel for a block shape: 512 threads may use 128 registers a thread,
-// 1024 threads 64.
-template <bool mixed>
-int launch_list(cgb_batch *b, const BatchArgs &A, const int *d_list, int count)
+// One cooperative launch (every CTA resident: team members wait for each
+// other) of the kernel for the block shape: 512 threads may use 128
+// registers a thread, 1024 threads 64.
+using BatchKernel = void (*)(BatchArgs, const int *, int);
+
+template <bool mixed, bool kTeams>
+BatchKernel pick_kernel(const cgb_batch *b)
 {
-    if (count == 0) return CGB_OK;
-    void (*k)(BatchArgs, const int *, int) =
-        b->block > 512 ? batch_kernel<mixed, 1024> : batch_kernel<mixed, 512>;
+    return b->block > 512 ? batch_kernel<mixed, 1024, 4, kTeams>
+                          : (b->unroll > 4 ? batch_kernel<mixed, 512, 8, kTeams>
+                                           : batch_kernel<mixed, 512, 4, kTeams>);
+}
+
+template <bool mixed>
+int launch_all(cgb_batch *b, const BatchArgs &A0)
+{
     const size_t smem = sizeof(double) * size_t(b->max_n + 8);
+    // residency does not depend on the instance (same shape, one CTA an SM
+    // at most by the launch bounds); the policy then says whether any
+    // system gets a team
+    BatchKernel k = pick_kernel<mixed, true>(b);
     BT_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int per_sm = 0;
     BT_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, b->block, smem));
     if (per_sm < 1) return set_error(CGB_ERR_STATE, "batch kernel cannot be resident");
-    const int grid = std::min(per_sm * b->sms, count);
+    const int resident = per_sm * b->sms;
+    int st = apply_policy(b, resident);
+    if (st) return st;
+    if (b->slots.size() == size_t(b->nsys)) {  // no teams
+        k = pick_kernel<mixed, false>(b);
+        BT_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        int per = 0;
+        BT_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, b->block, smem));
+        if (per < per_sm) return set_error(CGB_ERR_STATE, "batch kernel cannot be resident");
+    }
+    const int count = int(b->slots.size());
+    const int grid = std::min(resident, count);
     BT_TRY(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned), b->stream));
-    k<<<grid, b->block, smem, b->stream>>>(A, d_list, count);
-    BT_TRY(cudaGetLastError());
+    BT_TRY(cudaMemsetAsync(b->d_dev_status, 0, sizeof(int), b->stream));
+    BT_TRY(cudaMemsetAsync(b->d_team_sync, 0, sizeof(unsigned) * 2 * kSyncStride * b->nsys, b->stream));
+    BatchArgs A = A0;
+    const int *list = b->d_slots;
+    void *args[] = {&A, &list, const_cast<int *>(&count)};
+    BT_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(k), dim3(grid), dim3(b->block),
+                                       args, smem, b->stream));
     return CGB_OK;
 }
 
-// Mixed: all systems in FP32-SpMV refinement, then the ones marked status 1
-// again in FP64 (status stays 1 for them).  FP64: all systems once.
+// One launch over all systems (mixed: a system whose mixed solve gives up
+// is solved again in FP64 by the same CTAs and marked status 1).
 int launch(cgb_batch *b, const cgb_batch_params &P, double *ms)
 {
     BatchArgs A{};
     A.nsys = b->nsys;
     A.sys = b->d_sys;
-    A.order = b->d_order;
     A.rowstr = b->d_rowstr;
     A.colidx = b->d_colidx;
     A.a = b->d_a;
@@ -525,7 +814,11 @@ int launch(cgb_batch *b, const cgb_batch_params &P, double *ms)
     A.z = b->d_z;
     A.r = b->d_r;
     A.q = b->d_q;
+    A.pg = b->d_pg;
     A.queue = b->d_queue;
+    A.team_sync = b->d_team_sync;
+    A.team_part = b->d_team_part;
+    A.dev_status = b->d_dev_status;
     A.mode = P.mode == CGB_MODE_MIXED ? 1 : 0;
     A.niter = P.niter;
     A.cgitmax = P.cgitmax;
@@ -540,40 +833,15 @@ int launch(cgb_batch *b, const cgb_batch_params &P, double *ms)
     A.hstride = b->vec_total;
     A.recycle = P.recycle;
     BT_TRY(cudaEventRecord(b->ev0, b->stream));
-    int st;
-    if (A.mode == 1) {
-        st = launch_list<true>(b, A, b->d_order, b->nsys);
-        if (st) return st;
-        std::vector<int> status(b->nsys), order(b->nsys);
-        BT_TRY(cudaMemcpyAsync(status.data(), b->d_status, sizeof(int) * b->nsys,
-                               cudaMemcpyDeviceToHost, b->stream));
-        BT_TRY(cudaMemcpyAsync(order.data(), b->d_order, sizeof(int) * b->nsys,
-                               cudaMemcpyDeviceToHost, b->stream));
-        BT_TRY(cudaStreamSynchronize(b->stream));
-        std::vector<int> redo;
-        for (int k = 0; k < b->nsys; k++)
-            if (status[order[k]] != 0) redo.push_back(order[k]);
-        if (!redo.empty()) {
-            BT_TRY(cudaMemcpyAsync(b->d_redo, redo.data(), sizeof(int) * redo.size(),
-                                   cudaMemcpyHostToDevice, b->stream));
-            A.mode = 0;
-            A.cgitmax = kReferenceCgitmax;
-            A.recycle = 0;
-            st = launch_list<false>(b, A, b->d_redo, int(redo.size()));
-            if (st) return st;
-            // the FP64 pass wrote status 0 for these systems; mark them re-solved
-            BT_TRY(cudaStreamSynchronize(b->stream));
-            std::vector<int> ones(redo.size(), 1);
-            for (size_t i = 0; i < redo.size(); i++)
-                BT_TRY(cudaMemcpyAsync(b->d_status + redo[i], &ones[i], sizeof(int),
-                                       cudaMemcpyHostToDevice, b->stream));
-        }
-    } else {
-        st = launch_list<false>(b, A, b->d_order, b->nsys);
-        if (st) return st;
-    }
+    const int st = A.mode == 1 ? launch_all<true>(b, A) : launch_all<false>(b, A);
+    if (st) return st;
     BT_TRY(cudaEventRecord(b->ev1, b->stream));
     BT_TRY(cudaStreamSynchronize(b->stream));
+    int dev = 0;
+    BT_TRY(cudaMemcpy(&dev, b->d_dev_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (dev != kDevOk)
+        return set_error(CGB_ERR_TIMEOUT, "batch: a team wait ran past %lld ns (device status %d)",
+                         kTeamWaitNs, dev);
     float f = 0.f;
     BT_TRY(cudaEventElapsedTime(&f, b->ev0, b->ev1));
     if (ms) *ms = f;
@@ -638,6 +906,7 @@ int cgb_batch_create(int device, int nsys, const int *n, const int *const *rowst
     b->vec_total = vec_total;
     b->desc.resize(nsys);
     b->mean_len.resize(nsys);
+    b->nnz.resize(nsys);
     long long ro = 0, no = 0, vo = 0;
     for (int s = 0; s < nsys; s++) {
         SysDesc &d = b->desc[s];
@@ -647,26 +916,32 @@ int cgb_batch_create(int device, int nsys, const int *n, const int *const *rowst
         d.vec_off = vo;
         d.shift = shift[s];
         d.lanes = 32;
+        d.team = 1;
+        b->nnz[s] = rowstr[s][n[s]];
         b->mean_len[s] = double(rowstr[s][n[s]]) / n[s];
         ro += n[s] + 1;
         no += rowstr[s][n[s]];
         vo += n[s] + 8;
     }
-    std::vector<int> order(nsys);
+    std::vector<int> &order = b->order;
+    order.resize(nsys);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int i, int j) {
         return rowstr[i][n[i]] > rowstr[j][n[j]];
     });
     bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreate(&b->ev0) == cudaSuccess && cudaEventCreate(&b->ev1) == cudaSuccess &&
-              !balloc(&b->d_sys, nsys) && !balloc(&b->d_order, nsys) &&
+              !balloc(&b->d_sys, nsys) && !balloc(&b->d_slots, size_t(nsys) * kMaxTeam) &&
               !balloc(&b->d_rowstr, rows_total) && !balloc(&b->d_colidx, nnz_total + 64) &&
               !balloc(&b->d_a, nnz_total + 64) && !balloc(&b->d_a32, nnz_total + 64) &&
               !balloc(&b->d_x, vec_total) && !balloc(&b->d_z, vec_total) &&
               !balloc(&b->d_r, vec_total) && !balloc(&b->d_q, vec_total) &&
-              !balloc(&b->d_queue, 1) && !balloc(&b->d_zeta, nsys) && !balloc(&b->d_rnorm, nsys) &&
+              !balloc(&b->d_pg, vec_total) && !balloc(&b->d_queue, 1) &&
+              !balloc(&b->d_team_sync, size_t(nsys) * 2 * kSyncStride) &&
+              !balloc(&b->d_team_part, size_t(nsys) * 2 * kMaxTeam * kTeamValues) &&
+              !balloc(&b->d_dev_status, 1) && !balloc(&b->d_zeta, nsys) && !balloc(&b->d_rnorm, nsys) &&
               !balloc(&b->d_iters, nsys) && !balloc(&b->d_status, nsys) &&
-              !balloc(&b->d_redo, nsys) && !balloc(&b->d_hx, kMaxRecycle * vec_total) &&
+              !balloc(&b->d_hx, kMaxRecycle * vec_total) &&
               !balloc(&b->d_hw, kMaxRecycle * vec_total);
     if (!ok) {
         batch_release(b);
@@ -686,9 +961,7 @@ int cgb_batch_create(int device, int nsys, const int *n, const int *const *rowst
         }
     }
     to_fp32_batch<<<4 * b->sms, 256, 0, b->stream>>>(b->d_a, b->d_a32, nnz_total);
-    if (cudaMemcpy(b->d_order, order.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice) !=
-            cudaSuccess ||
-        cudaStreamSynchronize(b->stream) != cudaSuccess || apply_lanes(b) != CGB_OK) {
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) {
         batch_release(b);
         return set_error(CGB_ERR_CUDA, "batch set-up failed");
     }
@@ -725,47 +998,91 @@ int cgb_batch_solve(cgb_batch *b, const cgb_batch_params *params, double *zeta, 
 }
 
 // Autotuner: times the batch (mode and sizes of `params`) for each block
-// shape {512, 1024} and each lane policy (row-length thresholds for 4/8/16/32
-// lanes per row), keeps the fastest and reports it.
+// shape {512 threads with 4 or 8 entries a lane in flight, 1024 threads
+// with 4} and each lane policy (row-length thresholds for 4/8/16/32
+// lanes per row), then for the best of those each team policy (no teams,
+// team_frac 0.25, 0.5, 1), keeps the fastest and reports it.
 int cgb_batch_tune(cgb_batch *b, const cgb_batch_params *params, int *block_out, double *t0_out,
                    double *t1_out, double *t2_out, double *best_ms)
 {
     if (!b || !params) return set_error(CGB_ERR_INVALID, "batch: null argument");
     BT_TRY(cudaSetDevice(b->device));
     struct Cand {
-        int block;
+        int block, unroll;
         double t0, t1, t2;
+        double team_frac;
     };
-    const Cand cands[] = {{512, 16, 40, 96},  {512, 8, 24, 64},   {512, 24, 64, 160},
-                          {1024, 16, 40, 96}, {1024, 8, 24, 64},  {512, 1e9, 1e9, 0}};
+    const Cand shapes[] = {{512, 4, 16, 40, 96, 0.5},  {512, 4, 8, 24, 64, 0.5},
+                           {512, 4, 24, 64, 160, 0.5}, {512, 8, 16, 40, 96, 0.5},
+                           {512, 8, 8, 24, 64, 0.5},   {512, 8, 24, 64, 160, 0.5},
+                           {1024, 4, 16, 40, 96, 0.5}, {1024, 4, 8, 24, 64, 0.5},
+                           {512, 4, 1e9, 1e9, 0, 0.5}};
     double best = 1e30;
-    Cand bc = cands[0];
-    for (const Cand &c : cands) {
+    Cand bc = shapes[0];
+    auto trial = [&](const Cand &c) -> int {
         b->block = c.block;
+        b->unroll = c.unroll;
         b->t0 = c.t0;
         b->t1 = c.t1;
         b->t2 = c.t2;
-        int st = apply_lanes(b);
-        if (st) return st;
+        b->team_frac = c.team_frac;
         double ms = 0.0;
-        st = launch(b, *params, &ms);
+        const int st = launch(b, *params, &ms);
         if (st) return st;
         if (ms < best) {
             best = ms;
             bc = c;
         }
+        return CGB_OK;
+    };
+    for (const Cand &c : shapes) {
+        const int st = trial(c);
+        if (st) return st;
+    }
+    const Cand shape = bc;
+    for (double f : {0.0, 0.25, 1.0}) {
+        Cand c = shape;
+        c.team_frac = f;
+        const int st = trial(c);
+        if (st) return st;
     }
     b->block = bc.block;
+    b->unroll = bc.unroll;
     b->t0 = bc.t0;
     b->t1 = bc.t1;
     b->t2 = bc.t2;
-    int st = apply_lanes(b);
-    if (st) return st;
+    b->team_frac = bc.team_frac;
     if (block_out) *block_out = bc.block;
     if (t0_out) *t0_out = bc.t0;
     if (t1_out) *t1_out = bc.t1;
     if (t2_out) *t2_out = bc.t2;
     if (best_ms) *best_ms = best;
+    return CGB_OK;
+}
+
+int cgb_batch_policy(cgb_batch *b, int *unroll, double *team_frac, int *teams)
+{
+    if (!b) return set_error(CGB_ERR_INVALID, "batch: null argument");
+    if (unroll) *unroll = b->block > 512 ? 4 : b->unroll;
+    if (team_frac) *team_frac = b->team_frac;
+    if (teams) {
+        // the current policy's teams (tune may have tried another last)
+        if (b->resident > 0) {
+            const int st = apply_policy(b, b->resident);
+            if (st) return st;
+        }
+        int t = 0;
+        for (const SysDesc &d : b->desc) t += d.team > 1;
+        *teams = t;
+    }
+    return CGB_OK;
+}
+
+int cgb_batch_set_team_frac(cgb_batch *b, double team_frac)
+{
+    if (!b || !(team_frac >= 0.0) || team_frac > 1e6)
+        return set_error(CGB_ERR_INVALID, "batch: team_frac must be in [0, 1e6]");
+    b->team_frac = team_frac;
     return CGB_OK;
 }
 

@@ -764,6 +764,12 @@ static __global__ void __launch_bounds__(kSlicedBlock, 1) outer_step_fp64_sliced
     outer_step_body<SlicedSpmv>(A);
 }
 
+// the same with the L2 prefetch of each warp's next-block slices
+static __global__ void __launch_bounds__(kSlicedBlock, 1) outer_step_fp64_sliced_pf(OuterArgs A)
+{
+    outer_step_body<SlicedSpmvPf>(A);
+}
+
 template <int LPR>
 __global__ void __launch_bounds__(512, 2) outer_step_mixed(OuterArgs A)
 {
@@ -773,6 +779,11 @@ __global__ void __launch_bounds__(512, 2) outer_step_mixed(OuterArgs A)
 static __global__ void __launch_bounds__(kSlicedMixedBlock, 1) outer_step_mixed_sliced(OuterArgs A)
 {
     outer_step_mixed_body<SlicedSpmvMixed>(A);
+}
+
+static __global__ void __launch_bounds__(kSlicedMixedBlock, 1) outer_step_mixed_sliced_pf(OuterArgs A)
+{
+    outer_step_mixed_body<SlicedSpmvMixedPf>(A);
 }
 
 // lanes per row of the preconditioner products (F has about half of A's
@@ -852,6 +863,16 @@ static __global__ void __launch_bounds__(kSlicedBlock, 1) spmv_dot_sliced(SpmvAr
 static __global__ void __launch_bounds__(kSlicedBlock, 1) spmv_dot_sliced32(SpmvArgs S)
 {
     spmv_dot_body<SlicedSpmv, 2>(S);
+}
+
+static __global__ void __launch_bounds__(kSlicedBlock, 1) spmv_dot_sliced_pf(SpmvArgs S)
+{
+    spmv_dot_body<SlicedSpmvPf, 1>(S);
+}
+
+static __global__ void __launch_bounds__(kSlicedBlock, 1) spmv_dot_sliced32_pf(SpmvArgs S)
+{
+    spmv_dot_body<SlicedSpmvPf, 2>(S);
 }
 
 // ------------------------------------------------------------- utilities

@@ -62,7 +62,8 @@ __device__ __forceinline__ void raise_status(int *status, int code)
     atomicCAS(status, kDevOk, code);
 }
 
-// Grid-wide barrier for a co-resident (cooperative) grid.  Thread 0 of each
+// Barrier of `members` co-resident CTAs (the whole grid for grid_barrier;
+// the CTAs of one system's team in the batch kernel).  Thread 0 of each
 // CTA arrives with an acq_rel atomic; the last arriver resets the count and
 // releases the next generation; the others poll the generation with acquire
 // loads, which also makes every write issued before the barrier by any CTA
@@ -70,29 +71,30 @@ __device__ __forceinline__ void raise_status(int *status, int code)
 // another CTA has raised the status word, the barrier records kDevTimeout
 // (first failure wins) and returns false; the caller then leaves the kernel.
 // The host resets count/gen after a failed launch.
-__device__ __forceinline__ bool grid_barrier(const GridBarrier &gb)
+__device__ __forceinline__ bool counted_barrier(unsigned *count, unsigned *gen, unsigned members,
+                                                int *status, long long limit_ns)
 {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        const unsigned g = ld_acquire_u32(gb.gen);
+        const unsigned g = ld_acquire_u32(gen);
         __threadfence();
-        const unsigned arrived = atom_add_acq_rel_u32(gb.count, 1u);
-        if (arrived == gridDim.x - 1) {
-            atomicExch(gb.count, 0u);
-            st_release_u32(gb.gen, g + 1u);
+        const unsigned arrived = atom_add_acq_rel_u32(count, 1u);
+        if (arrived == members - 1) {
+            atomicExch(count, 0u);
+            st_release_u32(gen, g + 1u);
         } else {
             const unsigned long long t0 = global_ns();
             unsigned spins = 0;
-            while (ld_acquire_u32(gb.gen) == g) {
+            while (ld_acquire_u32(gen) == g) {
                 if (((++spins) & 63u) == 0u) {
-                    if (ld_relaxed_i32(gb.status) != kDevOk) {
+                    if (ld_relaxed_i32(status) != kDevOk) {
                         ok = 0;
                         break;
                     }
-                    if ((long long)(global_ns() - t0) > gb.limit_ns) {
-                        raise_status(gb.status, kDevTimeout);
+                    if ((long long)(global_ns() - t0) > limit_ns) {
+                        raise_status(status, kDevTimeout);
                         ok = 0;
                         break;
                     }
@@ -103,6 +105,11 @@ __device__ __forceinline__ bool grid_barrier(const GridBarrier &gb)
     }
     __syncthreads();
     return s_ok != 0;
+}
+
+__device__ __forceinline__ bool grid_barrier(const GridBarrier &gb)
+{
+    return counted_barrier(gb.count, gb.gen, gridDim.x, gb.status, gb.limit_ns);
 }
 
 template <int W>
@@ -122,6 +129,20 @@ __device__ __forceinline__ float group_sum_f(float v, unsigned mask)
 }
 
 __device__ __forceinline__ double warp_sum(double v) { return group_sum<32>(v, 0xffffffffu); }
+
+// group_sum / group_sum_f for a group width w (a power of two <= 32) known
+// only at run time: the same xor steps in the same order, so the same sums.
+__device__ __forceinline__ double group_sum_rt(double v, unsigned mask, int w)
+{
+    for (int off = w >> 1; off > 0; off >>= 1) v += __shfl_xor_sync(mask, v, off);
+    return v;
+}
+
+__device__ __forceinline__ float group_sum_f_rt(float v, unsigned mask, int w)
+{
+    for (int off = w >> 1; off > 0; off >>= 1) v += __shfl_xor_sync(mask, v, off);
+    return v;
+}
 
 // Sum of `v` over the CTA, valid in thread 0.  `scratch` holds >= 32 doubles.
 // Fixed shuffle/smem order: deterministic for a given launch shape.

@@ -272,6 +272,24 @@ __host__ __device__ inline size_t sliced_smem_bytes(int max_rows, int nacc)
     return 128 + kStagingBytes + size_t(nacc) * size_t(max_rows) * sizeof(double);
 }
 
+// L2 prefetch of one slice (all lanes' entries: per step pair 64 values and
+// 64 columns, contiguous), spread over the warp's lanes; prefetches do not
+// wait, so a warp pulls its next block's slices toward L2 while it works.
+template <typename ST>
+__device__ __forceinline__ void prefetch_slice_l2(const ST *vals, const unsigned short *scol,
+                                                  unsigned base, int wp, int lane)
+{
+    constexpr int kVLines = int((64 * sizeof(ST) + 127) / 128);  // 128-byte lines of values a pair
+    const int lines = wp * (kVLines + 1);
+    for (int L = lane; L < lines; L += 32) {
+        const int m = L / (kVLines + 1), k = L % (kVLines + 1);
+        const char *ptr = k < kVLines
+                              ? reinterpret_cast<const char *>(vals + base + 64u * unsigned(m)) + 128 * k
+                              : reinterpret_cast<const char *>(scol + base + 64u * unsigned(m));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+    }
+}
+
 // kU64 / kU32: step pairs in flight per lane for FP64 / FP32 values (more
 // for kernels with fewer, register-richer threads); BF16 values take twice
 // the FP32 count.
@@ -284,7 +302,7 @@ __host__ __device__ inline size_t sliced_smem_bytes(int max_rows, int nacc)
 // With an FP32 vector a warp reads its first slice's metadata of a block
 // before waiting for the block's copy, and the next slice's metadata while
 // it works on the current one.
-template <int kU64, int kU32, bool kOutline = false>
+template <int kU64, int kU32, bool kOutline = false, bool kL2Prefetch = true>
 struct SlicedSpmvT {
     static constexpr bool kSliced = true;
     // Dynamic shared memory: the control words first (fixed offsets), then
@@ -380,12 +398,26 @@ struct SlicedSpmvT {
             fence_proxy_async();  // v was written by generic stores before the grid barrier
             for (int b = 0; b < S && b < M.nblk; b++) issue(M, v, n, b, b);
         }
+        // this warp's slices of block b toward L2 (one block ahead of use)
+        // (only in the kL2Prefetch instances: it pays where the walk is
+        // latency-bound -- short column-block chunks -- and costs where it
+        // streams, so the plan's autotuner picks the instance)
+        auto prefetch_block = [&](int b) {
+            if (!kL2Prefetch || b >= M.nblk) return;
+            const int t0 = __ldg(M.chunk_slice + chunk0 + b);
+            const int t1 = __ldg(M.chunk_slice + chunk0 + b + 1);
+            for (int t = t0 + (warp + (b * 7) % nwarps) % nwarps; t < t1; t += nwarps)
+                prefetch_slice_l2(vals, M.scol, __ldg(M.slice_off + t), __ldg(M.slice_width + t) >> 1,
+                                  lane);
+        };
+        prefetch_block(0);
         __syncthreads();
         bool failed = false;
         for (int b = 0; b < M.nblk && !failed; b++) {
             const int slot = b % S;
             const int s0 = __ldg(M.chunk_slice + chunk0 + b);  // this matrix's blocks
             const int s1 = __ldg(M.chunk_slice + chunk0 + b + 1);
+            prefetch_block(b + 1);
             // rotate the warp -> slice assignment from block to block so the
             // widest slices do not always land on the same warps
             const int rot = (b * 7) % nwarps;
@@ -501,8 +533,10 @@ struct SlicedSpmvT {
 // Per kernel (pair counts and block shapes measured on B200): the FP64
 // outer step and the standalone SpMVs (768 threads, 80 registers), the
 // mixed outer step (768), the preconditioned one (512, 128 registers).
-using SlicedSpmv = SlicedSpmvT<6, 6>;
-using SlicedSpmvMixed = SlicedSpmvT<4, 6>;
-using SlicedSpmvPcg = SlicedSpmvT<4, 6>;
+using SlicedSpmv = SlicedSpmvT<6, 6, false, false>;
+using SlicedSpmvPf = SlicedSpmvT<6, 6, false, true>;
+using SlicedSpmvMixed = SlicedSpmvT<4, 6, false, false>;
+using SlicedSpmvMixedPf = SlicedSpmvT<4, 6, false, true>;
+using SlicedSpmvPcg = SlicedSpmvT<4, 6, false, false>;
 
 }  // namespace cgb

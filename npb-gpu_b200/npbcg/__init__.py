@@ -154,6 +154,10 @@ _SIGNATURES = {
     "cgb_batch_tune": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchParams),
                                       ctypes.POINTER(ctypes.c_int)] +
                        [ctypes.POINTER(ctypes.c_double)] * 4),
+    "cgb_batch_policy": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ctypes.c_int)]),
+    "cgb_batch_set_team_frac": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "cgb_host_alloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_longlong]),
     "cgb_host_free": (ctypes.c_int, [ctypes.c_void_p]),
     "cgb_device_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
@@ -323,8 +327,9 @@ class Session:
         _check(lib().cgb_plan_info(self._h, *[ctypes.byref(x) for x in v], ctypes.byref(smem),
                                    ctypes.byref(entries)))
         kind, lpr, grid, block = (x.value for x in v)
-        return dict(kind={1: "row", 2: "sliced"}.get(kind, kind), lanes_per_row=lpr, grid=grid,
-                    block=block, smem=smem.value, layout_entries=entries.value)
+        return dict(kind={1: "row", 2: "sliced", 3: "sliced"}.get(kind, kind), l2_prefetch=kind == 3,
+                    lanes_per_row=lpr, grid=grid, block=block, smem=smem.value,
+                    layout_entries=entries.value)
 
     def selftest_wait_timeout(self, limit_ns):
         """Returns (status, device_status) of the bounded-wait self-test."""
@@ -580,4 +585,16 @@ class Batch:
         _check(lib().cgb_batch_tune(self._h, ctypes.byref(P), ctypes.byref(block),
                                     *[ctypes.byref(x) for x in t]))
         return dict(block=block.value, thresholds=(t[0].value, t[1].value, t[2].value),
-                    best_ms=t[3].value)
+                    best_ms=t[3].value, **self.policy())
+
+    def policy(self):
+        """Entries a lane loads ahead, the team fraction, and how many systems
+        the last launch solved with a team of CTAs."""
+        u, f, t = ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
+        _check(lib().cgb_batch_policy(self._h, ctypes.byref(u), ctypes.byref(f), ctypes.byref(t)))
+        return dict(unroll=u.value, team_frac=f.value, teams=t.value)
+
+    def set_team_frac(self, frac):
+        """0: every system on one CTA; larger systems get teams of CTAs below
+        their work per CTA > frac x the batch's work per resident CTA."""
+        _check(lib().cgb_batch_set_team_frac(self._h, float(frac)))

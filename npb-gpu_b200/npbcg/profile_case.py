@@ -25,7 +25,7 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--niter", type=int, default=2)
     ap.add_argument("--lanes", type=int, default=0)
-    ap.add_argument("--kind", type=int, default=0, help="0 auto, 1 row, 2 sliced")
+    ap.add_argument("--kind", type=int, default=0, help="0 auto, 1 row, 2 sliced, 3 sliced with L2 prefetch")
     ap.add_argument("--fp32", action="store_true")
     a = ap.parse_args()
     c = npbcg.CLASSES[a.cls]

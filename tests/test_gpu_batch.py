@@ -125,6 +125,40 @@ def test_batch_tune_keeps_results(cgb):
     assert np.all(rel[conv] <= 1e-10), rel[conv].max()
 
 
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_batch_teams_match_single_cta(cgb, oracle, mode):
+    """Systems split over teams of 2, 4 and 8 CTAs (rows shared, the search
+    vector exchanged through global memory at each update) give the zeta of
+    the one-CTA solve to 1e-10 (the sums only change order), and the FP64
+    mode still matches the oracle."""
+    specs = [(20000, 13, 30.0, 314159265.0), (9000, 11, 19.0, 271828183.0),
+             (5000, 9, 15.0, 123456789.0), (1400, 7, 10.0, 314159265.0)]
+    systems, shifts = build(cgb, specs)
+    kw = dict(mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=200) if mode == "mixed" else {}
+    with cgb.Batch(systems, shifts) as b:
+        b.set_team_frac(0.0)
+        alone = b.solve(niter=8, **kw)
+        assert b.policy()["teams"] == 0
+        b.set_team_frac(0.001)   # every system above 0.1 % of the work per CTA: teams of 8
+        teams = b.solve(niter=8, **kw)
+        assert b.policy()["teams"] == len(specs)
+        # teams while the work per CTA is above 5 x the batch's mean per CTA:
+        # the three larger systems (12.5 to 100 x), not the smallest (2.2 x)
+        b.set_team_frac(5.0)
+        some = b.solve(niter=8, **kw)
+        assert b.policy()["teams"] == len(specs) - 1
+    for out in (teams, some):
+        assert np.array_equal(out["status"], alone["status"])
+        rel = np.abs(out["zeta"] - alone["zeta"]) / np.abs(alone["zeta"])
+        assert np.all(rel <= 1e-10), rel.max()
+        if mode == "fp64":
+            assert np.array_equal(out["iters"], alone["iters"])
+    if mode == "fp64":
+        rs, ci, a = systems[3]
+        o = oracle.power_iterate(rs, ci, a, shifts[3], 8)
+        assert abs(teams["zeta"][3] - o["zeta"][-1]) <= 1e-10 * abs(o["zeta"][-1])
+
+
 def test_batch_rejects_oversize(cgb):
     rs = np.zeros(27002, np.int32)
     with pytest.raises(cgb.CgbError) as e:

@@ -193,14 +193,16 @@ def test_spmv_timer_runs(cgb):
     assert 0 < ms < 50
 
 
-@pytest.mark.parametrize("kind,lpr", [(1, 8), (1, 16), (1, 32), (2, 0)])
+@pytest.mark.parametrize("kind,lpr", [(1, 8), (1, 16), (1, 32), (2, 0), (3, 0)])
 def test_spmv_kernels_agree_class_b(cgb, golden, kind, lpr):
-    """Row and sliced SpMV policies reproduce the reference trace."""
+    """Row and sliced SpMV policies (sliced with and without the L2 prefetch)
+    reproduce the reference trace."""
     n, nonzer, niter, shift = PARAMS["B"]
     rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
     with cgb.Session(rs, ci, a, spmv_kernel=kind, lanes_per_row=lpr) as s:
         plan = s.plan()
-        assert plan["kind"] == {1: "row", 2: "sliced"}[kind]
+        assert plan["kind"] == {1: "row", 2: "sliced", 3: "sliced"}[kind]
+        assert plan["l2_prefetch"] == (kind == 3)
         out = s.power_iterate(niter, shift)
         z, p, q, r, rn = s.conj_grad(np.ones(n))
     ref = np.array(golden["B"]["seeds"]["314159265.0"]["zeta"])
@@ -219,6 +221,21 @@ def test_sliced_spmv_matches_oracle_product(cgb, oracle):
     zo, po, qo, ro, rno = oracle.conj_grad(rs, ci, a, x)
     assert np.linalg.norm(z[:n] - zo[:n]) <= 1e-12 * np.linalg.norm(zo[:n])
     assert np.linalg.norm(r[:n] - ro[:n]) <= 1e-12 * np.linalg.norm(ro[:n])
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_l2_prefetch_changes_no_result(cgb, mode):
+    """The prefetch only moves lines toward L2: the sliced plan with it gives
+    bit-identical zeta and rnorm traces to the plan without it (class B)."""
+    n, nonzer, niter, shift = PARAMS["B"]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    kw = dict(mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=100) if mode == "mixed" else {}
+    outs = []
+    for kind in (2, 3):
+        with cgb.Session(rs, ci, a, spmv_kernel=kind) as s:
+            outs.append(s.power_iterate(5, shift, **kw))
+    assert np.array_equal(outs[0]["zeta"], outs[1]["zeta"])
+    assert np.array_equal(outs[0]["rnorm"], outs[1]["rnorm"])
 
 
 def test_sliced_refused_for_small_or_unsorted(cgb):
