@@ -126,15 +126,16 @@ def physical_index(local_rank):
 
 
 def load_traffic():
-    """Per-launch DRAM bytes of the outer-step kernel from the committed ncu summary."""
+    """Per-launch DRAM bytes of the outer-step kernel from the committed ncu
+    summary: (kernel, workload, MB of the stream kept in L2) -> bytes."""
     path = os.path.join(ROOT, "profiles", "traffic_per_launch.txt")
     out = {}
     if os.path.exists(path):
         for line in open(path):
             parts = line.split()
-            if len(parts) >= 3 and not line.startswith("#"):
+            if len(parts) >= 4 and not line.startswith("#"):
                 try:
-                    out[(parts[0], parts[1])] = float(parts[2])
+                    out[(parts[0], parts[1], int(parts[2]))] = float(parts[3])
                 except ValueError:
                     pass
     return out
@@ -397,7 +398,8 @@ def our_arm(args, rank, world, local_rank):
     bytes_launch = outer_step_bytes(n, nnz)
     achieved = bytes_launch / (kernel_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
-    traffic = load_traffic().get((kernel.split("<")[0], f"class{CLASS}"))
+    traffic = load_traffic().get((kernel.split("<")[0], f"class{CLASS}",
+                                  int(round(plan.get("l2_keep_mb", 0.0)))))
     spmv_ms = sess.time_spmv(50)
     spmv_gbs = spmv_bytes(n, nnz) / (spmv_ms / 1e3) / 1e9
 

@@ -276,6 +276,16 @@ int cgb_time_outer_steps(cgb_session *s, int niter, double shift, double *kernel
 int cgb_plan_info(cgb_session *s, int *kind, int *lanes_per_row, int *grid, int *block,
                   long long *smem_bytes, long long *layout_entries);
 
+/* Bytes of the sliced matrix stream that the solves keep resident in L2
+ * from one product to the next (a fraction budget / stream of its lines is
+ * loaded at L2 priority evict_last, the rest evict_first); chosen by the
+ * autotuner among 0, 48 MB and 64 MB; 0 for the row plan.  Products whose
+ * stream fits the budget read the matrix from L2 after the first. */
+int cgb_plan_l2_keep(cgb_session *s, double *bytes);
+/* Overrides the autotuner's choice (>= 0; 0 = pure stream).  Results do not
+ * depend on it: it changes cache priorities only. */
+int cgb_set_l2_keep(cgb_session *s, double bytes);
+
 /* Grid barrier time-out self-test: runs a 2-CTA kernel whose second CTA never
  * arrives, with a wait limit of `limit_ns`, and reports the status the host
  * reads back (CGB_ERR_TIMEOUT expected).  The session stays usable. */

@@ -876,6 +876,17 @@ static __global__ void __launch_bounds__(kSlicedBlock, 1) spmv_dot_sliced32_pf(S
 }
 
 // ------------------------------------------------------------- utilities
+// Demotes the L2 lines of [p, p + bytes) to normal eviction priority: the
+// lines a sliced walk kept at evict_last, so that whoever uses the L2 next
+// starts from plain replacement.  Touches no data (a priority hint on lines
+// that are cached, nothing for the others).
+static __global__ void l2_demote(const char *p, size_t bytes)
+{
+    const size_t step = size_t(gridDim.x) * blockDim.x * 128;
+    for (size_t o = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) * 128; o < bytes; o += step)
+        asm volatile("applypriority.global.L2::evict_normal [%0], 128;" ::"l"(p + o) : "memory");
+}
+
 // x = 1 over n+1 entries (cg.cu:485-488).
 static __global__ void fill_ones(double *x, int count)
 {

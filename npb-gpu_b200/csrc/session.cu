@@ -93,6 +93,7 @@ struct Plan {
     int block_mixed = 512;  // mixed outer step
     int block_pcg = 512;    // preconditioned outer step
     int prefetch = 0;       // sliced: L2 prefetch of the next block's slices
+    double l2_keep = 0.0;   // sliced: bytes of the matrix stream kept in L2 across products
     int grid = 0;
     size_t smem = 0;
 };
@@ -247,6 +248,7 @@ struct cgb_session {
     int seg_stride = 0;
     int nblk = 0;
     bool sorted = false;
+    bool l2_marked = false;  // a solve ran with an L2 keep fraction (lines at evict_last)
     int sliced_grid = 0;   // grid the layout was built for (0: none)
     int sliced_max_rows = 0;
     int sliced_nacc = 2;           // row accumulators (4 when they fit: FP32 pipeline depth)
@@ -266,6 +268,7 @@ struct cgb_session {
     // graph of the last power iteration shape
     cudaGraphExec_t graph = nullptr;
     cgb_solve_params g_params{};
+    std::vector<unsigned char> g_sig;  // GraphSig bytes of the captured iteration
     bool g_valid = false;
 
     double *x() { return d_vec; }
@@ -330,6 +333,19 @@ void release(cgb_session *s)
     if (!s) return;
     cudaSetDevice(s->device);
     drop_graph(s);
+    if (s->l2_marked) {
+        // lines this session kept at evict_last go back to normal priority
+        const SliceSet &t = s->sa;
+        const std::pair<const void *, size_t> spans[3] = {
+            {t.sval, size_t(t.entries) * sizeof(double)},
+            {t.sval32, size_t(t.entries) * sizeof(float)},
+            {t.scol, size_t(t.entries) * sizeof(unsigned short)}};
+        for (const auto &sp : spans)
+            if (sp.first && sp.second)
+                l2_demote<<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
+                    static_cast<const char *>(sp.first), sp.second);
+        cudaStreamSynchronize(s->stream);
+    }
     free_sliced(s);
     dev_free(s->d_rowstr);
     dev_free(s->d_colidx);
@@ -380,6 +396,19 @@ void set_slices(cgb_session *s, const SliceSet &t, MatrixView *M)
     M->interleaved = t.interleaved;
 }
 
+// Keep fractions of the sliced streams for a solve whose products are FP64
+// (fp32 = 0) or FP32 (fp32 = 1): the plan's L2 budget over the stream's
+// bytes (values + 16-bit columns); the other stream is not kept.
+void set_keep(const cgb_session *s, MatrixView *M, int fp32)
+{
+    M->keep64 = M->keep32 = M->keep16 = 0.f;
+    if (s->plan.kind != kKindSliced || s->plan.l2_keep <= 0.0 || s->sa.entries <= 0) return;
+    const double bytes = double(s->sa.entries) * (fp32 ? 6.0 : 10.0);
+    const float f = float(std::min(1.0, s->plan.l2_keep / bytes));
+    if (fp32) M->keep32 = f;
+    else M->keep64 = f;
+}
+
 MatrixView matrix_view(cgb_session *s)
 {
     MatrixView M{};
@@ -388,6 +417,7 @@ MatrixView matrix_view(cgb_session *s)
     M.a = s->d_a;
     M.a32 = s->d_a32;
     set_slices(s, s->sa, &M);
+    set_keep(s, &M, 0);
     return M;
 }
 
@@ -432,6 +462,7 @@ OuterArgs outer_args(cgb_session *s)
 
 cudaError_t launch_outer(cgb_session *s, OuterKernel k, const OuterArgs &A)
 {
+    if (A.M.keep64 > 0.f || A.M.keep32 > 0.f || A.M.keep16 > 0.f) s->l2_marked = true;
     const Plan &P = s->plan;
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(P.grid);
@@ -718,6 +749,8 @@ int time_plan_spmv(cgb_session *s, int reps, int fp32, double *ms_out)
 {
     if (fp32 && !s->d_a32) return set_error(CGB_ERR_STATE, "no FP32 copy (keep_fp32_copy = 0)");
     SpmvArgs S = spmv_args(s, fp32);
+    set_keep(s, &S.A.M, fp32);
+    if (S.A.M.keep64 > 0.f || S.A.M.keep32 > 0.f) s->l2_marked = true;
     const Plan &P = s->plan;
     fill_ones<<<s->prop.multiProcessorCount, 256, 0, s->stream>>>(s->p(), s->n + 1);
     if (fp32) {
@@ -807,8 +840,16 @@ int choose_plan(cgb_session *s)
     if (want == 0 || want == kKindSliced || want == kKindSlicedPrefetch) {
         // the sliced plan with and without the L2 prefetch of each warp's
         // next-block slices (latency-bound short chunks gain, streaming ones lose)
-        if (want != kKindSlicedPrefetch) add(kKindSliced, 0, 0);
-        if (want != kKindSliced) add(kKindSliced, 0, 1);
+        // each instance with the matrix stream kept in L2 for the budgets
+        // below (the fraction of lines at evict_last is budget / stream)
+        for (int pf = 0; pf < 2; pf++) {
+            if ((pf == 1 && want == kKindSliced) || (pf == 0 && want == kKindSlicedPrefetch)) continue;
+            for (double keep : {0.0, 48e6, 64e6}) {
+                const size_t before = cands.size();
+                add(kKindSliced, 0, pf);
+                if (cands.size() > before) cands.back().l2_keep = keep;
+            }
+        }
     }
     if (cands.empty()) return set_error(CGB_ERR_INVALID, "no kernel configuration fits these options");
     if (cands.size() == 1) return apply_plan(s, cands[0]);
@@ -878,7 +919,8 @@ int upload_matrix(cgb_session *s, const int *rowstr, const int *colidx, const do
         if (st) return st;
     }
     if (same_rows && (kept_kind == kKindRow || (s->sorted && build_sliced(s, kept_grid) == CGB_OK))) {
-        drop_graph(s);
+        // the captured graph stays if every launch argument is unchanged
+        // (buffers reused in place); cgb_power_iterate compares them
         return CGB_OK;
     }
     s->plan = Plan();
@@ -916,14 +958,9 @@ bool is_mixed(int mode) { return mode == CGB_MODE_MIXED || mode == CGB_MODE_MIXE
 
 // Enqueues one power iteration (x = 1, then niter outer-step kernels) on the
 // session stream.
-cudaError_t enqueue_power(cgb_session *s, const cgb_solve_params &P)
+// Arguments of every outer-step launch of a power iteration (`step` apart).
+OuterArgs power_args(cgb_session *s, const cgb_solve_params &P)
 {
-    cudaError_t e = cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream);
-    if (e != cudaSuccess) return e;
-    fill_ones<<<std::max(1, std::min(s->prop.multiProcessorCount, (s->n + 1 + 255) / 256)), 256, 0,
-                s->stream>>>(s->x(), s->n + 1);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
     OuterArgs A = outer_args(s);
     A.shift = P.shift;
     A.cgitmax = P.cgitmax;
@@ -932,9 +969,53 @@ cudaError_t enqueue_power(cgb_session *s, const cgb_solve_params &P)
     A.refresh_every = P.refresh_every > 0 ? P.refresh_every : 10;
     A.finish = 1;
     A.recycle = P.mode == CGB_MODE_FP64 ? 0 : P.recycle;
-    const OuterKernel k = P.mode == CGB_MODE_MIXED_LEARNED ? s->plan.pcg
-                          : P.mode == CGB_MODE_MIXED       ? s->plan.mixed
-                                                           : s->plan.fp64;
+    // the stream that dominates the mode is the one kept in L2 (none in the
+    // preconditioned mode: there it measured slower, 63.4 vs 62.0 ms at C)
+    if (P.mode == CGB_MODE_MIXED_LEARNED) A.M.keep64 = A.M.keep32 = A.M.keep16 = 0.f;
+    else set_keep(s, &A.M, is_mixed(P.mode) ? 1 : 0);
+    return A;
+}
+
+OuterKernel power_kernel(const cgb_session *s, const cgb_solve_params &P)
+{
+    return P.mode == CGB_MODE_MIXED_LEARNED ? s->plan.pcg
+           : P.mode == CGB_MODE_MIXED       ? s->plan.mixed
+                                            : s->plan.fp64;
+}
+
+// What a captured power iteration depends on besides its parameters: the
+// launch arguments and shapes.  Compared bytewise (built zero-filled), so a
+// re-upload that keeps every buffer and the plan keeps the graph.
+struct GraphSig {
+    OuterArgs A;
+    OuterKernel k;
+    int grid, block, block_mixed, block_pcg;
+    size_t smem;
+};
+
+void graph_sig(cgb_session *s, const cgb_solve_params &P, GraphSig *g)
+{
+    std::memset(g, 0, sizeof(*g));
+    const OuterArgs A = power_args(s, P);
+    std::memcpy(&g->A, &A, sizeof(A));
+    g->k = power_kernel(s, P);
+    g->grid = s->plan.grid;
+    g->block = s->plan.block;
+    g->block_mixed = s->plan.block_mixed;
+    g->block_pcg = s->plan.block_pcg;
+    g->smem = s->plan.smem;
+}
+
+cudaError_t enqueue_power(cgb_session *s, const cgb_solve_params &P)
+{
+    cudaError_t e = cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream);
+    if (e != cudaSuccess) return e;
+    fill_ones<<<std::max(1, std::min(s->prop.multiProcessorCount, (s->n + 1 + 255) / 256)), 256, 0,
+                s->stream>>>(s->x(), s->n + 1);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    OuterArgs A = power_args(s, P);
+    const OuterKernel k = power_kernel(s, P);
     // the sliced preconditioned kernel reads F / F^T slices (ensure_prec_slices)
     if (P.mode == CGB_MODE_MIXED_LEARNED && s->plan.kind == kKindSliced && A.F.srow == nullptr)
         return cudaErrorInvalidValue;
@@ -1188,7 +1269,12 @@ int cgb_power_iterate(cgb_session *s, const cgb_solve_params *params, double *ze
         if (st) return st;
     }
     if (s->opts.use_graph) {
-        if (!(s->g_valid && same_params(s->g_params, P))) {
+        GraphSig sig;
+        graph_sig(s, P, &sig);
+        const unsigned char *sb = reinterpret_cast<const unsigned char *>(&sig);
+        const bool same_sig = s->g_sig.size() == sizeof(sig) &&
+                              std::memcmp(s->g_sig.data(), sb, sizeof(sig)) == 0;
+        if (!(s->g_valid && same_params(s->g_params, P) && same_sig)) {
             drop_graph(s);
             cudaGraph_t g = nullptr;
             CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
@@ -1206,6 +1292,7 @@ int cgb_power_iterate(cgb_session *s, const cgb_solve_params *params, double *ze
                 return set_error(CGB_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
             }
             s->g_params = P;
+            s->g_sig.assign(sb, sb + sizeof(sig));
             s->g_valid = true;
         }
         CUDA_TRY(cudaEventRecord(s->ev0, s->stream));
@@ -1343,6 +1430,21 @@ int cgb_plan_info(cgb_session *s, int *kind, int *lanes_per_row, int *grid, int 
     if (block) *block = s->plan.block;
     if (smem_bytes) *smem_bytes = (long long)s->plan.smem;
     if (layout_entries) *layout_entries = s->plan.kind == kKindSliced ? s->sa.entries : s->nnz;
+    return CGB_OK;
+}
+
+int cgb_plan_l2_keep(cgb_session *s, double *bytes)
+{
+    if (!s || !bytes) return set_error(CGB_ERR_INVALID, "bad arguments");
+    *bytes = s->plan.kind == kKindSliced ? s->plan.l2_keep : 0.0;
+    return CGB_OK;
+}
+
+int cgb_set_l2_keep(cgb_session *s, double bytes)
+{
+    if (!s || !(bytes >= 0.0) || bytes > 1e12) return set_error(CGB_ERR_INVALID, "bytes must be in [0, 1e12]");
+    s->plan.l2_keep = bytes;
+    drop_graph(s);
     return CGB_OK;
 }
 

@@ -56,6 +56,62 @@ __device__ __forceinline__ double widen(double v) { return v; }
 __device__ __forceinline__ float widen(float v) { return v; }
 __device__ __forceinline__ float widen(__nv_bfloat16 v) { return __bfloat162float(v); }
 
+// L2 policy of a matrix stream: a `keep` fraction of its lines (chosen by
+// the hardware from their addresses, so the same lines every product) at
+// priority evict_last, the others evict_first.
+__device__ __forceinline__ uint64_t l2_stream_policy(float keep)
+{
+    uint64_t pol;
+    if (keep > 0.f)
+        asm("createpolicy.fractional.L2::evict_last.L2::evict_first.b64 %0, %1;"
+            : "=l"(pol)
+            : "f"(fminf(keep, 1.f)));
+    else
+        asm("createpolicy.fractional.L2::evict_first.b64 %0, %1;" : "=l"(pol) : "f"(1.f));
+    return pol;
+}
+
+// Read-only loads of the matrix stream under an L2 policy (not kept in L1).
+__device__ __forceinline__ double2 ld_stream(const double2 *p, uint64_t pol)
+{
+    double2 v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+        : "=d"(v.x), "=d"(v.y)
+        : "l"(p), "l"(pol));
+    return v;
+}
+
+__device__ __forceinline__ float2 ld_stream(const float2 *p, uint64_t pol)
+{
+    float2 v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
+        : "=f"(v.x), "=f"(v.y)
+        : "l"(p), "l"(pol));
+    return v;
+}
+
+__device__ __forceinline__ unsigned ld_stream_u32(const void *p, uint64_t pol)
+{
+    unsigned v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
+__device__ __forceinline__ __nv_bfloat162 ld_stream(const __nv_bfloat162 *p, uint64_t pol)
+{
+    const unsigned u = ld_stream_u32(p, pol);
+    __nv_bfloat162 v;
+    v.x = __ushort_as_bfloat16(static_cast<unsigned short>(u & 0xffffu));
+    v.y = __ushort_as_bfloat16(static_cast<unsigned short>(u >> 16));
+    return v;
+}
+
+__device__ __forceinline__ ushort2 ld_stream(const ushort2 *p, uint64_t pol)
+{
+    const unsigned u = ld_stream_u32(p, pol);
+    return make_ushort2(static_cast<unsigned short>(u & 0xffffu), static_cast<unsigned short>(u >> 16));
+}
+
 __device__ __forceinline__ double fma_vt(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float fma_vt(float a, float b, float c) { return fmaf(a, b, c); }
 
@@ -107,6 +163,11 @@ struct MatrixView {
     int interleaved;                          // 0: CTA c owns its contiguous row range;
                                               // 1: CTA c owns rows c, c + G, c + 2G, ...
     int nacc;                                 // accumulators in shared memory (2 or 4)
+    // sliced walk: fraction of the stream's 128-byte lines (FP64, FP32, BF16
+    // values with their columns) loaded with L2 priority evict_last -- kept
+    // in L2 from one product to the next -- the rest evict_first; 0 = all
+    // evict_first (a pure stream)
+    float keep64, keep32, keep16;
 };
 
 // Rows of CTA `c` of `grid` under interleaved ownership.
@@ -377,6 +438,8 @@ struct SlicedSpmvT {
         using P2 = typename Pair<ST>::T;
         constexpr int kU = sizeof(ST) == 8 ? kU64 : sizeof(ST) == 4 ? kU32 : 2 * kU32;
         const ST *__restrict__ vals = slice_values<ST>(M);
+        const uint64_t pol =
+            l2_stream_policy(sizeof(ST) == 8 ? M.keep64 : sizeof(ST) == 4 ? M.keep32 : M.keep16);
         // slots in use: as many blocks of the vector as the staging holds,
         // at most one accumulator each
         const int S = min(M.nacc, int(kStagingBytes / (size_t(M.width) * sizeof(VT))));
@@ -432,8 +495,8 @@ struct SlicedSpmvT {
                     for (int u = 0; u < kU; u++) {
                         if (m + u < wp) {
                             const unsigned e = off + 64u * unsigned(m + u);
-                            av[u] = __ldcs(reinterpret_cast<const P2 *>(vals + e));
-                            cv[u] = __ldcs(reinterpret_cast<const ushort2 *>(M.scol + e));
+                            av[u] = ld_stream(reinterpret_cast<const P2 *>(vals + e), pol);
+                            cv[u] = ld_stream(reinterpret_cast<const ushort2 *>(M.scol + e), pol);
                         }
                     }
 #pragma unroll

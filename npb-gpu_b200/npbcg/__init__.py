@@ -154,6 +154,8 @@ _SIGNATURES = {
     "cgb_batch_tune": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchParams),
                                       ctypes.POINTER(ctypes.c_int)] +
                        [ctypes.POINTER(ctypes.c_double)] * 4),
+    "cgb_plan_l2_keep": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    "cgb_set_l2_keep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "cgb_batch_policy": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_double),
                                         ctypes.POINTER(ctypes.c_int)]),
@@ -327,9 +329,16 @@ class Session:
         _check(lib().cgb_plan_info(self._h, *[ctypes.byref(x) for x in v], ctypes.byref(smem),
                                    ctypes.byref(entries)))
         kind, lpr, grid, block = (x.value for x in v)
+        keep = ctypes.c_double()
+        _check(lib().cgb_plan_l2_keep(self._h, ctypes.byref(keep)))
         return dict(kind={1: "row", 2: "sliced", 3: "sliced"}.get(kind, kind), l2_prefetch=kind == 3,
-                    lanes_per_row=lpr, grid=grid, block=block, smem=smem.value,
-                    layout_entries=entries.value)
+                    l2_keep_mb=keep.value / 1e6, lanes_per_row=lpr, grid=grid, block=block,
+                    smem=smem.value, layout_entries=entries.value)
+
+    def set_l2_keep(self, nbytes):
+        """Bytes of the sliced matrix stream kept in L2 across products
+        (overrides the autotuner; 0 = pure stream; results unchanged)."""
+        _check(lib().cgb_set_l2_keep(self._h, float(nbytes)))
 
     def selftest_wait_timeout(self, limit_ns):
         """Returns (status, device_status) of the bounded-wait self-test."""

@@ -27,6 +27,8 @@ def main():
     ap.add_argument("--lanes", type=int, default=0)
     ap.add_argument("--kind", type=int, default=0, help="0 auto, 1 row, 2 sliced, 3 sliced with L2 prefetch")
     ap.add_argument("--fp32", action="store_true")
+    ap.add_argument("--keep-mb", type=float, default=None,
+                    help="bytes (MB) of the sliced stream kept in L2 (default: the autotuner's)")
     a = ap.parse_args()
     c = npbcg.CLASSES[a.cls]
     rs, ci, av = npbcg.makea(c["n"], c["nonzer"], npbcg.RCOND, c["shift"])
@@ -52,6 +54,8 @@ def main():
         out["sweep"] = rows
     else:
         with npbcg.Session(rs, ci, av, lanes_per_row=a.lanes, spmv_kernel=a.kind) as s:
+            if a.keep_mb is not None:
+                s.set_l2_keep(a.keep_mb * 1e6)
             out["plan"] = s.plan()
             if a.what == "spmv":
                 ms = s.time_spmv(a.reps, fp32=a.fp32)

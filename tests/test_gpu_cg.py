@@ -238,6 +238,25 @@ def test_l2_prefetch_changes_no_result(cgb, mode):
     assert np.array_equal(outs[0]["rnorm"], outs[1]["rnorm"])
 
 
+@pytest.mark.parametrize("cls", ["B", "C"])
+def test_l2_keep_changes_no_result(cgb, cls):
+    """Keeping part of the matrix stream in L2 (evict_last loads) changes
+    cache priorities only: zeta and rnorm traces are bit-identical with and
+    without it, in the FP64 and the mixed mode."""
+    n, nonzer, niter, shift = PARAMS[cls]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    with cgb.Session(rs, ci, a, spmv_kernel=2) as s:
+        outs = {}
+        for keep in (0.0, 96e6):
+            s.set_l2_keep(keep)
+            assert abs(s.plan()["l2_keep_mb"] - keep / 1e6) < 1e-9
+            outs[keep] = (s.power_iterate(4, shift),
+                          s.power_iterate(4, shift, mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=100))
+    for k in (0, 1):
+        assert np.array_equal(outs[0.0][k]["zeta"], outs[96e6][k]["zeta"])
+        assert np.array_equal(outs[0.0][k]["rnorm"], outs[96e6][k]["rnorm"])
+
+
 def test_sliced_refused_for_small_or_unsorted(cgb):
     n, nonzer, niter, shift = PARAMS["W"]
     rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
