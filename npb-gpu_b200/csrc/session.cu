@@ -138,7 +138,8 @@ int check_device(int device, cudaDeviceProp *prop)
     return CGB_OK;
 }
 
-int validate_csr(int n, const int *rowstr, const int *colidx, const double *a)
+// Pointers and row pointers (rowstr[0] = 0, never decreasing).
+int validate_rowstr(int n, const int *rowstr, const int *colidx, const double *a)
 {
     if (n < 1 || !rowstr || !colidx || !a)
         return set_error(CGB_ERR_INVALID, "CSR: n must be >= 1 and arrays non-null");
@@ -146,6 +147,12 @@ int validate_csr(int n, const int *rowstr, const int *colidx, const double *a)
     for (int j = 0; j < n; j++)
         if (rowstr[j + 1] < rowstr[j])
             return set_error(CGB_ERR_BAD_MATRIX, "CSR: rowstr decreases at row %d", j);
+    return CGB_OK;
+}
+
+// Entries: columns in [0, n), finite values.
+int validate_entries(int n, const int *rowstr, const int *colidx, const double *a)
+{
     const long long nnz = rowstr[n];
     // entries checked in parallel chunks; the first bad entry (lowest index)
     // is reported, as a serial scan would
@@ -184,6 +191,12 @@ int validate_csr(int n, const int *rowstr, const int *colidx, const double *a)
     return CGB_OK;
 }
 
+int validate_csr(int n, const int *rowstr, const int *colidx, const double *a)
+{
+    const int st = validate_rowstr(n, rowstr, colidx, a);
+    return st ? st : validate_entries(n, rowstr, colidx, a);
+}
+
 // Row split with balanced (stored entries + a per-row allowance for the
 // vector updates) per CTA.
 void make_split(int n, const int *rowstr, int grid, std::vector<int> &split)
@@ -220,6 +233,11 @@ struct cgb_session {
     int *d_rowstr = nullptr;
     int *d_colidx = nullptr;
     double *d_a = nullptr;
+    // staging copy of a re-uploaded CSR: the host validates the entries while
+    // it crosses to the device, and only a valid matrix replaces the session's
+    int *d_rowstr_in = nullptr, *d_colidx_in = nullptr;
+    double *d_a_in = nullptr;
+    size_t cap_rowstr_in = 0, cap_colidx_in = 0, cap_a_in = 0;
     float *d_a32 = nullptr;
     // vectors: x, z, p, q, r (vstride doubles each) and p32
     double *d_vec = nullptr;
@@ -351,6 +369,9 @@ void release(cgb_session *s)
     dev_free(s->d_colidx);
     dev_free(s->d_a);
     dev_free(s->d_a32);
+    dev_free(s->d_rowstr_in);
+    dev_free(s->d_colidx_in);
+    dev_free(s->d_a_in);
     dev_free(s->d_vec);
     dev_free(s->d_p32);
     dev_free(s->d_r32);
@@ -874,7 +895,10 @@ int choose_plan(cgb_session *s)
     return apply_plan(s, cands[bi]);
 }
 
-int upload_matrix(cgb_session *s, const int *rowstr, const int *colidx, const double *a)
+// from_staging: the CSR is already on the device in the staging buffers
+// (cgb_upload); otherwise it is copied from the host arrays.
+int upload_matrix(cgb_session *s, const int *rowstr, const int *colidx, const double *a,
+                  bool from_staging = false)
 {
     const long long nnz = rowstr[s->n];
     if (nnz > s->nnz_cap) {
@@ -888,11 +912,13 @@ int upload_matrix(cgb_session *s, const int *rowstr, const int *colidx, const do
         s->nnz_cap = nnz;
     }
     s->nnz = nnz;
-    CUDA_TRY(cudaMemcpyAsync(s->d_rowstr, rowstr, sizeof(int) * (s->n + 1), cudaMemcpyHostToDevice,
+    const cudaMemcpyKind kind = from_staging ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    CUDA_TRY(cudaMemcpyAsync(s->d_rowstr, from_staging ? s->d_rowstr_in : rowstr,
+                             sizeof(int) * (s->n + 1), kind, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->d_colidx, from_staging ? s->d_colidx_in : colidx, sizeof(int) * nnz,
+                             kind, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->d_a, from_staging ? s->d_a_in : a, sizeof(double) * nnz, kind,
                              s->stream));
-    CUDA_TRY(cudaMemcpyAsync(s->d_colidx, colidx, sizeof(int) * nnz, cudaMemcpyHostToDevice,
-                             s->stream));
-    CUDA_TRY(cudaMemcpyAsync(s->d_a, a, sizeof(double) * nnz, cudaMemcpyHostToDevice, s->stream));
     CUDA_TRY(cudaMemsetAsync(s->d_colidx + nnz, 0, sizeof(int) * kPad, s->stream));
     CUDA_TRY(cudaMemsetAsync(s->d_a + nnz, 0, sizeof(double) * kPad, s->stream));
     if (s->d_a32) {
@@ -1207,10 +1233,26 @@ int cgb_create(int n, const int *rowstr, const int *colidx, const double *a,
 int cgb_upload(cgb_session *s, const int *rowstr, const int *colidx, const double *a)
 {
     if (!s) return set_error(CGB_ERR_INVALID, "session is null");
-    int st = validate_csr(s->n, rowstr, colidx, a);
+    int st = validate_rowstr(s->n, rowstr, colidx, a);
     if (st) return st;
     CUDA_TRY(cudaSetDevice(s->device));
-    return upload_matrix(s, rowstr, colidx, a);
+    // the copy to the staging buffers runs while the host checks the
+    // entries; the session's matrix changes only when they are valid
+    const size_t n1 = size_t(s->n) + 1, nnz = size_t(rowstr[s->n]);
+    if (dev_reserve(&s->d_rowstr_in, &s->cap_rowstr_in, n1) != cudaSuccess ||
+        dev_reserve(&s->d_colidx_in, &s->cap_colidx_in, nnz) != cudaSuccess ||
+        dev_reserve(&s->d_a_in, &s->cap_a_in, nnz) != cudaSuccess)
+        return set_error(CGB_ERR_NOMEM, "staging allocation of %zu entries failed", nnz);
+    CUDA_TRY(cudaMemcpyAsync(s->d_rowstr_in, rowstr, sizeof(int) * n1, cudaMemcpyHostToDevice,
+                             s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->d_colidx_in, colidx, sizeof(int) * nnz, cudaMemcpyHostToDevice,
+                             s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->d_a_in, a, sizeof(double) * nnz, cudaMemcpyHostToDevice, s->stream));
+    st = validate_entries(s->n, rowstr, colidx, a);
+    // the copies read the caller's arrays: done before returning either way
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (st) return st;
+    return upload_matrix(s, rowstr, colidx, a, true);
 }
 
 int cgb_destroy(cgb_session *s)

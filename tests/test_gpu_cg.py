@@ -302,6 +302,36 @@ def test_reupload_same_structure_keeps_plan(cgb, oracle):
     assert np.linalg.norm(z[:n] - zo[:n]) <= 1e-12 * np.linalg.norm(zo[:n])
 
 
+def test_rejected_upload_keeps_the_matrix(cgb):
+    """A re-upload is checked while it crosses to the device: a bad entry is
+    reported (first bad index, as at create) and the session keeps solving
+    with its previous matrix, bit-identically; a good upload then replaces
+    it (reusing the captured graph)."""
+    n, nonzer, niter, shift = PARAMS["B"]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    with cgb.Session(rs, ci, a) as s:
+        ref = s.power_iterate(3, shift)
+        bad_c = ci.copy()
+        bad_c[len(ci) // 2] = n + 5
+        with pytest.raises(cgb.CgbError) as e:
+            s.upload(rs, bad_c, a)
+        assert e.value.status == cgb.ERR_BAD_MATRIX
+        assert f"colidx[{len(ci) // 2}]" in str(e.value)
+        bad_a = a.copy()
+        bad_a[7] = np.nan
+        with pytest.raises(cgb.CgbError) as e:
+            s.upload(rs, ci, bad_a)
+        assert e.value.status == cgb.ERR_NUMERIC
+        again = s.power_iterate(3, shift)
+        assert np.array_equal(again["zeta"], ref["zeta"])
+        s.upload(rs, ci, a * 2.0)
+        doubled = s.power_iterate(3, shift)
+    # the same sliced plan on a fresh session of 2A gives the same bits
+    with cgb.Session(rs, ci, a * 2.0, spmv_kernel=2) as s2:
+        fresh = s2.power_iterate(3, shift)
+    assert np.array_equal(doubled["zeta"], fresh["zeta"])
+
+
 @pytest.mark.parametrize("kind", [1, 2])
 def test_mixed_precision_class_c(cgb, golden, kind):
     """FP32 SpMV inside FP64 refinement reaches the FP64 reference zeta.
