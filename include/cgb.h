@@ -62,12 +62,15 @@ long long cgb_nz_bound(int n, int nonzer);
 int cgb_makea(int n, int nonzer, double rcond, double shift, double seed, int *rowstr,
               int *colidx, double *a, long long nz_capacity, long long *nnz_out);
 
-/* cgb_makea with the assembly -- the n*(nonzer+1)^2 outer-product
- * contributions, their per-row sort and in-order duplicate sums
- * (sparse(), cg.cu:1611-1785) -- on CUDA device `device`; the vectors
- * (sprnvc/vecset, one sequential LCG stream) are drawn on the host.  Same
- * arguments, outputs and bit-identical result as cgb_makea; nonzer <= 31.
- * CGB_ERR_CAPACITY also when one row has more than 2048 contributions. */
+/* cgb_makea on CUDA device `device`: the vectors (sprnvc/vecset, one LCG
+ * stream with rejection sampling, cg.cu:1798-1857) drawn in parallel -- every
+ * possible start parsed at once, the chain from the first draw followed by
+ * jump pointers -- and the assembly (the n*(nonzer+1)^2 outer-product
+ * contributions, their per-row sort and in-order duplicate sums, sparse(),
+ * cg.cu:1611-1785) on the device; only the running product of the
+ * geometric weights stays on the host.  Same arguments, outputs and
+ * bit-identical result as cgb_makea; nonzer <= 31.  CGB_ERR_CAPACITY also
+ * when one row has more than 2048 contributions. */
 int cgb_makea_device(int device, int n, int nonzer, double rcond, double shift, double seed,
                      int *rowstr, int *colidx, double *a, long long nz_capacity,
                      long long *nnz_out);
@@ -97,6 +100,13 @@ void cgb_default_options(cgb_options *opts);
  * validated first.  `opts` may be NULL for the defaults. */
 int cgb_create(int n, const int *rowstr, const int *colidx, const double *a,
                const cgb_options *opts, cgb_session **out);
+
+/* A session on the generator's matrix (cgb_makea_device's arguments; the
+ * device is opts->device) without the CSR ever leaving the device: the
+ * generated arrays become the session's copy.  Same matrix, bit for bit, as
+ * cgb_create on cgb_makea's output.  No counterpart in the reference. */
+int cgb_create_generated(int n, int nonzer, double rcond, double shift, double seed,
+                         const cgb_options *opts, cgb_session **out);
 
 /* Replaces the session's matrix values/structure with another CSR of the
  * same order n from host memory (an H2D copy; same validation). */

@@ -1,12 +1,13 @@
 // cg_main.cpp -- `cg`, a drop-in for the reference benchmark binary cg.<CLASS>
 // (GMAP/NPB-GPU CUDA/CG/cg.cu main(), :337-645) on top of libcgb's C ABI.
 //
-//   cg S|W|A|B|C            an NPB class (setparams.cpp:751-785 parameters)
+//   cg S|W|A|B|C|D          an NPB class (setparams.cpp:751-785 parameters)
 //   cg U --n N --nonzer K --niter I --shift S [--seed X]   custom sizes
 //   options: --mode fp64|tol|mixed|learned  --tol T  --cgitmax M
 //            --weights FILE (learned mode: network weights, raw FP32; default
 //            the trained weights shipped beside the package, npbcg/lp_weights.f32)
 //            --device D  --json (one JSON result line instead of the report)
+//            --gpu-makea (generate the matrix with cgb_makea_device)
 //
 // Like the reference it generates the matrix (makea), runs the timed inverse
 // power iteration, prints the per-iteration "||r||  zeta" lines in the
@@ -55,7 +56,7 @@ void usage()
     std::fprintf(stderr,
                  "usage: cg S|W|A|B|C|D | cg U --n N --nonzer K --niter I --shift S [--seed X]\n"
                  "          [--mode fp64|tol|mixed|learned] [--tol T] [--cgitmax M]\n"
-                 "          [--weights FILE] [--device D] [--json]\n");
+                 "          [--weights FILE] [--device D] [--json] [--gpu-makea]\n");
 }
 
 // The weights shipped with the package: <dir of this binary>/../npbcg/lp_weights.f32.
@@ -123,7 +124,7 @@ int main(int argc, char **argv)
     }
     double seed = 314159265.0, tol = 1e-12;
     std::string weights;
-    int mode = CGB_MODE_FP64, cgitmax = 25, device = 0, json = 0;
+    int mode = CGB_MODE_FP64, cgitmax = 25, device = 0, json = 0, gpu_makea = 0;
     for (int i = 2; i < argc; i++) {
         const std::string a = argv[i];
         auto next = [&](void) -> const char * {
@@ -142,6 +143,7 @@ int main(int argc, char **argv)
         else if (a == "--cgitmax") cgitmax = std::atoi(next());
         else if (a == "--device") device = std::atoi(next());
         else if (a == "--json") json = 1;
+        else if (a == "--gpu-makea") gpu_makea = 1;
         else if (a == "--weights") weights = next();
         else if (a == "--mode") {
             const std::string m = next();
@@ -169,8 +171,10 @@ int main(int argc, char **argv)
     std::vector<int> rowstr(P.n + 1), colidx(cap);
     std::vector<double> a(cap);
     long long nnz = 0;
-    int st = cgb_makea(P.n, P.nonzer, 0.1, P.shift, seed, rowstr.data(), colidx.data(), a.data(),
-                       cap, &nnz);
+    int st = gpu_makea ? cgb_makea_device(device, P.n, P.nonzer, 0.1, P.shift, seed, rowstr.data(),
+                                          colidx.data(), a.data(), cap, &nnz)
+                       : cgb_makea(P.n, P.nonzer, 0.1, P.shift, seed, rowstr.data(), colidx.data(),
+                                   a.data(), cap, &nnz);
     if (st) return fail(st, "makea");
 
     cgb_options opt;

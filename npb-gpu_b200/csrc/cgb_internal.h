@@ -31,4 +31,17 @@ struct GenVectors {
 };
 int draw_generator_vectors(int n, int nonzer, double rcond, double seed, GenVectors &v);
 
+// The generator's CSR left on the device (makea_gpu.cu): rowstr / colidx / a
+// are device allocations the caller takes over (cudaFree), the row pointers
+// are also on the host.
+struct DeviceCsr {
+    int *rowstr = nullptr;
+    int *colidx = nullptr;
+    double *a = nullptr;
+    long long nnz = 0;
+    std::vector<int> h_rowstr;
+};
+int makea_on_device(int device, int n, int nonzer, double rcond, double shift, double seed,
+                    DeviceCsr *out);
+
 }  // namespace cgb

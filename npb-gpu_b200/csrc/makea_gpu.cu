@@ -2,8 +2,12 @@
 // the reference's makea() + sparse() (GMAP/NPB-GPU CUDA/CG/cg.cu:1303-1368,
 // :1611-1785) and to the host generator in makea.cpp.
 //
-// The n sparse vectors (one LCG stream with rejection sampling, inherently
-// sequential and cheap) are drawn on the host; the assembly -- n * (nonzer+1)^2
+// The n sparse vectors (one LCG stream with rejection sampling) are drawn
+// on the device in parallel (pair_ends ... draw_vectors below: a vector's
+// length in draws depends only on where it starts, so every start is parsed
+// at once and the chain from the first draw follows by jump pointers); the
+// geometric weights, a running product rounded at every step, are the one
+// O(n) loop left on the host.  The assembly -- n * (nonzer+1)^2
 // outer-product contributions, 38 M at class C -- runs on the device:
 //   1. per row, the vectors that touch it (an incidence transpose with
 //      atomic slots, then each row's short list sorted by vector index);
@@ -33,6 +37,151 @@ namespace gen {
 constexpr int kFoldThreads = 256;
 constexpr int kMaxRowContrib = 2048;  // contributions of one row held in shared memory
 constexpr int kGroupsPerThread = kMaxRowContrib / kFoldThreads;
+
+// ---------------------------------------------------------------- vectors
+// The n sparse vectors (sprnvc + vecset, cg.cu:1798-1857) from one LCG
+// stream.  Draw k of the stream is x_k * 2^-46, x_k = seed * 5^13^k mod 2^46
+// (c_randdp.cpp:84-114 in integer form); main() throws draw 1 away
+// (cg.cu:406-408), so the vectors consume pairs (value, where) = draws
+// (2 + 2m, 3 + 2m), m = 0, 1, ...  A candidate position is
+// int(pow2 * where) + 1 = (x >> (46 - log2 pow2)) + 1 (pow2 a power of two,
+// so the product is exact); it is rejected when > n or already drawn for
+// this vector.  How many pairs a vector consumes depends only on the pair
+// it starts at, which makes the draw parallel:
+//   1. pair_ends:   for every pair m < D, the pair after a vector starting at
+//                   m (D when it would run past the buffer);
+//   2. jump_double: ten rounds of J(m) <- J(J(m)): 1024 vectors ahead;
+//   3. chain_heads: one thread walks the 1024-vector jumps from pair 0, then
+//      chain_starts: a thread per 1024 vectors walks the single steps -> the
+//                   first pair of every vector;
+//   4. draw_vectors: vector i parsed again from its first pair, vecset's 0.5
+//                   at position i added -- the host draw's layout.
+constexpr uint64_t kMask46 = (uint64_t(1) << 46) - 1;
+constexpr uint64_t kMult = 1220703125ull;  // 5^13 (cg.cu:407)
+constexpr int kJumpRounds = 10;            // 2^10 vectors a jump
+constexpr int kMaxWidth = 32;              // nonzer + 1 <= 32
+
+__device__ __forceinline__ uint64_t lcg_at(uint64_t seed, uint64_t k)
+{
+    uint64_t r = seed & kMask46, b = kMult;
+    while (k) {
+        if (k & 1) r = (r * b) & kMask46;  // low 46 bits of the 64-bit product
+        b = (b * b) & kMask46;
+        k >>= 1;
+    }
+    return r;
+}
+
+// One vector from pair m: accepted 1-based positions into p1 (and values
+// into vv when kValues); returns the pair after its last pair, or D if the
+// vector would run past pair D.
+template <bool kValues>
+__device__ __forceinline__ long long parse_vector(uint64_t seed, long long m, long long D, int n,
+                                                  int nonzer, int shift_bits, int *p1, double *vv,
+                                                  int *have_out)
+{
+    uint64_t x = lcg_at(seed, uint64_t(2 + 2 * m));
+    int have = 0;
+    while (have < nonzer) {
+        if (m >= D) return D;
+        const uint64_t xv = x;               // value draw
+        x = (x * kMult) & kMask46;           // where draw
+        const int cand = int(x >> shift_bits) + 1;
+        x = (x * kMult) & kMask46;           // next pair's value draw
+        m++;
+        if (cand > n) continue;
+        bool seen = false;
+        for (int t = 0; t < have; t++) seen |= (p1[t] == cand);
+        if (seen) continue;
+        if (kValues) vv[have] = double(xv) * 0x1p-46;  // exact
+        p1[have] = cand;
+        have++;
+    }
+    *have_out = have;
+    return m;
+}
+
+__global__ void pair_ends(uint64_t seed, long long D, int n, int nonzer, int shift_bits, int *end)
+{
+    int p1[kMaxWidth];
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m <= D;
+         m += (long long)gridDim.x * blockDim.x) {
+        int have = 0;
+        end[m] = m == D ? int(D)
+                        : int(parse_vector<false>(seed, m, D, n, nonzer, shift_bits, p1, nullptr, &have));
+    }
+}
+
+__global__ void jump_double(long long D, const int *__restrict__ j_in, int *j_out)
+{
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m <= D;
+         m += (long long)gridDim.x * blockDim.x)
+        j_out[m] = j_in[j_in[m]];
+}
+
+// One thread: heads[k] = first pair of vector k * 1024.
+__global__ void chain_heads(const int *__restrict__ jump, long long D, int nheads, int *heads,
+                            int *overflow)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    int h = 0;
+    for (int k = 0; k < nheads; k++) {
+        if (h >= D) {
+            *overflow = 1;
+            return;
+        }
+        heads[k] = h;
+        h = jump[h];
+    }
+}
+
+// A thread per 1024 vectors: start[i] = first pair of vector i.
+__global__ void chain_starts(const int *__restrict__ end, const int *__restrict__ heads, long long D,
+                             int n, int *start, int *overflow)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i0 = k << kJumpRounds;
+    if (i0 >= n || *overflow) return;  // the heads are incomplete after an overflow
+    const int i1 = min(n, i0 + (1 << kJumpRounds));
+    int s = heads[k];
+    for (int i = i0; i < i1; i++) {
+        if (s < 0 || s >= D) {
+            *overflow = 1;
+            return;
+        }
+        start[i] = s;
+        s = end[s];
+    }
+    if (s >= D) *overflow = 1;  // the last vector ran past the buffer
+}
+
+__global__ void draw_vectors(uint64_t seed, long long D, int n, int nonzer, int shift_bits,
+                             const int *__restrict__ start, int width, int *count, int *pos,
+                             double *val)
+{
+    int p1[kMaxWidth];
+    double vv[kMaxWidth];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int have = 0;
+        (void)parse_vector<true>(seed, start[i], D, n, nonzer, shift_bits, p1, vv, &have);
+        bool set = false;
+        for (int t = 0; t < have; t++)
+            if (p1[t] == i + 1) {
+                vv[t] = 0.5;
+                set = true;
+            }
+        if (!set) {
+            vv[have] = 0.5;
+            p1[have] = i + 1;
+            have++;
+        }
+        count[i] = have;
+        for (int t = 0; t < have; t++) {
+            pos[size_t(i) * width + t] = p1[t] - 1;
+            val[size_t(i) * width + t] = vv[t];
+        }
+    }
+}
 
 // 1a. per row: vectors touching it, and its contribution count
 __global__ void row_counts(const int *__restrict__ count, const int *__restrict__ pos, int n,
@@ -256,6 +405,74 @@ struct DeviceBuffers {
 using namespace cgb;
 using namespace cgb::gen;
 
+#define GEN_TRY_IN(call)                                                                  \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            for (void *p_ : {(void *)end, (void *)jump, (void *)heads, (void *)start,      \
+                             (void *)flag})                                               \
+                if (p_) cudaFree(p_);                                                     \
+            return set_error(e_ == cudaErrorMemoryAllocation ? CGB_ERR_NOMEM : CGB_ERR_CUDA, \
+                             "makea_device: %s: %s", #call, cudaGetErrorString(e_));       \
+        }                                                                                 \
+    } while (0)
+
+namespace {
+
+// The generator's vectors into d->count / pos / val (see the kernels above).
+// The pair buffer starts at 1.3x the expected pairs and doubles while the
+// chain runs past it.
+int draw_on_device(double seed, int n, int nonzer, int sms, DeviceBuffers *d)
+{
+    int pow2 = 1, log2p = 0;
+    do {
+        pow2 *= 2;
+        log2p++;
+    } while (pow2 < n);
+    const int shift_bits = 46 - log2p;
+    const uint64_t useed = uint64_t(seed);
+    const int nheads = (n + (1 << kJumpRounds) - 1) >> kJumpRounds;
+    long long D = (long long)n * (long long)std::ceil(1.3 * nonzer * double(pow2) / n + 2.0) + 1024;
+    for (int attempt = 0; attempt < 6; attempt++, D *= 2) {
+        if (D + 1 > 0x7fffffffLL)
+            return set_error(CGB_ERR_CAPACITY, "makea_device: %lld draw pairs overflow int32", D);
+        int *end = nullptr, *jump = nullptr, *heads = nullptr, *start = nullptr, *flag = nullptr;
+        GEN_TRY_IN(galloc(&end, size_t(D) + 1));
+        GEN_TRY_IN(galloc(&jump, 2 * (size_t(D) + 1)));
+        GEN_TRY_IN(galloc(&heads, size_t(nheads)));
+        GEN_TRY_IN(galloc(&start, size_t(n)));
+        GEN_TRY_IN(galloc(&flag, 1));
+        GEN_TRY_IN(cudaMemset(flag, 0, sizeof(int)));
+        GEN_TRY_IN(cudaMemset(heads, 0xff, sizeof(int) * size_t(nheads)));  // -1: not reached
+        const int grid = 16 * sms;
+        pair_ends<<<grid, 256>>>(useed, D, n, nonzer, shift_bits, end);
+        const int *j_in = end;
+        int *j_out = jump;
+        for (int r = 0; r < kJumpRounds; r++) {
+            jump_double<<<grid, 256>>>(D, j_in, j_out);
+            j_in = j_out;
+            j_out = (j_out == jump) ? jump + (size_t(D) + 1) : jump;
+        }
+        chain_heads<<<1, 32>>>(j_in, D, nheads, heads, flag);
+        chain_starts<<<(nheads + 127) / 128, 128>>>(end, heads, D, n, start, flag);
+        GEN_TRY_IN(cudaGetLastError());
+        int overflow = 0;
+        GEN_TRY_IN(cudaMemcpy(&overflow, flag, sizeof(int), cudaMemcpyDeviceToHost));
+        if (!overflow) {
+            draw_vectors<<<grid, 256>>>(useed, D, n, nonzer, shift_bits, start, nonzer + 1, d->count,
+                                        d->pos, d->val);
+            GEN_TRY_IN(cudaGetLastError());
+            GEN_TRY_IN(cudaDeviceSynchronize());
+        }
+        for (void *p : {(void *)end, (void *)jump, (void *)heads, (void *)start, (void *)flag})
+            cudaFree(p);
+        if (!overflow) return CGB_OK;
+    }
+    return set_error(CGB_ERR_CAPACITY, "makea_device: the draw did not fit %lld pairs", D);
+}
+
+}  // namespace
+
 #define GEN_TRY(call)                                                                     \
     do {                                                                                  \
         cudaError_t e_ = (call);                                                          \
@@ -264,25 +481,24 @@ using namespace cgb::gen;
                              "makea_device: %s: %s", #call, cudaGetErrorString(e_));       \
     } while (0)
 
-extern "C" int cgb_makea_device(int device, int n, int nonzer, double rcond, double shift,
-                                double seed, int *rowstr, int *colidx, double *a,
-                                long long nz_capacity, long long *nnz_out)
+int cgb::makea_on_device(int device, int n, int nonzer, double rcond, double shift, double seed,
+                         DeviceCsr *out)
 {
-    if (!rowstr || !nnz_out) return set_error(CGB_ERR_INVALID, "makea_device: null outputs");
     if (!(rcond > 0.0) || !std::isfinite(shift))
         return set_error(CGB_ERR_INVALID, "makea_device: rcond must be > 0 and shift finite");
     if (nonzer + 1 > 32) return set_error(CGB_ERR_INVALID, "makea_device: nonzer must be <= 31");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
         return set_error(CGB_ERR_NO_DEVICE, "makea_device: no CUDA device %d", device);
-    GenVectors v;
-    int st = draw_generator_vectors(n, nonzer, rcond, seed, v);
-    if (st) return st;
+    if (n < 2 || nonzer < 1 || nonzer >= n)
+        return set_error(CGB_ERR_INVALID, "makea_device: need n >= 2, 1 <= nonzer < n");
+    if (!valid_seed(seed))
+        return set_error(CGB_ERR_INVALID, "makea_device: seed must be an odd integer in (1, 2^46)");
     GEN_TRY(cudaSetDevice(device));
     cudaDeviceProp prop;
     GEN_TRY(cudaGetDeviceProperties(&prop, device));
     if (prop.major != 10) return set_error(CGB_ERR_NO_DEVICE, "makea_device: device %d is not sm_100", device);
-    const int w = v.width, sms = prop.multiProcessorCount;
+    const int w = nonzer + 1, sms = prop.multiProcessorCount;
     DeviceBuffers d;
     GEN_TRY(galloc(&d.count, n));
     GEN_TRY(galloc(&d.pos, size_t(n) * w));
@@ -290,10 +506,20 @@ extern "C" int cgb_makea_device(int device, int n, int nonzer, double rcond, dou
     GEN_TRY(galloc(&d.scale, n));
     GEN_TRY(galloc(&d.nvec, n));
     GEN_TRY(galloc(&d.ncontrib, n));
-    GEN_TRY(cudaMemcpy(d.count, v.count.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    GEN_TRY(cudaMemcpy(d.pos, v.pos.data(), sizeof(int) * size_t(n) * w, cudaMemcpyHostToDevice));
-    GEN_TRY(cudaMemcpy(d.val, v.val.data(), sizeof(double) * size_t(n) * w, cudaMemcpyHostToDevice));
-    GEN_TRY(cudaMemcpy(d.scale, v.scale.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    {
+        // the geometric weights: a running product, rounded at every step
+        // as the reference's loop does (cg.cu:1695, :1755) -- host, O(n)
+        std::vector<double> scale(n);
+        const double ratio = std::pow(rcond, 1.0 / double(n));
+        double size = 1.0;
+        for (int i = 0; i < n; i++) {
+            scale[i] = size;
+            size = size * ratio;
+        }
+        GEN_TRY(cudaMemcpy(d.scale, scale.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    }
+    int st = draw_on_device(seed, n, nonzer, sms, &d);
+    if (st) return st;
     GEN_TRY(cudaMemset(d.nvec, 0, sizeof(int) * n));
     GEN_TRY(cudaMemset(d.ncontrib, 0, sizeof(unsigned long long) * n));
     const int grid = 8 * sms;
@@ -335,21 +561,48 @@ extern "C" int cgb_makea_device(int device, int n, int nonzer, double rcond, dou
     GEN_TRY(cudaMemcpy(ucount.data(), d.ucount, sizeof(int) * n, cudaMemcpyDeviceToHost));
     long long nnz = 0;
     for (int j = 0; j < n; j++) nnz += ucount[j];
-    *nnz_out = nnz;
-    if (nnz > nz_capacity)
-        return set_error(CGB_ERR_CAPACITY, "makea_device: nz_capacity %lld < nnz %lld", nz_capacity, nnz);
+    out->nnz = nnz;
     if (nnz > 0x7fffffffLL)
         return set_error(CGB_ERR_CAPACITY, "makea_device: nnz %lld overflows int32 rowstr", nnz);
-    if (!colidx || !a) return set_error(CGB_ERR_INVALID, "makea_device: null colidx/a");
-    rowstr[0] = 0;
+    std::vector<int> &rowstr = out->h_rowstr;
+    rowstr.assign(size_t(n) + 1, 0);
     for (int j = 0; j < n; j++) rowstr[j + 1] = rowstr[j] + ucount[j];
     GEN_TRY(galloc(&d.rowstr, size_t(n) + 1));
     GEN_TRY(galloc(&d.colidx, size_t(nnz)));
     GEN_TRY(galloc(&d.a, size_t(nnz)));
-    GEN_TRY(cudaMemcpy(d.rowstr, rowstr, sizeof(int) * (size_t(n) + 1), cudaMemcpyHostToDevice));
+    GEN_TRY(cudaMemcpy(d.rowstr, rowstr.data(), sizeof(int) * (size_t(n) + 1), cudaMemcpyHostToDevice));
     compact<<<grid, 256>>>(d.coff, d.rowstr, n, d.ccol, d.cval, d.colidx, d.a);
     GEN_TRY(cudaGetLastError());
-    GEN_TRY(cudaMemcpy(colidx, d.colidx, sizeof(int) * size_t(nnz), cudaMemcpyDeviceToHost));
-    GEN_TRY(cudaMemcpy(a, d.a, sizeof(double) * size_t(nnz), cudaMemcpyDeviceToHost));
+    GEN_TRY(cudaDeviceSynchronize());
+    // hand the CSR over (the buffers' destructor skips what it no longer owns)
+    out->rowstr = d.rowstr;
+    out->colidx = d.colidx;
+    out->a = d.a;
+    d.rowstr = d.colidx = nullptr;
+    d.a = nullptr;
     return CGB_OK;
+}
+
+extern "C" int cgb_makea_device(int device, int n, int nonzer, double rcond, double shift,
+                                double seed, int *rowstr, int *colidx, double *a,
+                                long long nz_capacity, long long *nnz_out)
+{
+    if (!rowstr || !nnz_out) return set_error(CGB_ERR_INVALID, "makea_device: null outputs");
+    DeviceCsr csr;
+    int st = makea_on_device(device, n, nonzer, rcond, shift, seed, &csr);
+    *nnz_out = csr.nnz;
+    if (st == CGB_OK && csr.nnz > nz_capacity)
+        st = set_error(CGB_ERR_CAPACITY, "makea_device: nz_capacity %lld < nnz %lld", nz_capacity,
+                       csr.nnz);
+    if (st == CGB_OK && (!colidx || !a)) st = set_error(CGB_ERR_INVALID, "makea_device: null colidx/a");
+    if (st == CGB_OK) {
+        std::memcpy(rowstr, csr.h_rowstr.data(), sizeof(int) * (size_t(n) + 1));
+        if (cudaMemcpy(colidx, csr.colidx, sizeof(int) * size_t(csr.nnz), cudaMemcpyDeviceToHost) !=
+                cudaSuccess ||
+            cudaMemcpy(a, csr.a, sizeof(double) * size_t(csr.nnz), cudaMemcpyDeviceToHost) != cudaSuccess)
+            st = set_error(CGB_ERR_CUDA, "makea_device: copy-out failed");
+    }
+    for (void *p : {(void *)csr.rowstr, (void *)csr.colidx, (void *)csr.a})
+        if (p) cudaFree(p);
+    return st;
 }

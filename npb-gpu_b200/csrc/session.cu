@@ -1156,13 +1156,14 @@ int cgb_device_info(int device, int *sm_count, int *cc_major, int *cc_minor,
     return CGB_OK;
 }
 
-int cgb_create(int n, const int *rowstr, const int *colidx, const double *a,
-               const cgb_options *opts, cgb_session **out)
+}  // extern "C"
+
+namespace {
+
+// A session without its matrix: options checked, device buffers allocated.
+int create_shell(int n, const cgb_options *opts, cgb_session **out)
 {
-    if (!out) return set_error(CGB_ERR_INVALID, "out is null");
-    *out = nullptr;
-    int st = validate_csr(n, rowstr, colidx, a);
-    if (st) return st;
+    int st = CGB_OK;
     cgb_options o;
     cgb_default_options(&o);
     if (opts) o = *opts;
@@ -1221,7 +1222,69 @@ int cgb_create(int n, const int *rowstr, const int *colidx, const double *a,
     CREATE_TRY(dev_alloc(&s->d_dot, 1));
 #undef CREATE_TRY
     st = ensure_trace(s, 128);
-    if (st == CGB_OK) st = upload_matrix(s, rowstr, colidx, a);
+    if (st != CGB_OK) {
+        release(s);
+        return st;
+    }
+    *out = s;
+    return CGB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cgb_create(int n, const int *rowstr, const int *colidx, const double *a,
+               const cgb_options *opts, cgb_session **out)
+{
+    if (!out) return set_error(CGB_ERR_INVALID, "out is null");
+    *out = nullptr;
+    int st = validate_csr(n, rowstr, colidx, a);
+    if (st) return st;
+    cgb_session *s = nullptr;
+    st = create_shell(n, opts, &s);
+    if (st) return st;
+    st = upload_matrix(s, rowstr, colidx, a);
+    if (st != CGB_OK) {
+        release(s);
+        return st;
+    }
+    *out = s;
+    return CGB_OK;
+}
+
+int cgb_create_generated(int n, int nonzer, double rcond, double shift, double seed,
+                         const cgb_options *opts, cgb_session **out)
+{
+    if (!out) return set_error(CGB_ERR_INVALID, "out is null");
+    *out = nullptr;
+    cgb_session *s = nullptr;
+    int st = create_shell(n, opts, &s);
+    if (st) return st;
+    DeviceCsr csr;
+    st = makea_on_device(s->device, n, nonzer, rcond, shift, seed, &csr);
+    if (st == CGB_OK) {
+        // the generated arrays become the staging copy the upload reads
+        dev_free(s->d_rowstr_in);
+        dev_free(s->d_colidx_in);
+        dev_free(s->d_a_in);
+        s->d_rowstr_in = csr.rowstr;
+        s->d_colidx_in = csr.colidx;
+        s->d_a_in = csr.a;
+        s->cap_rowstr_in = size_t(n) + 1;
+        s->cap_colidx_in = s->cap_a_in = size_t(csr.nnz);
+        csr.rowstr = csr.colidx = nullptr;
+        csr.a = nullptr;
+        st = cudaSetDevice(s->device) == cudaSuccess
+                 ? upload_matrix(s, csr.h_rowstr.data(), nullptr, nullptr, true)
+                 : set_error(CGB_ERR_CUDA, "cudaSetDevice failed");
+        // no host arrays behind this matrix: any host CSR passed later uploads
+        s->h_rowstr = nullptr;
+        s->h_colidx = nullptr;
+        s->h_a = nullptr;
+    }
+    for (void *p : {(void *)csr.rowstr, (void *)csr.colidx, (void *)csr.a})
+        if (p) cudaFree(p);
     if (st != CGB_OK) {
         release(s);
         return st;

@@ -102,6 +102,9 @@ _SIGNATURES = {
     "cgb_makea_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                         ctypes.c_double, ctypes.c_double, _I32, _I32, _F64,
                                         ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]),
+    "cgb_create_generated": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                            ctypes.POINTER(ctypes.c_void_p)]),
     "cgb_default_options": (None, [ctypes.POINTER(Options)]),
     "cgb_create": (ctypes.c_int, [ctypes.c_int, _I32, _I32, _F64, ctypes.POINTER(Options),
                                   ctypes.POINTER(ctypes.c_void_p)]),
@@ -251,6 +254,20 @@ class Session:
         _check(lib().cgb_create(self.n, *self._keep, ctypes.byref(opts), ctypes.byref(h)))
         self._h = h
 
+    @classmethod
+    def generated(cls, n, nonzer, shift, seed=SEED, rcond=RCOND, **options):
+        """A session on the generator's matrix built on the device, never
+        copied to the host (the same matrix as Session(*makea(...)))."""
+        self = cls.__new__(cls)
+        self.n = int(n)
+        self._keep = None
+        opts = default_options(**options)
+        h = ctypes.c_void_p()
+        _check(lib().cgb_create_generated(int(n), int(nonzer), float(rcond), float(shift),
+                                          float(seed), ctypes.byref(opts), ctypes.byref(h)))
+        self._h = h
+        return self
+
     def close(self):
         if getattr(self, "_h", None):
             lib().cgb_destroy(self._h)
@@ -274,13 +291,22 @@ class Session:
                       np.ascontiguousarray(a, np.float64))
         _check(lib().cgb_upload(self._h, *self._keep))
 
-    def conj_grad(self, x):
-        """One reference conj_grad from z = 0; returns (z, p, q, r, rnorm), n+1 entries each."""
+    def conj_grad(self, x, matrix=None):
+        """One reference conj_grad from z = 0; returns (z, p, q, r, rnorm), n+1 entries each.
+        `matrix` (rowstr, colidx, a): the CSR to pass, as the reference's call does
+        (uploaded when it is not the session's); default the arrays the session
+        was created or last uploaded with."""
         n = self.n
         xv = np.ones(n + 1, np.float64)
         xv[: min(len(x), n + 1)] = np.asarray(x, np.float64)[: n + 1]
         z, p, q, r = (np.zeros(n + 1) for _ in range(4))
         rn = ctypes.c_double()
+        if matrix is not None:
+            self._keep = (np.ascontiguousarray(matrix[0], np.int32),
+                          np.ascontiguousarray(matrix[1], np.int32),
+                          np.ascontiguousarray(matrix[2], np.float64))
+        if self._keep is None:
+            raise ValueError("this session's matrix has no host arrays: pass matrix=")
         rowstr, colidx, a = self._keep
         _check(lib().cgb_conj_grad(self._h, colidx, rowstr, xv, z, a, p, q, r, ctypes.byref(rn)))
         return z, p, q, r, rn.value
