@@ -3,6 +3,7 @@
     python npb-gpu_b200/npbcg/profile_case.py --cls B --what spmv --reps 3
     python npb-gpu_b200/npbcg/profile_case.py --cls B --what solve --niter 2
     python npb-gpu_b200/npbcg/profile_case.py --cls B --what sweep
+    python npb-gpu_b200/npbcg/profile_case.py --what batch --nsys 64 --niter 2
 
 `spmv` launches the standalone FP64 SpMV+dot kernel `reps` times (after one
 warm-up launch); `solve` runs one power iteration of `niter` outer steps;
@@ -21,7 +22,12 @@ import npbcg  # noqa: E402
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cls", default="B", choices=sorted(npbcg.CLASSES))
-    ap.add_argument("--what", default="spmv", choices=["spmv", "solve", "sweep"])
+    ap.add_argument("--what", default="spmv", choices=["spmv", "solve", "sweep", "batch"])
+    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed", "learned"],
+                    help="solve / batch: the solver mode (mixed: tol 1e-12, cgitmax 100)")
+    ap.add_argument("--nsys", type=int, default=64, help="batch: systems of the batched workload")
+    ap.add_argument("--tune", action="store_true",
+                    help="batch: run the autotuner first (12 launches at niter 1)")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--niter", type=int, default=2)
     ap.add_argument("--lanes", type=int, default=0)
@@ -30,6 +36,20 @@ def main():
     ap.add_argument("--keep-mb", type=float, default=None,
                     help="bytes (MB) of the sliced stream kept in L2 (default: the autotuner's)")
     a = ap.parse_args()
+    kw = {} if a.mode == "fp64" else dict(
+        mode=npbcg.MODE_MIXED if a.mode == "mixed" else npbcg.MODE_MIXED_LEARNED, tol=1e-12,
+        cgitmax=100)
+    if a.what == "batch":
+        # the batched workload's first nsys systems, niter outer steps each
+        specs = npbcg.batch_config5(nsys=a.nsys)
+        systems = [npbcg.makea(n, nz, npbcg.RCOND, sh, seed) for n, nz, sh, seed in specs]
+        with npbcg.Batch(systems, [sh for _, _, sh, _ in specs]) as b:
+            if a.tune:
+                b.tune(niter=1, **kw)
+            r = b.solve(niter=a.niter, **kw)
+            print(json.dumps({"what": "batch", "nsys": a.nsys, "niter": a.niter, "mode": a.mode,
+                              "device_ms": r["device_ms"], "policy": b.policy()}), flush=True)
+        return
     c = npbcg.CLASSES[a.cls]
     rs, ci, av = npbcg.makea(c["n"], c["nonzer"], npbcg.RCOND, c["shift"])
     n, nnz = c["n"], len(av)
@@ -62,7 +82,12 @@ def main():
                 b = (npbcg.spmv_bytes_fp32 if a.fp32 else npbcg.spmv_bytes_fp64)(n, nnz)
                 out.update(ms=ms, gbs=b / ms / 1e6)
             else:
-                r = s.power_iterate(a.niter, c["shift"])
+                if a.mode == "learned":
+                    model = npbcg.Gnn()
+                    model.load()
+                    with model.graph(rs, ci, av) as g:
+                        model.attach(g, s)
+                r = s.power_iterate(a.niter, c["shift"], **kw)
                 out.update(device_ms=r["device_ms"], zeta=float(r["zeta"][-1]))
     print(json.dumps(out), flush=True)
 
