@@ -532,7 +532,7 @@ def jacobi_factor(rowstr, colidx, a):
 
 
 # ------------------------------------------------------------------------ batches
-def batch_config5(nsys=512, seed=20241203, n_range=(1400, 20000), nonzer_range=(7, 13)):
+def uneven_batch_specs(nsys=512, seed=20241203, n_range=(1400, 20000), nonzer_range=(7, 13)):
     """The batched workload: per system n log-uniform in n_range, nonzer
     uniform in nonzer_range, shift = 10 + n/1000, rcond 0.1, its own odd LCG
     seed; all drawn from a fixed host PRNG.  Returns [(n, nonzer, shift, seed)]."""

@@ -41,7 +41,7 @@ def main():
         cgitmax=100)
     if a.what == "batch":
         # the batched workload's first nsys systems, niter outer steps each
-        specs = npbcg.batch_config5(nsys=a.nsys)
+        specs = npbcg.uneven_batch_specs(nsys=a.nsys)
         systems = [npbcg.makea(n, nz, npbcg.RCOND, sh, seed) for n, nz, sh, seed in specs]
         with npbcg.Batch(systems, [sh for _, _, sh, _ in specs]) as b:
             if a.tune:

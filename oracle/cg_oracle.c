@@ -1,7 +1,7 @@
 /*
  * cg_oracle.c -- CPU oracle for the NPB CG inverse-power-iteration path.
  *
- * TEST INFRASTRUCTURE ONLY.  This file is the checker, never the product:
+ * TEST INFRASTRUCTURE ONLY.  This file is the oracle of the tests, never the product:
  * only tests/, __graft_entry__.smoke() and the cpu_baseline / reference legs
  * of bench.py may load liboracle.so.  The shipped library (libcgb.so) neither
  * links nor calls anything here, and fails loudly when its CUDA code is

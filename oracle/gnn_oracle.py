@@ -1,6 +1,6 @@
 """CPU oracle of the learned preconditioner network -- TEST INFRASTRUCTURE ONLY.
 
-Only tests/ may import this module, as the checker of the CUDA forward,
+Only tests/ may import this module, as the oracle of the CUDA forward,
 backward and inference kernels in npb-gpu_b200/csrc/gnn.cu; the product
 never calls it.  It has no counterpart in the reference (the north-star
 addition "learned preconditioner"), so it restates the network as the

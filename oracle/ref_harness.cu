@@ -1,7 +1,7 @@
 /*
  * ref_harness.cu -- wraps the reference's own CG code as a shared library.
  *
- * TEST INFRASTRUCTURE ONLY (the checker and the CPU baseline, never the
+ * TEST INFRASTRUCTURE ONLY (the oracle of the tests and the CPU baseline, never the
  * product).  Compiled by oracle/Makefile straight from the reference
  * sources where they lie (CUDA/CG/cg.cu and CUDA/common/*.cpp|.cu of
  * GMAP/NPB-GPU); nothing of the reference is copied into this repository.

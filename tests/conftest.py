@@ -1,4 +1,4 @@
-"""Shared test set-up: the `gpu` marker, import paths and checker handles.
+"""Shared test set-up: the `gpu` marker, import paths and oracle handles.
 
 CPU tests (``-m "not gpu"``) cover the oracle against the reference's golden
 values, the bit-exact generator, and that libcgb.so loads and exports every

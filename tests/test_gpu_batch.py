@@ -2,8 +2,8 @@
 
 FP64 mode is the reference algorithm, so each system must match the
 single-system session (and the CPU oracle) to zeta relative 1e-10.  MIXED
-mode is judged against the FP64 mode of the same batch: zeta relative 1e-10
-where that judge has converged (its final rnorm <= 1e-10), and a system the
+mode is compared with the FP64 mode of the same batch: zeta relative 1e-10
+where that FP64 solve has converged (its final rnorm <= 1e-10), and a system the
 mixed iteration gives up on (status 1) is re-solved with the FP64 reference
 algorithm, bit-identically.
 """
@@ -39,20 +39,20 @@ def test_batch_fp64_matches_single_system_and_oracle(cgb, oracle):
     assert np.all(out["status"] == 0) and np.all(out["iters"] == 15 * 25)
 
 
-def test_batch_mixed_against_fp64_judge(cgb):
-    specs = cgb.batch_config5(nsys=48, seed=7, n_range=(1400, 8000))
+def test_batch_mixed_against_fp64_reference(cgb):
+    specs = cgb.uneven_batch_specs(nsys=48, seed=7, n_range=(1400, 8000))
     systems, shifts = build(cgb, specs)
     with cgb.Batch(systems, shifts) as b:
-        judge = b.solve(niter=15)
+        fp64 = b.solve(niter=15)
         mixed = b.solve(niter=15, mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=200)
-    converged = judge["rnorm"] <= 1e-10
+    converged = fp64["rnorm"] <= 1e-10
     assert converged.sum() >= 10
-    rel = np.abs(mixed["zeta"] - judge["zeta"]) / np.abs(judge["zeta"])
+    rel = np.abs(mixed["zeta"] - fp64["zeta"]) / np.abs(fp64["zeta"])
     ok = converged & (mixed["status"] == 0)
     assert np.all(rel[ok] <= 1e-10), rel[ok].max()
     fell = mixed["status"] == 1
-    assert np.array_equal(mixed["zeta"][fell], judge["zeta"][fell])
-    assert mixed["iters"][ok].sum() < judge["iters"][ok].sum()
+    assert np.array_equal(mixed["zeta"][fell], fp64["zeta"][fell])
+    assert mixed["iters"][ok].sum() < fp64["iters"][ok].sum()
 
 
 def test_batch_indefinite_system_falls_back(cgb):
@@ -62,12 +62,12 @@ def test_batch_indefinite_system_falls_back(cgb):
     specs = [(1400, 13, 11.4, 314159265.0), (1400, 7, 11.4, 314159265.0)]
     systems, shifts = build(cgb, specs)
     with cgb.Batch(systems, shifts) as b:
-        judge = b.solve(niter=15)
+        fp64 = b.solve(niter=15)
         mixed = b.solve(niter=15, mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=200)
     assert mixed["status"][0] == 1
-    assert mixed["zeta"][0] == judge["zeta"][0]
+    assert mixed["zeta"][0] == fp64["zeta"][0]
     assert mixed["status"][1] == 0
-    assert abs(mixed["zeta"][1] - judge["zeta"][1]) <= 1e-10 * abs(judge["zeta"][1])
+    assert abs(mixed["zeta"][1] - fp64["zeta"][1]) <= 1e-10 * abs(fp64["zeta"][1])
 
 
 def test_batch_fallback_is_the_reference_algorithm(cgb):
@@ -78,30 +78,30 @@ def test_batch_fallback_is_the_reference_algorithm(cgb):
              (1400, 13, 11.4, 314159265.0)]
     systems, shifts = build(cgb, specs)
     with cgb.Batch(systems, shifts) as b:
-        judge = b.solve(niter=5)
+        fp64 = b.solve(niter=5)
         mixed = b.solve(niter=5, mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=2)
     assert np.all(mixed["status"] == 1)
-    assert np.array_equal(mixed["zeta"], judge["zeta"])
-    assert np.array_equal(mixed["iters"], judge["iters"])
+    assert np.array_equal(mixed["zeta"], fp64["zeta"])
+    assert np.array_equal(mixed["iters"], fp64["iters"])
 
 
 def test_batch_galerkin_start(cgb):
     """The mixed mode's Galerkin start on previous iterates: the same
-    answers (within 1e-10 of the FP64 judge where it converged) with fewer
+    answers (within 1e-10 of the FP64 fp64 where it converged) with fewer
     inner iterations than a start from z = 0."""
-    specs = cgb.batch_config5(nsys=32, seed=5, n_range=(1400, 9000))
+    specs = cgb.uneven_batch_specs(nsys=32, seed=5, n_range=(1400, 9000))
     systems, shifts = build(cgb, specs)
     with cgb.Batch(systems, shifts) as b:
-        judge = b.solve(niter=15)
+        fp64 = b.solve(niter=15)
         cold = b.solve(niter=15, mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=200, recycle=0)
         warm = b.solve(niter=15, mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=200, recycle=4)
-    conv = judge["rnorm"] <= 1e-10
+    conv = fp64["rnorm"] <= 1e-10
     for out in (cold, warm):
         ok = conv & (out["status"] == 0)
-        rel = np.abs(out["zeta"] - judge["zeta"]) / np.abs(judge["zeta"])
+        rel = np.abs(out["zeta"] - fp64["zeta"]) / np.abs(fp64["zeta"])
         assert np.all(rel[ok] <= 1e-10), rel[ok].max()
         fell = out["status"] == 1
-        assert np.array_equal(out["zeta"][fell], judge["zeta"][fell])
+        assert np.array_equal(out["zeta"][fell], fp64["zeta"][fell])
     both = (cold["status"] == 0) & (warm["status"] == 0)
     assert both.sum() >= 8
     print(f"\nbatch inner iterations, z0 = 0 / Galerkin start: {cold['iters'][both].sum()} / "
@@ -112,7 +112,7 @@ def test_batch_galerkin_start(cgb):
 def test_batch_tune_keeps_results(cgb):
     """Retuning changes lanes per row and block shape, hence the order of
     the row sums; converged systems keep zeta to 1e-10."""
-    specs = cgb.batch_config5(nsys=24, seed=11, n_range=(1400, 6000))
+    specs = cgb.uneven_batch_specs(nsys=24, seed=11, n_range=(1400, 6000))
     systems, shifts = build(cgb, specs)
     with cgb.Batch(systems, shifts) as b:
         before = b.solve(niter=3)

@@ -152,7 +152,7 @@ def trained_model(cgb):
 def test_learned_preconditioner_class_c_unseen_seed(cgb, golden, tol):
     """Config: train on other seeds, test at n=150000, nonzer=15, shift=110
     (the NPB seed, never used in training); FP64 plain CG (the reference
-    trace) judges zeta: relative 1e-10 at every outer step, at the solver
+    trace) is the yardstick for zeta: relative 1e-10 at every outer step, at the solver
     tolerances the benchmark reports."""
     model, how = trained_model(cgb)
     n, nonzer, niter, shift = PARAMS["C"]

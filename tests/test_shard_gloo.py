@@ -28,7 +28,7 @@ def worker(rank, world, port, out_path):
     import datetime
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
                             world_size=world, timeout=datetime.timedelta(seconds=60))
-    specs = npbcg.batch_config5(nsys=10, seed=3, n_range=(150, 600), nonzer_range=(3, 6))
+    specs = npbcg.uneven_batch_specs(nsys=10, seed=3, n_range=(150, 600), nonzer_range=(3, 6))
     weights = [n * (nz + 1) ** 2 for n, nz, _, _ in specs]
     parts = npbcg.shard_systems(weights, world)
     o = Oracle(os.path.join(root, "oracle", "liboracle.so"))
@@ -70,7 +70,7 @@ def test_two_rank_gloo_batch(tmp_path, oracle):
     mp.start_processes(worker, args=(2, free_port(), out), nprocs=2, join=True,
                        start_method="spawn")
     got = np.load(out)
-    specs = npbcg.batch_config5(nsys=10, seed=3, n_range=(150, 600), nonzer_range=(3, 6))
+    specs = npbcg.uneven_batch_specs(nsys=10, seed=3, n_range=(150, 600), nonzer_range=(3, 6))
     want = []
     for n, nz, shift, seed in specs:
         rs, ci, a = oracle.makea(n, nz, 0.1, shift, seed)
