@@ -346,22 +346,27 @@ void invalidate_sliced(cgb_session *s)
     s->sliced_grid = 0;
 }
 
+// Enqueues the demotion of the sliced copy's L2 lines to normal priority.
+void demote_matrix_lines(cgb_session *s)
+{
+    const SliceSet &t = s->sa;
+    const std::pair<const void *, size_t> spans[3] = {
+        {t.sval, size_t(t.entries) * sizeof(double)},
+        {t.sval32, size_t(t.entries) * sizeof(float)},
+        {t.scol, size_t(t.entries) * sizeof(unsigned short)}};
+    for (const auto &sp : spans)
+        if (sp.first && sp.second)
+            l2_demote<<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
+                static_cast<const char *>(sp.first), sp.second);
+}
+
 void release(cgb_session *s)
 {
     if (!s) return;
     cudaSetDevice(s->device);
     drop_graph(s);
     if (s->l2_marked) {
-        // lines this session kept at evict_last go back to normal priority
-        const SliceSet &t = s->sa;
-        const std::pair<const void *, size_t> spans[3] = {
-            {t.sval, size_t(t.entries) * sizeof(double)},
-            {t.sval32, size_t(t.entries) * sizeof(float)},
-            {t.scol, size_t(t.entries) * sizeof(unsigned short)}};
-        for (const auto &sp : spans)
-            if (sp.first && sp.second)
-                l2_demote<<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
-                    static_cast<const char *>(sp.first), sp.second);
+        demote_matrix_lines(s);  // lines kept at evict_last go back to normal priority
         cudaStreamSynchronize(s->stream);
     }
     free_sliced(s);
@@ -809,6 +814,9 @@ int time_plan_outer(cgb_session *s, double *ms_out)
     constexpr int kSteps = 3;
     int st = ensure_trace(s, kSteps);
     if (st) return st;
+    // each candidate starts from neutral L2 priorities: lines the previous
+    // one kept at evict_last would otherwise flatter its timing
+    if (s->plan.kind == kKindSliced) demote_matrix_lines(s);
     CUDA_TRY(cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream));
     fill_ones<<<s->prop.multiProcessorCount, 256, 0, s->stream>>>(s->x(), s->n + 1);
     OuterArgs A = outer_args(s);
