@@ -296,6 +296,13 @@ int cgb_plan_l2_keep(cgb_session *s, double *bytes);
  * depend on it: it changes cache priorities only. */
 int cgb_set_l2_keep(cgb_session *s, double bytes);
 
+/* The checked build (lib/libcgb_checked.so, compiled with -DCGB_CHECKED)
+ * tests every index of the single-system SpMVs against its buffer and skips
+ * an access that would leave it.  *word receives the first failure since the
+ * last call (0 none; 1 matrix stream, 2 gathered vector, 3 output row) and
+ * is reset; -1 from the normal build. */
+int cgb_check_status(int *word);
+
 /* Grid barrier time-out self-test: runs a 2-CTA kernel whose second CTA never
  * arrives, with a wait limit of `limit_ns`, and reports the status the host
  * reads back (CGB_ERR_TIMEOUT expected).  The session stays usable. */
@@ -308,7 +315,8 @@ int cgb_selftest_wait_timeout(cgb_session *s, long long limit_ns, int *device_st
  * z = 0, then rnorm = ||x - A z||), but every pointer is caller-owned device
  * memory and the work space (p, q, r, partial sums, barrier words) sits in
  * one fixed array inside the library; this call allocates nothing.
- *   d_rowstr n+1, d_colidx / d_a nnz entries (sorted or not), d_x and d_z
+ *   d_rowstr n+1, d_colidx / d_a nnz entries (sorted or not; d_a 16-byte,
+ *   d_colidx 8-byte aligned, as cudaMalloc returns them), d_x and d_z
  *   n+1 doubles (entry n as the reference sets it), d_rnorm one double,
  *   d_status (nullable) one int: 0, or the device status on a failed wait.
  *   stream: a cudaStream_t (NULL = legacy default stream).  Asynchronous:

@@ -1,6 +1,6 @@
 """Build libcgb.so (sm_100a) in-tree: npb-gpu_b200/lib/libcgb.so.
 
-    python npb-gpu_b200/build.py [--verbose] [--ptxas-info]
+    python npb-gpu_b200/build.py [--verbose] [--ptxas-info] [--checked]
 
 nvcc cross-compiles for sm_100a without a GPU.  The host generator
 (makea.cpp) is compiled by the host compiler with -ffp-contract=off so its
@@ -20,6 +20,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["session.cu", "noalloc.cu", "gnn.cu", "batch.cu", "makea_gpu.cu"]
 CPP_SOURCES = ["makea.cpp"]
 LIB = os.path.join(LIBDIR, "libcgb.so")
+# the checked build: the single-system solver with every SpMV index tested
+CHECKED_SOURCES = ["session.cu", "noalloc.cu"]
+LIB_CHECKED = os.path.join(LIBDIR, "libcgb_checked.so")
 BINDIR = os.path.join(HERE, "bin")
 DRIVER = os.path.join(BINDIR, "cg")
 
@@ -88,10 +91,40 @@ def build(verbose=False, ptxas_info=False, force=False):
     return LIB
 
 
+def build_checked(verbose=False, force=False):
+    """lib/libcgb_checked.so: the library with the solver's translation units
+    compiled with -DCGB_CHECKED (bounds-tested SpMV indices, cgb_check_status);
+    the other objects are the normal build's."""
+    build(verbose, False, force)
+    cdir = os.path.join(BUILD, "checked")
+    os.makedirs(cdir, exist_ok=True)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    headers.append(os.path.join(os.path.dirname(HERE), "include", "cgb.h"))
+    objs = []
+    for src in CU_SOURCES + CPP_SOURCES:
+        if src in CHECKED_SOURCES:
+            s = os.path.join(CSRC, src)
+            o = os.path.join(cdir, src + ".o")
+            if force or sources_newer(o, [s] + headers):
+                run([nvcc(), "-c", s, "-o", o, *ARCH, "-O3", "-lineinfo", "-std=c++17",
+                     "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+                     "--expt-relaxed-constexpr", "-DCGB_CHECKED"], verbose)
+        else:
+            o = os.path.join(BUILD, src + ".o")
+        objs.append(o)
+    if force or sources_newer(LIB_CHECKED, objs):
+        run([nvcc(), "-shared", "-o", LIB_CHECKED, *objs, *ARCH, "-cudart", "static",
+             "-Xcompiler", "-pthread", "-lpthread"], verbose)
+    return LIB_CHECKED
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--ptxas-info", action="store_true")
     ap.add_argument("--force", action="store_true")
+    ap.add_argument("--checked", action="store_true", help="also build lib/libcgb_checked.so")
     a = ap.parse_args()
     print(build(a.verbose, a.ptxas_info, a.force))
+    if a.checked:
+        print(build_checked(a.verbose, a.force))

@@ -13,6 +13,29 @@ constexpr int kDevTimeout = 1;    // a grid-barrier wait ran past its limit
 constexpr int kDevNonFinite = 2;  // a reduction produced NaN/Inf
 constexpr int kDevBadShape = 3;   // launch shape does not match the session
 
+// Checked build (-DCGB_CHECKED, lib/libcgb_checked.so): every gather and
+// stream index of the SpMVs is tested against its buffer; a failure sets
+// this translation unit's check word (first failure wins, read by
+// cgb_check_status) and the access is skipped -- never a trap.  In the
+// normal build the test compiles to nothing.
+#ifdef CGB_CHECKED
+static __device__ int g_check_word;
+__device__ __forceinline__ bool cgb_in_range(long long i, long long n, int code)
+{
+    if (i >= 0 && i < n) return true;
+    atomicCAS(&g_check_word, 0, code);
+    return false;
+}
+#define CGB_IN_RANGE(i, n, code) cgb_in_range((long long)(i), (long long)(n), (code))
+#else
+#define CGB_IN_RANGE(i, n, code) true
+#endif
+// check codes: which index left its buffer
+constexpr int kCheckStream = 1;   // matrix stream entry (values / columns)
+constexpr int kCheckGather = 2;   // gathered vector index (column)
+constexpr int kCheckRow = 3;      // output / accumulator row
+constexpr int kCheckSplit = 4;    // row range of a CTA
+
 // State of the grid barrier.  count and gen sit on separate 128-byte lines.
 struct GridBarrier {
     unsigned int *count;  // CTAs arrived in the current generation

@@ -113,6 +113,10 @@ extern "C" int cgb_conj_grad_noalloc(int n, long long nnz, const int *d_rowstr, 
 {
     if (n < 1 || nnz < 0 || !d_rowstr || !d_colidx || !d_a || !d_x || !d_z || !d_rnorm)
         return set_error(CGB_ERR_INVALID, "noalloc conj_grad: null pointer or bad size");
+    // the SpMV reads entry pairs (16-byte value loads, 8-byte index loads)
+    if (reinterpret_cast<uintptr_t>(d_a) % 16 != 0 || reinterpret_cast<uintptr_t>(d_colidx) % 8 != 0)
+        return set_error(CGB_ERR_INVALID,
+                         "noalloc conj_grad: d_a must be 16-byte and d_colidx 8-byte aligned");
     if (n > kNoallocMaxN)
         return set_error(CGB_ERR_CAPACITY,
                          "noalloc conj_grad: n = %d exceeds the scratch capacity of %d rows", n,
@@ -156,6 +160,8 @@ extern "C" int cgb_conj_grad_noalloc(int n, long long nnz, const int *d_rowstr, 
     A.M.rowstr = d_rowstr;
     A.M.colidx = d_colidx;
     A.M.a = d_a;
+    A.M.csr_entries = nnz;  // the caller's arrays: no padding after them
+    A.M.ncols = n;
     A.x = const_cast<double *>(d_x);  // read only: finish = 0 leaves x untouched
     A.z = d_z;
     A.p = vec;

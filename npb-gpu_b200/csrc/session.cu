@@ -250,6 +250,7 @@ struct cgb_session {
     int *d_f_ptr = nullptr, *d_f_col = nullptr, *d_ft_ptr = nullptr, *d_ft_col = nullptr;
     float *d_f_val = nullptr, *d_ft_val = nullptr;
     bool has_prec = false;
+    long long prec_nnz = 0;  // entries of the preconditioner factor
     // reductions, barrier, status, trace
     double *d_part = nullptr;
     int gpad = 0;
@@ -420,6 +421,8 @@ void set_slices(cgb_session *s, const SliceSet &t, MatrixView *M)
     M->max_rows = s->sliced_max_rows;
     M->nacc = s->sliced_nacc;
     M->interleaved = t.interleaved;
+    M->slice_entries = t.entries + kPad;
+    M->ncols = s->n;
 }
 
 // Keep fractions of the sliced streams for a solve whose products are FP64
@@ -442,6 +445,8 @@ MatrixView matrix_view(cgb_session *s)
     M.colidx = s->d_colidx;
     M.a = s->d_a;
     M.a32 = s->d_a32;
+    M.csr_entries = s->nnz + kPad;
+    M.ncols = s->n;
     set_slices(s, s->sa, &M);
     set_keep(s, &M, 0);
     return M;
@@ -466,6 +471,8 @@ OuterArgs outer_args(cgb_session *s)
     A.FT.rowstr = s->d_ft_ptr;
     A.FT.colidx = s->d_ft_col;
     A.FT.a32 = s->d_ft_val;
+    A.F.csr_entries = A.FT.csr_entries = s->prec_nnz + kPad;
+    A.F.ncols = A.FT.ncols = s->n;
     if (s->prec_gen == s->layout_gen && s->prec_gen >= 0) {
         set_slices(s, s->sf, &A.F);
         set_slices(s, s->sft, &A.FT);
@@ -1490,6 +1497,7 @@ int cgb_set_preconditioner(cgb_session *s, const int *fptr, const int *fcol, con
         optr[i + 1] = int(ocol.size());
     }
     const long long nf = optr[n];
+    s->prec_nnz = nf;
     // transpose (rows of F^T = columns of F), rows in ascending order
     std::vector<int> tptr(n + 1, 0), tcol(nf);
     std::vector<float> tval(nf);
@@ -1543,6 +1551,19 @@ int cgb_plan_info(cgb_session *s, int *kind, int *lanes_per_row, int *grid, int 
     if (block) *block = s->plan.block;
     if (smem_bytes) *smem_bytes = (long long)s->plan.smem;
     if (layout_entries) *layout_entries = s->plan.kind == kKindSliced ? s->sa.entries : s->nnz;
+    return CGB_OK;
+}
+
+int cgb_check_status(int *word)
+{
+    if (!word) return set_error(CGB_ERR_INVALID, "word is null");
+#ifdef CGB_CHECKED
+    int zero = 0;
+    CUDA_TRY(cudaMemcpyFromSymbol(word, g_check_word, sizeof(int)));
+    CUDA_TRY(cudaMemcpyToSymbol(g_check_word, &zero, sizeof(int)));
+#else
+    *word = -1;
+#endif
     return CGB_OK;
 }
 

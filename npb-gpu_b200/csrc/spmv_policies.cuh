@@ -9,7 +9,8 @@
 //   RowSpmv<LPR>   CSR as the reference stores it; LPR lanes per row, each
 //                  lane two consecutive entries per chunk (one 16/8-byte load
 //                  of values, one 8-byte load of indices, from an even start,
-//                  masked to the row), four chunks in flight; the gathered
+//                  masked to the row; single loads for a last entry that
+//                  ends the arrays), four chunks in flight; the gathered
 //                  vector is read through L1/L2.
 //   SlicedSpmv     a sliced copy of the matrix built on the device (see
 //                  slices.cuh): per CTA and per column block of W columns,
@@ -163,6 +164,10 @@ struct MatrixView {
     int interleaved;                          // 0: CTA c owns its contiguous row range;
                                               // 1: CTA c owns rows c, c + G, c + 2G, ...
     int nacc;                                 // accumulators in shared memory (2 or 4)
+    // bounds of the checked build: CSR entries and sliced entries (each with
+    // the padding after them), columns of the gathered vector
+    long long csr_entries, slice_entries;
+    int ncols;
     // sliced walk: fraction of the stream's 128-byte lines (FP64, FP32, BF16
     // values with their columns) loaded with L2 priority evict_last -- kept
     // in L2 from one product to the next -- the rest evict_first; 0 = all
@@ -220,16 +225,30 @@ __device__ __forceinline__ double spmv_rows(const MatrixView &M, const VT *v, do
             for (int u = 0; u < kUnroll; u++) {
                 const int kk = k + u * kStep;
                 if (kk < k1) {
-                    av[u] = __ldcs(reinterpret_cast<const P2 *>(a + kk));
-                    cv[u] = __ldcs(reinterpret_cast<const int2 *>(M.colidx + kk));
+                    if (kk + 1 < M.csr_entries) {
+                        av[u] = __ldcs(reinterpret_cast<const P2 *>(a + kk));
+                        cv[u] = __ldcs(reinterpret_cast<const int2 *>(M.colidx + kk));
+                    } else if (CGB_IN_RANGE(kk, M.csr_entries, kCheckStream)) {
+                        // the last entry of an unpadded CSR (the caller's
+                        // arrays of cgb_conj_grad_noalloc): no pair load
+                        // past its end
+                        av[u].x = __ldcs(a + kk);
+                        av[u].y = VT(0);
+                        cv[u] = make_int2(__ldcs(M.colidx + kk), 0);
+                    } else {
+                        av[u].x = av[u].y = VT(0);
+                        cv[u] = make_int2(0, 0);
+                    }
                 }
             }
 #pragma unroll
             for (int u = 0; u < kUnroll; u++) {
                 const int kk = k + u * kStep;
                 if (kk < k1) {
-                    if (kk >= k0) s = fma_vt(av[u].x, v[cv[u].x], s);
-                    if (kk + 1 < k1) s = fma_vt(av[u].y, v[cv[u].y], s);
+                    if (kk >= k0 && CGB_IN_RANGE(cv[u].x, M.ncols, kCheckGather))
+                        s = fma_vt(av[u].x, v[cv[u].x], s);
+                    if (kk + 1 < k1 && CGB_IN_RANGE(cv[u].y, M.ncols, kCheckGather))
+                        s = fma_vt(av[u].y, v[cv[u].y], s);
                 }
             }
         }
@@ -495,19 +514,26 @@ struct SlicedSpmvT {
                     for (int u = 0; u < kU; u++) {
                         if (m + u < wp) {
                             const unsigned e = off + 64u * unsigned(m + u);
-                            av[u] = ld_stream(reinterpret_cast<const P2 *>(vals + e), pol);
-                            cv[u] = ld_stream(reinterpret_cast<const ushort2 *>(M.scol + e), pol);
+                            if (CGB_IN_RANGE(e + 1, M.slice_entries, kCheckStream)) {
+                                av[u] = ld_stream(reinterpret_cast<const P2 *>(vals + e), pol);
+                                cv[u] = ld_stream(reinterpret_cast<const ushort2 *>(M.scol + e), pol);
+                            } else {
+                                av[u].x = av[u].y = ST(0.f);
+                                cv[u] = make_ushort2(0, 0);
+                            }
                         }
                     }
 #pragma unroll
                     for (int u = 0; u < kU; u++) {
                         if (m + u < wp) {
-                            sum = fma_vt(VT(widen(av[u].x)), pv[cv[u].x], sum);
-                            sum = fma_vt(VT(widen(av[u].y)), pv[cv[u].y], sum);
+                            if (CGB_IN_RANGE(cv[u].x, M.width, kCheckGather))
+                                sum = fma_vt(VT(widen(av[u].x)), pv[cv[u].x], sum);
+                            if (CGB_IN_RANGE(cv[u].y, M.width, kCheckGather))
+                                sum = fma_vt(VT(widen(av[u].y)), pv[cv[u].y], sum);
                         }
                     }
                 }
-                if (row != 0xffffu) accb[row] += double(sum);
+                if (row != 0xffffu && CGB_IN_RANGE(row, M.max_rows, kCheckRow)) accb[row] += double(sum);
             };
             const VT *pv = reinterpret_cast<const VT *>(buf() + size_t(slot) * slot_bytes);
             double *accb = acc + size_t(slot) * M.max_rows;

@@ -158,6 +158,7 @@ _SIGNATURES = {
                                       ctypes.POINTER(ctypes.c_int)] +
                        [ctypes.POINTER(ctypes.c_double)] * 4),
     "cgb_plan_l2_keep": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    "cgb_check_status": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
     "cgb_set_l2_keep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "cgb_batch_policy": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_double),
