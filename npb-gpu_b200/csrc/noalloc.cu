@@ -113,14 +113,14 @@ extern "C" int cgb_conj_grad_noalloc(int n, long long nnz, const int *d_rowstr, 
 {
     if (n < 1 || nnz < 0 || !d_rowstr || !d_colidx || !d_a || !d_x || !d_z || !d_rnorm)
         return set_error(CGB_ERR_INVALID, "noalloc conj_grad: null pointer or bad size");
-    // the SpMV reads entry pairs (16-byte value loads, 8-byte index loads)
-    if (reinterpret_cast<uintptr_t>(d_a) % 16 != 0 || reinterpret_cast<uintptr_t>(d_colidx) % 8 != 0)
-        return set_error(CGB_ERR_INVALID,
-                         "noalloc conj_grad: d_a must be 16-byte and d_colidx 8-byte aligned");
     if (n > kNoallocMaxN)
         return set_error(CGB_ERR_CAPACITY,
                          "noalloc conj_grad: n = %d exceeds the scratch capacity of %d rows", n,
                          kNoallocMaxN);
+    // the SpMV reads entry pairs (16-byte value loads, 8-byte index loads)
+    if (reinterpret_cast<uintptr_t>(d_a) % 16 != 0 || reinterpret_cast<uintptr_t>(d_colidx) % 8 != 0)
+        return set_error(CGB_ERR_INVALID,
+                         "noalloc conj_grad: d_a must be 16-byte and d_colidx 8-byte aligned");
     int device = -1;
     if (cudaGetDevice(&device) != cudaSuccess)
         return set_error(CGB_ERR_NO_DEVICE, "no current CUDA device");

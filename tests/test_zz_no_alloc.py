@@ -60,6 +60,17 @@ def test_noalloc_conj_grad_matches_session(cgb):
         assert abs(float(d_rn.item()) - rn_ref) <= 1e-10 * xnorm, f"call {call}: rnorm"
 
 
+def test_noalloc_rejects_misaligned(cgb):
+    """The SpMV reads entry pairs: values must be 16-byte, columns 8-byte
+    aligned (as cudaMalloc returns them); anything else is refused before
+    any launch."""
+    st = cgb.lib().cgb_conj_grad_noalloc(100, 10, ctypes.c_void_p(256), ctypes.c_void_p(260),
+                                          ctypes.c_void_p(264), ctypes.c_void_p(256),
+                                          ctypes.c_void_p(256), ctypes.c_void_p(256), None, None)
+    assert st == cgb.ERR_INVALID
+    assert b"aligned" in cgb.lib().cgb_last_error()
+
+
 def test_noalloc_rejects_oversize(cgb):
     n = 262145
     null = ctypes.c_void_p(1)
