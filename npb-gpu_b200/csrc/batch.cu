@@ -950,12 +950,13 @@ int cgb_batch_create(int device, int nsys, const int *n, const int *const *rowst
     for (int s = 0; s < nsys; s++) {
         const SysDesc &d = b->desc[s];
         const long long nz = rowstr[s][n[s]];
-        if (cudaMemcpy(b->d_rowstr + d.row_off, rowstr[s], sizeof(int) * (n[s] + 1),
-                       cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(b->d_colidx + d.nnz_off, colidx[s], sizeof(int) * nz,
-                       cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(b->d_a + d.nnz_off, a[s], sizeof(double) * nz, cudaMemcpyHostToDevice) !=
-                cudaSuccess) {
+        // on the batch's stream, so the FP32 conversion below runs after them
+        if (cudaMemcpyAsync(b->d_rowstr + d.row_off, rowstr[s], sizeof(int) * (n[s] + 1),
+                            cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
+            cudaMemcpyAsync(b->d_colidx + d.nnz_off, colidx[s], sizeof(int) * nz,
+                            cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
+            cudaMemcpyAsync(b->d_a + d.nnz_off, a[s], sizeof(double) * nz, cudaMemcpyHostToDevice,
+                            b->stream) != cudaSuccess) {
             batch_release(b);
             return set_error(CGB_ERR_CUDA, "batch upload failed");
         }

@@ -36,7 +36,7 @@ namespace {
 constexpr int kNoallocMaxN = 262144;       // largest order served (NPB classes S..C fit)
 constexpr int kNoallocMaxGrid = 1024;      // CTAs of the cooperative launch
 constexpr size_t kLine = 256;
-constexpr size_t kHeaderBytes = 4 * kLine;  // barrier count, generation, status, trace
+constexpr size_t kHeaderBytes = 4 * kLine;  // barrier arrivals, (spare), status, trace
 constexpr size_t kSplitBytes = ((kNoallocMaxGrid + 1) * sizeof(int) + kLine - 1) / kLine * kLine;
 // the fixed-count FP64 kernel uses the slots below kSlotGram only
 constexpr size_t kPartBytes = size_t(kSlotGram) * kNoallocMaxGrid * sizeof(double);
@@ -139,8 +139,7 @@ extern "C" int cgb_conj_grad_noalloc(int n, long long nnz, const int *d_rowstr, 
         return set_error(CGB_ERR_CUDA, "noalloc conj_grad: kernel cannot be resident");
     const int grid = std::max(1, std::min({per_sm * prop.multiProcessorCount, n, kNoallocMaxGrid}));
 
-    unsigned *count = reinterpret_cast<unsigned *>(base);
-    unsigned *gen = reinterpret_cast<unsigned *>(base + kLine);
+    unsigned long long *arrivals = reinterpret_cast<unsigned long long *>(base);
     int *status = reinterpret_cast<int *>(base + 2 * kLine);
     StepTrace *trace = reinterpret_cast<StepTrace *>(base + 3 * kLine);
     int *split = reinterpret_cast<int *>(base + kHeaderBytes);
@@ -170,8 +169,7 @@ extern "C" int cgb_conj_grad_noalloc(int n, long long nnz, const int *d_rowstr, 
     A.row_split = split;
     A.part = part;
     A.gpad = kNoallocMaxGrid;
-    A.gb.count = count;
-    A.gb.gen = gen;
+    A.gb.arrivals = arrivals;
     A.gb.status = status;
     A.gb.limit_ns = 2000000000LL;
     A.shift = 0.0;

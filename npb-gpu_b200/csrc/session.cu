@@ -295,8 +295,8 @@ struct cgb_session {
     double *p() { return d_vec + 2 * vstride; }
     double *q() { return d_vec + 3 * vstride; }
     double *r() { return d_vec + 4 * vstride; }
-    unsigned *count() { return d_sync; }
-    unsigned *gen() { return d_sync + 32; }
+    // the grid barrier's 64-bit arrival count (its own 128-byte line)
+    unsigned long long *arrivals() { return reinterpret_cast<unsigned long long *>(d_sync); }
     unsigned *ticket() { return d_sync + 64; }
 };
 
@@ -480,8 +480,7 @@ OuterArgs outer_args(cgb_session *s)
     A.row_split = s->d_split;
     A.part = s->d_part;
     A.gpad = s->gpad;
-    A.gb.count = s->count();
-    A.gb.gen = s->gen();
+    A.gb.arrivals = s->arrivals();
     A.gb.status = s->d_status;
     A.gb.limit_ns = s->opts.wait_limit_ns > 0 ? s->opts.wait_limit_ns : kDefaultWaitNs;
     A.refresh_every = 10;
@@ -621,9 +620,10 @@ int build_sliced(cgb_session *s, int grid)
         return set_error(CGB_ERR_STATE, "sliced layout: %d rows per CTA exceed shared memory", max_rows);
     if (dev_reserve(&s->d_chunk_slice, &s->cap_chunk, chunk_slice.size()))
         return set_error(CGB_ERR_NOMEM, "sliced layout: metadata allocation failed");
-    CUDA_TRY(cudaMemcpy(s->d_split, split.data(), sizeof(int) * (grid + 1), cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(s->d_chunk_slice, chunk_slice.data(), sizeof(int) * chunk_slice.size(),
-                        cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpyAsync(s->d_split, split.data(), sizeof(int) * (grid + 1), cudaMemcpyHostToDevice,
+                             s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->d_chunk_slice, chunk_slice.data(), sizeof(int) * chunk_slice.size(),
+                             cudaMemcpyHostToDevice, s->stream));
     s->sa.chunk_slice = nullptr;  // the session's table
     const int st = [&] {
         SliceSet &t = s->sa;
@@ -668,8 +668,8 @@ int ensure_prec_slices(cgb_session *s)
         sets[m]->blocks = blocks;
         cudaError_t e = dev_alloc(&sets[m]->chunk_slice, chunk_slice.size());
         if (e == cudaSuccess)
-            e = cudaMemcpy(sets[m]->chunk_slice, chunk_slice.data(), sizeof(int) * chunk_slice.size(),
-                           cudaMemcpyHostToDevice);
+            e = cudaMemcpyAsync(sets[m]->chunk_slice, chunk_slice.data(), sizeof(int) * chunk_slice.size(),
+                                cudaMemcpyHostToDevice, s->stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(s->d_flag, 0, sizeof(int), s->stream);
         if (e == cudaSuccess) {
             build_segments<<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
@@ -761,7 +761,10 @@ int apply_plan(cgb_session *s, const Plan &pl)
 {
     std::vector<int> split;
     make_split(s->n, s->h_rowstr_copy.data(), pl.grid, split);
-    CUDA_TRY(cudaMemcpy(s->d_split, split.data(), sizeof(int) * (pl.grid + 1), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpyAsync(s->d_split, split.data(), sizeof(int) * (pl.grid + 1),
+                             cudaMemcpyHostToDevice, s->stream));
+    // the barrier's arrival count must be a multiple of the new grid size
+    CUDA_TRY(cudaMemsetAsync(s->d_sync, 0, sizeof(unsigned long long), s->stream));
     s->plan = pl;
     drop_graph(s);
     return CGB_OK;
@@ -803,7 +806,7 @@ int time_plan_spmv(cgb_session *s, int reps, int fp32, double *ms_out)
     int st = 0;
     CUDA_TRY(cudaMemcpy(&st, s->d_status, sizeof(int), cudaMemcpyDeviceToHost));
     if (st != kDevOk) {
-        CUDA_TRY(cudaMemset(s->d_status, 0, sizeof(int)));
+        CUDA_TRY(cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream));
         return set_error(CGB_ERR_TIMEOUT, "SpMV wait failed (status %d)", st);
     }
     return CGB_OK;
@@ -844,8 +847,8 @@ int time_plan_outer(cgb_session *s, double *ms_out)
     int dst = 0;
     CUDA_TRY(cudaMemcpy(&dst, s->d_status, sizeof(int), cudaMemcpyDeviceToHost));
     if (dst == kDevOk) return CGB_OK;
-    CUDA_TRY(cudaMemset(s->d_sync, 0, sizeof(unsigned) * 96));
-    CUDA_TRY(cudaMemset(s->d_status, 0, sizeof(int)));
+    CUDA_TRY(cudaMemsetAsync(s->d_sync, 0, sizeof(unsigned) * 96, s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream));
     if (dst == kDevNonFinite) return CGB_OK;
     return set_error(dst == kDevTimeout ? CGB_ERR_TIMEOUT : CGB_ERR_CUDA,
                      "outer step failed while timing the plan (device status %d)", dst);
@@ -986,8 +989,8 @@ int collect_status(cgb_session *s)
     int st = 0;
     CUDA_TRY(cudaMemcpy(&st, s->d_status, sizeof(int), cudaMemcpyDeviceToHost));
     if (st == kDevOk) return CGB_OK;
-    CUDA_TRY(cudaMemset(s->d_sync, 0, sizeof(unsigned) * 96));
-    CUDA_TRY(cudaMemset(s->d_status, 0, sizeof(int)));
+    CUDA_TRY(cudaMemsetAsync(s->d_sync, 0, sizeof(unsigned) * 96, s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream));
     if (st == kDevTimeout)
         return set_error(CGB_ERR_TIMEOUT, "a device wait hit its %lld ns limit",
                          (long long)(s->opts.wait_limit_ns > 0 ? s->opts.wait_limit_ns : kDefaultWaitNs));
@@ -1218,20 +1221,20 @@ int create_shell(int n, const cgb_options *opts, cgb_session **out)
     CREATE_TRY(cudaEventCreate(&s->ev1));
     CREATE_TRY(dev_alloc(&s->d_rowstr, size_t(n) + 1));
     CREATE_TRY(dev_alloc(&s->d_vec, 5 * s->vstride));
-    CREATE_TRY(cudaMemset(s->d_vec, 0, sizeof(double) * 5 * s->vstride));
+    CREATE_TRY(cudaMemsetAsync(s->d_vec, 0, sizeof(double) * 5 * s->vstride, s->stream));
     CREATE_TRY(dev_alloc(&s->d_p32, s->vstride));
-    CREATE_TRY(cudaMemset(s->d_p32, 0, sizeof(float) * s->vstride));
+    CREATE_TRY(cudaMemsetAsync(s->d_p32, 0, sizeof(float) * s->vstride, s->stream));
     CREATE_TRY(dev_alloc(&s->d_r32, s->vstride));
-    CREATE_TRY(cudaMemset(s->d_r32, 0, sizeof(float) * s->vstride));
+    CREATE_TRY(cudaMemsetAsync(s->d_r32, 0, sizeof(float) * s->vstride, s->stream));
     CREATE_TRY(dev_alloc(&s->d_y, s->vstride));
-    CREATE_TRY(cudaMemset(s->d_y, 0, sizeof(double) * s->vstride));
+    CREATE_TRY(cudaMemsetAsync(s->d_y, 0, sizeof(double) * s->vstride, s->stream));
     CREATE_TRY(dev_alloc(&s->d_hx, kMaxRecycle * s->vstride));
     CREATE_TRY(dev_alloc(&s->d_hw, kMaxRecycle * s->vstride));
     CREATE_TRY(dev_alloc(&s->d_part, size_t(kSlotCount) * s->gpad));
     CREATE_TRY(dev_alloc(&s->d_sync, 96));
-    CREATE_TRY(cudaMemset(s->d_sync, 0, sizeof(unsigned) * 96));
+    CREATE_TRY(cudaMemsetAsync(s->d_sync, 0, sizeof(unsigned) * 96, s->stream));
     CREATE_TRY(dev_alloc(&s->d_status, 1));
-    CREATE_TRY(cudaMemset(s->d_status, 0, sizeof(int)));
+    CREATE_TRY(cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream));
     CREATE_TRY(dev_alloc(&s->d_flag, 1));
     CREATE_TRY(dev_alloc(&s->d_split, size_t(s->gpad) + 1));
     CREATE_TRY(dev_alloc(&s->d_dot, 1));
@@ -1519,16 +1522,16 @@ int cgb_set_preconditioner(cgb_session *s, const int *fptr, const int *fcol, con
         dev_alloc(&s->d_f_val, size_t(nf) + kPad) || dev_alloc(&s->d_ft_ptr, size_t(n) + 1) ||
         dev_alloc(&s->d_ft_col, size_t(nf) + kPad) || dev_alloc(&s->d_ft_val, size_t(nf) + kPad))
         return set_error(CGB_ERR_NOMEM, "factor allocation failed");
-    CUDA_TRY(cudaMemset(s->d_f_col, 0, sizeof(int) * (nf + kPad)));
-    CUDA_TRY(cudaMemset(s->d_f_val, 0, sizeof(float) * (nf + kPad)));
-    CUDA_TRY(cudaMemset(s->d_ft_col, 0, sizeof(int) * (nf + kPad)));
-    CUDA_TRY(cudaMemset(s->d_ft_val, 0, sizeof(float) * (nf + kPad)));
-    CUDA_TRY(cudaMemcpy(s->d_f_ptr, optr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(s->d_f_col, ocol.data(), sizeof(int) * nf, cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(s->d_f_val, val32.data(), sizeof(float) * nf, cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(s->d_ft_ptr, tptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(s->d_ft_col, tcol.data(), sizeof(int) * nf, cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(s->d_ft_val, tval.data(), sizeof(float) * nf, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemsetAsync(s->d_f_col, 0, sizeof(int) * (nf + kPad), s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->d_f_val, 0, sizeof(float) * (nf + kPad), s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->d_ft_col, 0, sizeof(int) * (nf + kPad), s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->d_ft_val, 0, sizeof(float) * (nf + kPad), s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->d_f_ptr, optr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->d_f_col, ocol.data(), sizeof(int) * nf, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->d_f_val, val32.data(), sizeof(float) * nf, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->d_ft_ptr, tptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->d_ft_col, tcol.data(), sizeof(int) * nf, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->d_ft_val, tval.data(), sizeof(float) * nf, cudaMemcpyHostToDevice, s->stream));
     s->has_prec = true;
     drop_graph(s);
     return CGB_OK;
@@ -1634,8 +1637,7 @@ int cgb_selftest_wait_timeout(cgb_session *s, long long limit_ns, int *device_st
         return set_error(CGB_ERR_INVALID, "limit_ns must be in (0, 1e10]");
     CUDA_TRY(cudaSetDevice(s->device));
     GridBarrier gb;
-    gb.count = s->count();
-    gb.gen = s->gen();
+    gb.arrivals = s->arrivals();
     gb.status = s->d_status;
     gb.limit_ns = limit_ns;
     CUDA_TRY(cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream));
