@@ -78,8 +78,8 @@ struct BatchArgs {
     long long hstride;
     int recycle;
     // teams: the search vector's exchange copy (vec_off layout), per system
-    // a barrier (count, gen: kSyncStride words apart, 2 * kSyncStride words a
-    // system) and 2 x kMaxTeam x kTeamValues reduction slots
+    // a barrier's 64-bit arrival count (2 * kSyncStride words a system, one
+    // 256-byte line) and 2 x kMaxTeam x kTeamValues reduction slots
     double *pg;
     unsigned *team_sync;
     double *team_part;
@@ -98,7 +98,7 @@ struct Team {
 // The team's barrier words and reduction slots (computed where used: kept in
 // registers across the CG loop they would crowd it).
 struct TeamMem {
-    unsigned *count, *gen;
+    unsigned long long *arrivals;  // the team barrier's count (zeroed every launch)
     double *part;
     int *status;  // the launch's device status word
 };
@@ -106,8 +106,7 @@ struct TeamMem {
 __device__ __forceinline__ TeamMem team_mem(const BatchArgs &B, int id)
 {
     TeamMem M;
-    M.count = B.team_sync + size_t(id) * (2 * kSyncStride);
-    M.gen = M.count + kSyncStride;
+    M.arrivals = reinterpret_cast<unsigned long long *>(B.team_sync + size_t(id) * (2 * kSyncStride));
     M.part = B.team_part + size_t(id) * (2 * kMaxTeam * kTeamValues);
     M.status = B.dev_status;
     return M;
@@ -187,7 +186,7 @@ __device__ __forceinline__ double cta_sum(double v, double *red)
 
 __device__ __forceinline__ bool team_barrier(const TeamMem &M, const Team &T)
 {
-    return counted_barrier(M.count, M.gen, unsigned(T.size), M.status, kTeamWaitNs);
+    return counted_barrier(M.arrivals, unsigned(T.size), M.status, kTeamWaitNs);
 }
 
 // Team sum of one value per thread: the CTA sum, then (teams) the members'

@@ -105,33 +105,35 @@ __device__ __forceinline__ void raise_status(int *status, int code)
     atomicCAS(status, kDevOk, code);
 }
 
-// Barrier of `members` co-resident CTAs (the CTAs of one system's team in
-// the batch kernel, whose membership changes from system to system, hence
-// a resettable count and a generation word).  Thread 0 of each
-// CTA arrives with an acq_rel atomic; the last arriver resets the count and
-// releases the next generation; the others poll the generation with acquire
-// loads, which also makes every write issued before the barrier by any CTA
-// visible after it.  Every wait is bounded: past `limit_ns`, or as soon as
-// another CTA has raised the status word, the barrier records kDevTimeout
-// (first failure wins) and returns false; the caller then leaves the kernel.
-// The host resets count/gen after a failed launch.
-__device__ __forceinline__ bool counted_barrier(unsigned *count, unsigned *gen, unsigned members,
+// Barrier of `members` co-resident CTAs over a 64-bit count of arrivals
+// that only grows (the whole grid for grid_barrier; the CTAs of one
+// system's team in the batch kernel).  Thread 0 of each CTA adds its
+// arrival with an acq_rel atomic, which also tells it the target (the next
+// multiple of `members`); the last arriver goes on at once, the others poll
+// the count with acquire loads until it reaches the target.  Every arrival
+// is a release, so a CTA that sees the target sees every write made before
+// the barrier by any member.  One atomic and the polls are the whole cost
+// (no generation word to publish after the count): 1.36 against 2.19 us a
+// barrier for 148 CTAs.  The count must be a multiple of `members` when
+// the members first use it (zeroed by the host for a new grid size or
+// team, and after a failed launch).  Every wait is bounded: past
+// `limit_ns`, or as soon as another CTA has raised the status word, the
+// barrier records kDevTimeout (first failure wins) and returns false; the
+// caller then leaves the kernel.
+__device__ __forceinline__ bool counted_barrier(unsigned long long *arrivals, unsigned members,
                                                 int *status, long long limit_ns)
 {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        const unsigned g = ld_acquire_u32(gen);
-        __threadfence();
-        const unsigned arrived = atom_add_acq_rel_u32(count, 1u);
-        if (arrived == members - 1) {
-            atomicExch(count, 0u);
-            st_release_u32(gen, g + 1u);
-        } else {
+        const unsigned long long g = members;
+        const unsigned long long old = atom_add_acq_rel_u64(arrivals, 1ull);
+        const unsigned long long target = (old / g + 1ull) * g;
+        if (old + 1ull != target) {
             const unsigned long long t0 = global_ns();
             unsigned spins = 0;
-            while (ld_acquire_u32(gen) == g) {
+            while (ld_acquire_u64(arrivals) < target) {
                 if (((++spins) & 63u) == 0u) {
                     if (ld_relaxed_i32(status) != kDevOk) {
                         ok = 0;
@@ -151,44 +153,10 @@ __device__ __forceinline__ bool counted_barrier(unsigned *count, unsigned *gen, 
     return s_ok != 0;
 }
 
-// Grid-wide barrier for a co-resident (cooperative) grid.  Thread 0 of each
-// CTA adds its arrival with an acq_rel atomic, which also tells it the
-// target (the next multiple of the grid size); the last arriver goes on at
-// once, the others poll the count with acquire loads until it reaches the
-// target.  Every arrival is a release, so a CTA that sees the target sees
-// every write made before the barrier by any CTA.  One atomic and the polls
-// are the whole cost (no generation word to publish after the count): 1.36
-// against 2.19 us a barrier for 148 CTAs.  Bounded like counted_barrier.
+// Grid-wide barrier for a co-resident (cooperative) grid.
 __device__ __forceinline__ bool grid_barrier(const GridBarrier &gb)
 {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        const unsigned long long g = gridDim.x;
-        const unsigned long long old = atom_add_acq_rel_u64(gb.arrivals, 1ull);
-        const unsigned long long target = (old / g + 1ull) * g;
-        if (old + 1ull != target) {
-            const unsigned long long t0 = global_ns();
-            unsigned spins = 0;
-            while (ld_acquire_u64(gb.arrivals) < target) {
-                if (((++spins) & 63u) == 0u) {
-                    if (ld_relaxed_i32(gb.status) != kDevOk) {
-                        ok = 0;
-                        break;
-                    }
-                    if ((long long)(global_ns() - t0) > gb.limit_ns) {
-                        raise_status(gb.status, kDevTimeout);
-                        ok = 0;
-                        break;
-                    }
-                }
-            }
-        }
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
+    return counted_barrier(gb.arrivals, gridDim.x, gb.status, gb.limit_ns);
 }
 
 template <int W>
