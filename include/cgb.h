@@ -303,6 +303,11 @@ int cgb_set_l2_keep(cgb_session *s, double bytes);
  * is reset; -1 from the normal build. */
 int cgb_check_status(int *word);
 
+/* Device microseconds per grid barrier: `iters` barriers back to back in
+ * one cooperative launch of the plan's grid and the FP64 outer step's
+ * block size (after a short warm-up launch). */
+int cgb_time_barrier(cgb_session *s, int iters, double *us_per_barrier);
+
 /* Grid barrier time-out self-test: runs a 2-CTA kernel whose second CTA never
  * arrives, with a wait limit of `limit_ns`, and reports the status the host
  * reads back (CGB_ERR_TIMEOUT expected).  The session stays usable. */

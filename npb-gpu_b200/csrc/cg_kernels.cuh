@@ -1071,6 +1071,13 @@ __global__ void slice_fill(const int *__restrict__ seg, int seg_stride, int nblk
 
 // Self-test of the bounded wait: CTA 1 never arrives, so CTA 0's barrier
 // wait runs into its limit and records kDevTimeout.
+// `iters` grid barriers back to back: the barrier's cost (cgb_time_barrier).
+static __global__ void barrier_loop(GridBarrier gb, int iters)
+{
+    for (int i = 0; i < iters; i++)
+        if (!grid_barrier(gb)) return;
+}
+
 static __global__ void barrier_timeout_probe(GridBarrier gb)
 {
     if (blockIdx.x == 1) return;

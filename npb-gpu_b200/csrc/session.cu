@@ -1631,6 +1631,38 @@ int cgb_time_outer_steps(cgb_session *s, int niter, double shift, double *kernel
     return CGB_OK;
 }
 
+int cgb_time_barrier(cgb_session *s, int iters, double *us_per_barrier)
+{
+    if (!s || iters < 1 || iters > 10000000 || !us_per_barrier)
+        return set_error(CGB_ERR_INVALID, "bad arguments");
+    CUDA_TRY(cudaSetDevice(s->device));
+    GridBarrier gb;
+    gb.arrivals = s->arrivals();
+    gb.status = s->d_status;
+    gb.limit_ns = s->opts.wait_limit_ns > 0 ? s->opts.wait_limit_ns : kDefaultWaitNs;
+    CUDA_TRY(cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream));
+    // the plan's grid (its count stays a multiple of it) with the FP64
+    // outer step's block size
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(s->plan.grid);
+    cfg.blockDim = dim3(s->plan.block);
+    cfg.stream = s->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CUDA_TRY(cudaLaunchKernelEx(&cfg, barrier_loop, gb, 16));  // warm-up
+    CUDA_TRY(cudaEventRecord(s->ev0, s->stream));
+    CUDA_TRY(cudaLaunchKernelEx(&cfg, barrier_loop, gb, iters));
+    CUDA_TRY(cudaEventRecord(s->ev1, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    *us_per_barrier = 1e3 * double(ms) / iters;
+    return collect_status(s);
+}
+
 int cgb_selftest_wait_timeout(cgb_session *s, long long limit_ns, int *device_status)
 {
     if (!s || !device_status || limit_ns <= 0 || limit_ns > 10000000000LL)

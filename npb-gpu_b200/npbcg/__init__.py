@@ -159,6 +159,8 @@ _SIGNATURES = {
                        [ctypes.POINTER(ctypes.c_double)] * 4),
     "cgb_plan_l2_keep": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     "cgb_check_status": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
+    "cgb_time_barrier": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_double)]),
     "cgb_set_l2_keep": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "cgb_batch_policy": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_double),
@@ -366,6 +368,12 @@ class Session:
         """Bytes of the sliced matrix stream kept in L2 across products
         (overrides the autotuner; 0 = pure stream; results unchanged)."""
         _check(lib().cgb_set_l2_keep(self._h, float(nbytes)))
+
+    def time_barrier(self, iters=20000):
+        """Device microseconds per grid barrier of the session's plan."""
+        us = ctypes.c_double()
+        _check(lib().cgb_time_barrier(self._h, int(iters), ctypes.byref(us)))
+        return us.value
 
     def selftest_wait_timeout(self, limit_ns):
         """Returns (status, device_status) of the bounded-wait self-test."""

@@ -4,6 +4,7 @@
     python npb-gpu_b200/npbcg/profile_case.py --cls B --what solve --niter 2
     python npb-gpu_b200/npbcg/profile_case.py --cls B --what sweep
     python npb-gpu_b200/npbcg/profile_case.py --what batch --nsys 64 --niter 2
+    python npb-gpu_b200/npbcg/profile_case.py --cls B --what barrier --reps 20000
 
 `spmv` launches the standalone FP64 SpMV+dot kernel `reps` times (after one
 warm-up launch); `solve` runs one power iteration of `niter` outer steps;
@@ -22,7 +23,7 @@ import npbcg  # noqa: E402
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cls", default="B", choices=sorted(npbcg.CLASSES))
-    ap.add_argument("--what", default="spmv", choices=["spmv", "solve", "sweep", "batch"])
+    ap.add_argument("--what", default="spmv", choices=["spmv", "solve", "sweep", "batch", "barrier"])
     ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed", "learned"],
                     help="solve / batch: the solver mode (mixed: tol 1e-12, cgitmax 100)")
     ap.add_argument("--nsys", type=int, default=64, help="batch: systems of the batched workload")
@@ -77,7 +78,9 @@ def main():
             if a.keep_mb is not None:
                 s.set_l2_keep(a.keep_mb * 1e6)
             out["plan"] = s.plan()
-            if a.what == "spmv":
+            if a.what == "barrier":
+                out.update(us_per_barrier=[s.time_barrier(a.reps) for _ in range(3)])
+            elif a.what == "spmv":
                 ms = s.time_spmv(a.reps, fp32=a.fp32)
                 b = (npbcg.spmv_bytes_fp32 if a.fp32 else npbcg.spmv_bytes_fp64)(n, nnz)
                 out.update(ms=ms, gbs=b / ms / 1e6)

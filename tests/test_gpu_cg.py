@@ -187,6 +187,19 @@ def test_wait_timeout_selftest_leaves_session_usable(cgb):
     assert abs(out["zeta"][-1] - VERIFY["S"]) / VERIFY["S"] <= 1e-10
 
 
+def test_barrier_timer_and_solve_after_it(cgb, golden):
+    """The grid barrier's timer runs on the plan's grid, and the solve after
+    it (the barrier count has moved on) still matches the reference trace."""
+    n, nonzer, niter, shift = PARAMS["B"]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    with cgb.Session(rs, ci, a) as s:
+        us = s.time_barrier(5000)
+        assert 0.2 < us < 20.0
+        out = s.power_iterate(niter, shift)
+    ref = np.array(golden["B"]["seeds"]["314159265.0"]["zeta"])
+    assert np.max(np.abs(out["zeta"] - ref) / np.abs(ref)) <= 1e-10
+
+
 def test_spmv_timer_runs(cgb):
     s, _ = session_for(cgb, "A")
     ms = s.time_spmv(5)
