@@ -211,11 +211,24 @@ __device__ __forceinline__ double block_sum(double v, double *scratch)
 // Sum of the `nparts` per-CTA partials at `part`, computed identically by
 // every CTA (same order), returned to all threads through `bcast`.  Reads go
 // to L2 (ld.cg): the partials were written by other SMs during this launch.
+// The loads of a lane's partials are all issued before the first add (one
+// L2 round trip instead of one per partial); the adds keep the order
+// part[lane] + part[lane + 32] + ..., so the sum is the same in every CTA.
 __device__ __forceinline__ double all_partials(const double *part, int nparts, double *bcast)
 {
     if (threadIdx.x < 32) {
+        constexpr int kAhead = 8;  // 256 partials in one round trip
+        double v[kAhead];
+#pragma unroll
+        for (int u = 0; u < kAhead; u++) {
+            const int i = int(threadIdx.x) + 32 * u;
+            v[u] = i < nparts ? __ldcg(part + i) : 0.0;
+        }
         double s = 0.0;
-        for (int i = threadIdx.x; i < nparts; i += 32) s += __ldcg(part + i);
+#pragma unroll
+        for (int u = 0; u < kAhead; u++)
+            if (int(threadIdx.x) + 32 * u < nparts) s += v[u];
+        for (int i = int(threadIdx.x) + 32 * kAhead; i < nparts; i += 32) s += __ldcg(part + i);
         s = warp_sum(s);
         if (threadIdx.x == 0) *bcast = s;
     }
