@@ -91,6 +91,13 @@ typedef struct cgb_options {
                                  memory by TMA bulk copies), 3 = sliced with an L2 prefetch
                                  of each warp's slices of the next column block (0 times
                                  2 against 3 and keeps the faster) */
+    int panel_rows;           /* sliced kernel: most rows a CTA sums at a time, rounded down to
+                                 a multiple of 32 (0 = as many as its shared accumulators
+                                 hold, about 2100).  A CTA with more rows walks them in row
+                                 panels, every column block once per panel (class D: 5
+                                 panels); every row is summed in the same order, the fused dot
+                                 products add rows in another order.  No counterpart
+                                 in the reference. */
 } cgb_options;
 
 void cgb_default_options(cgb_options *opts);
@@ -295,6 +302,11 @@ int cgb_plan_l2_keep(cgb_session *s, double *bytes);
 /* Overrides the autotuner's choice (>= 0; 0 = pure stream).  Results do not
  * depend on it: it changes cache priorities only. */
 int cgb_set_l2_keep(cgb_session *s, double bytes);
+/* Row panels of the sliced plan: each CTA walks its rows of A in `*panels`
+ * pieces and the preconditioner's copies in `*prec_panels` (1 = one walk;
+ * more above about 2100 rows a CTA, or below opts->panel_rows); 0 and 0 for
+ * the row plan.  No counterpart in the reference. */
+int cgb_plan_panels(cgb_session *s, int *panels, int *prec_panels);
 
 /* The checked build (lib/libcgb_checked.so, compiled with -DCGB_CHECKED)
  * tests every index of the single-system SpMVs against its buffer and skips

@@ -786,6 +786,18 @@ static __global__ void __launch_bounds__(kSlicedMixedBlock, 1) outer_step_mixed_
     outer_step_mixed_body<SlicedSpmvMixedPf>(A);
 }
 
+// Row-panel instances: the sliced plan of a matrix whose rows per CTA do
+// not fit the shared accumulators (class D: 10 K rows a CTA).
+static __global__ void __launch_bounds__(kSlicedBlock, 1) outer_step_fp64_sliced_pn(OuterArgs A)
+{
+    outer_step_body<SlicedSpmvPanels>(A);
+}
+
+static __global__ void __launch_bounds__(kSlicedMixedBlock, 1) outer_step_mixed_sliced_pn(OuterArgs A)
+{
+    outer_step_mixed_body<SlicedSpmvMixedPanels>(A);
+}
+
 // lanes per row of the preconditioner products (F has about half of A's
 // entries per row)
 constexpr int kLanesF = 16;
@@ -799,6 +811,11 @@ __global__ void __launch_bounds__(512, 2) outer_step_pcg(OuterArgs A)
 static __global__ void __launch_bounds__(kSlicedPcgBlock, 1) outer_step_pcg_sliced(OuterArgs A)
 {
     outer_step_pcg_body<SlicedSpmvPcg, kLanesF>(A);
+}
+
+static __global__ void __launch_bounds__(kSlicedPcgBlock, 1) outer_step_pcg_sliced_pn(OuterArgs A)
+{
+    outer_step_pcg_body<SlicedSpmvPcgPanels, kLanesF>(A);
 }
 
 // Standalone q = A p with the p.q reduction fused (the work of reference
@@ -875,6 +892,16 @@ static __global__ void __launch_bounds__(kSlicedBlock, 1) spmv_dot_sliced32_pf(S
     spmv_dot_body<SlicedSpmvPf, 2>(S);
 }
 
+static __global__ void __launch_bounds__(kSlicedBlock, 1) spmv_dot_sliced_pn(SpmvArgs S)
+{
+    spmv_dot_body<SlicedSpmvPanels, 1>(S);
+}
+
+static __global__ void __launch_bounds__(kSlicedBlock, 1) spmv_dot_sliced32_pn(SpmvArgs S)
+{
+    spmv_dot_body<SlicedSpmvPanels, 2>(S);
+}
+
 // ------------------------------------------------------------- utilities
 // Demotes the L2 lines of [p, p + bytes) to normal eviction priority: the
 // lines a sliced walk kept at evict_last, so that whoever uses the L2 next
@@ -929,34 +956,50 @@ static __global__ void build_segments(const int *__restrict__ rowstr,
     }
 }
 
-// Sliced layout, step 1 -- one CTA per chunk (CTA c of the solve grid,
-// column block b): order the chunk's rows by descending segment length
+// Sliced layout, step 1 -- one CTA per chunk (row panel k of CTA c of the
+// solve grid, column block b; chunk (c*panels + k)*nblk + b): order the
+// chunk's rows by descending segment length
 // (counting sort on min(len, 255)), 32 to a slice; srow gets the local row of
 // each (slice, lane), 0xffff for the tail; slice_width the longest segment,
 // rounded up to even.
 // Placement order within a bin does not matter: each row is summed by one
 // lane in its CSR order wherever it lands.
-// Global row of local row i of CTA c: row_split[c] + i, or (interleaved,
-// grid G) c + G i.
-__device__ __forceinline__ int chunk_row(const int *row_split, int interleave_grid, int c, int i)
+// Rows of CTA c: row_split[c] + i for i < row_split[c+1] - row_split[c], or
+// (interleaved, grid G) c + G i for i < interleaved_rows(n, c, G).  Row
+// panel k of `panels` takes the local rows [panel_begin(rows, k), panel_begin(
+// rows, k+1)); pc = c*panels + k names the panel, local row i of a panel is
+// i after its first.
+__device__ __forceinline__ int cta_rows(const int *row_split, int interleave_grid, int n, int c)
 {
-    return interleave_grid ? c + interleave_grid * i : row_split[c] + i;
+    return interleave_grid ? interleaved_rows(n, c, interleave_grid) : row_split[c + 1] - row_split[c];
+}
+__device__ __forceinline__ int panel_rows(const int *row_split, int interleave_grid, int n,
+                                          int panels, int pc)
+{
+    const int rows = cta_rows(row_split, interleave_grid, n, pc / panels), k = pc % panels;
+    return panel_begin(rows, k + 1, panels) - panel_begin(rows, k, panels);
+}
+__device__ __forceinline__ int chunk_row(const int *row_split, int interleave_grid, int n, int panels,
+                                         int pc, int i)
+{
+    const int c = pc / panels;
+    const int li = panel_begin(cta_rows(row_split, interleave_grid, n, c), pc % panels, panels) + i;
+    return interleave_grid ? c + interleave_grid * li : row_split[c] + li;
 }
 
 static __global__ void slice_sort_rows(const int *__restrict__ seg, int seg_stride, int nblk,
                                        const int *__restrict__ row_split, int interleave_grid,
-                                       int n, const int *__restrict__ chunk_slice,
+                                       int panels, int n, const int *__restrict__ chunk_slice,
                                        unsigned short *srow, int *slice_width)
 {
     __shared__ int hist[256];
-    const int c = blockIdx.x / nblk, b = blockIdx.x % nblk;
-    const int nrows = interleave_grid ? interleaved_rows(n, c, interleave_grid)
-                                      : row_split[c + 1] - row_split[c];
+    const int pc = blockIdx.x / nblk, b = blockIdx.x % nblk;
+    const int nrows = panel_rows(row_split, interleave_grid, n, panels, pc);
     const int s0 = chunk_slice[blockIdx.x], ns = chunk_slice[blockIdx.x + 1] - s0;
     const int *lo = seg + size_t(b) * seg_stride;
     const int *hi = seg + size_t(b + 1) * seg_stride;
-#define SEG_LEN(i) (hi[chunk_row(row_split, interleave_grid, c, (i))] - \
-                    lo[chunk_row(row_split, interleave_grid, c, (i))])
+#define SEG_LEN(i) (hi[chunk_row(row_split, interleave_grid, n, panels, pc, (i))] - \
+                    lo[chunk_row(row_split, interleave_grid, n, panels, pc, (i))])
     for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
     __syncthreads();
     for (int i = threadIdx.x; i < nrows; i += blockDim.x)
@@ -1024,8 +1067,8 @@ static __global__ void slice_offsets(const int *__restrict__ width, int total, u
 // 16-bit local columns; padding steps get value 0, column 0.
 template <typename ST>
 __global__ void slice_fill(const int *__restrict__ seg, int seg_stride, int nblk, int width,
-                           const int *__restrict__ row_split, int interleave_grid,
-                           const int *__restrict__ chunk_slice,
+                           const int *__restrict__ row_split, int interleave_grid, int panels,
+                           int n, const int *__restrict__ chunk_slice,
                            int nchunks, const int *__restrict__ colidx, const ST *__restrict__ a,
                            const unsigned short *__restrict__ srow,
                            const int *__restrict__ slice_width,
@@ -1041,11 +1084,11 @@ __global__ void slice_fill(const int *__restrict__ seg, int seg_stride, int nblk
             if (chunk_slice[mid] <= s) lo = mid;
             else hi = mid;
         }
-        const int c = lo / nblk, b = lo % nblk;
+        const int pc = lo / nblk, b = lo % nblk;
         const unsigned short row = srow[size_t(s) * 32 + lane];
         int e0 = 0, e1 = 0;
         if (row != 0xffffu) {
-            const int j = chunk_row(row_split, interleave_grid, c, row);
+            const int j = chunk_row(row_split, interleave_grid, n, panels, pc, row);
             e0 = seg[size_t(b) * seg_stride + j];
             e1 = seg[size_t(b + 1) * seg_stride + j];
         }

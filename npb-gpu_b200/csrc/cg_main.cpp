@@ -7,6 +7,7 @@
 //            --weights FILE (learned mode: network weights, raw FP32; default
 //            the trained weights shipped beside the package, npbcg/lp_weights.f32)
 //            --device D  --json (one JSON result line instead of the report)
+//            --spmv row|sliced (SpMV plan; default: the autotuner's choice)
 //            --gpu-makea (generate the matrix with cgb_makea_device)
 //
 // Like the reference it generates the matrix (makea), runs the timed inverse
@@ -56,7 +57,8 @@ void usage()
     std::fprintf(stderr,
                  "usage: cg S|W|A|B|C|D | cg U --n N --nonzer K --niter I --shift S [--seed X]\n"
                  "          [--mode fp64|tol|mixed|learned] [--tol T] [--cgitmax M]\n"
-                 "          [--weights FILE] [--device D] [--json] [--gpu-makea]\n");
+                 "          [--weights FILE] [--device D] [--json] [--gpu-makea]\n"
+                 "          [--spmv row|sliced]\n");
 }
 
 // The weights shipped with the package: <dir of this binary>/../npbcg/lp_weights.f32.
@@ -124,7 +126,7 @@ int main(int argc, char **argv)
     }
     double seed = 314159265.0, tol = 1e-12;
     std::string weights;
-    int mode = CGB_MODE_FP64, cgitmax = 25, device = 0, json = 0, gpu_makea = 0;
+    int mode = CGB_MODE_FP64, cgitmax = 25, device = 0, json = 0, gpu_makea = 0, spmv = 0;
     for (int i = 2; i < argc; i++) {
         const std::string a = argv[i];
         auto next = [&](void) -> const char * {
@@ -144,6 +146,15 @@ int main(int argc, char **argv)
         else if (a == "--device") device = std::atoi(next());
         else if (a == "--json") json = 1;
         else if (a == "--gpu-makea") gpu_makea = 1;
+        else if (a == "--spmv") {
+            const std::string k = next();
+            if (k == "row") spmv = 1;
+            else if (k == "sliced") spmv = 2;
+            else {
+                usage();
+                return 2;
+            }
+        }
         else if (a == "--weights") weights = next();
         else if (a == "--mode") {
             const std::string m = next();
@@ -180,6 +191,7 @@ int main(int argc, char **argv)
     cgb_options opt;
     cgb_default_options(&opt);
     opt.device = device;
+    opt.spmv_kernel = spmv;
     cgb_session *s = nullptr;
     st = cgb_create(P.n, rowstr.data(), colidx.data(), a.data(), &opt, &s);
     if (st) return fail(st, "create");
@@ -205,6 +217,13 @@ int main(int argc, char **argv)
     std::vector<int> iters(P.niter);
     st = cgb_power_iterate(s, &sp, zeta.data(), rnorm.data(), iters.data(), nullptr, &res);
     if (st) return fail(st, "power_iterate");
+    // the plan the autotuner chose: row (1) or sliced (2, 3 with the L2
+    // prefetch), and the sliced walk's row panels
+    int kind = 0, lpr = 0, grid = 0, block = 0, panels = 0, prec_panels = 0;
+    long long smem = 0, entries = 0;
+    if (cgb_plan_info(s, &kind, &lpr, &grid, &block, &smem, &entries) ||
+        cgb_plan_panels(s, &panels, &prec_panels))
+        kind = panels = 0;
     cgb_destroy(s);
 
     const double t = res.device_ms / 1e3;
@@ -218,9 +237,10 @@ int main(int argc, char **argv)
         std::printf("{\"class\": \"%c\", \"n\": %d, \"nonzer\": %d, \"niter\": %d, \"shift\": %.17g, "
                     "\"nnz\": %lld, \"mode\": %d, \"zeta\": %.17g, \"rnorm\": %.17g, "
                     "\"seconds\": %.9g, \"mops\": %.6g, \"inner_total\": %d, \"verified\": %s, "
-                    "\"rel_err\": %.6g}\n",
+                    "\"rel_err\": %.6g, \"plan_kind\": %d, \"panels\": %d}\n",
                     P.name, P.n, P.nonzer, P.niter, P.shift, nnz, mode, res.zeta, res.rnorm, t,
-                    mops, res.total_inner, verify ? (ok ? "true" : "false") : "null", err);
+                    mops, res.total_inner, verify ? (ok ? "true" : "false") : "null", err, kind,
+                    panels);
         return verify && !ok ? 1 : 0;
     }
     std::printf("\n\n NAS Parallel Benchmarks 4.1 - CG Benchmark (B200 sm_100a build)\n\n");

@@ -271,6 +271,7 @@ struct cgb_session {
     int sliced_grid = 0;   // grid the layout was built for (0: none)
     int sliced_max_rows = 0;
     int sliced_nacc = 2;           // row accumulators (4 when they fit: FP32 pipeline depth)
+    int prec_panels = 1;           // row panels of the factor copies' interleaved rows
     int *d_chunk_slice = nullptr;  // shared by A, F and F^T (same row split)
     size_t cap_chunk = 0, cap_seg = 0;  // allocated elements of d_chunk_slice, d_seg
     cgb::SliceSet sa;              // A: FP64 values (+ FP32 copy)
@@ -421,6 +422,7 @@ void set_slices(cgb_session *s, const SliceSet &t, MatrixView *M)
     M->max_rows = s->sliced_max_rows;
     M->nacc = s->sliced_nacc;
     M->interleaved = t.interleaved;
+    M->panels = t.panels;
     M->slice_entries = t.entries + kPad;
     M->ncols = s->n;
 }
@@ -534,18 +536,22 @@ int build_segments_table(cgb_session *s)
 // Chunk table of a sliced copy: first slice of each (CTA c, block b), 32
 // rows a slice; rows per CTA from `rows_of(c)`.  Returns the slice count.
 template <typename RowsOf>
-int chunk_table(int grid, int nblk, RowsOf rows_of, std::vector<int> &chunk_slice)
+int chunk_table(int grid, int panels, int nblk, RowsOf rows_of, std::vector<int> &chunk_slice)
 {
-    chunk_slice.assign(size_t(grid) * nblk + 1, 0);
+    const size_t chunks = size_t(grid) * panels * nblk;
+    chunk_slice.assign(chunks + 1, 0);
     int total = 0;
     for (int c = 0; c < grid; c++) {
         const int rows = rows_of(c);
-        for (int b = 0; b < nblk; b++) {
-            chunk_slice[size_t(c) * nblk + b] = total;
-            total += (rows + 31) / 32;
+        for (int k = 0; k < panels; k++) {
+            const int prow = panel_begin(rows, k + 1, panels) - panel_begin(rows, k, panels);
+            for (int b = 0; b < nblk; b++) {
+                chunk_slice[(size_t(c) * panels + k) * nblk + b] = total;
+                total += (prow + 31) / 32;
+            }
         }
     }
-    chunk_slice[size_t(grid) * nblk] = total;
+    chunk_slice[chunks] = total;
     return total;
 }
 
@@ -559,7 +565,7 @@ int fill_set(cgb_session *s, int grid, bool interleave, const int *seg, const in
 {
     const int nblk = t->blocks ? t->blocks : s->nblk;
     const int bcols = t->block_cols ? t->block_cols : kSliceWidth;
-    const int nchunks = grid * nblk;
+    const int nchunks = grid * t->panels * nblk;
     const int ig = interleave ? grid : 0;
     t->interleaved = interleave ? 1 : 0;
     if (dev_reserve(&t->srow, &t->cap_srow, size_t(total) * 32) ||
@@ -567,7 +573,8 @@ int fill_set(cgb_session *s, int grid, bool interleave, const int *seg, const in
         dev_reserve(&t->off, &t->cap_off, size_t(total) + 1))
         return set_error(CGB_ERR_NOMEM, "sliced layout: metadata allocation failed");
     slice_sort_rows<<<nchunks, 256, 0, s->stream>>>(seg, s->seg_stride, nblk, s->d_split, ig,
-                                                   s->n, t->chunk_slice, t->srow, t->width);
+                                                   t->panels, s->n, t->chunk_slice, t->srow,
+                                                   t->width);
     CUDA_TRY(cudaGetLastError());
     slice_offsets<<<1, 1024, 0, s->stream>>>(t->width, total, t->off);
     CUDA_TRY(cudaGetLastError());
@@ -582,7 +589,7 @@ int fill_set(cgb_session *s, int grid, bool interleave, const int *seg, const in
         (want16 && dev_reserve(&t->sval16, &t->cap_sval16, size_t(entries) + kPad)))
         return set_error(CGB_ERR_NOMEM, "sliced layout: %u entries do not fit", entries);
     slice_fill<ST><<<4 * s->prop.multiProcessorCount, 256, 0, s->stream>>>(
-        seg, s->seg_stride, nblk, bcols, s->d_split, ig, t->chunk_slice, nchunks,
+        seg, s->seg_stride, nblk, bcols, s->d_split, ig, t->panels, s->n, t->chunk_slice, nchunks,
         d_colidx, vals, t->srow, t->width, t->off, total, t->sval, t->sval32, t->sval16, t->scol);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(s->stream));
@@ -595,29 +602,42 @@ int build_sliced(cgb_session *s, int grid)
     invalidate_sliced(s);
     std::vector<int> split;
     make_split(s->n, s->h_rowstr_copy.data(), grid, split);
-    std::vector<int> chunk_slice;
-    const int total = chunk_table(grid, s->nblk, [&](int c) { return split[c + 1] - split[c]; },
-                                  chunk_slice);
-    // accumulators: the largest row range, or the interleaved share of the
-    // preconditioner's copies
-    int max_rows = interleaved_rows(s->n, 0, grid);
-    for (int c = 0; c < grid; c++) max_rows = std::max(max_rows, split[c + 1] - split[c]);
-    s->sliced_max_rows = (max_rows + 31) & ~31;
     // dynamic shared memory must fit beside the kernels' static arrays
     size_t static_smem = 0;
     for (const void *k : {(const void *)outer_step_fp64_sliced, (const void *)outer_step_mixed_sliced,
                           (const void *)outer_step_pcg_sliced, (const void *)spmv_dot_sliced,
                           (const void *)spmv_dot_sliced32, (const void *)outer_step_fp64_sliced_pf,
                           (const void *)outer_step_mixed_sliced_pf, (const void *)spmv_dot_sliced_pf,
-                          (const void *)spmv_dot_sliced32_pf}) {
+                          (const void *)spmv_dot_sliced32_pf, (const void *)outer_step_fp64_sliced_pn,
+                          (const void *)outer_step_mixed_sliced_pn, (const void *)outer_step_pcg_sliced_pn,
+                          (const void *)spmv_dot_sliced_pn, (const void *)spmv_dot_sliced32_pn}) {
         cudaFuncAttributes fa;
         CUDA_TRY(cudaFuncGetAttributes(&fa, k));
         static_smem = std::max(static_smem, size_t(fa.sharedSizeBytes));
     }
     const size_t room = kSmemLimit - std::min(kSmemLimit, static_smem);
+    // rows two accumulators can hold beside the staging (a multiple of 32,
+    // below the 16-bit local-row marker)
+    const size_t fixed = sliced_smem_bytes(0, 2);
+    int cap = room > fixed ? int(std::min<size_t>((room - fixed) / (2 * sizeof(double)), 0xffe0) & ~size_t(31))
+                           : 0;
+    if (cap < 32) return set_error(CGB_ERR_STATE, "sliced layout: no shared memory for accumulators");
+    if (s->opts.panel_rows > 0) cap = std::min(cap, std::max(32, s->opts.panel_rows & ~31));
+    // accumulators: the largest row range, or the interleaved share of the
+    // preconditioner's copies; a CTA whose rows exceed them walks its rows
+    // in row panels (every column block once per panel)
+    int rows_a = 0;
+    for (int c = 0; c < grid; c++) rows_a = std::max(rows_a, split[c + 1] - split[c]);
+    const int rows_f = interleaved_rows(s->n, 0, grid);
+    const int pa = std::max(1, (rows_a + cap - 1) / cap), pf = std::max(1, (rows_f + cap - 1) / cap);
+    const int max_rows = std::max((rows_a + pa - 1) / pa, (rows_f + pf - 1) / pf);
+    s->sliced_max_rows = (max_rows + 31) & ~31;
     s->sliced_nacc = sliced_smem_bytes(s->sliced_max_rows, kMaxSlots) <= room ? kMaxSlots : 2;
-    if (s->sliced_max_rows >= 0xffff || sliced_smem_bytes(s->sliced_max_rows, 2) > room)
-        return set_error(CGB_ERR_STATE, "sliced layout: %d rows per CTA exceed shared memory", max_rows);
+    s->prec_panels = pf;
+    s->sa.panels = pa;
+    std::vector<int> chunk_slice;
+    const int total = chunk_table(grid, pa, s->nblk, [&](int c) { return split[c + 1] - split[c]; },
+                                  chunk_slice);
     if (dev_reserve(&s->d_chunk_slice, &s->cap_chunk, chunk_slice.size()))
         return set_error(CGB_ERR_NOMEM, "sliced layout: metadata allocation failed");
     CUDA_TRY(cudaMemcpyAsync(s->d_split, split.data(), sizeof(int) * (grid + 1), cudaMemcpyHostToDevice,
@@ -652,7 +672,8 @@ int ensure_prec_slices(cgb_session *s)
     // row, so fewer, fuller blocks keep the per-block latency down
     const int bcols = kFactorBlockCols, blocks = (n + bcols - 1) / bcols;
     std::vector<int> chunk_slice;
-    const int total = chunk_table(grid, blocks, [&](int c) { return interleaved_rows(n, c, grid); },
+    const int panels = s->prec_panels;
+    const int total = chunk_table(grid, panels, blocks, [&](int c) { return interleaved_rows(n, c, grid); },
                                   chunk_slice);
     const size_t count = size_t(blocks + 1) * s->seg_stride;
     int *seg = nullptr;
@@ -666,6 +687,7 @@ int ensure_prec_slices(cgb_session *s)
     for (int m = 0; m < 2 && st == CGB_OK; m++) {
         sets[m]->block_cols = bcols;
         sets[m]->blocks = blocks;
+        sets[m]->panels = panels;
         cudaError_t e = dev_alloc(&sets[m]->chunk_slice, chunk_slice.size());
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(sets[m]->chunk_slice, chunk_slice.data(), sizeof(int) * chunk_slice.size(),
@@ -716,16 +738,21 @@ bool make_plan(cgb_session *s, int kind, int lpr, Plan *pl, int prefetch = 0)
         // 32-bit slice offsets: keep the padded copy well below 2^32 entries
         if (!s->sorted || s->d_seg == nullptr || s->n < 2 * kSliceWidth || s->nnz > (1LL << 30))
             return false;
-        P.fp64 = prefetch ? outer_step_fp64_sliced_pf : outer_step_fp64_sliced;
-        P.mixed = prefetch ? outer_step_mixed_sliced_pf : outer_step_mixed_sliced;
-        P.pcg = outer_step_pcg_sliced;
-        P.spmv = prefetch ? spmv_dot_sliced_pf : spmv_dot_sliced;
-        P.spmv32 = prefetch ? spmv_dot_sliced32_pf : spmv_dot_sliced32;
+        const int grid = std::min(s->prop.multiProcessorCount, s->n);
+        if (s->sliced_grid != grid && build_sliced(s, grid) != CGB_OK) return false;
+        // more rows a CTA than the accumulators hold: the row-panel
+        // instances (which have no L2-prefetch form)
+        const bool pa = s->sa.panels > 1, pp = pa || s->prec_panels > 1;
+        if (pa && prefetch) return false;
+        P.fp64 = pa ? outer_step_fp64_sliced_pn : prefetch ? outer_step_fp64_sliced_pf : outer_step_fp64_sliced;
+        P.mixed = pa ? outer_step_mixed_sliced_pn
+                     : prefetch ? outer_step_mixed_sliced_pf : outer_step_mixed_sliced;
+        P.pcg = pp ? outer_step_pcg_sliced_pn : outer_step_pcg_sliced;
+        P.spmv = pa ? spmv_dot_sliced_pn : prefetch ? spmv_dot_sliced_pf : spmv_dot_sliced;
+        P.spmv32 = pa ? spmv_dot_sliced32_pn : prefetch ? spmv_dot_sliced32_pf : spmv_dot_sliced32;
         P.block = kSlicedBlock;
         P.block_mixed = kSlicedMixedBlock;
         P.block_pcg = kSlicedPcgBlock;
-        const int grid = std::min(s->prop.multiProcessorCount, s->n);
-        if (s->sliced_grid != grid && build_sliced(s, grid) != CGB_OK) return false;
         P.smem = sliced_smem_bytes(s->sliced_max_rows, s->sliced_nacc);
         for (OuterKernel k : {P.fp64, P.mixed, P.pcg})
             if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)))
@@ -1144,6 +1171,7 @@ void cgb_default_options(cgb_options *o)
     o->use_graph = 1;
     o->keep_fp32_copy = 1;
     o->spmv_kernel = 0;
+    o->panel_rows = 0;
 }
 
 void cgb_default_solve_params(cgb_solve_params *p)
@@ -1574,6 +1602,15 @@ int cgb_plan_l2_keep(cgb_session *s, double *bytes)
 {
     if (!s || !bytes) return set_error(CGB_ERR_INVALID, "bad arguments");
     *bytes = s->plan.kind == kKindSliced ? s->plan.l2_keep : 0.0;
+    return CGB_OK;
+}
+
+int cgb_plan_panels(cgb_session *s, int *panels, int *prec_panels)
+{
+    if (!s || !panels || !prec_panels) return set_error(CGB_ERR_INVALID, "bad arguments");
+    const bool sliced = s->plan.kind == kKindSliced;
+    *panels = sliced ? s->sa.panels : 0;
+    *prec_panels = sliced ? s->prec_panels : 0;
     return CGB_OK;
 }
 

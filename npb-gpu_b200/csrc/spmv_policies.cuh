@@ -12,8 +12,8 @@
 //                  masked to the row; single loads for a last entry that
 //                  ends the arrays), four chunks in flight; the gathered
 //                  vector is read through L1/L2.
-//   SlicedSpmv     a sliced copy of the matrix built on the device (see
-//                  slices.cuh): per CTA and per column block of W columns,
+//   SlicedSpmv     a sliced copy of the matrix built on the device (built by
+//                  cg_kernels.cuh): per CTA and per column block of W columns,
 //                  the CTA's rows sorted by length and packed 32 to a slice,
 //                  stored column-major by step pairs (entry k of the slice's
 //                  lane i at offset + 64 (k/2) + 2 i + k%2, widths rounded up
@@ -136,6 +136,7 @@ struct SliceSet {
     unsigned short *scol = nullptr;   // local columns
     int *chunk_slice = nullptr;       // own chunk table (null: the session's)
     int interleaved = 0;              // rows owned round-robin by the CTAs
+    int panels = 1;                   // pieces a CTA's rows are walked in
     int block_cols = 0, blocks = 0;   // columns per block, blocks (0: the session's)
     long long entries = 0;            // padded entries
     // allocated capacities (elements): a rebuild reuses buffers that fit
@@ -157,13 +158,17 @@ struct MatrixView {
     const unsigned short *__restrict__ srow;  // local row per (slice, lane); 0xffff = none
     const unsigned *__restrict__ slice_off;   // first entry of each slice
     const int *__restrict__ slice_width;      // steps of each slice
-    const int *__restrict__ chunk_slice;      // (c*nblk + b) -> first slice
+    const int *__restrict__ chunk_slice;      // ((c*panels + k)*nblk + b) -> first slice
     int nblk;                                 // column blocks
     int width;                                // columns per block
     int max_rows;                             // shared accumulator capacity
     int interleaved;                          // 0: CTA c owns its contiguous row range;
                                               // 1: CTA c owns rows c, c + G, c + 2G, ...
     int nacc;                                 // accumulators in shared memory (2 or 4)
+    int panels;                               // a CTA's rows are walked in this many
+                                              // consecutive pieces (row panels), each
+                                              // over every column block: 1 unless the
+                                              // rows exceed the accumulators
     // bounds of the checked build: CSR entries and sliced entries (each with
     // the padding after them), columns of the gathered vector
     long long csr_entries, slice_entries;
@@ -179,6 +184,12 @@ struct MatrixView {
 __host__ __device__ inline int interleaved_rows(int n, int c, int grid)
 {
     return c < n ? (n - c + grid - 1) / grid : 0;
+}
+
+// First of a CTA's `rows` rows (local index) in row panel k of `panels`.
+__host__ __device__ inline int panel_begin(int rows, int k, int panels)
+{
+    return int((long long)rows * k / panels);
 }
 
 template <typename VT>
@@ -382,7 +393,10 @@ __device__ __forceinline__ void prefetch_slice_l2(const ST *vals, const unsigned
 // With an FP32 vector a warp reads its first slice's metadata of a block
 // before waiting for the block's copy, and the next slice's metadata while
 // it works on the current one.
-template <int kU64, int kU32, bool kOutline = false, bool kL2Prefetch = true>
+// kPanels: walk the CTA's rows in M.panels row panels (instances for
+// matrices whose rows per CTA exceed the accumulators); without it one walk
+// over the CTA's rows, and the per-panel bookkeeping compiles away.
+template <int kU64, int kU32, bool kOutline = false, bool kL2Prefetch = true, bool kPanels = false>
 struct SlicedSpmvT {
     static constexpr bool kSliced = true;
     // Dynamic shared memory: the control words first (fixed offsets), then
@@ -463,156 +477,165 @@ struct SlicedSpmvT {
         // at most one accumulator each
         const int S = min(M.nacc, int(kStagingBytes / (size_t(M.width) * sizeof(VT))));
         const size_t slot_bytes = size_t(M.width) * sizeof(VT);
-        const int chunk0 = blockIdx.x * M.nblk;
         const int lane = threadIdx.x & 31;
         const int warp = threadIdx.x >> 5;
         const int nwarps = blockDim.x >> 5;
         // output rows: the CTA's range, or (interleaved copy) every grid-th row
-        const int base = M.interleaved ? int(blockIdx.x) : row0;
-        const int stride = M.interleaved ? int(gridDim.x) : 1;
-        const int nrows = M.interleaved ? interleaved_rows(n, blockIdx.x, gridDim.x) : row1 - row0;
         double *const acc = SlicedSpmvT::acc();
         uint64_t *const bars = SlicedSpmvT::bars();
         int *const cnt = SlicedSpmvT::cnt();
         int *const abort = abort_flag();
-        for (int i = threadIdx.x; i < S * M.max_rows; i += blockDim.x) acc[i] = 0.0;
-        if (threadIdx.x == 0) {
-            fence_proxy_async();  // v was written by generic stores before the grid barrier
-            for (int b = 0; b < S && b < M.nblk; b++) issue(M, v, n, b, b);
-        }
-        // this warp's slices of block b toward L2 (one block ahead of use)
-        // (only in the kL2Prefetch instances: it pays where the walk is
-        // latency-bound -- short column-block chunks -- and costs where it
-        // streams, so the plan's autotuner picks the instance)
-        auto prefetch_block = [&](int b) {
-            if (!kL2Prefetch || b >= M.nblk) return;
-            const int t0 = __ldg(M.chunk_slice + chunk0 + b);
-            const int t1 = __ldg(M.chunk_slice + chunk0 + b + 1);
-            for (int t = t0 + (warp + (b * 7) % nwarps) % nwarps; t < t1; t += nwarps)
-                prefetch_slice_l2(vals, M.scol, __ldg(M.slice_off + t), __ldg(M.slice_width + t) >> 1,
-                                  lane);
-        };
-        prefetch_block(0);
-        __syncthreads();
-        bool failed = false;
-        for (int b = 0; b < M.nblk && !failed; b++) {
-            const int slot = b % S;
-            const int s0 = __ldg(M.chunk_slice + chunk0 + b);  // this matrix's blocks
-            const int s1 = __ldg(M.chunk_slice + chunk0 + b + 1);
-            prefetch_block(b + 1);
-            // rotate the warp -> slice assignment from block to block so the
-            // widest slices do not always land on the same warps
-            const int rot = (b * 7) % nwarps;
-            // one slice: lane `lane` of slice entries at off, wp step pairs
-            auto run_slice = [&](unsigned off, int wp, unsigned short row, const VT *pv,
-                                 double *accb) {
-                VT sum = VT(0);
-                for (int m = 0; m < wp; m += kU) {
-                    P2 av[kU];
-                    ushort2 cv[kU];
-#pragma unroll
-                    for (int u = 0; u < kU; u++) {
-                        if (m + u < wp) {
-                            const unsigned e = off + 64u * unsigned(m + u);
-                            if (CGB_IN_RANGE(e + 1, M.slice_entries, kCheckStream)) {
-                                av[u] = ld_stream(reinterpret_cast<const P2 *>(vals + e), pol);
-                                cv[u] = ld_stream(reinterpret_cast<const ushort2 *>(M.scol + e), pol);
-                            } else {
-                                av[u].x = av[u].y = ST(0.f);
-                                cv[u] = make_ushort2(0, 0);
+        double dacc = 0.0;
+        // row panel pk: local rows [i0, i0 + nrows) of the CTA, a walk over
+        // every column block of its own chunks (one panel unless the CTA's
+        // rows exceed the accumulators)
+        const int panels = kPanels ? M.panels : 1;
+        for (int pk = 0; pk < panels; pk++) {
+            const int chunk0 = (int(blockIdx.x) * panels + pk) * M.nblk;
+            if (pk > 0) __syncthreads();  // the previous panel's sums are read out
+            for (int i = threadIdx.x; i < S * M.max_rows; i += blockDim.x) acc[i] = 0.0;
+            if (threadIdx.x == 0) {
+                fence_proxy_async();  // v was written by generic stores before the grid barrier
+                for (int b = 0; b < S && b < M.nblk; b++) issue(M, v, n, b, b);
+            }
+            // this warp's slices of block b toward L2 (one block ahead of use)
+            // (only in the kL2Prefetch instances: it pays where the walk is
+            // latency-bound -- short column-block chunks -- and costs where it
+            // streams, so the plan's autotuner picks the instance)
+            auto prefetch_block = [&](int b) {
+                if (!kL2Prefetch || b >= M.nblk) return;
+                const int t0 = __ldg(M.chunk_slice + chunk0 + b);
+                const int t1 = __ldg(M.chunk_slice + chunk0 + b + 1);
+                for (int t = t0 + (warp + (b * 7) % nwarps) % nwarps; t < t1; t += nwarps)
+                    prefetch_slice_l2(vals, M.scol, __ldg(M.slice_off + t), __ldg(M.slice_width + t) >> 1,
+                                      lane);
+            };
+            prefetch_block(0);
+            __syncthreads();
+            bool failed = false;
+            for (int b = 0; b < M.nblk && !failed; b++) {
+                const int slot = b % S;
+                const int s0 = __ldg(M.chunk_slice + chunk0 + b);  // this matrix's blocks
+                const int s1 = __ldg(M.chunk_slice + chunk0 + b + 1);
+                prefetch_block(b + 1);
+                // rotate the warp -> slice assignment from block to block so the
+                // widest slices do not always land on the same warps
+                const int rot = (b * 7) % nwarps;
+                // one slice: lane `lane` of slice entries at off, wp step pairs
+                auto run_slice = [&](unsigned off, int wp, unsigned short row, const VT *pv,
+                                     double *accb) {
+                    VT sum = VT(0);
+                    for (int m = 0; m < wp; m += kU) {
+                        P2 av[kU];
+                        ushort2 cv[kU];
+    #pragma unroll
+                        for (int u = 0; u < kU; u++) {
+                            if (m + u < wp) {
+                                const unsigned e = off + 64u * unsigned(m + u);
+                                if (CGB_IN_RANGE(e + 1, M.slice_entries, kCheckStream)) {
+                                    av[u] = ld_stream(reinterpret_cast<const P2 *>(vals + e), pol);
+                                    cv[u] = ld_stream(reinterpret_cast<const ushort2 *>(M.scol + e), pol);
+                                } else {
+                                    av[u].x = av[u].y = ST(0.f);
+                                    cv[u] = make_ushort2(0, 0);
+                                }
+                            }
+                        }
+    #pragma unroll
+                        for (int u = 0; u < kU; u++) {
+                            if (m + u < wp) {
+                                if (CGB_IN_RANGE(cv[u].x, M.width, kCheckGather))
+                                    sum = fma_vt(VT(widen(av[u].x)), pv[cv[u].x], sum);
+                                if (CGB_IN_RANGE(cv[u].y, M.width, kCheckGather))
+                                    sum = fma_vt(VT(widen(av[u].y)), pv[cv[u].y], sum);
                             }
                         }
                     }
-#pragma unroll
-                    for (int u = 0; u < kU; u++) {
-                        if (m + u < wp) {
-                            if (CGB_IN_RANGE(cv[u].x, M.width, kCheckGather))
-                                sum = fma_vt(VT(widen(av[u].x)), pv[cv[u].x], sum);
-                            if (CGB_IN_RANGE(cv[u].y, M.width, kCheckGather))
-                                sum = fma_vt(VT(widen(av[u].y)), pv[cv[u].y], sum);
+                    if (row != 0xffffu && CGB_IN_RANGE(row, M.max_rows, kCheckRow)) accb[row] += double(sum);
+                };
+                const VT *pv = reinterpret_cast<const VT *>(buf() + size_t(slot) * slot_bytes);
+                double *accb = acc + size_t(slot) * M.max_rows;
+                if constexpr (sizeof(VT) == 8) {
+                    // FP64 vector: long slices, the plain walk measures fastest
+                    if (!mbar_wait(&bars[slot], (parity >> slot) & 1u, limit_ns, abort)) {
+                        failed = true;
+                        *abort = 1;
+                        break;
+                    }
+                    parity ^= 1u << slot;
+                    for (int s = s0 + (warp + rot) % nwarps; s < s1; s += nwarps)
+                        run_slice(__ldg(M.slice_off + s) + 2u * lane, __ldg(M.slice_width + s) >> 1,
+                                  __ldg(M.srow + size_t(s) * 32 + lane), pv, accb);
+                } else {
+                    // FP32 vector: the first slice's metadata before the wait,
+                    // the next slice's while the current one streams
+                    int s = s0 + (warp + rot) % nwarps;
+                    unsigned off = 0;
+                    int wp = 0;
+                    unsigned short row = 0xffffu;
+                    if (s < s1) {
+                        off = __ldg(M.slice_off + s) + 2u * lane;
+                        wp = __ldg(M.slice_width + s) >> 1;
+                        row = __ldg(M.srow + size_t(s) * 32 + lane);
+                    }
+                    if (!mbar_wait(&bars[slot], (parity >> slot) & 1u, limit_ns, abort)) {
+                        failed = true;
+                        *abort = 1;
+                        break;
+                    }
+                    parity ^= 1u << slot;
+                    while (s < s1) {
+                        const int sn = s + nwarps;
+                        unsigned offn = 0;
+                        int wpn = 0;
+                        unsigned short rown = 0xffffu;
+                        if (sn < s1) {
+                            offn = __ldg(M.slice_off + sn) + 2u * lane;
+                            wpn = __ldg(M.slice_width + sn) >> 1;
+                            rown = __ldg(M.srow + size_t(sn) * 32 + lane);
+                        }
+                        run_slice(off, wp, row, pv, accb);
+                        s = sn;
+                        off = offn;
+                        wp = wpn;
+                        row = rown;
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    __threadfence_block();
+                    if (atomicAdd(&cnt[slot], 1) == nwarps - 1) {
+                        cnt[slot] = 0;
+                        if (b + S < M.nblk) {
+                            fence_proxy_async();  // all warps' reads of the slot before the refill
+                            issue(M, v, n, b + S, slot);
                         }
                     }
                 }
-                if (row != 0xffffu && CGB_IN_RANGE(row, M.max_rows, kCheckRow)) accb[row] += double(sum);
-            };
-            const VT *pv = reinterpret_cast<const VT *>(buf() + size_t(slot) * slot_bytes);
-            double *accb = acc + size_t(slot) * M.max_rows;
-            if constexpr (sizeof(VT) == 8) {
-                // FP64 vector: long slices, the plain walk measures fastest
-                if (!mbar_wait(&bars[slot], (parity >> slot) & 1u, limit_ns, abort)) {
-                    failed = true;
-                    *abort = 1;
-                    break;
-                }
-                parity ^= 1u << slot;
-                for (int s = s0 + (warp + rot) % nwarps; s < s1; s += nwarps)
-                    run_slice(__ldg(M.slice_off + s) + 2u * lane, __ldg(M.slice_width + s) >> 1,
-                              __ldg(M.srow + size_t(s) * 32 + lane), pv, accb);
-            } else {
-                // FP32 vector: the first slice's metadata before the wait,
-                // the next slice's while the current one streams
-                int s = s0 + (warp + rot) % nwarps;
-                unsigned off = 0;
-                int wp = 0;
-                unsigned short row = 0xffffu;
-                if (s < s1) {
-                    off = __ldg(M.slice_off + s) + 2u * lane;
-                    wp = __ldg(M.slice_width + s) >> 1;
-                    row = __ldg(M.srow + size_t(s) * 32 + lane);
-                }
-                if (!mbar_wait(&bars[slot], (parity >> slot) & 1u, limit_ns, abort)) {
-                    failed = true;
-                    *abort = 1;
-                    break;
-                }
-                parity ^= 1u << slot;
-                while (s < s1) {
-                    const int sn = s + nwarps;
-                    unsigned offn = 0;
-                    int wpn = 0;
-                    unsigned short rown = 0xffffu;
-                    if (sn < s1) {
-                        offn = __ldg(M.slice_off + sn) + 2u * lane;
-                        wpn = __ldg(M.slice_width + sn) >> 1;
-                        rown = __ldg(M.srow + size_t(sn) * 32 + lane);
-                    }
-                    run_slice(off, wp, row, pv, accb);
-                    s = sn;
-                    off = offn;
-                    wp = wpn;
-                    row = rown;
-                }
             }
-            __syncwarp();
-            if (lane == 0) {
-                __threadfence_block();
-                if (atomicAdd(&cnt[slot], 1) == nwarps - 1) {
-                    cnt[slot] = 0;
-                    if (b + S < M.nblk) {
-                        fence_proxy_async();  // all warps' reads of the slot before the refill
-                        issue(M, v, n, b + S, slot);
-                    }
+            if (__syncthreads_or(failed)) {
+                ok = false;
+                if (threadIdx.x == 0) {
+                    raise_status(status, kDevTimeout);
+                    // let issued copies land before the CTA leaves (a completed
+                    // phase returns at once)
+                    for (int i = 0; i < S; i++) (void)mbar_wait(&bars[i], (parity >> i) & 1u, limit_ns, nullptr);
                 }
+                __syncthreads();
+                return 0.0;
             }
-        }
-        if (__syncthreads_or(failed)) {
-            ok = false;
-            if (threadIdx.x == 0) {
-                raise_status(status, kDevTimeout);
-                // let issued copies land before the CTA leaves (a completed
-                // phase returns at once)
-                for (int i = 0; i < S; i++) (void)mbar_wait(&bars[i], (parity >> i) & 1u, limit_ns, nullptr);
+            const int own = M.interleaved ? interleaved_rows(n, blockIdx.x, gridDim.x) : row1 - row0;
+            const int stride = M.interleaved ? int(gridDim.x) : 1;
+            const int i0 = panel_begin(own, pk, panels);
+            const int nrows = panel_begin(own, pk + 1, panels) - i0;
+            const int base = (M.interleaved ? int(blockIdx.x) : row0) + i0 * stride;
+            for (int i = threadIdx.x; i < nrows; i += blockDim.x) {
+                double t = acc[i];
+                for (int k = 1; k < S; k++) t += acc[size_t(k) * M.max_rows + i];
+                const int row = base + i * stride;
+                out[row] = t;
+                if (dotv) dacc = fma(dotv[row], t, dacc);
             }
-            __syncthreads();
-            return 0.0;
-        }
-        double dacc = 0.0;
-        for (int i = threadIdx.x; i < nrows; i += blockDim.x) {
-            double t = acc[i];
-            for (int k = 1; k < S; k++) t += acc[size_t(k) * M.max_rows + i];
-            const int row = base + i * stride;
-            out[row] = t;
-            if (dotv) dacc = fma(dotv[row], t, dacc);
         }
         ok = true;
         return dacc;
@@ -627,5 +650,9 @@ using SlicedSpmvPf = SlicedSpmvT<6, 6, false, true>;
 using SlicedSpmvMixed = SlicedSpmvT<4, 6, false, false>;
 using SlicedSpmvMixedPf = SlicedSpmvT<4, 6, false, true>;
 using SlicedSpmvPcg = SlicedSpmvT<4, 6, false, false>;
+// row-panel instances (no L2 prefetch)
+using SlicedSpmvPanels = SlicedSpmvT<6, 6, false, false, true>;
+using SlicedSpmvMixedPanels = SlicedSpmvT<4, 6, false, false, true>;
+using SlicedSpmvPcgPanels = SlicedSpmvT<4, 6, false, false, true>;
 
 }  // namespace cgb

@@ -64,7 +64,7 @@ class Options(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("lanes_per_row", ctypes.c_int),
                 ("block_threads", ctypes.c_int), ("wait_limit_ns", ctypes.c_longlong),
                 ("use_graph", ctypes.c_int), ("keep_fp32_copy", ctypes.c_int),
-                ("spmv_kernel", ctypes.c_int)]
+                ("spmv_kernel", ctypes.c_int), ("panel_rows", ctypes.c_int)]
 
 
 class SolveParams(ctypes.Structure):
@@ -158,6 +158,8 @@ _SIGNATURES = {
                                       ctypes.POINTER(ctypes.c_int)] +
                        [ctypes.POINTER(ctypes.c_double)] * 4),
     "cgb_plan_l2_keep": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    "cgb_plan_panels": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int)]),
     "cgb_check_status": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
     "cgb_time_barrier": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                         ctypes.POINTER(ctypes.c_double)]),
@@ -360,9 +362,12 @@ class Session:
         kind, lpr, grid, block = (x.value for x in v)
         keep = ctypes.c_double()
         _check(lib().cgb_plan_l2_keep(self._h, ctypes.byref(keep)))
+        pa, pf = ctypes.c_int(), ctypes.c_int()
+        _check(lib().cgb_plan_panels(self._h, ctypes.byref(pa), ctypes.byref(pf)))
         return dict(kind={1: "row", 2: "sliced", 3: "sliced"}.get(kind, kind), l2_prefetch=kind == 3,
                     l2_keep_mb=keep.value / 1e6, lanes_per_row=lpr, grid=grid, block=block,
-                    smem=smem.value, layout_entries=entries.value)
+                    smem=smem.value, layout_entries=entries.value, panels=pa.value,
+                    prec_panels=pf.value)
 
     def set_l2_keep(self, nbytes):
         """Bytes of the sliced matrix stream kept in L2 across products

@@ -270,6 +270,56 @@ def test_l2_keep_changes_no_result(cgb, cls):
         assert np.array_equal(outs[0.0][k]["rnorm"], outs[96e6][k]["rnorm"])
 
 
+def test_row_panels_change_no_result(cgb):
+    """Row panels -- a CTA walking its rows in pieces, every column block
+    once per piece, as class D's 10 K rows a CTA need -- sum every row in
+    the same order as one walk; only the fused dot products (p.q, r.y) add
+    a CTA's rows in another order.  Forced at class B (panel_rows = 160),
+    the FP64, mixed and preconditioned zeta traces agree with the one-walk
+    layout's to 1e-12 (rounding; the parity bar is 1e-10), and so does the
+    z of one conj_grad."""
+    n, nonzer, niter, shift = PARAMS["B"]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    factor = cgb.jacobi_factor(rs, ci, a)
+    outs, zs = [], []
+    for rows in (0, 160):
+        with cgb.Session(rs, ci, a, spmv_kernel=2, panel_rows=rows) as s:
+            pl = s.plan()
+            assert pl["kind"] == "sliced"
+            if rows:
+                assert pl["panels"] >= 3 and pl["prec_panels"] >= 3, pl
+            else:
+                assert pl["panels"] == 1 and pl["prec_panels"] == 1, pl
+            zs.append(s.conj_grad(np.ones(n))[0][:n])
+            r = [s.power_iterate(4, shift),
+                 s.power_iterate(4, shift, mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=100)]
+            s.set_preconditioner(*factor)
+            r.append(s.power_iterate(4, shift, mode=cgb.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=100))
+            outs.append(r)
+    assert np.linalg.norm(zs[0] - zs[1]) <= 1e-12 * np.linalg.norm(zs[0])
+    for k in range(3):
+        z0, z1 = outs[0][k]["zeta"], outs[1][k]["zeta"]
+        assert np.max(np.abs(z0 - z1) / np.abs(z0)) <= 1e-12, k
+        assert np.all(outs[1][k]["rnorm"] <= 1e-10 * np.sqrt(n)), k  # 1e-10 ||x||, x = 1 first
+
+
+def test_class_d_sliced_row_panels(cgb):
+    """Class D (n = 1.5 M, 694 M entries; 10 K rows a CTA) on the sliced
+    plan walks row panels; its first outer steps agree with the row plan's
+    to 1e-12 (FP64, different summation order within rows)."""
+    n, nonzer, shift = 1500000, 21, 500.0
+    out = {}
+    for kind in (1, 2):
+        with cgb.Session.generated(n, nonzer, shift, spmv_kernel=kind) as s:
+            pl = s.plan()
+            assert pl["kind"] == ("row" if kind == 1 else "sliced")
+            if kind == 2:
+                assert pl["panels"] >= 4, pl
+            out[kind] = s.power_iterate(2, shift)
+    assert np.max(np.abs(out[1]["zeta"] - out[2]["zeta"]) / np.abs(out[1]["zeta"])) <= 1e-12
+    assert np.all(out[2]["rnorm"] < 1e-10)
+
+
 def test_sliced_refused_for_small_or_unsorted(cgb):
     n, nonzer, niter, shift = PARAMS["W"]
     rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
