@@ -637,6 +637,11 @@ struct SlicedSpmvT {
                 if (dotv) dacc = fma(dotv[row], t, dacc);
             }
         }
+        // with one panel, row i's sum is written by thread i % blockDim, the
+        // thread that reads it next in the callers' row loops; panels shift
+        // that mapping, so the CTA synchronizes before any of its threads
+        // reads an output row
+        if constexpr (kPanels) __syncthreads();
         ok = true;
         return dacc;
     }

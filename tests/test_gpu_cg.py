@@ -275,14 +275,17 @@ def test_row_panels_change_no_result(cgb):
     once per piece, as class D's 10 K rows a CTA need -- sum every row in
     the same order as one walk; only the fused dot products (p.q, r.y) add
     a CTA's rows in another order.  Forced at class B (panel_rows = 160),
-    the FP64, mixed and preconditioned zeta traces agree with the one-walk
-    layout's to 1e-12 (rounding; the parity bar is 1e-10), and so does the
-    z of one conj_grad."""
+    the z of one conj_grad and the FP64 zeta trace agree with the one-walk
+    layout's to 1e-12 (rounding).  The mixed and preconditioned solves stop
+    where the residual passes the tolerance, so rounding can move the stop
+    by an iteration: their zetas agree to the parity bar, 1e-10.  A second
+    session with panels repeats the first bit for bit (no race between a
+    panel's output rows and the threads that read them next)."""
     n, nonzer, niter, shift = PARAMS["B"]
     rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
     factor = cgb.jacobi_factor(rs, ci, a)
     outs, zs = [], []
-    for rows in (0, 160):
+    for rows in (0, 160, 160):
         with cgb.Session(rs, ci, a, spmv_kernel=2, panel_rows=rows) as s:
             pl = s.plan()
             assert pl["kind"] == "sliced"
@@ -298,8 +301,11 @@ def test_row_panels_change_no_result(cgb):
             outs.append(r)
     assert np.linalg.norm(zs[0] - zs[1]) <= 1e-12 * np.linalg.norm(zs[0])
     for k in range(3):
+        assert np.array_equal(outs[1][k]["zeta"], outs[2][k]["zeta"]), k
+        assert outs[1][k]["total_inner"] == outs[2][k]["total_inner"], k
+    for k, bound in enumerate((1e-12, 1e-10, 1e-10)):
         z0, z1 = outs[0][k]["zeta"], outs[1][k]["zeta"]
-        assert np.max(np.abs(z0 - z1) / np.abs(z0)) <= 1e-12, k
+        assert np.max(np.abs(z0 - z1) / np.abs(z0)) <= bound, k
         assert np.all(outs[1][k]["rnorm"] <= 1e-10 * np.sqrt(n)), k  # 1e-10 ||x||, x = 1 first
 
 
