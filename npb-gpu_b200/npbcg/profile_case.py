@@ -34,6 +34,8 @@ def main():
     ap.add_argument("--lanes", type=int, default=0)
     ap.add_argument("--kind", type=int, default=0, help="0 auto, 1 row, 2 sliced, 3 sliced with L2 prefetch")
     ap.add_argument("--fp32", action="store_true")
+    ap.add_argument("--panel-rows", type=int, default=0,
+                    help="sliced plan: most rows a CTA sums at a time (forces row panels)")
     ap.add_argument("--keep-mb", type=float, default=None,
                     help="bytes (MB) of the sliced stream kept in L2 (default: the autotuner's)")
     a = ap.parse_args()
@@ -74,7 +76,8 @@ def main():
             out["autotuned"] = s.plan()
         out["sweep"] = rows
     else:
-        with npbcg.Session(rs, ci, av, lanes_per_row=a.lanes, spmv_kernel=a.kind) as s:
+        with npbcg.Session(rs, ci, av, lanes_per_row=a.lanes, spmv_kernel=a.kind,
+                           panel_rows=a.panel_rows) as s:
             if a.keep_mb is not None:
                 s.set_l2_keep(a.keep_mb * 1e6)
             out["plan"] = s.plan()
