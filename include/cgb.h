@@ -130,6 +130,14 @@ int cgb_destroy(cgb_session *s);
 int cgb_conj_grad(cgb_session *s, const int *colidx, const int *rowstr, const double *x,
                   double *z, const double *a, double *p, double *q, double *r, double *rnorm);
 
+/* Tells the session that the caller changed, in place, the host arrays it was
+ * created or last uploaded with: the next cgb_conj_grad uploads them again
+ * even though the pointers are the same.  (The reference's CPU conj_grad
+ * reads a[] on every call, cg.cu:653-801; its GPU path copies the matrix once
+ * in setup_gpu, cg.cu:1390-1603.  cgb_conj_grad compares pointers only, so
+ * without this call an edit in place is not seen.)  No other effect. */
+int cgb_matrix_changed(cgb_session *s);
+
 /* ------------------------------------------------------- power iteration */
 #define CGB_MODE_FP64 0         /* reference algorithm: fixed cgitmax FP64 CG steps */
 #define CGB_MODE_FP64_TOL 1     /* FP64 CG stopped at relative residual tol */
@@ -337,12 +345,15 @@ int cgb_selftest_wait_timeout(cgb_session *s, long long limit_ns, int *device_st
  *   n+1 doubles (entry n as the reference sets it), d_rnorm one double,
  *   d_status (nullable) one int: 0, or the device status on a failed wait.
  *   stream: a cudaStream_t (NULL = legacy default stream).  Asynchronous:
- *   synchronise the stream before reading the outputs.
+ *   synchronise the stream before reading the outputs.  A solve that gave
+ *   up on a device wait leaves *d_rnorm NaN (and *d_status nonzero), so a
+ *   caller that passes no status word still sees the failure.
  * Limit: n <= 262144 (CGB_ERR_CAPACITY above).  The array (about 6.3 MB) is
  * held on every GPU that loads the library until exit.  Calls share it:
  * calls that overlap on the GPU race, so serialise them.  Runs on the
- * calling thread's current device; the first call on a device looks the
- * array up there, so make that first call before any stream capture. */
+ * calling thread's current device; the first call on a device (per CUDA
+ * context: again after a cudaDeviceReset) looks the array up there and
+ * caches its address, so make that first call before any stream capture. */
 int cgb_conj_grad_noalloc(int n, long long nnz, const int *d_rowstr, const int *d_colidx,
                           const double *d_a, const double *d_x, double *d_z, double *d_rnorm,
                           int *d_status, void *stream);

@@ -19,9 +19,14 @@
 //     behind; the call clears the words that must start at zero.  Calls that
 //     overlap on the GPU (two streams, or two host threads) race on the
 //     array: serialise them.
-//   * The first call on a device looks the array's device address up
-//     (cudaGetSymbolAddress) with that device current; make that first call
+//   * The first call on a device (per CUDA context) looks the array's device
+//     address up (cudaGetSymbolAddress) with that device current, and caches
+//     it with the SM count and the kernels' occupancy; make that first call
 //     before any stream capture.
+//   * The call is asynchronous: *d_rnorm and *d_status are written on the
+//     stream; synchronise it before reading them.  A solve that gave up on a
+//     wait leaves *d_rnorm NaN and *d_status nonzero.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -51,24 +56,117 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 namespace {
 
-std::mutex g_scratch_mu;
-void *g_scratch_addr[64];
+// What a call needs to know about the current device, looked up once per
+// CUDA context (set-up) and kept: the scratch array's device address, the
+// SM count and how many CTAs of each kernel instance fit on an SM.  The key
+// is the context's unique id (cuCtxGetId), so a context created after a
+// cudaDeviceReset -- where the library's module, and with it the array,
+// is loaded again and may move -- or a driver-API context of the caller's
+// gets its own set-up instead of a stale address.
+using RowKernel = void (*)(OuterArgs);
+constexpr int kNoallocInstances = 4;  // outer_step_fp64<16>, <8>, <4>, <2>
 
-// Device address of the scratch array on the current device (looked up once
-// per device, with that device current).
-int scratch_address(int device, unsigned char **out)
+RowKernel noalloc_instance(int i)
+{
+    switch (i) {
+    case 0: return outer_step_fp64<16>;
+    case 1: return outer_step_fp64<8>;
+    case 2: return outer_step_fp64<4>;
+    default: return outer_step_fp64<2>;
+    }
+}
+
+// lanes per row from the mean row length (instance index above)
+int noalloc_pick(double mean_len)
+{
+    if (mean_len >= 40.0) return 0;
+    if (mean_len >= 16.0) return 1;
+    if (mean_len >= 6.0) return 2;
+    return 3;
+}
+
+struct DeviceSetup {
+    bool valid = false;
+    unsigned long long ctx_id = 0;
+    unsigned char *scratch = nullptr;
+    int sm_count = 0;
+    int per_sm[kNoallocInstances] = {};
+};
+
+std::mutex g_setup_mu;
+DeviceSetup g_setup[64];
+
+// The calling thread's current context id (0 when no context is current or
+// the driver entry points are unavailable; the cache is then per device).
+unsigned long long current_ctx_id()
+{
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+    });
+    if (!get_current || !get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return 0;
+    if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Set-up of `device` (current on this thread) for the current context: the
+// scratch array's device address (cudaGetSymbolAddress, which also makes
+// the context current if none was), the compute capability check, the SM
+// count and the occupancy of each kernel instance.  Nothing here allocates.
+int device_setup(int device, DeviceSetup *out)
 {
     if (device < 0 || device >= 64) return set_error(CGB_ERR_NO_DEVICE, "device %d unsupported", device);
-    std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[device]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || p == nullptr)
-            return set_error(CGB_ERR_CUDA, "cudaGetSymbolAddress(scratch) failed: %s",
-                             cudaGetErrorString(e));
-        g_scratch_addr[device] = p;
+    std::lock_guard<std::mutex> lock(g_setup_mu);
+    DeviceSetup &d = g_setup[device];
+    const unsigned long long id = current_ctx_id();
+    if (d.valid && id == d.ctx_id && id != 0) {
+        *out = d;
+        return CGB_OK;
     }
-    *out = static_cast<unsigned char *>(g_scratch_addr[device]);
+    if (d.valid && id == 0 && d.ctx_id == 0) {  // no context ids: per device
+        *out = d;
+        return CGB_OK;
+    }
+    int major = 0, sms = 0;
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess ||
+        major != 10)
+        return set_error(CGB_ERR_NO_DEVICE, "current device is not sm_100");
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms < 1)
+        return set_error(CGB_ERR_NO_DEVICE, "SM count query failed");
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr)
+        return set_error(CGB_ERR_CUDA, "cudaGetSymbolAddress(scratch) failed: %s", cudaGetErrorString(e));
+    DeviceSetup fresh;
+    fresh.scratch = static_cast<unsigned char *>(p);
+    fresh.sm_count = sms;
+    for (int i = 0; i < kNoallocInstances; i++) {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, noalloc_instance(i), 512, 0) !=
+                cudaSuccess ||
+            per_sm < 1)
+            return set_error(CGB_ERR_CUDA, "noalloc conj_grad: kernel cannot be resident");
+        fresh.per_sm[i] = per_sm;
+    }
+    fresh.ctx_id = current_ctx_id();  // the context is current now
+    fresh.valid = true;
+    d = fresh;
+    *out = d;
     return CGB_OK;
 }
 
@@ -89,17 +187,6 @@ __global__ void noalloc_split(const int *__restrict__ rowstr, int n, int grid, i
         }
         split[c] = lo;
     }
-}
-
-using RowKernel = void (*)(OuterArgs);
-
-RowKernel noalloc_kernel(double mean_len)
-{
-    if (mean_len >= 96.0) return outer_step_fp64<16>;
-    if (mean_len >= 40.0) return outer_step_fp64<16>;
-    if (mean_len >= 16.0) return outer_step_fp64<8>;
-    if (mean_len >= 6.0) return outer_step_fp64<4>;
-    return outer_step_fp64<2>;
 }
 
 }  // namespace
@@ -124,20 +211,15 @@ extern "C" int cgb_conj_grad_noalloc(int n, long long nnz, const int *d_rowstr, 
     int device = -1;
     if (cudaGetDevice(&device) != cudaSuccess)
         return set_error(CGB_ERR_NO_DEVICE, "no current CUDA device");
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10)
-        return set_error(CGB_ERR_NO_DEVICE, "current device is not sm_100");
-    unsigned char *base = nullptr;
-    int st = scratch_address(device, &base);
+    DeviceSetup dev;
+    int st = device_setup(device, &dev);
     if (st) return st;
+    unsigned char *base = dev.scratch;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
 
-    RowKernel kernel = noalloc_kernel(double(nnz) / double(n));
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 512, 0) != cudaSuccess ||
-        per_sm < 1)
-        return set_error(CGB_ERR_CUDA, "noalloc conj_grad: kernel cannot be resident");
-    const int grid = std::max(1, std::min({per_sm * prop.multiProcessorCount, n, kNoallocMaxGrid}));
+    const int pick = noalloc_pick(double(nnz) / double(n));
+    RowKernel kernel = noalloc_instance(pick);
+    const int grid = std::max(1, std::min({dev.per_sm[pick] * dev.sm_count, n, kNoallocMaxGrid}));
 
     unsigned long long *arrivals = reinterpret_cast<unsigned long long *>(base);
     int *status = reinterpret_cast<int *>(base + 2 * kLine);
@@ -146,9 +228,12 @@ extern "C" int cgb_conj_grad_noalloc(int n, long long nnz, const int *d_rowstr, 
     double *part = reinterpret_cast<double *>(base + kHeaderBytes + kSplitBytes);
     double *vec = reinterpret_cast<double *>(base + kHeaderBytes + kSplitBytes + kPartBytes);
 
-    // barrier words, status and trace must start at zero; the rest is
-    // written before it is read
-    if (cudaMemsetAsync(base, 0, kHeaderBytes, s) != cudaSuccess)
+    // barrier words and status must start at zero.  The trace record starts
+    // as NaN bytes: a solve that leaves early (a failed wait) never writes
+    // it, so *d_rnorm then reads NaN rather than a stale or zero residual.
+    // Everything else is written before it is read.
+    if (cudaMemsetAsync(base, 0, 3 * kLine, s) != cudaSuccess ||
+        cudaMemsetAsync(base + 3 * kLine, 0xff, kLine, s) != cudaSuccess)
         return set_error(CGB_ERR_CUDA, "noalloc conj_grad: clearing the scratch header failed");
     noalloc_split<<<1, 256, 0, s>>>(d_rowstr, n, grid, split);
     if (cudaGetLastError() != cudaSuccess)

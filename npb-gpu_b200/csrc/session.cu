@@ -1404,6 +1404,16 @@ int cgb_conj_grad(cgb_session *s, const int *colidx, const int *rowstr, const do
     return CGB_OK;
 }
 
+int cgb_matrix_changed(cgb_session *s)
+{
+    if (!s) return set_error(CGB_ERR_INVALID, "session is null");
+    // no host array compares equal now: the next cgb_conj_grad uploads
+    s->h_rowstr = nullptr;
+    s->h_colidx = nullptr;
+    s->h_a = nullptr;
+    return CGB_OK;
+}
+
 int cgb_power_iterate(cgb_session *s, const cgb_solve_params *params, double *zeta_trace,
                       double *rnorm_trace, int *iters_trace, double *x_out,
                       cgb_solve_result *res)

@@ -112,6 +112,7 @@ _SIGNATURES = {
     "cgb_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "cgb_conj_grad": (ctypes.c_int, [ctypes.c_void_p, _I32, _I32, _F64, _F64, _F64, _F64, _F64,
                                      _F64, ctypes.POINTER(ctypes.c_double)]),
+    "cgb_matrix_changed": (ctypes.c_int, [ctypes.c_void_p]),
     "cgb_default_solve_params": (None, [ctypes.POINTER(SolveParams)]),
     "cgb_power_iterate": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SolveParams),
                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -315,6 +316,11 @@ class Session:
         rowstr, colidx, a = self._keep
         _check(lib().cgb_conj_grad(self._h, colidx, rowstr, xv, z, a, p, q, r, ctypes.byref(rn)))
         return z, p, q, r, rn.value
+
+    def matrix_changed(self):
+        """The host arrays the session holds were edited in place: the next
+        conj_grad uploads them again (cgb_matrix_changed)."""
+        _check(lib().cgb_matrix_changed(self._h))
 
     def power_iterate(self, niter, shift, mode=MODE_FP64, cgitmax=25, tol=1e-12,
                       refresh_every=10, want_x=False, recycle=4):

@@ -70,10 +70,19 @@ def test_power_iterate_matches_reference(cgb, golden, cls):
 
 
 @pytest.mark.slow
-def test_power_iterate_class_c(cgb):
+def test_power_iterate_class_c(cgb, golden):
+    """The reference algorithm (fixed 25 CG steps) at class C against the
+    reference's own trace, every outer step: zeta relative 1e-10, rnorm
+    absolute 1e-10 (||x|| = 1 after the first step)."""
     n, nonzer, niter, shift = PARAMS["C"]
+    e = golden["C"]["seeds"]["314159265.0"]
     s, _ = session_for(cgb, "C")
     out = s.power_iterate(niter, shift)
+    ref_zeta = np.array(e["zeta"])
+    assert len(ref_zeta) == niter
+    assert np.max(np.abs(out["zeta"] - ref_zeta) / np.abs(ref_zeta)) <= 1e-10
+    assert np.max(np.abs(out["rnorm"] - np.array(e["rnorm"]))) <= 1e-10
+    assert np.all(out["iters"] == 25)
     assert abs(out["zeta"][-1] - VERIFY["C"]) / VERIFY["C"] <= 1e-10
 
 
@@ -145,6 +154,28 @@ def test_conj_grad_reuploads_changed_matrix(cgb, oracle):
     z, *_ , rn = s.conj_grad(np.ones(n))
     zo, *_ = oracle.conj_grad(rs2, ci2, a2, np.ones(n))
     assert np.linalg.norm(z[:n] - zo[:n]) <= 1e-12 * np.linalg.norm(zo[:n])
+
+
+def test_conj_grad_sees_in_place_edit_after_matrix_changed(cgb, oracle):
+    """cgb_conj_grad re-uploads when the arrays' pointers change; an edit in
+    place needs cgb_matrix_changed (the reference's CPU conj_grad reads a[]
+    on every call)."""
+    n, nonzer, _, shift = PARAMS["S"]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    s = cgb.Session(rs, ci, a)
+    x = np.ones(n)
+    z0, *_ = s.conj_grad(x)
+    held = s._keep[2]              # the very array the session was given
+    held *= 1.5                    # still negative definite
+    z_stale, *_ = s.conj_grad(x)   # same pointers: not seen
+    assert np.array_equal(z_stale, z0)
+    s.matrix_changed()
+    z1, *_, rn1 = s.conj_grad(x)
+    zo, *_, rno = oracle.conj_grad(rs, ci, held, x)
+    assert np.linalg.norm(z1[:n] - zo[:n]) <= 1e-12 * np.linalg.norm(zo[:n])
+    assert abs(rn1 - rno) <= 1e-10 * np.sqrt(n)
+    # z of 1.5 A is z of A over 1.5
+    assert np.linalg.norm(1.5 * z1[:n] - z0[:n]) <= 1e-11 * np.linalg.norm(z0[:n])
 
 
 def test_tolerance_mode_reaches_reference_zeta(cgb, golden):

@@ -3,12 +3,14 @@
 It serves callers that may not allocate GPU memory on this path (their
 device memory comes from their own pool, or the loop must never allocate):
 they pass their own device buffers for inputs and outputs, and the solver's
-work space lives in a fixed array inside libcgb.  Checked through the C ABI
-against the session entry point cgb_conj_grad on the same matrix, twice in a
-row (the second call runs on the array the first one left behind), with the
-tolerances of the other GPU tests: z relative 1e-12, rnorm absolute
-1e-10 * ||x||.  The test allocates its buffers with torch; the entry point
-itself allocates nothing.  This file is collected last on purpose.
+work space lives in a fixed array inside libcgb.  Checked through the C ABI,
+twice in a row (the second call runs on the array the first one left
+behind), against the session entry point cgb_conj_grad on the same matrix
+and against the CPU oracle's restatement of the reference conj_grad
+(cg.cu:653-801), with the tolerances of the other GPU tests: z relative
+1e-12, rnorm absolute 1e-10 * ||x||.  The test allocates its buffers with
+torch; the entry point itself allocates nothing.  This file is collected
+last on purpose.
 """
 import ctypes
 
@@ -22,7 +24,7 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
-def test_noalloc_conj_grad_matches_session(cgb):
+def test_noalloc_conj_grad_matches_session(cgb, oracle):
     import torch
 
     n, nonzer, shift = 14000, 11, 20.0
@@ -31,6 +33,7 @@ def test_noalloc_conj_grad_matches_session(cgb):
     x[:n] = 1.0 + 0.25 * np.cos(np.arange(n) * 0.013)
     with cgb.Session(rs, ci, a) as s:
         z_ref, _, _, _, rn_ref = s.conj_grad(x)
+    z_orc, _, _, _, rn_orc = oracle.conj_grad(rs, ci, a, x[:n])
 
     dev = torch.device("cuda", 0)
     d_rs = torch.from_numpy(rs).to(dev)
@@ -55,9 +58,13 @@ def test_noalloc_conj_grad_matches_session(cgb):
         assert int(d_st.item()) == 0, f"call {call}: device status {int(d_st.item())}"
         z = d_z.cpu().numpy()
         err = np.linalg.norm(z[:n] - z_ref[:n]) / np.linalg.norm(z_ref[:n])
-        assert err <= 1e-12, f"call {call}: z differs by {err:.3e}"
+        assert err <= 1e-12, f"call {call}: z differs from the session's by {err:.3e}"
+        err = np.linalg.norm(z[:n] - z_orc[:n]) / np.linalg.norm(z_orc[:n])
+        assert err <= 1e-12, f"call {call}: z differs from the oracle's by {err:.3e}"
         assert z[n] == 0.0
-        assert abs(float(d_rn.item()) - rn_ref) <= 1e-10 * xnorm, f"call {call}: rnorm"
+        rn = float(d_rn.item())
+        assert abs(rn - rn_ref) <= 1e-10 * xnorm, f"call {call}: rnorm vs the session"
+        assert abs(rn - rn_orc) <= 1e-10 * xnorm, f"call {call}: rnorm vs the oracle"
 
 
 def test_noalloc_rejects_misaligned(cgb):
