@@ -126,19 +126,29 @@ def physical_index(local_rank):
 
 
 def load_traffic():
-    """Per-launch DRAM bytes of the outer-step kernel from the committed ncu
-    summary: (kernel, workload, MB of the stream kept in L2) -> bytes."""
+    """Per-launch DRAM bytes (ncu: dram__bytes_read.sum + dram__bytes_write.sum)
+    of the kernels this bench reports, from the committed summary
+    profiles/traffic_per_launch.txt -- used only when that summary was
+    captured on this build: its `# build <hash>` line must equal the hash of
+    the library's sources (npbcg.source_fingerprint).  Returns ({(kernel,
+    workload, keep_mb): bytes}, a note saying where the numbers come from)."""
+    import npbcg
     path = os.path.join(ROOT, "profiles", "traffic_per_launch.txt")
-    out = {}
+    out, build = {}, None
     if os.path.exists(path):
         for line in open(path):
             parts = line.split()
-            if len(parts) >= 4 and not line.startswith("#"):
+            if line.startswith("# build") and len(parts) >= 3:
+                build = parts[2]
+            elif len(parts) >= 4 and not line.startswith("#"):
                 try:
                     out[(parts[0], parts[1], int(parts[2]))] = float(parts[3])
                 except ValueError:
                     pass
-    return out
+    here = npbcg.source_fingerprint()
+    if build != here:
+        return {}, f"none: no ncu capture of this build ({here}; the summary is of {build})"
+    return out, f"ncu capture of this build ({here}), profiles/traffic_per_launch.txt"
 
 
 def peaks():
@@ -220,8 +230,10 @@ def solver_modes_section(npbcg, device):
                 best = r
         return best
 
+    nnz = len(a)
     with npbcg.Session(rs, ci, a, device=device) as s:
         out["plan"] = s.plan()
+        out["roofline_classC"] = class_c_roofline(npbcg, s, n, nnz, niter, shift)
         plain = timed(s)
         zp = float(plain["zeta"][-1])
         runs, tols = {"fp64_fixed25": plain}, {"fp64_fixed25": None}
@@ -253,6 +265,12 @@ def solver_modes_section(npbcg, device):
                          "zeta_rel_err_vs_verify": abs(z - c["zeta"]) / c["zeta"],
                          "max_step_zeta_rel_err_vs_fp64_plain":
                              float(np.max(np.abs(r["zeta"] - plain["zeta"]) / np.abs(plain["zeta"]))),
+                         # ||x|| = 1 after the first outer step, sqrt(n) before
+                         "rnorm": float(r["rnorm"][-1]),
+                         "rnorm_abs_err_vs_fp64_plain": abs(float(r["rnorm"][-1]) -
+                                                            float(plain["rnorm"][-1])),
+                         "max_step_rnorm_abs_err_vs_fp64_plain":
+                             float(np.max(np.abs(r["rnorm"] - plain["rnorm"]))),
                          "inner_iterations": int(r["total_inner"]),
                          "refreshes": int(r.get("refreshes", 0)),
                          "fallbacks": int(r.get("fallbacks", 0)),
@@ -260,43 +278,115 @@ def solver_modes_section(npbcg, device):
     return out
 
 
+def class_c_roofline(npbcg, s, n, nnz, niter, shift):
+    """The SpMV roofline at class C (n=150000, nonzer=15): the plan's FP64
+    outer-step kernel (25 CG iterations + the residual product a launch) and
+    the standalone SpMV with the fused p.q (FP64 and FP32), each timed with
+    CUDA events on the library's stream; algorithmic bytes as in
+    outer_step_bytes / spmv_bytes; DRAM bytes from an ncu capture of this
+    build when there is one; and what one kernel boundary costs the solve's
+    CUDA graph (graphs of empty kernels of the outer step's shape)."""
+    plan = s.plan()
+    peak, peak_kind = peaks()
+    if plan["kind"] == "sliced":
+        kernel = "outer_step_fp64_sliced_pf" if plan["l2_prefetch"] else "outer_step_fp64_sliced"
+        spmv_kernel = "spmv_dot_sliced_pf" if plan["l2_prefetch"] else "spmv_dot_sliced"
+    else:
+        kernel = f"outer_step_fp64<{plan['lanes_per_row']}>"
+        spmv_kernel = f"spmv_dot_row<{plan['lanes_per_row']}>"
+    kernel_ms, gap_ms = s.time_outer_steps(niter, shift)
+    spmv_ms = s.time_spmv(50)
+    spmv32_ms = s.time_spmv(50, fp32=True)
+    table, note = load_traffic()
+    keep = int(round(plan.get("l2_keep_mb", 0.0)))
+    ob = outer_step_bytes(n, nnz)
+    sb = spmv_bytes(n, nnz)
+    sb32 = 8 * nnz + 4 * (n + 1) + 8 * n
+    out = {"workload": f"NPB class C: n={n} nonzer=15 nnz={nnz}", "peak": peak,
+           "peak_source": peak_kind, "plan": plan}
+    for name, k, ms, nbytes in (("outer_step", kernel, kernel_ms, ob),
+                                ("spmv_fp64", spmv_kernel, spmv_ms, sb),
+                                ("spmv_fp32", spmv_kernel.replace("spmv_dot_sliced", "spmv_dot_sliced32"),
+                                 spmv32_ms, sb32)):
+        gbs = nbytes / (ms / 1e3) / 1e9
+        traffic = table.get((k.split("<")[0], "classC", keep))
+        out[name] = {"kernel": k, "launch_ms": ms, "algorithmic_bytes_per_launch": nbytes,
+                     "achieved_gbs": gbs, "frac": gbs / peak, "traffic": traffic,
+                     "traffic_source": note if traffic is not None else
+                     (note if not table else "none: kernel not in the capture")}
+    out["graph_launch_overhead_ms_per_step"] = gap_ms
+    return out
+
+
 # -------------------------------------------------------------- batched
-def batched_section(npbcg, device, nsys=512, niter=15):
+def batched_section(npbcg, device, nsys=512, niter=15, rank=0, world=1, dist=None):
     """512 generator systems (n log-uniform in [1400, 20000], nonzer in 7..13,
-    shift = 10 + n/1000, own seeds) in one persistent launch: the FP64
-    reference algorithm (the yardstick) and the mixed-precision solver after the
-    autotuner; aggregate solves/s and each system's zeta error against the
-    ref_run."""
+    shift = 10 + n/1000, own seeds) in one persistent launch per GPU: the
+    FP64 reference algorithm (the yardstick) and the mixed-precision solver
+    after the autotuner; aggregate solves/s and each system's zeta error
+    against the FP64 reference algorithm.  With several ranks the systems
+    are sharded by size (npbcg.batch_shard: no exchange during the solve),
+    each rank solves its shard in its own launch, and rank 0 gathers the
+    per-system results; the aggregate rate is all systems over the slowest
+    rank's device time.  Returns None on ranks other than 0."""
     specs = npbcg.uneven_batch_specs(nsys=nsys)
-    systems = [npbcg.makea(n, nz, npbcg.RCOND, sh, seed) for n, nz, sh, seed in specs]
-    shifts = [sh for _, _, sh, _ in specs]
+    mine = list(range(nsys)) if world == 1 else npbcg.batch_shard(specs, rank, world)
+    systems = [npbcg.makea(specs[i][0], specs[i][1], npbcg.RCOND, specs[i][2], specs[i][3])
+               for i in mine]
+    shifts = [specs[i][2] for i in mine]
     with npbcg.Batch(systems, shifts, device=device) as b:
         # the autotuner picks block shape and lanes per row for each mode
         tuned_fp64 = b.tune(niter=1)
         ref_run = b.solve(niter=niter)
         tuned = b.tune(niter=1, mode=npbcg.MODE_MIXED, tol=1e-12, cgitmax=200)
         mixed = b.solve(niter=niter, mode=npbcg.MODE_MIXED, tol=1e-12, cgitmax=200)
-    conv = ref_run["rnorm"] <= 1e-10
-    rel = np.abs(mixed["zeta"] - ref_run["zeta"]) / np.abs(ref_run["zeta"])
     # algorithmic bytes of the FP64 reference algorithm: niter x (25 CG + residual) SpMVs per system
-    ref_bytes = sum(niter * (CGITMAX + 1) * spmv_bytes(len(s[0]) - 1, len(s[2])) for s in systems)
-    ref_gbs = ref_bytes / (ref_run["device_ms"] / 1e3) / 1e9
+    local_bytes = sum(niter * (CGITMAX + 1) * spmv_bytes(len(s[0]) - 1, len(s[2])) for s in systems)
+    local_nnz = sum(len(s[2]) for s in systems)
+    if world > 1:
+        loc = {"zeta_ref": ref_run["zeta"], "rnorm_ref": ref_run["rnorm"], "zeta": mixed["zeta"],
+               "status": mixed["status"], "iters": mixed["iters"],
+               "device_ms": ref_run["device_ms"]}
+        g_ref = npbcg.gather_shards(loc, mine, nsys, dist, rank)
+        g_mix = npbcg.gather_shards({"device_ms": mixed["device_ms"]}, mine, nsys, dist, rank)
+        tot = [None] * world if rank == 0 else None
+        dist.gather_object((local_bytes, local_nnz, len(mine)), tot, dst=0)
+        if rank != 0:
+            return None
+        ref_ms = max(g_ref["device_ms_per_rank"])
+        mix_ms = max(g_mix["device_ms_per_rank"])
+        zref, rref, zmix = g_ref["zeta_ref"], g_ref["rnorm_ref"], g_ref["zeta"]
+        status, iters = g_ref["status"], g_ref["iters"]
+        total_bytes = sum(t[0] for t in tot)
+        total_nnz = sum(t[1] for t in tot)
+        shard_info = {"ranks": world, "systems_per_rank": [t[2] for t in tot],
+                      "fp64_ms_per_rank": g_ref["device_ms_per_rank"],
+                      "mixed_ms_per_rank": g_mix["device_ms_per_rank"]}
+    else:
+        ref_ms, mix_ms = ref_run["device_ms"], mixed["device_ms"]
+        zref, rref, zmix = ref_run["zeta"], ref_run["rnorm"], mixed["zeta"]
+        status, iters = mixed["status"], mixed["iters"]
+        total_bytes, total_nnz, shard_info = local_bytes, local_nnz, None
+    conv = rref <= 1e-10
+    rel = np.abs(zmix - zref) / np.abs(zref)
+    ref_gbs = total_bytes / (ref_ms / 1e3) / 1e9
     peak, _ = peaks()
     return {
         "workload": f"{nsys} systems, n log-uniform in [1400, 20000], nonzer 7..13, "
                     f"shift 10 + n/1000, {niter} outer steps each",
-        "total_nnz": int(sum(len(s[2]) for s in systems)),
-        "autotuned": {"fp64": tuned_fp64, "mixed": tuned},
-        "fp64_reference": {"ms": ref_run["device_ms"], "solves_per_s": nsys / ref_run["device_ms"] * 1e3,
-                       "spmv_gbs": ref_gbs, "frac_of_peak": ref_gbs / peak},
-        "mixed": {"ms": mixed["device_ms"], "solves_per_s": nsys / mixed["device_ms"] * 1e3,
-                  "refit_in_fp64": int((mixed["status"] == 1).sum()),
-                  "inner_iterations": int(mixed["iters"].sum())},
+        "total_nnz": int(total_nnz),
+        "sharding": shard_info,
+        "autotuned": {"fp64": tuned_fp64, "mixed": tuned} if world == 1 else "per rank",
+        "fp64_reference": {"ms": ref_ms, "solves_per_s": nsys / ref_ms * 1e3,
+                           "spmv_gbs": ref_gbs, "frac_of_peak": ref_gbs / (peak * world)},
+        "mixed": {"ms": mix_ms, "solves_per_s": nsys / mix_ms * 1e3,
+                  "refit_in_fp64": int((status == 1).sum()),
+                  "inner_iterations": int(iters.sum())},
         "reference_converged_systems": int(conv.sum()),
         "max_zeta_rel_err_converged": float(rel[conv].max()) if conv.any() else None,
         "within_1e-10_converged": int((rel[conv] <= 1e-10).sum()),
         "within_1e-10_all": int((rel <= 1e-10).sum()),
-        "speedup_mixed_vs_fp64": ref_run["device_ms"] / mixed["device_ms"],
+        "speedup_mixed_vs_fp64": ref_ms / mix_ms,
     }
 
 
@@ -398,8 +488,9 @@ def our_arm(args, rank, world, local_rank):
     bytes_launch = outer_step_bytes(n, nnz)
     achieved = bytes_launch / (kernel_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
-    traffic = load_traffic().get((kernel.split("<")[0], f"class{CLASS}",
-                                  int(round(plan.get("l2_keep_mb", 0.0)))))
+    traffic_table, traffic_note = load_traffic()
+    traffic = traffic_table.get((kernel.split("<")[0], f"class{CLASS}",
+                                 int(round(plan.get("l2_keep_mb", 0.0)))))
     spmv_ms = sess.time_spmv(50)
     spmv_gbs = spmv_bytes(n, nnz) / (spmv_ms / 1e3) / 1e9
 
@@ -421,11 +512,14 @@ def our_arm(args, rank, world, local_rank):
             "zeta": zeta, "zeta_rel_err": zeta_err,
             "spmv_standalone": {"ms": spmv_ms, "gbs": spmv_gbs,
                                 "frac_of_peak": spmv_gbs / peak},
-            "outer_step_kernel_ms": kernel_ms, "graph_gap_ms_per_step": gap_ms,
+            "outer_step_kernel_ms": kernel_ms,
+            "graph_launch_overhead_ms_per_step": gap_ms,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "kernel": kernel,
                          "algorithmic_bytes_per_launch": bytes_launch,
-                         "launch_ms": kernel_ms, "peak_source": peak_kind},
+                         "launch_ms": kernel_ms, "peak_source": peak_kind,
+                         "traffic_source": traffic_note if traffic is not None else
+                         (traffic_note if not traffic_table else "none: kernel not in the capture")},
             "plan": plan,
             "clocks": clocks,
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d,
@@ -434,8 +528,7 @@ def our_arm(args, rank, world, local_rank):
         }
         if not args.no_solver_modes:
             line["solver_modes"] = solver_modes_section(npbcg, device)
-        if not args.no_batched and world == 1:
-            line["batched"] = batched_section(npbcg, device)
+            line["roofline_classC"] = line["solver_modes"].pop("roofline_classC")
         if world == 1 and not args.no_cpu_baseline:
             nref, nnz_ref, times = cpu_reference_run(CPU_SAMPLE_STEPS)
             sample_bytes = CPU_SAMPLE_STEPS * (CGITMAX + 1) * spmv_bytes(nref, nnz_ref)
@@ -450,6 +543,11 @@ def our_arm(args, rank, world, local_rank):
                 "openmp_port": {"value": sample_bytes / omp_s / 1e9, "unit": "GB/s",
                                 "cores": threads, "kind": "port", "seconds": omp_s},
             }
+    if not args.no_batched:
+        # every rank solves its shard of the batched workload; rank 0 gathers
+        batched = batched_section(npbcg, device, rank=rank, world=world, dist=dist)
+        if line is not None:
+            line["batched"] = batched
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

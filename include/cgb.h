@@ -286,9 +286,12 @@ int cgb_batch_set_team_frac(cgb_batch *b, double team_frac);
  * device milliseconds per launch. */
 int cgb_time_spmv(cgb_session *s, int reps, int fp32, double *ms_per_launch);
 
-/* Per-launch device times of one FP64 outer step kernel, and the gap the
- * graph adds per outer step: runs `niter` steps with events between the
- * kernels.  Outputs are means in milliseconds. */
+/* Per-launch device time of the FP64 outer step kernel (`niter` steps of the
+ * reference algorithm with events between the kernels, mean in ms) and what
+ * one kernel boundary costs the solve's CUDA graph (graph_gap_ms): graphs of
+ * niter and of 1 launches of an empty kernel with the outer step's shape
+ * (grid, block, shared memory, cooperative), timed with events, their
+ * difference over niter - 1 (best of five; ms per outer step). */
 int cgb_time_outer_steps(cgb_session *s, int niter, double shift, double *kernel_ms,
                          double *graph_gap_ms);
 

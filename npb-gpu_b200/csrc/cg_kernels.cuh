@@ -1121,6 +1121,12 @@ static __global__ void barrier_loop(GridBarrier gb, int iters)
         if (!grid_barrier(gb)) return;
 }
 
+// An empty persistent kernel: launched with an outer step's shape (grid,
+// block, dynamic shared memory, cooperative) it costs what a kernel
+// boundary costs in the solve's graph -- launch, CTA dispatch, teardown --
+// and nothing else (cgb_time_outer_steps).
+static __global__ void __launch_bounds__(1024, 1) launch_probe(int) {}
+
 static __global__ void barrier_timeout_probe(GridBarrier gb)
 {
     if (blockIdx.x == 1) return;

@@ -1116,6 +1116,63 @@ int check_params(cgb_session *s, const cgb_solve_params &P)
     return CGB_OK;
 }
 
+// What one more kernel costs a solve's graph beyond its own work: graphs
+// of `niter` and of 1 launch of an empty kernel with the FP64 outer step's
+// shape (grid, block, dynamic shared memory, cooperative), each timed with
+// events around the graph launch; the difference over niter - 1 launches
+// is the launch, dispatch and teardown cost of one outer step.  Best of
+// five alternating trials (ms per launch).
+int time_launch_overhead(cgb_session *s, int niter, double *ms_out)
+{
+    const Plan &P = s->plan;
+    CUDA_TRY(cudaFuncSetAttribute(launch_probe, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(P.smem)));
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(P.grid);
+    cfg.blockDim = dim3(P.block);
+    cfg.dynamicSmemBytes = P.smem;
+    cfg.stream = s->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaGraphExec_t ex[2] = {nullptr, nullptr};
+    const int counts[2] = {std::max(niter, 2), 1};
+    int st = CGB_OK;
+    for (int g = 0; g < 2 && st == CGB_OK; g++) {
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+        for (int i = 0; i < counts[g] && e == cudaSuccess; i++) e = cudaLaunchKernelEx(&cfg, launch_probe, i);
+        cudaError_t e2 = cudaStreamEndCapture(s->stream, &graph);
+        if (e == cudaSuccess && e2 == cudaSuccess) e = cudaGraphInstantiate(&ex[g], graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (e != cudaSuccess || e2 != cudaSuccess)
+            st = set_error(CGB_ERR_CUDA, "launch-overhead graph: %s",
+                           cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    double best[2] = {1e30, 1e30};
+    for (int trial = 0; trial < 6 && st == CGB_OK; trial++) {
+        for (int g = 0; g < 2; g++) {
+            float ms = 0.f;
+            if (cudaEventRecord(s->ev0, s->stream) != cudaSuccess ||
+                cudaGraphLaunch(ex[g], s->stream) != cudaSuccess ||
+                cudaEventRecord(s->ev1, s->stream) != cudaSuccess ||
+                cudaStreamSynchronize(s->stream) != cudaSuccess ||
+                cudaEventElapsedTime(&ms, s->ev0, s->ev1) != cudaSuccess) {
+                st = set_error(CGB_ERR_CUDA, "launch-overhead timing failed");
+                break;
+            }
+            if (trial > 0) best[g] = std::min(best[g], double(ms));  // trial 0 warms up
+        }
+    }
+    for (auto &x : ex)
+        if (x) cudaGraphExecDestroy(x);
+    if (st) return st;
+    *ms_out = std::max(0.0, (best[0] - best[1]) / (counts[0] - 1));
+    return CGB_OK;
+}
+
 bool same_params(const cgb_solve_params &a, const cgb_solve_params &b)
 {
     return a.niter == b.niter && a.shift == b.shift && a.mode == b.mode && a.cgitmax == b.cgitmax &&
@@ -1666,16 +1723,8 @@ int cgb_time_outer_steps(cgb_session *s, int niter, double shift, double *kernel
     st = collect_status(s);
     if (st) return st;
     *kernel_ms = total / niter;
-    // the graph's per-step cost beyond one kernel: time a graph of niter steps
-    cgb_solve_params P;
-    cgb_default_solve_params(&P);
-    P.niter = niter;
-    P.shift = shift;
-    cgb_solve_result res;
-    st = cgb_power_iterate(s, &P, nullptr, nullptr, nullptr, nullptr, &res);
-    if (st) return st;
-    *graph_gap_ms = res.device_ms / niter - *kernel_ms;
-    return CGB_OK;
+    st = time_launch_overhead(s, niter, graph_gap_ms);
+    return st;
 }
 
 int cgb_time_barrier(cgb_session *s, int iters, double *us_per_barrier)

@@ -393,6 +393,20 @@ class Session:
         return st, dev.value
 
 
+def source_fingerprint():
+    """A hash of the library's CUDA/C++ sources (csrc/): names a build, so a
+    profile captured on one build is not read as another's."""
+    import hashlib
+    h = hashlib.sha256()
+    csrc = os.path.join(os.path.dirname(_HERE), "csrc")
+    for name in sorted(os.listdir(csrc)):
+        if name.endswith((".cu", ".cuh", ".h", ".cpp")):
+            h.update(name.encode())
+            with open(os.path.join(csrc, name), "rb") as f:
+                h.update(f.read())
+    return h.hexdigest()[:16]
+
+
 def spmv_bytes_fp64(n, nnz):
     """Algorithmic bytes of one FP64 CSR SpMV: values + indices + row pointers + p + q."""
     return 12 * nnz + 4 * (n + 1) + 8 * n + 8 * n
@@ -578,6 +592,39 @@ def shard_systems(weights, world):
         parts[r].append(i)
         load[r] += weights[i]
     return [sorted(p) for p in parts]
+
+
+def batch_shard(specs, rank, world):
+    """The systems (indices into `specs`, [(n, nonzer, shift, seed)]) that rank
+    `rank` of `world` solves: a greedy split by the CSR size bound
+    n (nonzer + 1)^2, largest first to the least loaded rank.  Independent
+    systems need no exchange: each rank builds and solves its own Batch."""
+    weights = [n * (nz + 1) ** 2 for n, nz, _, _ in specs]
+    return shard_systems(weights, world)[rank]
+
+
+def gather_shards(local, index, nsys, dist, rank):
+    """Rank 0 assembles the per-system arrays of every rank's shard
+    (`local`: dict of equal-length arrays for the systems `index`) into
+    arrays over all `nsys` systems, plus each rank's device_ms; other ranks
+    get None.  `dist` is torch.distributed (gloo or NCCL)."""
+    payload = {k: np.asarray(v).tolist() for k, v in local.items() if k != "device_ms"}
+    payload["index"] = list(index)
+    payload["device_ms"] = float(local.get("device_ms", 0.0))
+    parts = [None] * dist.get_world_size() if rank == 0 else None
+    dist.gather_object(payload, parts, dst=0)
+    if rank != 0:
+        return None
+    out = {"device_ms_per_rank": [p["device_ms"] for p in parts]}
+    for key in parts[0]:
+        if key in ("index", "device_ms"):
+            continue
+        sample = np.asarray(parts[0][key])
+        arr = np.zeros(nsys, dtype=sample.dtype if sample.size else np.float64)
+        for p in parts:
+            arr[np.asarray(p["index"], dtype=np.int64)] = np.asarray(p[key])
+        out[key] = arr
+    return out
 
 
 class Batch:

@@ -1,9 +1,10 @@
 """Multi-rank batched solving: systems are split over ranks by a greedy
 stored-entry balance (npbcg.shard_systems) with no data-path collective, and
-the per-system results are gathered on rank 0.  Run here as two gloo ranks
-on the CPU, each solving its shard with the CPU oracle (the GPU kernel is
-covered by test_gpu_batch); the gathered zetas must equal a one-process
-solve of all systems."""
+the per-system results are gathered on rank 0 (npbcg.batch_shard,
+npbcg.gather_shards).  Run here as two gloo ranks on the CPU, each solving
+its shard with the CPU oracle (test_gpu_shard runs the same split on the
+GPU batch kernel); the gathered zetas and residuals must equal a
+one-process solve of all systems."""
 import os
 import socket
 
@@ -29,21 +30,22 @@ def worker(rank, world, port, out_path):
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
                             world_size=world, timeout=datetime.timedelta(seconds=60))
     specs = npbcg.uneven_batch_specs(nsys=10, seed=3, n_range=(150, 600), nonzer_range=(3, 6))
-    weights = [n * (nz + 1) ** 2 for n, nz, _, _ in specs]
-    parts = npbcg.shard_systems(weights, world)
+    mine = npbcg.batch_shard(specs, rank, world)
     o = Oracle(os.path.join(root, "oracle", "liboracle.so"))
-    mine = {}
-    for i in parts[rank]:
+    zeta, rnorm = [], []
+    for i in mine:
         n, nz, shift, seed = specs[i]
         rs, ci, a = o.makea(n, nz, 0.1, shift, seed)
-        mine[i] = float(o.power_iterate(rs, ci, a, shift, 5)["zeta"][-1])
-    gathered = [None] * world
-    dist.all_gather_object(gathered, mine)
+        r = o.power_iterate(rs, ci, a, shift, 5)
+        zeta.append(float(r["zeta"][-1]))
+        rnorm.append(float(r["rnorm"][-1]))
+    g = npbcg.gather_shards({"zeta": zeta, "rnorm": rnorm, "device_ms": 1.0 + rank}, mine,
+                            len(specs), dist, rank)
     if rank == 0:
-        merged = {}
-        for d in gathered:
-            merged.update(d)
-        np.save(out_path, np.array([merged[i] for i in range(len(specs))]))
+        assert g["device_ms_per_rank"] == [1.0 + r for r in range(world)]
+        np.save(out_path, np.stack([g["zeta"], g["rnorm"]]))
+    else:
+        assert g is None
     dist.barrier()
     dist.destroy_process_group()
 
@@ -71,8 +73,14 @@ def test_two_rank_gloo_batch(tmp_path, oracle):
                        start_method="spawn")
     got = np.load(out)
     specs = npbcg.uneven_batch_specs(nsys=10, seed=3, n_range=(150, 600), nonzer_range=(3, 6))
-    want = []
+    want_z, want_r = [], []
     for n, nz, shift, seed in specs:
         rs, ci, a = oracle.makea(n, nz, 0.1, shift, seed)
-        want.append(oracle.power_iterate(rs, ci, a, shift, 5)["zeta"][-1])
-    assert np.array_equal(got, np.array(want))
+        r = oracle.power_iterate(rs, ci, a, shift, 5)
+        want_z.append(r["zeta"][-1])
+        want_r.append(r["rnorm"][-1])
+    assert np.array_equal(got[0], np.array(want_z))
+    assert np.array_equal(got[1], np.array(want_r))
+    # every system solved exactly once
+    parts = [npbcg.batch_shard(specs, r, 2) for r in range(2)]
+    assert sorted(parts[0] + parts[1]) == list(range(len(specs)))
