@@ -340,21 +340,50 @@ def batched_section(npbcg, device, nsys=512, niter=15, rank=0, world=1, dist=Non
         ref_run = b.solve(niter=niter)
         tuned = b.tune(niter=1, mode=npbcg.MODE_MIXED, tol=1e-12, cgitmax=200)
         mixed = b.solve(niter=niter, mode=npbcg.MODE_MIXED, tol=1e-12, cgitmax=200)
+        learned = ident = tuned_l = None
+        if os.path.exists(npbcg.WEIGHTS_PATH):
+            # the learned preconditioner (one network inference per system),
+            # then the same kernel with F = I (the method without the network)
+            model = npbcg.Gnn(device=device)
+            model.load()
+            t0 = time.perf_counter()
+            b.attach_learned(model)
+            attach_s = time.perf_counter() - t0
+            model.close()
+            tuned_l = b.tune(niter=1, mode=npbcg.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=200)
+            learned = b.solve(niter=niter, mode=npbcg.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=200)
+            learned["fallbacks"] = b.fallbacks()
+            learned["attach_s"] = attach_s
+            b.attach_identity()
+            ident = b.solve(niter=niter, mode=npbcg.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=200)
     # algorithmic bytes of the FP64 reference algorithm: niter x (25 CG + residual) SpMVs per system
     local_bytes = sum(niter * (CGITMAX + 1) * spmv_bytes(len(s[0]) - 1, len(s[2])) for s in systems)
     local_nnz = sum(len(s[2]) for s in systems)
+    has_l = learned is not None
     if world > 1:
         loc = {"zeta_ref": ref_run["zeta"], "rnorm_ref": ref_run["rnorm"], "zeta": mixed["zeta"],
                "status": mixed["status"], "iters": mixed["iters"],
                "device_ms": ref_run["device_ms"]}
+        if has_l:
+            loc.update(zeta_l=learned["zeta"], status_l=learned["status"], iters_l=learned["iters"],
+                       fb_l=learned["fallbacks"], zeta_i=ident["zeta"], iters_i=ident["iters"])
         g_ref = npbcg.gather_shards(loc, mine, nsys, dist, rank)
         g_mix = npbcg.gather_shards({"device_ms": mixed["device_ms"]}, mine, nsys, dist, rank)
+        g_l = npbcg.gather_shards({"device_ms": learned["device_ms"] if has_l else 0.0},
+                                  mine, nsys, dist, rank)
+        g_i = npbcg.gather_shards({"device_ms": ident["device_ms"] if has_l else 0.0},
+                                  mine, nsys, dist, rank)
         tot = [None] * world if rank == 0 else None
         dist.gather_object((local_bytes, local_nnz, len(mine)), tot, dst=0)
         if rank != 0:
             return None
         ref_ms = max(g_ref["device_ms_per_rank"])
         mix_ms = max(g_mix["device_ms_per_rank"])
+        if has_l:
+            lrn = dict(zeta=g_ref["zeta_l"], status=g_ref["status_l"], iters=g_ref["iters_l"],
+                       fallbacks=g_ref["fb_l"], device_ms=max(g_l["device_ms_per_rank"]))
+            idn = dict(zeta=g_ref["zeta_i"], iters=g_ref["iters_i"],
+                       device_ms=max(g_i["device_ms_per_rank"]))
         zref, rref, zmix = g_ref["zeta_ref"], g_ref["rnorm_ref"], g_ref["zeta"]
         status, iters = g_ref["status"], g_ref["iters"]
         total_bytes = sum(t[0] for t in tot)
@@ -367,13 +396,38 @@ def batched_section(npbcg, device, nsys=512, niter=15, rank=0, world=1, dist=Non
         zref, rref, zmix = ref_run["zeta"], ref_run["rnorm"], mixed["zeta"]
         status, iters = mixed["status"], mixed["iters"]
         total_bytes, total_nnz, shard_info = local_bytes, local_nnz, None
+        lrn, idn = learned, ident
     conv = rref <= 1e-10
     rel = np.abs(zmix - zref) / np.abs(zref)
     ref_gbs = total_bytes / (ref_ms / 1e3) / 1e9
     peak, _ = peaks()
+    learned_out = None
+    if has_l:
+        rel_l = np.abs(lrn["zeta"] - zref) / np.abs(zref)
+        rel_i = np.abs(idn["zeta"] - zref) / np.abs(zref)
+        solved = lrn["status"] != 1
+        learned_out = {
+            "ms": lrn["device_ms"], "solves_per_s": nsys / lrn["device_ms"] * 1e3,
+            "autotuned": tuned_l if world == 1 else "per rank",
+            "attach_s": learned.get("attach_s"),
+            "refit_in_fp64": int((lrn["status"] == 1).sum()),
+            "systems_with_plain_cg_fallback": int((lrn["status"] == 2).sum()),
+            "inner_iterations": int(lrn["iters"].sum()),
+            "inner_iterations_preconditioned_systems": int(lrn["iters"][solved].sum()),
+            "max_zeta_rel_err_converged": float(rel_l[conv].max()) if conv.any() else None,
+            "within_1e-10_converged": int((rel_l[conv] <= 1e-10).sum()),
+            "within_1e-10_all": int((rel_l <= 1e-10).sum()),
+            "speedup_vs_fp64": ref_ms / lrn["device_ms"],
+            "speedup_vs_mixed": mix_ms / lrn["device_ms"],
+            "identity_factor": {
+                "ms": idn["device_ms"], "inner_iterations_preconditioned_systems":
+                    int(idn["iters"][solved].sum()),
+                "max_zeta_rel_err_converged": float(rel_i[conv].max()) if conv.any() else None},
+        }
     return {
         "workload": f"{nsys} systems, n log-uniform in [1400, 20000], nonzer 7..13, "
                     f"shift 10 + n/1000, {niter} outer steps each",
+        "mixed_learned": learned_out,
         "total_nnz": int(total_nnz),
         "sharding": shard_info,
         "autotuned": {"fp64": tuned_fp64, "mixed": tuned} if world == 1 else "per rank",

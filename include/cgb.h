@@ -227,6 +227,9 @@ int cgb_gnn_train_step(cgb_gnn *m, cgb_gnn_graph *g, unsigned seed, int cg_steps
 int cgb_gnn_infer(cgb_gnn *m, cgb_gnn_graph *g, float *goff, float *gdiag);
 /* Infers G and installs F = G / sqrt(delta) as the session's preconditioner. */
 int cgb_gnn_attach(cgb_gnn *m, cgb_gnn_graph *g, cgb_session *s);
+/* The same for system `sys` of a batch (g built on that system's matrix). */
+typedef struct cgb_batch cgb_batch;
+int cgb_gnn_attach_batch(cgb_gnn *m, cgb_gnn_graph *g, cgb_batch *b, int sys);
 
 /* ------------------------------------------------------------- batches */
 /* Many independent systems of uneven order (n <= 27000 each) solved in one
@@ -245,11 +248,13 @@ typedef struct cgb_batch cgb_batch;
 
 typedef struct cgb_batch_params {
     int niter;          /* outer steps per system */
-    int mode;           /* CGB_MODE_FP64 (fixed cgitmax steps) or CGB_MODE_MIXED */
-    int cgitmax;        /* inner steps: exact (FP64) or cap (MIXED) */
-    double tol;         /* MIXED: stop when ||x - A z|| <= tol ||x|| */
-    int refresh_every;  /* MIXED: true-residual replacement at least every k steps */
-    int recycle;        /* MIXED: Galerkin start on the last `recycle` iterates (0..4, default 4) */
+    int mode;           /* CGB_MODE_FP64 (fixed cgitmax steps), CGB_MODE_MIXED or
+                           CGB_MODE_MIXED_LEARNED (MIXED preconditioned by each system's
+                           M = F^T F, cgb_batch_set_preconditioner) */
+    int cgitmax;        /* inner steps: exact (FP64) or cap (MIXED*) */
+    double tol;         /* MIXED*: stop when ||x - A z|| <= tol ||x|| */
+    int refresh_every;  /* MIXED*: true-residual replacement at least every k steps */
+    int recycle;        /* MIXED*: Galerkin start on the last `recycle` iterates (0..4, default 4) */
 } cgb_batch_params;
 
 void cgb_default_batch_params(cgb_batch_params *p);
@@ -259,8 +264,10 @@ int cgb_batch_create(int device, int nsys, const int *n, const int *const *rowst
                      cgb_batch **out);
 int cgb_batch_destroy(cgb_batch *b);
 /* Per-system outputs (nsys entries each, nullable): final zeta, rnorm, inner
- * iterations summed over the outer steps, status (0, or 1 = re-solved in
- * FP64); *device_ms the launch's device time. */
+ * iterations summed over the outer steps, status (0; 1 = re-solved in FP64
+ * with the reference algorithm; 2 = CGB_MODE_MIXED_LEARNED, where some outer
+ * step's preconditioned iteration stalled and that step finished as plain
+ * CG, cgb_batch_fallbacks counts them); *device_ms the launch's device time. */
 int cgb_batch_solve(cgb_batch *b, const cgb_batch_params *params, double *zeta, double *rnorm,
                     int *iters, int *status, double *device_ms);
 /* Autotuner: times the batch for each candidate block shape and lane policy
@@ -278,6 +285,19 @@ int cgb_batch_tune(cgb_batch *b, const cgb_batch_params *params, int *block, dou
 int cgb_batch_policy(cgb_batch *b, int *unroll, double *team_frac, int *teams);
 /* Sets the team fraction (0 = every system on one CTA; default 0.5). */
 int cgb_batch_set_team_frac(cgb_batch *b, double team_frac);
+/* The preconditioner of system `sys` in CGB_MODE_MIXED_LEARNED: M = F^T F with
+ * F lower triangular in CSR (n+1 row pointers, columns <= row, a positive
+ * diagonal in every row), as cgb_set_preconditioner takes it; stored with
+ * BF16 values and 16-bit columns.  Every system needs one before a learned
+ * solve (the learned factor is G diag(-A)^-1/2 with G from cgb_gnn_infer;
+ * cgb_gnn_attach_batch installs it).  In the solve, both factor products
+ * gather from a shared-memory copy of the vector.  No counterpart in the
+ * reference. */
+int cgb_batch_set_preconditioner(cgb_batch *b, int sys, const int *fptr, const int *fcol,
+                                 const double *fval);
+/* Outer steps per system (nsys ints) of the last learned solve that fell back
+ * to plain CG (0 for the other modes). */
+int cgb_batch_fallbacks(cgb_batch *b, int *fallbacks);
 
 /* ---------------------------------------------------------- diagnostics */
 /* Time `reps` launches of the standalone SpMV (q = A p with the p.q

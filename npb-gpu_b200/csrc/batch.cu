@@ -23,6 +23,14 @@
 //          indefinite system an eigenvalue of A near zero can make zeta
 //          sensitive beyond what a 1e-12 residual pins down, so agreement
 //          with the reference needs the reference's own iteration there.)
+//   learned  the mixed mode preconditioned by M = F^T F per system (F lower
+//          triangular with a positive diagonal, cgb_batch_set_preconditioner:
+//          the learned factor G diag(-A)^-1/2), CG on -A; the factor's values
+//          are BF16 with 16-bit columns, both factor products gather from a
+//          shared-memory copy of the vector.  An outer step whose
+//          preconditioned iteration stalls (|r|^2 not halved in four steps,
+//          or r.y <= 0) continues as plain CG; a system showing p.Ap >= 0 is
+//          re-solved with the FP64 reference algorithm, as in the mixed mode.
 // Lanes per row are a per-system choice (the autotuner's, by row length).
 #include <cuda_runtime.h>
 
@@ -32,6 +40,8 @@
 #include <new>
 #include <numeric>
 #include <vector>
+
+#include <cuda_bf16.h>
 
 #include "cgb_internal.h"
 #include "device_common.cuh"
@@ -52,11 +62,19 @@ struct SysDesc {
     int n;
     int lanes;           // lanes per row (2, 4, 8, 16, 32)
     int team;            // CTAs that solve the system together (1, 2, 4 or 8)
+    int flanes;          // lanes per row of the preconditioner's factor products
     long long row_off;   // into rowstr_all (n+1 entries)
     long long nnz_off;   // into colidx_all / a_all
     long long vec_off;   // into the vector arrays (n+8 entries)
+    long long f_row_off; // into the factor row pointers (F and F^T: n+1 entries each)
+    long long f_off;     // into the factor entries (F and F^T: the same count)
     double shift;
 };
+
+// Batch modes (the launch's kernel).
+constexpr int kModeFixed = 0;
+constexpr int kModeMixed = 1;
+constexpr int kModeLearned = 2;
 
 struct BatchArgs {
     int nsys;
@@ -84,6 +102,16 @@ struct BatchArgs {
     unsigned *team_sync;
     double *team_part;
     int *dev_status;     // kDevOk, or kDevTimeout once a team wait ran out
+    // learned mode: the factor F (lower, rows of F) and F^T (rows of F^T),
+    // BF16 values and 16-bit columns; the preconditioned residual y (FP64)
+    // and two FP32 exchange vectors (r and F r) in the vec_off layout, and
+    // per system the outer steps that fell back to plain CG
+    const int *fptr, *ftptr;
+    const unsigned short *fcol, *ftcol;
+    const __nv_bfloat16 *fval, *ftval;
+    double *y;
+    float *rg, *tg;
+    int *fallbacks;
 };
 
 // This CTA's part of a system: rows [lo, hi) of `size` members (balanced by
@@ -249,9 +277,15 @@ __device__ __forceinline__ void team_gather_p(const Team &T, const double *pg, d
 // is a run-time value: one instance of the solver serves every system (an
 // instance per lane count inlined under one switch needed 128 registers a
 // thread and spilled; one needs about 84).
-template <bool F32, int kU>
+template <typename T>
+struct NoDeduce {
+    using type = T;
+};
+
+template <bool F32, int kU, typename VS = double>
 __device__ __forceinline__ double sys_spmv(const BatchArgs &B, const SysDesc &S, int lo, int hi,
-                                           const double *v_sh, const double *v_gl, double *q,
+                                           const typename NoDeduce<VS>::type *v_sh,
+                                           const double *v_gl, double *q,
                                            const double *dv_sh, bool v_gl_shared = false)
 {
     const int *rowstr = B.rowstr + S.row_off;
@@ -283,7 +317,7 @@ __device__ __forceinline__ double sys_spmv(const BatchArgs &B, const SysDesc &S,
 #pragma unroll
             for (int u = 0; u < kU; u++) {
                 if (k + u * LPR < k1) {
-                    const double pv = v_sh ? v_sh[c[u]]
+                    const double pv = v_sh ? double(v_sh[c[u]])
                                            : (v_gl_shared ? __ldcg(v_gl + c[u]) : v_gl[c[u]]);
                     if (F32) s32 = fmaf(af[u], float(pv), s32);
                     else s64 = fma(av[u], pv, s64);
@@ -382,8 +416,10 @@ static __device__ __forceinline__ GalerkinOut galerkin_body(GalerkinIn in)
         const double rv = in.x[j] - az;
         in.z[j] = z0;
         in.r[j] = rv;
-        in.p[j] = rv;
-        if (team) in.pg[j] = rv;
+        if (in.p) {  // (the learned mode sets its own start vectors)
+            in.p[j] = rv;
+            if (team) in.pg[j] = rv;
+        }
         acc = fma(rv, rv, acc);
     }
     out.acc = acc;
@@ -564,23 +600,360 @@ __device__ int solve_system(const BatchArgs &B, const SysDesc &S, Team &T, int c
     return kSolveOk;
 }
 
+// One factor product for rows [lo, hi): out[row] = sum_k val[k] v[col[k]]
+// (BF16 values widened to FP32, 16-bit columns, v an FP32 vector in shared
+// memory, FP32 row sums) with `lanes` lanes a row, written as FP32 (out32)
+// and/or FP64 (out64); returns this thread's share of sum dot[row] out[row]
+// (dot may be null).
+template <int kU>
+__device__ __forceinline__ double sys_fprod(const int *ptr, const unsigned short *col,
+                                            const __nv_bfloat16 *val, int lanes, int lo, int hi,
+                                            const float *v, float *out32, double *out64,
+                                            const double *dot)
+{
+    const int LPR = lanes;
+    const int lane = threadIdx.x & (LPR - 1), grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
+    const unsigned mask =
+        LPR == 32 ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) & ~(LPR - 1)));
+    double dacc = 0.0;
+    for (int row = lo + grp; row < hi; row += ngrp) {
+        const int k0 = ptr[row], k1 = ptr[row + 1];
+        float s = 0.f;
+        for (int k = k0 + lane; k < k1; k += kU * LPR) {
+            unsigned short c[kU];
+            __nv_bfloat16 w[kU];
+#pragma unroll
+            for (int u = 0; u < kU; u++) {
+                const int kk = k + u * LPR;
+                if (kk < k1) {
+                    c[u] = __ldcs(col + kk);
+                    w[u] = __ushort_as_bfloat16(__ldcs(reinterpret_cast<const unsigned short *>(val) + kk));
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; u++)
+                if (k + u * LPR < k1) s = fmaf(__bfloat162float(w[u]), v[c[u]], s);
+        }
+        s = group_sum_f_rt(s, mask, LPR);
+        if (lane == 0) {
+            if (out32) out32[row] = s;
+            if (out64) out64[row] = double(s);
+            if (dot) dacc = fma(dot[row], double(s), dacc);
+        }
+    }
+    return dacc;
+}
+
+// Team copy of an FP32 vector held in shared memory: this CTA wrote its rows
+// [lo, hi) to both v_sh and the global copy g; after a team barrier the
+// other members' rows come from g.
+__device__ __forceinline__ void team_gather_f(const Team &T, const float *g, float *v_sh, int n)
+{
+    if (T.size == 1) return;
+    for (int j = threadIdx.x; j < T.lo; j += blockDim.x) v_sh[j] = __ldcg(g + j);
+    for (int j = T.hi + threadIdx.x; j < n; j += blockDim.x) v_sh[j] = __ldcg(g + j);
+    __syncthreads();
+}
+
+// The learned mode's view of one system: its vectors and factor arrays.
+struct PcgSys {
+    double *x, *z, *r, *q, *pg, *y;
+    float *rg, *tg, *p32, *v32;
+    const int *fptr, *ftptr;
+    const unsigned short *fcol, *ftcol;
+    const __nv_bfloat16 *fval, *ftval;
+};
+
+// y = M r' = F^T (F r') (use) or y = r' (plain CG), and rho = r'.y (a team
+// sum).  On entry v32 holds r' in FP32 for every row; on return it holds
+// F r' (use).  False: a team wait failed.
+template <int kU>
+__device__ __forceinline__ bool pcg_apply(const BatchArgs &B, const SysDesc &S, Team &T,
+                                          const PcgSys &V, bool use, double *red, double &rho)
+{
+    const int n = S.n, lo = T.lo, hi = T.hi;
+    const bool team = T.size > 1;
+    double dacc = 0.0;
+    if (use) {
+        // t = F r' (own rows) to the global copy
+        sys_fprod<kU>(V.fptr, V.fcol, V.fval, S.flanes, lo, hi, V.v32, V.tg, nullptr, nullptr);
+        // every row of t into v32, once every thread (and member) is done with r'
+        if (team) {
+            if (!team_barrier(team_mem(B, T.id), T)) return false;
+            for (int j = threadIdx.x; j < n; j += blockDim.x) V.v32[j] = __ldcg(V.tg + j);
+        } else {
+            __syncthreads();
+            for (int j = threadIdx.x; j < n; j += blockDim.x) V.v32[j] = V.tg[j];
+        }
+        __syncthreads();
+        // y = F^T t (own rows), with the r'.y share
+        dacc = sys_fprod<kU>(V.ftptr, V.ftcol, V.ftval, S.flanes, lo, hi, V.v32, nullptr, V.y, V.r);
+    } else {
+        for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+            const double rv = V.r[j];
+            V.y[j] = rv;
+            dacc = fma(rv, rv, dacc);
+        }
+    }
+    return team_sum(B, T, dacc, red, rho);
+}
+
+// After this CTA wrote its rows of p to pg (FP64) and p32: the whole p32
+// (a team barrier and the other members' rows from pg; or a CTA barrier).
+template <bool kTeams>
+__device__ __forceinline__ bool pcg_publish_p(const BatchArgs &B, const Team &T, const PcgSys &V,
+                                              int n)
+{
+    if (kTeams && T.size > 1) {
+        if (!team_barrier(team_mem(B, T.id), T)) return false;
+        for (int j = threadIdx.x; j < T.lo; j += blockDim.x) V.p32[j] = float(__ldcg(V.pg + j));
+        for (int j = T.hi + threadIdx.x; j < n; j += blockDim.x) V.p32[j] = float(__ldcg(V.pg + j));
+    }
+    __syncthreads();
+    return true;
+}
+
+// One system's power iteration in the learned mode: preconditioned CG on
+// A' = -A with b' = -x (the same solution z), M = F^T F, FP32 products
+// (A32 and the factors) inside FP64 refinement with the mixed mode's
+// true-residual replacement and restart, stopped at a true residual
+// ||x - A z|| <= tol ||x||.  Shared memory holds p and the factor
+// products' vector in FP32; the FP64 search vector is pg.  An outer step
+// whose preconditioned iteration stalls continues as plain CG
+// (*fallbacks_out counts those steps); p.A'p <= 0 (A not negative
+// definite), a non-finite residual or no convergence gives up, and the
+// caller re-solves with the FP64 reference algorithm.
+template <int kU, bool kTeams>
+__device__ int solve_system_pcg(const BatchArgs &B, const SysDesc &S, Team &T, int cgitmax,
+                                double *smem, double *red, int *iters_out, double *zeta_out,
+                                double *rnorm_out, int *fallbacks_out)
+{
+    if (!kTeams) {
+        T.size = 1;
+        T.lo = 0;
+        T.hi = S.n;
+    }
+    const int n = S.n, lo = T.lo, hi = T.hi;
+    const bool team = kTeams && T.size > 1;
+    PcgSys V;
+    V.x = B.x + S.vec_off;
+    V.z = B.z + S.vec_off;
+    V.r = B.r + S.vec_off;
+    V.q = B.q + S.vec_off;
+    V.pg = B.pg + S.vec_off;
+    V.y = B.y + S.vec_off;
+    V.rg = B.rg + S.vec_off;
+    V.tg = B.tg + S.vec_off;
+    V.p32 = reinterpret_cast<float *>(smem);
+    V.v32 = V.p32 + ((n + 8 + 3) & ~3);
+    V.fptr = B.fptr + S.f_row_off;
+    V.ftptr = B.ftptr + S.f_row_off;
+    V.fcol = B.fcol + S.f_off;
+    V.ftcol = B.ftcol + S.f_off;
+    V.fval = B.fval + S.f_off;
+    V.ftval = B.ftval + S.f_off;
+    for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) V.x[j] = 1.0;
+    __syncthreads();
+    int total = 0, fallbacks = 0;
+    double zeta = 0.0, rnorm = 0.0;
+    for (int outer = 0; outer < B.niter; outer++) {
+        double acc = 0.0, xx = 0.0;
+        const int m = B.recycle;
+        const int v = m > 0 ? min(outer, m) : 0;
+        if (v > 0) {
+            // Galerkin start: z0, r = x - A z0 (no p written)
+            GalerkinIn in{B.hx, B.hw, B.hstride, S.vec_off, V.x, V.z, V.r, V.pg, nullptr, T,
+                          team_mem(B, T.id), outer, m, v};
+            const GalerkinOut g = kTeams ? batch_galerkin(in) : galerkin_body(in);
+            if (!g.ok) return kSolveAborted;
+            T.par = g.par;
+            xx = g.xx;
+            for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+                const double rv = -V.r[j];  // r' = A z0 - x
+                V.r[j] = rv;
+                V.v32[j] = float(rv);
+                if (team) V.rg[j] = float(rv);
+                acc = fma(rv, rv, acc);
+            }
+        } else {
+            for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+                const double xv = V.x[j];
+                V.z[j] = 0.0;
+                V.r[j] = -xv;
+                V.v32[j] = float(-xv);
+                if (team) V.rg[j] = float(-xv);
+                acc = fma(xv, xv, acc);
+            }
+        }
+        double rr;
+        if (!team_sum(B, T, acc, red, rr)) return kSolveAborted;  // barrier: r' published
+        team_gather_f(T, V.rg, V.v32, n);
+        if (v == 0) xx = rr;
+        const double stop2 = B.tol * B.tol * xx;
+        double rr_cycle = rr;
+        double hist[4] = {rr, rr, rr, rr};  // |r'|^2 of the last four steps
+        bool use = true;
+        double rho = 0.0;
+        if (!pcg_apply<kU>(B, S, T, V, use, red, rho)) return kSolveAborted;
+        if (!(rho > 0.0)) {
+            use = false;
+            if (!pcg_apply<kU>(B, S, T, V, false, red, rho)) return kSolveAborted;
+        }
+        for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+            const double pv = V.y[j];
+            V.pg[j] = pv;
+            V.p32[j] = float(pv);
+        }
+        if (!pcg_publish_p<kTeams>(B, T, V, n)) return kSolveAborted;
+        int it = 0, since = 0;
+        bool fresh = true;
+        for (;;) {
+            bool refresh = false;
+            if (rr <= stop2) {
+                if (fresh) break;
+                refresh = true;
+            } else if (!fresh && (since >= B.refresh_every || rr <= 1e-12 * rr_cycle)) {
+                refresh = true;
+            }
+            if (!refresh && it >= cgitmax) return kSolveGaveUp;  // not converged
+            bool restart = refresh;
+            if (refresh) {
+                // r' = A z - x with the FP64 matrix (z published by the last team sum)
+                sys_spmv<false, kU>(B, S, lo, hi, nullptr, V.z, V.q, nullptr, team);
+                __syncthreads();
+                acc = 0.0;
+                for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+                    const double rv = V.q[j] - V.x[j];
+                    V.r[j] = rv;
+                    V.v32[j] = float(rv);
+                    if (team) V.rg[j] = float(rv);
+                    acc = fma(rv, rv, acc);
+                }
+                if (!team_sum(B, T, acc, red, rr)) return kSolveAborted;
+                team_gather_f(T, V.rg, V.v32, n);
+                rr_cycle = rr;
+                hist[0] = hist[1] = hist[2] = hist[3] = rr;
+                since = 0;
+                fresh = true;
+                if (rr <= stop2) break;
+            } else {
+                // q = A32 p32 (FP32 products); p.A'p = -p.q
+                const double dpart = sys_spmv<true, kU, float>(B, S, lo, hi, V.p32, nullptr, V.q, V.pg);
+                double d;
+                if (!team_sum(B, T, dpart, red, d)) return kSolveAborted;
+                const double pAp = -d;
+                if (!(pAp > 0.0)) return kSolveGaveUp;  // not negative definite (or NaN)
+                const double alpha = rho / pAp;
+                acc = 0.0;
+                for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+                    V.z[j] = fma(alpha, V.pg[j], V.z[j]);
+                    const double rv = fma(alpha, V.q[j], V.r[j]);  // r' -= alpha A'p
+                    V.r[j] = rv;
+                    V.v32[j] = float(rv);
+                    if (team) V.rg[j] = float(rv);
+                    acc = fma(rv, rv, acc);
+                }
+                if (!team_sum(B, T, acc, red, rr)) return kSolveAborted;
+                if (!(rr < INFINITY)) return kSolveGaveUp;  // non-finite residual
+                team_gather_f(T, V.rg, V.v32, n);
+                it++;
+                since++;
+                fresh = false;
+                // stall: no halving of |r'|^2 over four steps
+                if (use && since >= 4 && rr > 0.25 * hist[0]) {
+                    use = false;
+                    restart = true;
+                }
+                hist[0] = hist[1];
+                hist[1] = hist[2];
+                hist[2] = hist[3];
+                hist[3] = rr;
+            }
+            double rho_new = 0.0;
+            if (!pcg_apply<kU>(B, S, T, V, use, red, rho_new)) return kSolveAborted;
+            if (use && !(rho_new > 0.0)) {
+                use = false;
+                restart = true;
+                if (!pcg_apply<kU>(B, S, T, V, false, red, rho_new)) return kSolveAborted;
+            }
+            const double beta = restart ? 0.0 : rho_new / rho;
+            rho = rho_new;
+            for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+                const double pv = fma(beta, V.pg[j], V.y[j]);
+                V.pg[j] = pv;
+                V.p32[j] = float(pv);
+            }
+            if (!pcg_publish_p<kTeams>(B, T, V, n)) return kSolveAborted;
+        }
+        total += it;
+        if (!use) fallbacks++;
+        // q = A z: from the true residual r' = A z - x just accepted, else a product
+        if (fresh) {
+            for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) V.q[j] = V.x[j] + V.r[j];
+        } else {
+            sys_spmv<false, kU>(B, S, lo, hi, nullptr, V.z, V.q, nullptr, team);
+        }
+        __syncthreads();
+        double res = 0.0, xz = 0.0, zz = 0.0;
+        for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+            const double xv = V.x[j], zv = V.z[j], dv = xv - V.q[j];
+            res = fma(dv, dv, res);
+            xz = fma(xv, zv, xz);
+            zz = fma(zv, zv, zz);
+        }
+        double t0, t1, t2;
+        if (!team_sum(B, T, res, red, t0) || !team_sum(B, T, xz, red, t1) ||
+            !team_sum(B, T, zz, red, t2))
+            return kSolveAborted;
+        rnorm = sqrt(t0);
+        zeta = S.shift + 1.0 / t1;
+        const double norm = 1.0 / sqrt(t2);
+        if (m > 0) {
+            const long long slot = (outer + 1) % m * B.hstride + S.vec_off;
+            for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+                const double xn = norm * V.z[j];
+                B.hx[slot + j] = xn;
+                B.hw[slot + j] = norm * V.q[j];
+                V.x[j] = xn;
+            }
+        } else {
+            for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) V.x[j] = norm * V.z[j];
+        }
+        __syncthreads();
+    }
+    *iters_out = total;
+    *zeta_out = zeta;
+    *rnorm_out = rnorm;
+    *fallbacks_out = fallbacks;
+    return kSolveOk;
+}
+
 // This CTA's share (member `member` of the system's team) of one system.  A
-// mixed solve that gives up (an indefinite system shows p.Ap >= 0 within the
-// first iterations) is redone at once by the same team with the reference
-// algorithm (FP64, exactly the reference's 25 CG iterations an outer step)
-// and marked status 1; its outputs are that solve's alone.  False: a team
-// wait failed and the CTA must stop.
-template <bool mixed, int kU, bool kTeams>
+// mixed or learned solve that gives up (an indefinite system shows
+// p.Ap >= 0 within the first iterations) is redone at once by the same team
+// with the reference algorithm (FP64, exactly the reference's 25 CG
+// iterations an outer step) and marked status 1; its outputs are that
+// solve's alone.  A learned solve in which some outer step fell back to
+// plain CG is marked status 2.  False: a team wait failed and the CTA must
+// stop.
+template <int kMode, int kU, bool kTeams>
 __device__ bool run_system(const BatchArgs &B, int id, int member, const SysDesc &S, double *p,
                            double *red)
 {
     Team T = make_team(B, id, S, member);
-    int iters = 0;
+    int iters = 0, fallbacks = 0;
     double zeta = 0.0, rnorm = 0.0;
-    int rc = solve_system<mixed, kU, kTeams>(B, S, T, B.cgitmax, p, red, &iters, &zeta, &rnorm);
-    const bool gave_up = mixed && rc == kSolveGaveUp;
+    int rc;
+    if constexpr (kMode == kModeLearned)
+        rc = solve_system_pcg<kU, kTeams>(B, S, T, B.cgitmax, p, red, &iters, &zeta, &rnorm,
+                                          &fallbacks);
+    else
+        rc = solve_system<kMode == kModeMixed, kU, kTeams>(B, S, T, B.cgitmax, p, red, &iters,
+                                                           &zeta, &rnorm);
+    const bool gave_up = kMode != kModeFixed && rc == kSolveGaveUp;
     if (gave_up) {
         __syncthreads();
+        fallbacks = 0;
         rc = solve_system<false, kU, kTeams>(B, S, T, kReferenceCgitmax, p, red, &iters, &zeta,
                                              &rnorm);
     }
@@ -589,7 +962,8 @@ __device__ bool run_system(const BatchArgs &B, int id, int member, const SysDesc
         B.zeta[id] = zeta;
         B.rnorm[id] = rnorm;
         B.iters[id] = iters;
-        B.status[id] = gave_up ? 1 : 0;
+        B.status[id] = gave_up ? 1 : (fallbacks > 0 ? 2 : 0);
+        if (B.fallbacks) B.fallbacks[id] = fallbacks;
     }
     return true;
 }
@@ -602,7 +976,7 @@ __device__ bool run_system(const BatchArgs &B, int id, int member, const SysDesc
 // uses the first (the loads in flight per SM are threads x kUnroll).
 // kTeams: compiled with the team exchanges (a launch whose systems all run
 // alone takes the instance without them, which needs fewer registers).
-template <bool mixed, int kMaxThreads, int kUnroll, bool kTeams>
+template <int kMode, int kMaxThreads, int kUnroll, bool kTeams>
 __global__ void __launch_bounds__(kMaxThreads, 1) batch_kernel(BatchArgs B, const int *list, int count)
 {
     extern __shared__ __align__(16) double p_sh[];
@@ -618,7 +992,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) batch_kernel(BatchArgs B, cons
         const int slot = list[k];
         const int id = slot / kMaxTeam;
         const SysDesc S = B.sys[id];
-        if (!run_system<mixed, kUnroll, kTeams>(B, id, slot % kMaxTeam, S, p_sh, red)) break;
+        if (!run_system<kMode, kUnroll, kTeams>(B, id, slot % kMaxTeam, S, p_sh, red)) break;
     }
 }
 
@@ -671,6 +1045,18 @@ struct cgb_batch {
     int *d_iters = nullptr, *d_status = nullptr;
     double *d_hx = nullptr, *d_hw = nullptr;  // Galerkin-start ring, kMaxRecycle x vec_total each
     long long vec_total = 0;
+    // learned mode: per system the factor F (lower) and F^T as CSR with BF16
+    // value bits and 16-bit columns (host copies until the next learned
+    // solve packs them), and the device arrays they are packed into
+    std::vector<std::vector<int>> h_fptr, h_ftptr;
+    std::vector<std::vector<unsigned short>> h_fcol, h_ftcol, h_fval, h_ftval;
+    std::vector<double> fmean;     // factor entries per row
+    bool prec_dirty = false;
+    int *d_fptr = nullptr, *d_ftptr = nullptr;
+    unsigned short *d_fcol = nullptr, *d_ftcol = nullptr, *d_fval = nullptr, *d_ftval = nullptr;
+    double *d_y = nullptr;
+    float *d_rg = nullptr, *d_tg = nullptr;
+    int *d_fallbacks = nullptr;
     int block = 512;
     int unroll = 4;  // 512-thread shape: 4 or 8 entries a lane in flight (1024 threads: 4)
     // lane policy: lanes = 32 if mean >= t2, 16 if >= t1, 8 if >= t0, else 4
@@ -705,6 +1091,8 @@ void batch_release(cgb_batch *b)
     bfree(b->d_queue); bfree(b->d_team_sync); bfree(b->d_team_part); bfree(b->d_dev_status);
     bfree(b->d_zeta); bfree(b->d_rnorm); bfree(b->d_iters); bfree(b->d_status);
     bfree(b->d_hx); bfree(b->d_hw);
+    bfree(b->d_fptr); bfree(b->d_ftptr); bfree(b->d_fcol); bfree(b->d_ftcol); bfree(b->d_fval);
+    bfree(b->d_ftval); bfree(b->d_y); bfree(b->d_rg); bfree(b->d_tg); bfree(b->d_fallbacks);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -737,6 +1125,7 @@ int apply_policy(cgb_batch *b, int grid)
     for (int i : b->order) {
         SysDesc &d = b->desc[i];
         d.lanes = lanes_by_policy(b, b->mean_len[i]);
+        d.flanes = b->fmean.empty() ? 4 : lanes_by_policy(b, b->fmean[i]);
         int t = 1;
         if (b->team_frac > 0.0)
             while (t < kMaxTeam && 2 * t <= grid && work[i] / t > b->team_frac * per_cta) t *= 2;
@@ -755,22 +1144,24 @@ int apply_policy(cgb_batch *b, int grid)
 // registers a thread, 1024 threads 64.
 using BatchKernel = void (*)(BatchArgs, const int *, int);
 
-template <bool mixed, bool kTeams>
+template <int kMode, bool kTeams>
 BatchKernel pick_kernel(const cgb_batch *b)
 {
-    return b->block > 512 ? batch_kernel<mixed, 1024, 4, kTeams>
-                          : (b->unroll > 4 ? batch_kernel<mixed, 512, 8, kTeams>
-                                           : batch_kernel<mixed, 512, 4, kTeams>);
+    return b->block > 512 ? batch_kernel<kMode, 1024, 4, kTeams>
+                          : (b->unroll > 4 ? batch_kernel<kMode, 512, 8, kTeams>
+                                           : batch_kernel<kMode, 512, 4, kTeams>);
 }
 
-template <bool mixed>
+template <int kMode>
 int launch_all(cgb_batch *b, const BatchArgs &A0)
 {
-    const size_t smem = sizeof(double) * size_t(b->max_n + 8);
+    // p (FP64), or in the learned mode p and the factor products' vector in
+    // FP32 (the second starting at a 16-byte boundary)
+    const size_t smem = sizeof(double) * size_t(b->max_n + 10);
     // residency does not depend on the instance (same shape, one CTA an SM
     // at most by the launch bounds); the policy then says whether any
     // system gets a team
-    BatchKernel k = pick_kernel<mixed, true>(b);
+    BatchKernel k = pick_kernel<kMode, true>(b);
     BT_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int per_sm = 0;
     BT_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, b->block, smem));
@@ -779,7 +1170,7 @@ int launch_all(cgb_batch *b, const BatchArgs &A0)
     int st = apply_policy(b, resident);
     if (st) return st;
     if (b->slots.size() == size_t(b->nsys)) {  // no teams
-        k = pick_kernel<mixed, false>(b);
+        k = pick_kernel<kMode, false>(b);
         BT_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
         int per = 0;
         BT_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, b->block, smem));
@@ -795,6 +1186,61 @@ int launch_all(cgb_batch *b, const BatchArgs &A0)
     void *args[] = {&A, &list, const_cast<int *>(&count)};
     BT_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(k), dim3(grid), dim3(b->block),
                                        args, smem, b->stream));
+    return CGB_OK;
+}
+
+// Round-to-nearest-even FP32 -> BF16 bits (NaN kept quiet).
+unsigned short bf16_bits(float f)
+{
+    unsigned u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7fffffffu) > 0x7f800000u) return static_cast<unsigned short>((u >> 16) | 0x40u);
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return static_cast<unsigned short>(u >> 16);
+}
+
+// Packs every system's factor into the device arrays (after
+// cgb_batch_set_preconditioner changed one) and allocates the learned
+// mode's vectors.  Every system must have a factor.
+int pack_factors(cgb_batch *b)
+{
+    if (!b->prec_dirty && b->d_fptr) return CGB_OK;
+    long long rows = 0, ents = 0;
+    for (int i = 0; i < b->nsys; i++) {
+        if (b->h_fptr[i].empty())
+            return set_error(CGB_ERR_STATE,
+                             "batch: learned mode needs a preconditioner for every system (system %d has none)", i);
+        rows += b->desc[i].n + 1;
+        ents += b->h_fptr[i].back();
+    }
+    bfree(b->d_fptr); bfree(b->d_ftptr); bfree(b->d_fcol); bfree(b->d_ftcol);
+    bfree(b->d_fval); bfree(b->d_ftval);
+    if (balloc(&b->d_fptr, rows) || balloc(&b->d_ftptr, rows) || balloc(&b->d_fcol, ents + 64) ||
+        balloc(&b->d_ftcol, ents + 64) || balloc(&b->d_fval, ents + 64) ||
+        balloc(&b->d_ftval, ents + 64) ||
+        (!b->d_y && (balloc(&b->d_y, b->vec_total) || balloc(&b->d_rg, b->vec_total) ||
+                     balloc(&b->d_tg, b->vec_total) || balloc(&b->d_fallbacks, b->nsys))))
+        return set_error(CGB_ERR_NOMEM, "batch: factor allocation failed");
+    b->fmean.assign(b->nsys, 0.0);
+    long long ro = 0, eo = 0;
+    for (int i = 0; i < b->nsys; i++) {
+        SysDesc &d = b->desc[i];
+        const long long ne = b->h_fptr[i].back();
+        d.f_row_off = ro;
+        d.f_off = eo;
+        b->fmean[i] = double(ne) / d.n;
+        const size_t nr = size_t(d.n) + 1;
+        BT_TRY(cudaMemcpyAsync(b->d_fptr + ro, b->h_fptr[i].data(), sizeof(int) * nr, cudaMemcpyHostToDevice, b->stream));
+        BT_TRY(cudaMemcpyAsync(b->d_ftptr + ro, b->h_ftptr[i].data(), sizeof(int) * nr, cudaMemcpyHostToDevice, b->stream));
+        BT_TRY(cudaMemcpyAsync(b->d_fcol + eo, b->h_fcol[i].data(), 2 * ne, cudaMemcpyHostToDevice, b->stream));
+        BT_TRY(cudaMemcpyAsync(b->d_ftcol + eo, b->h_ftcol[i].data(), 2 * ne, cudaMemcpyHostToDevice, b->stream));
+        BT_TRY(cudaMemcpyAsync(b->d_fval + eo, b->h_fval[i].data(), 2 * ne, cudaMemcpyHostToDevice, b->stream));
+        BT_TRY(cudaMemcpyAsync(b->d_ftval + eo, b->h_ftval[i].data(), 2 * ne, cudaMemcpyHostToDevice, b->stream));
+        ro += (long long)nr;
+        eo += ne;
+    }
+    BT_TRY(cudaStreamSynchronize(b->stream));  // the host copies may change after this
+    b->prec_dirty = false;
     return CGB_OK;
 }
 
@@ -818,7 +1264,23 @@ int launch(cgb_batch *b, const cgb_batch_params &P, double *ms)
     A.team_sync = b->d_team_sync;
     A.team_part = b->d_team_part;
     A.dev_status = b->d_dev_status;
-    A.mode = P.mode == CGB_MODE_MIXED ? 1 : 0;
+    A.mode = P.mode == CGB_MODE_MIXED ? kModeMixed
+             : P.mode == CGB_MODE_MIXED_LEARNED ? kModeLearned : kModeFixed;
+    A.fallbacks = b->d_fallbacks;  // (allocated by the first learned solve)
+    if (A.mode == kModeLearned) {
+        const int st = pack_factors(b);
+        if (st) return st;
+        A.fptr = b->d_fptr;
+        A.ftptr = b->d_ftptr;
+        A.fcol = b->d_fcol;
+        A.ftcol = b->d_ftcol;
+        A.fval = reinterpret_cast<const __nv_bfloat16 *>(b->d_fval);
+        A.ftval = reinterpret_cast<const __nv_bfloat16 *>(b->d_ftval);
+        A.y = b->d_y;
+        A.rg = b->d_rg;
+        A.tg = b->d_tg;
+        A.fallbacks = b->d_fallbacks;
+    }
     A.niter = P.niter;
     A.cgitmax = P.cgitmax;
     A.refresh_every = P.refresh_every > 0 ? P.refresh_every : 10;
@@ -832,7 +1294,9 @@ int launch(cgb_batch *b, const cgb_batch_params &P, double *ms)
     A.hstride = b->vec_total;
     A.recycle = P.recycle;
     BT_TRY(cudaEventRecord(b->ev0, b->stream));
-    const int st = A.mode == 1 ? launch_all<true>(b, A) : launch_all<false>(b, A);
+    const int st = A.mode == kModeLearned ? launch_all<kModeLearned>(b, A)
+                   : A.mode == kModeMixed ? launch_all<kModeMixed>(b, A)
+                                          : launch_all<kModeFixed>(b, A);
     if (st) return st;
     BT_TRY(cudaEventRecord(b->ev1, b->stream));
     BT_TRY(cudaStreamSynchronize(b->stream));
@@ -904,6 +1368,12 @@ int cgb_batch_create(int device, int nsys, const int *n, const int *const *rowst
     b->total_nnz = nnz_total;
     b->vec_total = vec_total;
     b->desc.resize(nsys);
+    b->h_fptr.resize(nsys);
+    b->h_ftptr.resize(nsys);
+    b->h_fcol.resize(nsys);
+    b->h_ftcol.resize(nsys);
+    b->h_fval.resize(nsys);
+    b->h_ftval.resize(nsys);
     b->mean_len.resize(nsys);
     b->nnz.resize(nsys);
     long long ro = 0, no = 0, vo = 0;
@@ -915,7 +1385,9 @@ int cgb_batch_create(int device, int nsys, const int *n, const int *const *rowst
         d.vec_off = vo;
         d.shift = shift[s];
         d.lanes = 32;
+        d.flanes = 4;
         d.team = 1;
+        d.f_row_off = d.f_off = 0;
         b->nnz[s] = rowstr[s][n[s]];
         b->mean_len[s] = double(rowstr[s][n[s]]) / n[s];
         ro += n[s] + 1;
@@ -980,10 +1452,12 @@ int cgb_batch_solve(cgb_batch *b, const cgb_batch_params *params, double *zeta, 
 {
     if (!b || !params) return set_error(CGB_ERR_INVALID, "batch: null argument");
     const cgb_batch_params P = *params;
-    if (P.niter < 1 || P.cgitmax < 1 || (P.mode != CGB_MODE_FP64 && P.mode != CGB_MODE_MIXED) ||
-        (P.mode == CGB_MODE_MIXED && !(P.tol > 0.0)) || P.recycle < 0 || P.recycle > kMaxRecycle)
+    if (P.niter < 1 || P.cgitmax < 1 ||
+        (P.mode != CGB_MODE_FP64 && P.mode != CGB_MODE_MIXED && P.mode != CGB_MODE_MIXED_LEARNED) ||
+        (P.mode != CGB_MODE_FP64 && !(P.tol > 0.0)) || P.recycle < 0 || P.recycle > kMaxRecycle)
         return set_error(CGB_ERR_INVALID,
-                         "batch: niter, cgitmax >= 1; mode FP64 or MIXED (tol > 0); recycle 0..%d",
+                         "batch: niter, cgitmax >= 1; mode FP64, MIXED or MIXED_LEARNED (tol > 0); "
+                         "recycle 0..%d",
                          kMaxRecycle);
     BT_TRY(cudaSetDevice(b->device));
     double ms = 0.0;
@@ -1075,6 +1549,86 @@ int cgb_batch_policy(cgb_batch *b, int *unroll, double *team_frac, int *teams)
         for (const SysDesc &d : b->desc) t += d.team > 1;
         *teams = t;
     }
+    return CGB_OK;
+}
+
+int cgb_batch_set_preconditioner(cgb_batch *b, int sys, const int *fptr, const int *fcol,
+                                 const double *fval)
+{
+    if (!b || !fptr || !fcol || !fval) return set_error(CGB_ERR_INVALID, "batch: null argument");
+    if (sys < 0 || sys >= b->nsys) return set_error(CGB_ERR_INVALID, "batch: no system %d", sys);
+    const int n = b->desc[sys].n;
+    if (fptr[0] != 0) return set_error(CGB_ERR_BAD_MATRIX, "factor: fptr[0] != 0");
+    for (int i = 0; i < n; i++) {
+        if (fptr[i + 1] < fptr[i]) return set_error(CGB_ERR_BAD_MATRIX, "factor: fptr decreases at %d", i);
+        bool diag = false;
+        for (int k = fptr[i]; k < fptr[i + 1]; k++) {
+            if (fcol[k] < 0 || fcol[k] > i)
+                return set_error(CGB_ERR_BAD_MATRIX, "factor: entry (%d, %d) not in the lower triangle", i, fcol[k]);
+            if (!std::isfinite(fval[k])) return set_error(CGB_ERR_NUMERIC, "factor: non-finite value in row %d", i);
+            if (fcol[k] == i) {
+                if (!(fval[k] > 0.0)) return set_error(CGB_ERR_NUMERIC, "factor: diagonal of row %d not positive", i);
+                diag = true;
+            }
+        }
+        if (!diag) return set_error(CGB_ERR_BAD_MATRIX, "factor: row %d has no diagonal", i);
+    }
+    // rows in ascending column order, repeated columns summed, values to BF16
+    std::vector<int> optr(n + 1, 0), ocol;
+    std::vector<float> oval;
+    std::vector<std::pair<int, double>> row;
+    for (int i = 0; i < n; i++) {
+        row.clear();
+        for (int k = fptr[i]; k < fptr[i + 1]; k++) row.emplace_back(fcol[k], fval[k]);
+        std::stable_sort(row.begin(), row.end(), [](const std::pair<int, double> &x,
+                                                    const std::pair<int, double> &y) {
+            return x.first < y.first;
+        });
+        for (size_t k = 0; k < row.size(); k++) {
+            if (k > 0 && row[k].first == row[k - 1].first) {
+                row[k].second += row[k - 1].second;
+                ocol.pop_back();
+                oval.pop_back();
+            }
+            ocol.push_back(row[k].first);
+            oval.push_back(float(row[k].second));
+        }
+        optr[i + 1] = int(ocol.size());
+    }
+    const int nf = optr[n];
+    std::vector<int> tptr(n + 1, 0);
+    for (int k = 0; k < nf; k++) tptr[ocol[k] + 1]++;
+    for (int i = 0; i < n; i++) tptr[i + 1] += tptr[i];
+    std::vector<unsigned short> tcol(nf), tval(nf), fc(nf), fv(nf);
+    std::vector<int> cur(tptr.begin(), tptr.end() - 1);
+    for (int i = 0; i < n; i++)
+        for (int k = optr[i]; k < optr[i + 1]; k++) {
+            const unsigned short bits = bf16_bits(oval[k]);
+            fc[k] = static_cast<unsigned short>(ocol[k]);
+            fv[k] = bits;
+            const int at = cur[ocol[k]]++;
+            tcol[at] = static_cast<unsigned short>(i);
+            tval[at] = bits;
+        }
+    b->h_fptr[sys] = std::move(optr);
+    b->h_ftptr[sys] = std::move(tptr);
+    b->h_fcol[sys] = std::move(fc);
+    b->h_fval[sys] = std::move(fv);
+    b->h_ftcol[sys] = std::move(tcol);
+    b->h_ftval[sys] = std::move(tval);
+    b->prec_dirty = true;
+    return CGB_OK;
+}
+
+int cgb_batch_fallbacks(cgb_batch *b, int *fallbacks)
+{
+    if (!b || !fallbacks) return set_error(CGB_ERR_INVALID, "batch: null argument");
+    if (!b->d_fallbacks) {
+        std::fill(fallbacks, fallbacks + b->nsys, 0);
+        return CGB_OK;
+    }
+    BT_TRY(cudaSetDevice(b->device));
+    BT_TRY(cudaMemcpy(fallbacks, b->d_fallbacks, sizeof(int) * b->nsys, cudaMemcpyDeviceToHost));
     return CGB_OK;
 }
 

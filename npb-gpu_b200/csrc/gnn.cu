@@ -902,6 +902,44 @@ int cgb_gnn_infer(cgb_gnn *m, cgb_gnn_graph *g, float *goff_host, float *gdiag_h
     return CGB_OK;
 }
 
+// F = G / sqrt(delta) on the lower pattern of A (strictly lower entries in
+// column order, then the diagonal) as CSR.
+static int learned_factor(cgb_gnn *m, cgb_gnn_graph *g, std::vector<int> &fptr,
+                          std::vector<int> &fcol, std::vector<double> &fval)
+{
+    const int n = g->n;
+    std::vector<float> goff(g->nnz_low), gdiag(n);
+    int st = cgb_gnn_infer(m, g, goff.data(), gdiag.data());
+    if (st) return st;
+    fptr.assign(n + 1, 0);
+    fcol.assign(g->nnz_low + n, 0);
+    fval.assign(g->nnz_low + n, 0.0);
+    long long at = 0;
+    for (int i = 0; i < n; i++) {
+        fptr[i] = int(at);
+        for (int k = g->h_low_ptr[i]; k < g->h_low_ptr[i + 1]; k++) {
+            const int j = g->h_low_col[k];
+            fcol[at] = j;
+            fval[at++] = double(goff[k]) * g->dscale[j];
+        }
+        fcol[at] = i;
+        fval[at++] = double(gdiag[i]) * g->dscale[i];
+    }
+    fptr[n] = int(at);
+    return CGB_OK;
+}
+
+// The learned factor as system `sys`'s preconditioner in a batch.
+int cgb_gnn_attach_batch(cgb_gnn *m, cgb_gnn_graph *g, cgb_batch *b, int sys)
+{
+    if (!m || !g || !b) return set_error(CGB_ERR_INVALID, "bad arguments");
+    std::vector<int> fptr, fcol;
+    std::vector<double> fval;
+    int st = learned_factor(m, g, fptr, fcol, fval);
+    if (st) return st;
+    return cgb_batch_set_preconditioner(b, sys, fptr.data(), fcol.data(), fval.data());
+}
+
 // Learned preconditioner into a session: F = G / sqrt(delta) on the lower
 // pattern of A (strictly lower entries in column order, then the diagonal).
 int cgb_gnn_attach(cgb_gnn *m, cgb_gnn_graph *g, cgb_session *s)

@@ -169,6 +169,11 @@ _SIGNATURES = {
                                         ctypes.POINTER(ctypes.c_double),
                                         ctypes.POINTER(ctypes.c_int)]),
     "cgb_batch_set_team_frac": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "cgb_batch_set_preconditioner": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _I32, _I32,
+                                                    _F64]),
+    "cgb_batch_fallbacks": (ctypes.c_int, [ctypes.c_void_p, _I32]),
+    "cgb_gnn_attach_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_int]),
     "cgb_host_alloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_longlong]),
     "cgb_host_free": (ctypes.c_int, [ctypes.c_void_p]),
     "cgb_device_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
@@ -695,6 +700,33 @@ class Batch:
         u, f, t = ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
         _check(lib().cgb_batch_policy(self._h, ctypes.byref(u), ctypes.byref(f), ctypes.byref(t)))
         return dict(unroll=u.value, team_frac=f.value, teams=t.value)
+
+    def set_preconditioner(self, sys, fptr, fcol, fval):
+        """M = F^T F for system `sys` in the learned mode (F lower CSR with a
+        positive diagonal; stored with BF16 values)."""
+        _check(lib().cgb_batch_set_preconditioner(self._h, int(sys),
+                                                  np.ascontiguousarray(fptr, np.int32),
+                                                  np.ascontiguousarray(fcol, np.int32),
+                                                  np.ascontiguousarray(fval, np.float64)))
+
+    def attach_learned(self, model):
+        """The network's factor F = G / sqrt(delta) for every system (one
+        inference per system matrix)."""
+        for i, (rs, ci, a) in enumerate(self._keep):
+            with model.graph(rs, ci, a) as g:
+                _check(lib().cgb_gnn_attach_batch(model._h, g._h, self._h, i))
+
+    def attach_identity(self):
+        """F = I for every system: the learned mode's kernel without the
+        network (plain CG in the preconditioned solver)."""
+        for i, (rs, _, _) in enumerate(self._keep):
+            self.set_preconditioner(i, *identity_factor(len(rs) - 1))
+
+    def fallbacks(self):
+        """Per system: outer steps of the last learned solve that fell back to plain CG."""
+        out = np.zeros(self.nsys, np.int32)
+        _check(lib().cgb_batch_fallbacks(self._h, out))
+        return out
 
     def set_team_frac(self, frac):
         """0: every system on one CTA; larger systems get teams of CTAs below

@@ -164,3 +164,96 @@ def test_batch_rejects_oversize(cgb):
     with pytest.raises(cgb.CgbError) as e:
         cgb.Batch([(rs, np.zeros(0, np.int32), np.zeros(0))], [1.0])
     assert e.value.status == cgb.ERR_CAPACITY
+
+
+# ------------------------------------------------------------ learned mode
+def learned_model(cgb):
+    import os
+    if not os.path.exists(cgb.WEIGHTS_PATH):
+        pytest.skip("no trained weights")
+    m = cgb.Gnn()
+    m.load()
+    return m
+
+
+def test_batch_learned_against_fp64_reference(cgb):
+    """CGB_MODE_MIXED_LEARNED with the trained network's factor per system:
+    zeta relative 1e-10 against the FP64 reference algorithm of the same
+    batch wherever that one converged; indefinite systems give up and are
+    re-solved with the reference algorithm (bit-identical); the network
+    needs fewer inner iterations than the unpreconditioned mixed mode on
+    the systems both solved."""
+    specs = cgb.uneven_batch_specs(nsys=48, seed=7, n_range=(1400, 8000))
+    systems, shifts = build(cgb, specs)
+    model = learned_model(cgb)
+    with cgb.Batch(systems, shifts) as b:
+        fp64 = b.solve(niter=15)
+        mixed = b.solve(niter=15, mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=200)
+        b.attach_learned(model)
+        lrn = b.solve(niter=15, mode=cgb.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=200)
+        fb = b.fallbacks()
+    model.close()
+    converged = fp64["rnorm"] <= 1e-10
+    rel = np.abs(lrn["zeta"] - fp64["zeta"]) / np.abs(fp64["zeta"])
+    ok = converged & (lrn["status"] != 1)
+    assert ok.sum() >= 10
+    assert np.all(rel[ok] <= 1e-10), rel[ok].max()
+    fell = lrn["status"] == 1
+    assert np.array_equal(lrn["zeta"][fell], fp64["zeta"][fell])
+    # the same systems are indefinite in both preconditioned and plain mixed
+    assert np.array_equal(fell, mixed["status"] == 1)
+    assert np.all((lrn["status"] == 2) == (fb > 0))
+    both = ok & (mixed["status"] == 0)
+    assert lrn["iters"][both].sum() < mixed["iters"][both].sum()
+
+
+def test_batch_learned_identity_factor_is_plain_cg(cgb):
+    """F = I: the preconditioned solver is plain CG, so it takes the mixed
+    mode's iterations (to within a few per cent: the products round
+    differently) and reaches the same zeta."""
+    specs = cgb.uneven_batch_specs(nsys=24, seed=5, n_range=(1400, 6000))
+    systems, shifts = build(cgb, specs)
+    with cgb.Batch(systems, shifts) as b:
+        b.set_team_frac(0.0)
+        mixed = b.solve(niter=15, mode=cgb.MODE_MIXED, tol=1e-12, cgitmax=200)
+        b.attach_identity()
+        ident = b.solve(niter=15, mode=cgb.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=200)
+    assert np.array_equal(ident["status"] == 1, mixed["status"] == 1)
+    ok = mixed["status"] == 0
+    rel = np.abs(ident["zeta"][ok] - mixed["zeta"][ok]) / np.abs(mixed["zeta"][ok])
+    assert np.all(rel <= 1e-10)
+    a, m = ident["iters"][ok].sum(), mixed["iters"][ok].sum()
+    assert abs(a - m) <= 0.05 * m
+
+
+def test_batch_learned_teams_agree(cgb):
+    """Teams of CTAs (the largest systems split over 2-8 CTAs that exchange
+    the FP32 vectors through global memory) against every system on one
+    CTA: zeta relative 1e-10."""
+    specs = cgb.uneven_batch_specs(nsys=16, seed=9, n_range=(6000, 20000))
+    systems, shifts = build(cgb, specs)
+    model = learned_model(cgb)
+    with cgb.Batch(systems, shifts) as b:
+        b.attach_learned(model)
+        b.set_team_frac(0.0)
+        solo = b.solve(niter=15, mode=cgb.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=200)
+        b.set_team_frac(0.05)
+        team = b.solve(niter=15, mode=cgb.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=200)
+        assert b.policy()["teams"] > 0
+    model.close()
+    assert np.array_equal(solo["status"] == 1, team["status"] == 1)
+    rel = np.abs(solo["zeta"] - team["zeta"]) / np.abs(solo["zeta"])
+    assert np.all(rel <= 1e-10), rel.max()
+
+
+def test_batch_learned_needs_every_factor(cgb):
+    specs = [(1400, 7, 10.0, 314159265.0), (2000, 9, 12.0, 271828183.0)]
+    systems, shifts = build(cgb, specs)
+    with cgb.Batch(systems, shifts) as b:
+        b.set_preconditioner(0, *cgb.identity_factor(1400))
+        with pytest.raises(cgb.CgbError) as e:
+            b.solve(niter=2, mode=cgb.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=50)
+        assert e.value.status == cgb.ERR_STATE
+        with pytest.raises(cgb.CgbError) as e:
+            b.set_preconditioner(1, np.zeros(2001, np.int32), np.zeros(0, np.int32), np.zeros(0))
+        assert e.value.status == cgb.ERR_BAD_MATRIX
