@@ -184,8 +184,9 @@ int cgb_power_iterate(cgb_session *s, const cgb_solve_params *params, double *ze
 /* Installs the preconditioner of CGB_MODE_MIXED_LEARNED: the factor F of
  * M = F^T F, which approximates (-A)^-1 (A is negative definite; the solver
  * runs CG on -A).  F is lower triangular in CSR (n+1 row pointers, columns
- * <= row, every row holding a positive diagonal), FP64 values stored FP32 on
- * the device.  The learned factor is G diag(-A)^-1/2 with G from
+ * <= row, every row holding a positive diagonal).  On the device the
+ * values are FP32 (row plan) or BF16 in sliced copies that gather a BF16
+ * vector (sliced plan).  The learned factor is G diag(-A)^-1/2 with G from
  * cgb_gnn_infer; F = diag(-A)^-1/2 is Jacobi.  No counterpart in the
  * reference. */
 int cgb_set_preconditioner(cgb_session *s, const int *fptr, const int *fcol, const double *fval);
@@ -288,7 +289,8 @@ int cgb_batch_set_team_frac(cgb_batch *b, double team_frac);
 /* The preconditioner of system `sys` in CGB_MODE_MIXED_LEARNED: M = F^T F with
  * F lower triangular in CSR (n+1 row pointers, columns <= row, a positive
  * diagonal in every row), as cgb_set_preconditioner takes it; stored with
- * BF16 values and 16-bit columns.  Every system needs one before a learned
+ * the diagonal in FP32 and the other entries as BF16 values with 16-bit
+ * columns.  Every system needs one before a learned
  * solve (the learned factor is G diag(-A)^-1/2 with G from cgb_gnn_infer;
  * cgb_gnn_attach_batch installs it).  In the solve, both factor products
  * gather from a shared-memory copy of the vector.  No counterpart in the

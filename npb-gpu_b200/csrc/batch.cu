@@ -25,9 +25,10 @@
 //          with the reference needs the reference's own iteration there.)
 //   learned  the mixed mode preconditioned by M = F^T F per system (F lower
 //          triangular with a positive diagonal, cgb_batch_set_preconditioner:
-//          the learned factor G diag(-A)^-1/2), CG on -A; the factor's values
-//          are BF16 with 16-bit columns, both factor products gather from a
-//          shared-memory copy of the vector.  An outer step whose
+//          the learned factor G diag(-A)^-1/2), CG on -A; the factor's
+//          off-diagonal values are BF16 with 16-bit columns, its diagonal
+//          FP32 (applied to FP64 vectors); both factor products gather from
+//          a shared-memory copy of the vector.  An outer step whose
 //          preconditioned iteration stalls (|r|^2 not halved in four steps,
 //          or r.y <= 0) continues as plain CG; a system showing p.Ap >= 0 is
 //          re-solved with the FP64 reference algorithm, as in the mixed mode.
@@ -109,6 +110,7 @@ struct BatchArgs {
     const int *fptr, *ftptr;
     const unsigned short *fcol, *ftcol;
     const __nv_bfloat16 *fval, *ftval;
+    const float *fdiag;  // the factor's diagonal (FP32, at f_row_off), kept out of the CSR
     double *y;
     float *rg, *tg;
     int *fallbacks;
@@ -600,16 +602,17 @@ __device__ int solve_system(const BatchArgs &B, const SysDesc &S, Team &T, int c
     return kSolveOk;
 }
 
-// One factor product for rows [lo, hi): out[row] = sum_k val[k] v[col[k]]
-// (BF16 values widened to FP32, 16-bit columns, v an FP32 vector in shared
-// memory, FP32 row sums) with `lanes` lanes a row, written as FP32 (out32)
-// and/or FP64 (out64); returns this thread's share of sum dot[row] out[row]
-// (dot may be null).
+// One factor product for rows [lo, hi): out[row] = sum_k val[k] v[col[k]] +
+// diag[row] dvec[row] -- the off-diagonal entries (BF16 values widened to
+// FP32, 16-bit columns, v an FP32 vector in shared memory, FP32 row sums)
+// and the diagonal (FP32) times an FP64 vector -- with `lanes` lanes a row,
+// written as FP32 (out32) and/or FP64 (out64); returns this thread's share
+// of sum dot[row] out[row] (dot may be null).
 template <int kU>
 __device__ __forceinline__ double sys_fprod(const int *ptr, const unsigned short *col,
                                             const __nv_bfloat16 *val, int lanes, int lo, int hi,
-                                            const float *v, float *out32, double *out64,
-                                            const double *dot)
+                                            const float *v, const float *diag, const double *dvec,
+                                            float *out32, double *out64, const double *dot)
 {
     const int LPR = lanes;
     const int lane = threadIdx.x & (LPR - 1), grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
@@ -636,9 +639,10 @@ __device__ __forceinline__ double sys_fprod(const int *ptr, const unsigned short
         }
         s = group_sum_f_rt(s, mask, LPR);
         if (lane == 0) {
-            if (out32) out32[row] = s;
-            if (out64) out64[row] = double(s);
-            if (dot) dacc = fma(dot[row], double(s), dacc);
+            const double t = fma(double(diag[row]), dvec[row], double(s));
+            if (out32) out32[row] = float(t);
+            if (out64) out64[row] = t;
+            if (dot) dacc = fma(dot[row], t, dacc);
         }
     }
     return dacc;
@@ -659,6 +663,7 @@ __device__ __forceinline__ void team_gather_f(const Team &T, const float *g, flo
 struct PcgSys {
     double *x, *z, *r, *q, *pg, *y;
     float *rg, *tg, *p32, *v32;
+    const float *fdiag;
     const int *fptr, *ftptr;
     const unsigned short *fcol, *ftcol;
     const __nv_bfloat16 *fval, *ftval;
@@ -675,8 +680,9 @@ __device__ __forceinline__ bool pcg_apply(const BatchArgs &B, const SysDesc &S, 
     const bool team = T.size > 1;
     double dacc = 0.0;
     if (use) {
-        // t = F r' (own rows) to the global copy
-        sys_fprod<kU>(V.fptr, V.fcol, V.fval, S.flanes, lo, hi, V.v32, V.tg, nullptr, nullptr);
+        // t = F r' (own rows) to the global copy, and in FP64 to q
+        sys_fprod<kU>(V.fptr, V.fcol, V.fval, S.flanes, lo, hi, V.v32, V.fdiag, V.r, V.tg, V.q,
+                      nullptr);
         // every row of t into v32, once every thread (and member) is done with r'
         if (team) {
             if (!team_barrier(team_mem(B, T.id), T)) return false;
@@ -687,7 +693,8 @@ __device__ __forceinline__ bool pcg_apply(const BatchArgs &B, const SysDesc &S, 
         }
         __syncthreads();
         // y = F^T t (own rows), with the r'.y share
-        dacc = sys_fprod<kU>(V.ftptr, V.ftcol, V.ftval, S.flanes, lo, hi, V.v32, nullptr, V.y, V.r);
+        dacc = sys_fprod<kU>(V.ftptr, V.ftcol, V.ftval, S.flanes, lo, hi, V.v32, V.fdiag, V.q,
+                             nullptr, V.y, V.r);
     } else {
         for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
             const double rv = V.r[j];
@@ -746,6 +753,7 @@ __device__ int solve_system_pcg(const BatchArgs &B, const SysDesc &S, Team &T, i
     V.tg = B.tg + S.vec_off;
     V.p32 = reinterpret_cast<float *>(smem);
     V.v32 = V.p32 + ((n + 8 + 3) & ~3);
+    V.fdiag = B.fdiag + S.f_row_off;
     V.fptr = B.fptr + S.f_row_off;
     V.ftptr = B.ftptr + S.f_row_off;
     V.fcol = B.fcol + S.f_off;
@@ -1050,9 +1058,11 @@ struct cgb_batch {
     // solve packs them), and the device arrays they are packed into
     std::vector<std::vector<int>> h_fptr, h_ftptr;
     std::vector<std::vector<unsigned short>> h_fcol, h_ftcol, h_fval, h_ftval;
+    std::vector<std::vector<float>> h_fdiag;
     std::vector<double> fmean;     // factor entries per row
     bool prec_dirty = false;
     int *d_fptr = nullptr, *d_ftptr = nullptr;
+    float *d_fdiag = nullptr;
     unsigned short *d_fcol = nullptr, *d_ftcol = nullptr, *d_fval = nullptr, *d_ftval = nullptr;
     double *d_y = nullptr;
     float *d_rg = nullptr, *d_tg = nullptr;
@@ -1092,7 +1102,7 @@ void batch_release(cgb_batch *b)
     bfree(b->d_zeta); bfree(b->d_rnorm); bfree(b->d_iters); bfree(b->d_status);
     bfree(b->d_hx); bfree(b->d_hw);
     bfree(b->d_fptr); bfree(b->d_ftptr); bfree(b->d_fcol); bfree(b->d_ftcol); bfree(b->d_fval);
-    bfree(b->d_ftval); bfree(b->d_y); bfree(b->d_rg); bfree(b->d_tg); bfree(b->d_fallbacks);
+    bfree(b->d_ftval); bfree(b->d_fdiag); bfree(b->d_y); bfree(b->d_rg); bfree(b->d_tg); bfree(b->d_fallbacks);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -1214,8 +1224,9 @@ int pack_factors(cgb_batch *b)
         ents += b->h_fptr[i].back();
     }
     bfree(b->d_fptr); bfree(b->d_ftptr); bfree(b->d_fcol); bfree(b->d_ftcol);
-    bfree(b->d_fval); bfree(b->d_ftval);
-    if (balloc(&b->d_fptr, rows) || balloc(&b->d_ftptr, rows) || balloc(&b->d_fcol, ents + 64) ||
+    bfree(b->d_fval); bfree(b->d_ftval); bfree(b->d_fdiag);
+    if (balloc(&b->d_fptr, rows) || balloc(&b->d_ftptr, rows) || balloc(&b->d_fdiag, rows) ||
+        balloc(&b->d_fcol, ents + 64) ||
         balloc(&b->d_ftcol, ents + 64) || balloc(&b->d_fval, ents + 64) ||
         balloc(&b->d_ftval, ents + 64) ||
         (!b->d_y && (balloc(&b->d_y, b->vec_total) || balloc(&b->d_rg, b->vec_total) ||
@@ -1228,10 +1239,11 @@ int pack_factors(cgb_batch *b)
         const long long ne = b->h_fptr[i].back();
         d.f_row_off = ro;
         d.f_off = eo;
-        b->fmean[i] = double(ne) / d.n;
+        b->fmean[i] = double(ne) / d.n;  // off-diagonal entries a row
         const size_t nr = size_t(d.n) + 1;
         BT_TRY(cudaMemcpyAsync(b->d_fptr + ro, b->h_fptr[i].data(), sizeof(int) * nr, cudaMemcpyHostToDevice, b->stream));
         BT_TRY(cudaMemcpyAsync(b->d_ftptr + ro, b->h_ftptr[i].data(), sizeof(int) * nr, cudaMemcpyHostToDevice, b->stream));
+        BT_TRY(cudaMemcpyAsync(b->d_fdiag + ro, b->h_fdiag[i].data(), sizeof(float) * d.n, cudaMemcpyHostToDevice, b->stream));
         BT_TRY(cudaMemcpyAsync(b->d_fcol + eo, b->h_fcol[i].data(), 2 * ne, cudaMemcpyHostToDevice, b->stream));
         BT_TRY(cudaMemcpyAsync(b->d_ftcol + eo, b->h_ftcol[i].data(), 2 * ne, cudaMemcpyHostToDevice, b->stream));
         BT_TRY(cudaMemcpyAsync(b->d_fval + eo, b->h_fval[i].data(), 2 * ne, cudaMemcpyHostToDevice, b->stream));
@@ -1272,6 +1284,7 @@ int launch(cgb_batch *b, const cgb_batch_params &P, double *ms)
         if (st) return st;
         A.fptr = b->d_fptr;
         A.ftptr = b->d_ftptr;
+        A.fdiag = b->d_fdiag;
         A.fcol = b->d_fcol;
         A.ftcol = b->d_ftcol;
         A.fval = reinterpret_cast<const __nv_bfloat16 *>(b->d_fval);
@@ -1369,6 +1382,7 @@ int cgb_batch_create(int device, int nsys, const int *n, const int *const *rowst
     b->vec_total = vec_total;
     b->desc.resize(nsys);
     b->h_fptr.resize(nsys);
+    b->h_fdiag.resize(nsys);
     b->h_ftptr.resize(nsys);
     b->h_fcol.resize(nsys);
     b->h_ftcol.resize(nsys);
@@ -1573,9 +1587,11 @@ int cgb_batch_set_preconditioner(cgb_batch *b, int sys, const int *fptr, const i
         }
         if (!diag) return set_error(CGB_ERR_BAD_MATRIX, "factor: row %d has no diagonal", i);
     }
-    // rows in ascending column order, repeated columns summed, values to BF16
+    // rows in ascending column order, repeated columns summed; the diagonal
+    // (FP32) apart, the rest to BF16 (rounding the diagonal, ~1, to BF16
+    // would perturb M about as much as the off-diagonal part corrects)
     std::vector<int> optr(n + 1, 0), ocol;
-    std::vector<float> oval;
+    std::vector<float> oval, dg(n, 0.f);
     std::vector<std::pair<int, double>> row;
     for (int i = 0; i < n; i++) {
         row.clear();
@@ -1593,6 +1609,9 @@ int cgb_batch_set_preconditioner(cgb_batch *b, int sys, const int *fptr, const i
             ocol.push_back(row[k].first);
             oval.push_back(float(row[k].second));
         }
+        dg[i] = oval.back();  // the diagonal: the last of the ascending columns <= i
+        ocol.pop_back();
+        oval.pop_back();
         optr[i + 1] = int(ocol.size());
     }
     const int nf = optr[n];
@@ -1610,6 +1629,7 @@ int cgb_batch_set_preconditioner(cgb_batch *b, int sys, const int *fptr, const i
             tcol[at] = static_cast<unsigned short>(i);
             tval[at] = bits;
         }
+    b->h_fdiag[sys] = std::move(dg);
     b->h_fptr[sys] = std::move(optr);
     b->h_ftptr[sys] = std::move(tptr);
     b->h_fcol[sys] = std::move(fc);

@@ -52,9 +52,11 @@ struct OuterArgs {
     MatrixView M;
     double *x, *z, *p, *q, *r;
     float *p32;                         // FP32 search vector (mixed modes)
-    float *r32;                         // FP32 residual (preconditioned mode)
+    float *r32;                         // FP32 residual (preconditioned mode, row plan)
+    __nv_bfloat16 *r16, *t16;           // BF16 residual and F r (preconditioned mode, sliced plan)
     double *y;                          // preconditioned residual (preconditioned mode)
-    MatrixView F, FT;                   // preconditioner factor F (lower) and F^T, FP32
+    MatrixView F, FT;                   // preconditioner factor F (lower) and F^T (FP32 CSR;
+                                        // BF16 sliced copies)
     const int *__restrict__ row_split;  // gridDim.x + 1 entries
     double *part;                       // kSlotCount * gpad
     int gpad;
@@ -554,7 +556,9 @@ __device__ __forceinline__ void outer_step_mixed_body(const OuterArgs &A)
 //    interleaving gives every CTA a fair sample of row lengths.  Their
 //    values are stored in BF16 (4 bytes an entry with the 16-bit column;
 //    products and sums in FP32): M = F~^T F~ of the rounded factor is still
-//    SPD and the same operator in every application.  The F^T product fuses
+//    SPD.  The vectors they gather (r, then F r) are staged in BF16 too, so
+//    a 96 KB slot holds a 49152-column block (4 blocks at class C, not 7);
+//    rounding them measured no extra iterations on these matrices.  The F^T product fuses
 //    the r.y partial over the rows it computes.
 //  - row policy: CSR rows of F and F^T with LPRG lanes per row over the
 //    CTA's own rows.
@@ -568,19 +572,19 @@ __device__ __forceinline__ bool apply_prec(Spmv &sp, const OuterArgs &A, int row
     if (use) {
         if constexpr (Spmv::kSliced) {
             bool ok = true;
-            (void)sp.template apply<float, __nv_bfloat16>(A.F, A.r32, A.q, nullptr, A.n,
-                                                          A.gb.limit_ns, A.gb.status,
-                                                          ok);  // t = F r (interleaved rows)
+            (void)sp.template apply<__nv_bfloat16, __nv_bfloat16>(
+                A.F, A.r16, A.q, nullptr, A.n, A.gb.limit_ns, A.gb.status,
+                ok);  // t = F r (interleaved rows)
             if (!ok) return false;
             const int G = gridDim.x, nr = interleaved_rows(A.n, blockIdx.x, G);
             for (int i = threadIdx.x; i < nr; i += blockDim.x) {
                 const int j = blockIdx.x + G * i;
-                A.p32[j] = float(A.q[j]);
+                A.t16[j] = __float2bfloat16_rn(float(A.q[j]));
             }
             if (!grid_barrier(A.gb)) return false;
-            acc = sp.template apply<float, __nv_bfloat16>(A.FT, A.p32, A.y, A.r, A.n,
-                                                          A.gb.limit_ns, A.gb.status,
-                                                          ok);  // y = F^T t, r.y
+            acc = sp.template apply<__nv_bfloat16, __nv_bfloat16>(
+                A.FT, A.t16, A.y, A.r, A.n, A.gb.limit_ns, A.gb.status,
+                ok);  // y = F^T t, r.y
             if (!ok) return false;
         } else {
             spmv_rows<LPRG, float>(A.F, A.r32, A.q, row0, row1, nullptr);  // t = F r
@@ -603,6 +607,16 @@ __device__ __forceinline__ bool apply_prec(Spmv &sp, const OuterArgs &A, int row
     return true;
 }
 
+// r' in the precision the factor products gather: BF16 for the sliced
+// copies (rounding the gathered vector to BF16 measured no extra
+// iterations on these matrices), FP32 for the row plan.
+template <class Spmv>
+__device__ __forceinline__ void put_r_lowp(const OuterArgs &A, int j, double rv)
+{
+    if constexpr (Spmv::kSliced) A.r16[j] = __float2bfloat16_rn(float(rv));
+    else A.r32[j] = float(rv);
+}
+
 template <class Spmv, int LPRG>
 __device__ __forceinline__ void outer_step_pcg_body(const OuterArgs &A)
 {
@@ -623,7 +637,7 @@ __device__ __forceinline__ void outer_step_pcg_body(const OuterArgs &A)
         for (int j = row0 + threadIdx.x; j < vend; j += blockDim.x) {
             const double rv = A.q[j] - A.x[j];
             A.r[j] = rv;
-            A.r32[j] = float(rv);
+            put_r_lowp<Spmv>(A, j, rv);
             if (j < A.n) acc = fma(rv, rv, acc);
         }
     } else {
@@ -633,7 +647,7 @@ __device__ __forceinline__ void outer_step_pcg_body(const OuterArgs &A)
             A.q[j] = 0.0;
             A.z[j] = 0.0;
             A.r[j] = -xv;
-            A.r32[j] = float(-xv);
+            put_r_lowp<Spmv>(A, j, -xv);
             if (j < A.n) acc = fma(xv, xv, acc);
         }
     }
@@ -676,7 +690,7 @@ __device__ __forceinline__ void outer_step_pcg_body(const OuterArgs &A)
             for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) {
                 const double rv = A.r[j] - A.x[j];
                 A.r[j] = rv;
-                A.r32[j] = float(rv);
+                put_r_lowp<Spmv>(A, j, rv);
                 acc = fma(rv, rv, acc);
             }
             put_partial(A, kSlotRho, acc, scratch);
@@ -701,7 +715,7 @@ __device__ __forceinline__ void outer_step_pcg_body(const OuterArgs &A)
                 A.z[j] = fma(alpha, A.p[j], A.z[j]);
                 const double rv = fma(alpha, A.q[j], A.r[j]);  // r' -= alpha A'p
                 A.r[j] = rv;
-                A.r32[j] = float(rv);
+                put_r_lowp<Spmv>(A, j, rv);
                 acc = fma(rv, rv, acc);
             }
             put_partial(A, kSlotRho, acc, scratch);

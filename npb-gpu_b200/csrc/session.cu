@@ -243,6 +243,7 @@ struct cgb_session {
     double *d_vec = nullptr;
     float *d_p32 = nullptr;
     float *d_r32 = nullptr;
+    __nv_bfloat16 *d_r16 = nullptr, *d_t16 = nullptr;  // the sliced factor products' vectors
     double *d_y = nullptr;
     double *d_hx = nullptr, *d_hw = nullptr;  // Galerkin-start ring: kMaxRecycle vectors each
     size_t vstride = 0;
@@ -382,6 +383,8 @@ void release(cgb_session *s)
     dev_free(s->d_vec);
     dev_free(s->d_p32);
     dev_free(s->d_r32);
+    dev_free(s->d_r16);
+    dev_free(s->d_t16);
     dev_free(s->d_y);
     dev_free(s->d_hx);
     dev_free(s->d_hw);
@@ -466,6 +469,8 @@ OuterArgs outer_args(cgb_session *s)
     A.r = s->r();
     A.p32 = s->d_p32;
     A.r32 = s->d_r32;
+    A.r16 = s->d_r16;
+    A.t16 = s->d_t16;
     A.y = s->d_y;
     A.F.rowstr = s->d_f_ptr;
     A.F.colidx = s->d_f_col;
@@ -1311,6 +1316,10 @@ int create_shell(int n, const cgb_options *opts, cgb_session **out)
     CREATE_TRY(cudaMemsetAsync(s->d_p32, 0, sizeof(float) * s->vstride, s->stream));
     CREATE_TRY(dev_alloc(&s->d_r32, s->vstride));
     CREATE_TRY(cudaMemsetAsync(s->d_r32, 0, sizeof(float) * s->vstride, s->stream));
+    CREATE_TRY(dev_alloc(&s->d_r16, s->vstride));
+    CREATE_TRY(cudaMemsetAsync(s->d_r16, 0, 2 * s->vstride, s->stream));
+    CREATE_TRY(dev_alloc(&s->d_t16, s->vstride));
+    CREATE_TRY(cudaMemsetAsync(s->d_t16, 0, 2 * s->vstride, s->stream));
     CREATE_TRY(dev_alloc(&s->d_y, s->vstride));
     CREATE_TRY(cudaMemsetAsync(s->d_y, 0, sizeof(double) * s->vstride, s->stream));
     CREATE_TRY(dev_alloc(&s->d_hx, kMaxRecycle * s->vstride));

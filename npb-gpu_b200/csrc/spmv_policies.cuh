@@ -28,7 +28,9 @@
 //                  loads; each row accumulates in registers, then into one of
 //                  two shared accumulators (by block parity: blocks b and b+1
 //                  may run at once, b+2 only after all of b), summed at the
-//                  end -- deterministic.
+//                  end -- deterministic.  The preconditioner's factor copies
+//                  gather a BF16 vector (FP32 row sums), so a staged block
+//                  spans twice the columns.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -115,6 +117,17 @@ __device__ __forceinline__ ushort2 ld_stream(const ushort2 *p, uint64_t pol)
 
 __device__ __forceinline__ double fma_vt(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float fma_vt(float a, float b, float c) { return fmaf(a, b, c); }
+
+// Row-sum type of a gathered vector type: FP64 and FP32 sum in their own
+// precision, a BF16 vector (the factor products) in FP32.
+template <typename VT>
+struct SumType {
+    using T = VT;
+};
+template <>
+struct SumType<__nv_bfloat16> {
+    using T = float;
+};
 
 template <int W, typename VT>
 __device__ __forceinline__ VT group_sum_vt(VT v, unsigned mask)
@@ -355,7 +368,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, long l
 // staging (2 slots of 12288 doubles, or up to 4 slots of 12288 floats) and
 // one accumulator of max_rows doubles per slot in use.
 constexpr int kSliceWidth = 12288;  // columns per block
-constexpr int kFactorBlockCols = 24576;  // columns per block of the preconditioner's copies
+constexpr int kFactorBlockCols = 49152;  // columns per block of the preconditioner's copies
+                                         // (a BF16 vector: 96 KB a block)
 constexpr size_t kStagingBytes = 2 * size_t(12288) * 8;
 constexpr int kMaxSlots = 4;
 __host__ __device__ inline size_t sliced_smem_bytes(int max_rows, int nacc)
@@ -524,7 +538,8 @@ struct SlicedSpmvT {
                 // one slice: lane `lane` of slice entries at off, wp step pairs
                 auto run_slice = [&](unsigned off, int wp, unsigned short row, const VT *pv,
                                      double *accb) {
-                    VT sum = VT(0);
+                    using AT = typename SumType<VT>::T;
+                    AT sum = AT(0);
                     for (int m = 0; m < wp; m += kU) {
                         P2 av[kU];
                         ushort2 cv[kU];
@@ -545,9 +560,9 @@ struct SlicedSpmvT {
                         for (int u = 0; u < kU; u++) {
                             if (m + u < wp) {
                                 if (CGB_IN_RANGE(cv[u].x, M.width, kCheckGather))
-                                    sum = fma_vt(VT(widen(av[u].x)), pv[cv[u].x], sum);
+                                    sum = fma_vt(AT(widen(av[u].x)), AT(widen(pv[cv[u].x])), sum);
                                 if (CGB_IN_RANGE(cv[u].y, M.width, kCheckGather))
-                                    sum = fma_vt(VT(widen(av[u].y)), pv[cv[u].y], sum);
+                                    sum = fma_vt(AT(widen(av[u].y)), AT(widen(pv[cv[u].y])), sum);
                             }
                         }
                     }
