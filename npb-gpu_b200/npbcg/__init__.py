@@ -398,17 +398,23 @@ class Session:
         return st, dev.value
 
 
-def source_fingerprint():
-    """A hash of the library's CUDA/C++ sources (csrc/): names a build, so a
-    profile captured on one build is not read as another's."""
+# the sources of the single-system solver's kernels and of the host code that
+# plans and launches them
+SOLVER_SOURCES = ("cg_kernels.cuh", "spmv_policies.cuh", "device_common.cuh", "galerkin.cuh",
+                  "session.cu")
+
+
+def source_fingerprint(names=SOLVER_SOURCES):
+    """A hash of the single-system solver's sources (csrc/): names a build of
+    those kernels, so a profile captured on one build is not read as
+    another's."""
     import hashlib
     h = hashlib.sha256()
     csrc = os.path.join(os.path.dirname(_HERE), "csrc")
-    for name in sorted(os.listdir(csrc)):
-        if name.endswith((".cu", ".cuh", ".h", ".cpp")):
-            h.update(name.encode())
-            with open(os.path.join(csrc, name), "rb") as f:
-                h.update(f.read())
+    for name in sorted(names):
+        h.update(name.encode())
+        with open(os.path.join(csrc, name), "rb") as f:
+            h.update(f.read())
     return h.hexdigest()[:16]
 
 
