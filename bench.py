@@ -131,7 +131,8 @@ def load_traffic():
     profiles/traffic_per_launch.txt -- used only when that summary was
     captured on this build: its `# build <hash>` line must equal the hash of
     the library's sources (npbcg.source_fingerprint).  Returns ({(kernel,
-    workload, keep_mb): bytes}, a note saying where the numbers come from)."""
+    workload): bytes}, a note saying where the numbers come from).  (ncu
+    replays from cold caches: the L2 keep budget does not change them.)"""
     import npbcg
     path = os.path.join(ROOT, "profiles", "traffic_per_launch.txt")
     out, build = {}, None
@@ -140,9 +141,9 @@ def load_traffic():
             parts = line.split()
             if line.startswith("# build") and len(parts) >= 3:
                 build = parts[2]
-            elif len(parts) >= 4 and not line.startswith("#"):
+            elif len(parts) >= 3 and not line.startswith("#"):
                 try:
-                    out[(parts[0], parts[1], int(parts[2]))] = float(parts[3])
+                    out[(parts[0], parts[1])] = float(parts[-1])
                 except ValueError:
                     pass
     here = npbcg.source_fingerprint()
@@ -298,7 +299,6 @@ def class_c_roofline(npbcg, s, n, nnz, niter, shift):
     spmv_ms = s.time_spmv(50)
     spmv32_ms = s.time_spmv(50, fp32=True)
     table, note = load_traffic()
-    keep = int(round(plan.get("l2_keep_mb", 0.0)))
     ob = outer_step_bytes(n, nnz)
     sb = spmv_bytes(n, nnz)
     sb32 = 8 * nnz + 4 * (n + 1) + 8 * n
@@ -309,7 +309,7 @@ def class_c_roofline(npbcg, s, n, nnz, niter, shift):
                                 ("spmv_fp32", spmv_kernel.replace("spmv_dot_sliced", "spmv_dot_sliced32"),
                                  spmv32_ms, sb32)):
         gbs = nbytes / (ms / 1e3) / 1e9
-        traffic = table.get((k.split("<")[0], "classC", keep))
+        traffic = table.get((k.split("<")[0], "classC"))
         out[name] = {"kernel": k, "launch_ms": ms, "algorithmic_bytes_per_launch": nbytes,
                      "achieved_gbs": gbs, "frac": gbs / peak, "traffic": traffic,
                      "traffic_source": note if traffic is not None else
@@ -543,8 +543,7 @@ def our_arm(args, rank, world, local_rank):
     achieved = bytes_launch / (kernel_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
     traffic_table, traffic_note = load_traffic()
-    traffic = traffic_table.get((kernel.split("<")[0], f"class{CLASS}",
-                                 int(round(plan.get("l2_keep_mb", 0.0)))))
+    traffic = traffic_table.get((kernel.split("<")[0], f"class{CLASS}"))
     spmv_ms = sess.time_spmv(50)
     spmv_gbs = spmv_bytes(n, nnz) / (spmv_ms / 1e3) / 1e9
 

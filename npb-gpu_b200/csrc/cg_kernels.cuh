@@ -617,47 +617,64 @@ __device__ __forceinline__ void put_r_lowp(const OuterArgs &A, int j, double rv)
     else A.r32[j] = float(rv);
 }
 
+// Solver state of the preconditioned body that does not need registers:
+// thread 0 writes it after a reduction every thread already holds, and the
+// CTA barriers of the next phase order the write before any read.  The
+// stall test compares |r|^2 with its value four iterations earlier through
+// a ring of five, so the slot read and the slot written in one iteration
+// differ.
+struct PcgShared {
+    double stop2;       // (tol ||x||)^2
+    double rr_cycle;    // |r|^2 at the last true residual
+    double ring[5];     // |r|^2 after iteration k (k % 5; the refresh value at its own k)
+};
+
 template <class Spmv, int LPRG>
 __device__ __forceinline__ void outer_step_pcg_body(const OuterArgs &A)
 {
     __shared__ double scratch[32];
     __shared__ double bcast[8];
+    __shared__ PcgShared st;
     const int row0 = A.row_split[blockIdx.x];
     const int row1 = A.row_split[blockIdx.x + 1];
     Spmv sp;
     sp.setup(A.M, row0, row1);
     bool ok = true;
-    const int vend = (blockIdx.x == gridDim.x - 1) ? row1 + 1 : row1;
-    const int v = recycle_depth(A);
-    double xx = 0.0;
-    double acc = 0.0;
-    if (v > 0) {
-        // Galerkin start: r' = b' - A' z0 = A z0 - x
-        if (!galerkin_start(galerkin_args(A), row0, row1, vend, v, &xx)) return;
-        for (int j = row0 + threadIdx.x; j < vend; j += blockDim.x) {
-            const double rv = A.q[j] - A.x[j];
-            A.r[j] = rv;
-            put_r_lowp<Spmv>(A, j, rv);
-            if (j < A.n) acc = fma(rv, rv, acc);
+    {
+        const int vend = (blockIdx.x == gridDim.x - 1) ? row1 + 1 : row1;
+        const int v = recycle_depth(A);
+        double xx = 0.0;
+        double acc = 0.0;
+        if (v > 0) {
+            // Galerkin start: r' = b' - A' z0 = A z0 - x
+            if (!galerkin_start(galerkin_args(A), row0, row1, vend, v, &xx)) return;
+            for (int j = row0 + threadIdx.x; j < vend; j += blockDim.x) {
+                const double rv = A.q[j] - A.x[j];
+                A.r[j] = rv;
+                put_r_lowp<Spmv>(A, j, rv);
+                if (j < A.n) acc = fma(rv, rv, acc);
+            }
+        } else {
+            // z0 = 0, r' = b' = -x
+            for (int j = row0 + threadIdx.x; j < vend; j += blockDim.x) {
+                const double xv = A.x[j];
+                A.q[j] = 0.0;
+                A.z[j] = 0.0;
+                A.r[j] = -xv;
+                put_r_lowp<Spmv>(A, j, -xv);
+                if (j < A.n) acc = fma(xv, xv, acc);
+            }
         }
-    } else {
-        // z0 = 0, r' = b' = -x
-        for (int j = row0 + threadIdx.x; j < vend; j += blockDim.x) {
-            const double xv = A.x[j];
-            A.q[j] = 0.0;
-            A.z[j] = 0.0;
-            A.r[j] = -xv;
-            put_r_lowp<Spmv>(A, j, -xv);
-            if (j < A.n) acc = fma(xv, xv, acc);
+        put_partial(A, kSlotRho, acc, scratch);
+        CGB_BARRIER_OR_RETURN(A);
+        const double rr = get_total(A, kSlotRho, &bcast[3]);
+        if (v == 0) xx = rr;
+        if (threadIdx.x == 0) {
+            st.stop2 = A.tol * A.tol * xx;
+            st.rr_cycle = rr;
+            st.ring[0] = rr;
         }
     }
-    put_partial(A, kSlotRho, acc, scratch);
-    CGB_BARRIER_OR_RETURN(A);
-    double rr = get_total(A, kSlotRho, &bcast[0]);
-    if (v == 0) xx = rr;
-    const double stop2 = A.tol * A.tol * xx;
-    double rr_cycle = rr;
-    double hist[4] = {rr, rr, rr, rr};  // |r|^2 of the last four steps
     bool use_prec = true;
     int fallbacks = 0;
     double rho = 0.0;
@@ -673,11 +690,14 @@ __device__ __forceinline__ void outer_step_pcg_body(const OuterArgs &A)
     bool fresh = true;
     for (;;) {
         bool refresh = false;
-        if (rr <= stop2) {
-            if (fresh) break;
-            refresh = true;
-        } else if (!fresh && (since >= A.refresh_every || rr <= kDrift2 * rr_cycle)) {
-            refresh = true;
+        {
+            const double rr = bcast[3];  // |r|^2 (every path leaves it there)
+            if (rr <= st.stop2) {
+                if (fresh) break;
+                refresh = true;
+            } else if (!fresh && (since >= A.refresh_every || rr <= kDrift2 * st.rr_cycle)) {
+                refresh = true;
+            }
         }
         if (!refresh && it >= A.cgitmax) break;
         bool restart = refresh;
@@ -686,7 +706,7 @@ __device__ __forceinline__ void outer_step_pcg_body(const OuterArgs &A)
             spmv<Spmv, double>(sp, A, A.z, A.r, nullptr, ok);
             CGB_OK_OR_RETURN(ok);
             __syncthreads();
-            acc = 0.0;
+            double acc = 0.0;
             for (int j = row0 + threadIdx.x; j < row1; j += blockDim.x) {
                 const double rv = A.r[j] - A.x[j];
                 A.r[j] = rv;
@@ -695,16 +715,18 @@ __device__ __forceinline__ void outer_step_pcg_body(const OuterArgs &A)
             }
             put_partial(A, kSlotRho, acc, scratch);
             CGB_BARRIER_OR_RETURN(A);
-            rr = get_total(A, kSlotRho, &bcast[3]);
-            rr_cycle = rr;
-            hist[0] = hist[1] = hist[2] = hist[3] = rr;
+            const double rr = get_total(A, kSlotRho, &bcast[3]);
+            if (threadIdx.x == 0) {
+                st.rr_cycle = rr;
+                st.ring[it % 5] = rr;
+            }
             refreshes++;
             since = 0;
             fresh = true;
-            if (rr <= stop2) break;
+            if (rr <= st.stop2) break;
         } else {
             // q = A32 p32; p.A'p = -p.q
-            acc = spmv<Spmv, float>(sp, A, A.p32, A.q, A.p, ok);
+            double acc = spmv<Spmv, float>(sp, A, A.p32, A.q, A.p, ok);
             CGB_OK_OR_RETURN(ok);
             put_partial(A, kSlotD, acc, scratch);
             CGB_BARRIER_OR_RETURN(A);
@@ -720,20 +742,18 @@ __device__ __forceinline__ void outer_step_pcg_body(const OuterArgs &A)
             }
             put_partial(A, kSlotRho, acc, scratch);
             CGB_BARRIER_OR_RETURN(A);
-            rr = get_total(A, kSlotRho, &bcast[3]);
+            const double rr = get_total(A, kSlotRho, &bcast[3]);
             it++;
             since++;
             fresh = false;
-            // stall: no halving of |r|^2 over four steps, or lost positivity
-            if (use_prec && (!(pAp > 0.0) || (since >= 4 && rr > 0.25 * hist[0]))) {
+            // stall: no halving of |r|^2 over four steps (the ring slot of
+            // it - 4, not the one written below), or lost positivity
+            if (use_prec && (!(pAp > 0.0) || (since >= 4 && rr > 0.25 * st.ring[(it + 1) % 5]))) {
                 use_prec = false;
                 fallbacks++;
                 restart = true;
             }
-            hist[0] = hist[1];
-            hist[1] = hist[2];
-            hist[2] = hist[3];
-            hist[3] = rr;
+            if (threadIdx.x == 0) st.ring[it % 5] = rr;
         }
         // y = M r', new rho; p = y + beta p (beta = 0 on a restart)
         double rho_new = 0.0;
@@ -754,7 +774,7 @@ __device__ __forceinline__ void outer_step_pcg_body(const OuterArgs &A)
         CGB_BARRIER_OR_RETURN(A);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) A.trace[A.step].spare[0] = double(fallbacks);
-    end_solve(sp, A, row0, row1, it, rr, refreshes, fresh, scratch, bcast, -1.0);
+    end_solve(sp, A, row0, row1, it, bcast[3], refreshes, fresh, scratch, bcast, -1.0);
 }
 
 // Block shapes of the sliced kernels (one CTA per SM; each thread may use

@@ -395,9 +395,9 @@ __device__ __forceinline__ void prefetch_slice_l2(const ST *vals, const unsigned
     }
 }
 
-// kU64 / kU32: step pairs in flight per lane for FP64 / FP32 values (more
-// for kernels with fewer, register-richer threads); BF16 values take twice
-// the FP32 count.
+// kU64 / kU32 / kU16: step pairs in flight per lane for FP64 / FP32 / BF16
+// values (more for kernels with fewer, register-richer threads; BF16 by
+// default twice the FP32 count).
 //
 // Pipeline: a block of the vector is staged by one bulk copy into a slot
 // (S slots: 2 for an FP64 vector, M.nacc for an FP32 one); warps walk the
@@ -410,7 +410,8 @@ __device__ __forceinline__ void prefetch_slice_l2(const ST *vals, const unsigned
 // kPanels: walk the CTA's rows in M.panels row panels (instances for
 // matrices whose rows per CTA exceed the accumulators); without it one walk
 // over the CTA's rows, and the per-panel bookkeeping compiles away.
-template <int kU64, int kU32, bool kOutline = false, bool kL2Prefetch = true, bool kPanels = false>
+template <int kU64, int kU32, bool kOutline = false, bool kL2Prefetch = true, bool kPanels = false,
+          int kU16 = 2 * kU32>
 struct SlicedSpmvT {
     static constexpr bool kSliced = true;
     // Dynamic shared memory: the control words first (fixed offsets), then
@@ -483,7 +484,7 @@ struct SlicedSpmvT {
                                                  int *status, bool &ok)
     {
         using P2 = typename Pair<ST>::T;
-        constexpr int kU = sizeof(ST) == 8 ? kU64 : sizeof(ST) == 4 ? kU32 : 2 * kU32;
+        constexpr int kU = sizeof(ST) == 8 ? kU64 : sizeof(ST) == 4 ? kU32 : kU16;
         const ST *__restrict__ vals = slice_values<ST>(M);
         const uint64_t pol =
             l2_stream_policy(sizeof(ST) == 8 ? M.keep64 : sizeof(ST) == 4 ? M.keep32 : M.keep16);
@@ -669,7 +670,7 @@ using SlicedSpmv = SlicedSpmvT<6, 6, false, false>;
 using SlicedSpmvPf = SlicedSpmvT<6, 6, false, true>;
 using SlicedSpmvMixed = SlicedSpmvT<4, 6, false, false>;
 using SlicedSpmvMixedPf = SlicedSpmvT<4, 6, false, true>;
-using SlicedSpmvPcg = SlicedSpmvT<4, 6, false, false>;
+using SlicedSpmvPcg = SlicedSpmvT<4, 10, false, false, false, 8>;
 // row-panel instances (no L2 prefetch)
 using SlicedSpmvPanels = SlicedSpmvT<6, 6, false, false, true>;
 using SlicedSpmvMixedPanels = SlicedSpmvT<4, 6, false, false, true>;

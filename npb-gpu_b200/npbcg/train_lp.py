@@ -4,7 +4,7 @@
 
 Training data (the generator's matrices at seeds the NPB classes never
 use): 128 matrices at n=14000, nonzer=11, shift=20 and 128 at n=75000,
-nonzer=13, shift=60, each seen once, 4 Adam steps per matrix on 32 probe
+nonzer=13, shift=60, each seen once, 16 Adam steps per matrix on 32 probe
 vectors: residual histories (the residuals after 0, 2, 4 or 8 batched CG
 steps on the scaled matrix, one of the starting vectors all ones like the
 benchmark's first x) and plain normal vectors.  Forward, backward and the
@@ -33,7 +33,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--small", action="store_true")
     ap.add_argument("--out", default=npbcg.WEIGHTS_PATH)
-    ap.add_argument("--steps-per-matrix", type=int, default=4)
+    ap.add_argument("--steps-per-matrix", type=int, default=16)
     ap.add_argument("--lr", type=float, default=2e-3)
     a = ap.parse_args()
     counts = (16, 4) if a.small else (128, 128)
