@@ -148,12 +148,12 @@ def trained_model(cgb):
     return model, "short run"
 
 
-@pytest.mark.parametrize("tol", [1e-12, 1e-11])
+@pytest.mark.parametrize("tol", [1e-12, 1e-11, 1e-10])
 def test_learned_preconditioner_class_c_unseen_seed(cgb, golden, tol):
     """Config: train on other seeds, test at n=150000, nonzer=15, shift=110
     (the NPB seed, never used in training); FP64 plain CG (the reference
     trace) is the yardstick for zeta: relative 1e-10 at every outer step, at the solver
-    tolerances the benchmark reports."""
+    tolerances the benchmark reports (1e-10 is the configuration's own)."""
     model, how = trained_model(cgb)
     n, nonzer, niter, shift = PARAMS["C"]
     rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
