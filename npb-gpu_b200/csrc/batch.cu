@@ -1593,7 +1593,22 @@ int cgb_batch_set_preconditioner(cgb_batch *b, int sys, const int *fptr, const i
     std::vector<int> optr(n + 1, 0), ocol;
     std::vector<float> oval, dg(n, 0.f);
     std::vector<std::pair<int, double>> row;
+    ocol.reserve(size_t(fptr[n]));
+    oval.reserve(size_t(fptr[n]));
     for (int i = 0; i < n; i++) {
+        bool ascending = true;  // the common case (the learned factor's rows): no sort
+        for (int k = fptr[i] + 1; k < fptr[i + 1]; k++) ascending &= fcol[k] > fcol[k - 1];
+        if (ascending) {
+            for (int k = fptr[i]; k < fptr[i + 1]; k++) {
+                ocol.push_back(fcol[k]);
+                oval.push_back(float(fval[k]));
+            }
+            dg[i] = oval.back();
+            ocol.pop_back();
+            oval.pop_back();
+            optr[i + 1] = int(ocol.size());
+            continue;
+        }
         row.clear();
         for (int k = fptr[i]; k < fptr[i + 1]; k++) row.emplace_back(fcol[k], fval[k]);
         std::stable_sort(row.begin(), row.end(), [](const std::pair<int, double> &x,

@@ -1586,6 +1586,16 @@ int cgb_set_preconditioner(cgb_session *s, const int *fptr, const int *fcol, con
     val32.reserve(size_t(fptr[n]));
     std::vector<std::pair<int, double>> row;
     for (int i = 0; i < n; i++) {
+        bool ascending = true;  // the common case (the learned factor's rows): no sort
+        for (int k = fptr[i] + 1; k < fptr[i + 1]; k++) ascending &= fcol[k] > fcol[k - 1];
+        if (ascending) {
+            for (int k = fptr[i]; k < fptr[i + 1]; k++) {
+                ocol.push_back(fcol[k]);
+                val32.push_back(float(fval[k]));
+            }
+            optr[i + 1] = int(ocol.size());
+            continue;
+        }
         row.clear();
         for (int k = fptr[i]; k < fptr[i + 1]; k++) row.emplace_back(fcol[k], fval[k]);
         std::stable_sort(row.begin(), row.end(),

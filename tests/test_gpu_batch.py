@@ -257,3 +257,38 @@ def test_batch_learned_needs_every_factor(cgb):
         with pytest.raises(cgb.CgbError) as e:
             b.set_preconditioner(1, np.zeros(2001, np.int32), np.zeros(0, np.int32), np.zeros(0))
         assert e.value.status == cgb.ERR_BAD_MATRIX
+
+
+def test_batch_factor_rows_sorted_and_merged(cgb):
+    """cgb_batch_set_preconditioner takes rows in any column order and sums
+    repeated columns: a factor given with its rows reversed and each
+    off-diagonal entry split in two halves solves bit for bit like the
+    same factor given sorted."""
+    specs = [(1400, 7, 10.0, 314159265.0), (2000, 9, 12.0, 271828183.0)]
+    systems, shifts = build(cgb, specs)
+    outs = []
+    for shuffled in (False, True):
+        with cgb.Batch(systems, shifts) as b:
+            b.set_team_frac(0.0)
+            for i, (rs, ci, a) in enumerate(systems):
+                n = len(rs) - 1
+                # F = I - 0.001 L (L: A's strict lower pattern, values 1)
+                lptr, lcol = cgb.strict_lower_pattern(rs, ci)
+                rows_p, rows_c, rows_v = [0], [], []
+                for r in range(n):
+                    cols = list(lcol[lptr[r]:lptr[r + 1]])
+                    vals = [-1e-3] * len(cols)
+                    if shuffled:
+                        cols = cols[::-1] + cols
+                        vals = [v / 2 for v in vals[::-1]] + [v / 2 for v in vals]
+                        cols, vals = [r] + cols, [1.0] + vals
+                    else:
+                        cols, vals = cols + [r], vals + [1.0]
+                    rows_c += cols
+                    rows_v += vals
+                    rows_p.append(len(rows_c))
+                b.set_preconditioner(i, np.array(rows_p, np.int32), np.array(rows_c, np.int32),
+                                     np.array(rows_v))
+            outs.append(b.solve(niter=5, mode=cgb.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=100))
+    assert np.array_equal(outs[0]["zeta"], outs[1]["zeta"])
+    assert np.array_equal(outs[0]["iters"], outs[1]["iters"])
