@@ -161,15 +161,23 @@ def peaks():
 
 
 # ------------------------------------------------------------------ CPU arms
-def cpu_reference_run(outer_steps, repeats=1):
-    """Times the reference's own serial CPU conj_grad loop (oracle/_ref)."""
+def cpu_reference_run(outer_steps, repeats=1, gpu_steps=0):
+    """Times the reference's own serial CPU conj_grad loop (oracle/_ref);
+    with gpu_steps > 0 also the reference's own GPU loop (conj_grad_gpu and
+    its eleven kernels, cg.cu:489-522, 803-1265) on the same matrix, best of
+    two runs after a warm-up: (n, nnz, CPU times, GPU run or None)."""
     from oracle_py import RefLib
     ref = RefLib(os.path.join(ROOT, "oracle", "_ref", f"libref_{CLASS}.so"))
     nnz = ref.makea(copy_out=False)
     times = []
     for _ in range(repeats):
         times.append(ref.power(outer_steps)["seconds"])
-    return ref.n, nnz, times
+    gpu = None
+    if gpu_steps > 0:
+        ref.power_gpu(2)
+        runs = [ref.power_gpu(gpu_steps) for _ in range(2)]
+        gpu = min(runs, key=lambda r: r["seconds"])
+    return ref.n, nnz, times, gpu
 
 
 def cpu_openmp_run(rowstr, colidx, a, shift, outer_steps, threads):
@@ -182,7 +190,7 @@ def reference_arm(args, rank, world):
     if rank != 0:
         return 0
     c = CLASSES[CLASS]
-    n, nnz, times = cpu_reference_run(REF_STEP_OUTER, repeats=args.warmup + args.steps)
+    n, nnz, times, _ = cpu_reference_run(REF_STEP_OUTER, repeats=args.warmup + args.steps)
     timed = times[args.warmup:]
     per_step_bytes = REF_STEP_OUTER * (CGITMAX + 1) * spmv_bytes(n, nnz)
     total = sum(timed)
@@ -338,10 +346,12 @@ def batched_section(npbcg, device, nsys=512, niter=15, rank=0, world=1, dist=Non
                for i in mine]
     shifts = [specs[i][2] for i in mine]
     with npbcg.Batch(systems, shifts, device=device) as b:
-        # the autotuner picks block shape and lanes per row for each mode
+        # the autotuner picks block shape, lanes per row and teams for each
+        # mode, timing three outer steps (the tolerance modes reach their
+        # Galerkin-started regime only after the first)
         tuned_fp64 = b.tune(niter=1)
         ref_run = b.solve(niter=niter)
-        tuned = b.tune(niter=1, mode=npbcg.MODE_MIXED, tol=1e-12, cgitmax=200)
+        tuned = b.tune(niter=3, mode=npbcg.MODE_MIXED, tol=1e-12, cgitmax=200)
         mixed = b.solve(niter=niter, mode=npbcg.MODE_MIXED, tol=1e-12, cgitmax=200)
         learned = ident = tuned_l = None
         if os.path.exists(npbcg.WEIGHTS_PATH):
@@ -353,7 +363,7 @@ def batched_section(npbcg, device, nsys=512, niter=15, rank=0, world=1, dist=Non
             b.attach_learned(model)
             attach_s = time.perf_counter() - t0
             model.close()
-            tuned_l = b.tune(niter=1, mode=npbcg.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=200)
+            tuned_l = b.tune(niter=3, mode=npbcg.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=200)
             learned = b.solve(niter=niter, mode=npbcg.MODE_MIXED_LEARNED, tol=1e-12, cgitmax=200)
             learned["fallbacks"] = b.fallbacks()
             learned["attach_s"] = attach_s
@@ -586,8 +596,20 @@ def our_arm(args, rank, world, local_rank):
             line["solver_modes"] = solver_modes_section(npbcg, device)
             line["roofline_classC"] = line["solver_modes"].pop("roofline_classC")
         if world == 1 and not args.no_cpu_baseline:
-            nref, nnz_ref, times = cpu_reference_run(CPU_SAMPLE_STEPS)
+            nref, nnz_ref, times, rgpu = cpu_reference_run(CPU_SAMPLE_STEPS, gpu_steps=niter)
             sample_bytes = CPU_SAMPLE_STEPS * (CGITMAX + 1) * spmv_bytes(nref, nnz_ref)
+            # informative: the reference's own CUDA code on this GPU, the same
+            # 75-step solve, its wall time as the reference's timer takes it
+            rg_bytes = niter * (CGITMAX + 1) * spmv_bytes(nref, nnz_ref)
+            line["reference_gpu"] = {
+                "what": "the reference's conj_grad_gpu loop (cg.cu:489-522, 803-1265), compiled "
+                        "from its sources with its device flags for sm_100a, same matrix",
+                "seconds": rgpu["seconds"], "value": rg_bytes / rgpu["seconds"] / 1e9,
+                "unit": "GB/s", "zeta": float(rgpu["zeta"][-1]),
+                "zeta_rel_err_vs_verify": abs(float(rgpu["zeta"][-1]) - c["zeta"]) / c["zeta"],
+                "our_device_speedup": (rgpu["seconds"] * 1e3) / ms_per_step,
+                "our_e2e_speedup": e2e_value / (rg_bytes / rgpu["seconds"] / 1e9),
+            }
             ser = sample_bytes / times[0] / 1e9
             threads = os.cpu_count() or 1
             omp_s = cpu_openmp_run(rs, ci, a, shift, CPU_SAMPLE_STEPS, threads)

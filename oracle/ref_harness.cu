@@ -16,6 +16,11 @@
  *                   on the last generated matrix
  *   ref_power       the reference outer loop (cg.cu:485-520) driven by the
  *                   CPU conj_grad: per-step zeta and rnorm, wall seconds
+ *   ref_power_gpu   the same loop as the reference times it on the GPU
+ *                   (cg.cu:489-522: setup_gpu, then conj_grad_gpu and the
+ *                   gpu_kernel_ten / eleven norms, release_gpu after): an
+ *                   informative comparator of the GPU arm, compiled with the
+ *                   reference's device flags (make.def OPTIMIZATIONS)
  */
 #include <chrono>
 #include <cmath>
@@ -122,4 +127,39 @@ extern "C" double ref_power(int niter, double *zeta_trace, double *rnorm_trace)
         if (rnorm_trace) rnorm_trace[it - 1] = rnorm;
     }
     return harness_now() - t0;
+}
+
+/* The reference's GPU outer loop (cg.cu:489-522): x = 1, setup_gpu() (the
+ * uploads, outside the timed region as in main), niter steps of
+ * conj_grad_gpu + gpu_kernel_ten / gpu_kernel_eleven, release_gpu().
+ * Returns the wall seconds of the loop (the reference's own timer brackets
+ * the same region); traces may be NULL. */
+extern "C" double ref_power_gpu(int niter, double *zeta_trace, double *rnorm_trace)
+{
+    if (g_nnz < 0)
+        return -1.0;
+    for (int i = 0; i < NA + 1; i++)
+        x[i] = 1.0;
+    for (int j = 0; j < lastcol - firstcol + 1; j++) {
+        q[j] = 0.0;
+        z[j] = 0.0;
+        r[j] = 0.0;
+        p[j] = 0.0;
+    }
+    setup_gpu();
+    cudaDeviceSynchronize();
+    double t0 = harness_now();
+    for (int it = 1; it <= niter; it++) {
+        double rnorm = 0.0, norm_temp1 = 0.0, norm_temp2 = 0.0;
+        conj_grad_gpu(&rnorm);
+        gpu_kernel_ten(&norm_temp1, &norm_temp2);
+        norm_temp2 = 1.0 / sqrt(norm_temp2);
+        if (zeta_trace) zeta_trace[it - 1] = SHIFT + 1.0 / norm_temp1;
+        if (rnorm_trace) rnorm_trace[it - 1] = rnorm;
+        gpu_kernel_eleven(norm_temp2);
+    }
+    cudaDeviceSynchronize();
+    const double secs = harness_now() - t0;
+    release_gpu();
+    return secs;
 }

@@ -92,6 +92,8 @@ class RefLib:
         lib.ref_makea.restype = ctypes.c_int
         lib.ref_power.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         lib.ref_power.restype = ctypes.c_double
+        lib.ref_power_gpu.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        lib.ref_power_gpu.restype = ctypes.c_double
         lib.ref_conj_grad.argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_void_p]
         lib.ref_conj_grad.restype = ctypes.c_int
         na, nz, ni = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
@@ -114,6 +116,13 @@ class RefLib:
     def power(self, niter):
         zt, rt = np.zeros(niter), np.zeros(niter)
         secs = self.lib.ref_power(niter, zt.ctypes.data, rt.ctypes.data)
+        return dict(zeta=zt, rnorm=rt, seconds=secs)
+
+    def power_gpu(self, niter):
+        """The reference's own GPU loop (conj_grad_gpu, cg.cu:803-846) on
+        the last generated matrix: traces and the loop's wall seconds."""
+        zt, rt = np.zeros(niter), np.zeros(niter)
+        secs = self.lib.ref_power_gpu(niter, zt.ctypes.data, rt.ctypes.data)
         return dict(zeta=zt, rnorm=rt, seconds=secs)
 
     def conj_grad(self, x):

@@ -145,6 +145,23 @@ def test_conj_grad_against_reference_library(cgb, oracle):
     assert abs(rn - rnr) <= 1e-10 * np.linalg.norm(x)
 
 
+def test_reference_gpu_loop_matches_reference_trace(golden):
+    """The reference's own GPU loop (conj_grad_gpu, compiled from its
+    sources into oracle/_ref), which the bench times beside ours, computes
+    the reference's trace: zeta relative 1e-10, rnorm absolute 1e-10."""
+    path = ref_lib_path("S")
+    if not os.path.exists(path):
+        pytest.skip("oracle/_ref not built")
+    from oracle_py import RefLib
+    ref = RefLib(path)
+    ref.makea(copy_out=False)
+    out = ref.power_gpu(ref.niter)
+    e = golden["S"]["seeds"]["314159265.0"]
+    assert out["seconds"] > 0
+    assert np.max(np.abs(out["zeta"] - np.array(e["zeta"])) / np.array(e["zeta"])) <= 1e-10
+    assert np.max(np.abs(out["rnorm"] - np.array(e["rnorm"]))) <= 1e-10
+
+
 def test_conj_grad_reuploads_changed_matrix(cgb, oracle):
     n, nonzer, _, shift = PARAMS["S"]
     rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
