@@ -241,6 +241,21 @@ def solver_modes_section(npbcg, device):
         return best
 
     nnz = len(a)
+    # informative: the reference's own GPU loop on the same matrix, 75 steps
+    # (best of two after a warm-up), before our sessions hold the device
+    ref_gpu_ms = None
+    ref_path = os.path.join(ROOT, "oracle", "_ref", "libref_C.so")
+    if os.path.exists(ref_path):
+        from oracle_py import RefLib
+        ref = RefLib(ref_path)
+        ref.set_matrix(rs, ci, a)
+        ref.power_gpu(2)
+        ref_gpu = min((ref.power_gpu(niter) for _ in range(2)), key=lambda r: r["seconds"])
+        ref_gpu_ms = 1e3 * ref_gpu["seconds"]
+        out["reference_gpu_fixed25"] = {
+            "ms": ref_gpu_ms, "zeta": float(ref_gpu["zeta"][-1]),
+            "what": "the reference's conj_grad_gpu loop (cg.cu:489-522), wall time as its timer "
+                    "takes it, on this GPU"}
     with npbcg.Session(rs, ci, a, device=device) as s:
         out["plan"] = s.plan()
         out["roofline_classC"] = class_c_roofline(npbcg, s, n, nnz, niter, shift)
@@ -286,7 +301,9 @@ def solver_modes_section(npbcg, device):
                          "inner_iterations": int(r["total_inner"]),
                          "refreshes": int(r.get("refreshes", 0)),
                          "fallbacks": int(r.get("fallbacks", 0)),
-                         "speedup_vs_fp64_fixed25": plain["device_ms"] / r["device_ms"]}
+                         "speedup_vs_fp64_fixed25": plain["device_ms"] / r["device_ms"],
+                         "speedup_vs_reference_gpu": (ref_gpu_ms / r["device_ms"]
+                                                      if ref_gpu_ms else None)}
     return out
 
 

@@ -16,6 +16,8 @@
  *                   on the last generated matrix
  *   ref_power       the reference outer loop (cg.cu:485-520) driven by the
  *                   CPU conj_grad: per-step zeta and rnorm, wall seconds
+ *   ref_set_matrix  loads a CSR (the generator's, produced elsewhere bit for
+ *                   bit) into the reference's arrays instead of ref_makea
  *   ref_power_gpu   the same loop as the reference times it on the GPU
  *                   (cg.cu:489-522: setup_gpu, then conj_grad_gpu and the
  *                   gpu_kernel_ten / eleven norms, release_gpu after): an
@@ -80,6 +82,24 @@ extern "C" int ref_makea(double seed, int *rowstr_out, int *colidx_out, double *
     if (a_out)
         memcpy(a_out, a, sizeof(double) * (size_t)g_nnz);
     return g_nnz;
+}
+
+/* Loads rowstr (NA+1), colidx and a (nnz entries) into the reference's
+ * arrays, as ref_makea leaves them; returns nnz, or -1 when it exceeds NZ. */
+extern "C" int ref_set_matrix(const int *rowstr_in, const int *colidx_in, const double *a_in)
+{
+    const int nnz = rowstr_in[NA];
+    if (nnz < 0 || (long long)nnz > (long long)NZ)
+        return -1;
+    firstrow = 0;
+    lastrow = NA - 1;
+    firstcol = 0;
+    lastcol = NA - 1;
+    memcpy(rowstr, rowstr_in, sizeof(int) * (NA + 1));
+    memcpy(colidx, colidx_in, sizeof(int) * (size_t)nnz);
+    memcpy(a, a_in, sizeof(double) * (size_t)nnz);
+    g_nnz = nnz;
+    return nnz;
 }
 
 /* One reference conj_grad on the last generated matrix.  x_in has NA

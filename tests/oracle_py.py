@@ -94,6 +94,8 @@ class RefLib:
         lib.ref_power.restype = ctypes.c_double
         lib.ref_power_gpu.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         lib.ref_power_gpu.restype = ctypes.c_double
+        lib.ref_set_matrix.argtypes = [ctypes.c_void_p] * 3
+        lib.ref_set_matrix.restype = ctypes.c_int
         lib.ref_conj_grad.argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_void_p]
         lib.ref_conj_grad.restype = ctypes.c_int
         na, nz, ni = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
@@ -117,6 +119,16 @@ class RefLib:
         zt, rt = np.zeros(niter), np.zeros(niter)
         secs = self.lib.ref_power(niter, zt.ctypes.data, rt.ctypes.data)
         return dict(zeta=zt, rnorm=rt, seconds=secs)
+
+    def set_matrix(self, rowstr, colidx, a):
+        """Loads a CSR into the reference's arrays (in place of makea)."""
+        rs = np.ascontiguousarray(rowstr, np.int32)
+        ci = np.ascontiguousarray(colidx, np.int32)
+        av = np.ascontiguousarray(a, np.float64)
+        nnz = self.lib.ref_set_matrix(rs.ctypes.data, ci.ctypes.data, av.ctypes.data)
+        if nnz < 0:
+            raise ValueError("matrix larger than the reference's NZ")
+        return nnz
 
     def power_gpu(self, niter):
         """The reference's own GPU loop (conj_grad_gpu, cg.cu:803-846) on

@@ -110,6 +110,26 @@ def test_reference_library_agrees_with_oracle(oracle):
     assert zr[4] == zo[4]
 
 
+def test_reference_library_takes_the_product_csr(cgb, golden):
+    """ref_set_matrix loads a CSR into the reference's arrays in place of
+    its makea (the bench hands it the product generator's class-C matrix
+    rather than spending the reference's 13 s on generating it): with the
+    product's bit-identical class-S CSR the reference's own CPU loop
+    reproduces its golden trace bit for bit."""
+    import os
+    path = ref_lib_path("S")
+    if not os.path.exists(path):
+        pytest.skip("oracle/_ref not built")
+    from oracle_py import RefLib
+    ref = RefLib(path)
+    rs, ci, a = cgb.makea(1400, 7, 0.1, 10.0)
+    assert ref.set_matrix(rs, ci, a) == len(a)
+    out = ref.power(15)
+    e = golden["S"]["seeds"]["314159265.0"]
+    assert np.array_equal(out["zeta"], np.array(e["zeta"]))
+    assert np.array_equal(out["rnorm"], np.array(e["rnorm"]))
+
+
 def test_oracle_zeta_converges_with_outer_steps(golden):
     """Documents how fast the power iteration settles (time-to-zeta depends on it)."""
     z = np.array(golden["S"]["seeds"]["314159265.0"]["zeta"])
