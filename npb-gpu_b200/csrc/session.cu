@@ -724,7 +724,7 @@ int ensure_prec_slices(cgb_session *s)
 
 // Fills `pl` for (kind, lpr): kernels, occupancy-sized cooperative grid,
 // shared memory.  Returns false when the configuration cannot run here.
-bool make_plan(cgb_session *s, int kind, int lpr, Plan *pl, int prefetch = 0)
+bool make_plan(cgb_session *s, int kind, int lpr, Plan *pl, int prefetch = 0, int grid_cap = 0)
 {
     Plan P;
     P.kind = kind;
@@ -783,6 +783,7 @@ bool make_plan(cgb_session *s, int kind, int lpr, Plan *pl, int prefetch = 0)
     }
     per_sm = std::min(per_sm, kind == kKindSliced ? 1 : 4);
     P.grid = std::max(1, std::min(per_sm * s->prop.multiProcessorCount, s->n));
+    if (grid_cap > 0) P.grid = std::min(P.grid, grid_cap);
     if (P.grid > s->gpad) return false;
     *pl = P;
     return true;
@@ -886,6 +887,10 @@ int time_plan_outer(cgb_session *s, double *ms_out)
                      "outer step failed while timing the plan (device status %d)", dst);
 }
 
+// Below this order the autotuner also tries the row plan on 16, 32 and 64
+// CTAs.
+constexpr int kSmallGridRows = 40000;
+
 // Picks the plan: the one the options force, else the candidate with the
 // fastest FP64 outer step (the session's autotuner; the outer step, not a
 // standalone product, because the candidates' order can differ between the
@@ -906,6 +911,15 @@ int choose_plan(cgb_session *s)
             const int l = lanes_for_mean(mean);
             add(kKindRow, l, 0);
             if (want == 0 && l > 2) add(kKindRow, l / 2, 0);
+            // a small matrix on every SM is mostly grid barriers (class S:
+            // 1400 rows, about 5 a CTA on 296 CTAs): also a few CTAs, each
+            // with many rows, whose barriers cost less than the parallelism
+            // they give up
+            if (want == 0 && s->n < kSmallGridRows)
+                for (int cap : {16, 32, 64}) {
+                    Plan p;
+                    if (make_plan(s, kKindRow, l, &p, 0, cap) && p.grid == cap) cands.push_back(p);
+                }
         }
     }
     if (want == 0 || want == kKindSliced || want == kKindSlicedPrefetch) {
