@@ -383,6 +383,63 @@ int cgb_conj_grad_noalloc(int n, long long nnz, const int *d_rowstr, const int *
                           const double *d_a, const double *d_x, double *d_z, double *d_rnorm,
                           int *d_status, void *stream);
 
+/* ---- One system split by rows over several GPUs -----------------------
+ * The reference algorithm (conj_grad of cg.cu:653-801, cgitmax FP64 steps,
+ * inside the outer loop of cg.cu:485-520) on a matrix whose rows are
+ * divided among `world` ranks, one process (or one call) per GPU.  Rank r
+ * owns the rows [r m, min((r+1) m, n)), m = ceil(n / world)
+ * (cgb_part_rows), stored as CSR with GLOBAL column indices.  Per CG step
+ * the ranks exchange the search vector once (an all-gather of their rows)
+ * and two scalars (all-reduces of p.q and r.r); scalars stay on the device.
+ * The result is the reference's to rounding: the sums are ordered
+ * differently than on one GPU, but identically from run to run. */
+typedef struct cgb_part cgb_part;
+
+#define CGB_NCCL_ID_BYTES 128
+
+/* Rows [*row0, *row1) of `rank` among `world` for an n-row matrix.  No GPU
+ * needed. */
+int cgb_part_rows(int n, int world, int rank, int *row0, int *row1);
+
+/* A new NCCL unique id (CGB_NCCL_ID_BYTES bytes) for rank 0 to hand to the
+ * others.  NCCL is loaded on first use (libnccl.so.2); CGB_ERR_STATE when it
+ * cannot be found. */
+int cgb_nccl_unique_id(void *id_out);
+
+/* One rank's share.  rowstr (row1 - row0 + 1 entries, rowstr[0] == 0),
+ * colidx and a are this rank's rows of the global CSR: its rows
+ * row0..row1-1 with their global columns.  With nccl_id (from
+ * cgb_nccl_unique_id on one rank, the same bytes on all) the call joins the
+ * world's communicator, a collective call: every rank makes it.  Without it
+ * the part can only be driven by cgb_part_group_power_iterate (world 1 also
+ * by cgb_part_power_iterate). */
+int cgb_part_create(int device, int n, int world, int rank, const int *rowstr, const int *colidx,
+                    const double *a, const void *nccl_id, cgb_part **out);
+int cgb_part_destroy(cgb_part *p);
+
+/* One rank's share of the NPB matrix makea(n, nonzer, rcond, shift, seed)
+ * generated on the device: only this rank's rows are assembled (the same
+ * entries, bit for bit, as those rows of cgb_makea), so no rank -- and no
+ * host -- ever holds the whole matrix.  Each rank's block needs fewer than
+ * 2^31 entries; the whole matrix may have more (class E: about 6.4e9). */
+int cgb_part_create_generated(int device, int n, int nonzer, double rcond, double shift, double seed,
+                              int world, int rank, const void *nccl_id, cgb_part **out);
+
+/* niter outer steps of the power iteration from x = 1, every rank calling
+ * it with the same arguments (collective).  zeta_trace / rnorm_trace (niter
+ * doubles each, nullable) get every step's zeta and ||x - A z||, the same on
+ * every rank; device_ms the device time of this rank's steps. */
+int cgb_part_power_iterate(cgb_part *p, int niter, double shift, int cgitmax, double *zeta_trace,
+                           double *rnorm_trace, double *device_ms);
+
+/* The same solve for all `k` == world ranks of one world from one process,
+ * all parts on one device and created without an NCCL id: the ranks'
+ * kernels run one after another on one stream and the exchanges are device
+ * copies and a summing kernel, so the partitioned data flow runs -- and is
+ * tested -- on a single GPU.  parts[i] must be rank i. */
+int cgb_part_group_power_iterate(cgb_part **parts, int k, int niter, double shift, int cgitmax,
+                                 double *zeta_trace, double *rnorm_trace, double *device_ms);
+
 /* Host memory that the device copies at full speed (cudaHostAlloc). */
 int cgb_host_alloc(void **ptr, long long bytes);
 int cgb_host_free(void *ptr);

@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["session.cu", "noalloc.cu", "gnn.cu", "batch.cu", "makea_gpu.cu"]
+CU_SOURCES = ["session.cu", "noalloc.cu", "gnn.cu", "batch.cu", "makea_gpu.cu", "part.cu"]
 CPP_SOURCES = ["makea.cpp"]
 LIB = os.path.join(LIBDIR, "libcgb.so")
 # the checked build: the single-system solver with every SpMV index tested

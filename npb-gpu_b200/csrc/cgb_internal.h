@@ -33,7 +33,8 @@ int draw_generator_vectors(int n, int nonzer, double rcond, double seed, GenVect
 
 // The generator's CSR left on the device (makea_gpu.cu): rowstr / colidx / a
 // are device allocations the caller takes over (cudaFree), the row pointers
-// are also on the host.
+// are also on the host.  With a row range [row0, row1) only those rows are
+// assembled (rowstr rebased to 0, columns global): one rank's block.
 struct DeviceCsr {
     int *rowstr = nullptr;
     int *colidx = nullptr;
@@ -42,6 +43,6 @@ struct DeviceCsr {
     std::vector<int> h_rowstr;
 };
 int makea_on_device(int device, int n, int nonzer, double rcond, double shift, double seed,
-                    DeviceCsr *out);
+                    DeviceCsr *out, int row0 = 0, int row1 = -1);
 
 }  // namespace cgb

@@ -183,31 +183,37 @@ __global__ void draw_vectors(uint64_t seed, long long D, int n, int nonzer, int 
     }
 }
 
+// The assembly covers the rows [row0, row0 + nr) (all n, or one rank's
+// block of a row-partitioned solve); arrays indexed by row below are local
+// to that range, column indices stay global.
+
 // 1a. per row: vectors touching it, and its contribution count
 __global__ void row_counts(const int *__restrict__ count, const int *__restrict__ pos, int n,
-                           int width, int *nvec, unsigned long long *ncontrib)
+                           int width, int row0, int nr, int *nvec, unsigned long long *ncontrib)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int c = count[i];
         for (int s = 0; s < c; s++) {
-            const int row = pos[size_t(i) * width + s];
-            atomicAdd(&nvec[row], 1);
-            atomicAdd(&ncontrib[row], (unsigned long long)c);
+            const unsigned lr = unsigned(pos[size_t(i) * width + s] - row0);
+            if (lr >= unsigned(nr)) continue;
+            atomicAdd(&nvec[lr], 1);
+            atomicAdd(&ncontrib[lr], (unsigned long long)c);
         }
     }
 }
 
 // 1b. per row: the (vector, entry) keys i * 32 + s, unordered
 __global__ void fill_lists(const int *__restrict__ count, const int *__restrict__ pos, int n,
-                           int width, const long long *__restrict__ voff, int *cursor,
-                           unsigned *list)
+                           int width, int row0, int nr, const long long *__restrict__ voff,
+                           int *cursor, unsigned *list)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int c = count[i];
         for (int s = 0; s < c; s++) {
-            const int row = pos[size_t(i) * width + s];
-            const int at = atomicAdd(&cursor[row], 1);
-            list[voff[row] + at] = unsigned(i) * 32u + unsigned(s);
+            const unsigned lr = unsigned(pos[size_t(i) * width + s] - row0);
+            if (lr >= unsigned(nr)) continue;
+            const int at = atomicAdd(&cursor[lr], 1);
+            list[voff[lr] + at] = unsigned(i) * 32u + unsigned(s);
         }
     }
 }
@@ -233,15 +239,16 @@ __global__ void sort_lists(const long long *__restrict__ voff, int n, unsigned *
 // 2. one warp per row: contributions in generation order
 __global__ void contributions(const int *__restrict__ count, const int *__restrict__ pos,
                               const double *__restrict__ val, const double *__restrict__ scale,
-                              int n, int width, double rcond, double shift,
+                              int row0, int nr, int width, double rcond, double shift,
                               const long long *__restrict__ voff, const unsigned *__restrict__ list,
                               const long long *__restrict__ coff, int *ccol, double *cval)
 {
     const int lane = threadIdx.x & 31;
-    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n;
-         row += (gridDim.x * blockDim.x) >> 5) {
-        long long at = coff[row];
-        for (long long k = voff[row]; k < voff[row + 1]; k++) {
+    for (int lr = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; lr < nr;
+         lr += (gridDim.x * blockDim.x) >> 5) {
+        const int row = row0 + lr;
+        long long at = coff[lr];
+        for (long long k = voff[lr]; k < voff[lr + 1]; k++) {
             const unsigned key = list[k];
             const int i = int(key >> 5), s = int(key & 31u);
             const int c = count[i];
@@ -482,7 +489,7 @@ int draw_on_device(double seed, int n, int nonzer, int sms, DeviceBuffers *d)
     } while (0)
 
 int cgb::makea_on_device(int device, int n, int nonzer, double rcond, double shift, double seed,
-                         DeviceCsr *out)
+                         DeviceCsr *out, int row0, int row1)
 {
     if (!(rcond > 0.0) || !std::isfinite(shift))
         return set_error(CGB_ERR_INVALID, "makea_device: rcond must be > 0 and shift finite");
@@ -494,6 +501,10 @@ int cgb::makea_on_device(int device, int n, int nonzer, double rcond, double shi
         return set_error(CGB_ERR_INVALID, "makea_device: need n >= 2, 1 <= nonzer < n");
     if (!valid_seed(seed))
         return set_error(CGB_ERR_INVALID, "makea_device: seed must be an odd integer in (1, 2^46)");
+    if (row1 < 0) row1 = n;
+    if (row0 < 0 || row0 >= row1 || row1 > n)
+        return set_error(CGB_ERR_INVALID, "makea_device: rows [%d, %d) not within [0, %d)", row0, row1, n);
+    const int nr = row1 - row0;
     GEN_TRY(cudaSetDevice(device));
     cudaDeviceProp prop;
     GEN_TRY(cudaGetDeviceProperties(&prop, device));
@@ -504,8 +515,8 @@ int cgb::makea_on_device(int device, int n, int nonzer, double rcond, double shi
     GEN_TRY(galloc(&d.pos, size_t(n) * w));
     GEN_TRY(galloc(&d.val, size_t(n) * w));
     GEN_TRY(galloc(&d.scale, n));
-    GEN_TRY(galloc(&d.nvec, n));
-    GEN_TRY(galloc(&d.ncontrib, n));
+    GEN_TRY(galloc(&d.nvec, nr));
+    GEN_TRY(galloc(&d.ncontrib, nr));
     {
         // the geometric weights: a running product, rounded at every step
         // as the reference's loop does (cg.cu:1695, :1755) -- host, O(n)
@@ -520,58 +531,73 @@ int cgb::makea_on_device(int device, int n, int nonzer, double rcond, double shi
     }
     int st = draw_on_device(seed, n, nonzer, sms, &d);
     if (st) return st;
-    GEN_TRY(cudaMemset(d.nvec, 0, sizeof(int) * n));
-    GEN_TRY(cudaMemset(d.ncontrib, 0, sizeof(unsigned long long) * n));
+    GEN_TRY(cudaMemset(d.nvec, 0, sizeof(int) * nr));
+    GEN_TRY(cudaMemset(d.ncontrib, 0, sizeof(unsigned long long) * nr));
     const int grid = 8 * sms;
-    row_counts<<<grid, 256>>>(d.count, d.pos, n, w, d.nvec, d.ncontrib);
+    row_counts<<<grid, 256>>>(d.count, d.pos, n, w, row0, nr, d.nvec, d.ncontrib);
     GEN_TRY(cudaGetLastError());
-    // offsets (host scans of n counts)
-    std::vector<int> nvec(n);
-    std::vector<unsigned long long> ncon(n);
-    GEN_TRY(cudaMemcpy(nvec.data(), d.nvec, sizeof(int) * n, cudaMemcpyDeviceToHost));
-    GEN_TRY(cudaMemcpy(ncon.data(), d.ncontrib, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost));
-    std::vector<long long> voff(size_t(n) + 1, 0), coff(size_t(n) + 1, 0);
-    for (int j = 0; j < n; j++) {
+    // offsets (host scans of the range's counts)
+    std::vector<int> nvec(nr);
+    std::vector<unsigned long long> ncon(nr);
+    GEN_TRY(cudaMemcpy(nvec.data(), d.nvec, sizeof(int) * nr, cudaMemcpyDeviceToHost));
+    GEN_TRY(cudaMemcpy(ncon.data(), d.ncontrib, sizeof(unsigned long long) * nr, cudaMemcpyDeviceToHost));
+    std::vector<long long> voff(size_t(nr) + 1, 0), coff(size_t(nr) + 1, 0);
+    for (int j = 0; j < nr; j++) {
         voff[j + 1] = voff[j] + nvec[j];
         coff[j + 1] = coff[j] + (long long)ncon[j];
     }
-    const long long nlist = voff[n], ncon_total = coff[n];
-    GEN_TRY(galloc(&d.voff, size_t(n) + 1));
-    GEN_TRY(galloc(&d.coff, size_t(n) + 1));
-    GEN_TRY(galloc(&d.cursor, n));
+    const long long nlist = voff[nr], ncon_total = coff[nr];
+    GEN_TRY(galloc(&d.voff, size_t(nr) + 1));
+    GEN_TRY(galloc(&d.coff, size_t(nr) + 1));
+    GEN_TRY(galloc(&d.cursor, nr));
     GEN_TRY(galloc(&d.list, size_t(nlist)));
     GEN_TRY(galloc(&d.ccol, size_t(ncon_total)));
     GEN_TRY(galloc(&d.cval, size_t(ncon_total)));
-    GEN_TRY(galloc(&d.ucount, n));
+    GEN_TRY(galloc(&d.ucount, nr));
     GEN_TRY(galloc(&d.flag, 1));
-    GEN_TRY(cudaMemcpy(d.voff, voff.data(), sizeof(long long) * (size_t(n) + 1), cudaMemcpyHostToDevice));
-    GEN_TRY(cudaMemcpy(d.coff, coff.data(), sizeof(long long) * (size_t(n) + 1), cudaMemcpyHostToDevice));
-    GEN_TRY(cudaMemset(d.cursor, 0, sizeof(int) * n));
+    GEN_TRY(cudaMemcpy(d.voff, voff.data(), sizeof(long long) * (size_t(nr) + 1), cudaMemcpyHostToDevice));
+    GEN_TRY(cudaMemcpy(d.coff, coff.data(), sizeof(long long) * (size_t(nr) + 1), cudaMemcpyHostToDevice));
+    GEN_TRY(cudaMemset(d.cursor, 0, sizeof(int) * nr));
     GEN_TRY(cudaMemset(d.flag, 0, sizeof(int)));
-    fill_lists<<<grid, 256>>>(d.count, d.pos, n, w, d.voff, d.cursor, d.list);
-    sort_lists<<<grid, 256>>>(d.voff, n, d.list);
-    contributions<<<grid, 256>>>(d.count, d.pos, d.val, d.scale, n, w, rcond, shift, d.voff, d.list,
-                                 d.coff, d.ccol, d.cval);
-    fold_rows<<<std::min(n, 16 * sms), kFoldThreads>>>(d.coff, n, d.ccol, d.cval, d.ucount, d.flag);
+    fill_lists<<<grid, 256>>>(d.count, d.pos, n, w, row0, nr, d.voff, d.cursor, d.list);
+    sort_lists<<<grid, 256>>>(d.voff, nr, d.list);
+    contributions<<<grid, 256>>>(d.count, d.pos, d.val, d.scale, row0, nr, w, rcond, shift, d.voff,
+                                 d.list, d.coff, d.ccol, d.cval);
+    fold_rows<<<std::min(nr, 16 * sms), kFoldThreads>>>(d.coff, nr, d.ccol, d.cval, d.ucount, d.flag);
     GEN_TRY(cudaGetLastError());
     int flag = 0;
     GEN_TRY(cudaMemcpy(&flag, d.flag, sizeof(int), cudaMemcpyDeviceToHost));
     if (flag) return set_error(CGB_ERR_CAPACITY, "makea_device: a row exceeds the fold capacity");
-    std::vector<int> ucount(n);
-    GEN_TRY(cudaMemcpy(ucount.data(), d.ucount, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    std::vector<int> ucount(nr);
+    GEN_TRY(cudaMemcpy(ucount.data(), d.ucount, sizeof(int) * nr, cudaMemcpyDeviceToHost));
     long long nnz = 0;
-    for (int j = 0; j < n; j++) nnz += ucount[j];
+    for (int j = 0; j < nr; j++) nnz += ucount[j];
     out->nnz = nnz;
     if (nnz > 0x7fffffffLL)
-        return set_error(CGB_ERR_CAPACITY, "makea_device: nnz %lld overflows int32 rowstr", nnz);
+        return set_error(CGB_ERR_CAPACITY, "makea_device: nnz %lld of rows [%d, %d) overflows int32 rowstr",
+                         nnz, row0, row1);
     std::vector<int> &rowstr = out->h_rowstr;
-    rowstr.assign(size_t(n) + 1, 0);
-    for (int j = 0; j < n; j++) rowstr[j + 1] = rowstr[j] + ucount[j];
-    GEN_TRY(galloc(&d.rowstr, size_t(n) + 1));
+    rowstr.assign(size_t(nr) + 1, 0);
+    for (int j = 0; j < nr; j++) rowstr[j + 1] = rowstr[j] + ucount[j];
+    // the vectors and lists are spent (the copies above waited for the
+    // kernels): free them before the CSR is allocated, so the peak is the
+    // contributions plus the CSR
+    for (int **q : {&d.count, &d.pos, &d.nvec, &d.cursor})
+        if (*q) {
+            cudaFree(*q);
+            *q = nullptr;
+        }
+    for (double **q : {&d.val, &d.scale}) {
+        cudaFree(*q);
+        *q = nullptr;
+    }
+    cudaFree(d.list);
+    d.list = nullptr;
+    GEN_TRY(galloc(&d.rowstr, size_t(nr) + 1));
     GEN_TRY(galloc(&d.colidx, size_t(nnz)));
     GEN_TRY(galloc(&d.a, size_t(nnz)));
-    GEN_TRY(cudaMemcpy(d.rowstr, rowstr.data(), sizeof(int) * (size_t(n) + 1), cudaMemcpyHostToDevice));
-    compact<<<grid, 256>>>(d.coff, d.rowstr, n, d.ccol, d.cval, d.colidx, d.a);
+    GEN_TRY(cudaMemcpy(d.rowstr, rowstr.data(), sizeof(int) * (size_t(nr) + 1), cudaMemcpyHostToDevice));
+    compact<<<grid, 256>>>(d.coff, d.rowstr, nr, d.ccol, d.cval, d.colidx, d.a);
     GEN_TRY(cudaGetLastError());
     GEN_TRY(cudaDeviceSynchronize());
     // hand the CSR over (the buffers' destructor skips what it no longer owns)

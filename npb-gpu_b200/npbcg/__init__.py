@@ -174,6 +174,24 @@ _SIGNATURES = {
     "cgb_batch_fallbacks": (ctypes.c_int, [ctypes.c_void_p, _I32]),
     "cgb_gnn_attach_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                             ctypes.c_int]),
+    "cgb_part_rows": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "cgb_nccl_unique_id": (ctypes.c_int, [ctypes.c_void_p]),
+    "cgb_part_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _I32,
+                                       _I32, _F64, ctypes.c_void_p,
+                                       ctypes.POINTER(ctypes.c_void_p)]),
+    "cgb_part_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "cgb_part_create_generated": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                 ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                                 ctypes.POINTER(ctypes.c_void_p)]),
+    "cgb_part_power_iterate": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
+                                              ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.POINTER(ctypes.c_double)]),
+    "cgb_part_group_power_iterate": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_double, ctypes.c_int,
+                                                    ctypes.c_void_p, ctypes.c_void_p,
+                                                    ctypes.POINTER(ctypes.c_double)]),
     "cgb_host_alloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_longlong]),
     "cgb_host_free": (ctypes.c_int, [ctypes.c_void_p]),
     "cgb_device_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
@@ -738,3 +756,110 @@ class Batch:
         """0: every system on one CTA; larger systems get teams of CTAs below
         their work per CTA > frac x the batch's work per resident CTA."""
         _check(lib().cgb_batch_set_team_frac(self._h, float(frac)))
+
+
+NCCL_ID_BYTES = 128
+
+
+def part_rows(n, world, rank):
+    """Rows [row0, row1) that rank `rank` of `world` owns of an n-row matrix
+    (blocks of ceil(n / world) rows)."""
+    r0, r1 = ctypes.c_int(), ctypes.c_int()
+    _check(lib().cgb_part_rows(int(n), int(world), int(rank), ctypes.byref(r0), ctypes.byref(r1)))
+    return r0.value, r1.value
+
+
+def row_block(rowstr, colidx, a, row0, row1):
+    """Rows row0..row1-1 of a CSR, column indices kept global:
+    (rowstr rebased to 0, colidx, a)."""
+    k0, k1 = int(rowstr[row0]), int(rowstr[row1])
+    rs = (np.asarray(rowstr[row0:row1 + 1], np.int64) - k0).astype(np.int32)
+    return rs, np.ascontiguousarray(colidx[k0:k1], np.int32), np.ascontiguousarray(a[k0:k1], np.float64)
+
+
+def nccl_unique_id():
+    """A new NCCL unique id (bytes) for rank 0 to broadcast to the others."""
+    buf = ctypes.create_string_buffer(NCCL_ID_BYTES)
+    _check(lib().cgb_nccl_unique_id(buf))
+    return buf.raw
+
+
+def _id_buffer(nccl_id):
+    if nccl_id is None:
+        return None
+    if len(nccl_id) != NCCL_ID_BYTES:
+        raise CgbError(ERR_INVALID, f"nccl_id must be {NCCL_ID_BYTES} bytes")
+    return ctypes.create_string_buffer(bytes(nccl_id), NCCL_ID_BYTES)
+
+
+class Part:
+    """One rank's row block of a system split over GPUs (cgb_part).
+
+    `rowstr, colidx, a` are the WHOLE matrix's CSR; the rank keeps its own
+    rows (part_rows).  With `nccl_id` (the same bytes on every rank) the
+    constructor joins the world's NCCL communicator -- every rank must make
+    it -- and power_iterate is a collective call.  Without it, a world of
+    one solves alone and a larger world is driven from one process by
+    group_power_iterate."""
+
+    def __init__(self, rowstr, colidx, a, world=1, rank=0, nccl_id=None, device=0):
+        self.n = int(len(rowstr) - 1)
+        self.world, self.rank = int(world), int(rank)
+        self.rows = part_rows(self.n, world, rank)
+        self._keep = row_block(rowstr, colidx, a, *self.rows)
+        h = ctypes.c_void_p()
+        _check(lib().cgb_part_create(device, self.n, self.world, self.rank, *self._keep,
+                                     _id_buffer(nccl_id), ctypes.byref(h)))
+        self._h = h
+
+    @classmethod
+    def generated(cls, n, nonzer, shift, seed=SEED, rcond=RCOND, world=1, rank=0, nccl_id=None,
+                  device=0):
+        """This rank's rows of makea(n, nonzer, rcond, shift, seed), assembled
+        on the device (the whole matrix is never built)."""
+        self = cls.__new__(cls)
+        self.n, self.world, self.rank = int(n), int(world), int(rank)
+        self.rows = part_rows(n, world, rank)
+        self._keep = None
+        h = ctypes.c_void_p()
+        _check(lib().cgb_part_create_generated(device, n, nonzer, rcond, shift, seed, self.world,
+                                               self.rank, _id_buffer(nccl_id), ctypes.byref(h)))
+        self._h = h
+        return self
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cgb_part_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def power_iterate(self, niter, shift, cgitmax=25):
+        """The reference outer loop over this world; every rank calls it."""
+        z, r = np.zeros(niter), np.zeros(niter)
+        ms = ctypes.c_double()
+        _check(lib().cgb_part_power_iterate(self._h, niter, shift, cgitmax, _ptr(z), _ptr(r),
+                                            ctypes.byref(ms)))
+        return dict(zeta=z, rnorm=r, device_ms=ms.value)
+
+
+def group_power_iterate(parts, niter, shift, cgitmax=25):
+    """All ranks of one world (Part objects without an NCCL id, on one
+    device, in rank order) solved from this process."""
+    P = ctypes.c_void_p * len(parts)
+    hs = P(*[p._h.value for p in parts])
+    z, r = np.zeros(niter), np.zeros(niter)
+    ms = ctypes.c_double()
+    _check(lib().cgb_part_group_power_iterate(ctypes.cast(hs, ctypes.c_void_p), len(parts), niter,
+                                              shift, cgitmax, _ptr(z), _ptr(r), ctypes.byref(ms)))
+    return dict(zeta=z, rnorm=r, device_ms=ms.value)
