@@ -12,9 +12,12 @@ Metric: SpMV-equivalent HBM GB/s = (SpMV algorithmic bytes x SpMVs per solve)
 / solve time, next to time-to-zeta (the solve's wall time with zeta within
 1e-10 of the reference verification value).
 
-Multi-GPU (torchrun, one rank per GPU): the single system does not shard, so
-each rank solves its own replica (weak scaling, no data-path collective);
-value = all ranks' bytes / the slowest rank's time.
+Multi-GPU (torchrun, one rank per GPU): the class-B system is too small to
+shard, so each rank solves its own replica (weak scaling, no data-path
+collective); value = all ranks' bytes / the slowest rank's time.  Beside it,
+`row_partitioned` splits one class-D system by rows over all ranks (strong
+scaling: NCCL all-gather of p and two scalar all-reduces per CG step), and
+`batched` shards the uneven batch by system.
 
 `--impl reference` times the reference's own CPU code (oracle/_ref, the
 reference cg.cu compiled as is: serial, it has no threading) on the same
@@ -478,6 +481,54 @@ def batched_section(npbcg, device, nsys=512, niter=15, rank=0, world=1, dist=Non
 CLASSES = None
 
 
+PART_CLASS = dict(name="D", n=1500000, nonzer=21, niter=100, shift=500.0, zeta=52.514532105794)
+
+
+def row_partitioned_section(npbcg, device, rank, world, dist):
+    """Class D as one system split by rows over the ranks (npbcg.Part: each
+    rank generates and holds its row block; per CG step an NCCL all-gather
+    of p and two scalar all-reduces, all on the device).  Every rank takes
+    the same steps; the time is the slowest rank's device time."""
+    import torch
+    c = PART_CLASS
+    nid = npbcg.nccl_unique_id() if rank == 0 else None
+    if dist is not None:
+        box = [nid]
+        dist.broadcast_object_list(box, src=0)
+        nid = box[0]
+    part = npbcg.Part.generated(c["n"], c["nonzer"], c["shift"], world=world, rank=rank,
+                                nccl_id=nid, device=device)
+    try:
+        part.power_iterate(1, c["shift"])  # warm-up (the reference's untimed step)
+        if dist is not None:
+            dist.barrier()
+        out = part.power_iterate(c["niter"], c["shift"])
+        ms, nnz = out["device_ms"], part.nnz
+        if dist is not None:
+            dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+            t = torch.tensor([ms, float(nnz)], dtype=torch.float64, device=dev)
+            tmax = t.clone()
+            dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+            dist.all_reduce(t)
+            ms, nnz = float(tmax[0].item()), int(t[1].item())
+    finally:
+        part.close()
+    if rank != 0:
+        return None
+    zeta = float(out["zeta"][-1])
+    solve_bytes = c["niter"] * (CGITMAX + 1) * spmv_bytes(c["n"], nnz)
+    return {
+        "what": f"NPB class {c['name']} (n={c['n']}, nnz={nnz}) split into {world} row block(s), "
+                "one per rank, generated on each rank's GPU; reference algorithm, "
+                f"{c['niter']} outer steps; NCCL all-gather of p + 2 scalar all-reduces per CG step, "
+                "outer step captured as a CUDA graph",
+        "ranks": world, "seconds": ms / 1e3, "ms_per_outer_step": ms / c["niter"],
+        "value": solve_bytes / (ms / 1e3) / 1e9, "unit": "GB/s (algorithmic, whole job)",
+        "zeta": zeta, "zeta_rel_err_vs_verify": abs(zeta - c["zeta"]) / c["zeta"],
+        "verified": abs(zeta - c["zeta"]) / c["zeta"] <= 1e-10,
+    }
+
+
 def our_arm(args, rank, world, local_rank):
     import torch
     import npbcg
@@ -638,6 +689,10 @@ def our_arm(args, rank, world, local_rank):
                 "openmp_port": {"value": sample_bytes / omp_s / 1e9, "unit": "GB/s",
                                 "cores": threads, "kind": "port", "seconds": omp_s},
             }
+    if not args.no_partitioned:
+        part = row_partitioned_section(npbcg, device, rank, world, dist)
+        if line is not None:
+            line["row_partitioned"] = part
     if not args.no_batched:
         # every rank solves its shard of the batched workload; rank 0 gathers
         batched = batched_section(npbcg, device, rank=rank, world=world, dist=dist)
@@ -665,6 +720,8 @@ def main():
     ap.add_argument("--no-solver-modes", action="store_true",
                     help="skip the class C comparison of the solver modes")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-partitioned", action="store_true",
+                    help="skip class D split by rows over the ranks")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     import npbcg

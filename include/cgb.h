@@ -417,6 +417,10 @@ int cgb_part_create(int device, int n, int world, int rank, const int *rowstr, c
                     const double *a, const void *nccl_id, cgb_part **out);
 int cgb_part_destroy(cgb_part *p);
 
+/* The part's rows [*row0, *row1) and its stored entries.  Any output may be
+ * NULL. */
+int cgb_part_info(const cgb_part *p, int *row0, int *row1, long long *nnz);
+
 /* One rank's share of the NPB matrix makea(n, nonzer, rcond, shift, seed)
  * generated on the device: only this rank's rows are assembled (the same
  * entries, bit for bit, as those rows of cgb_makea), so no rank -- and no

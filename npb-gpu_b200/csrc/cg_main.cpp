@@ -1,7 +1,7 @@
 // cg_main.cpp -- `cg`, a drop-in for the reference benchmark binary cg.<CLASS>
 // (GMAP/NPB-GPU CUDA/CG/cg.cu main(), :337-645) on top of libcgb's C ABI.
 //
-//   cg S|W|A|B|C|D          an NPB class (setparams.cpp:751-785 parameters)
+//   cg S|W|A|B|C|D|E        an NPB class (setparams.cpp:751-785 parameters)
 //   cg U --n N --nonzer K --niter I --shift S [--seed X]   custom sizes
 //   options: --mode fp64|tol|mixed|learned  --tol T  --cgitmax M
 //            --weights FILE (learned mode: network weights, raw FP32; default
@@ -9,6 +9,12 @@
 //            --device D  --json (one JSON result line instead of the report)
 //            --spmv row|sliced (SpMV plan; default: the autotuner's choice)
 //            --gpu-makea (generate the matrix with cgb_makea_device)
+//            --ranks K (the row-partitioned solver: the rows split into K
+//            blocks, each generated on the device, all K ranks driven from
+//            this process on one GPU; the reference algorithm only.  Class E
+//            always runs this way: its 6.4e9 entries overflow the int32 row
+//            pointers of one CSR, cg.cu:81, so it takes the fewest blocks of
+//            fewer than 2^31 entries each)
 //
 // Like the reference it generates the matrix (makea), runs the timed inverse
 // power iteration, prints the per-iteration "||r||  zeta" lines in the
@@ -44,6 +50,7 @@ const ClassParams kClasses[] = {
     {'B', 75000, 13, 75, 60.0, 22.712745482631},
     {'C', 150000, 15, 75, 110.0, 28.973605592845},
     {'D', 1500000, 21, 100, 500.0, 52.514532105794},
+    {'E', 9000000, 26, 100, 1500.0, 77.522164599383},
 };
 
 int fail(int st, const char *what)
@@ -55,10 +62,10 @@ int fail(int st, const char *what)
 void usage()
 {
     std::fprintf(stderr,
-                 "usage: cg S|W|A|B|C|D | cg U --n N --nonzer K --niter I --shift S [--seed X]\n"
+                 "usage: cg S|W|A|B|C|D|E | cg U --n N --nonzer K --niter I --shift S [--seed X]\n"
                  "          [--mode fp64|tol|mixed|learned] [--tol T] [--cgitmax M]\n"
                  "          [--weights FILE] [--device D] [--json] [--gpu-makea]\n"
-                 "          [--spmv row|sliced]\n");
+                 "          [--spmv row|sliced] [--ranks K]\n");
 }
 
 // The weights shipped with the package: <dir of this binary>/../npbcg/lp_weights.f32.
@@ -104,6 +111,33 @@ int attach_learned(cgb_session *s, const std::string &path, int device, int n,
     return st ? fail(st, "learned preconditioner") : 0;
 }
 
+// The row-partitioned solve: K row blocks generated on the device, one
+// untimed outer step (as the reference's untimed iteration, cg.cu:453-482),
+// then the timed niter steps.  Fills the traces, the device milliseconds
+// and the stored entries.
+int run_partitioned(const ClassParams &P, double seed, int K, int cgitmax, int device,
+                    std::vector<double> &zeta, std::vector<double> &rnorm, double *ms,
+                    long long *nnz)
+{
+    std::vector<cgb_part *> parts(size_t(K), nullptr);
+    int st = CGB_OK;
+    *nnz = 0;
+    for (int r = 0; r < K && !st; r++) {
+        st = cgb_part_create_generated(device, P.n, P.nonzer, 0.1, P.shift, seed, K, r, nullptr, &parts[r]);
+        long long k = 0;
+        if (!st) st = cgb_part_info(parts[r], nullptr, nullptr, &k);
+        *nnz += k;
+    }
+    if (!st) st = cgb_part_group_power_iterate(parts.data(), K, 1, P.shift, cgitmax, nullptr, nullptr, nullptr);
+    if (!st)
+        st = cgb_part_group_power_iterate(parts.data(), K, P.niter, P.shift, cgitmax, zeta.data(),
+                                          rnorm.data(), ms);
+    const int failed = st;
+    for (cgb_part *p : parts)
+        if (p) cgb_part_destroy(p);
+    return failed ? fail(failed, "partitioned solve") : 0;
+}
+
 }  // namespace
 
 int main(int argc, char **argv)
@@ -126,7 +160,7 @@ int main(int argc, char **argv)
     }
     double seed = 314159265.0, tol = 1e-12;
     std::string weights;
-    int mode = CGB_MODE_FP64, cgitmax = 25, device = 0, json = 0, gpu_makea = 0, spmv = 0;
+    int mode = CGB_MODE_FP64, cgitmax = 25, device = 0, json = 0, gpu_makea = 0, spmv = 0, ranks = 0;
     for (int i = 2; i < argc; i++) {
         const std::string a = argv[i];
         auto next = [&](void) -> const char * {
@@ -146,6 +180,7 @@ int main(int argc, char **argv)
         else if (a == "--device") device = std::atoi(next());
         else if (a == "--json") json = 1;
         else if (a == "--gpu-makea") gpu_makea = 1;
+        else if (a == "--ranks") ranks = std::atoi(next());
         else if (a == "--spmv") {
             const std::string k = next();
             if (k == "row") spmv = 1;
@@ -177,60 +212,80 @@ int main(int argc, char **argv)
     }
     // a custom size or another seed has no verification value (cg.cu:548-551)
     const bool verify = known && seed == 314159265.0;
-
     const long long cap = cgb_nz_bound(P.n, P.nonzer);
-    std::vector<int> rowstr(P.n + 1), colidx(cap);
-    std::vector<double> a(cap);
-    long long nnz = 0;
-    int st = gpu_makea ? cgb_makea_device(device, P.n, P.nonzer, 0.1, P.shift, seed, rowstr.data(),
-                                          colidx.data(), a.data(), cap, &nnz)
-                       : cgb_makea(P.n, P.nonzer, 0.1, P.shift, seed, rowstr.data(), colidx.data(),
-                                   a.data(), cap, &nnz);
-    if (st) return fail(st, "makea");
-
-    cgb_options opt;
-    cgb_default_options(&opt);
-    opt.device = device;
-    opt.spmv_kernel = spmv;
-    cgb_session *s = nullptr;
-    st = cgb_create(P.n, rowstr.data(), colidx.data(), a.data(), &opt, &s);
-    if (st) return fail(st, "create");
-    if (mode == CGB_MODE_MIXED_LEARNED &&
-        attach_learned(s, weights.empty() ? default_weights() : weights, device, P.n, rowstr,
-                       colidx, a) != 0) {
-        cgb_destroy(s);
-        return 1;
+    if (ranks == 0 && cap > 0x7fffffffLL) ranks = int((cap + 0x7ffffffeLL) / 0x7fffffffLL);
+    if (ranks < 0 || (ranks > 0 && mode != CGB_MODE_FP64)) {
+        std::fprintf(stderr, "cg: --ranks K >= 1 runs the reference algorithm (--mode fp64) only\n");
+        return 2;
     }
 
-    cgb_solve_params sp;
-    cgb_default_solve_params(&sp);
-    sp.niter = P.niter;
-    sp.shift = P.shift;
-    sp.mode = mode;
-    sp.cgitmax = cgitmax;
-    sp.tol = tol;
-    // one untimed solve first, as the reference does one untimed iteration (cg.cu:453-482)
-    cgb_solve_result res;
-    st = cgb_power_iterate(s, &sp, nullptr, nullptr, nullptr, nullptr, &res);
-    if (st) return fail(st, "power_iterate (warm-up)");
+    double device_ms = 0.0, zeta_last = 0.0, rnorm_last = 0.0;
+    int total_inner = 0, kind = 0, panels = 0;
+    long long nnz = 0;
     std::vector<double> zeta(P.niter), rnorm(P.niter);
-    std::vector<int> iters(P.niter);
-    st = cgb_power_iterate(s, &sp, zeta.data(), rnorm.data(), iters.data(), nullptr, &res);
-    if (st) return fail(st, "power_iterate");
-    // the plan the autotuner chose: row (1) or sliced (2, 3 with the L2
-    // prefetch), and the sliced walk's row panels
-    int kind = 0, lpr = 0, grid = 0, block = 0, panels = 0, prec_panels = 0;
-    long long smem = 0, entries = 0;
-    if (cgb_plan_info(s, &kind, &lpr, &grid, &block, &smem, &entries) ||
-        cgb_plan_panels(s, &panels, &prec_panels))
-        kind = panels = 0;
-    cgb_destroy(s);
+    if (ranks > 0) {
+        if (run_partitioned(P, seed, ranks, cgitmax, device, zeta, rnorm, &device_ms, &nnz)) return 1;
+        zeta_last = zeta[P.niter - 1];
+        rnorm_last = rnorm[P.niter - 1];
+        total_inner = P.niter * cgitmax;
+        kind = 4;  // plan_kind 4: row blocks (panels = their count)
+        panels = ranks;
+    } else {
+        std::vector<int> rowstr(P.n + 1), colidx(cap);
+        std::vector<double> a(cap);
+        int st = gpu_makea ? cgb_makea_device(device, P.n, P.nonzer, 0.1, P.shift, seed, rowstr.data(),
+                                              colidx.data(), a.data(), cap, &nnz)
+                           : cgb_makea(P.n, P.nonzer, 0.1, P.shift, seed, rowstr.data(), colidx.data(),
+                                       a.data(), cap, &nnz);
+        if (st) return fail(st, "makea");
 
-    const double t = res.device_ms / 1e3;
+        cgb_options opt;
+        cgb_default_options(&opt);
+        opt.device = device;
+        opt.spmv_kernel = spmv;
+        cgb_session *s = nullptr;
+        st = cgb_create(P.n, rowstr.data(), colidx.data(), a.data(), &opt, &s);
+        if (st) return fail(st, "create");
+        if (mode == CGB_MODE_MIXED_LEARNED &&
+            attach_learned(s, weights.empty() ? default_weights() : weights, device, P.n, rowstr,
+                           colidx, a) != 0) {
+            cgb_destroy(s);
+            return 1;
+        }
+
+        cgb_solve_params sp;
+        cgb_default_solve_params(&sp);
+        sp.niter = P.niter;
+        sp.shift = P.shift;
+        sp.mode = mode;
+        sp.cgitmax = cgitmax;
+        sp.tol = tol;
+        // one untimed solve first, as the reference does one untimed iteration (cg.cu:453-482)
+        cgb_solve_result res;
+        st = cgb_power_iterate(s, &sp, nullptr, nullptr, nullptr, nullptr, &res);
+        if (st) return fail(st, "power_iterate (warm-up)");
+        std::vector<int> iters(P.niter);
+        st = cgb_power_iterate(s, &sp, zeta.data(), rnorm.data(), iters.data(), nullptr, &res);
+        if (st) return fail(st, "power_iterate");
+        // the plan the autotuner chose: row (1) or sliced (2, 3 with the L2
+        // prefetch), and the sliced walk's row panels
+        int lpr = 0, grid = 0, block = 0, prec_panels = 0;
+        long long smem = 0, entries = 0;
+        if (cgb_plan_info(s, &kind, &lpr, &grid, &block, &smem, &entries) ||
+            cgb_plan_panels(s, &panels, &prec_panels))
+            kind = panels = 0;
+        cgb_destroy(s);
+        device_ms = res.device_ms;
+        zeta_last = res.zeta;
+        rnorm_last = res.rnorm;
+        total_inner = res.total_inner;
+    }
+
+    const double t = device_ms / 1e3;
     const double nz1 = double(P.nonzer) * (P.nonzer + 1);
     const double mops =
         t > 0 ? 2.0 * P.niter * P.n * (3.0 + nz1 + 25.0 * (5.0 + nz1) + 3.0) / t / 1e6 : 0.0;
-    const double err = verify ? std::fabs(res.zeta - P.zeta_verify) / P.zeta_verify : -1.0;
+    const double err = verify ? std::fabs(zeta_last - P.zeta_verify) / P.zeta_verify : -1.0;
     const bool ok = verify && err <= 1.0e-10;
 
     if (json) {
@@ -238,8 +293,8 @@ int main(int argc, char **argv)
                     "\"nnz\": %lld, \"mode\": %d, \"zeta\": %.17g, \"rnorm\": %.17g, "
                     "\"seconds\": %.9g, \"mops\": %.6g, \"inner_total\": %d, \"verified\": %s, "
                     "\"rel_err\": %.6g, \"plan_kind\": %d, \"panels\": %d}\n",
-                    P.name, P.n, P.nonzer, P.niter, P.shift, nnz, mode, res.zeta, res.rnorm, t,
-                    mops, res.total_inner, verify ? (ok ? "true" : "false") : "null", err, kind,
+                    P.name, P.n, P.nonzer, P.niter, P.shift, nnz, mode, zeta_last, rnorm_last, t,
+                    mops, total_inner, verify ? (ok ? "true" : "false") : "null", err, kind,
                     panels);
         return verify && !ok ? 1 : 0;
     }
@@ -253,11 +308,11 @@ int main(int argc, char **argv)
     if (verify) {
         if (ok) {
             std::printf(" VERIFICATION SUCCESSFUL\n");
-            std::printf(" Zeta is    %20.13e\n", res.zeta);
+            std::printf(" Zeta is    %20.13e\n", zeta_last);
             std::printf(" Error is   %20.13e\n", err);
         } else {
             std::printf(" VERIFICATION FAILED\n");
-            std::printf(" Zeta                %20.13e\n", res.zeta);
+            std::printf(" Zeta                %20.13e\n", zeta_last);
             std::printf(" The correct zeta is %20.13e\n", P.zeta_verify);
         }
     } else {
@@ -276,7 +331,8 @@ int main(int argc, char **argv)
     if (!verify) std::printf(" Verification    =            NOT PERFORMED\n");
     else std::printf(" Verification    =             %12s\n", ok ? "SUCCESSFUL" : "UNSUCCESSFUL");
     std::printf(" Mode            = %s\n", mode_names[mode & 3]);
-    std::printf(" Inner CG steps  =             %12d\n", res.total_inner);
+    std::printf(" Inner CG steps  =             %12d\n", total_inner);
     std::printf(" Nonzeros        =             %12lld\n", nnz);
+    if (ranks > 0) std::printf(" Row blocks      =             %12d\n", ranks);
     return verify && !ok ? 1 : 0;
 }

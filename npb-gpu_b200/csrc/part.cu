@@ -672,6 +672,15 @@ int cgb_part_create_generated(int device, int n, int nonzer, double rcond, doubl
     return CGB_OK;
 }
 
+int cgb_part_info(const cgb_part *p, int *row0, int *row1, long long *nnz)
+{
+    if (!p) return set_error(CGB_ERR_INVALID, "part: null part");
+    if (row0) *row0 = p->row0;
+    if (row1) *row1 = p->row0 + p->n_own;
+    if (nnz) *nnz = p->nnz;
+    return CGB_OK;
+}
+
 int cgb_part_destroy(cgb_part *p)
 {
     part_release(p);

@@ -181,6 +181,8 @@ _SIGNATURES = {
                                        _I32, _F64, ctypes.c_void_p,
                                        ctypes.POINTER(ctypes.c_void_p)]),
     "cgb_part_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "cgb_part_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)]),
     "cgb_part_create_generated": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                  ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                                  ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
@@ -843,6 +845,13 @@ class Part:
 
     def __exit__(self, *exc):
         self.close()
+
+    @property
+    def nnz(self):
+        """Stored entries of this rank's rows."""
+        k = ctypes.c_longlong()
+        _check(lib().cgb_part_info(self._h, None, None, ctypes.byref(k)))
+        return k.value
 
     def power_iterate(self, niter, shift, cgitmax=25):
         """The reference outer loop over this world; every rank calls it."""

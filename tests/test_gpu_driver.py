@@ -61,6 +61,13 @@ def test_driver_rejects_bad_arguments():
         assert "usage: cg" in r.stderr
 
 
+def test_driver_row_blocks_take_the_reference_algorithm_only():
+    r = run_cg("S", "--ranks", "2", "--mode", "mixed", timeout=60)
+    assert r.returncode == 2 and "--ranks" in r.stderr
+    r = run_cg("S", "--ranks", "-1", timeout=60)
+    assert r.returncode == 2
+
+
 def test_driver_fails_loudly_without_a_gpu():
     import npbcg
     try:
@@ -133,3 +140,20 @@ def test_driver_class_c_json(golden):
     assert line["inner_total"] == 25 * niter
     want = reference_mops(niter, n, nonzer, line["seconds"])
     assert abs(line["mops"] - want) <= 1e-5 * want
+
+
+@pytest.mark.gpu
+def test_driver_row_blocks_class_s_match_reference(golden):
+    """`cg S --ranks 3`: the row-partitioned solver (three row blocks
+    generated on the device) prints the reference's trace and verifies."""
+    n, nonzer, niter, shift = PARAMS["S"]
+    r = run_cg("S", "--ranks", "3")
+    assert r.returncode == 0, r.stderr
+    its, rn, ze = parse_trace(r.stdout)
+    e = golden["S"]["seeds"]["314159265.0"]
+    assert its == list(range(1, niter + 1))
+    assert np.max(np.abs(ze - np.array(e["zeta"])) / np.array(e["zeta"])) <= 1e-10
+    assert np.max(np.abs(rn - np.array(e["rnorm"]))) <= 1e-10
+    assert field(r.stdout, "Verification") == "SUCCESSFUL"
+    assert int(field(r.stdout, "Nonzeros")) == e["nnz"]
+    assert int(field(r.stdout, "Row blocks")) == 3
