@@ -481,7 +481,7 @@ def batched_section(npbcg, device, nsys=512, niter=15, rank=0, world=1, dist=Non
 CLASSES = None
 
 
-PART_CLASS = dict(name="D", n=1500000, nonzer=21, niter=100, shift=500.0, zeta=52.514532105794)
+PART_CLASS = "D"
 
 
 def row_partitioned_section(npbcg, device, rank, world, dist):
@@ -490,14 +490,31 @@ def row_partitioned_section(npbcg, device, rank, world, dist):
     of p and two scalar all-reduces, all on the device).  Every rank takes
     the same steps; the time is the slowest rank's device time."""
     import torch
-    c = PART_CLASS
+    c = dict(npbcg.CLASSES[PART_CLASS], name=PART_CLASS)
     nid = npbcg.nccl_unique_id() if rank == 0 else None
+    dev = "cuda" if dist is None or dist.get_backend() == "nccl" else "cpu"
     if dist is not None:
         box = [nid]
         dist.broadcast_object_list(box, src=0)
         nid = box[0]
-    part = npbcg.Part.generated(c["n"], c["nonzer"], c["shift"], world=world, rank=rank,
-                                nccl_id=nid, device=device)
+    # every rank builds its block first; the communicator is joined only
+    # when all of them have one, so a rank that failed cannot leave the
+    # others waiting in a collective
+    part, err = None, None
+    try:
+        part = npbcg.Part.generated(c["n"], c["nonzer"], c["shift"], world=world, rank=rank,
+                                    device=device)
+    except npbcg.CgbError as e:
+        err = str(e)
+    ok = torch.tensor([0.0 if part is None else 1.0], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(ok, op=dist.ReduceOp.MIN)
+    if ok.item() < 1.0:
+        if part is not None:
+            part.close()
+        return {"unavailable": err or "another rank could not build its row block"} if rank == 0 else None
+    part.join(nid)
+    part.set_wait_limit(300.0)
     try:
         part.power_iterate(1, c["shift"])  # warm-up (the reference's untimed step)
         if dist is not None:
@@ -505,7 +522,6 @@ def row_partitioned_section(npbcg, device, rank, world, dist):
         out = part.power_iterate(c["niter"], c["shift"])
         ms, nnz = out["device_ms"], part.nnz
         if dist is not None:
-            dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
             t = torch.tensor([ms, float(nnz)], dtype=torch.float64, device=dev)
             tmax = t.clone()
             dist.all_reduce(tmax, op=dist.ReduceOp.MAX)

@@ -417,6 +417,17 @@ int cgb_part_create(int device, int n, int world, int rank, const int *rowstr, c
                     const double *a, const void *nccl_id, cgb_part **out);
 int cgb_part_destroy(cgb_part *p);
 
+/* Joins the world's NCCL communicator (a collective call: every rank makes
+ * it with the same id) -- for parts created without an id, e.g. after every
+ * rank has checked that all ranks built their blocks. */
+int cgb_part_join(cgb_part *p, const void *nccl_id);
+
+/* Longest a rank waits for a solve's collectives (default 600 s).  A rank
+ * whose peers fail (NCCL's asynchronous error) or stay silent past the limit
+ * aborts its communicator and returns CGB_ERR_TIMEOUT / CGB_ERR_CUDA instead
+ * of waiting for ever; the part then makes no more collectives. */
+int cgb_part_set_wait_limit(cgb_part *p, double seconds);
+
 /* The part's rows [*row0, *row1) and its stored entries.  Any output may be
  * NULL. */
 int cgb_part_info(const cgb_part *p, int *row0, int *row1, long long *nnz);

@@ -26,10 +26,12 @@
 #include <nccl.h>  // types only: the functions are looked up at run time
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "cgb_internal.h"
@@ -61,6 +63,8 @@ struct NcclApi {
     ncclResult_t (*all_gather)(const void *, void *, size_t, ncclDataType_t, ncclComm_t,
                                cudaStream_t) = nullptr;
     const char *(*error_string)(ncclResult_t) = nullptr;
+    ncclResult_t (*comm_abort)(ncclComm_t) = nullptr;
+    ncclResult_t (*async_error)(ncclComm_t, ncclResult_t *) = nullptr;
     bool ok = false;
 };
 
@@ -80,8 +84,10 @@ const NcclApi *nccl()
         a.all_reduce = reinterpret_cast<decltype(a.all_reduce)>(dlsym(h, "ncclAllReduce"));
         a.all_gather = reinterpret_cast<decltype(a.all_gather)>(dlsym(h, "ncclAllGather"));
         a.error_string = reinterpret_cast<decltype(a.error_string)>(dlsym(h, "ncclGetErrorString"));
+        a.comm_abort = reinterpret_cast<decltype(a.comm_abort)>(dlsym(h, "ncclCommAbort"));
+        a.async_error = reinterpret_cast<decltype(a.async_error)>(dlsym(h, "ncclCommGetAsyncError"));
         a.ok = a.get_unique_id && a.comm_init_rank && a.comm_destroy && a.all_reduce &&
-               a.all_gather && a.error_string;
+               a.all_gather && a.error_string && a.comm_abort && a.async_error;
         g_nccl = a;
     });
     return g_nccl.ok ? &g_nccl : nullptr;
@@ -158,13 +164,112 @@ __global__ void __launch_bounds__(kBlock) k_start(PartArgs P, int slot)
 
 // q = A p for the own rows (p gathered whole); local p.q (kLocD) unless
 // `dot` is 0.
+// L2 hints: the matrix stream is read once a product (evict_first, not
+// kept in L1); the gathered vector -- up to 72 MB at class E, within the
+// 126 MB L2 -- is read ~nnz/n times a product (evict_last).
+__device__ __forceinline__ uint64_t policy_first()
+{
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, %1;" : "=l"(pol) : "f"(1.f));
+    return pol;
+}
+
+__device__ __forceinline__ uint64_t policy_last()
+{
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, %1;" : "=l"(pol) : "f"(1.f));
+    return pol;
+}
+
+__device__ __forceinline__ int2 ld_cols2(const int *p, uint64_t pol)
+{
+    int2 v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.s32 {%0, %1}, [%2], %3;"
+        : "=r"(v.x), "=r"(v.y)
+        : "l"(p), "l"(pol));
+    return v;
+}
+
+__device__ __forceinline__ int ld_col1(const int *p, uint64_t pol)
+{
+    int v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
+__device__ __forceinline__ double ld_val1(const double *p, uint64_t pol)
+{
+    double v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
+__device__ __forceinline__ double ld_gather(const double *p, uint64_t pol)
+{
+    double v;
+    asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
+// q = A p over this CTA's rows [r0, r1): LPR lanes a row, two entries a lane
+// a load (pair loads from even entries; the last entry of the block alone),
+// four loads in flight, lanes summed by a fixed xor tree.  Returns this
+// thread's share of dotv . q.
+template <int LPR>
+__device__ __forceinline__ double part_rows(const MatrixView &M, const double *__restrict__ v,
+                                            double *out, int r0, int r1, const double *dotv)
+{
+    constexpr int kStep = 2 * LPR, kUnroll = 4;
+    const uint64_t first = policy_first(), last = policy_last();
+    const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
+    const unsigned mask =
+        LPR == 32 ? 0xffffffffu : (((1u << LPR) - 1u) << ((threadIdx.x & 31) & ~(LPR - 1)));
+    const long long end = M.csr_entries;
+    double dacc = 0.0;
+    for (int row = r0 + grp; row < r1; row += ngrp) {
+        const int k0 = __ldg(M.rowstr + row), k1 = __ldg(M.rowstr + row + 1);
+        double s = 0.0;
+        for (int k = (k0 & ~1) + 2 * lane; k < k1; k += kUnroll * kStep) {
+            double2 av[kUnroll];
+            int2 cv[kUnroll];
+#pragma unroll
+            for (int u = 0; u < kUnroll; u++) {
+                const int kk = k + u * kStep;
+                if (kk < k1) {
+                    if (kk + 1 < end) {
+                        av[u] = ld_stream(reinterpret_cast<const double2 *>(M.a + kk), first);
+                        cv[u] = ld_cols2(M.colidx + kk, first);
+                    } else {
+                        av[u] = make_double2(ld_val1(M.a + kk, first), 0.0);
+                        cv[u] = make_int2(ld_col1(M.colidx + kk, first), 0);
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kUnroll; u++) {
+                const int kk = k + u * kStep;
+                if (kk < k1) {
+                    if (kk >= k0) s = fma(av[u].x, ld_gather(v + cv[u].x, last), s);
+                    if (kk + 1 < k1) s = fma(av[u].y, ld_gather(v + cv[u].y, last), s);
+                }
+            }
+        }
+        s = group_sum<LPR>(s, mask);
+        if (lane == 0) {
+            out[row] = s;
+            if (dotv) dacc = fma(dotv[row], s, dacc);
+        }
+    }
+    return dacc;
+}
+
 template <int LPR>
 __global__ void __launch_bounds__(kBlock) k_spmv(PartArgs P, MatrixView M, const double *pfull,
                                                  double *out, int dot)
 {
     int r0, r1;
     cta_rows(P.n_own, r0, r1);
-    double acc = spmv_rows<LPR, double>(M, pfull, out, r0, r1, dot ? P.pown : nullptr);
+    double acc = part_rows<LPR>(M, pfull, out, r0, r1, dot ? P.pown : nullptr);
     if (dot) grid_sums(&acc, 1, P.part, P.ticket, P.sc + kLocD);
 }
 
@@ -263,7 +368,9 @@ struct cgb_part {
     unsigned *d_ticket = nullptr;
     int trace_cap = 0;
     ncclComm_t comm = nullptr;
-    bool warmed = false;  // the communicator's first collectives made
+    bool warmed = false;   // the communicator's first collectives made
+    bool aborted = false;  // the communicator was aborted (a peer failed or a wait ran out)
+    double wait_limit_s = 600.0;
 };
 
 namespace {
@@ -456,11 +563,54 @@ int enqueue_step(cgb_part *const *parts, int k, Collectives &C, double shift, in
     });
 }
 
+// Waits for `stream`.  With a communicator the wait is a poll that also
+// watches NCCL's asynchronous error state and the part's time limit: a
+// failed or silent peer makes this rank abort its communicator (its NCCL
+// kernels then return) instead of waiting for ever.  The part cannot make
+// collectives afterwards.
+int wait_stream(cgb_part *p, cudaStream_t stream)
+{
+    if (!p || !p->comm) {
+        PART_TRY(cudaStreamSynchronize(stream));
+        return CGB_OK;
+    }
+    const NcclApi *api = nccl();
+    const auto t0 = std::chrono::steady_clock::now();
+    auto seconds = [&] {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    };
+    for (;;) {
+        const cudaError_t e = cudaStreamQuery(stream);
+        if (e == cudaSuccess) return CGB_OK;
+        if (e != cudaErrorNotReady)
+            return set_error(CGB_ERR_CUDA, "part: the solve failed: %s", cudaGetErrorString(e));
+        ncclResult_t ar = ncclSuccess;
+        api->async_error(p->comm, &ar);
+        const bool expired = seconds() > p->wait_limit_s;
+        if ((ar != ncclSuccess && ar != ncclInProgress) || expired) {
+            api->comm_abort(p->comm);
+            p->comm = nullptr;
+            p->aborted = true;
+            // the aborted communicator's kernels return; give them a bounded while
+            const auto t1 = std::chrono::steady_clock::now();
+            while (cudaStreamQuery(stream) == cudaErrorNotReady &&
+                   std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count() < 10.0)
+                std::this_thread::sleep_for(std::chrono::microseconds(200));
+            return expired ? set_error(CGB_ERR_TIMEOUT, "part: rank %d waited %.0f s for its peers; "
+                                       "communicator aborted", p->rank, p->wait_limit_s)
+                           : set_error(CGB_ERR_CUDA, "part: NCCL reported %s; communicator aborted",
+                                       api->error_string(ar));
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
 // x = 1 and the step count 0 on every rank, then the outer step captured
 // once as a graph and launched niter times between ev0 and ev1.
 int run_solve(cgb_part *const *parts, int k, Collectives &C, int niter, double shift, int cgitmax,
               cudaStream_t stream, cudaEvent_t ev0, cudaEvent_t ev1)
 {
+    cgb_part *const watch = parts[0]->comm ? parts[0] : nullptr;
     for (int i = 0; i < k; i++) {
         cgb_part *p = parts[i];
         k_fill_ones<<<p->grid, kBlock, 0, stream>>>(p->d_x, p->m);
@@ -481,8 +631,8 @@ int run_solve(cgb_part *const *parts, int k, Collectives &C, int niter, double s
         e = cudaEventRecord(ev0, stream);
         for (int step = 0; step < niter && e == cudaSuccess; step++) e = cudaGraphLaunch(exec, stream);
         if (e == cudaSuccess) e = cudaEventRecord(ev1, stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) st = set_error(CGB_ERR_CUDA, "part: the solve failed: %s", cudaGetErrorString(e));
+        else st = wait_stream(watch, stream);
     }
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -550,20 +700,9 @@ int part_finish(cgb_part *p, const void *nccl_id)
     const double mean = double(p->nnz) / p->n_own;
     p->lpr = mean >= 96 ? 32 : mean >= 40 ? 16 : mean >= 16 ? 8 : mean >= 6 ? 4 : 2;
     if (!nccl_id) return CGB_OK;
-    const NcclApi *api = nccl();
-    if (!api) {
-        part_release(p);
-        return set_error(CGB_ERR_STATE, "part: libnccl.so.2 not found");
-    }
-    ncclUniqueId id;
-    std::memcpy(&id, nccl_id, sizeof(id));
-    const ncclResult_t r = api->comm_init_rank(&p->comm, p->world, id, p->rank);
-    if (r != ncclSuccess) {
-        p->comm = nullptr;
-        part_release(p);
-        return set_error(CGB_ERR_CUDA, "ncclCommInitRank: %s", api->error_string(r));
-    }
-    return CGB_OK;
+    const int st = cgb_part_join(p, nccl_id);
+    if (st) part_release(p);
+    return st;
 }
 
 int read_traces(cgb_part *p, int niter, double *zeta, double *rnorm)
@@ -672,6 +811,30 @@ int cgb_part_create_generated(int device, int n, int nonzer, double rcond, doubl
     return CGB_OK;
 }
 
+int cgb_part_join(cgb_part *p, const void *nccl_id)
+{
+    if (!p || !nccl_id) return set_error(CGB_ERR_INVALID, "part: null part or id");
+    if (p->comm || p->aborted) return set_error(CGB_ERR_STATE, "part: already joined a communicator");
+    PART_TRY(cudaSetDevice(p->device));
+    const NcclApi *api = nccl();
+    if (!api) return set_error(CGB_ERR_STATE, "part: libnccl.so.2 not found");
+    ncclUniqueId id;
+    std::memcpy(&id, nccl_id, sizeof(id));
+    const ncclResult_t r = api->comm_init_rank(&p->comm, p->world, id, p->rank);
+    if (r != ncclSuccess) {
+        p->comm = nullptr;
+        return set_error(CGB_ERR_CUDA, "ncclCommInitRank: %s", api->error_string(r));
+    }
+    return CGB_OK;
+}
+
+int cgb_part_set_wait_limit(cgb_part *p, double seconds)
+{
+    if (!p || !(seconds > 0.0)) return set_error(CGB_ERR_INVALID, "part: a positive limit required");
+    p->wait_limit_s = seconds;
+    return CGB_OK;
+}
+
 int cgb_part_info(const cgb_part *p, int *row0, int *row1, long long *nnz)
 {
     if (!p) return set_error(CGB_ERR_INVALID, "part: null part");
@@ -692,8 +855,10 @@ int cgb_part_power_iterate(cgb_part *p, int niter, double shift, int cgitmax, do
 {
     if (!p || niter < 1 || cgitmax < 1 || !std::isfinite(shift))
         return set_error(CGB_ERR_INVALID, "part: niter, cgitmax >= 1 and a finite shift required");
+    if (p->aborted) return set_error(CGB_ERR_STATE, "part: its communicator was aborted");
     if (!p->comm && p->world > 1)
-        return set_error(CGB_ERR_STATE, "part: a rank of world %d needs an NCCL id at create", p->world);
+        return set_error(CGB_ERR_STATE, "part: a rank of world %d needs a communicator (an NCCL id "
+                         "at create, or cgb_part_join)", p->world);
     PART_TRY(cudaSetDevice(p->device));
     int st = ensure_trace(p, niter);
     if (st) return st;
@@ -707,8 +872,9 @@ int cgb_part_power_iterate(cgb_part *p, int niter, double shift, int cgitmax, do
     if (!p->warmed) {
         // NCCL sets up its connections on a communicator's first collectives:
         // make them outside the capture (their results are overwritten)
-        if ((st = C.allreduce(kLocD, kGlobD, 1)) || (st = C.allgather(false))) return st;
-        PART_TRY(cudaStreamSynchronize(p->stream));
+        if ((st = C.allreduce(kLocD, kGlobD, 1)) || (st = C.allgather(false)) ||
+            (st = wait_stream(p, p->stream)))
+            return st;
         p->warmed = true;
     }
     st = run_solve(parts, 1, C, niter, shift, cgitmax, p->stream, p->ev0, p->ev1);

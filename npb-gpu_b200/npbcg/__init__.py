@@ -48,6 +48,10 @@ CLASSES = {
     "A": dict(n=14000, nonzer=11, niter=15, shift=20.0, zeta=17.130235054029),
     "B": dict(n=75000, nonzer=13, niter=75, shift=60.0, zeta=22.712745482631),
     "C": dict(n=150000, nonzer=15, niter=75, shift=110.0, zeta=28.973605592845),
+    # D and E: beyond what one CSR of this library holds in E's case (6.3e9
+    # entries); the row-partitioned solver (Part) runs both
+    "D": dict(n=1500000, nonzer=21, niter=100, shift=500.0, zeta=52.514532105794),
+    "E": dict(n=9000000, nonzer=26, niter=100, shift=1500.0, zeta=77.522164599383),
 }
 RCOND = 0.1
 SEED = 314159265.0
@@ -181,6 +185,8 @@ _SIGNATURES = {
                                        _I32, _F64, ctypes.c_void_p,
                                        ctypes.POINTER(ctypes.c_void_p)]),
     "cgb_part_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "cgb_part_join": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "cgb_part_set_wait_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "cgb_part_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)]),
     "cgb_part_create_generated": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -845,6 +851,14 @@ class Part:
 
     def __exit__(self, *exc):
         self.close()
+
+    def join(self, nccl_id):
+        """Joins the world's NCCL communicator (collective: every rank, same id)."""
+        _check(lib().cgb_part_join(self._h, _id_buffer(nccl_id)))
+
+    def set_wait_limit(self, seconds):
+        """Longest wait for the peers' collectives before the communicator is aborted."""
+        _check(lib().cgb_part_set_wait_limit(self._h, float(seconds)))
 
     @property
     def nnz(self):

@@ -5,11 +5,13 @@
     python npb-gpu_b200/npbcg/profile_case.py --cls B --what sweep
     python npb-gpu_b200/npbcg/profile_case.py --what batch --nsys 64 --niter 2
     python npb-gpu_b200/npbcg/profile_case.py --cls B --what barrier --reps 20000
+    python npb-gpu_b200/npbcg/profile_case.py --cls D --what part --ranks 1 --niter 1
 
 `spmv` launches the standalone FP64 SpMV+dot kernel `reps` times (after one
 warm-up launch); `solve` runs one power iteration of `niter` outer steps;
-`sweep` prints SpMV timings for every lanes-per-row choice.  Each prints one
-JSON line.
+`sweep` prints SpMV timings for every lanes-per-row choice; `part` runs the
+row-partitioned solver on `ranks` device-generated row blocks, all driven
+from this process.  Each prints one JSON line.
 """
 import argparse
 import json
@@ -23,7 +25,9 @@ import npbcg  # noqa: E402
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cls", default="B", choices=sorted(npbcg.CLASSES))
-    ap.add_argument("--what", default="spmv", choices=["spmv", "solve", "sweep", "batch", "barrier"])
+    ap.add_argument("--what", default="spmv",
+                    choices=["spmv", "solve", "sweep", "batch", "barrier", "part"])
+    ap.add_argument("--ranks", type=int, default=1, help="part: row blocks")
     ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed", "learned"],
                     help="solve / batch: the solver mode (mixed: tol 1e-12, cgitmax 100)")
     ap.add_argument("--nsys", type=int, default=64, help="batch: systems of the batched workload")
@@ -54,6 +58,16 @@ def main():
                               "device_ms": r["device_ms"], "policy": b.policy()}), flush=True)
         return
     c = npbcg.CLASSES[a.cls]
+    if a.what == "part":
+        parts = [npbcg.Part.generated(c["n"], c["nonzer"], c["shift"], world=a.ranks, rank=r)
+                 for r in range(a.ranks)]
+        r = npbcg.group_power_iterate(parts, a.niter, c["shift"])
+        print(json.dumps({"cls": a.cls, "what": "part", "ranks": a.ranks, "niter": a.niter,
+                          "nnz": sum(p.nnz for p in parts), "device_ms": r["device_ms"],
+                          "zeta": float(r["zeta"][-1])}), flush=True)
+        for p in parts:
+            p.close()
+        return
     rs, ci, av = npbcg.makea(c["n"], c["nonzer"], npbcg.RCOND, c["shift"])
     n, nnz = c["n"], len(av)
     out = {"cls": a.cls, "n": n, "nnz": nnz, "what": a.what}

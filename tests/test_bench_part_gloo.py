@@ -23,14 +23,23 @@ def free_port():
         return s.getsockname()[1]
 
 
-def fake_npbcg(npbcg, rank, seen):
+def fake_npbcg(npbcg, rank, seen, fail_rank=-1):
     class FakePart:
         @classmethod
         def generated(cls, n, nonzer, shift, world=1, rank=0, nccl_id=None, device=0):
-            seen.update(n=n, nonzer=nonzer, shift=shift, world=world, rank=rank, id=nccl_id.hex())
+            assert nccl_id is None  # the communicator is joined after every block is built
+            if rank == fail_rank:
+                raise npbcg.CgbError(npbcg.ERR_NOMEM, "out of device memory")
+            seen.update(n=n, nonzer=nonzer, shift=shift, world=world, rank=rank)
             self = cls()
             self.rank = rank
             return self
+
+        def join(self, nccl_id):
+            seen["id"] = nccl_id.hex()
+
+        def set_wait_limit(self, seconds):
+            seen["limit"] = seconds
 
         @property
         def nnz(self):
@@ -51,7 +60,7 @@ def fake_npbcg(npbcg, rank, seen):
     return fake
 
 
-def worker(rank, world, port, out_path):
+def worker(rank, world, port, out_path, fail_rank=-1):
     import datetime
     import sys
     import torch.distributed as dist
@@ -62,7 +71,8 @@ def worker(rank, world, port, out_path):
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
                             world_size=world, timeout=datetime.timedelta(seconds=60))
     seen = {}
-    out = bench.row_partitioned_section(fake_npbcg(npbcg, rank, seen), 0, rank, world, dist)
+    out = bench.row_partitioned_section(fake_npbcg(npbcg, rank, seen, fail_rank), 0, rank, world,
+                                        dist)
     with open(f"{out_path}.{rank}", "w") as f:
         json.dump({"out": out, "seen": seen}, f)
     dist.barrier()
@@ -85,3 +95,17 @@ def test_row_partitioned_section_two_ranks(tmp_path):
     o = got[0]["out"]
     assert o["ranks"] == 2 and o["seconds"] == pytest.approx(0.110)  # the slowest rank
     assert "nnz=2001" in o["what"] and o["verified"]
+
+
+def test_row_partitioned_section_rank_fails_to_build(tmp_path):
+    """A rank that cannot build its block: no rank joins the communicator or
+    enters a collective of the solve; rank 0 reports the section unavailable."""
+    import torch.multiprocessing as mp
+    out_path = str(tmp_path / "part.json")
+    mp.start_processes(worker, args=(2, free_port(), out_path, 1), nprocs=2, join=True,
+                       start_method="spawn")
+    got = [json.load(open(f"{out_path}.{r}")) for r in range(2)]
+    assert "unavailable" in got[0]["out"] and got[1]["out"] is None
+    for r in range(2):
+        assert "id" not in got[r]["seen"] and "calls" not in got[r]["seen"]
+    assert got[0]["seen"].get("closed")  # rank 0 built its block and released it
