@@ -33,7 +33,77 @@ class Oracle:
                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                           ctypes.POINTER(ctypes.c_double)]
         lib.orc_max_threads.restype = ctypes.c_int
+        # MG (mg_oracle.c)
+        dp = ctypes.POINTER(ctypes.c_double)
+        lib.orc_mg_run.restype = ctypes.c_int
+        lib.orc_mg_run.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp,
+                                   ctypes.c_void_p, ctypes.c_void_p, dp]
+        lib.orc_mg_zran3.restype = None
+        lib.orc_mg_zran3.argtypes = [ctypes.c_int, F64, ctypes.c_void_p, ctypes.c_void_p]
+        lib.orc_mg_resid.restype = None
+        lib.orc_mg_resid.argtypes = [ctypes.c_int, F64, F64, F64, F64]
+        lib.orc_mg_psinv.restype = None
+        lib.orc_mg_psinv.argtypes = [ctypes.c_int, F64, F64, F64]
+        lib.orc_mg_rprj3.restype = None
+        lib.orc_mg_rprj3.argtypes = [ctypes.c_int, F64, ctypes.c_int, F64]
+        lib.orc_mg_interp.restype = None
+        lib.orc_mg_interp.argtypes = [ctypes.c_int, F64, ctypes.c_int, F64]
+        lib.orc_mg_norm2u3.restype = None
+        lib.orc_mg_norm2u3.argtypes = [ctypes.c_int, F64, dp, dp]
         self.lib = lib
+
+    # ---- MG: grids are float64 cubes of side m, index (i3 * m + i2) * m + i1
+    MG_A = np.array([-8.0 / 3.0, 0.0, 1.0 / 6.0, 1.0 / 12.0])
+    MG_C = (np.array([-3.0 / 8.0, 1.0 / 32.0, -1.0 / 64.0, 0.0]),
+            np.array([-3.0 / 17.0, 1.0 / 33.0, -1.0 / 61.0, 0.0]))
+
+    def mg_run(self, lt, nit, smoother, grids=False):
+        m = (1 << lt) + 2
+        a, b, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        u = np.zeros(m ** 3) if grids else None
+        r = np.zeros(m ** 3) if grids else None
+        rc = self.lib.orc_mg_run(lt, nit, smoother, ctypes.byref(a), ctypes.byref(b),
+                                 None if u is None else u.ctypes.data,
+                                 None if r is None else r.ctypes.data, ctypes.byref(t))
+        if rc != 0:
+            raise RuntimeError(f"orc_mg_run failed: {rc}")
+        out = dict(rnm2=a.value, rnmu=b.value, seconds=t.value)
+        if grids:
+            out.update(u=u, r=r)
+        return out
+
+    def mg_zran3(self, m):
+        v = np.zeros(m ** 3)
+        plus, minus = np.zeros(30, np.int32), np.zeros(30, np.int32)
+        self.lib.orc_mg_zran3(m, v, plus.ctypes.data, minus.ctypes.data)
+        return v, plus.reshape(10, 3), minus.reshape(10, 3)
+
+    def mg_resid(self, m, u, v):
+        r = np.zeros(m ** 3)
+        self.lib.orc_mg_resid(m, np.ascontiguousarray(u), np.ascontiguousarray(v), r, self.MG_A)
+        return r
+
+    def mg_psinv(self, m, r, u, smoother):
+        u = np.array(u, dtype=np.float64)
+        self.lib.orc_mg_psinv(m, np.ascontiguousarray(r), u, self.MG_C[smoother])
+        return u
+
+    def mg_rprj3(self, mk, r):
+        mj = mk // 2 + 1
+        s = np.zeros(mj ** 3)
+        self.lib.orc_mg_rprj3(mk, np.ascontiguousarray(r), mj, s)
+        return s
+
+    def mg_interp(self, mj, z, u):
+        mk = 2 * mj - 2
+        u = np.array(u, dtype=np.float64)
+        self.lib.orc_mg_interp(mj, np.ascontiguousarray(z), mk, u)
+        return u
+
+    def mg_norm(self, m, r):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self.lib.orc_mg_norm2u3(m, np.ascontiguousarray(r), ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
 
     def makea(self, n, nonzer, rcond, shift, seed=314159265.0):
         cap = self.lib.orc_nz_bound(n, nonzer)
