@@ -455,6 +455,42 @@ int cgb_part_power_iterate(cgb_part *p, int niter, double shift, int cgitmax, do
 int cgb_part_group_power_iterate(cgb_part **parts, int k, int niter, double shift, int cgitmax,
                                  double *zeta_trace, double *rnorm_trace, double *device_ms);
 
+/* ---- NPB MG: the V-cycle multigrid benchmark ----------------------------
+ * The reference's MG (CUDA/MG/mg.cu): a multigrid V-cycle for the 3-D
+ * Poisson problem on a periodic 2^lt cube.  The right-hand side v is zero
+ * except +1 at the ten largest and -1 at the ten smallest values of the LCG
+ * laid over the grid (zran3, mg.cu:2175-2303); u starts at zero.  Classes
+ * (mg.cu:388-410): S lt 5 nit 4, W 7/4, A 8/4, B 8/20, C 9/20, D 10/50;
+ * smoother 0 (the S(a) coefficients) for S, W, A and 1 (S(b)) otherwise
+ * (mg.cu:422-442).  Grids are (2^lt + 2)^3 doubles with one ghost layer. */
+typedef struct cgb_mg cgb_mg;
+
+/* Grids for every level on `device`, v generated on the device. */
+int cgb_mg_create(int device, int lt, int smoother, cgb_mg **out);
+int cgb_mg_destroy(cgb_mg *g);
+
+/* The reference's timed region (mg.cu:498-508) from u = 0: resid, norm,
+ * nit x (V-cycle mg3P, resid), norm.  rnm2 = sqrt(sum r^2 / n^3), rnmu =
+ * max |r| of the final residual (norm2u3, mg.cu:1201-1230); device_ms the
+ * device time of the region (any output may be NULL).  Verify rnm2 against
+ * the class's value at relative 1e-8 (mg.cu:528-543). */
+int cgb_mg_run(cgb_mg *g, int nit, double *rnm2, double *rnmu, double *device_ms);
+
+/* The finest level's u (which 0), v (1) or r (2): (2^lt + 2)^3 doubles,
+ * index (i3 * m + i2) * m + i1. */
+int cgb_mg_read(cgb_mg *g, int which, double *out, long long count);
+
+/* zran3's points (i1, i2, i3), ten each: plus in ascending value (largest
+ * last), minus in descending value (smallest last), the reference's lists. */
+int cgb_mg_points(cgb_mg *g, int *plus, int *minus);
+
+/* One operator on host grids (tests): op 0 resid (in1 u, in2 v -> out r),
+ * 1 psinv (in1 r; out u, updated), 2 rprj3 (in1 r of side m -> out of side
+ * m/2 + 1), 3 interp (in1 z of side m; out u of side 2m - 2, added to),
+ * 4 interp assigning.  m even, at least 4. */
+int cgb_mg_apply(int device, int op, int m, int smoother, const double *in1, const double *in2,
+                 double *out);
+
 /* Host memory that the device copies at full speed (cudaHostAlloc). */
 int cgb_host_alloc(void **ptr, long long bytes);
 int cgb_host_free(void *ptr);

@@ -17,7 +17,9 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["session.cu", "noalloc.cu", "gnn.cu", "batch.cu", "makea_gpu.cu", "part.cu"]
+CU_SOURCES = ["session.cu", "noalloc.cu", "gnn.cu", "batch.cu", "makea_gpu.cu", "part.cu", "mg.cu"]
+# per-source flags: the MG operators keep the reference's separate roundings
+EXTRA_FLAGS = {"mg.cu": ["-fmad=false"]}
 CPP_SOURCES = ["makea.cpp"]
 LIB = os.path.join(LIBDIR, "libcgb.so")
 # the checked build: the single-system solver with every SpMV index tested
@@ -66,7 +68,7 @@ def build(verbose=False, ptxas_info=False, force=False):
         if force or sources_newer(o, [s] + headers):
             cmd = [nvcc(), "-c", s, "-o", o, *ARCH, "-O3", "-lineinfo", "-std=c++17",
                    "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
-                   "--expt-relaxed-constexpr"]
+                   "--expt-relaxed-constexpr", *EXTRA_FLAGS.get(src, [])]
             if ptxas_info:
                 cmd += ["-Xptxas", "-v"]
             r = run(cmd, verbose)

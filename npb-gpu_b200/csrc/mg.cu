@@ -1,0 +1,710 @@
+// mg.cu -- the NPB MG benchmark's V-cycle on the GPU: a multigrid solve of
+// the 3-D Poisson problem on a periodic 2^lt cube (GMAP/NPB-GPU
+// CUDA/MG/mg.cu: main's timed loop :498-508, mg3P :1078-1133).
+//
+// Grids are cubes of side m = 2^k + 2 (one ghost layer a face), x fastest,
+// one buffer per level for u and r, v on the finest level only.  Every
+// operator is one kernel that streams its grids once:
+//   resid   r = v - A u       (:1572-1625)  27-point, a[1] = 0
+//   psinv   u = u + C r       (:1395-1440)  27-point, c[3] = 0
+//   rprj3   s = P^T r         (:1724-1790)  full weighting onto the coarse grid
+//   interp  u (+)= P z        (:836-890)    trilinear prolongation
+//   norm2u3                   (:1201-1230)  deterministic two-level reduction
+// A warp covers 32 consecutive x of one (y, z) row: each lane forms the
+// row sums of its own column (the reference's u1/u2 line buffers) and takes
+// its neighbours' from the adjacent lanes by shuffles, so a point costs 10
+// loads instead of 27, all coalesced.  The periodic ghost exchange (comm3,
+// :687-716, which only copies interior values) is fused: the thread that
+// writes an interior point also writes that value into each ghost cell that
+// mirrors it.  On coarse levels the reference zeroes u and then adds the
+// prolongation; here interp assigns 0 + P z in one pass.
+//
+// Arithmetic: every sum in the reference's order and no fused multiply-add
+// (this file is compiled with -fmad=false), so each grid equals the serial
+// reference's operation for operation; only the norm's sum runs in another
+// (fixed) order.  The whole timed region is one CUDA graph.
+//
+// zran3 (:2175-2303): the LCG value of interior point (i1, i2, i3) is draw
+// L + 1 of the stream seeded 314159265 with multiplier 5^13, L = (i1-1) +
+// n (i2-1) + n^2 (i3-1).  Each thread jumps to its chunk's first draw and
+// steps through the chunk, keeping the values above 1 - C/N and below C/N
+// (a few hundred candidates); the host picks the ten largest and smallest
+// among them -- the values are distinct, so that is the reference's choice.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <utility>
+#include <vector>
+
+#include "cgb_internal.h"
+
+namespace cgb {
+namespace mg {
+
+constexpr int kMaxLevels = 11;   // lt <= 10: a 1024^3 grid (class D)
+constexpr int kRows = 8;         // (y) rows of a stencil CTA; x is a warp
+constexpr int kNormBlocks = 592;
+constexpr int kNormThreads = 256;
+constexpr int kCandCap = 8192;   // zran3 candidates kept per side
+constexpr int kChunk = 64;       // zran3 draws a thread steps through
+constexpr uint64_t kMask46 = (uint64_t(1) << 46) - 1;
+constexpr uint64_t kMult = 1220703125ull;  // 5^13
+constexpr uint64_t kSeed = 314159265ull;
+
+struct Coef {
+    double a0, a2, a3;  // resid: a[1] = 0 is left out, as the reference does
+    double c0, c1, c2;  // psinv: c[3] = 0 is left out
+};
+
+__device__ __forceinline__ size_t at(int m, int i3, int i2, int i1)
+{
+    return (size_t(i3) * m + i2) * m + i1;
+}
+
+// The indices along one axis that hold the value of interior index i: i
+// itself and, at the two ends, the ghost that mirrors it (comm3's copies).
+__device__ __forceinline__ int images(int m, int i, int *out)
+{
+    int k = 0;
+    out[k++] = i;
+    if (i == m - 2) out[k++] = 0;
+    if (i == 1) out[k++] = m - 1;
+    return k;
+}
+
+// g(i1, i2, i3) = val and every ghost cell that comm3 would fill from it.
+__device__ __forceinline__ void store_periodic(double *g, int m, int i3, int i2, int i1, double val)
+{
+    int x[2], y[2], z[2];
+    const int nx = images(m, i1, x), ny = images(m, i2, y), nz = images(m, i3, z);
+    for (int c = 0; c < nz; c++)
+        for (int b = 0; b < ny; b++)
+            for (int a = 0; a < nx; a++) g[at(m, z[c], y[b], x[a])] = val;
+}
+
+// Row sums of column i1 around (i2, i3): the four edge neighbours (s1,
+// the reference's u1) and the four corners (s2, its u2), in its order.
+__device__ __forceinline__ void column_sums(const double *__restrict__ g, int m, int i3, int i2,
+                                            int i1, double &s1, double &s2)
+{
+    s1 = g[at(m, i3, i2 - 1, i1)] + g[at(m, i3, i2 + 1, i1)] + g[at(m, i3 - 1, i2, i1)] +
+         g[at(m, i3 + 1, i2, i1)];
+    s2 = g[at(m, i3 - 1, i2 - 1, i1)] + g[at(m, i3 - 1, i2 + 1, i1)] + g[at(m, i3 + 1, i2 - 1, i1)] +
+         g[at(m, i3 + 1, i2 + 1, i1)];
+}
+
+// The column sums of x - 1, x, x + 1 for this lane (x = i1): its own, and
+// its neighbours' from the adjacent lanes, computed directly at the warp's
+// two ends.  Lanes past the row (i1 > m - 1) load nothing.
+struct Stencil {
+    double s1m, s1, s1p, s2m, s2, s2p;
+};
+
+__device__ __forceinline__ Stencil stencil_row(const double *__restrict__ g, int m, int i3, int i2,
+                                               int i1)
+{
+    const int lane = threadIdx.x & 31;
+    Stencil st;
+    st.s1 = st.s2 = 0.0;
+    if (i1 <= m - 1) column_sums(g, m, i3, i2, i1, st.s1, st.s2);
+    st.s1m = __shfl_up_sync(0xffffffffu, st.s1, 1);
+    st.s2m = __shfl_up_sync(0xffffffffu, st.s2, 1);
+    st.s1p = __shfl_down_sync(0xffffffffu, st.s1, 1);
+    st.s2p = __shfl_down_sync(0xffffffffu, st.s2, 1);
+    if (lane == 0 && i1 <= m - 2) column_sums(g, m, i3, i2, i1 - 1, st.s1m, st.s2m);
+    if (lane == 31 && i1 <= m - 2) column_sums(g, m, i3, i2, i1 + 1, st.s1p, st.s2p);
+    return st;
+}
+
+// r = v - A u on the interior (r may be v).  Block (32, kRows): x =
+// 1 + 32 bx + tx, y = 1 + kRows by + ty, z = 1 + bz.
+__global__ void __launch_bounds__(32 * kRows) k_resid(const double *__restrict__ u, const double *v,
+                                                      double *r, int m, Coef cf)
+{
+    const int i1 = 1 + int(blockIdx.x) * 32 + int(threadIdx.x);
+    const int i2 = 1 + int(blockIdx.y) * kRows + int(threadIdx.y);
+    const int i3 = 1 + int(blockIdx.z);
+    if (i2 > m - 2) return;  // whole warps: a warp is one row
+    const Stencil s = stencil_row(u, m, i3, i2, i1);
+    if (i1 > m - 2) return;
+    const size_t c = at(m, i3, i2, i1);
+    const double val = v[c] - cf.a0 * u[c] - cf.a2 * (s.s2 + s.s1m + s.s1p) - cf.a3 * (s.s2m + s.s2p);
+    store_periodic(r, m, i3, i2, i1, val);
+}
+
+// u = u + C r on the interior (in place: each point reads only its own u).
+__global__ void __launch_bounds__(32 * kRows) k_psinv(const double *__restrict__ r, double *u, int m,
+                                                      Coef cf)
+{
+    const int i1 = 1 + int(blockIdx.x) * 32 + int(threadIdx.x);
+    const int i2 = 1 + int(blockIdx.y) * kRows + int(threadIdx.y);
+    const int i3 = 1 + int(blockIdx.z);
+    if (i2 > m - 2) return;
+    const Stencil s = stencil_row(r, m, i3, i2, i1);
+    if (i1 > m - 2) return;
+    const size_t c = at(m, i3, i2, i1);
+    const double val = u[c] + cf.c0 * r[c] + cf.c1 * (r[c - 1] + r[c + 1] + s.s1) +
+                       cf.c2 * (s.s2 + s.s1m + s.s1p);
+    store_periodic(u, m, i3, i2, i1, val);
+}
+
+// s (side mj) = restriction of r (side mk = 2 mj - 2).  A thread per coarse
+// column j1 in [1, mj - 1]: its x1 / y1 (at fine i1 = 2 j1 - 1), the next
+// lane's for i1 + 2; outputs for j1 <= mj - 2.
+__global__ void __launch_bounds__(32 * kRows) k_rprj3(const double *__restrict__ r, int mk, double *s,
+                                                      int mj)
+{
+    const int lane = threadIdx.x & 31;
+    const int j1 = 1 + int(blockIdx.x) * 32 + int(threadIdx.x);
+    const int j2 = 1 + int(blockIdx.y) * kRows + int(threadIdx.y);
+    const int j3 = 1 + int(blockIdx.z);
+    if (j2 > mj - 2) return;
+    const int i1 = 2 * j1 - 1, i2 = 2 * j2 - 1, i3 = 2 * j3 - 1;
+    auto xy1 = [&](int x, double &x1, double &y1) {
+        x1 = r[at(mk, i3 + 1, i2, x)] + r[at(mk, i3 + 1, i2 + 2, x)] + r[at(mk, i3, i2 + 1, x)] +
+             r[at(mk, i3 + 2, i2 + 1, x)];
+        y1 = r[at(mk, i3, i2, x)] + r[at(mk, i3 + 2, i2, x)] + r[at(mk, i3, i2 + 2, x)] +
+             r[at(mk, i3 + 2, i2 + 2, x)];
+    };
+    double x1 = 0.0, y1 = 0.0;
+    if (j1 <= mj - 1) xy1(i1, x1, y1);
+    double x1p = __shfl_down_sync(0xffffffffu, x1, 1);
+    double y1p = __shfl_down_sync(0xffffffffu, y1, 1);
+    if (j1 > mj - 2) return;
+    if (lane == 31) xy1(i1 + 2, x1p, y1p);
+    const double y2 = r[at(mk, i3, i2, i1 + 1)] + r[at(mk, i3 + 2, i2, i1 + 1)] +
+                      r[at(mk, i3, i2 + 2, i1 + 1)] + r[at(mk, i3 + 2, i2 + 2, i1 + 1)];
+    const double x2 = r[at(mk, i3 + 1, i2, i1 + 1)] + r[at(mk, i3 + 1, i2 + 2, i1 + 1)] +
+                      r[at(mk, i3, i2 + 1, i1 + 1)] + r[at(mk, i3 + 2, i2 + 1, i1 + 1)];
+    const double val = 0.5 * r[at(mk, i3 + 1, i2 + 1, i1 + 1)] +
+                       0.25 * (r[at(mk, i3 + 1, i2 + 1, i1)] + r[at(mk, i3 + 1, i2 + 1, i1 + 2)] + x2) +
+                       0.125 * (x1 + x1p + y2) + 0.0625 * (y1 + y1p);
+    store_periodic(s, mj, j3, j2, j1, val);
+}
+
+// u (side mk = 2 mj - 2) += (or, assign: =) prolongation of z (side mj).
+// A thread per coarse cell (i1, i2, i3) in [0, mj - 2]^3 writes its eight
+// fine points as four pairs.  Covers every fine cell, ghosts included.
+__global__ void __launch_bounds__(32 * kRows) k_interp(const double *__restrict__ z, int mj, double *u,
+                                                       int mk, int assign)
+{
+    const int i1 = int(blockIdx.x) * 32 + int(threadIdx.x);
+    const int i2 = int(blockIdx.y) * kRows + int(threadIdx.y);
+    const int i3 = int(blockIdx.z);
+    if (i1 > mj - 2 || i2 > mj - 2) return;
+    const double z000 = z[at(mj, i3, i2, i1)], z001 = z[at(mj, i3, i2, i1 + 1)];
+    const double z010 = z[at(mj, i3, i2 + 1, i1)], z011 = z[at(mj, i3, i2 + 1, i1 + 1)];
+    const double z100 = z[at(mj, i3 + 1, i2, i1)], z101 = z[at(mj, i3 + 1, i2, i1 + 1)];
+    const double z110 = z[at(mj, i3 + 1, i2 + 1, i1)], z111 = z[at(mj, i3 + 1, i2 + 1, i1 + 1)];
+    // the reference's line buffers at i1 and i1 + 1
+    const double z1a = z010 + z000, z1b = z011 + z001;
+    const double z2a = z100 + z000, z2b = z101 + z001;
+    const double z3a = z110 + z100 + z1a, z3b = z111 + z101 + z1b;
+    const double add[4][2] = {{z000, 0.5 * (z001 + z000)},
+                              {0.5 * z1a, 0.25 * (z1a + z1b)},
+                              {0.5 * z2a, 0.25 * (z2a + z2b)},
+                              {0.25 * z3a, 0.125 * (z3a + z3b)}};
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int f3 = 2 * i3 + (q >> 1), f2 = 2 * i2 + (q & 1);
+        double2 *p = reinterpret_cast<double2 *>(u + at(mk, f3, f2, 2 * i1));
+        double2 w;
+        if (assign) {
+            w.x = 0.0 + add[q][0];
+            w.y = 0.0 + add[q][1];
+        } else {
+            const double2 o = *p;
+            w.x = o.x + add[q][0];
+            w.y = o.y + add[q][1];
+        }
+        *p = w;
+    }
+}
+
+// Sum of squares and largest magnitude over the interior: per-thread
+// sums over a fixed stride, per-block tree, the last block (ticket) adds
+// the blocks in order.  out[0] = sum, out[1] = max.
+__global__ void __launch_bounds__(kNormThreads) k_norm(const double *__restrict__ r, int m, double *part,
+                                                       unsigned *ticket, double *out)
+{
+    __shared__ double ss[kNormThreads], sm[kNormThreads];
+    __shared__ bool last;
+    const long long n = m - 2, total = n * n * n;
+    double s = 0.0, mx = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i1 = 1 + int(t % n), i2 = 1 + int((t / n) % n), i3 = 1 + int(t / (n * n));
+        const double x = r[at(m, i3, i2, i1)];
+        s = s + x * x;
+        mx = fmax(mx, fabs(x));
+    }
+    ss[threadIdx.x] = s;
+    sm[threadIdx.x] = mx;
+    __syncthreads();
+    for (int w = kNormThreads / 2; w > 0; w >>= 1) {
+        if (int(threadIdx.x) < w) {
+            ss[threadIdx.x] = ss[threadIdx.x] + ss[threadIdx.x + w];
+            sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + w]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = ss[0];
+        part[2 * blockIdx.x + 1] = sm[0];
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double a = 0.0, b = 0.0;
+        for (int i = 0; i < int(gridDim.x); i++) {
+            a = a + __ldcg(part + 2 * i);
+            b = fmax(b, __ldcg(part + 2 * i + 1));
+        }
+        out[0] = a;
+        out[1] = b;
+        *ticket = 0u;
+    }
+}
+
+__device__ __forceinline__ uint64_t lcg_mul(uint64_t a, uint64_t b) { return (a * b) & kMask46; }
+
+// kSeed * kMult^e mod 2^46 (the low 46 bits of the 64-bit products are exact)
+__device__ __forceinline__ uint64_t lcg_jump(uint64_t e)
+{
+    uint64_t r = kSeed, b = kMult;
+    while (e) {
+        if (e & 1) r = lcg_mul(r, b);
+        b = lcg_mul(b, b);
+        e >>= 1;
+    }
+    return r;
+}
+
+// zran3's candidates: draws above hi_t and below lo_t, with their linear
+// index L, appended to the lists (counts may pass the capacity: the host
+// then retries with tighter thresholds).
+__global__ void k_zran3_candidates(long long total, double hi_t, double lo_t, double *hv, long long *hl,
+                                   unsigned *hn, double *lv, long long *ll, unsigned *ln)
+{
+    const long long first = (blockIdx.x * (long long)blockDim.x + threadIdx.x) * kChunk;
+    if (first >= total) return;
+    const long long end = first + kChunk < total ? first + kChunk : total;
+    uint64_t x = lcg_jump(uint64_t(first) + 1);
+    for (long long L = first; L < end; L++) {
+        const double val = double(x) * 0x1p-46;  // exact
+        if (val > hi_t) {
+            const unsigned k = atomicAdd(hn, 1u);
+            if (k < unsigned(kCandCap)) {
+                hv[k] = val;
+                hl[k] = L;
+            }
+        }
+        if (val < lo_t) {
+            const unsigned k = atomicAdd(ln, 1u);
+            if (k < unsigned(kCandCap)) {
+                lv[k] = val;
+                ll[k] = L;
+            }
+        }
+        x = lcg_mul(x, kMult);
+    }
+}
+
+// v = -1 at the minus points, then +1 at the plus points, with ghosts
+// (v is zero beforehand).  pts: 10 minus then 10 plus (i1, i2, i3).
+__global__ void k_set_points(double *v, int m, const int *pts)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (int i = 0; i < 20; i++)
+        store_periodic(v, m, pts[3 * i + 2], pts[3 * i + 1], pts[3 * i], i < 10 ? -1.0 : 1.0);
+}
+
+}  // namespace mg
+}  // namespace cgb
+
+using namespace cgb;
+using namespace cgb::mg;
+
+struct cgb_mg {
+    int device = 0, lt = 0, smoother = 0;
+    int m[kMaxLevels + 1] = {};
+    double *u[kMaxLevels + 1] = {}, *r[kMaxLevels + 1] = {};
+    double *v = nullptr;
+    double *d_part = nullptr, *d_norm = nullptr;
+    unsigned *d_ticket = nullptr;
+    int plus[30] = {}, minus[30] = {};
+    Coef cf{};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int graph_nit = -1;
+};
+
+namespace {
+
+#define MG_TRY(call)                                                                      \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return set_error(e_ == cudaErrorMemoryAllocation ? CGB_ERR_NOMEM : CGB_ERR_CUDA, \
+                             "mg: %s: %s", #call, cudaGetErrorString(e_));                \
+    } while (0)
+
+size_t cells(int m) { return size_t(m) * m * m; }
+
+Coef coefficients(int smoother)
+{
+    // main's coefficients (mg.cu:422-442)
+    Coef cf{-8.0 / 3.0, 1.0 / 6.0, 1.0 / 12.0, -3.0 / 8.0, 1.0 / 32.0, -1.0 / 64.0};
+    if (smoother) {
+        cf.c0 = -3.0 / 17.0;
+        cf.c1 = 1.0 / 33.0;
+        cf.c2 = -1.0 / 61.0;
+    }
+    return cf;
+}
+
+void mg_release(cgb_mg *g)
+{
+    if (!g) return;
+    cudaSetDevice(g->device);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    for (int k = 0; k <= kMaxLevels; k++) {
+        if (g->u[k]) cudaFree(g->u[k]);
+        if (g->r[k]) cudaFree(g->r[k]);
+    }
+    for (void *p : {(void *)g->v, (void *)g->d_part, (void *)g->d_norm, (void *)g->d_ticket})
+        if (p) cudaFree(p);
+    if (g->ev0) cudaEventDestroy(g->ev0);
+    if (g->ev1) cudaEventDestroy(g->ev1);
+    if (g->stream) cudaStreamDestroy(g->stream);
+    delete g;
+}
+
+// x covers [1, m - 1] (the last interior point's right neighbour is a
+// column sum), y and z the interior.
+dim3 stencil_grid(int m)
+{
+    return dim3(unsigned((m - 1 + 31) / 32), unsigned((m - 2 + kRows - 1) / kRows), unsigned(m - 2));
+}
+
+dim3 interp_grid(int mj)
+{
+    return dim3(unsigned((mj - 1 + 31) / 32), unsigned((mj - 1 + kRows - 1) / kRows), unsigned(mj - 1));
+}
+
+void launch_resid(cgb_mg *g, int k, const double *u, const double *v, double *r)
+{
+    k_resid<<<stencil_grid(g->m[k]), dim3(32, kRows), 0, g->stream>>>(u, v, r, g->m[k], g->cf);
+}
+
+void launch_psinv(cgb_mg *g, int k, const double *r, double *u)
+{
+    k_psinv<<<stencil_grid(g->m[k]), dim3(32, kRows), 0, g->stream>>>(r, u, g->m[k], g->cf);
+}
+
+void launch_rprj3(cgb_mg *g, int k)  // level k -> k - 1
+{
+    const int mj = g->m[k - 1];
+    k_rprj3<<<stencil_grid(mj), dim3(32, kRows), 0, g->stream>>>(g->r[k], g->m[k], g->r[k - 1], mj);
+}
+
+void launch_interp(cgb_mg *g, int k, int assign)  // level k - 1 -> k
+{
+    const int mj = g->m[k - 1];
+    k_interp<<<interp_grid(mj), dim3(32, kRows), 0, g->stream>>>(g->u[k - 1], mj, g->u[k], g->m[k], assign);
+}
+
+void launch_norm(cgb_mg *g)
+{
+    k_norm<<<kNormBlocks, kNormThreads, 0, g->stream>>>(g->r[g->lt], g->m[g->lt], g->d_part, g->d_ticket,
+                                                        g->d_norm);
+}
+
+// One V-cycle (mg3P, :1078-1133) then the main loop's resid.
+void enqueue_iteration(cgb_mg *g)
+{
+    const int lt = g->lt;
+    for (int k = lt; k >= 2; k--) launch_rprj3(g, k);
+    cudaMemsetAsync(g->u[1], 0, sizeof(double) * cells(g->m[1]), g->stream);
+    launch_psinv(g, 1, g->r[1], g->u[1]);
+    for (int k = 2; k <= lt - 1; k++) {
+        launch_interp(g, k, 1);  // zero3 + interp
+        launch_resid(g, k, g->u[k], g->r[k], g->r[k]);
+        launch_psinv(g, k, g->r[k], g->u[k]);
+    }
+    launch_interp(g, lt, 0);
+    launch_resid(g, lt, g->u[lt], g->v, g->r[lt]);
+    launch_psinv(g, lt, g->r[lt], g->u[lt]);
+    launch_resid(g, lt, g->u[lt], g->v, g->r[lt]);
+}
+
+// zran3 on the device: the candidates, then the host's choice of the ten
+// largest and smallest, then v.
+int generate_v(cgb_mg *g)
+{
+    const int m = g->m[g->lt], n = m - 2;
+    const long long total = (long long)n * n * n;
+    double *hv = nullptr, *lv = nullptr;
+    long long *hl = nullptr, *ll = nullptr;
+    unsigned *cnt = nullptr;
+    int *pts = nullptr;
+    auto release = [&] {
+        for (void *p : {(void *)hv, (void *)lv, (void *)hl, (void *)ll, (void *)cnt, (void *)pts})
+            if (p) cudaFree(p);
+    };
+    if (cudaMalloc(&hv, sizeof(double) * kCandCap) != cudaSuccess ||
+        cudaMalloc(&lv, sizeof(double) * kCandCap) != cudaSuccess ||
+        cudaMalloc(&hl, sizeof(long long) * kCandCap) != cudaSuccess ||
+        cudaMalloc(&ll, sizeof(long long) * kCandCap) != cudaSuccess ||
+        cudaMalloc(&cnt, 2 * sizeof(unsigned)) != cudaSuccess || cudaMalloc(&pts, 60 * sizeof(int)) != cudaSuccess) {
+        release();
+        return set_error(CGB_ERR_NOMEM, "mg: zran3 buffers");
+    }
+    double expect = 256.0;
+    std::vector<std::pair<double, long long>> hi, lo;
+    int st = CGB_OK;
+    for (int attempt = 0; attempt < 12; attempt++) {
+        const double frac = std::min(0.5, expect / double(total));
+        const unsigned threads = 256;
+        const long long chunks = (total + kChunk - 1) / kChunk;
+        const unsigned blocks = unsigned((chunks + threads - 1) / threads);
+        unsigned h_cnt[2] = {0, 0};
+        if (cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), g->stream) != cudaSuccess) {
+            st = set_error(CGB_ERR_CUDA, "mg: zran3 memset");
+            break;
+        }
+        k_zran3_candidates<<<blocks, threads, 0, g->stream>>>(total, 1.0 - frac, frac, hv, hl, cnt, lv, ll,
+                                                              cnt + 1);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(h_cnt, cnt, sizeof(h_cnt), cudaMemcpyDeviceToHost, g->stream) != cudaSuccess ||
+            cudaStreamSynchronize(g->stream) != cudaSuccess) {
+            st = set_error(CGB_ERR_CUDA, "mg: zran3 candidates failed");
+            break;
+        }
+        if (h_cnt[0] > unsigned(kCandCap) || h_cnt[1] > unsigned(kCandCap)) {
+            expect /= 4.0;
+            continue;
+        }
+        if ((h_cnt[0] < 10 || h_cnt[1] < 10) && frac < 0.5) {
+            expect *= 8.0;
+            continue;
+        }
+        std::vector<double> a(h_cnt[0]), b(h_cnt[1]);
+        std::vector<long long> ai(h_cnt[0]), bi(h_cnt[1]);
+        if (cudaMemcpy(a.data(), hv, sizeof(double) * a.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(ai.data(), hl, sizeof(long long) * ai.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(b.data(), lv, sizeof(double) * b.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(bi.data(), ll, sizeof(long long) * bi.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+            st = set_error(CGB_ERR_CUDA, "mg: zran3 copy-out failed");
+            break;
+        }
+        for (size_t i = 0; i < a.size(); i++) hi.emplace_back(a[i], ai[i]);
+        for (size_t i = 0; i < b.size(); i++) lo.emplace_back(b[i], bi[i]);
+        break;
+    }
+    if (!st && (hi.size() < 10 || lo.size() < 10))
+        st = set_error(CGB_ERR_STATE, "mg: zran3 found fewer than ten candidates a side");
+    if (!st) {
+        // the reference's lists: the ten largest ascending (largest last),
+        // the ten smallest descending (smallest last)
+        std::sort(hi.begin(), hi.end());
+        std::sort(lo.begin(), lo.end(), [](const std::pair<double, long long> &x,
+                                           const std::pair<double, long long> &y) { return x.first > y.first; });
+        hi.erase(hi.begin(), hi.end() - 10);
+        lo.erase(lo.begin(), lo.end() - 10);
+        int h_pts[60];
+        auto put = [&](int *dst, long long L) {
+            dst[0] = 1 + int(L % n);
+            dst[1] = 1 + int((L / n) % n);
+            dst[2] = 1 + int(L / ((long long)n * n));
+        };
+        for (int i = 0; i < 10; i++) {
+            put(g->minus + 3 * i, lo[i].second);
+            put(g->plus + 3 * i, hi[i].second);
+            put(h_pts + 3 * i, lo[i].second);
+            put(h_pts + 30 + 3 * i, hi[i].second);
+        }
+        if (cudaMemsetAsync(g->v, 0, sizeof(double) * cells(m), g->stream) != cudaSuccess ||
+            cudaMemcpyAsync(pts, h_pts, sizeof(h_pts), cudaMemcpyHostToDevice, g->stream) != cudaSuccess)
+            st = set_error(CGB_ERR_CUDA, "mg: v upload failed");
+        if (!st) {
+            k_set_points<<<1, 32, 0, g->stream>>>(g->v, m, pts);
+            if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(g->stream) != cudaSuccess)
+                st = set_error(CGB_ERR_CUDA, "mg: v set-up failed");
+        }
+    }
+    release();
+    return st;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cgb_mg_create(int device, int lt, int smoother, cgb_mg **out)
+{
+    if (!out) return set_error(CGB_ERR_INVALID, "mg: null output");
+    *out = nullptr;
+    if (lt < 2 || lt > kMaxLevels - 1) return set_error(CGB_ERR_INVALID, "mg: lt must be in [2, %d]", kMaxLevels - 1);
+    if (smoother != 0 && smoother != 1) return set_error(CGB_ERR_INVALID, "mg: smoother must be 0 or 1");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count)
+        return set_error(CGB_ERR_NO_DEVICE, "mg: no CUDA device %d", device);
+    int major = 0;
+    MG_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+    if (major != 10) return set_error(CGB_ERR_NO_DEVICE, "mg: device %d is not sm_100", device);
+    MG_TRY(cudaSetDevice(device));
+    cgb_mg *g = new (std::nothrow) cgb_mg;
+    if (!g) return set_error(CGB_ERR_NOMEM, "mg: allocation failed");
+    g->device = device;
+    g->lt = lt;
+    g->smoother = smoother;
+    g->cf = coefficients(smoother);
+    bool ok = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreate(&g->ev0) == cudaSuccess && cudaEventCreate(&g->ev1) == cudaSuccess &&
+              cudaMalloc(&g->d_part, sizeof(double) * 2 * kNormBlocks) == cudaSuccess &&
+              cudaMalloc(&g->d_norm, sizeof(double) * 2) == cudaSuccess &&
+              cudaMalloc(&g->d_ticket, sizeof(unsigned)) == cudaSuccess &&
+              cudaMemset(g->d_ticket, 0, sizeof(unsigned)) == cudaSuccess;
+    for (int k = 1; k <= lt && ok; k++) {
+        g->m[k] = (1 << k) + 2;
+        ok = cudaMalloc(&g->u[k], sizeof(double) * cells(g->m[k])) == cudaSuccess &&
+             cudaMalloc(&g->r[k], sizeof(double) * cells(g->m[k])) == cudaSuccess &&
+             cudaMemset(g->u[k], 0, sizeof(double) * cells(g->m[k])) == cudaSuccess &&
+             cudaMemset(g->r[k], 0, sizeof(double) * cells(g->m[k])) == cudaSuccess;
+    }
+    ok = ok && cudaMalloc(&g->v, sizeof(double) * cells(g->m[lt])) == cudaSuccess;
+    if (!ok) {
+        mg_release(g);
+        return set_error(CGB_ERR_NOMEM, "mg: device allocation failed (2^%d grid)", lt);
+    }
+    const int st = generate_v(g);
+    if (st) {
+        mg_release(g);
+        return st;
+    }
+    *out = g;
+    return CGB_OK;
+}
+
+int cgb_mg_destroy(cgb_mg *g)
+{
+    mg_release(g);
+    return CGB_OK;
+}
+
+int cgb_mg_run(cgb_mg *g, int nit, double *rnm2, double *rnmu, double *device_ms)
+{
+    if (!g || nit < 0) return set_error(CGB_ERR_INVALID, "mg: null grid or negative nit");
+    MG_TRY(cudaSetDevice(g->device));
+    const int lt = g->lt, m = g->m[lt];
+    if (g->graph_nit != nit) {
+        if (g->exec) cudaGraphExecDestroy(g->exec);
+        g->exec = nullptr;
+        g->graph_nit = -1;
+        // the timed region of main (:498-508): resid, norm, nit x (V-cycle,
+        // resid), norm -- one graph
+        cudaGraph_t graph = nullptr;
+        MG_TRY(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+        launch_resid(g, lt, g->u[lt], g->v, g->r[lt]);
+        launch_norm(g);
+        for (int it = 0; it < nit; it++) enqueue_iteration(g);
+        launch_norm(g);
+        const cudaError_t e1 = cudaGetLastError();
+        const cudaError_t e2 = cudaStreamEndCapture(g->stream, &graph);
+        if (e1 != cudaSuccess || e2 != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            return set_error(CGB_ERR_CUDA, "mg: capture failed: %s",
+                             cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+        }
+        const cudaError_t e3 = cudaGraphInstantiate(&g->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e3 != cudaSuccess) {
+            g->exec = nullptr;
+            return set_error(CGB_ERR_CUDA, "mg: graph instantiation: %s", cudaGetErrorString(e3));
+        }
+        g->graph_nit = nit;
+    }
+    // u = 0 on the finest level (main's zero3 before the timed region)
+    MG_TRY(cudaMemsetAsync(g->u[lt], 0, sizeof(double) * cells(m), g->stream));
+    MG_TRY(cudaEventRecord(g->ev0, g->stream));
+    MG_TRY(cudaGraphLaunch(g->exec, g->stream));
+    MG_TRY(cudaEventRecord(g->ev1, g->stream));
+    double h[2] = {0.0, 0.0};
+    MG_TRY(cudaMemcpyAsync(h, g->d_norm, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    MG_TRY(cudaStreamSynchronize(g->stream));
+    float ms = 0.f;
+    MG_TRY(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+    const double n = double(m - 2);
+    if (rnm2) *rnm2 = std::sqrt(h[0] / (n * n * n));
+    if (rnmu) *rnmu = h[1];
+    if (device_ms) *device_ms = ms;
+    if (!std::isfinite(h[0])) return set_error(CGB_ERR_NUMERIC, "mg: non-finite residual norm");
+    return CGB_OK;
+}
+
+int cgb_mg_read(cgb_mg *g, int which, double *out, long long count)
+{
+    if (!g || !out || which < 0 || which > 2) return set_error(CGB_ERR_INVALID, "mg: bad read");
+    const size_t need = cells(g->m[g->lt]);
+    if (count < (long long)need) return set_error(CGB_ERR_CAPACITY, "mg: %zu doubles needed", need);
+    MG_TRY(cudaSetDevice(g->device));
+    const double *src = which == 0 ? g->u[g->lt] : which == 1 ? g->v : g->r[g->lt];
+    MG_TRY(cudaMemcpy(out, src, sizeof(double) * need, cudaMemcpyDeviceToHost));
+    return CGB_OK;
+}
+
+int cgb_mg_points(cgb_mg *g, int *plus, int *minus)
+{
+    if (!g) return set_error(CGB_ERR_INVALID, "mg: null grid");
+    if (plus) std::memcpy(plus, g->plus, sizeof(g->plus));
+    if (minus) std::memcpy(minus, g->minus, sizeof(g->minus));
+    return CGB_OK;
+}
+
+int cgb_mg_apply(int device, int op, int m, int smoother, const double *in1, const double *in2,
+                 double *out)
+{
+    if (op < 0 || op > 4 || m < 4 || m > (op >= 3 ? 514 : 1026) || (m & 1) || !in1 || !out ||
+        (op == 0 && !in2))
+        return set_error(CGB_ERR_INVALID, "mg: bad operator call");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count)
+        return set_error(CGB_ERR_NO_DEVICE, "mg: no CUDA device %d", device);
+    MG_TRY(cudaSetDevice(device));
+    const int mo = op == 2 ? m / 2 + 1 : op >= 3 ? 2 * m - 2 : m;
+    const size_t ci = cells(m), co = cells(mo);
+    double *a = nullptr, *b = nullptr, *c = nullptr;
+    const Coef cf = coefficients(smoother);
+    int st = CGB_OK;
+    if (cudaMalloc(&a, sizeof(double) * ci) != cudaSuccess || cudaMalloc(&b, sizeof(double) * ci) != cudaSuccess ||
+        cudaMalloc(&c, sizeof(double) * co) != cudaSuccess)
+        st = set_error(CGB_ERR_NOMEM, "mg: operator buffers");
+    if (!st && (cudaMemcpy(a, in1, sizeof(double) * ci, cudaMemcpyHostToDevice) != cudaSuccess ||
+                (in2 && cudaMemcpy(b, in2, sizeof(double) * ci, cudaMemcpyHostToDevice) != cudaSuccess) ||
+                cudaMemcpy(c, out, sizeof(double) * co, cudaMemcpyHostToDevice) != cudaSuccess))
+        st = set_error(CGB_ERR_CUDA, "mg: operator upload");
+    if (!st) {
+        switch (op) {
+        case 0: k_resid<<<stencil_grid(m), dim3(32, kRows)>>>(a, b, c, m, cf); break;
+        case 1: k_psinv<<<stencil_grid(m), dim3(32, kRows)>>>(a, c, m, cf); break;
+        case 2: k_rprj3<<<stencil_grid(mo), dim3(32, kRows)>>>(a, m, c, mo); break;
+        default: k_interp<<<interp_grid(m), dim3(32, kRows)>>>(a, m, c, mo, op == 4); break;
+        }
+        if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
+            cudaMemcpy(out, c, sizeof(double) * co, cudaMemcpyDeviceToHost) != cudaSuccess)
+            st = set_error(CGB_ERR_CUDA, "mg: operator failed");
+    }
+    for (double *p : {a, b, c})
+        if (p) cudaFree(p);
+    return st;
+}
+
+}  // extern "C"

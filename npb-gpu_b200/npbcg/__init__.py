@@ -200,6 +200,15 @@ _SIGNATURES = {
                                                     ctypes.c_double, ctypes.c_int,
                                                     ctypes.c_void_p, ctypes.c_void_p,
                                                     ctypes.POINTER(ctypes.c_double)]),
+    "cgb_mg_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_void_p)]),
+    "cgb_mg_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "cgb_mg_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                  ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "cgb_mg_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _F64, ctypes.c_longlong]),
+    "cgb_mg_points": (ctypes.c_int, [ctypes.c_void_p, _I32, _I32]),
+    "cgb_mg_apply": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_void_p, ctypes.c_void_p, _F64]),
     "cgb_host_alloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_longlong]),
     "cgb_host_free": (ctypes.c_int, [ctypes.c_void_p]),
     "cgb_device_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
@@ -886,3 +895,80 @@ def group_power_iterate(parts, niter, shift, cgitmax=25):
     _check(lib().cgb_part_group_power_iterate(ctypes.cast(hs, ctypes.c_void_p), len(parts), niter,
                                               shift, cgitmax, _ptr(z), _ptr(r), ctypes.byref(ms)))
     return dict(zeta=z, rnorm=r, device_ms=ms.value)
+
+
+# NPB MG classes (the reference's mg.cu main :388-410, verification norms
+# :528-543): lt (grid 2^lt a side), nit, smoother set, rnm2
+MG_CLASSES = {
+    "S": dict(lt=5, nit=4, smoother=0, rnm2=0.5307707005734e-04),
+    "W": dict(lt=7, nit=4, smoother=0, rnm2=0.6467329375339e-05),
+    "A": dict(lt=8, nit=4, smoother=0, rnm2=0.2433365309069e-05),
+    "B": dict(lt=8, nit=20, smoother=1, rnm2=0.1800564401355e-05),
+    "C": dict(lt=9, nit=20, smoother=1, rnm2=0.5706732285740e-06),
+    "D": dict(lt=10, nit=50, smoother=1, rnm2=0.1583275060440e-09),
+}
+MG_VERIFY_EPSILON = 1.0e-8
+
+
+class Mg:
+    """The NPB MG benchmark's grids on one GPU (cgb_mg): v generated on the
+    device, u and r for every level of the V-cycle."""
+
+    def __init__(self, lt, smoother, device=0):
+        self.lt, self.smoother = int(lt), int(smoother)
+        self.m = (1 << self.lt) + 2
+        h = ctypes.c_void_p()
+        _check(lib().cgb_mg_create(device, self.lt, self.smoother, ctypes.byref(h)))
+        self._h = h
+
+    @classmethod
+    def for_class(cls, name, device=0):
+        c = MG_CLASSES[name]
+        return cls(c["lt"], c["smoother"], device)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cgb_mg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def run(self, nit):
+        """The reference's timed region from u = 0: {rnm2, rnmu, device_ms}."""
+        a, b, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(lib().cgb_mg_run(self._h, int(nit), ctypes.byref(a), ctypes.byref(b), ctypes.byref(t)))
+        return dict(rnm2=a.value, rnmu=b.value, device_ms=t.value)
+
+    def grid(self, which):
+        """The finest level's 'u', 'v' or 'r' as a flat float64 array."""
+        out = np.zeros(self.m ** 3)
+        _check(lib().cgb_mg_read(self._h, {"u": 0, "v": 1, "r": 2}[which], out, out.size))
+        return out
+
+    def points(self):
+        """zran3's (i1, i2, i3) of the +1 and -1 points, the reference's list order."""
+        plus, minus = np.zeros(30, np.int32), np.zeros(30, np.int32)
+        _check(lib().cgb_mg_points(self._h, plus, minus))
+        return plus.reshape(10, 3), minus.reshape(10, 3)
+
+
+def mg_apply(op, m, in1, in2=None, out=None, smoother=0, device=0):
+    """One MG operator on host grids (0 resid, 1 psinv, 2 rprj3, 3 interp
+    adding, 4 interp assigning); returns the output grid."""
+    mo = m // 2 + 1 if op == 2 else 2 * m - 2 if op >= 3 else m
+    res = np.zeros(mo ** 3) if out is None else np.array(out, dtype=np.float64)
+    a = np.ascontiguousarray(in1, np.float64)
+    b = None if in2 is None else np.ascontiguousarray(in2, np.float64)
+    _check(lib().cgb_mg_apply(device, op, m, smoother, a.ctypes.data_as(ctypes.c_void_p),
+                              None if b is None else b.ctypes.data_as(ctypes.c_void_p), res))
+    return res
