@@ -6,12 +6,15 @@
     python npb-gpu_b200/npbcg/profile_case.py --what batch --nsys 64 --niter 2
     python npb-gpu_b200/npbcg/profile_case.py --cls B --what barrier --reps 20000
     python npb-gpu_b200/npbcg/profile_case.py --cls D --what part --ranks 1 --niter 1
+    python npb-gpu_b200/npbcg/profile_case.py --what mg --mg-class A --niter 4
 
 `spmv` launches the standalone FP64 SpMV+dot kernel `reps` times (after one
 warm-up launch); `solve` runs one power iteration of `niter` outer steps;
 `sweep` prints SpMV timings for every lanes-per-row choice; `part` runs the
 row-partitioned solver on `ranks` device-generated row blocks, all driven
-from this process.  Each prints one JSON line.
+from this process; `mg` runs the MG benchmark's timed region (niter
+V-cycles) of an MG class once after one warm-up run.  Each prints one JSON
+line.
 """
 import argparse
 import json
@@ -26,7 +29,9 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cls", default="B", choices=sorted(npbcg.CLASSES))
     ap.add_argument("--what", default="spmv",
-                    choices=["spmv", "solve", "sweep", "batch", "barrier", "part"])
+                    choices=["spmv", "solve", "sweep", "batch", "barrier", "part", "mg"])
+    ap.add_argument("--mg-class", default="A", choices=sorted(npbcg.MG_CLASSES),
+                    help="mg: the MG class")
     ap.add_argument("--ranks", type=int, default=1, help="part: row blocks")
     ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed", "learned"],
                     help="solve / batch: the solver mode (mixed: tol 1e-12, cgitmax 100)")
@@ -56,6 +61,12 @@ def main():
             r = b.solve(niter=a.niter, **kw)
             print(json.dumps({"what": "batch", "nsys": a.nsys, "niter": a.niter, "mode": a.mode,
                               "device_ms": r["device_ms"], "policy": b.policy()}), flush=True)
+        return
+    if a.what == "mg":
+        with npbcg.Mg.for_class(a.mg_class) as g:
+            g.run(a.niter)
+            r = g.run(a.niter)
+        print(json.dumps({"what": "mg", "class": a.mg_class, "niter": a.niter, **r}), flush=True)
         return
     c = npbcg.CLASSES[a.cls]
     if a.what == "part":

@@ -214,3 +214,41 @@ class RefLib:
         self.lib.ref_conj_grad(np.ascontiguousarray(x, np.float64).ctypes.data, z.ctypes.data,
                                r.ctypes.data, p.ctypes.data, q.ctypes.data, rn.ctypes.data)
         return z, p, q, r, float(rn[0])
+
+
+class RefMgLib:
+    """The reference's own MG code for one NPB class (oracle/_ref/libref_mg_<class>.so)."""
+
+    def __init__(self, path):
+        lib = ctypes.CDLL(path)
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        lib.ref_mg_info.restype = None
+        lib.ref_mg_info.argtypes = [ip, ip]
+        lib.ref_mg_cpu.restype = ctypes.c_int
+        lib.ref_mg_cpu.argtypes = [dp, dp, dp, ctypes.c_void_p, ctypes.c_void_p]
+        lib.ref_mg_gpu.restype = ctypes.c_int
+        lib.ref_mg_gpu.argtypes = [dp, dp, dp]
+        self.lib = lib
+        lt, nit = ctypes.c_int(), ctypes.c_int()
+        lib.ref_mg_info(ctypes.byref(lt), ctypes.byref(nit))
+        self.lt, self.nit = lt.value, nit.value
+        self.m = (1 << self.lt) + 2
+
+    def cpu(self, grids=False):
+        a, b, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        u = np.zeros(self.m ** 3) if grids else None
+        r = np.zeros(self.m ** 3) if grids else None
+        self.lib.ref_mg_cpu(ctypes.byref(a), ctypes.byref(b), ctypes.byref(t),
+                            None if u is None else u.ctypes.data, None if r is None else r.ctypes.data)
+        out = dict(rnm2=a.value, rnmu=b.value, seconds=t.value)
+        if grids:
+            out.update(u=u, r=r)
+        return out
+
+    def gpu(self):
+        a, b, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        rc = self.lib.ref_mg_gpu(ctypes.byref(a), ctypes.byref(b), ctypes.byref(t))
+        if rc != 0:
+            raise RuntimeError("ref_mg_gpu failed")
+        return dict(rnm2=a.value, rnmu=b.value, seconds=t.value)

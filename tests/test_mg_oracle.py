@@ -6,8 +6,10 @@ relative 1e-8 of it.  The oracle, a plain-C restatement of the reference's
 serial operators in its own order of operations, must reproduce those norms
 far closer than that: the norms are printed to 13 significant digits, so
 the bar here is 1e-12.  Classes S, W, A (and B, marked slow) run on the CPU
-in seconds.  Also: zran3's twenty points (distinct, inside the grid, the
-largest / smallest draws) and the periodic ghost layer.
+in seconds.  The oracle also equals the reference's own serial operators,
+compiled from its sources into oracle/_ref, bit for bit (u, r, norms).
+Also: zran3's twenty points (distinct, inside the grid, the largest /
+smallest draws) and the periodic ghost layer.
 """
 import numpy as np
 import pytest
@@ -63,3 +65,23 @@ def test_ghost_layer_is_periodic(oracle):
     assert np.array_equal(r[0], r[m - 2]) and np.array_equal(r[m - 1], r[1])
     assert np.array_equal(r[:, 0], r[:, m - 2]) and np.array_equal(r[:, m - 1], r[:, 1])
     assert np.array_equal(r[:, :, 0], r[:, :, m - 2]) and np.array_equal(r[:, :, m - 1], r[:, :, 1])
+
+
+@pytest.mark.parametrize("cls", ["S", "W", "A"])
+def test_oracle_equals_reference_cpu_code(oracle, cls):
+    """The reference's own serial MG operators, compiled from its sources
+    (oracle/_ref/libref_mg_<class>.so, built by oracle/Makefile), against the
+    oracle: u, r and the norms bit for bit."""
+    import os
+    from conftest import REF_DIR
+    from oracle_py import RefMgLib
+    path = os.path.join(REF_DIR, f"libref_mg_{cls}.so")
+    if not os.path.exists(path):
+        pytest.skip("the reference's MG library was not built (make -C oracle)")
+    ref = RefMgLib(path)
+    lt, nit, smoother, _ = MG_CLASSES[cls]
+    assert (ref.lt, ref.nit) == (lt, nit)
+    want = ref.cpu(grids=True)
+    got = oracle.mg_run(lt, nit, smoother, grids=True)
+    assert got["rnm2"] == want["rnm2"] and got["rnmu"] == want["rnmu"]
+    assert np.array_equal(got["u"], want["u"]) and np.array_equal(got["r"], want["r"])
