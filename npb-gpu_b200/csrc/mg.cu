@@ -10,10 +10,12 @@
 //   rprj3   s = P^T r         (:1724-1790)  full weighting onto the coarse grid
 //   interp  u (+)= P z        (:836-890)    trilinear prolongation
 //   norm2u3                   (:1201-1230)  deterministic two-level reduction
-// A warp covers 32 consecutive x of one (y, z) row: each lane forms the
-// row sums of its own column (the reference's u1/u2 line buffers) and takes
-// its neighbours' from the adjacent lanes by shuffles, so a point costs 10
-// loads instead of 27, all coalesced.  The periodic ghost exchange (comm3,
+// The 27-point operators stage their input in shared memory, plane by plane
+// along z (a ring of three planes of a 32 x 8 tile with its halo, the next
+// plane loading while the current one is computed); a warp covers 32
+// consecutive x of one row, each lane forms the column sums of its own x
+// (the reference's u1/u2 line buffers) and takes its neighbours' from the
+// adjacent lanes by shuffles.  The periodic ghost exchange (comm3,
 // :687-716, which only copies interior values) is fused: the thread that
 // writes an interior point also writes that value into each ghost cell that
 // mirrors it.  On coarse levels the reference zeroes u and then adds the
@@ -47,7 +49,7 @@ namespace mg {
 
 constexpr int kMaxLevels = 11;   // lt <= 10: a 1024^3 grid (class D)
 constexpr int kRows = 8;         // (y) rows of a stencil CTA; x is a warp
-constexpr int kNormBlocks = 592;
+constexpr int kNormBlocks = 1184;
 constexpr int kNormThreads = 256;
 constexpr int kCandCap = 8192;   // zran3 candidates kept per side
 constexpr int kChunk = 64;       // zran3 draws a thread steps through
@@ -86,70 +88,90 @@ __device__ __forceinline__ void store_periodic(double *g, int m, int i3, int i2,
             for (int a = 0; a < nx; a++) g[at(m, z[c], y[b], x[a])] = val;
 }
 
-// Row sums of column i1 around (i2, i3): the four edge neighbours (s1,
-// the reference's u1) and the four corners (s2, its u2), in its order.
-__device__ __forceinline__ void column_sums(const double *__restrict__ g, int m, int i3, int i2,
-                                            int i1, double &s1, double &s2)
-{
-    s1 = g[at(m, i3, i2 - 1, i1)] + g[at(m, i3, i2 + 1, i1)] + g[at(m, i3 - 1, i2, i1)] +
-         g[at(m, i3 + 1, i2, i1)];
-    s2 = g[at(m, i3 - 1, i2 - 1, i1)] + g[at(m, i3 - 1, i2 + 1, i1)] + g[at(m, i3 + 1, i2 - 1, i1)] +
-         g[at(m, i3 + 1, i2 + 1, i1)];
-}
+// The 27-point operators with the input grid staged in shared memory: a
+// CTA owns a 32 x kRows tile of (x, y) and walks kPlanes z planes, keeping
+// planes z-1, z, z+1 of the tile plus a one-cell halo in a ring of three
+// (34 x (kRows + 2) doubles each), so each input value is read from L2/HBM
+// about once instead of by nine threads.  The next plane's loads are issued
+// before the current plane's arithmetic and land in registers, so their
+// latency hides behind it.  kPsinv: u = u + C g (g = r); otherwise
+// out = w - A g (g = u, w = v; out may be w).
+constexpr int kPlanes = 32;
+constexpr int kTileW = 34, kTileH = kRows + 2, kTile = kTileW * kTileH;
+constexpr int kThreads = 32 * kRows;
+static_assert(kTile <= 2 * kThreads, "a thread stages at most two tile cells");
 
-// The column sums of x - 1, x, x + 1 for this lane (x = i1): its own, and
-// its neighbours' from the adjacent lanes, computed directly at the warp's
-// two ends.  Lanes past the row (i1 > m - 1) load nothing.
-struct Stencil {
-    double s1m, s1, s1p, s2m, s2, s2p;
-};
-
-__device__ __forceinline__ Stencil stencil_row(const double *__restrict__ g, int m, int i3, int i2,
-                                               int i1)
+template <bool kPsinv>
+__global__ void __launch_bounds__(kThreads) k_stencil(const double *__restrict__ g, const double *w,
+                                                      double *out, int m, Coef cf)
 {
-    const int lane = threadIdx.x & 31;
-    Stencil st;
-    st.s1 = st.s2 = 0.0;
-    if (i1 <= m - 1) column_sums(g, m, i3, i2, i1, st.s1, st.s2);
-    st.s1m = __shfl_up_sync(0xffffffffu, st.s1, 1);
-    st.s2m = __shfl_up_sync(0xffffffffu, st.s2, 1);
-    st.s1p = __shfl_down_sync(0xffffffffu, st.s1, 1);
-    st.s2p = __shfl_down_sync(0xffffffffu, st.s2, 1);
-    if (lane == 0 && i1 <= m - 2) column_sums(g, m, i3, i2, i1 - 1, st.s1m, st.s2m);
-    if (lane == 31 && i1 <= m - 2) column_sums(g, m, i3, i2, i1 + 1, st.s1p, st.s2p);
-    return st;
-}
-
-// r = v - A u on the interior (r may be v).  Block (32, kRows): x =
-// 1 + 32 bx + tx, y = 1 + kRows by + ty, z = 1 + bz.
-__global__ void __launch_bounds__(32 * kRows) k_resid(const double *__restrict__ u, const double *v,
-                                                      double *r, int m, Coef cf)
-{
-    const int i1 = 1 + int(blockIdx.x) * 32 + int(threadIdx.x);
-    const int i2 = 1 + int(blockIdx.y) * kRows + int(threadIdx.y);
-    const int i3 = 1 + int(blockIdx.z);
-    if (i2 > m - 2) return;  // whole warps: a warp is one row
-    const Stencil s = stencil_row(u, m, i3, i2, i1);
-    if (i1 > m - 2) return;
-    const size_t c = at(m, i3, i2, i1);
-    const double val = v[c] - cf.a0 * u[c] - cf.a2 * (s.s2 + s.s1m + s.s1p) - cf.a3 * (s.s2m + s.s2p);
-    store_periodic(r, m, i3, i2, i1, val);
-}
-
-// u = u + C r on the interior (in place: each point reads only its own u).
-__global__ void __launch_bounds__(32 * kRows) k_psinv(const double *__restrict__ r, double *u, int m,
-                                                      Coef cf)
-{
-    const int i1 = 1 + int(blockIdx.x) * 32 + int(threadIdx.x);
-    const int i2 = 1 + int(blockIdx.y) * kRows + int(threadIdx.y);
-    const int i3 = 1 + int(blockIdx.z);
-    if (i2 > m - 2) return;
-    const Stencil s = stencil_row(r, m, i3, i2, i1);
-    if (i1 > m - 2) return;
-    const size_t c = at(m, i3, i2, i1);
-    const double val = u[c] + cf.c0 * r[c] + cf.c1 * (r[c - 1] + r[c + 1] + s.s1) +
-                       cf.c2 * (s.s2 + s.s1m + s.s1p);
-    store_periodic(u, m, i3, i2, i1, val);
+    __shared__ double ring[3][kTile];
+    const int n = m - 2;
+    const int tx = threadIdx.x, ty = threadIdx.y, t = ty * 32 + tx;
+    const int x0 = 1 + int(blockIdx.x) * 32, y0 = 1 + int(blockIdx.y) * kRows;
+    const int z0 = 1 + int(blockIdx.z) * kPlanes, z1 = min(n, z0 + kPlanes - 1);
+    const int x = x0 + tx, y = y0 + ty;
+    const size_t plane = size_t(m) * m;
+    // the (up to two) tile cells this thread stages, as offsets in a plane
+    const int e1 = t + kThreads;
+    const int gx0 = x0 - 1 + t % kTileW, gy0 = y0 - 1 + t / kTileW;
+    const int gx1 = x0 - 1 + e1 % kTileW, gy1 = y0 - 1 + e1 / kTileW;
+    const bool in0 = gx0 <= m - 1 && gy0 <= m - 1;
+    const bool in1 = e1 < kTile && gx1 <= m - 1 && gy1 <= m - 1;
+    const size_t o0 = size_t(gy0) * m + gx0, o1 = size_t(gy1) * m + gx1;
+    auto fetch = [&](int z, double &a, double &b) {
+        a = in0 ? g[z * plane + o0] : 0.0;
+        b = in1 ? g[z * plane + o1] : 0.0;
+    };
+    auto put = [&](int z, double a, double b) {
+        ring[z % 3][t] = a;
+        if (e1 < kTile) ring[z % 3][e1] = b;
+    };
+    {
+        double a, b, c, d, e, f;
+        fetch(z0 - 1, a, b);
+        fetch(z0, c, d);
+        fetch(z0 + 1, e, f);
+        put(z0 - 1, a, b);
+        put(z0, c, d);
+        put(z0 + 1, e, f);
+    }
+    __syncthreads();
+    const int lx = tx + 1, ly = ty + 1;
+    const bool store = x <= n && y <= n;
+    for (int z = z0; z <= z1; z++) {
+        double na = 0.0, nb = 0.0;
+        if (z + 1 <= z1) fetch(z + 2, na, nb);  // in flight during this plane
+        const size_t c = at(m, z, y, x);
+        const double wc = store ? (kPsinv ? out[c] : w[c]) : 0.0;
+        const double *Pm = ring[(z - 1) % 3], *P0 = ring[z % 3], *Pp = ring[(z + 1) % 3];
+        // column sums (the reference's u1 / u2) of column k of this row
+        auto sums = [&](int k, double &s1, double &s2) {
+            s1 = P0[(ly - 1) * kTileW + k] + P0[(ly + 1) * kTileW + k] + Pm[ly * kTileW + k] +
+                 Pp[ly * kTileW + k];
+            s2 = Pm[(ly - 1) * kTileW + k] + Pm[(ly + 1) * kTileW + k] + Pp[(ly - 1) * kTileW + k] +
+                 Pp[(ly + 1) * kTileW + k];
+        };
+        double s1, s2;
+        sums(lx, s1, s2);
+        double s1m = __shfl_up_sync(0xffffffffu, s1, 1), s2m = __shfl_up_sync(0xffffffffu, s2, 1);
+        double s1p = __shfl_down_sync(0xffffffffu, s1, 1), s2p = __shfl_down_sync(0xffffffffu, s2, 1);
+        if (tx == 0) sums(lx - 1, s1m, s2m);
+        if (tx == 31) sums(lx + 1, s1p, s2p);
+        if (store) {
+            const double gc = P0[ly * kTileW + lx];
+            double val;
+            if constexpr (kPsinv)
+                val = wc + cf.c0 * gc + cf.c1 * (P0[ly * kTileW + lx - 1] + P0[ly * kTileW + lx + 1] + s1) +
+                      cf.c2 * (s2 + s1m + s1p);
+            else
+                val = wc - cf.a0 * gc - cf.a2 * (s2 + s1m + s1p) - cf.a3 * (s2m + s2p);
+            store_periodic(out, m, z, y, x, val);
+        }
+        __syncthreads();  // every read of plane z-1's slot is done
+        if (z + 1 <= z1) put(z + 2, na, nb);
+        __syncthreads();
+    }
 }
 
 // s (side mj) = restriction of r (side mk = 2 mj - 2).  A thread per coarse
@@ -225,22 +247,41 @@ __global__ void __launch_bounds__(32 * kRows) k_interp(const double *__restrict_
     }
 }
 
-// Sum of squares and largest magnitude over the interior: per-thread
-// sums over a fixed stride, per-block tree, the last block (ticket) adds
-// the blocks in order.  out[0] = sum, out[1] = max.
+// Sum of squares and largest magnitude over the interior: block b takes
+// rows (i2, i3) b, b + grid, ... and its threads stride x; a thread loads
+// kBatch of its values ahead, then adds them in its fixed order.  Per-block
+// tree, then the last block (ticket) adds the blocks in order.
+// out[0] = sum, out[1] = max.
+constexpr int kBatch = 8;
+
 __global__ void __launch_bounds__(kNormThreads) k_norm(const double *__restrict__ r, int m, double *part,
                                                        unsigned *ticket, double *out)
 {
     __shared__ double ss[kNormThreads], sm[kNormThreads];
     __shared__ bool last;
-    const long long n = m - 2, total = n * n * n;
+    const int n = m - 2;
+    const int per_row = (n + kNormThreads - 1) / kNormThreads;  // x slots a thread has per row
+    const long long rows = (long long)n * n;
+    const long long mine = rows > blockIdx.x ? (rows - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    const long long items = mine * per_row;
     double s = 0.0, mx = 0.0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int i1 = 1 + int(t % n), i2 = 1 + int((t / n) % n), i3 = 1 + int(t / (n * n));
-        const double x = r[at(m, i3, i2, i1)];
-        s = s + x * x;
-        mx = fmax(mx, fabs(x));
+    for (long long q0 = 0; q0 < items; q0 += kBatch) {
+        double xv[kBatch];
+#pragma unroll
+        for (int b = 0; b < kBatch; b++) {
+            const long long q = q0 + b;
+            xv[b] = 0.0;
+            if (q < items) {
+                const long long row = blockIdx.x + (q / per_row) * gridDim.x;
+                const int i1 = 1 + int(threadIdx.x) + int(q % per_row) * kNormThreads;
+                if (i1 <= n) xv[b] = r[at(m, 1 + int(row / n), 1 + int(row % n), i1)];
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < kBatch; b++) {
+            s = s + xv[b] * xv[b];
+            mx = fmax(mx, fabs(xv[b]));
+        }
     }
     ss[threadIdx.x] = s;
     sm[threadIdx.x] = mx;
@@ -394,6 +435,12 @@ dim3 stencil_grid(int m)
     return dim3(unsigned((m - 1 + 31) / 32), unsigned((m - 2 + kRows - 1) / kRows), unsigned(m - 2));
 }
 
+dim3 stencil25_grid(int m)
+{
+    const int n = m - 2;
+    return dim3(unsigned((n + 31) / 32), unsigned((n + kRows - 1) / kRows), unsigned((n + kPlanes - 1) / kPlanes));
+}
+
 dim3 interp_grid(int mj)
 {
     return dim3(unsigned((mj - 1 + 31) / 32), unsigned((mj - 1 + kRows - 1) / kRows), unsigned(mj - 1));
@@ -401,12 +448,12 @@ dim3 interp_grid(int mj)
 
 void launch_resid(cgb_mg *g, int k, const double *u, const double *v, double *r)
 {
-    k_resid<<<stencil_grid(g->m[k]), dim3(32, kRows), 0, g->stream>>>(u, v, r, g->m[k], g->cf);
+    k_stencil<false><<<stencil25_grid(g->m[k]), dim3(32, kRows), 0, g->stream>>>(u, v, r, g->m[k], g->cf);
 }
 
 void launch_psinv(cgb_mg *g, int k, const double *r, double *u)
 {
-    k_psinv<<<stencil_grid(g->m[k]), dim3(32, kRows), 0, g->stream>>>(r, u, g->m[k], g->cf);
+    k_stencil<true><<<stencil25_grid(g->m[k]), dim3(32, kRows), 0, g->stream>>>(r, nullptr, u, g->m[k], g->cf);
 }
 
 void launch_rprj3(cgb_mg *g, int k)  // level k -> k - 1
@@ -693,8 +740,8 @@ int cgb_mg_apply(int device, int op, int m, int smoother, const double *in1, con
         st = set_error(CGB_ERR_CUDA, "mg: operator upload");
     if (!st) {
         switch (op) {
-        case 0: k_resid<<<stencil_grid(m), dim3(32, kRows)>>>(a, b, c, m, cf); break;
-        case 1: k_psinv<<<stencil_grid(m), dim3(32, kRows)>>>(a, c, m, cf); break;
+        case 0: k_stencil<false><<<stencil25_grid(m), dim3(32, kRows)>>>(a, b, c, m, cf); break;
+        case 1: k_stencil<true><<<stencil25_grid(m), dim3(32, kRows)>>>(a, nullptr, c, m, cf); break;
         case 2: k_rprj3<<<stencil_grid(mo), dim3(32, kRows)>>>(a, m, c, mo); break;
         default: k_interp<<<interp_grid(m), dim3(32, kRows)>>>(a, m, c, mo, op == 4); break;
         }
