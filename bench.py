@@ -17,7 +17,9 @@ shard, so each rank solves its own replica (weak scaling, no data-path
 collective); value = all ranks' bytes / the slowest rank's time.  Beside it,
 `row_partitioned` splits one class-D system by rows over all ranks (strong
 scaling: NCCL all-gather of p and two scalar all-reduces per CG step), and
-`batched` shards the uneven batch by system.
+`batched` shards the uneven batch by system.  `mg` runs the NPB MG
+benchmark (class C) on every rank's GPU beside the reference's own GPU code
+for MG.
 
 `--impl reference` times the reference's own CPU code (oracle/_ref, the
 reference cg.cu compiled as is: serial, it has no threading) on the same
@@ -545,6 +547,55 @@ def row_partitioned_section(npbcg, device, rank, world, dist):
     }
 
 
+MG_CLASS = "C"
+
+
+def mg_section(npbcg, device, rank, world, dist):
+    """NPB MG class C (512^3, 20 V-cycles) on each rank's GPU (replicas: the
+    MG grid is not split), next to the reference's own GPU code for MG on
+    the same GPU and its serial CPU code (rank 0, one GPU)."""
+    import torch
+    c = npbcg.MG_CLASSES[MG_CLASS]
+    n = 1 << c["lt"]
+    with npbcg.Mg.for_class(MG_CLASS, device) as g:
+        g.run(c["nit"])  # the graph's capture and a warm-up
+        runs = [g.run(c["nit"]) for _ in range(3)]
+    ms = max(r["device_ms"] for r in runs)
+    if dist is not None:
+        dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    if rank != 0:
+        return None
+    rnm2 = runs[-1]["rnm2"]
+    nbytes = npbcg.mg_region_bytes(c["lt"], c["nit"])
+    peak, peak_kind = peaks()
+    out = {
+        "what": f"NPB MG class {MG_CLASS}: {n}^3 grid, {c['nit']} V-cycles (resid, psinv, rprj3, "
+                "interp kernels, timed region as one CUDA graph), FP64",
+        "ms": ms, "mops": 58.0 * c["nit"] * n ** 3 * 1e-6 / (ms / 1e3),
+        "rnm2": rnm2, "rel_err_vs_verify": abs(rnm2 - c["rnm2"]) / c["rnm2"],
+        "verified": abs(rnm2 - c["rnm2"]) / c["rnm2"] <= npbcg.MG_VERIFY_EPSILON,
+        "algorithmic_bytes": nbytes, "achieved_gbs": nbytes / (ms / 1e3) / 1e9,
+        "frac_of_peak": nbytes / (ms / 1e3) / 1e9 / peak, "peak_source": peak_kind,
+        "replicas": world,
+    }
+    ref_path = os.path.join(ROOT, "oracle", "_ref", f"libref_mg_{MG_CLASS}.so")
+    if world == 1 and os.path.exists(ref_path):
+        from oracle_py import RefMgLib
+        ref = RefMgLib(ref_path)
+        ref.gpu()
+        rg = min((ref.gpu() for _ in range(2)), key=lambda r: r["seconds"])
+        out["reference_gpu"] = {
+            "what": "the reference's timed MG region on this GPU (mg.cu:486-517: resid_gpu, "
+                    "norm2u3_gpu, mg3P_gpu ...), compiled from its sources with its device flags",
+            "ms": rg["seconds"] * 1e3, "rnm2": rg["rnm2"],
+            "our_speedup": rg["seconds"] * 1e3 / ms,
+        }
+    return out
+
+
 def our_arm(args, rank, world, local_rank):
     import torch
     import npbcg
@@ -705,6 +756,10 @@ def our_arm(args, rank, world, local_rank):
                 "openmp_port": {"value": sample_bytes / omp_s / 1e9, "unit": "GB/s",
                                 "cores": threads, "kind": "port", "seconds": omp_s},
             }
+    if not args.no_mg:
+        mg = mg_section(npbcg, device, rank, world, dist)
+        if line is not None:
+            line["mg"] = mg
     if not args.no_partitioned:
         part = row_partitioned_section(npbcg, device, rank, world, dist)
         if line is not None:
@@ -736,6 +791,7 @@ def main():
     ap.add_argument("--no-solver-modes", action="store_true",
                     help="skip the class C comparison of the solver modes")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-mg", action="store_true", help="skip the NPB MG class C section")
     ap.add_argument("--no-partitioned", action="store_true",
                     help="skip class D split by rows over the ranks")
     args = ap.parse_args()

@@ -27,6 +27,7 @@ CHECKED_SOURCES = ["session.cu", "noalloc.cu"]
 LIB_CHECKED = os.path.join(LIBDIR, "libcgb_checked.so")
 BINDIR = os.path.join(HERE, "bin")
 DRIVER = os.path.join(BINDIR, "cg")
+MG_DRIVER = os.path.join(BINDIR, "mg")
 
 
 def nvcc():
@@ -84,11 +85,15 @@ def build(verbose=False, ptxas_info=False, force=False):
     if force or sources_newer(LIB, objs):
         run([nvcc(), "-shared", "-o", LIB, *objs, *ARCH, "-cudart", "static",
              "-Xcompiler", "-pthread", "-lpthread"], verbose)
-    # the NPB-style command-line driver, linked against libcgb.so
+    # the NPB-style command-line drivers, linked against libcgb.so
     os.makedirs(BINDIR, exist_ok=True)
     main_src = os.path.join(CSRC, "cg_main.cpp")
     if force or sources_newer(DRIVER, [main_src, LIB] + headers):
         run([nvcc(), "-O2", "-std=c++17", "-o", DRIVER, main_src, "-L" + LIBDIR, "-lcgb",
+             "-Xlinker", "-rpath=$ORIGIN/../lib"], verbose)
+    mg_src = os.path.join(CSRC, "mg_main.cpp")
+    if force or sources_newer(MG_DRIVER, [mg_src, LIB] + headers):
+        run([nvcc(), "-O2", "-std=c++17", "-o", MG_DRIVER, mg_src, "-L" + LIBDIR, "-lcgb",
              "-Xlinker", "-rpath=$ORIGIN/../lib"], verbose)
     return LIB
 

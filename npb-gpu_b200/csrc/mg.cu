@@ -248,59 +248,58 @@ __global__ void __launch_bounds__(32 * kRows) k_interp(const double *__restrict_
 }
 
 // Sum of squares and largest magnitude over the interior: block b takes
-// rows (i2, i3) b, b + grid, ... and its threads stride x; a thread loads
-// kBatch of its values ahead, then adds them in its fixed order.  Per-block
+// rows (i2, i3) b, b + grid, ... and its threads stride x (at most four
+// values of a row each: n <= 1024); the loads of four rows are issued
+// before their values are added in the thread's fixed order.  Per-block
 // tree, then the last block (ticket) adds the blocks in order.
 // out[0] = sum, out[1] = max.
-constexpr int kBatch = 8;
+constexpr int kRowsAhead = 4, kMaxPerRow = 4;
 
 __global__ void __launch_bounds__(kNormThreads) k_norm(const double *__restrict__ r, int m, double *part,
                                                        unsigned *ticket, double *out)
 {
     __shared__ double ss[kNormThreads], sm[kNormThreads];
     __shared__ bool last;
-    const int n = m - 2;
-    const int per_row = (n + kNormThreads - 1) / kNormThreads;  // x slots a thread has per row
-    const long long rows = (long long)n * n;
-    const long long mine = rows > blockIdx.x ? (rows - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
-    const long long items = mine * per_row;
+    const int n = m - 2, rows = n * n, tid = threadIdx.x;
     double s = 0.0, mx = 0.0;
-    for (long long q0 = 0; q0 < items; q0 += kBatch) {
-        double xv[kBatch];
+    for (int row0 = blockIdx.x; row0 < rows; row0 += kRowsAhead * gridDim.x) {
+        double xv[kRowsAhead][kMaxPerRow];
 #pragma unroll
-        for (int b = 0; b < kBatch; b++) {
-            const long long q = q0 + b;
-            xv[b] = 0.0;
-            if (q < items) {
-                const long long row = blockIdx.x + (q / per_row) * gridDim.x;
-                const int i1 = 1 + int(threadIdx.x) + int(q % per_row) * kNormThreads;
-                if (i1 <= n) xv[b] = r[at(m, 1 + int(row / n), 1 + int(row % n), i1)];
+        for (int u = 0; u < kRowsAhead; u++) {
+            const int row = row0 + u * int(gridDim.x);
+            const double *line = row < rows ? r + at(m, 1 + row / n, 1 + row % n, 0) : nullptr;
+#pragma unroll
+            for (int j = 0; j < kMaxPerRow; j++) {
+                const int i1 = 1 + tid + j * kNormThreads;
+                xv[u][j] = (line && i1 <= n) ? line[i1] : 0.0;
             }
         }
 #pragma unroll
-        for (int b = 0; b < kBatch; b++) {
-            s = s + xv[b] * xv[b];
-            mx = fmax(mx, fabs(xv[b]));
-        }
+        for (int u = 0; u < kRowsAhead; u++)
+#pragma unroll
+            for (int j = 0; j < kMaxPerRow; j++) {
+                s = s + xv[u][j] * xv[u][j];
+                mx = fmax(mx, fabs(xv[u][j]));
+            }
     }
-    ss[threadIdx.x] = s;
-    sm[threadIdx.x] = mx;
+    ss[tid] = s;
+    sm[tid] = mx;
     __syncthreads();
     for (int w = kNormThreads / 2; w > 0; w >>= 1) {
-        if (int(threadIdx.x) < w) {
-            ss[threadIdx.x] = ss[threadIdx.x] + ss[threadIdx.x + w];
-            sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + w]);
+        if (tid < w) {
+            ss[tid] = ss[tid] + ss[tid + w];
+            sm[tid] = fmax(sm[tid], sm[tid + w]);
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         part[2 * blockIdx.x] = ss[0];
         part[2 * blockIdx.x + 1] = sm[0];
         __threadfence();
         last = atomicAdd(ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (last && threadIdx.x == 0) {
+    if (last && tid == 0) {
         __threadfence();
         double a = 0.0, b = 0.0;
         for (int i = 0; i < int(gridDim.x); i++) {

@@ -972,3 +972,16 @@ def mg_apply(op, m, in1, in2=None, out=None, smoother=0, device=0):
     _check(lib().cgb_mg_apply(device, op, m, smoother, a.ctypes.data_as(ctypes.c_void_p),
                               None if b is None else b.ctypes.data_as(ctypes.c_void_p), res))
     return res
+
+
+def mg_region_bytes(lt, nit):
+    """Algorithmic bytes of the MG timed region (resid, norm, nit x (V-cycle,
+    resid), norm): every grid an operator reads or writes, counted once per
+    operator, ghost layers included; a level-k grid is (2^k + 2)^3 doubles."""
+    c = {k: 8.0 * ((1 << k) + 2) ** 3 for k in range(1, lt + 1)}
+    cycle = sum(c[k] + c[k - 1] for k in range(2, lt + 1))          # rprj3
+    cycle += c[1] + 3 * c[1]                                          # zero, psinv
+    cycle += sum(c[k - 1] + c[k] + 3 * c[k] + 3 * c[k] for k in range(2, lt))  # interp, resid, psinv
+    cycle += c[lt - 1] + 2 * c[lt] + 3 * c[lt] + 3 * c[lt]            # interp (adding), resid, psinv
+    cycle += 3 * c[lt]                                                # the main loop's resid
+    return 3 * c[lt] + 2 * c[lt] + nit * cycle

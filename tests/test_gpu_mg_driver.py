@@ -1,0 +1,88 @@
+"""The NPB-style MG driver `npb-gpu_b200/bin/mg`, a drop-in for the
+reference's mg.<CLASS> binary (GMAP/NPB-GPU CUDA/MG/mg.cu main, :356-623).
+
+Its report must carry the reference's verification block (mg.cu:526-552,
+epsilon 1e-8 on the L2 norm) and its Mop/s, recomputed here from the
+reported time with the reference's operation count 58 nit n^3
+(mg.cu:554-559).  The CPU tests check the argument handling and that
+without a GPU the driver fails loudly (no CPU fallback).
+"""
+import json
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+MG = os.path.join(ROOT, "npb-gpu_b200", "bin", "mg")
+VERIFY = {"S": (32, 4, 0.5307707005734e-04), "W": (128, 4, 0.6467329375339e-05),
+          "B": (256, 20, 0.1800564401355e-05)}
+
+
+def run_mg(*args, timeout=600):
+    if not os.path.exists(MG):
+        pytest.skip("npb-gpu_b200/bin/mg not built")
+    return subprocess.run([MG, *args], capture_output=True, text=True, timeout=timeout)
+
+
+def field(text, name):
+    m = re.search(r"^\s*" + re.escape(name) + r"\s*=\s*(.+?)\s*$", text, re.M)
+    assert m, f"no '{name}' line in the report"
+    return m.group(1)
+
+
+def test_mg_driver_rejects_bad_arguments():
+    for args in ([], ["X"], ["SS"], ["S", "--nit", "0"], ["S", "--what"]):
+        r = run_mg(*args, timeout=60)
+        assert r.returncode == 2, (args, r.returncode)
+        assert "usage: mg" in r.stderr
+
+
+def test_mg_driver_fails_loudly_without_a_gpu():
+    import npbcg
+    try:
+        npbcg.device_info(0)
+        pytest.skip("a CUDA device is present")
+    except npbcg.CgbError:
+        pass
+    r = run_mg("S", timeout=120)
+    assert r.returncode == 1 and "mg: create failed" in r.stderr
+    assert "VERIFICATION" not in r.stdout
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cls", ["S", "W"])
+def test_mg_driver_report_verifies(cls):
+    n, nit, want = VERIFY[cls]
+    r = run_mg(cls)
+    assert r.returncode == 0, r.stderr
+    assert " VERIFICATION SUCCESSFUL" in r.stdout
+    norm = float(re.search(r"L2 Norm is\s+(\S+)", r.stdout).group(1))
+    assert abs(norm - want) / want <= 1e-8
+    assert field(r.stdout, "class_npb") == cls
+    assert int(field(r.stdout, "Iterations")) == nit
+    assert field(r.stdout, "Verification") == "SUCCESSFUL"
+    t = float(field(r.stdout, "Time in seconds"))
+    mops = float(field(r.stdout, "Mop/s total"))
+    expect = 58.0 * nit * n ** 3 * 1e-6 / t
+    assert abs(mops - expect) <= expect * (1e-6 / t + 1e-6) + 0.01
+
+
+@pytest.mark.gpu
+def test_mg_driver_json_class_b():
+    n, nit, want = VERIFY["B"]
+    r = run_mg("B", "--json")
+    assert r.returncode == 0, r.stderr
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["class"] == "B" and line["n"] == n and line["nit"] == nit
+    assert line["verified"] is True and line["rel_err"] <= 1e-8
+    assert abs(line["mops"] - 58.0 * nit * n ** 3 * 1e-6 / line["seconds"]) <= 1e-5 * line["mops"]
+
+
+@pytest.mark.gpu
+def test_mg_driver_other_iteration_count_is_unverified():
+    r = run_mg("S", "--nit", "2")
+    assert r.returncode == 0, r.stderr
+    assert "NO VERIFICATION PERFORMED" in r.stdout
+    assert field(r.stdout, "Verification") == "NOT PERFORMED"
