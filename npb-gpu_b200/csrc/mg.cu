@@ -11,7 +11,7 @@
 //   interp  u (+)= P z        (:836-890)    trilinear prolongation
 //   norm2u3                   (:1201-1230)  deterministic two-level reduction
 // The 27-point operators stage their input in shared memory, plane by plane
-// along z (a ring of three planes of a 32 x 8 tile with its halo, the next
+// along z (a ring of three planes of a 32 x 4 tile with its halo, the next
 // plane loading while the current one is computed); a warp covers 32
 // consecutive x of one row, each lane forms the column sums of its own x
 // (the reference's u1/u2 line buffers) and takes its neighbours' from the
@@ -48,7 +48,7 @@ namespace cgb {
 namespace mg {
 
 constexpr int kMaxLevels = 11;   // lt <= 10: a 1024^3 grid (class D)
-constexpr int kRows = 8;         // (y) rows of a stencil CTA; x is a warp
+constexpr int kRows = 4;         // (y) rows of a stencil CTA; x is a warp
 constexpr int kNormBlocks = 1184;
 constexpr int kNormThreads = 256;
 constexpr int kCandCap = 8192;   // zran3 candidates kept per side
@@ -96,7 +96,7 @@ __device__ __forceinline__ void store_periodic(double *g, int m, int i3, int i2,
 // before the current plane's arithmetic and land in registers, so their
 // latency hides behind it.  kPsinv: u = u + C g (g = r); otherwise
 // out = w - A g (g = u, w = v; out may be w).
-constexpr int kPlanes = 32;
+constexpr int kPlanes = 16;
 constexpr int kTileW = 34, kTileH = kRows + 2, kTile = kTileW * kTileH;
 constexpr int kThreads = 32 * kRows;
 static_assert(kTile <= 2 * kThreads, "a thread stages at most two tile cells");
