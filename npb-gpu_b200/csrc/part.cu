@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -74,8 +75,16 @@ std::once_flag g_nccl_once;
 const NcclApi *nccl()
 {
     std::call_once(g_nccl_once, [] {
-        void *h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
-        if (!h) h = dlopen("libnccl.so", RTLD_NOW | RTLD_GLOBAL);
+        // The NCCL to use: the one CGB_NCCL_LIBRARY names; else one already
+        // in the process (a framework's, e.g. torch's); else the system's.
+        // A process holds one libnccl.so.2 (later users bind to the loaded
+        // one by its soname), so the first to load it picks it for all.
+        void *h = nullptr;
+        const char *path = std::getenv("CGB_NCCL_LIBRARY");
+        if (path && *path) h = dlopen(path, RTLD_NOW | RTLD_LOCAL);
+        if (!h) h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_NOLOAD);
+        if (!h) h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_LOCAL);
+        if (!h) h = dlopen("libnccl.so", RTLD_NOW | RTLD_LOCAL);
         if (!h) return;
         NcclApi a;
         a.get_unique_id = reinterpret_cast<decltype(a.get_unique_id)>(dlsym(h, "ncclGetUniqueId"));

@@ -794,8 +794,25 @@ def row_block(rowstr, colidx, a, row0, row1):
     return rs, np.ascontiguousarray(colidx[k0:k1], np.int32), np.ascontiguousarray(a[k0:k1], np.float64)
 
 
+def _choose_nccl():
+    """Point libcgb at the NCCL that torch is built against (the pip
+    nvidia-nccl package), when there is one and no choice was made: a
+    process can hold only one libnccl.so.2, and whichever loads first binds
+    every later user, so libcgb and torch must agree."""
+    if os.environ.get("CGB_NCCL_LIBRARY"):
+        return
+    import importlib.util
+    spec = importlib.util.find_spec("nvidia")
+    for base in (spec.submodule_search_locations or []) if spec else []:
+        cand = os.path.join(base, "nccl", "lib", "libnccl.so.2")
+        if os.path.exists(cand):
+            os.environ["CGB_NCCL_LIBRARY"] = cand
+            return
+
+
 def nccl_unique_id():
     """A new NCCL unique id (bytes) for rank 0 to broadcast to the others."""
+    _choose_nccl()
     buf = ctypes.create_string_buffer(NCCL_ID_BYTES)
     _check(lib().cgb_nccl_unique_id(buf))
     return buf.raw
@@ -804,6 +821,7 @@ def nccl_unique_id():
 def _id_buffer(nccl_id):
     if nccl_id is None:
         return None
+    _choose_nccl()
     if len(nccl_id) != NCCL_ID_BYTES:
         raise CgbError(ERR_INVALID, f"nccl_id must be {NCCL_ID_BYTES} bytes")
     return ctypes.create_string_buffer(bytes(nccl_id), NCCL_ID_BYTES)

@@ -135,3 +135,15 @@ def test_exchange_plan_matches_reference(tmp_path, golden, world):
     assert np.max(np.abs(zeta - ref) / ref) <= 1e-10
     assert np.max(np.abs(rnorm - np.array(e["rnorm"]))) <= 1e-10
     assert abs(zeta[-1] - golden["verify"]["S"]) / golden["verify"]["S"] <= 1e-10
+
+
+def test_nccl_choice_agrees_with_torch():
+    """libcgb loads NCCL on first use; a process holds one libnccl.so.2, so
+    loading a different one than torch's would leave torch unable to load
+    its own.  In a fresh process: libcgb's NCCL first, torch afterwards."""
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, %r); import npbcg; npbcg.nccl_unique_id(); "
+            "import torch.distributed; print('ok')" % os.path.join(ROOT, "npb-gpu_b200"))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-2000:]
