@@ -11,11 +11,11 @@
 //   interp  u (+)= P z        (:836-890)    trilinear prolongation
 //   norm2u3                   (:1201-1230)  deterministic two-level reduction
 // The 27-point operators stage their input in shared memory, plane by plane
-// along z (a ring of three planes of a 32 x 4 tile with its halo, the next
-// plane loading while the current one is computed); a warp covers 32
-// consecutive x of one row, each lane forms the column sums of its own x
-// (the reference's u1/u2 line buffers) and takes its neighbours' from the
-// adjacent lanes by shuffles.  The periodic ghost exchange (comm3,
+// along z (a ring of three planes of a 32 x 8 tile with its halo, the next
+// plane loading while the current one is computed); a thread computes one x
+// of two rows from the column sums (the reference's u1/u2 line buffers) of
+// the staged rows, and takes its x neighbours' sums from the adjacent lanes
+// by shuffles.  The periodic ghost exchange (comm3,
 // :687-716, which only copies interior values) is fused: the thread that
 // writes an interior point also writes that value into each ghost cell that
 // mirrors it.  On coarse levels the reference zeroes u and then adds the
@@ -48,7 +48,7 @@ namespace cgb {
 namespace mg {
 
 constexpr int kMaxLevels = 11;   // lt <= 10: a 1024^3 grid (class D)
-constexpr int kRows = 4;         // (y) rows of a stencil CTA; x is a warp
+constexpr int kRows = 4;         // (y) rows of a restriction / prolongation CTA; x is a warp
 constexpr int kNormBlocks = 1184;
 constexpr int kNormThreads = 256;
 constexpr int kCandCap = 8192;   // zran3 candidates kept per side
@@ -88,88 +88,124 @@ __device__ __forceinline__ void store_periodic(double *g, int m, int i3, int i2,
             for (int a = 0; a < nx; a++) g[at(m, z[c], y[b], x[a])] = val;
 }
 
-// The 27-point operators with the input grid staged in shared memory: a
-// CTA owns a 32 x kRows tile of (x, y) and walks kPlanes z planes, keeping
-// planes z-1, z, z+1 of the tile plus a one-cell halo in a ring of three
-// (34 x (kRows + 2) doubles each), so each input value is read from L2/HBM
-// about once instead of by nine threads.  The next plane's loads are issued
-// before the current plane's arithmetic and land in registers, so their
-// latency hides behind it.  kPsinv: u = u + C g (g = r); otherwise
-// out = w - A g (g = u, w = v; out may be w).
+// The 27-point operators (resid, psinv) stage their input grid in shared
+// memory: a CTA owns a 32 x 8 (x, y) tile and walks kPlanes z planes,
+// keeping planes z-1, z, z+1 of the tile plus a one-cell halo in a ring of
+// three (34 x 10 doubles each), so each input value is read from L2/HBM
+// about once instead of by nine threads; the next plane's loads are issued
+// into registers before the current plane is computed.  A thread owns one
+// x of two consecutive rows, so the four rows of each staged plane around
+// them serve both points' column sums (12 shared reads for two points
+// instead of 16, the centres with them).  A warp is 32 consecutive x: a
+// lane takes its neighbours' column sums by shuffles.  kPsinv:
+// u = u + C g (g = r); otherwise out = w - A g (g = u, w = v; out may be w).
 constexpr int kPlanes = 16;
-constexpr int kTileW = 34, kTileH = kRows + 2, kTile = kTileW * kTileH;
-constexpr int kThreads = 32 * kRows;
-static_assert(kTile <= 2 * kThreads, "a thread stages at most two tile cells");
+constexpr int kTileW = 34;
+
+constexpr int kRB = 2;                    // rows a thread
+constexpr int kWarpsRB = 4;
+constexpr int kRowsRB = kRB * kWarpsRB;   // 8 rows a tile
+constexpr int kTileRB = kTileW * (kRowsRB + 2);
+constexpr int kThreadsRB = 32 * kWarpsRB;
+constexpr int kStageRB = (kTileRB + kThreadsRB - 1) / kThreadsRB;  // cells a thread stages
 
 template <bool kPsinv>
-__global__ void __launch_bounds__(kThreads) k_stencil(const double *__restrict__ g, const double *w,
-                                                      double *out, int m, Coef cf)
+__global__ void __launch_bounds__(kThreadsRB) k_stencil_rb(const double *__restrict__ g, const double *w,
+                                                           double *out, int m, Coef cf)
 {
-    __shared__ double ring[3][kTile];
+    __shared__ double ring[3][kTileRB];
     const int n = m - 2;
-    const int tx = threadIdx.x, ty = threadIdx.y, t = ty * 32 + tx;
-    const int x0 = 1 + int(blockIdx.x) * 32, y0 = 1 + int(blockIdx.y) * kRows;
+    const int tx = threadIdx.x, wy = threadIdx.y, t = wy * 32 + tx;
+    const int x0 = 1 + int(blockIdx.x) * 32, y0 = 1 + int(blockIdx.y) * kRowsRB;
     const int z0 = 1 + int(blockIdx.z) * kPlanes, z1 = min(n, z0 + kPlanes - 1);
-    const int x = x0 + tx, y = y0 + ty;
+    const int x = x0 + tx, yb = y0 + wy * kRB;
     const size_t plane = size_t(m) * m;
-    // the (up to two) tile cells this thread stages, as offsets in a plane
-    const int e1 = t + kThreads;
-    const int gx0 = x0 - 1 + t % kTileW, gy0 = y0 - 1 + t / kTileW;
-    const int gx1 = x0 - 1 + e1 % kTileW, gy1 = y0 - 1 + e1 / kTileW;
-    const bool in0 = gx0 <= m - 1 && gy0 <= m - 1;
-    const bool in1 = e1 < kTile && gx1 <= m - 1 && gy1 <= m - 1;
-    const size_t o0 = size_t(gy0) * m + gx0, o1 = size_t(gy1) * m + gx1;
-    auto fetch = [&](int z, double &a, double &b) {
-        a = in0 ? g[z * plane + o0] : 0.0;
-        b = in1 ? g[z * plane + o1] : 0.0;
+    size_t off[kStageRB];
+    bool inside[kStageRB];
+#pragma unroll
+    for (int q = 0; q < kStageRB; q++) {
+        const int e = t + q * kThreadsRB;
+        const int gx = x0 - 1 + e % kTileW, gy = y0 - 1 + e / kTileW;
+        inside[q] = e < kTileRB && gx <= m - 1 && gy <= m - 1;
+        off[q] = size_t(gy) * m + gx;
+    }
+    auto fetch = [&](int z, double *v) {
+#pragma unroll
+        for (int q = 0; q < kStageRB; q++) v[q] = inside[q] ? g[z * plane + off[q]] : 0.0;
     };
-    auto put = [&](int z, double a, double b) {
-        ring[z % 3][t] = a;
-        if (e1 < kTile) ring[z % 3][e1] = b;
+    auto put = [&](int z, const double *v) {
+#pragma unroll
+        for (int q = 0; q < kStageRB; q++) {
+            const int e = t + q * kThreadsRB;
+            if (e < kTileRB) ring[z % 3][e] = v[q];
+        }
     };
     {
-        double a, b, c, d, e, f;
-        fetch(z0 - 1, a, b);
-        fetch(z0, c, d);
-        fetch(z0 + 1, e, f);
-        put(z0 - 1, a, b);
-        put(z0, c, d);
-        put(z0 + 1, e, f);
+        double a[kStageRB], b[kStageRB], c[kStageRB];
+        fetch(z0 - 1, a);
+        fetch(z0, b);
+        fetch(z0 + 1, c);
+        put(z0 - 1, a);
+        put(z0, b);
+        put(z0 + 1, c);
     }
     __syncthreads();
-    const int lx = tx + 1, ly = ty + 1;
-    const bool store = x <= n && y <= n;
+    const int lx = tx + 1, lr = wy * kRB;  // the tile row above this thread's first row
     for (int z = z0; z <= z1; z++) {
-        double na = 0.0, nb = 0.0;
-        if (z + 1 <= z1) fetch(z + 2, na, nb);  // in flight during this plane
-        const size_t c = at(m, z, y, x);
-        const double wc = store ? (kPsinv ? out[c] : w[c]) : 0.0;
+        double next[kStageRB];
+        if (z + 1 <= z1) fetch(z + 2, next);  // in flight during this plane
+        double wc[kRB];
+#pragma unroll
+        for (int i = 0; i < kRB; i++) {
+            const int y = yb + i;
+            wc[i] = (x <= n && y <= n) ? (kPsinv ? out[at(m, z, y, x)] : w[at(m, z, y, x)]) : 0.0;
+        }
         const double *Pm = ring[(z - 1) % 3], *P0 = ring[z % 3], *Pp = ring[(z + 1) % 3];
-        // column sums (the reference's u1 / u2) of column k of this row
-        auto sums = [&](int k, double &s1, double &s2) {
-            s1 = P0[(ly - 1) * kTileW + k] + P0[(ly + 1) * kTileW + k] + Pm[ly * kTileW + k] +
-                 Pp[ly * kTileW + k];
-            s2 = Pm[(ly - 1) * kTileW + k] + Pm[(ly + 1) * kTileW + k] + Pp[(ly - 1) * kTileW + k] +
-                 Pp[(ly + 1) * kTileW + k];
+        // rows lr .. lr + kRB + 1 of column k in the three planes, and the
+        // kRB rows' column sums (the reference's u1, u2) and centres
+        auto column = [&](int k, double *s1, double *s2, double *ctr) {
+            double a[kRB + 2], b[kRB + 2], c[kRB + 2];
+#pragma unroll
+            for (int j = 0; j < kRB + 2; j++) {
+                a[j] = P0[(lr + j) * kTileW + k];
+                b[j] = Pm[(lr + j) * kTileW + k];
+                c[j] = Pp[(lr + j) * kTileW + k];
+            }
+#pragma unroll
+            for (int i = 0; i < kRB; i++) {
+                s1[i] = a[i] + a[i + 2] + b[i + 1] + c[i + 1];
+                s2[i] = b[i] + b[i + 2] + c[i] + c[i + 2];
+                ctr[i] = a[i + 1];
+            }
         };
-        double s1, s2;
-        sums(lx, s1, s2);
-        double s1m = __shfl_up_sync(0xffffffffu, s1, 1), s2m = __shfl_up_sync(0xffffffffu, s2, 1);
-        double s1p = __shfl_down_sync(0xffffffffu, s1, 1), s2p = __shfl_down_sync(0xffffffffu, s2, 1);
-        if (tx == 0) sums(lx - 1, s1m, s2m);
-        if (tx == 31) sums(lx + 1, s1p, s2p);
-        if (store) {
-            const double gc = P0[ly * kTileW + lx];
+        double s1[kRB], s2[kRB], ctr[kRB], s1m[kRB], s2m[kRB], cm[kRB], s1p[kRB], s2p[kRB], cp[kRB];
+        column(lx, s1, s2, ctr);
+#pragma unroll
+        for (int i = 0; i < kRB; i++) {
+            s1m[i] = __shfl_up_sync(0xffffffffu, s1[i], 1);
+            s2m[i] = __shfl_up_sync(0xffffffffu, s2[i], 1);
+            s1p[i] = __shfl_down_sync(0xffffffffu, s1[i], 1);
+            s2p[i] = __shfl_down_sync(0xffffffffu, s2[i], 1);
+            cm[i] = __shfl_up_sync(0xffffffffu, ctr[i], 1);
+            cp[i] = __shfl_down_sync(0xffffffffu, ctr[i], 1);
+        }
+        if (tx == 0) column(lx - 1, s1m, s2m, cm);
+        if (tx == 31) column(lx + 1, s1p, s2p, cp);
+#pragma unroll
+        for (int i = 0; i < kRB; i++) {
+            const int y = yb + i;
+            if (x > n || y > n) continue;
             double val;
             if constexpr (kPsinv)
-                val = wc + cf.c0 * gc + cf.c1 * (P0[ly * kTileW + lx - 1] + P0[ly * kTileW + lx + 1] + s1) +
-                      cf.c2 * (s2 + s1m + s1p);
+                val = wc[i] + cf.c0 * ctr[i] + cf.c1 * (cm[i] + cp[i] + s1[i]) +
+                      cf.c2 * (s2[i] + s1m[i] + s1p[i]);
             else
-                val = wc - cf.a0 * gc - cf.a2 * (s2 + s1m + s1p) - cf.a3 * (s2m + s2p);
+                val = wc[i] - cf.a0 * ctr[i] - cf.a2 * (s2[i] + s1m[i] + s1p[i]) -
+                      cf.a3 * (s2m[i] + s2p[i]);
             store_periodic(out, m, z, y, x, val);
         }
         __syncthreads();  // every read of plane z-1's slot is done
-        if (z + 1 <= z1) put(z + 2, na, nb);
+        if (z + 1 <= z1) put(z + 2, next);
         __syncthreads();
     }
 }
@@ -434,25 +470,26 @@ dim3 stencil_grid(int m)
     return dim3(unsigned((m - 1 + 31) / 32), unsigned((m - 2 + kRows - 1) / kRows), unsigned(m - 2));
 }
 
-dim3 stencil25_grid(int m)
-{
-    const int n = m - 2;
-    return dim3(unsigned((n + 31) / 32), unsigned((n + kRows - 1) / kRows), unsigned((n + kPlanes - 1) / kPlanes));
-}
 
 dim3 interp_grid(int mj)
 {
     return dim3(unsigned((mj - 1 + 31) / 32), unsigned((mj - 1 + kRows - 1) / kRows), unsigned(mj - 1));
 }
 
+dim3 stencil_rb_grid(int m)
+{
+    const int n = m - 2;
+    return dim3(unsigned((n + 31) / 32), unsigned((n + kRowsRB - 1) / kRowsRB), unsigned((n + kPlanes - 1) / kPlanes));
+}
+
 void launch_resid(cgb_mg *g, int k, const double *u, const double *v, double *r)
 {
-    k_stencil<false><<<stencil25_grid(g->m[k]), dim3(32, kRows), 0, g->stream>>>(u, v, r, g->m[k], g->cf);
+    k_stencil_rb<false><<<stencil_rb_grid(g->m[k]), dim3(32, kWarpsRB), 0, g->stream>>>(u, v, r, g->m[k], g->cf);
 }
 
 void launch_psinv(cgb_mg *g, int k, const double *r, double *u)
 {
-    k_stencil<true><<<stencil25_grid(g->m[k]), dim3(32, kRows), 0, g->stream>>>(r, nullptr, u, g->m[k], g->cf);
+    k_stencil_rb<true><<<stencil_rb_grid(g->m[k]), dim3(32, kWarpsRB), 0, g->stream>>>(r, nullptr, u, g->m[k], g->cf);
 }
 
 void launch_rprj3(cgb_mg *g, int k)  // level k -> k - 1
@@ -739,8 +776,8 @@ int cgb_mg_apply(int device, int op, int m, int smoother, const double *in1, con
         st = set_error(CGB_ERR_CUDA, "mg: operator upload");
     if (!st) {
         switch (op) {
-        case 0: k_stencil<false><<<stencil25_grid(m), dim3(32, kRows)>>>(a, b, c, m, cf); break;
-        case 1: k_stencil<true><<<stencil25_grid(m), dim3(32, kRows)>>>(a, nullptr, c, m, cf); break;
+        case 0: k_stencil_rb<false><<<stencil_rb_grid(m), dim3(32, kWarpsRB)>>>(a, b, c, m, cf); break;
+        case 1: k_stencil_rb<true><<<stencil_rb_grid(m), dim3(32, kWarpsRB)>>>(a, nullptr, c, m, cf); break;
         case 2: k_rprj3<<<stencil_grid(mo), dim3(32, kRows)>>>(a, m, c, mo); break;
         default: k_interp<<<interp_grid(m), dim3(32, kRows)>>>(a, m, c, mo, op == 4); break;
         }
