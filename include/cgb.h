@@ -491,6 +491,16 @@ int cgb_mg_points(cgb_mg *g, int *plus, int *minus);
 int cgb_mg_apply(int device, int op, int m, int smoother, const double *in1, const double *in2,
                  double *out);
 
+/* ---- NPB EP: Gaussian pairs from one random stream -----------------------
+ * The reference's EP (CUDA/EP/ep.cu): 2^m pairs of uniform deviates from the
+ * LCG seeded 271828183 (multiplier 5^13), the pairs inside the unit disc
+ * turned into Gaussian deviates; their sums sx, sy and the counts q[0..9]
+ * of pairs with floor(max(|X|, |Y|)) = l.  Classes (setparams.cpp:826-845):
+ * m = 24 S, 25 W, 28 A, 30 B, 32 C, 36 D, 40 E; verify sx, sy at relative
+ * 1e-8 against ep.cu:189-212.  device_ms: the kernel's device time.  Any
+ * output may be NULL; q holds 10 doubles. */
+int cgb_ep_run(int device, int m, double *sx, double *sy, double *q, double *device_ms);
+
 /* Host memory that the device copies at full speed (cudaHostAlloc). */
 int cgb_host_alloc(void **ptr, long long bytes);
 int cgb_host_free(void *ptr);

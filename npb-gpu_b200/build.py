@@ -17,9 +17,11 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["session.cu", "noalloc.cu", "gnn.cu", "batch.cu", "makea_gpu.cu", "part.cu", "mg.cu"]
-# per-source flags: the MG operators keep the reference's separate roundings
-EXTRA_FLAGS = {"mg.cu": ["-fmad=false"]}
+CU_SOURCES = ["session.cu", "noalloc.cu", "gnn.cu", "batch.cu", "makea_gpu.cu", "part.cu", "mg.cu",
+              "ep.cu"]
+# per-source flags: MG's operators and EP's deviates keep the reference's
+# separate roundings
+EXTRA_FLAGS = {"mg.cu": ["-fmad=false"], "ep.cu": ["-fmad=false"]}
 CPP_SOURCES = ["makea.cpp"]
 LIB = os.path.join(LIBDIR, "libcgb.so")
 # the checked build: the single-system solver with every SpMV index tested
@@ -28,6 +30,7 @@ LIB_CHECKED = os.path.join(LIBDIR, "libcgb_checked.so")
 BINDIR = os.path.join(HERE, "bin")
 DRIVER = os.path.join(BINDIR, "cg")
 MG_DRIVER = os.path.join(BINDIR, "mg")
+EP_DRIVER = os.path.join(BINDIR, "ep")
 
 
 def nvcc():
@@ -91,10 +94,11 @@ def build(verbose=False, ptxas_info=False, force=False):
     if force or sources_newer(DRIVER, [main_src, LIB] + headers):
         run([nvcc(), "-O2", "-std=c++17", "-o", DRIVER, main_src, "-L" + LIBDIR, "-lcgb",
              "-Xlinker", "-rpath=$ORIGIN/../lib"], verbose)
-    mg_src = os.path.join(CSRC, "mg_main.cpp")
-    if force or sources_newer(MG_DRIVER, [mg_src, LIB] + headers):
-        run([nvcc(), "-O2", "-std=c++17", "-o", MG_DRIVER, mg_src, "-L" + LIBDIR, "-lcgb",
-             "-Xlinker", "-rpath=$ORIGIN/../lib"], verbose)
+    for name, target in (("mg_main.cpp", MG_DRIVER), ("ep_main.cpp", EP_DRIVER)):
+        src = os.path.join(CSRC, name)
+        if force or sources_newer(target, [src, LIB] + headers):
+            run([nvcc(), "-O2", "-std=c++17", "-o", target, src, "-L" + LIBDIR, "-lcgb",
+                 "-Xlinker", "-rpath=$ORIGIN/../lib"], verbose)
     return LIB
 
 

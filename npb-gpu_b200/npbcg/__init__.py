@@ -209,6 +209,9 @@ _SIGNATURES = {
     "cgb_mg_points": (ctypes.c_int, [ctypes.c_void_p, _I32, _I32]),
     "cgb_mg_apply": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_void_p, ctypes.c_void_p, _F64]),
+    "cgb_ep_run": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                  ctypes.POINTER(ctypes.c_double), _F64,
+                                  ctypes.POINTER(ctypes.c_double)]),
     "cgb_host_alloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_longlong]),
     "cgb_host_free": (ctypes.c_int, [ctypes.c_void_p]),
     "cgb_device_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
@@ -1003,3 +1006,25 @@ def mg_region_bytes(lt, nit):
     cycle += c[lt - 1] + 2 * c[lt] + 3 * c[lt] + 3 * c[lt]            # interp (adding), resid, psinv
     cycle += 3 * c[lt]                                                # the main loop's resid
     return 3 * c[lt] + 2 * c[lt] + nit * cycle
+
+
+# NPB EP classes: m (2^m pairs; setparams.cpp:826-845) and the verification
+# sums (ep.cu:189-212)
+EP_CLASSES = {
+    "S": dict(m=24, sx=-3.247834652034740e+3, sy=-6.958407078382297e+3),
+    "W": dict(m=25, sx=-2.863319731645753e+3, sy=-6.320053679109499e+3),
+    "A": dict(m=28, sx=-4.295875165629892e+3, sy=-1.580732573678431e+4),
+    "B": dict(m=30, sx=4.033815542441498e+4, sy=-2.660669192809235e+4),
+    "C": dict(m=32, sx=4.764367927995374e+4, sy=-8.084072988043731e+4),
+    "D": dict(m=36, sx=1.982481200946593e+5, sy=-1.020596636361769e+5),
+    "E": dict(m=40, sx=-5.319717441530e+05, sy=-3.688834557731e+05),
+}
+EP_VERIFY_EPSILON = 1.0e-8
+
+
+def ep_run(m, device=0):
+    """NPB EP with 2^m pairs on the GPU: {sx, sy, q (10 counts), device_ms}."""
+    sx, sy, ms = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    q = np.zeros(10)
+    _check(lib().cgb_ep_run(device, int(m), ctypes.byref(sx), ctypes.byref(sy), q, ctypes.byref(ms)))
+    return dict(sx=sx.value, sy=sy.value, q=q, device_ms=ms.value)

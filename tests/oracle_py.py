@@ -48,6 +48,8 @@ class Oracle:
         lib.orc_mg_rprj3.argtypes = [ctypes.c_int, F64, ctypes.c_int, F64]
         lib.orc_mg_interp.restype = None
         lib.orc_mg_interp.argtypes = [ctypes.c_int, F64, ctypes.c_int, F64]
+        lib.orc_ep_run.restype = ctypes.c_int
+        lib.orc_ep_run.argtypes = [ctypes.c_int, dp, dp, F64, dp]
         lib.orc_mg_norm2u3.restype = None
         lib.orc_mg_norm2u3.argtypes = [ctypes.c_int, F64, dp, dp]
         self.lib = lib
@@ -99,6 +101,15 @@ class Oracle:
         u = np.array(u, dtype=np.float64)
         self.lib.orc_mg_interp(mj, np.ascontiguousarray(z), mk, u)
         return u
+
+    def ep_run(self, m):
+        """NPB EP with 2^m pairs (ep_oracle.c): {sx, sy, q, seconds}."""
+        sx, sy, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        q = np.zeros(10)
+        rc = self.lib.orc_ep_run(m, ctypes.byref(sx), ctypes.byref(sy), q, ctypes.byref(t))
+        if rc != 0:
+            raise RuntimeError(f"orc_ep_run failed: {rc}")
+        return dict(sx=sx.value, sy=sy.value, q=q, seconds=t.value)
 
     def mg_norm(self, m, r):
         a, b = ctypes.c_double(), ctypes.c_double()

@@ -1,5 +1,6 @@
-"""The NPB-style MG driver `npb-gpu_b200/bin/mg`, a drop-in for the
-reference's mg.<CLASS> binary (GMAP/NPB-GPU CUDA/MG/mg.cu main, :356-623).
+"""The NPB-style MG and EP drivers `npb-gpu_b200/bin/mg` and `bin/ep`,
+drop-ins for the reference's mg.<CLASS> and ep.<CLASS> binaries
+(GMAP/NPB-GPU CUDA/MG/mg.cu main :356-623, CUDA/EP/ep.cu main :114-275).
 
 Its report must carry the reference's verification block (mg.cu:526-552,
 epsilon 1e-8 on the L2 norm) and its Mop/s, recomputed here from the
@@ -86,3 +87,36 @@ def test_mg_driver_other_iteration_count_is_unverified():
     assert r.returncode == 0, r.stderr
     assert "NO VERIFICATION PERFORMED" in r.stdout
     assert field(r.stdout, "Verification") == "NOT PERFORMED"
+
+
+# ------------------------------------------------------------------ EP driver
+EP = os.path.join(ROOT, "npb-gpu_b200", "bin", "ep")
+
+
+def run_ep(*args, timeout=600):
+    if not os.path.exists(EP):
+        pytest.skip("npb-gpu_b200/bin/ep not built")
+    return subprocess.run([EP, *args], capture_output=True, text=True, timeout=timeout)
+
+
+def test_ep_driver_rejects_bad_arguments():
+    for args in ([], ["X"], ["SS"], ["S", "--what"]):
+        r = run_ep(*args, timeout=60)
+        assert r.returncode == 2 and "usage: ep" in r.stderr
+
+
+@pytest.mark.gpu
+def test_ep_driver_report_verifies():
+    r = run_ep("W")
+    assert r.returncode == 0, r.stderr
+    assert field(r.stdout, "Verification") == "SUCCESSFUL"
+    sums = re.search(r"Sums =\s+(\S+)\s+(\S+)", r.stdout)
+    sx, sy = float(sums.group(1)), float(sums.group(2))
+    assert abs(sx + 2.863319731645753e+3) / 2.863319731645753e+3 <= 1e-8
+    assert abs(sy + 6.320053679109499e+3) / 6.320053679109499e+3 <= 1e-8
+    t = float(field(r.stdout, "Time in seconds"))
+    mops = float(field(r.stdout, "Mop/s total"))
+    expect = 2.0 ** 26 / t / 1e6
+    assert abs(mops - expect) <= expect * (1e-6 / t + 1e-6) + 0.01
+    line = json.loads(run_ep("S", "--json").stdout.strip().splitlines()[-1])
+    assert line["verified"] is True and line["m"] == 24
