@@ -19,7 +19,7 @@ collective); value = all ranks' bytes / the slowest rank's time.  Beside it,
 scaling: NCCL all-gather of p and two scalar all-reduces per CG step), and
 `batched` shards the uneven batch by system.  `mg` runs the NPB MG
 benchmark (class C) on every rank's GPU beside the reference's own GPU code
-for MG.
+for MG, and `ep` the NPB EP benchmark (class C) likewise.
 
 `--impl reference` times the reference's own CPU code (oracle/_ref, the
 reference cg.cu compiled as is: serial, it has no threading) on the same
@@ -596,6 +596,44 @@ def mg_section(npbcg, device, rank, world, dist):
     return out
 
 
+EP_CLASS = "C"
+
+
+def ep_section(npbcg, device, rank):
+    """NPB EP class C (2^32 pairs) on each rank's GPU, next to the reference's
+    own EP kernel on the same GPU (rank 0).  The reference's timer stops right
+    after its kernel launch (ep.cu:166-172); its time here is the wall time to
+    its sums on the host."""
+    c = npbcg.EP_CLASSES[EP_CLASS]
+    npbcg.ep_run(c["m"], device)  # warm-up
+    runs = [npbcg.ep_run(c["m"], device) for _ in range(3)]
+    if rank != 0:
+        return None
+    ms = max(r["device_ms"] for r in runs)
+    r = runs[-1]
+    out = {
+        "what": f"NPB EP class {EP_CLASS}: 2^{c['m']} pairs, one kernel, FP64 log/sqrt",
+        "ms": ms, "mops": 2.0 ** (c["m"] + 1) / (ms / 1e3) / 1e6,
+        "sx_rel_err": abs(r["sx"] - c["sx"]) / abs(c["sx"]),
+        "sy_rel_err": abs(r["sy"] - c["sy"]) / abs(c["sy"]),
+        "verified": max(abs(r["sx"] - c["sx"]) / abs(c["sx"]),
+                        abs(r["sy"] - c["sy"]) / abs(c["sy"])) <= npbcg.EP_VERIFY_EPSILON,
+    }
+    ref_path = os.path.join(ROOT, "oracle", "_ref", f"libref_ep_{EP_CLASS}.so")
+    if os.path.exists(ref_path):
+        from oracle_py import RefEpLib
+        ref = RefEpLib(ref_path)
+        ref.gpu()
+        rg = min((ref.gpu() for _ in range(2)), key=lambda x: x["seconds_wall"])
+        out["reference_gpu"] = {
+            "what": "the reference's EP kernel on this GPU (ep.cu:159-186: one thread per batch of "
+                    "2^16 pairs), compiled from its sources with its device flags; wall time to "
+                    "its sums on the host",
+            "ms": rg["seconds_wall"] * 1e3, "our_speedup": rg["seconds_wall"] * 1e3 / ms,
+        }
+    return out
+
+
 def our_arm(args, rank, world, local_rank):
     import torch
     import npbcg
@@ -760,6 +798,9 @@ def our_arm(args, rank, world, local_rank):
         mg = mg_section(npbcg, device, rank, world, dist)
         if line is not None:
             line["mg"] = mg
+        ep = ep_section(npbcg, device, rank)
+        if line is not None:
+            line["ep"] = ep
     if not args.no_partitioned:
         part = row_partitioned_section(npbcg, device, rank, world, dist)
         if line is not None:
@@ -791,7 +832,7 @@ def main():
     ap.add_argument("--no-solver-modes", action="store_true",
                     help="skip the class C comparison of the solver modes")
     ap.add_argument("--no-batched", action="store_true")
-    ap.add_argument("--no-mg", action="store_true", help="skip the NPB MG class C section")
+    ap.add_argument("--no-mg", action="store_true", help="skip the NPB MG and EP class C sections")
     ap.add_argument("--no-partitioned", action="store_true",
                     help="skip class D split by rows over the ranks")
     args = ap.parse_args()

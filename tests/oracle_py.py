@@ -263,3 +263,24 @@ class RefMgLib:
         if rc != 0:
             raise RuntimeError("ref_mg_gpu failed")
         return dict(rnm2=a.value, rnmu=b.value, seconds=t.value)
+
+
+class RefEpLib:
+    """The reference's own EP GPU code for one NPB class (oracle/_ref/libref_ep_<class>.so)."""
+
+    def __init__(self, path):
+        lib = ctypes.CDLL(path)
+        dp = ctypes.POINTER(ctypes.c_double)
+        lib.ref_ep_m.restype = ctypes.c_int
+        lib.ref_ep_gpu.restype = ctypes.c_int
+        lib.ref_ep_gpu.argtypes = [dp, dp, F64, dp, dp]
+        self.lib = lib
+        self.m = lib.ref_ep_m()
+
+    def gpu(self):
+        sx, sy, tl, tw = (ctypes.c_double() for _ in range(4))
+        q = np.zeros(10)
+        rc = self.lib.ref_ep_gpu(ctypes.byref(sx), ctypes.byref(sy), q, ctypes.byref(tl), ctypes.byref(tw))
+        if rc != 0:
+            raise RuntimeError("ref_ep_gpu failed")
+        return dict(sx=sx.value, sy=sy.value, q=q, seconds_launch=tl.value, seconds_wall=tw.value)

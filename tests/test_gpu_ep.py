@@ -38,3 +38,20 @@ def test_ep_repeatable_and_invalid(cgb):
         with pytest.raises(cgb.CgbError) as e:
             cgb.ep_run(m)
         assert e.value.status == cgb.ERR_INVALID
+
+
+def test_reference_gpu_ep_agrees(cgb):
+    """The reference's own EP kernel (compiled from its sources into
+    oracle/_ref) on the same GPU: its sums verify, and ours agree with them."""
+    import os
+    from conftest import REF_DIR
+    from oracle_py import RefEpLib
+    path = os.path.join(REF_DIR, "libref_ep_S.so")
+    if not os.path.exists(path):
+        pytest.skip("the reference's EP library was not built (make -C oracle)")
+    ref = RefEpLib(path).gpu()
+    c = cgb.EP_CLASSES["S"]
+    assert abs(ref["sx"] - c["sx"]) / abs(c["sx"]) <= cgb.EP_VERIFY_EPSILON
+    ours = cgb.ep_run(c["m"])
+    assert abs(ours["sx"] - ref["sx"]) <= 1e-10 * abs(ref["sx"])
+    assert abs(ours["sy"] - ref["sy"]) <= 1e-10 * abs(ref["sy"])
