@@ -50,14 +50,22 @@ __device__ __forceinline__ uint64_t jump(uint64_t e)
     return r;
 }
 
-// Thread g takes pairs [g chunk, (g + 1) chunk).  part: per block sx, sy,
-// then kNQ counts (as doubles, exact below 2^53).
+// Thread g takes pairs [g chunk, (g + 1) chunk).  The pairs inside the
+// disc are compacted per warp before their deviates are formed: each lane
+// draws one pair a step, the accepted ones go to the warp's queue in shared
+// memory (ballot order), and whenever 32 are queued every lane forms one
+// deviate pair -- so no lane of a log idles on a rejected pair (about 21 %
+// of them).  part: per block sx, sy, then kNQ counts (as doubles, exact
+// below 2^53).
+constexpr int kQueue = 64;  // a warp's queue: up to 31 waiting + 32 arriving
+
 __global__ void __launch_bounds__(kThreads) k_ep(int log_chunk, double *part, unsigned *ticket, double *out)
 {
     __shared__ double ssx[kThreads], ssy[kThreads];
     __shared__ unsigned long long sq[kNQ][kThreads];
+    __shared__ double qx1[kThreads / 32][kQueue], qx2[kThreads / 32][kQueue], qt[kThreads / 32][kQueue];
     __shared__ bool last;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint64_t g = uint64_t(blockIdx.x) * kThreads + tid;
     const long long chunk = 1LL << log_chunk;
     uint64_t x = jump(2 * (g << log_chunk));  // the seed before this thread's first pair
@@ -65,6 +73,17 @@ __global__ void __launch_bounds__(kThreads) k_ep(int log_chunk, double *part, un
     unsigned q[kNQ];
 #pragma unroll
     for (int k = 0; k < kNQ; k++) q[k] = 0;
+    double *wx1 = qx1[warp], *wx2 = qx2[warp], *wt = qt[warp];
+    int queued = 0;  // the same in every lane of the warp
+    auto deviates = [&](double x1, double x2, double t) {
+        const double f = sqrt(-2.0 * log(t) / t);
+        const double t3 = x1 * f, t4 = x2 * f;
+        const int l = int(fmax(fabs(t3), fabs(t4)));
+#pragma unroll
+        for (int k = 0; k < kNQ; k++) q[k] += (l == k) ? 1u : 0u;
+        sx = sx + t3;
+        sy = sy + t4;
+    };
     for (long long i = 0; i < chunk; i++) {
         x = lcg_mul(x, kMult);
         const double u1 = double(x) * 0x1p-46;
@@ -72,16 +91,24 @@ __global__ void __launch_bounds__(kThreads) k_ep(int log_chunk, double *part, un
         const double u2 = double(x) * 0x1p-46;
         const double x1 = 2.0 * u1 - 1.0, x2 = 2.0 * u2 - 1.0;
         const double t = x1 * x1 + x2 * x2;
-        if (t <= 1.0) {
-            const double f = sqrt(-2.0 * log(t) / t);
-            const double t3 = x1 * f, t4 = x2 * f;
-            const int l = int(fmax(fabs(t3), fabs(t4)));
-#pragma unroll
-            for (int k = 0; k < kNQ; k++) q[k] += (l == k) ? 1u : 0u;
-            sx = sx + t3;
-            sy = sy + t4;
+        const bool keep = t <= 1.0;
+        const unsigned mask = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+            const int at = queued + __popc(mask & ((1u << lane) - 1u));
+            wx1[at] = x1;
+            wx2[at] = x2;
+            wt[at] = t;
+        }
+        queued += __popc(mask);
+        __syncwarp();
+        if (queued >= 32) {  // the newest 32: one per lane
+            const int at = queued - 32 + lane;
+            deviates(wx1[at], wx2[at], wt[at]);
+            queued -= 32;
+            __syncwarp();
         }
     }
+    if (lane < queued) deviates(wx1[lane], wx2[lane], wt[lane]);
     ssx[tid] = sx;
     ssy[tid] = sy;
 #pragma unroll
