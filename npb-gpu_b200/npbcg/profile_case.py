@@ -7,14 +7,15 @@
     python npb-gpu_b200/npbcg/profile_case.py --cls B --what barrier --reps 20000
     python npb-gpu_b200/npbcg/profile_case.py --cls D --what part --ranks 1 --niter 1
     python npb-gpu_b200/npbcg/profile_case.py --what mg --mg-class A --niter 4
+    python npb-gpu_b200/npbcg/profile_case.py --what ep --ep-class B
 
 `spmv` launches the standalone FP64 SpMV+dot kernel `reps` times (after one
 warm-up launch); `solve` runs one power iteration of `niter` outer steps;
 `sweep` prints SpMV timings for every lanes-per-row choice; `part` runs the
 row-partitioned solver on `ranks` device-generated row blocks, all driven
 from this process; `mg` runs the MG benchmark's timed region (niter
-V-cycles) of an MG class once after one warm-up run.  Each prints one JSON
-line.
+V-cycles) of an MG class once after one warm-up run; `ep` runs the EP
+kernel of an EP class once.  Each prints one JSON line.
 """
 import argparse
 import json
@@ -29,7 +30,9 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cls", default="B", choices=sorted(npbcg.CLASSES))
     ap.add_argument("--what", default="spmv",
-                    choices=["spmv", "solve", "sweep", "batch", "barrier", "part", "mg"])
+                    choices=["spmv", "solve", "sweep", "batch", "barrier", "part", "mg", "ep"])
+    ap.add_argument("--ep-class", default="B", choices=sorted(npbcg.EP_CLASSES),
+                    help="ep: the EP class")
     ap.add_argument("--mg-class", default="A", choices=sorted(npbcg.MG_CLASSES),
                     help="mg: the MG class")
     ap.add_argument("--ranks", type=int, default=1, help="part: row blocks")
@@ -61,6 +64,11 @@ def main():
             r = b.solve(niter=a.niter, **kw)
             print(json.dumps({"what": "batch", "nsys": a.nsys, "niter": a.niter, "mode": a.mode,
                               "device_ms": r["device_ms"], "policy": b.policy()}), flush=True)
+        return
+    if a.what == "ep":
+        r = npbcg.ep_run(npbcg.EP_CLASSES[a.ep_class]["m"])
+        print(json.dumps({"what": "ep", "class": a.ep_class, "sx": r["sx"], "sy": r["sy"],
+                          "device_ms": r["device_ms"]}), flush=True)
         return
     if a.what == "mg":
         with npbcg.Mg.for_class(a.mg_class) as g:
