@@ -48,6 +48,11 @@ class Oracle:
         lib.orc_mg_rprj3.argtypes = [ctypes.c_int, F64, ctypes.c_int, F64]
         lib.orc_mg_interp.restype = None
         lib.orc_mg_interp.argtypes = [ctypes.c_int, F64, ctypes.c_int, F64]
+        I64 = np.ctypeslib.ndpointer(np.int64, flags="C")
+        lib.orc_is_keys.restype = ctypes.c_int
+        lib.orc_is_keys.argtypes = [ctypes.c_int, ctypes.c_int, I32]
+        lib.orc_is_run.restype = ctypes.c_longlong
+        lib.orc_is_run.argtypes = [ctypes.c_char, ctypes.c_int, ctypes.c_int, I64, I64, ctypes.c_void_p]
         lib.orc_ep_run.restype = ctypes.c_int
         lib.orc_ep_run.argtypes = [ctypes.c_int, dp, dp, F64, dp]
         lib.orc_mg_norm2u3.restype = None
@@ -101,6 +106,21 @@ class Oracle:
         u = np.array(u, dtype=np.float64)
         self.lib.orc_mg_interp(mj, np.ascontiguousarray(z), mk, u)
         return u
+
+    def is_keys(self, total_log2, max_log2):
+        keys = np.zeros(1 << total_log2, np.int32)
+        self.lib.orc_is_keys(total_log2, max_log2, keys)
+        return keys
+
+    def is_run(self, cls, total_log2, max_log2, test_index, test_rank, counts=False):
+        """NPB IS (is_oracle.c): the passed count (51 verifies) and, with
+        counts, the last iteration's running sums of the key counts."""
+        c = np.zeros(1 << max_log2, np.int64) if counts else None
+        passed = self.lib.orc_is_run(cls.encode(), total_log2, max_log2,
+                                     np.ascontiguousarray(test_index, np.int64),
+                                     np.ascontiguousarray(test_rank, np.int64),
+                                     None if c is None else c.ctypes.data)
+        return (passed, c) if counts else passed
 
     def ep_run(self, m):
         """NPB EP with 2^m pairs (ep_oracle.c): {sx, sy, q, seconds}."""
