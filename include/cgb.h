@@ -501,6 +501,30 @@ int cgb_mg_apply(int device, int op, int m, int smoother, const double *in1, con
  * output may be NULL; q holds 10 doubles. */
 int cgb_ep_run(int device, int m, double *sx, double *sy, double *q, double *device_ms);
 
+/* ---- NPB IS: ranking integer keys ---------------------------------------
+ * The reference's IS (CUDA/IS/is.cu): 2^total_log2 keys below 2^max_log2,
+ * key i = (int)(2^max_log2 / 4 * (r1 + r2 + r3 + r4)) from the LCG's draws
+ * 4i+1 .. 4i+4 (seed 314159265, multiplier 5^13), generated on the device.
+ * Classes (is.cu:86-140): S 16/11, W 20/16, A 23/19, B 25/21, C 27/23,
+ * D 31/27; cls 'U' takes any sizes and skips the class's partial checks. */
+typedef struct cgb_is cgb_is;
+
+int cgb_is_create(int device, char cls, int total_log2, int max_log2, cgb_is **out);
+int cgb_is_destroy(cgb_is *s);
+
+/* main's sequence (is.cu:398-505): one untimed ranking pass, the timed ten
+ * passes (each rewrites two keys, counts the keys by value, takes the
+ * running sums and checks the class's five test ranks, is.cu:157-190), then
+ * the full check (every key placed by the last running sums, the result in
+ * order).  *passed: the checks passed -- 5 x 10 + 1 = 51 verifies (1 for
+ * cls 'U'); *device_ms: the ten passes' device time.  Repeatable: the keys
+ * a run rewrites are restored first. */
+int cgb_is_run(cgb_is *s, long long *passed, double *device_ms);
+
+/* After a run: which 0 the keys (int32, 2^total_log2), 1 per value the
+ * number of keys below it (uint32, 2^max_log2), 2 the sorted keys (int32). */
+int cgb_is_read(cgb_is *s, int which, void *out, long long count);
+
 /* Host memory that the device copies at full speed (cudaHostAlloc). */
 int cgb_host_alloc(void **ptr, long long bytes);
 int cgb_host_free(void *ptr);

@@ -212,6 +212,12 @@ _SIGNATURES = {
     "cgb_ep_run": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                   ctypes.POINTER(ctypes.c_double), _F64,
                                   ctypes.POINTER(ctypes.c_double)]),
+    "cgb_is_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_char, ctypes.c_int, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_void_p)]),
+    "cgb_is_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "cgb_is_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
+                                  ctypes.POINTER(ctypes.c_double)]),
+    "cgb_is_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong]),
     "cgb_host_alloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_longlong]),
     "cgb_host_free": (ctypes.c_int, [ctypes.c_void_p]),
     "cgb_device_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
@@ -1028,3 +1034,51 @@ def ep_run(m, device=0):
     q = np.zeros(10)
     _check(lib().cgb_ep_run(device, int(m), ctypes.byref(sx), ctypes.byref(sy), q, ctypes.byref(ms)))
     return dict(sx=sx.value, sy=sy.value, q=q, device_ms=ms.value)
+
+
+# NPB IS classes (is.cu:86-140): (TOTAL_KEYS_LOG_2, MAX_KEY_LOG_2)
+IS_CLASSES = {"S": (16, 11), "W": (20, 16), "A": (23, 19), "B": (25, 21), "C": (27, 23), "D": (31, 27)}
+IS_PASSED = 51  # 5 test keys x 10 iterations + the full check
+
+
+class IntSort:
+    """The NPB IS benchmark's keys on one GPU (cgb_is)."""
+
+    def __init__(self, cls="U", total_log2=None, max_log2=None, device=0):
+        if cls != "U":
+            total_log2, max_log2 = IS_CLASSES[cls]
+        self.cls, self.total_log2, self.max_log2 = cls, int(total_log2), int(max_log2)
+        h = ctypes.c_void_p()
+        _check(lib().cgb_is_create(device, cls.encode(), self.total_log2, self.max_log2, ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cgb_is_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def run(self):
+        """main's sequence: {passed (51 verifies), device_ms (the ten timed passes)}."""
+        p, t = ctypes.c_longlong(), ctypes.c_double()
+        _check(lib().cgb_is_run(self._h, ctypes.byref(p), ctypes.byref(t)))
+        return dict(passed=p.value, device_ms=t.value)
+
+    def read(self, which):
+        """'keys', 'below' (per value: keys below it) or 'sorted'."""
+        w = {"keys": 0, "below": 1, "sorted": 2}[which]
+        n = 1 << (self.max_log2 if w == 1 else self.total_log2)
+        out = np.zeros(n, np.uint32 if w == 1 else np.int32)
+        _check(lib().cgb_is_read(self._h, w, out.ctypes.data_as(ctypes.c_void_p), n))
+        return out
