@@ -634,6 +634,40 @@ def ep_section(npbcg, device, rank):
     return out
 
 
+IS_CLASS = "C"
+
+
+def is_section(npbcg, device, rank):
+    """NPB IS class C (2^27 keys below 2^23) on each rank's GPU, next to the
+    reference's own IS kernels on the same GPU (rank 0).  Both times cover the
+    ten timed ranking passes (is.cu:415-430); the reference's is the wall time
+    to a device synchronisation after its tenth pass."""
+    total_log2, max_log2 = npbcg.IS_CLASSES[IS_CLASS]
+    with npbcg.IntSort(IS_CLASS, device=device) as s:
+        runs = [s.run() for _ in range(4)][1:]
+    if rank != 0:
+        return None
+    ms = max(r["device_ms"] for r in runs)
+    keys = float(1 << total_log2)
+    out = {
+        "what": f"NPB IS class {IS_CLASS}: 2^{total_log2} keys below 2^{max_log2}, ten ranking passes",
+        "ms": ms, "mops": 10.0 * keys / (ms / 1e3) / 1e6,
+        "passed": min(r["passed"] for r in runs), "verified": all(r["passed"] == npbcg.IS_PASSED for r in runs),
+    }
+    ref_path = os.path.join(ROOT, "oracle", "_ref", f"libref_is_{IS_CLASS}.so")
+    if os.path.exists(ref_path):
+        from oracle_py import RefIsLib
+        ref = RefIsLib(ref_path)
+        ref.gpu()
+        rg = min((ref.gpu() for _ in range(2)), key=lambda x: x["seconds"])
+        out["reference_gpu"] = {
+            "what": "the reference's IS kernels on this GPU (is.cu rank_gpu: seven kernels a pass), "
+                    "compiled from its sources with its block sizes; wall time of the ten passes",
+            "ms": rg["seconds"] * 1e3, "passed": rg["passed"], "our_speedup": rg["seconds"] * 1e3 / ms,
+        }
+    return out
+
+
 def our_arm(args, rank, world, local_rank):
     import torch
     import npbcg
@@ -801,6 +835,9 @@ def our_arm(args, rank, world, local_rank):
         ep = ep_section(npbcg, device, rank)
         if line is not None:
             line["ep"] = ep
+        is_ = is_section(npbcg, device, rank)
+        if line is not None:
+            line["is"] = is_
     if not args.no_partitioned:
         part = row_partitioned_section(npbcg, device, rank, world, dist)
         if line is not None:
@@ -832,7 +869,7 @@ def main():
     ap.add_argument("--no-solver-modes", action="store_true",
                     help="skip the class C comparison of the solver modes")
     ap.add_argument("--no-batched", action="store_true")
-    ap.add_argument("--no-mg", action="store_true", help="skip the NPB MG and EP class C sections")
+    ap.add_argument("--no-mg", action="store_true", help="skip the NPB MG, EP and IS class C sections")
     ap.add_argument("--no-partitioned", action="store_true",
                     help="skip class D split by rows over the ranks")
     args = ap.parse_args()

@@ -8,6 +8,7 @@
     python npb-gpu_b200/npbcg/profile_case.py --cls D --what part --ranks 1 --niter 1
     python npb-gpu_b200/npbcg/profile_case.py --what mg --mg-class A --niter 4
     python npb-gpu_b200/npbcg/profile_case.py --what ep --ep-class B
+    python npb-gpu_b200/npbcg/profile_case.py --what is --is-class B
 
 `spmv` launches the standalone FP64 SpMV+dot kernel `reps` times (after one
 warm-up launch); `solve` runs one power iteration of `niter` outer steps;
@@ -15,7 +16,9 @@ warm-up launch); `solve` runs one power iteration of `niter` outer steps;
 row-partitioned solver on `ranks` device-generated row blocks, all driven
 from this process; `mg` runs the MG benchmark's timed region (niter
 V-cycles) of an MG class once after one warm-up run; `ep` runs the EP
-kernel of an EP class once.  Each prints one JSON line.
+kernel of an EP class once; `is` runs the IS benchmark (one untimed and ten
+timed ranking passes, the full check) of an IS class once.  Each prints one
+JSON line.
 """
 import argparse
 import json
@@ -30,9 +33,11 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cls", default="B", choices=sorted(npbcg.CLASSES))
     ap.add_argument("--what", default="spmv",
-                    choices=["spmv", "solve", "sweep", "batch", "barrier", "part", "mg", "ep"])
+                    choices=["spmv", "solve", "sweep", "batch", "barrier", "part", "mg", "ep", "is"])
     ap.add_argument("--ep-class", default="B", choices=sorted(npbcg.EP_CLASSES),
                     help="ep: the EP class")
+    ap.add_argument("--is-class", default="B", choices=sorted(npbcg.IS_CLASSES),
+                    help="is: the IS class")
     ap.add_argument("--mg-class", default="A", choices=sorted(npbcg.MG_CLASSES),
                     help="mg: the MG class")
     ap.add_argument("--ranks", type=int, default=1, help="part: row blocks")
@@ -68,6 +73,12 @@ def main():
     if a.what == "ep":
         r = npbcg.ep_run(npbcg.EP_CLASSES[a.ep_class]["m"])
         print(json.dumps({"what": "ep", "class": a.ep_class, "sx": r["sx"], "sy": r["sy"],
+                          "device_ms": r["device_ms"]}), flush=True)
+        return
+    if a.what == "is":
+        with npbcg.IntSort(a.is_class) as s:
+            r = s.run()
+        print(json.dumps({"what": "is", "class": a.is_class, "passed": r["passed"],
                           "device_ms": r["device_ms"]}), flush=True)
         return
     if a.what == "mg":

@@ -304,3 +304,19 @@ class RefEpLib:
         if rc != 0:
             raise RuntimeError("ref_ep_gpu failed")
         return dict(sx=sx.value, sy=sy.value, q=q, seconds_launch=tl.value, seconds_wall=tw.value)
+
+
+class RefIsLib:
+    """The reference's own IS GPU code for one NPB class (oracle/_ref/libref_is_<class>.so)."""
+
+    def __init__(self, path):
+        lib = ctypes.CDLL(path)
+        lib.ref_is_gpu.restype = ctypes.c_longlong
+        lib.ref_is_gpu.argtypes = [ctypes.POINTER(ctypes.c_double)]
+        self.lib = lib
+
+    def gpu(self):
+        """main's sequence: {passed (51 verifies), seconds (the ten timed passes, wall)}."""
+        t = ctypes.c_double()
+        passed = self.lib.ref_is_gpu(ctypes.byref(t))
+        return dict(passed=int(passed), seconds=t.value)

@@ -52,3 +52,18 @@ def test_is_custom_size_and_invalid(cgb):
         h = __import__("ctypes").c_void_p()
         cgb._check(cgb.lib().cgb_is_create(0, b"S", 20, 11, __import__("ctypes").byref(h)))
     assert e.value.status == cgb.ERR_INVALID
+
+
+def test_reference_gpu_is_agrees(cgb):
+    """The reference's own IS kernels (compiled from its sources into
+    oracle/_ref) on the same GPU pass all 51 of their checks, as ours do."""
+    import os
+    from conftest import REF_DIR
+    from oracle_py import RefIsLib
+    path = os.path.join(REF_DIR, "libref_is_S.so")
+    if not os.path.exists(path):
+        pytest.skip("the reference's IS library was not built (make -C oracle)")
+    ref = RefIsLib(path).gpu()
+    assert ref["passed"] == cgb.IS_PASSED and ref["seconds"] > 0
+    with cgb.IntSort("S") as s:
+        assert s.run()["passed"] == cgb.IS_PASSED

@@ -1,6 +1,7 @@
-"""The NPB-style MG and EP drivers `npb-gpu_b200/bin/mg` and `bin/ep`,
-drop-ins for the reference's mg.<CLASS> and ep.<CLASS> binaries
-(GMAP/NPB-GPU CUDA/MG/mg.cu main :356-623, CUDA/EP/ep.cu main :114-275).
+"""The NPB-style MG, EP and IS drivers `npb-gpu_b200/bin/mg`, `bin/ep` and
+`bin/is`, drop-ins for the reference's mg.<CLASS>, ep.<CLASS> and is.<CLASS>
+binaries (GMAP/NPB-GPU CUDA/MG/mg.cu main :356-623, CUDA/EP/ep.cu main
+:114-275, CUDA/IS/is.cu main :335-505).
 
 Its report must carry the reference's verification block (mg.cu:526-552,
 epsilon 1e-8 on the L2 norm) and its Mop/s, recomputed here from the
@@ -120,3 +121,33 @@ def test_ep_driver_report_verifies():
     assert abs(mops - expect) <= expect * (1e-6 / t + 1e-6) + 0.01
     line = json.loads(run_ep("S", "--json").stdout.strip().splitlines()[-1])
     assert line["verified"] is True and line["m"] == 24
+
+
+# ------------------------------------------------------------------ IS driver
+IS = os.path.join(ROOT, "npb-gpu_b200", "bin", "is")
+
+
+def run_is(*args, timeout=600):
+    if not os.path.exists(IS):
+        pytest.skip("npb-gpu_b200/bin/is not built")
+    return subprocess.run([IS, *args], capture_output=True, text=True, timeout=timeout)
+
+
+def test_is_driver_rejects_bad_arguments():
+    for args in ([], ["E"], ["SS"], ["S", "--what"]):
+        r = run_is(*args, timeout=60)
+        assert r.returncode == 2 and "usage: is" in r.stderr
+
+
+@pytest.mark.gpu
+def test_is_driver_report_verifies():
+    r = run_is("W")
+    assert r.returncode == 0, r.stderr
+    assert field(r.stdout, "Verification") == "SUCCESSFUL"
+    assert field(r.stdout, "Checks passed") == "51 of 51"
+    t = float(field(r.stdout, "Time in seconds"))
+    mops = float(field(r.stdout, "Mop/s total"))
+    expect = 10 * 2.0 ** 20 / t / 1e6  # is.cu:484
+    assert abs(mops - expect) <= expect * (1e-6 / t + 1e-6) + 0.01
+    line = json.loads(run_is("S", "--json").stdout.strip().splitlines()[-1])
+    assert line["verified"] is True and line["passed"] == 51 and line["keys"] == 2 ** 16
