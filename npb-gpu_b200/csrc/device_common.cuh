@@ -241,4 +241,64 @@ __device__ __forceinline__ double2 ld_stream(const double2 *p) { return __ldcs(p
 __device__ __forceinline__ int2 ld_stream(const int2 *p) { return __ldcs(p); }
 __device__ __forceinline__ float2 ld_stream(const float2 *p) { return __ldcs(p); }
 
+// ---------------------------------------------- bulk copies and mbarriers
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+                 : "memory");
+}
+
+// Orders this thread's earlier generic-proxy accesses (and those it has
+// observed) before its later async-proxy (TMA) accesses.
+__device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async;" ::: "memory");
+}
+
+// 1-D bulk copy global -> shared completing on `bar`; issued by one thread.
+// src, dst 16-byte aligned, bytes a multiple of 16.  Never multicast.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes,
+                                          uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Bounded wait for phase `parity` of `bar`; gives up after limit_ns or when
+// *abort is set by another warp of the CTA.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, long long limit_ns,
+                                          volatile int *abort)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try_wait(bar, parity)) {
+        if (abort && *abort) return false;
+        if ((long long)(global_ns() - t0) > limit_ns) return false;
+    }
+    return true;
+}
+
 }  // namespace cgb

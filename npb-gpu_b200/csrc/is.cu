@@ -25,6 +25,7 @@
 #include <new>
 
 #include "cgb_internal.h"
+#include "device_common.cuh"
 
 namespace cgb {
 namespace is {
@@ -103,12 +104,272 @@ __global__ void k_prep(int32_t *keys, int it, Params P, long long *probe)
     for (int i = 0; i < kTests; i++) probe[i] = keys[P.index[i]];
 }
 
-__global__ void __launch_bounds__(kThreads) k_hist(const int32_t *__restrict__ keys, long long n,
-                                                   unsigned *counts)
+// A ranking pass counts keys by value in three steps, all in shared memory:
+// (1) each CTA counts its run of keys by bucket (the value's high bits),
+// (2) after a scan of those counts (bucket-major, CTA-minor) each CTA copies
+// its keys into their buckets' places, (3) one CTA a bucket counts the
+// bucket's keys by value and writes their running sums, which start at the
+// keys in the buckets before.  Global atomics into a table of every value
+// would run at the L2's atomic rate; this costs two more passes over the
+// keys at HBM rate instead.
+constexpr int kWideThreads = 512;   // (1) and (2): two CTAs an SM
+constexpr int kRankThreads = 512;   // (3)
+constexpr int kUnroll = 4;          // 16-byte loads in flight a thread
+constexpr int kMinBucketLog2 = 13;  // at least 2^13 values a bucket
+constexpr int kMaxBucketsLog2 = 12; // at most 2^12 buckets
+constexpr int kCountWords = 8192;   // shared words of (1)'s private tables
+constexpr int kScatterKeys = kWideThreads * 4 * kUnroll;  // (2)'s tile: 8192 keys
+constexpr int kTileWords = kScatterKeys / 4;              // its 16-byte words
+constexpr int kBarBytes = 128;                            // (2)'s mbarriers, before the slots
+constexpr long long kWaitLimitNs = 2000000000LL;          // a bulk copy's time limit
+
+// (1) hist[b G + g] = CTA g's keys in bucket b; a warp adds into one of
+// `copies` private tables, so that few buckets do not mean many collisions.
+__global__ void __launch_bounds__(kWideThreads) k_bucket_count(const int32_t *__restrict__ keys, long long n,
+                                                               long long chunk4, int shift, int nb, int copies,
+                                                               unsigned *__restrict__ hist)
 {
-    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
-         j += (long long)gridDim.x * blockDim.x)
-        atomicAdd(&counts[keys[j]], 1u);
+    extern __shared__ unsigned tab[];
+    for (int i = threadIdx.x; i < copies * nb; i += blockDim.x) tab[i] = 0u;
+    __syncthreads();
+    unsigned *mine = tab + ((threadIdx.x >> 5) % copies) * nb;
+    const unsigned top = unsigned(nb - 1);
+    const int4 *k4 = reinterpret_cast<const int4 *>(keys);
+    const long long j0 = blockIdx.x * chunk4, j1 = min(n >> 2, j0 + chunk4), step = blockDim.x;
+    long long j = j0 + threadIdx.x;
+    for (; j + (kUnroll - 1) * step < j1; j += kUnroll * step) {
+        int4 v[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) v[u] = __ldcs(k4 + j + u * step);
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+            atomicAdd(&mine[unsigned(v[u].x >> shift) & top], 1u);
+            atomicAdd(&mine[unsigned(v[u].y >> shift) & top], 1u);
+            atomicAdd(&mine[unsigned(v[u].z >> shift) & top], 1u);
+            atomicAdd(&mine[unsigned(v[u].w >> shift) & top], 1u);
+        }
+    }
+    for (; j < j1; j += step) {
+        const int4 v = __ldcs(k4 + j);
+        atomicAdd(&mine[unsigned(v.x >> shift) & top], 1u);
+        atomicAdd(&mine[unsigned(v.y >> shift) & top], 1u);
+        atomicAdd(&mine[unsigned(v.z >> shift) & top], 1u);
+        atomicAdd(&mine[unsigned(v.w >> shift) & top], 1u);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        unsigned t = 0u;
+        for (int c = 0; c < copies; c++) t += tab[c * nb + b];
+        hist[(long long)b * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+// Exclusive scan of a[0 .. nb) in place by a block of kWideThreads (nb a
+// power of two, at most kScanPer kWideThreads); wsum: kWideThreads / 32 words.
+constexpr int kScanPer = (1 << kMaxBucketsLog2) / kWideThreads;  // values a thread, at most
+static_assert(kScanPer >= 1 && kScanPer * kWideThreads == (1 << kMaxBucketsLog2), "bucket scan split");
+
+__device__ __forceinline__ void scan_buckets(unsigned *a, int nb, unsigned *wsum)
+{
+    const int per = nb > kWideThreads ? nb / kWideThreads : 1, i0 = threadIdx.x * per;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned loc[kScanPer], sum = 0u;
+#pragma unroll
+    for (int k = 0; k < kScanPer; k++) {
+        loc[k] = (k < per && i0 + k < nb) ? a[i0 + k] : 0u;
+        sum += loc[k];
+    }
+    unsigned x = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        unsigned y = lane < kWideThreads / 32 ? wsum[lane] : 0u;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned z = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += z;
+        }
+        if (lane < kWideThreads / 32) wsum[lane] = y;
+    }
+    __syncthreads();
+    unsigned before = (w > 0 ? wsum[w - 1] : 0u) + x - sum;
+#pragma unroll
+    for (int k = 0; k < kScanPer; k++)
+        if (k < per && i0 + k < nb) {
+            a[i0 + k] = before;
+            before += loc[k];
+        }
+}
+
+// (2) incl: the inclusive scan of hist, so CTA g's keys of bucket b go to
+// the places from incl[b G + g - 1] upwards.  The CTA's run of keys arrives
+// in tiles by bulk copies (one thread issues them into a ring of `ring`
+// slots, each completing on its mbarrier), so the next tiles are on their
+// way while this one is sorted.  A tile is ordered by bucket in its own
+// slot (a counting sort: the tile's counts, their scan, each key at its
+// bucket's start plus its arrival), then written out in that order, so a
+// warp's stores are runs of one bucket's places instead of 32 scattered
+// words.  The order inside a bucket does not matter to the counts.  A copy
+// that does not complete within kWaitLimitNs sets *err and ends the CTA
+// (after a bounded wait for its other copies in flight).
+__global__ void __launch_bounds__(kWideThreads) k_bucket_scatter(const int32_t *__restrict__ keys, long long n,
+                                                                 long long chunk4, int shift, int nb, int ring,
+                                                                 const unsigned *__restrict__ incl,
+                                                                 int32_t *__restrict__ out, unsigned *err)
+{
+    extern __shared__ __align__(128) unsigned char sm[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm);                     // ring mbarriers
+    int32_t *slots = reinterpret_cast<int32_t *>(sm + kBarBytes);        // ring x kScatterKeys
+    unsigned *cur = reinterpret_cast<unsigned *>(slots + size_t(ring) * kScatterKeys);  // nb
+    unsigned *tix = cur + nb;                                            // nb
+    __shared__ unsigned wsum[kWideThreads / 32];
+    __shared__ int go;
+    const unsigned top = unsigned(nb - 1);
+    const long long j0 = blockIdx.x * chunk4, j1 = min(n >> 2, j0 + chunk4);
+    const long long ntiles = j1 > j0 ? (j1 - j0 + kTileWords - 1) / kTileWords : 0;
+    auto issue = [&](long long t) {
+        const long long a = j0 + t * kTileWords;
+        const unsigned words = unsigned(min((long long)kTileWords, j1 - a));
+        bulk_load(slots + size_t(t % ring) * kScatterKeys, keys + 4 * a, 16u * words, &bar[t % ring]);
+    };
+    if (threadIdx.x == 0) {
+        for (int r = 0; r < ring; r++) mbar_init(&bar[r], 1);
+        fence_proxy_async();
+        for (long long t = 0; t < min((long long)ring, ntiles); t++) issue(t);
+    }
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        const long long at = (long long)b * gridDim.x + blockIdx.x;
+        cur[b] = at == 0 ? 0u : incl[at - 1];
+        tix[b] = 0u;
+    }
+    __syncthreads();
+    for (long long t = 0; t < ntiles; t++) {
+        const int slot = int(t % ring);
+        if (threadIdx.x == 0) go = mbar_wait(&bar[slot], unsigned((t / ring) & 1), kWaitLimitNs, nullptr) ? 1 : 0;
+        __syncthreads();
+        if (!go) {
+            if (threadIdx.x == 0) {
+                atomicExch(err, 1u);
+                for (long long u = t; u < min(ntiles, t + ring); u++)
+                    mbar_wait(&bar[u % ring], unsigned((u / ring) & 1), kWaitLimitNs, nullptr);
+            }
+            return;
+        }
+        int32_t *tile = slots + size_t(slot) * kScatterKeys;
+        const int words = int(min((long long)kTileWords, j1 - (j0 + t * kTileWords)));
+        const int4 *t4 = reinterpret_cast<const int4 *>(tile);
+        int4 v[kUnroll];
+        unsigned off[kUnroll][4];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+            const int w = threadIdx.x + u * kWideThreads;
+            v[u] = w < words ? t4[w] : make_int4(-1, -1, -1, -1);
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+            if (v[u].x < 0) continue;  // past the end of the run: the whole 16-byte word
+            off[u][0] = atomicAdd(&tix[unsigned(v[u].x >> shift) & top], 1u);
+            off[u][1] = atomicAdd(&tix[unsigned(v[u].y >> shift) & top], 1u);
+            off[u][2] = atomicAdd(&tix[unsigned(v[u].z >> shift) & top], 1u);
+            off[u][3] = atomicAdd(&tix[unsigned(v[u].w >> shift) & top], 1u);
+        }
+        __syncthreads();  // every key of the slot is in registers: the slot becomes the staging
+        scan_buckets(tix, nb, wsum);
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+            if (v[u].x < 0) continue;
+            tile[tix[unsigned(v[u].x >> shift) & top] + off[u][0]] = v[u].x;
+            tile[tix[unsigned(v[u].y >> shift) & top] + off[u][1]] = v[u].y;
+            tile[tix[unsigned(v[u].z >> shift) & top] + off[u][2]] = v[u].z;
+            tile[tix[unsigned(v[u].w >> shift) & top] + off[u][3]] = v[u].w;
+        }
+        __syncthreads();
+        const int tile_n = 4 * words;
+        for (int p = threadIdx.x; p < tile_n; p += blockDim.x) {
+            const int32_t key = tile[p];
+            const unsigned b = unsigned(key >> shift) & top;
+            out[cur[b] + (unsigned(p) - tix[b])] = key;
+        }
+        __syncthreads();
+        for (int b = threadIdx.x; b < nb; b += blockDim.x)
+            cur[b] += (b + 1 < nb ? tix[b + 1] : unsigned(tile_n)) - tix[b];
+        __syncthreads();
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) tix[b] = 0u;
+        if (threadIdx.x == 0 && t + ring < ntiles) {
+            fence_proxy_async();  // every warp's accesses of the slot before its refill
+            issue(t + ring);
+        }
+        __syncthreads();
+    }
+}
+
+// (3) One CTA a bucket (`width` values), the fullest buckets first (from
+// the middle of the value range outwards, where the sum of four uniforms
+// puts most keys): counts by value in shared memory, then their running
+// sums from the bucket's start, each warp scanning its share of the values.
+__global__ void __launch_bounds__(kRankThreads) k_bucket_rank(const int32_t *__restrict__ bkeys,
+                                                              const unsigned *__restrict__ incl, int G, int nb,
+                                                              int width, unsigned *__restrict__ counts)
+{
+    extern __shared__ unsigned cnt[];
+    __shared__ unsigned wtot[kRankThreads / 32];
+    const int i = blockIdx.x, half = nb / 2;
+    const int b = (i & 1) ? half - 1 - (i >> 1) : half + (i >> 1);
+    const long long s = b == 0 ? 0 : incl[(long long)b * G - 1], e = incl[(long long)b * G + G - 1];
+    for (int v = threadIdx.x; v < width; v += blockDim.x) cnt[v] = 0u;
+    __syncthreads();
+    const unsigned mask = unsigned(width - 1);
+    const long long a = min(e, (s + 3) & ~3LL), e4 = e >> 2;
+    if (threadIdx.x < a - s) atomicAdd(&cnt[unsigned(bkeys[s + threadIdx.x]) & mask], 1u);
+    const int4 *k4 = reinterpret_cast<const int4 *>(bkeys);
+    const long long step = blockDim.x;
+    long long j = (a >> 2) + threadIdx.x;
+    for (; j + (kUnroll - 1) * step < e4; j += kUnroll * step) {
+        int4 v[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) v[u] = __ldcs(k4 + j + u * step);
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+            atomicAdd(&cnt[unsigned(v[u].x) & mask], 1u);
+            atomicAdd(&cnt[unsigned(v[u].y) & mask], 1u);
+            atomicAdd(&cnt[unsigned(v[u].z) & mask], 1u);
+            atomicAdd(&cnt[unsigned(v[u].w) & mask], 1u);
+        }
+    }
+    for (; j < e4; j += step) {
+        const int4 v = __ldcs(k4 + j);
+        atomicAdd(&cnt[unsigned(v.x) & mask], 1u);
+        atomicAdd(&cnt[unsigned(v.y) & mask], 1u);
+        atomicAdd(&cnt[unsigned(v.z) & mask], 1u);
+        atomicAdd(&cnt[unsigned(v.w) & mask], 1u);
+    }
+    const long long t0 = max(a, e4 << 2);
+    if (threadIdx.x < e - t0) atomicAdd(&cnt[unsigned(bkeys[t0 + threadIdx.x]) & mask], 1u);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = kRankThreads / 32;
+    const int seg = width / nw, lo = w * seg, hi = lo + seg;
+    unsigned sum = 0u;
+    for (int c = lo + lane; c < hi; c += 32) sum += cnt[c];
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) wtot[w] = sum;
+    __syncthreads();
+    unsigned carry = unsigned(s);
+    for (int k = 0; k < w; k++) carry += wtot[k];
+    unsigned *dst = counts + (long long)b * width;
+    for (int c0 = lo; c0 < hi; c0 += 32) {
+        const int c = c0 + lane;
+        unsigned x = c < hi ? cnt[c] : 0u;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (c < hi) dst[c] = carry + x;
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
 }
 
 // Inclusive scan of a block's values in shared memory (kThreads values).
@@ -243,10 +504,13 @@ struct cgb_is {
     int device = 0, sms = 148;
     Params P{};
     int32_t *keys = nullptr, *sorted = nullptr, *backup = nullptr;  // backup: keys[0 .. 2 kIters]
-    unsigned *counts = nullptr, *totals = nullptr;
+    unsigned *counts = nullptr, *totals = nullptr, *hist = nullptr;
     long long *probe = nullptr;
     unsigned long long *passed = nullptr, *bad = nullptr;
-    int tiles = 0;
+    int tiles = 0;                                      // scan tiles of hist
+    int grid = 0, shift = 0, nb = 1, width = 0, copies = 1, ring = 2;  // the bucket pass
+    unsigned *err = nullptr;                            // set by a bulk copy that timed out
+    long long chunk4 = 0;                               // 16-byte words a CTA of (1), (2)
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -268,7 +532,7 @@ void is_release(cgb_is *s)
     cudaSetDevice(s->device);
     if (s->exec) cudaGraphExecDestroy(s->exec);
     for (void *p : {(void *)s->keys, (void *)s->sorted, (void *)s->backup, (void *)s->counts,
-                    (void *)s->totals, (void *)s->probe, (void *)s->passed, (void *)s->bad})
+                    (void *)s->totals, (void *)s->hist, (void *)s->err, (void *)s->probe, (void *)s->passed, (void *)s->bad})
         if (p) cudaFree(p);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
@@ -276,16 +540,27 @@ void is_release(cgb_is *s)
     delete s;
 }
 
+size_t scatter_smem(int nb, int ring)
+{
+    return kBarBytes + sizeof(int32_t) * size_t(ring) * kScatterKeys + sizeof(unsigned) * 2 * size_t(nb);
+}
+
 // One ranking pass (rank_gpu, is.cu:725-800) at iteration it.
 void enqueue_rank(cgb_is *s, int it)
 {
     const cudaStream_t st = s->stream;
+    const int len = s->grid * s->nb;
     k_prep<<<1, 32, 0, st>>>(s->keys, it, s->P, s->probe);
-    cudaMemsetAsync(s->counts, 0, sizeof(unsigned) * size_t(s->P.maxk), st);
-    k_hist<<<8 * s->sms, kThreads, 0, st>>>(s->keys, s->P.n, s->counts);
-    k_scan_tiles<<<s->tiles, kThreads, 0, st>>>(s->counts, s->P.maxk, s->totals);
+    k_bucket_count<<<s->grid, kWideThreads, sizeof(unsigned) * s->copies * s->nb, st>>>(
+        s->keys, s->P.n, s->chunk4, s->shift, s->nb, s->copies, s->hist);
+    k_scan_tiles<<<s->tiles, kThreads, 0, st>>>(s->hist, len, s->totals);
     k_scan_totals<<<1, kThreads, 0, st>>>(s->totals, s->tiles);
-    k_scan_add<<<s->tiles, kThreads, 0, st>>>(s->counts, s->P.maxk, s->totals);
+    k_scan_add<<<s->tiles, kThreads, 0, st>>>(s->hist, len, s->totals);
+    // the buckets go to `sorted`, which the full check overwrites after the timed passes
+    k_bucket_scatter<<<s->grid, kWideThreads, scatter_smem(s->nb, s->ring), st>>>(
+        s->keys, s->P.n, s->chunk4, s->shift, s->nb, s->ring, s->hist, s->sorted, s->err);
+    k_bucket_rank<<<s->nb, kRankThreads, sizeof(unsigned) * s->width, st>>>(s->sorted, s->hist, s->grid, s->nb,
+                                                                           s->width, s->counts);
     k_check<<<1, 32, 0, st>>>(s->counts, s->probe, s->P, it, s->passed);
 }
 
@@ -325,15 +600,40 @@ int cgb_is_create(int device, char cls, int total_log2, int max_log2, cgb_is **o
     if (!s) return set_error(CGB_ERR_NOMEM, "is: allocation failed");
     s->device = device;
     s->P = P;
-    IS_TRY(cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device));
-    s->tiles = (P.maxk + kTileVals - 1) / kTileVals;
-    const bool ok = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
+    if (cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        is_release(s);
+        return set_error(CGB_ERR_CUDA, "is: device attributes");
+    }
+    // buckets of 2^shift values: at least 2^kMinBucketLog2 of them (or all
+    // values), at most 2^kMaxBucketsLog2 buckets
+    s->shift = std::min(max_log2, std::max(kMinBucketLog2, max_log2 - kMaxBucketsLog2));
+    s->nb = 1 << (max_log2 - s->shift);
+    s->width = 1 << s->shift;
+    s->copies = std::max(1, std::min(32, kCountWords / s->nb));
+    s->grid = 2 * s->sms;
+    // three tiles in flight a CTA where two CTAs an SM still fit, else two
+    int smem_sm = 0;
+    if (cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device) != cudaSuccess) {
+        is_release(s);
+        return set_error(CGB_ERR_CUDA, "is: device attributes");
+    }
+    s->ring = 2 * (scatter_smem(s->nb, 3) + 1024) <= size_t(smem_sm) ? 3 : 2;
+    s->chunk4 = ((P.n >> 2) + s->grid - 1) / s->grid;
+    s->tiles = (s->grid * s->nb + kTileVals - 1) / kTileVals;
+    const bool ok = cudaFuncSetAttribute(k_bucket_rank, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(sizeof(unsigned)) * s->width) == cudaSuccess &&
+                    cudaFuncSetAttribute(k_bucket_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(scatter_smem(s->nb, s->ring))) == cudaSuccess &&
+                    cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
                     cudaEventCreate(&s->ev0) == cudaSuccess && cudaEventCreate(&s->ev1) == cudaSuccess &&
                     cudaMalloc(&s->keys, sizeof(int32_t) * size_t(P.n)) == cudaSuccess &&
                     cudaMalloc(&s->sorted, sizeof(int32_t) * size_t(P.n)) == cudaSuccess &&
                     cudaMalloc(&s->backup, sizeof(int32_t) * (2 * kIters + 1)) == cudaSuccess &&
                     cudaMalloc(&s->counts, sizeof(unsigned) * size_t(P.maxk)) == cudaSuccess &&
                     cudaMalloc(&s->totals, sizeof(unsigned) * size_t(s->tiles)) == cudaSuccess &&
+                    cudaMalloc(&s->hist, sizeof(unsigned) * size_t(s->grid) * s->nb) == cudaSuccess &&
+                    cudaMalloc(&s->err, sizeof(unsigned)) == cudaSuccess &&
+                    cudaMemset(s->err, 0, sizeof(unsigned)) == cudaSuccess &&
                     cudaMalloc(&s->probe, sizeof(long long) * kTests) == cudaSuccess &&
                     cudaMalloc(&s->passed, sizeof(unsigned long long)) == cudaSuccess &&
                     cudaMalloc(&s->bad, sizeof(unsigned long long)) == cudaSuccess;
@@ -400,9 +700,15 @@ int cgb_is_run(cgb_is *s, long long *passed, double *device_ms)
     k_disorder<<<8 * s->sms, kThreads, 0, st>>>(s->sorted, s->P.n, s->bad);
     IS_TRY(cudaGetLastError());
     unsigned long long h_passed = 0, h_bad = 0;
+    unsigned h_err = 0;
     IS_TRY(cudaMemcpyAsync(&h_passed, s->passed, sizeof(h_passed), cudaMemcpyDeviceToHost, st));
     IS_TRY(cudaMemcpyAsync(&h_bad, s->bad, sizeof(h_bad), cudaMemcpyDeviceToHost, st));
+    IS_TRY(cudaMemcpyAsync(&h_err, s->err, sizeof(h_err), cudaMemcpyDeviceToHost, st));
     IS_TRY(cudaStreamSynchronize(st));
+    if (h_err) {
+        cudaMemset(s->err, 0, sizeof(unsigned));
+        return set_error(CGB_ERR_CUDA, "is: a bulk copy of keys did not complete in time");
+    }
     float ms = 0.f;
     IS_TRY(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     if (passed) *passed = (long long)h_passed + (h_bad == 0 ? 1 : 0);
