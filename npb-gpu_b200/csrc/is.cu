@@ -112,11 +112,23 @@ __global__ void k_prep(int32_t *keys, int it, Params P, long long *probe)
 // keys in the buckets before.  Global atomics into a table of every value
 // would run at the L2's atomic rate; this costs two more passes over the
 // keys at HBM rate instead.
-constexpr int kWideThreads = 512;   // (1) and (2): two CTAs an SM
-constexpr int kRankThreads = 512;   // (3)
+#ifndef IS_WIDE_THREADS
+#define IS_WIDE_THREADS 512
+#endif
+#ifndef IS_RING
+#define IS_RING 3
+#endif
+constexpr int kWideThreads = IS_WIDE_THREADS;  // (1) and (2)
+#ifndef IS_RANK_THREADS
+#define IS_RANK_THREADS 1024
+#endif
+constexpr int kRankThreads = IS_RANK_THREADS;  // (3)
 constexpr int kUnroll = 4;          // 16-byte loads in flight a thread
-constexpr int kMinBucketLog2 = 13;  // at least 2^13 values a bucket
-constexpr int kMaxBucketsLog2 = 12; // at most 2^12 buckets
+constexpr int kBucketsLog2 = 8;      // about 2^8 buckets: enough CTAs for (3), long runs for (2)
+constexpr int kMaxBucketLog2 = 15;   // at most 2^15 values a bucket: (3)'s table, 128 KB;
+                                     // a key's place in its bucket fits 16 bits
+constexpr int kMinBucketLog2 = 10;   // at least 2^10 values a bucket (or all of them)
+constexpr int kMaxBucketsLog2 = 27 - kMaxBucketLog2;  // so at most 2^12 buckets (values below 2^27)
 constexpr int kCountWords = 8192;   // shared words of (1)'s private tables
 constexpr int kScatterKeys = kWideThreads * 4 * kUnroll;  // (2)'s tile: 8192 keys
 constexpr int kTileWords = kScatterKeys / 4;              // its 16-byte words
@@ -125,7 +137,7 @@ constexpr long long kWaitLimitNs = 2000000000LL;          // a bulk copy's time 
 
 // (1) hist[b G + g] = CTA g's keys in bucket b; a warp adds into one of
 // `copies` private tables, so that few buckets do not mean many collisions.
-__global__ void __launch_bounds__(kWideThreads) k_bucket_count(const int32_t *__restrict__ keys, long long n,
+__global__ void __launch_bounds__(kWideThreads, 1024 / kWideThreads) k_bucket_count(const int32_t *__restrict__ keys, long long n,
                                                                long long chunk4, int shift, int nb, int copies,
                                                                unsigned *__restrict__ hist)
 {
@@ -164,19 +176,24 @@ __global__ void __launch_bounds__(kWideThreads) k_bucket_count(const int32_t *__
     }
 }
 
-// Exclusive scan of a[0 .. nb) in place by a block of kWideThreads (nb a
-// power of two, at most kScanPer kWideThreads); wsum: kWideThreads / 32 words.
-constexpr int kScanPer = (1 << kMaxBucketsLog2) / kWideThreads;  // values a thread, at most
+// A tile's bucket counts t[0 .. nb) turned, in place, into the buckets'
+// starts in the tile (exclusive scan) by a block of kWideThreads (nb a power
+// of two, at most kScanPer kWideThreads), each thread owning a run of
+// buckets; for those buckets the same thread also sets delta (the bucket's
+// place in `out` less its start in the tile), advances cur by the counts and
+// clears nxt (the next tile's counts).  wsum: kWideThreads / 32 words.
+constexpr int kScanPer = (1 << kMaxBucketsLog2) / kWideThreads;  // buckets a thread, at most
 static_assert(kScanPer >= 1 && kScanPer * kWideThreads == (1 << kMaxBucketsLog2), "bucket scan split");
 
-__device__ __forceinline__ void scan_buckets(unsigned *a, int nb, unsigned *wsum)
+__device__ __forceinline__ void scan_tile_buckets(unsigned *t, unsigned *cur, unsigned *delta, unsigned *nxt, int nb,
+                                                  unsigned *wsum)
 {
     const int per = nb > kWideThreads ? nb / kWideThreads : 1, i0 = threadIdx.x * per;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     unsigned loc[kScanPer], sum = 0u;
 #pragma unroll
     for (int k = 0; k < kScanPer; k++) {
-        loc[k] = (k < per && i0 + k < nb) ? a[i0 + k] : 0u;
+        loc[k] = (k < per && i0 + k < nb) ? t[i0 + k] : 0u;
         sum += loc[k];
     }
     unsigned x = sum;
@@ -195,12 +212,16 @@ __device__ __forceinline__ void scan_buckets(unsigned *a, int nb, unsigned *wsum
         if (lane < kWideThreads / 32) wsum[lane] = y;
     }
     __syncthreads();
-    unsigned before = (w > 0 ? wsum[w - 1] : 0u) + x - sum;
+    unsigned start = (w > 0 ? wsum[w - 1] : 0u) + x - sum;
 #pragma unroll
     for (int k = 0; k < kScanPer; k++)
         if (k < per && i0 + k < nb) {
-            a[i0 + k] = before;
-            before += loc[k];
+            const int b = i0 + k;
+            t[b] = start;
+            delta[b] = cur[b] - start;  // modulo 2^32: delta + (a place in the tile) is the place in out
+            cur[b] += loc[k];
+            nxt[b] = 0u;
+            start += loc[k];
         }
 }
 
@@ -212,24 +233,28 @@ __device__ __forceinline__ void scan_buckets(unsigned *a, int nb, unsigned *wsum
 // slot (a counting sort: the tile's counts, their scan, each key at its
 // bucket's start plus its arrival), then written out in that order, so a
 // warp's stores are runs of one bucket's places instead of 32 scattered
-// words.  The order inside a bucket does not matter to the counts.  A copy
-// that does not complete within kWaitLimitNs sets *err and ends the CTA
-// (after a bounded wait for its other copies in flight).
-__global__ void __launch_bounds__(kWideThreads) k_bucket_scatter(const int32_t *__restrict__ keys, long long n,
+// words.  The order inside a bucket does not matter to the counts.  The
+// tile counts alternate between two tables, so one tile's counting needs
+// no barrier after the previous tile's write-out.  A copy that does not
+// complete within kWaitLimitNs sets *err and ends the CTA (after a bounded
+// wait for its other copies in flight).
+__global__ void __launch_bounds__(kWideThreads, 1024 / kWideThreads) k_bucket_scatter(const int32_t *__restrict__ keys, long long n,
                                                                  long long chunk4, int shift, int nb, int ring,
                                                                  const unsigned *__restrict__ incl,
-                                                                 int32_t *__restrict__ out, unsigned *err)
+                                                                 uint16_t *__restrict__ out, unsigned *err)
 {
     extern __shared__ __align__(128) unsigned char sm[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm);                     // ring mbarriers
     int32_t *slots = reinterpret_cast<int32_t *>(sm + kBarBytes);        // ring x kScatterKeys
     unsigned *cur = reinterpret_cast<unsigned *>(slots + size_t(ring) * kScatterKeys);  // nb
-    unsigned *tix = cur + nb;                                            // nb
+    unsigned *delta = cur + nb;                                          // nb
+    unsigned *tix = delta + nb;                                          // 2 x nb
     __shared__ unsigned wsum[kWideThreads / 32];
     __shared__ int go;
     const unsigned top = unsigned(nb - 1);
     const long long j0 = blockIdx.x * chunk4, j1 = min(n >> 2, j0 + chunk4);
     const long long ntiles = j1 > j0 ? (j1 - j0 + kTileWords - 1) / kTileWords : 0;
+    long long issued = 0;  // thread 0's count of tiles whose copies were issued
     auto issue = [&](long long t) {
         const long long a = j0 + t * kTileWords;
         const unsigned words = unsigned(min((long long)kTileWords, j1 - a));
@@ -238,25 +263,31 @@ __global__ void __launch_bounds__(kWideThreads) k_bucket_scatter(const int32_t *
     if (threadIdx.x == 0) {
         for (int r = 0; r < ring; r++) mbar_init(&bar[r], 1);
         fence_proxy_async();
-        for (long long t = 0; t < min((long long)ring, ntiles); t++) issue(t);
+        for (; issued < min((long long)ring, ntiles); issued++) issue(issued);
     }
     for (int b = threadIdx.x; b < nb; b += blockDim.x) {
         const long long at = (long long)b * gridDim.x + blockIdx.x;
         cur[b] = at == 0 ? 0u : incl[at - 1];
         tix[b] = 0u;
+        tix[nb + b] = 0u;
     }
     __syncthreads();
     for (long long t = 0; t < ntiles; t++) {
         const int slot = int(t % ring);
+        unsigned *tc = tix + (t & 1) * nb, *tn = tix + ((t + 1) & 1) * nb;
         if (threadIdx.x == 0) go = mbar_wait(&bar[slot], unsigned((t / ring) & 1), kWaitLimitNs, nullptr) ? 1 : 0;
-        __syncthreads();
+        __syncthreads();  // also: every thread is past the previous tile's write-out
         if (!go) {
             if (threadIdx.x == 0) {
                 atomicExch(err, 1u);
-                for (long long u = t; u < min(ntiles, t + ring); u++)
+                for (long long u = t; u < issued; u++)
                     mbar_wait(&bar[u % ring], unsigned((u / ring) & 1), kWaitLimitNs, nullptr);
             }
             return;
+        }
+        if (threadIdx.x == 0 && t > 0 && issued < ntiles) {
+            fence_proxy_async();  // every warp's accesses of the previous tile's slot before its refill
+            issue(issued++);
         }
         int32_t *tile = slots + size_t(slot) * kScatterKeys;
         const int words = int(min((long long)kTileWords, j1 - (j0 + t * kTileWords)));
@@ -271,39 +302,28 @@ __global__ void __launch_bounds__(kWideThreads) k_bucket_scatter(const int32_t *
 #pragma unroll
         for (int u = 0; u < kUnroll; u++) {
             if (v[u].x < 0) continue;  // past the end of the run: the whole 16-byte word
-            off[u][0] = atomicAdd(&tix[unsigned(v[u].x >> shift) & top], 1u);
-            off[u][1] = atomicAdd(&tix[unsigned(v[u].y >> shift) & top], 1u);
-            off[u][2] = atomicAdd(&tix[unsigned(v[u].z >> shift) & top], 1u);
-            off[u][3] = atomicAdd(&tix[unsigned(v[u].w >> shift) & top], 1u);
+            off[u][0] = atomicAdd(&tc[unsigned(v[u].x >> shift) & top], 1u);
+            off[u][1] = atomicAdd(&tc[unsigned(v[u].y >> shift) & top], 1u);
+            off[u][2] = atomicAdd(&tc[unsigned(v[u].z >> shift) & top], 1u);
+            off[u][3] = atomicAdd(&tc[unsigned(v[u].w >> shift) & top], 1u);
         }
         __syncthreads();  // every key of the slot is in registers: the slot becomes the staging
-        scan_buckets(tix, nb, wsum);
+        scan_tile_buckets(tc, cur, delta, tn, nb, wsum);
         __syncthreads();
 #pragma unroll
         for (int u = 0; u < kUnroll; u++) {
             if (v[u].x < 0) continue;
-            tile[tix[unsigned(v[u].x >> shift) & top] + off[u][0]] = v[u].x;
-            tile[tix[unsigned(v[u].y >> shift) & top] + off[u][1]] = v[u].y;
-            tile[tix[unsigned(v[u].z >> shift) & top] + off[u][2]] = v[u].z;
-            tile[tix[unsigned(v[u].w >> shift) & top] + off[u][3]] = v[u].w;
+            tile[tc[unsigned(v[u].x >> shift) & top] + off[u][0]] = v[u].x;
+            tile[tc[unsigned(v[u].y >> shift) & top] + off[u][1]] = v[u].y;
+            tile[tc[unsigned(v[u].z >> shift) & top] + off[u][2]] = v[u].z;
+            tile[tc[unsigned(v[u].w >> shift) & top] + off[u][3]] = v[u].w;
         }
         __syncthreads();
         const int tile_n = 4 * words;
         for (int p = threadIdx.x; p < tile_n; p += blockDim.x) {
             const int32_t key = tile[p];
-            const unsigned b = unsigned(key >> shift) & top;
-            out[cur[b] + (unsigned(p) - tix[b])] = key;
+            out[delta[unsigned(key >> shift) & top] + unsigned(p)] = uint16_t(key);  // the bucket's low bits
         }
-        __syncthreads();
-        for (int b = threadIdx.x; b < nb; b += blockDim.x)
-            cur[b] += (b + 1 < nb ? tix[b + 1] : unsigned(tile_n)) - tix[b];
-        __syncthreads();
-        for (int b = threadIdx.x; b < nb; b += blockDim.x) tix[b] = 0u;
-        if (threadIdx.x == 0 && t + ring < ntiles) {
-            fence_proxy_async();  // every warp's accesses of the slot before its refill
-            issue(t + ring);
-        }
-        __syncthreads();
     }
 }
 
@@ -311,7 +331,7 @@ __global__ void __launch_bounds__(kWideThreads) k_bucket_scatter(const int32_t *
 // the middle of the value range outwards, where the sum of four uniforms
 // puts most keys): counts by value in shared memory, then their running
 // sums from the bucket's start, each warp scanning its share of the values.
-__global__ void __launch_bounds__(kRankThreads) k_bucket_rank(const int32_t *__restrict__ bkeys,
+__global__ void __launch_bounds__(kRankThreads) k_bucket_rank(const uint16_t *__restrict__ bkeys,
                                                               const unsigned *__restrict__ incl, int G, int nb,
                                                               int width, unsigned *__restrict__ counts)
 {
@@ -323,31 +343,37 @@ __global__ void __launch_bounds__(kRankThreads) k_bucket_rank(const int32_t *__r
     for (int v = threadIdx.x; v < width; v += blockDim.x) cnt[v] = 0u;
     __syncthreads();
     const unsigned mask = unsigned(width - 1);
-    const long long a = min(e, (s + 3) & ~3LL), e4 = e >> 2;
+    auto add2 = [&](unsigned pair) {  // two 16-bit keys
+        atomicAdd(&cnt[pair & 0xffffu & mask], 1u);
+        atomicAdd(&cnt[(pair >> 16) & mask], 1u);
+    };
+    // the keys before the first 16-byte boundary, the 16-byte words (8 keys
+    // each), the keys after the last boundary
+    const long long a = min(e, (s + 7) & ~7LL), e8 = e >> 3;
     if (threadIdx.x < a - s) atomicAdd(&cnt[unsigned(bkeys[s + threadIdx.x]) & mask], 1u);
-    const int4 *k4 = reinterpret_cast<const int4 *>(bkeys);
+    const uint4 *k8 = reinterpret_cast<const uint4 *>(bkeys);
     const long long step = blockDim.x;
-    long long j = (a >> 2) + threadIdx.x;
-    for (; j + (kUnroll - 1) * step < e4; j += kUnroll * step) {
-        int4 v[kUnroll];
+    long long j = (a >> 3) + threadIdx.x;
+    for (; j + (kUnroll - 1) * step < e8; j += kUnroll * step) {
+        uint4 v[kUnroll];
 #pragma unroll
-        for (int u = 0; u < kUnroll; u++) v[u] = __ldcs(k4 + j + u * step);
+        for (int u = 0; u < kUnroll; u++) v[u] = __ldcs(k8 + j + u * step);
 #pragma unroll
         for (int u = 0; u < kUnroll; u++) {
-            atomicAdd(&cnt[unsigned(v[u].x) & mask], 1u);
-            atomicAdd(&cnt[unsigned(v[u].y) & mask], 1u);
-            atomicAdd(&cnt[unsigned(v[u].z) & mask], 1u);
-            atomicAdd(&cnt[unsigned(v[u].w) & mask], 1u);
+            add2(v[u].x);
+            add2(v[u].y);
+            add2(v[u].z);
+            add2(v[u].w);
         }
     }
-    for (; j < e4; j += step) {
-        const int4 v = __ldcs(k4 + j);
-        atomicAdd(&cnt[unsigned(v.x) & mask], 1u);
-        atomicAdd(&cnt[unsigned(v.y) & mask], 1u);
-        atomicAdd(&cnt[unsigned(v.z) & mask], 1u);
-        atomicAdd(&cnt[unsigned(v.w) & mask], 1u);
+    for (; j < e8; j += step) {
+        const uint4 v = __ldcs(k8 + j);
+        add2(v.x);
+        add2(v.y);
+        add2(v.z);
+        add2(v.w);
     }
-    const long long t0 = max(a, e4 << 2);
+    const long long t0 = max(a, e8 << 3);
     if (threadIdx.x < e - t0) atomicAdd(&cnt[unsigned(bkeys[t0 + threadIdx.x]) & mask], 1u);
     __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = kRankThreads / 32;
@@ -542,7 +568,7 @@ void is_release(cgb_is *s)
 
 size_t scatter_smem(int nb, int ring)
 {
-    return kBarBytes + sizeof(int32_t) * size_t(ring) * kScatterKeys + sizeof(unsigned) * 2 * size_t(nb);
+    return kBarBytes + sizeof(int32_t) * size_t(ring) * kScatterKeys + sizeof(unsigned) * 4 * size_t(nb);
 }
 
 // One ranking pass (rank_gpu, is.cu:725-800) at iteration it.
@@ -556,10 +582,12 @@ void enqueue_rank(cgb_is *s, int it)
     k_scan_tiles<<<s->tiles, kThreads, 0, st>>>(s->hist, len, s->totals);
     k_scan_totals<<<1, kThreads, 0, st>>>(s->totals, s->tiles);
     k_scan_add<<<s->tiles, kThreads, 0, st>>>(s->hist, len, s->totals);
-    // the buckets go to `sorted`, which the full check overwrites after the timed passes
+    // the buckets (each key's low 16 bits: a bucket is at most 2^15 values)
+    // go to `sorted`, which the full check overwrites after the timed passes
     k_bucket_scatter<<<s->grid, kWideThreads, scatter_smem(s->nb, s->ring), st>>>(
-        s->keys, s->P.n, s->chunk4, s->shift, s->nb, s->ring, s->hist, s->sorted, s->err);
-    k_bucket_rank<<<s->nb, kRankThreads, sizeof(unsigned) * s->width, st>>>(s->sorted, s->hist, s->grid, s->nb,
+        s->keys, s->P.n, s->chunk4, s->shift, s->nb, s->ring, s->hist, reinterpret_cast<uint16_t *>(s->sorted), s->err);
+    k_bucket_rank<<<s->nb, kRankThreads, sizeof(unsigned) * s->width, st>>>(
+        reinterpret_cast<const uint16_t *>(s->sorted), s->hist, s->grid, s->nb,
                                                                            s->width, s->counts);
     k_check<<<1, 32, 0, st>>>(s->counts, s->probe, s->P, it, s->passed);
 }
@@ -604,27 +632,37 @@ int cgb_is_create(int device, char cls, int total_log2, int max_log2, cgb_is **o
         is_release(s);
         return set_error(CGB_ERR_CUDA, "is: device attributes");
     }
-    // buckets of 2^shift values: at least 2^kMinBucketLog2 of them (or all
-    // values), at most 2^kMaxBucketsLog2 buckets
-    s->shift = std::min(max_log2, std::max(kMinBucketLog2, max_log2 - kMaxBucketsLog2));
+    // buckets of 2^shift values: about 2^kBucketsLog2 of them, but
+    // 2^kMinBucketLog2 .. 2^kMaxBucketLog2 values each (or all values)
+    s->shift = std::min(kMaxBucketLog2, std::max(max_log2 - kBucketsLog2, std::min(max_log2, kMinBucketLog2)));
     s->nb = 1 << (max_log2 - s->shift);
     s->width = 1 << s->shift;
     s->copies = std::max(1, std::min(32, kCountWords / s->nb));
-    s->grid = 2 * s->sms;
-    // three tiles in flight a CTA where two CTAs an SM still fit, else two
-    int smem_sm = 0;
-    if (cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device) != cudaSuccess) {
+    // the scatter's CTAs an SM with a ring of IS_RING slots, or of two if
+    // that fits more of them; (1) and (2) run on the same grid
+    int per_sm[2] = {0, 0};
+    const int rings[2] = {IS_RING, 2};
+    if (cudaFuncSetAttribute(k_bucket_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(scatter_smem(s->nb, std::max(IS_RING, 2)))) != cudaSuccess ||
+        cudaFuncSetAttribute(k_bucket_rank, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(sizeof(unsigned)) * s->width) != cudaSuccess) {
         is_release(s);
-        return set_error(CGB_ERR_CUDA, "is: device attributes");
+        return set_error(CGB_ERR_CUDA, "is: kernel attributes");
     }
-    s->ring = 2 * (scatter_smem(s->nb, 3) + 1024) <= size_t(smem_sm) ? 3 : 2;
+    for (int k = 0; k < 2; k++)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[k], k_bucket_scatter, kWideThreads,
+                                                          scatter_smem(s->nb, rings[k])) != cudaSuccess)
+            per_sm[k] = 0;
+    const int pick = per_sm[0] >= per_sm[1] ? 0 : 1;
+    if (per_sm[pick] < 1) {
+        is_release(s);
+        return set_error(CGB_ERR_CUDA, "is: the bucket scatter does not fit an SM");
+    }
+    s->ring = rings[pick];
+    s->grid = per_sm[pick] * s->sms;
     s->chunk4 = ((P.n >> 2) + s->grid - 1) / s->grid;
     s->tiles = (s->grid * s->nb + kTileVals - 1) / kTileVals;
-    const bool ok = cudaFuncSetAttribute(k_bucket_rank, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(sizeof(unsigned)) * s->width) == cudaSuccess &&
-                    cudaFuncSetAttribute(k_bucket_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(scatter_smem(s->nb, s->ring))) == cudaSuccess &&
-                    cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
+    const bool ok = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
                     cudaEventCreate(&s->ev0) == cudaSuccess && cudaEventCreate(&s->ev1) == cudaSuccess &&
                     cudaMalloc(&s->keys, sizeof(int32_t) * size_t(P.n)) == cudaSuccess &&
                     cudaMalloc(&s->sorted, sizeof(int32_t) * size_t(P.n)) == cudaSuccess &&
