@@ -112,28 +112,36 @@ __global__ void k_prep(int32_t *keys, int it, Params P, long long *probe)
 // keys in the buckets before.  Global atomics into a table of every value
 // would run at the L2's atomic rate; this costs two more passes over the
 // keys at HBM rate instead.
+// Compile-time shapes of the bucket pass (-D to override).
 #ifndef IS_WIDE_THREADS
-#define IS_WIDE_THREADS 512
+#define IS_WIDE_THREADS 1024  // (1) and (2): threads a CTA
 #endif
 #ifndef IS_RING
-#define IS_RING 3
+#define IS_RING 3  // (2): tiles in flight a CTA (two where three do not fit)
 #endif
-constexpr int kWideThreads = IS_WIDE_THREADS;  // (1) and (2)
 #ifndef IS_RANK_THREADS
-#define IS_RANK_THREADS 1024
+#define IS_RANK_THREADS 1024  // (3): threads a CTA
 #endif
-constexpr int kRankThreads = IS_RANK_THREADS;  // (3)
-constexpr int kUnroll = 4;          // 16-byte loads in flight a thread
+#ifndef IS_SCATTER_UNROLL
+#define IS_SCATTER_UNROLL 4  // (2): 16-byte words a thread a tile
+#endif
+#ifndef IS_SCATTER_MIN_CTAS
+#define IS_SCATTER_MIN_CTAS (1024 / IS_WIDE_THREADS)
+#endif
+constexpr int kWideThreads = IS_WIDE_THREADS;
+constexpr int kRankThreads = IS_RANK_THREADS;
+constexpr int kUnroll = 4;           // (1), (3): 16-byte loads in flight a thread
 constexpr int kBucketsLog2 = 8;      // about 2^8 buckets: enough CTAs for (3), long runs for (2)
 constexpr int kMaxBucketLog2 = 15;   // at most 2^15 values a bucket: (3)'s table, 128 KB;
                                      // a key's place in its bucket fits 16 bits
 constexpr int kMinBucketLog2 = 10;   // at least 2^10 values a bucket (or all of them)
 constexpr int kMaxBucketsLog2 = 27 - kMaxBucketLog2;  // so at most 2^12 buckets (values below 2^27)
-constexpr int kCountWords = 8192;   // shared words of (1)'s private tables
-constexpr int kScatterKeys = kWideThreads * 4 * kUnroll;  // (2)'s tile: 8192 keys
-constexpr int kTileWords = kScatterKeys / 4;              // its 16-byte words
-constexpr int kBarBytes = 128;                            // (2)'s mbarriers, before the slots
-constexpr long long kWaitLimitNs = 2000000000LL;          // a bulk copy's time limit
+constexpr int kCountWords = 8192;    // shared words of (1)'s private tables
+constexpr int kScatterUnroll = IS_SCATTER_UNROLL;
+constexpr int kScatterKeys = kWideThreads * 4 * kScatterUnroll;  // (2)'s tile: 16384 keys
+constexpr int kTileWords = kScatterKeys / 4;                     // its 16-byte words
+constexpr int kBarBytes = 128;                                   // (2)'s mbarriers, before the slots
+constexpr long long kWaitLimitNs = 2000000000LL;                 // a bulk copy's time limit
 
 // (1) hist[b G + g] = CTA g's keys in bucket b; a warp adds into one of
 // `copies` private tables, so that few buckets do not mean many collisions.
@@ -238,7 +246,7 @@ __device__ __forceinline__ void scan_tile_buckets(unsigned *t, unsigned *cur, un
 // no barrier after the previous tile's write-out.  A copy that does not
 // complete within kWaitLimitNs sets *err and ends the CTA (after a bounded
 // wait for its other copies in flight).
-__global__ void __launch_bounds__(kWideThreads, 1024 / kWideThreads) k_bucket_scatter(const int32_t *__restrict__ keys, long long n,
+__global__ void __launch_bounds__(kWideThreads, IS_SCATTER_MIN_CTAS) k_bucket_scatter(const int32_t *__restrict__ keys, long long n,
                                                                  long long chunk4, int shift, int nb, int ring,
                                                                  const unsigned *__restrict__ incl,
                                                                  uint16_t *__restrict__ out, unsigned *err)
@@ -292,15 +300,15 @@ __global__ void __launch_bounds__(kWideThreads, 1024 / kWideThreads) k_bucket_sc
         int32_t *tile = slots + size_t(slot) * kScatterKeys;
         const int words = int(min((long long)kTileWords, j1 - (j0 + t * kTileWords)));
         const int4 *t4 = reinterpret_cast<const int4 *>(tile);
-        int4 v[kUnroll];
-        unsigned off[kUnroll][4];
+        int4 v[kScatterUnroll];
+        unsigned off[kScatterUnroll][4];
 #pragma unroll
-        for (int u = 0; u < kUnroll; u++) {
+        for (int u = 0; u < kScatterUnroll; u++) {
             const int w = threadIdx.x + u * kWideThreads;
             v[u] = w < words ? t4[w] : make_int4(-1, -1, -1, -1);
         }
 #pragma unroll
-        for (int u = 0; u < kUnroll; u++) {
+        for (int u = 0; u < kScatterUnroll; u++) {
             if (v[u].x < 0) continue;  // past the end of the run: the whole 16-byte word
             off[u][0] = atomicAdd(&tc[unsigned(v[u].x >> shift) & top], 1u);
             off[u][1] = atomicAdd(&tc[unsigned(v[u].y >> shift) & top], 1u);
@@ -311,7 +319,7 @@ __global__ void __launch_bounds__(kWideThreads, 1024 / kWideThreads) k_bucket_sc
         scan_tile_buckets(tc, cur, delta, tn, nb, wsum);
         __syncthreads();
 #pragma unroll
-        for (int u = 0; u < kUnroll; u++) {
+        for (int u = 0; u < kScatterUnroll; u++) {
             if (v[u].x < 0) continue;
             tile[tc[unsigned(v[u].x >> shift) & top] + off[u][0]] = v[u].x;
             tile[tc[unsigned(v[u].y >> shift) & top] + off[u][1]] = v[u].y;
@@ -639,22 +647,31 @@ int cgb_is_create(int device, char cls, int total_log2, int max_log2, cgb_is **o
     s->width = 1 << s->shift;
     s->copies = std::max(1, std::min(32, kCountWords / s->nb));
     // the scatter's CTAs an SM with a ring of IS_RING slots, or of two if
-    // that fits more of them; (1) and (2) run on the same grid
-    int per_sm[2] = {0, 0};
-    const int rings[2] = {IS_RING, 2};
-    if (cudaFuncSetAttribute(k_bucket_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(scatter_smem(s->nb, std::max(IS_RING, 2)))) != cudaSuccess ||
+    // that fits more of them (or is all that fits); (1) and (2) run on the
+    // same grid
+    int optin = 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess ||
         cudaFuncSetAttribute(k_bucket_rank, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(sizeof(unsigned)) * s->width) != cudaSuccess) {
         is_release(s);
         return set_error(CGB_ERR_CUDA, "is: kernel attributes");
     }
-    for (int k = 0; k < 2; k++)
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[k], k_bucket_scatter, kWideThreads,
-                                                          scatter_smem(s->nb, rings[k])) != cudaSuccess)
+    int per_sm[2] = {0, 0};
+    const int rings[2] = {IS_RING, 2};
+    for (int k = 0; k < 2; k++) {
+        const size_t bytes = scatter_smem(s->nb, rings[k]);
+        if (bytes > size_t(optin) ||
+            cudaFuncSetAttribute(k_bucket_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)) !=
+                cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[k], k_bucket_scatter, kWideThreads, bytes) !=
+                cudaSuccess)
             per_sm[k] = 0;
+    }
+    cudaGetLastError();  // a ring that did not fit is no error
     const int pick = per_sm[0] >= per_sm[1] ? 0 : 1;
-    if (per_sm[pick] < 1) {
+    if (per_sm[pick] < 1 ||
+        cudaFuncSetAttribute(k_bucket_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(scatter_smem(s->nb, rings[pick]))) != cudaSuccess) {
         is_release(s);
         return set_error(CGB_ERR_CUDA, "is: the bucket scatter does not fit an SM");
     }
