@@ -668,6 +668,47 @@ def is_section(npbcg, device, rank):
     return out
 
 
+FT_CLASS = "C"
+
+
+def ft_section(npbcg, device, rank):
+    """NPB FT class C (512^3, 20 iterations) on each rank's GPU, next to the
+    reference's own FT kernels on the same GPU (rank 0).  Both times cover
+    main's timed region (ft.cu:391-412); the reference's is its wall time to
+    the checksums on the host."""
+    nx, ny, nz, niter = npbcg.FT_CLASSES[FT_CLASS]
+    with npbcg.Ft(nx, ny, nz, device=device) as f:
+        runs = [f.run(niter) for _ in range(4)][1:]
+    if rank != 0:
+        return None
+    ms = max(r["device_ms"] for r in runs)
+    nt = float(nx * ny * nz)
+    # ft.cu:418-421
+    mflops = 1.0e-6 * nt * (14.8157 + 7.19641 * np.log(nt) + (5.23518 + 7.21113 * np.log(nt)) * niter) / (ms / 1e3)
+    # per iteration: evolve + z (u0 read, u0 and u1 written), y and x (read + write): 112 B a point
+    algorithmic = nt * (16 * 3 + 4 * 16 + niter * 112)
+    out = {
+        "what": f"NPB FT class {FT_CLASS}: {nx}x{ny}x{nz}, {niter} iterations (one shared-memory "
+                "Stockham pass an axis, evolve fused into the z pass), FP64",
+        "ms": ms, "mflops": mflops,
+        "max_rel_err": max(npbcg.ft_verify(FT_CLASS, r["sums"]) for r in runs),
+        "verified": all(npbcg.ft_verify(FT_CLASS, r["sums"]) <= npbcg.FT_VERIFY_EPSILON for r in runs),
+        "algorithmic_bytes": algorithmic, "achieved_gbs": algorithmic / (ms / 1e3) / 1e9,
+    }
+    ref_path = os.path.join(ROOT, "oracle", "_ref", f"libref_ft_{FT_CLASS}.so")
+    if os.path.exists(ref_path):
+        from oracle_py import RefFtLib
+        ref = RefFtLib(ref_path)
+        rg = ref.gpu()
+        out["reference_gpu"] = {
+            "what": "the reference's timed FT region on this GPU (ft.cu:391-412: radix-2 Stockham "
+                    "stages in global memory), compiled from its sources with its block sizes",
+            "ms": rg["seconds"] * 1e3, "our_speedup": rg["seconds"] * 1e3 / ms,
+            "max_rel_err": npbcg.ft_verify(FT_CLASS, rg["sums"]),
+        }
+    return out
+
+
 def our_arm(args, rank, world, local_rank):
     import torch
     import npbcg
@@ -838,6 +879,9 @@ def our_arm(args, rank, world, local_rank):
         is_ = is_section(npbcg, device, rank)
         if line is not None:
             line["is"] = is_
+        ft = ft_section(npbcg, device, rank)
+        if line is not None:
+            line["ft"] = ft
     if not args.no_partitioned:
         part = row_partitioned_section(npbcg, device, rank, world, dist)
         if line is not None:
@@ -869,7 +913,7 @@ def main():
     ap.add_argument("--no-solver-modes", action="store_true",
                     help="skip the class C comparison of the solver modes")
     ap.add_argument("--no-batched", action="store_true")
-    ap.add_argument("--no-mg", action="store_true", help="skip the NPB MG, EP and IS class C sections")
+    ap.add_argument("--no-mg", action="store_true", help="skip the NPB MG, EP, IS and FT class C sections")
     ap.add_argument("--no-partitioned", action="store_true",
                     help="skip class D split by rows over the ranks")
     args = ap.parse_args()

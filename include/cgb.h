@@ -525,6 +525,35 @@ int cgb_is_run(cgb_is *s, long long *passed, double *device_ms);
  * number of keys below it (uint32, 2^max_log2), 2 the sorted keys (int32). */
 int cgb_is_read(cgb_is *s, int which, void *out, long long count);
 
+/* ---- NPB FT: a 3-D FFT evolution ---------------------------------------
+ * The reference's FT (CUDA/FT/ft.cu): an nx x ny x nz complex field (x
+ * fastest, interleaved real and imaginary doubles) from the LCG's stream
+ * (element e: draws 2e+1, 2e+2 after the seed 314159265), transformed
+ * forward once, then each iteration multiplied by exp(-4 alpha pi^2 |k|^2)
+ * (alpha 1e-6), transformed back and checksummed.  Dimensions: powers of
+ * two in [32, 2048].  Classes (setparams.cpp:797-803): S 64^3 (6
+ * iterations), W 128x128x32 (6), A 256x256x128 (6), B 512x256x256 (20),
+ * C 512^3 (20), D 2048x1024x1024 (25). */
+typedef struct cgb_ft cgb_ft;
+
+/* Replaces main's setup_gpu (ft.cu:1469-1636): the device arrays. */
+int cgb_ft_create(int device, int nx, int ny, int nz, cgb_ft **out);
+int cgb_ft_destroy(cgb_ft *f);
+
+/* main's timed region (ft.cu:391-408): the index map, the initial
+ * conditions, the roots, the forward transform (x, y, z lines, exponent
+ * sign +1), then niter x (evolve, the inverse transform: z, y, x lines,
+ * sign -1, and the checksum of ft.cu:1124-1153).  sums: 2 niter doubles
+ * (real, imaginary of each iteration's checksum), verified by a class at
+ * relative 1e-12 (ft.cu:1638-1830); device_ms: the region's device time.
+ * niter in [1, 64]; either output may be NULL. */
+int cgb_ft_run(cgb_ft *f, int niter, double *sums, double *device_ms);
+
+/* After a run: which 0 u0 (the evolved field in Fourier space), 1 u1 (the
+ * last inverse transform), 2 the twiddle factors (nx ny nz doubles);
+ * count: doubles available at out (2 nx ny nz for u0 and u1). */
+int cgb_ft_read(cgb_ft *f, int which, double *out, long long count);
+
 /* Host memory that the device copies at full speed (cudaHostAlloc). */
 int cgb_host_alloc(void **ptr, long long bytes);
 int cgb_host_free(void *ptr);

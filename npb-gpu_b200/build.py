@@ -18,7 +18,7 @@ LIBDIR = os.path.join(HERE, "lib")
 BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["session.cu", "noalloc.cu", "gnn.cu", "batch.cu", "makea_gpu.cu", "part.cu", "mg.cu",
-              "ep.cu", "is.cu"]
+              "ep.cu", "is.cu", "ft.cu"]
 # per-source flags: MG's operators and EP's deviates keep the reference's
 # separate roundings
 EXTRA_FLAGS = {"mg.cu": ["-fmad=false"], "ep.cu": ["-fmad=false"]}

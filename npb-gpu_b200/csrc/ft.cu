@@ -1,0 +1,581 @@
+// ft.cu -- the NPB FT benchmark on the GPU: a 3-D complex field evolved in
+// Fourier space and transformed back every iteration (GMAP/NPB-GPU
+// CUDA/FT/ft.cu: main :335-420, fft :1258-1278, evolve :1245-1256,
+// checksum :1124-1153, initial conditions :1188-1227, index map :1166-1186).
+//
+// Layout: u0, u1 as double2 (real, imaginary), x fastest, as the reference.
+// A transform along one axis is one kernel: a CTA stages a tile of L lines
+// of that axis in shared memory (rows of L consecutive x values for the y
+// and z axes, so every row is one coalesced run; L whole x lines for the x
+// axis), transforms every line there by radix-8 Stockham stages (a 4 or a 2
+// last), each stage's butterflies in registers between two barriers, and
+// writes the tile back.  So each axis costs one read and one write of the
+// field.  The inverse transform's first axis (z) also does evolve: it reads
+// u0, multiplies each point by its twiddle factor (looked up by the point's
+// squared frequency in a table that stays in L2), writes the evolved u0
+// back and transforms that; the checksum reads its 1024 points in a fixed
+// order.
+//
+// Transform sign: sign +1 is sum x_j exp(+2 pi i jk / n), the reference's
+// is = 1 (its forward transform); sign -1 its is = -1.  Results agree with
+// the reference's radix-2 Stockham to rounding (the checksums verify at the
+// reference's 1e-12; parity tests hold the fields to the oracle).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <new>
+
+#include "cgb_internal.h"
+
+namespace cgb {
+namespace ft {
+
+constexpr uint64_t kMask46 = (uint64_t(1) << 46) - 1;
+constexpr uint64_t kMult = 1220703125ull;  // A = 5^13 (ft.cu:129)
+constexpr uint64_t kSeed = 314159265ull;   // SEED (ft.cu:128)
+constexpr double kAlpha = 1.0e-6;          // ALPHA (ft.cu:131)
+constexpr double kPi = 3.141592653589793238;
+constexpr double kAp = -4.0 * kAlpha * kPi * kPi;  // AP (ft.cu:132), the same order of operations
+constexpr int kPoints = 1024;                     // CHECKSUM_TASKS
+constexpr int kInitPer = 16;                      // elements a thread of the initial conditions
+constexpr int kMaxIter = 64;
+constexpr double kRoot2Half = 0.70710678118654752440;
+
+__device__ __forceinline__ uint64_t lcg_mul(uint64_t a, uint64_t b) { return (a * b) & kMask46; }
+
+// kSeed * kMult^e mod 2^46
+__device__ __forceinline__ uint64_t jump(uint64_t e)
+{
+    uint64_t r = kSeed, b = kMult;
+    while (e) {
+        if (e & 1) r = lcg_mul(r, b);
+        b = lcg_mul(b, b);
+        e >>= 1;
+    }
+    return r;
+}
+
+// Element e holds draws 2e+1 and 2e+2 after the seed (the planes' seeds of
+// ft.cu:1188-1213 and their rows' vranlc runs are one stream in that order).
+__global__ void k_initial(double2 *u, long long nt)
+{
+    const long long e0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) * kInitPer;
+    if (e0 >= nt) return;
+    uint64_t x = jump(2 * uint64_t(e0));
+    const long long e1 = min(nt, e0 + kInitPer);
+    for (long long e = e0; e < e1; e++) {
+        x = lcg_mul(x, kMult);
+        const double re = double(x) * 0x1p-46;
+        x = lcg_mul(x, kMult);
+        u[e] = make_double2(re, double(x) * 0x1p-46);
+    }
+}
+
+// The index map's integer argument (ft.cu:1166-1186): the squared signed
+// frequencies, i'^2 + (j'^2 + k'^2), summed in the reference's order.
+__device__ __forceinline__ int k2_of(int i, int j, int k, int nx, int ny, int nz)
+{
+    const int kk = ((k + nz / 2) % nz) - nz / 2, jj = ((j + ny / 2) % ny) - ny / 2;
+    const int ii = ((i + nx / 2) % nx) - nx / 2;
+    const int kj2 = jj * jj + kk * kk;
+    return ii * ii + kj2;
+}
+
+// The twiddle factors by their argument: twk2[k2] = exp(AP k2) for every k2
+// up to (nx^2 + ny^2 + nz^2) / 4.  The factor of a point is twk2[k2 of the
+// point], the same double the reference's per-point map holds, from a table
+// small enough to stay in L2 (1.5 MB at 512^3).
+__global__ void k_twiddle_table(double *twk2, int k2max)
+{
+    for (int k2 = blockIdx.x * blockDim.x + threadIdx.x; k2 <= k2max; k2 += gridDim.x * blockDim.x)
+        twk2[k2] = exp(kAp * (double)k2);
+}
+
+// The per-point map itself, for reading out (cgb_ft_read)
+__global__ void k_indexmap(double *tw, const double *__restrict__ twk2, int nx, int ny, int nz)
+{
+    const long long nt = (long long)nx * ny * nz;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nt;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int i = int(e % nx), j = int((e / nx) % ny), k = int(e / ((long long)nx * ny));
+        tw[e] = twk2[k2_of(i, j, k, nx, ny, nz)];
+    }
+}
+
+// W[k] = exp(2 pi i k / n), k < n
+__global__ void k_roots(double2 *W, int n)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    double s, c;
+    sincospi(2.0 * k / n, &s, &c);
+    W[k] = make_double2(c, s);
+}
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// (i SIGN) z
+template <int SIGN>
+__device__ __forceinline__ double2 rot90(double2 z)
+{
+    return SIGN > 0 ? make_double2(-z.y, z.x) : make_double2(z.y, -z.x);
+}
+
+template <int SIGN>
+__device__ __forceinline__ void dft2(double2 *x)
+{
+    const double2 t = x[0];
+    x[0] = cadd(t, x[1]);
+    x[1] = csub(t, x[1]);
+}
+
+// y_k = sum_j x_j w^(jk), w = exp(2 pi i SIGN / 4), in place, natural order
+template <int SIGN>
+__device__ __forceinline__ void dft4(double2 *x)
+{
+    const double2 c0 = cadd(x[0], x[2]), c1 = csub(x[0], x[2]);
+    const double2 c2 = cadd(x[1], x[3]), c3 = rot90<SIGN>(csub(x[1], x[3]));
+    x[0] = cadd(c0, c2);
+    x[2] = csub(c0, c2);
+    x[1] = cadd(c1, c3);
+    x[3] = csub(c1, c3);
+}
+
+// the 8-point transform: the sums and the twiddled differences of the two
+// halves, each by a 4-point transform, to the even and the odd outputs
+template <int SIGN>
+__device__ __forceinline__ void dft8(double2 *x)
+{
+    double2 a[4], b[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        a[k] = cadd(x[k], x[k + 4]);
+        b[k] = csub(x[k], x[k + 4]);
+    }
+    const double c = kRoot2Half, s = SIGN * kRoot2Half;
+    b[1] = make_double2(c * b[1].x - s * b[1].y, s * b[1].x + c * b[1].y);
+    b[2] = rot90<SIGN>(b[2]);
+    b[3] = make_double2(-c * b[3].x - s * b[3].y, s * b[3].x - c * b[3].y);
+    dft4<SIGN>(a);
+    dft4<SIGN>(b);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        x[2 * k] = a[k];
+        x[2 * k + 1] = b[k];
+    }
+}
+
+template <int R, int SIGN>
+__device__ __forceinline__ void dft(double2 *x)
+{
+    if constexpr (R == 8) dft8<SIGN>(x);
+    else if constexpr (R == 4) dft4<SIGN>(x);
+    else dft2<SIGN>(x);
+}
+
+// Radix of the stage whose sub-transforms have NS points: 8 while 8 divides
+// what is left, then 4 or 2.
+template <int N, int NS>
+struct StageRadix {
+    static constexpr int value = ((N / NS) % 8 == 0) ? 8 : ((N / NS) % 4 == 0 ? 4 : 2);
+};
+
+// Shared-memory place of point n of line l: rows of P, one spare point
+// after every 8 rows, so that the first radix-8 stage's writes (rows 8j + r
+// for consecutive j, 128 P bytes apart without it) fall on different banks.
+template <int P>
+__device__ __forceinline__ int sidx(int n, int l)
+{
+    return n * P + l + (n >> 3);
+}
+template <int N, int P>
+constexpr int smem_points()
+{
+    return N * P + N / 8;
+}
+
+// One Stockham stage over L lines of N points in s[sidx(n, l)]: butterfly j
+// of a line takes the points j + r N/R, twiddles them by
+// W^((j mod NS) r N/(NS R)), transforms them and puts them at
+// (j / NS) NS R + (j mod NS) + r NS.  T threads, each (N/R) L / T
+// butterflies; all reads before the barrier, all writes after it.
+template <int N, int L, int P, int NS, int R, int SIGN>
+__device__ __forceinline__ void stage(double2 *s, const double2 *__restrict__ W, int wscale)
+{
+    constexpr int T = N * L / 8, PER = (N / R) * L / T;
+    double2 v[PER][R];
+#pragma unroll
+    for (int p = 0; p < PER; p++) {
+        const int b = threadIdx.x + p * T, l = b % L, j = b / L;
+#pragma unroll
+        for (int r = 0; r < R; r++) v[p][r] = s[sidx<P>(j + r * (N / R), l)];
+        if constexpr (NS > 1) {
+            const int jm = j % NS;
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                double2 w = __ldg(W + jm * r * (N / (NS * R)) * wscale);
+                if constexpr (SIGN < 0) w.y = -w.y;
+                v[p][r] = cmul(v[p][r], w);
+            }
+        }
+        dft<R, SIGN>(v[p]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < PER; p++) {
+        const int b = threadIdx.x + p * T, l = b % L, j = b / L;
+        const int d = (j / NS) * NS * R + (j % NS);
+#pragma unroll
+        for (int r = 0; r < R; r++) s[sidx<P>(d + r * NS, l)] = v[p][r];
+    }
+    __syncthreads();
+}
+
+template <int N, int L, int P, int NS, int SIGN>
+__device__ __forceinline__ void stages(double2 *s, const double2 *__restrict__ W, int wscale)
+{
+    if constexpr (NS < N) {
+        constexpr int R = StageRadix<N, NS>::value;
+        stage<N, L, P, NS, R, SIGN>(s, W, wscale);
+        stages<N, L, P, NS * R, SIGN>(s, W, wscale);
+    }
+}
+
+// Lines a CTA: about FT_TILE_POINTS points a tile, 2 .. 16 lines (x
+// lines), 4 .. 32 lines (y and z: a row of L consecutive x values is the
+// run each strided row read fetches).
+#ifndef FT_TILE_POINTS
+#define FT_TILE_POINTS 4096
+#endif
+#ifndef FT_ROW_POINTS
+#define FT_ROW_POINTS 4096
+#endif
+constexpr int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+template <int N, int AXIS>
+struct Tile {
+    static constexpr int L = AXIS == 0 ? clampi(FT_TILE_POINTS / N, 2, 16) : clampi(FT_ROW_POINTS / N, 4, 32);
+    static constexpr int T = N * L / 8;  // threads: one radix-8 butterfly each a stage
+};
+
+// One axis of the transform: AXIS 0 (x), 1 (y), 2 (z).  in and out may be
+// the same array (a CTA reads its whole tile before writing it).  EVOLVE:
+// in is u0; each point is first multiplied by its twiddle factor and the
+// product written back to u0 (ft.cu:1245-1256), then transformed into out.
+template <int N, int AXIS, int SIGN, bool EVOLVE>
+__global__ void __launch_bounds__(Tile<N, AXIS>::T, (1024 / Tile<N, AXIS>::T) < 1 ? 1 : 1024 / Tile<N, AXIS>::T)
+    k_fft(const double2 *in, double2 *out, double2 *u0, const double *__restrict__ twk2,
+          const double2 *__restrict__ W, int wscale, int nx, int ny, int nz)
+{
+    static_assert(!EVOLVE || AXIS == 2, "evolve rides on the z lines");
+    constexpr int L = Tile<N, AXIS>::L, P = AXIS == 0 ? L + 1 : L, T = Tile<N, AXIS>::T;
+    extern __shared__ double2 sbuf[];
+    long long base, sn, sl;
+    int x0 = 0, q = 0;  // y and z lines: the tile's first x and its z (y lines) or y (z lines)
+    if constexpr (AXIS == 0) {
+        base = (long long)blockIdx.x * L * nx;
+        sn = 1;
+        sl = nx;
+    } else {
+        const int tiles_x = nx / L;
+        x0 = (blockIdx.x % tiles_x) * L;
+        q = blockIdx.x / tiles_x;
+        base = AXIS == 1 ? (long long)q * nx * ny + x0 : (long long)q * nx + x0;
+        sn = AXIS == 1 ? (long long)nx : (long long)nx * ny;
+        sl = 1;
+    }
+    // evolve: the signed frequencies (ft.cu:1176-1182, i' = i or i - n),
+    // the tile's j'^2 once
+    int jj2 = 0;
+    if constexpr (EVOLVE) {
+        const int jj = q < ny / 2 ? q : q - ny;
+        jj2 = jj * jj;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const int i = threadIdx.x + k * T;
+        const int n = AXIS == 0 ? i % N : i / L, l = AXIS == 0 ? i / N : i % L;
+        const long long e = base + n * sn + l * sl;
+        double2 v = in[e];
+        if constexpr (EVOLVE) {
+            // the point is (x0 + l, q, n); its squared frequency, summed as
+            // the reference sums it (integers: exact in any order)
+            const int xi = x0 + l, ii = xi < nx / 2 ? xi : xi - nx, kk = n < nz / 2 ? n : n - nz;
+            const double t = __ldg(twk2 + (ii * ii + (jj2 + kk * kk)));
+            v = make_double2(v.x * t, v.y * t);
+            u0[e] = v;
+        }
+        sbuf[sidx<P>(n, l)] = v;
+    }
+    __syncthreads();
+    stages<N, L, P, 1, SIGN>(sbuf, W, wscale);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const int i = threadIdx.x + k * T;
+        const int n = AXIS == 0 ? i % N : i / L, l = AXIS == 0 ? i / N : i % L;
+        out[base + n * sn + l * sl] = sbuf[sidx<P>(n, l)];
+    }
+}
+
+// sums[it] = the sum of u1 at the 1024 points, over nt (a fixed-order tree)
+__global__ void __launch_bounds__(kPoints) k_checksum(const double2 *u1, int nx, int ny, int nz, int it,
+                                                      double2 *sums)
+{
+    __shared__ double2 sh[kPoints];
+    const int j = threadIdx.x + 1;
+    const long long e = (long long)(j % nx) + (long long)(3 * j % ny) * nx + (long long)(5 * j % nz) * nx * ny;
+    sh[threadIdx.x] = u1[e];
+    __syncthreads();
+    for (int w = kPoints / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] = cadd(sh[threadIdx.x], sh[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double nt = (double)nx * ny * nz;
+        sums[it] = make_double2(sh[0].x / nt, sh[0].y / nt);
+    }
+}
+
+using FftKernel = void (*)(const double2 *, double2 *, double2 *, const double *, const double2 *, int, int, int,
+                           int);
+
+struct Launch {
+    FftKernel k = nullptr;
+    int threads = 0, lines = 0;
+    size_t smem = 0;
+};
+
+template <int N, int AXIS, int SIGN, bool EVOLVE>
+Launch make_launch()
+{
+    constexpr int L = Tile<N, AXIS>::L, P = AXIS == 0 ? L + 1 : L;
+    Launch a;
+    a.k = k_fft<N, AXIS, SIGN, EVOLVE>;
+    a.threads = Tile<N, AXIS>::T;
+    a.lines = L;
+    a.smem = sizeof(double2) * smem_points<N, P>();
+    return a;
+}
+
+template <int AXIS, int SIGN, bool EVOLVE>
+Launch pick(int n)
+{
+    switch (n) {
+    case 32: return make_launch<32, AXIS, SIGN, EVOLVE>();
+    case 64: return make_launch<64, AXIS, SIGN, EVOLVE>();
+    case 128: return make_launch<128, AXIS, SIGN, EVOLVE>();
+    case 256: return make_launch<256, AXIS, SIGN, EVOLVE>();
+    case 512: return make_launch<512, AXIS, SIGN, EVOLVE>();
+    case 1024: return make_launch<1024, AXIS, SIGN, EVOLVE>();
+    case 2048: return make_launch<2048, AXIS, SIGN, EVOLVE>();
+    default: return Launch{};
+    }
+}
+
+}  // namespace ft
+}  // namespace cgb
+
+using namespace cgb;
+using namespace cgb::ft;
+
+struct cgb_ft {
+    int device = 0, nx = 0, ny = 0, nz = 0, maxdim = 0;
+    long long nt = 0;
+    double2 *u0 = nullptr, *u1 = nullptr, *W = nullptr, *sums = nullptr;
+    double *twk2 = nullptr;  // the twiddle factors by k2
+    int k2max = 0;
+    Launch fwd[3], inv[3];  // x, y, z passes; inv[2] evolves
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int exec_niter = -1;
+};
+
+namespace {
+
+#define FT_TRY(call)                                                                      \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return set_error(e_ == cudaErrorMemoryAllocation ? CGB_ERR_NOMEM : CGB_ERR_CUDA, \
+                             "ft: %s: %s", #call, cudaGetErrorString(e_));                \
+    } while (0)
+
+void ft_release(cgb_ft *f)
+{
+    if (!f) return;
+    cudaSetDevice(f->device);
+    if (f->exec) cudaGraphExecDestroy(f->exec);
+    for (void *p : {(void *)f->u0, (void *)f->u1, (void *)f->W, (void *)f->sums, (void *)f->twk2})
+        if (p) cudaFree(p);
+    if (f->ev0) cudaEventDestroy(f->ev0);
+    if (f->ev1) cudaEventDestroy(f->ev1);
+    if (f->stream) cudaStreamDestroy(f->stream);
+    delete f;
+}
+
+bool pow2_in(int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; }
+
+void run_pass(cgb_ft *f, const Launch &a, int axis, const double2 *in, double2 *out)
+{
+    const int dims[3] = {f->nx, f->ny, f->nz};
+    const unsigned tiles = unsigned(f->nt / ((long long)dims[axis] * a.lines));
+    a.k<<<tiles, a.threads, a.smem, f->stream>>>(in, out, f->u0, f->twk2, f->W, f->maxdim / dims[axis], f->nx, f->ny,
+                                                  f->nz);
+}
+
+// main's timed region (ft.cu:391-408): index map (as its table by k2),
+// initial conditions, the roots, the forward transform u1 -> u0, then
+// niter x (evolve, inverse transform, checksum)
+void enqueue_benchmark(cgb_ft *f, int niter)
+{
+    const cudaStream_t st = f->stream;
+    k_roots<<<(f->maxdim + 255) / 256, 256, 0, st>>>(f->W, f->maxdim);
+    k_twiddle_table<<<(f->k2max + 256) / 256, 256, 0, st>>>(f->twk2, f->k2max);
+    const long long init_threads = (f->nt + kInitPer - 1) / kInitPer;
+    k_initial<<<unsigned((init_threads + 255) / 256), 256, 0, st>>>(f->u1, f->nt);
+    run_pass(f, f->fwd[0], 0, f->u1, f->u1);
+    run_pass(f, f->fwd[1], 1, f->u1, f->u1);
+    run_pass(f, f->fwd[2], 2, f->u1, f->u0);
+    for (int it = 1; it <= niter; it++) {
+        run_pass(f, f->inv[2], 2, f->u0, f->u1);
+        run_pass(f, f->inv[1], 1, f->u1, f->u1);
+        run_pass(f, f->inv[0], 0, f->u1, f->u1);
+        k_checksum<<<1, kPoints, 0, st>>>(f->u1, f->nx, f->ny, f->nz, it, f->sums);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int cgb_ft_create(int device, int nx, int ny, int nz, cgb_ft **out)
+{
+    if (!out) return set_error(CGB_ERR_INVALID, "ft: null output");
+    *out = nullptr;
+    if (!pow2_in(nx, 32, 2048) || !pow2_in(ny, 32, 2048) || !pow2_in(nz, 32, 2048))
+        return set_error(CGB_ERR_INVALID, "ft: each dimension a power of two in [32, 2048]");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count)
+        return set_error(CGB_ERR_NO_DEVICE, "ft: no CUDA device %d", device);
+    int major = 0;
+    FT_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+    if (major != 10) return set_error(CGB_ERR_NO_DEVICE, "ft: device %d is not sm_100", device);
+    FT_TRY(cudaSetDevice(device));
+    cgb_ft *f = new (std::nothrow) cgb_ft;
+    if (!f) return set_error(CGB_ERR_NOMEM, "ft: allocation failed");
+    f->device = device;
+    f->nx = nx;
+    f->ny = ny;
+    f->nz = nz;
+    f->maxdim = std::max(nx, std::max(ny, nz));
+    f->nt = (long long)nx * ny * nz;
+    f->k2max = (nx / 2) * (nx / 2) + (ny / 2) * (ny / 2) + (nz / 2) * (nz / 2);
+    f->fwd[0] = pick<0, 1, false>(nx);
+    f->fwd[1] = pick<1, 1, false>(ny);
+    f->fwd[2] = pick<2, 1, false>(nz);
+    f->inv[0] = pick<0, -1, false>(nx);
+    f->inv[1] = pick<1, -1, false>(ny);
+    f->inv[2] = pick<2, -1, true>(nz);
+    bool ok = true;
+    for (const Launch *a : {&f->fwd[0], &f->fwd[1], &f->fwd[2], &f->inv[0], &f->inv[1], &f->inv[2]})
+        ok = ok && a->k &&
+             cudaFuncSetAttribute(a->k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(a->smem)) == cudaSuccess;
+    ok = ok && cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreate(&f->ev0) == cudaSuccess && cudaEventCreate(&f->ev1) == cudaSuccess;
+    if (!ok) {
+        ft_release(f);
+        return set_error(CGB_ERR_CUDA, "ft: kernel set-up failed");
+    }
+    ok = cudaMalloc(&f->u0, sizeof(double2) * size_t(f->nt)) == cudaSuccess &&
+         cudaMalloc(&f->u1, sizeof(double2) * size_t(f->nt)) == cudaSuccess &&
+         cudaMalloc(&f->twk2, sizeof(double) * size_t(f->k2max + 1)) == cudaSuccess &&
+         cudaMalloc(&f->W, sizeof(double2) * size_t(f->maxdim)) == cudaSuccess &&
+         cudaMalloc(&f->sums, sizeof(double2) * (kMaxIter + 1)) == cudaSuccess;
+    if (!ok) {
+        ft_release(f);
+        return set_error(CGB_ERR_NOMEM, "ft: device allocation failed (%d x %d x %d)", nx, ny, nz);
+    }
+    *out = f;
+    return CGB_OK;
+}
+
+int cgb_ft_destroy(cgb_ft *f)
+{
+    ft_release(f);
+    return CGB_OK;
+}
+
+int cgb_ft_run(cgb_ft *f, int niter, double *sums, double *device_ms)
+{
+    if (!f) return set_error(CGB_ERR_INVALID, "ft: null instance");
+    if (niter < 1 || niter > kMaxIter) return set_error(CGB_ERR_INVALID, "ft: niter must be in [1, %d]", kMaxIter);
+    FT_TRY(cudaSetDevice(f->device));
+    const cudaStream_t st = f->stream;
+    if (!f->exec || f->exec_niter != niter) {
+        if (f->exec) cudaGraphExecDestroy(f->exec);
+        f->exec = nullptr;
+        cudaGraph_t graph = nullptr;
+        FT_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        enqueue_benchmark(f, niter);
+        const cudaError_t e1 = cudaGetLastError();
+        const cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+        if (e1 != cudaSuccess || e2 != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            return set_error(CGB_ERR_CUDA, "ft: capture failed: %s", cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+        }
+        const cudaError_t e3 = cudaGraphInstantiate(&f->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e3 != cudaSuccess) {
+            f->exec = nullptr;
+            return set_error(CGB_ERR_CUDA, "ft: graph instantiation failed");
+        }
+        f->exec_niter = niter;
+    }
+    FT_TRY(cudaEventRecord(f->ev0, st));
+    FT_TRY(cudaGraphLaunch(f->exec, st));
+    FT_TRY(cudaEventRecord(f->ev1, st));
+    double2 h[kMaxIter + 1];
+    FT_TRY(cudaMemcpyAsync(h, f->sums, sizeof(double2) * (niter + 1), cudaMemcpyDeviceToHost, st));
+    FT_TRY(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    FT_TRY(cudaEventElapsedTime(&ms, f->ev0, f->ev1));
+    if (sums)
+        for (int it = 1; it <= niter; it++) {
+            sums[2 * (it - 1)] = h[it].x;
+            sums[2 * (it - 1) + 1] = h[it].y;
+        }
+    if (device_ms) *device_ms = ms;
+    return CGB_OK;
+}
+
+int cgb_ft_read(cgb_ft *f, int which, double *out, long long count)
+{
+    if (!f || !out || which < 0 || which > 2) return set_error(CGB_ERR_INVALID, "ft: bad read");
+    const long long need = which == 2 ? f->nt : 2 * f->nt;
+    if (count < need) return set_error(CGB_ERR_CAPACITY, "ft: %lld doubles needed", need);
+    FT_TRY(cudaSetDevice(f->device));
+    if (which == 2) {  // the per-point map, expanded from the table into a scratch array
+        double *tw = nullptr;
+        FT_TRY(cudaMalloc(&tw, sizeof(double) * size_t(f->nt)));
+        k_twiddle_table<<<(f->k2max + 256) / 256, 256, 0, f->stream>>>(f->twk2, f->k2max);
+        k_indexmap<<<8 * 148, 256, 0, f->stream>>>(tw, f->twk2, f->nx, f->ny, f->nz);
+        const cudaError_t e1 = cudaGetLastError(), e2 = cudaStreamSynchronize(f->stream);
+        const cudaError_t e3 = cudaMemcpy(out, tw, sizeof(double) * size_t(need), cudaMemcpyDeviceToHost);
+        cudaFree(tw);
+        if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+            return set_error(CGB_ERR_CUDA, "ft: reading the twiddle factors failed");
+        return CGB_OK;
+    }
+    const void *src = which == 0 ? (const void *)f->u0 : (const void *)f->u1;
+    FT_TRY(cudaMemcpy(out, src, sizeof(double) * size_t(need), cudaMemcpyDeviceToHost));
+    return CGB_OK;
+}
+
+}  // extern "C"

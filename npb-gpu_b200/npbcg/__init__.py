@@ -218,6 +218,11 @@ _SIGNATURES = {
     "cgb_is_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
                                   ctypes.POINTER(ctypes.c_double)]),
     "cgb_is_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong]),
+    "cgb_ft_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_void_p)]),
+    "cgb_ft_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "cgb_ft_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _F64, ctypes.POINTER(ctypes.c_double)]),
+    "cgb_ft_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _F64, ctypes.c_longlong]),
     "cgb_host_alloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_longlong]),
     "cgb_host_free": (ctypes.c_int, [ctypes.c_void_p]),
     "cgb_device_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
@@ -1082,3 +1087,110 @@ class IntSort:
         out = np.zeros(n, np.uint32 if w == 1 else np.int32)
         _check(lib().cgb_is_read(self._h, w, out.ctypes.data_as(ctypes.c_void_p), n))
         return out
+
+
+# NPB FT: (nx, ny, nz, niter) per class (setparams.cpp:797-803) and the
+# reference's checksums (real, imaginary) per iteration (ft.cu:1655-1810)
+FT_CLASSES = {"S": (64, 64, 64, 6), "W": (128, 128, 32, 6), "A": (256, 256, 128, 6),
+              "B": (512, 256, 256, 20), "C": (512, 512, 512, 20), "D": (2048, 1024, 1024, 25)}
+FT_VERIFY_EPSILON = 1.0e-12
+FT_CHECKSUMS = {
+    "S": [(5.546087004964E+02, 4.845363331978E+02), (5.546385409189E+02, 4.865304269511E+02),
+          (5.546148406171E+02, 4.883910722336E+02), (5.545423607415E+02, 4.901273169046E+02),
+          (5.544255039624E+02, 4.917475857993E+02), (5.542683411902E+02, 4.932597244941E+02)],
+    "W": [(5.673612178944E+02, 5.293246849175E+02), (5.631436885271E+02, 5.282149986629E+02),
+          (5.594024089970E+02, 5.270996558037E+02), (5.560698047020E+02, 5.260027904925E+02),
+          (5.530898991250E+02, 5.249400845633E+02), (5.504159734538E+02, 5.239212247086E+02)],
+    "A": [(5.046735008193E+02, 5.114047905510E+02), (5.059412319734E+02, 5.098809666433E+02),
+          (5.069376896287E+02, 5.098144042213E+02), (5.077892868474E+02, 5.101336130759E+02),
+          (5.085233095391E+02, 5.104914655194E+02), (5.091487099959E+02, 5.107917842803E+02)],
+    "B": [(5.177643571579E+02, 5.077803458597E+02), (5.154521291263E+02, 5.088249431599E+02),
+          (5.146409228649E+02, 5.096208912659E+02), (5.142378756213E+02, 5.101023387619E+02),
+          (5.139626667737E+02, 5.103976610617E+02), (5.137423460082E+02, 5.105948019802E+02),
+          (5.135547056878E+02, 5.107404165783E+02), (5.133910925466E+02, 5.108576573661E+02),
+          (5.132470705390E+02, 5.109577278523E+02), (5.131197729984E+02, 5.110460304483E+02),
+          (5.130070319283E+02, 5.111252433800E+02), (5.129070537032E+02, 5.111968077718E+02),
+          (5.128182883502E+02, 5.112616233064E+02), (5.127393733383E+02, 5.113203605551E+02),
+          (5.126691062020E+02, 5.113735928093E+02), (5.126064276004E+02, 5.114218460548E+02),
+          (5.125504076570E+02, 5.114656139760E+02), (5.125002331720E+02, 5.115053595966E+02),
+          (5.124551951846E+02, 5.115415130407E+02), (5.124146770029E+02, 5.115744692211E+02)],
+    "C": [(5.195078707457E+02, 5.149019699238E+02), (5.155422171134E+02, 5.127578201997E+02),
+          (5.144678022222E+02, 5.122251847514E+02), (5.140150594328E+02, 5.121090289018E+02),
+          (5.137550426810E+02, 5.121143685824E+02), (5.135811056728E+02, 5.121496764568E+02),
+          (5.134569343165E+02, 5.121870921893E+02), (5.133651975661E+02, 5.122193250322E+02),
+          (5.132955192805E+02, 5.122454735794E+02), (5.132410471738E+02, 5.122663649603E+02),
+          (5.131971141679E+02, 5.122830879827E+02), (5.131605205716E+02, 5.122965869718E+02),
+          (5.131290734194E+02, 5.123075927445E+02), (5.131012720314E+02, 5.123166486553E+02),
+          (5.130760908195E+02, 5.123241541685E+02), (5.130528295923E+02, 5.123304037599E+02),
+          (5.130310107773E+02, 5.123356167976E+02), (5.130103090133E+02, 5.123399592211E+02),
+          (5.129905029333E+02, 5.123435588985E+02), (5.129714421109E+02, 5.123465164008E+02)],
+    "D": [(5.122230065252E+02, 5.118534037109E+02), (5.120463975765E+02, 5.117061181082E+02),
+          (5.119865766760E+02, 5.117096364601E+02), (5.119518799488E+02, 5.117373863950E+02),
+          (5.119269088223E+02, 5.117680347632E+02), (5.119082416858E+02, 5.117967875532E+02),
+          (5.118943814638E+02, 5.118225281841E+02), (5.118842385057E+02, 5.118451629348E+02),
+          (5.118769435632E+02, 5.118649119387E+02), (5.118718203448E+02, 5.118820803844E+02),
+          (5.118683569061E+02, 5.118969781011E+02), (5.118661708593E+02, 5.119098918835E+02),
+          (5.118649768950E+02, 5.119210777066E+02), (5.118645605626E+02, 5.119307604484E+02),
+          (5.118647586618E+02, 5.119391362671E+02), (5.118654451572E+02, 5.119463757241E+02),
+          (5.118665212451E+02, 5.119526269238E+02), (5.118679083821E+02, 5.119580184108E+02),
+          (5.118695433664E+02, 5.119626617538E+02), (5.118713748264E+02, 5.119666538138E+02),
+          (5.118733606701E+02, 5.119700787219E+02), (5.118754661974E+02, 5.119730095953E+02),
+          (5.118776626738E+02, 5.119755100241E+02), (5.118799262314E+02, 5.119776353561E+02),
+          (5.118822370068E+02, 5.119794338060E+02)],
+}
+
+
+def ft_verify(cls, sums):
+    """The largest relative error of a run's checksums against the class's
+    (ft.cu:1811-1822: |(sum - ref) / ref| per iteration)."""
+    ref = FT_CHECKSUMS[cls]
+    return max(abs(complex(*s) - complex(*r)) / abs(complex(*r)) for s, r in zip(sums, ref))
+
+
+class Ft:
+    """The NPB FT benchmark's arrays on one GPU (cgb_ft)."""
+
+    def __init__(self, nx, ny, nz, device=0):
+        self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
+        h = ctypes.c_void_p()
+        _check(lib().cgb_ft_create(device, self.nx, self.ny, self.nz, ctypes.byref(h)))
+        self._h = h
+
+    @classmethod
+    def for_class(cls, name, device=0):
+        nx, ny, nz, _ = FT_CLASSES[name]
+        return cls(nx, ny, nz, device)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cgb_ft_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def run(self, niter):
+        """main's timed region: {sums: [(re, im)] * niter, device_ms}."""
+        sums = np.zeros(2 * niter)
+        t = ctypes.c_double()
+        _check(lib().cgb_ft_run(self._h, int(niter), sums, ctypes.byref(t)))
+        return dict(sums=[(sums[2 * i], sums[2 * i + 1]) for i in range(niter)], device_ms=t.value)
+
+    def read(self, which):
+        """'u0' or 'u1' (complex, shape (nz, ny, nx)) or 'twiddle' (float, same shape)."""
+        w = {"u0": 0, "u1": 1, "twiddle": 2}[which]
+        nt = self.nx * self.ny * self.nz
+        out = np.zeros(nt if w == 2 else 2 * nt)
+        _check(lib().cgb_ft_read(self._h, w, out, out.size))
+        if w == 2:
+            return out.reshape(self.nz, self.ny, self.nx)
+        return out.view(np.complex128).reshape(self.nz, self.ny, self.nx)

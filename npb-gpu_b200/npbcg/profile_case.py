@@ -9,6 +9,7 @@
     python npb-gpu_b200/npbcg/profile_case.py --what mg --mg-class A --niter 4
     python npb-gpu_b200/npbcg/profile_case.py --what ep --ep-class B
     python npb-gpu_b200/npbcg/profile_case.py --what is --is-class B
+    python npb-gpu_b200/npbcg/profile_case.py --what ft --ft-class B
 
 `spmv` launches the standalone FP64 SpMV+dot kernel `reps` times (after one
 warm-up launch); `solve` runs one power iteration of `niter` outer steps;
@@ -17,8 +18,9 @@ row-partitioned solver on `ranks` device-generated row blocks, all driven
 from this process; `mg` runs the MG benchmark's timed region (niter
 V-cycles) of an MG class once after one warm-up run; `ep` runs the EP
 kernel of an EP class once; `is` runs the IS benchmark (one untimed and ten
-timed ranking passes, the full check) of an IS class once.  Each prints one
-JSON line.
+timed ranking passes, the full check) of an IS class once; `ft` runs the FT
+benchmark's timed region of an FT class once after one warm-up run.  Each
+prints one JSON line.
 """
 import argparse
 import json
@@ -33,9 +35,11 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cls", default="B", choices=sorted(npbcg.CLASSES))
     ap.add_argument("--what", default="spmv",
-                    choices=["spmv", "solve", "sweep", "batch", "barrier", "part", "mg", "ep", "is"])
+                    choices=["spmv", "solve", "sweep", "batch", "barrier", "part", "mg", "ep", "is", "ft"])
     ap.add_argument("--ep-class", default="B", choices=sorted(npbcg.EP_CLASSES),
                     help="ep: the EP class")
+    ap.add_argument("--ft-class", default="B", choices=sorted(npbcg.FT_CLASSES),
+                    help="ft: the FT class")
     ap.add_argument("--is-class", default="B", choices=sorted(npbcg.IS_CLASSES),
                     help="is: the IS class")
     ap.add_argument("--mg-class", default="A", choices=sorted(npbcg.MG_CLASSES),
@@ -74,6 +78,14 @@ def main():
         r = npbcg.ep_run(npbcg.EP_CLASSES[a.ep_class]["m"])
         print(json.dumps({"what": "ep", "class": a.ep_class, "sx": r["sx"], "sy": r["sy"],
                           "device_ms": r["device_ms"]}), flush=True)
+        return
+    if a.what == "ft":
+        nx, ny, nz, niter = npbcg.FT_CLASSES[a.ft_class]
+        with npbcg.Ft(nx, ny, nz) as f:
+            f.run(niter)
+            r = f.run(niter)
+        print(json.dumps({"what": "ft", "class": a.ft_class, "device_ms": r["device_ms"],
+                          "max_rel_err": npbcg.ft_verify(a.ft_class, r["sums"])}), flush=True)
         return
     if a.what == "is":
         with npbcg.IntSort(a.is_class) as s:

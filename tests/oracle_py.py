@@ -57,6 +57,14 @@ class Oracle:
         lib.orc_ep_run.argtypes = [ctypes.c_int, dp, dp, F64, dp]
         lib.orc_mg_norm2u3.restype = None
         lib.orc_mg_norm2u3.argtypes = [ctypes.c_int, F64, dp, dp]
+        lib.orc_ft_run.restype = ctypes.c_int
+        lib.orc_ft_run.argtypes = [ctypes.c_int] * 4 + [F64, ctypes.c_void_p]
+        lib.orc_ft_fft3d.restype = None
+        lib.orc_ft_fft3d.argtypes = [ctypes.c_int] * 4 + [F64]
+        lib.orc_ft_initial.restype = None
+        lib.orc_ft_initial.argtypes = [ctypes.c_int] * 3 + [F64]
+        lib.orc_ft_indexmap.restype = None
+        lib.orc_ft_indexmap.argtypes = [ctypes.c_int] * 3 + [F64]
         self.lib = lib
 
     # ---- MG: grids are float64 cubes of side m, index (i3 * m + i2) * m + i1
@@ -130,6 +138,35 @@ class Oracle:
         if rc != 0:
             raise RuntimeError(f"orc_ep_run failed: {rc}")
         return dict(sx=sx.value, sy=sy.value, q=q, seconds=t.value)
+
+    # ---- FT: fields are complex arrays of shape (nz, ny, nx)
+    def ft_run(self, nx, ny, nz, niter, field=False):
+        """NPB FT (ft_oracle.c): the checksums [(re, im)] * niter and, with
+        field, the last inverse transform u1."""
+        sums = np.zeros(2 * niter)
+        u1 = np.zeros(2 * nx * ny * nz) if field else None
+        rc = self.lib.orc_ft_run(nx, ny, nz, niter, sums, None if u1 is None else u1.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("orc_ft_run: out of memory")
+        out = [(sums[2 * i], sums[2 * i + 1]) for i in range(niter)]
+        return (out, u1.view(np.complex128).reshape(nz, ny, nx)) if field else out
+
+    def ft_fft3d(self, direction, a):
+        """The reference's 3-D transform of a complex (nz, ny, nx) array."""
+        nz, ny, nx = a.shape
+        buf = np.ascontiguousarray(a, np.complex128).view(np.float64).ravel().copy()
+        self.lib.orc_ft_fft3d(direction, nx, ny, nz, buf)
+        return buf.view(np.complex128).reshape(nz, ny, nx)
+
+    def ft_initial(self, nx, ny, nz):
+        buf = np.zeros(2 * nx * ny * nz)
+        self.lib.orc_ft_initial(nx, ny, nz, buf)
+        return buf.view(np.complex128).reshape(nz, ny, nx)
+
+    def ft_indexmap(self, nx, ny, nz):
+        buf = np.zeros(nx * ny * nz)
+        self.lib.orc_ft_indexmap(nx, ny, nz, buf)
+        return buf.reshape(nz, ny, nx)
 
     def mg_norm(self, m, r):
         a, b = ctypes.c_double(), ctypes.c_double()
@@ -320,3 +357,23 @@ class RefIsLib:
         t = ctypes.c_double()
         passed = self.lib.ref_is_gpu(ctypes.byref(t))
         return dict(passed=int(passed), seconds=t.value)
+
+
+class RefFtLib:
+    """The reference's own FT GPU code for one NPB class (oracle/_ref/libref_ft_<class>.so)."""
+
+    def __init__(self, path):
+        lib = ctypes.CDLL(path)
+        lib.ref_ft_niter.restype = ctypes.c_int
+        lib.ref_ft_gpu.restype = ctypes.c_int
+        lib.ref_ft_gpu.argtypes = [F64, ctypes.POINTER(ctypes.c_double)]
+        self.lib = lib
+        self.niter = lib.ref_ft_niter()
+
+    def gpu(self):
+        """main's sequence: {sums: [(re, im)] * niter, seconds (the timed region, wall)}."""
+        sums = np.zeros(2 * self.niter)
+        t = ctypes.c_double()
+        if self.lib.ref_ft_gpu(sums, ctypes.byref(t)) != self.niter:
+            raise RuntimeError("ref_ft_gpu failed")
+        return dict(sums=[(sums[2 * i], sums[2 * i + 1]) for i in range(self.niter)], seconds=t.value)
