@@ -32,6 +32,7 @@ DRIVER = os.path.join(BINDIR, "cg")
 MG_DRIVER = os.path.join(BINDIR, "mg")
 EP_DRIVER = os.path.join(BINDIR, "ep")
 IS_DRIVER = os.path.join(BINDIR, "is")
+FT_DRIVER = os.path.join(BINDIR, "ft")
 
 
 def nvcc():
@@ -95,7 +96,8 @@ def build(verbose=False, ptxas_info=False, force=False):
     if force or sources_newer(DRIVER, [main_src, LIB] + headers):
         run([nvcc(), "-O2", "-std=c++17", "-o", DRIVER, main_src, "-L" + LIBDIR, "-lcgb",
              "-Xlinker", "-rpath=$ORIGIN/../lib"], verbose)
-    for name, target in (("mg_main.cpp", MG_DRIVER), ("ep_main.cpp", EP_DRIVER), ("is_main.cpp", IS_DRIVER)):
+    for name, target in (("mg_main.cpp", MG_DRIVER), ("ep_main.cpp", EP_DRIVER), ("is_main.cpp", IS_DRIVER),
+                         ("ft_main.cpp", FT_DRIVER)):
         src = os.path.join(CSRC, name)
         if force or sources_newer(target, [src, LIB] + headers):
             run([nvcc(), "-O2", "-std=c++17", "-o", target, src, "-L" + LIBDIR, "-lcgb",

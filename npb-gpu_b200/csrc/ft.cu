@@ -297,21 +297,37 @@ __global__ void __launch_bounds__(Tile<N, AXIS>::T, (1024 / Tile<N, AXIS>::T) < 
         const int jj = q < ny / 2 ? q : q - ny;
         jj2 = jj * jj;
     }
+    // every load of the tile before any store: the evolved points go back to
+    // u0, which is `in`, so a store between loads would order them
+    double2 v[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) {
         const int i = threadIdx.x + k * T;
         const int n = AXIS == 0 ? i % N : i / L, l = AXIS == 0 ? i / N : i % L;
-        const long long e = base + n * sn + l * sl;
-        double2 v = in[e];
-        if constexpr (EVOLVE) {
+        v[k] = in[base + n * sn + l * sl];
+    }
+    if constexpr (EVOLVE) {
+        double t[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
             // the point is (x0 + l, q, n); its squared frequency, summed as
             // the reference sums it (integers: exact in any order)
+            const int i = threadIdx.x + k * T, n = i / L, l = i % L;
             const int xi = x0 + l, ii = xi < nx / 2 ? xi : xi - nx, kk = n < nz / 2 ? n : n - nz;
-            const double t = __ldg(twk2 + (ii * ii + (jj2 + kk * kk)));
-            v = make_double2(v.x * t, v.y * t);
-            u0[e] = v;
+            t[k] = __ldg(twk2 + (ii * ii + (jj2 + kk * kk)));
         }
-        sbuf[sidx<P>(n, l)] = v;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int i = threadIdx.x + k * T, n = i / L, l = i % L;
+            v[k] = make_double2(v[k].x * t[k], v[k].y * t[k]);
+            u0[base + n * sn + l * sl] = v[k];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const int i = threadIdx.x + k * T;
+        const int n = AXIS == 0 ? i % N : i / L, l = AXIS == 0 ? i / N : i % L;
+        sbuf[sidx<P>(n, l)] = v[k];
     }
     __syncthreads();
     stages<N, L, P, 1, SIGN>(sbuf, W, wscale);

@@ -1,7 +1,8 @@
-"""The NPB-style MG, EP and IS drivers `npb-gpu_b200/bin/mg`, `bin/ep` and
-`bin/is`, drop-ins for the reference's mg.<CLASS>, ep.<CLASS> and is.<CLASS>
-binaries (GMAP/NPB-GPU CUDA/MG/mg.cu main :356-623, CUDA/EP/ep.cu main
-:114-275, CUDA/IS/is.cu main :335-505).
+"""The NPB-style MG, EP, IS and FT drivers `npb-gpu_b200/bin/mg`, `bin/ep`,
+`bin/is` and `bin/ft`, drop-ins for the reference's mg.<CLASS>, ep.<CLASS>,
+is.<CLASS> and ft.<CLASS> binaries (GMAP/NPB-GPU CUDA/MG/mg.cu main
+:356-623, CUDA/EP/ep.cu main :114-275, CUDA/IS/is.cu main :335-505,
+CUDA/FT/ft.cu main :335-505).
 
 Its report must carry the reference's verification block (mg.cu:526-552,
 epsilon 1e-8 on the L2 norm) and its Mop/s, recomputed here from the
@@ -151,3 +152,37 @@ def test_is_driver_report_verifies():
     assert abs(mops - expect) <= expect * (1e-6 / t + 1e-6) + 0.01
     line = json.loads(run_is("S", "--json").stdout.strip().splitlines()[-1])
     assert line["verified"] is True and line["passed"] == 51 and line["keys"] == 2 ** 16
+
+
+# ------------------------------------------------------------------ FT driver
+FT = os.path.join(ROOT, "npb-gpu_b200", "bin", "ft")
+
+
+def run_ft(*args, timeout=600):
+    if not os.path.exists(FT):
+        pytest.skip("npb-gpu_b200/bin/ft not built")
+    return subprocess.run([FT, *args], capture_output=True, text=True, timeout=timeout)
+
+
+def test_ft_driver_rejects_bad_arguments():
+    for args in ([], ["E"], ["SS"], ["S", "--what"]):
+        r = run_ft(*args, timeout=60)
+        assert r.returncode == 2 and "usage: ft" in r.stderr
+
+
+@pytest.mark.gpu
+def test_ft_driver_report_verifies():
+    import math
+    r = run_ft("W")
+    assert r.returncode == 0, r.stderr
+    assert field(r.stdout, "Verification") == "SUCCESSFUL"
+    lines = re.findall(r"^T =\s+(\d+)\s+Checksum =\s+(\S+)\s+(\S+)$", r.stdout, re.M)
+    assert [int(t) for t, _, _ in lines] == list(range(1, 7))
+    assert abs(float(lines[0][1]) - 5.673612178944E+02) <= 1e-9 * 5.673612178944E+02
+    t = float(field(r.stdout, "Time in seconds"))
+    mops = float(field(r.stdout, "Mop/s total"))
+    nt = 128.0 * 128 * 32
+    expect = 1e-6 * nt * (14.8157 + 7.19641 * math.log(nt) + (5.23518 + 7.21113 * math.log(nt)) * 6) / t
+    assert abs(mops - expect) <= expect * (1e-6 / t + 1e-6) + 0.01
+    line = json.loads(run_ft("S", "--json").stdout.strip().splitlines()[-1])
+    assert line["verified"] is True and line["niter"] == 6 and line["max_rel_err"] <= 1e-12
