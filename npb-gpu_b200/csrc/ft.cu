@@ -7,9 +7,10 @@
 // A transform along one axis is one kernel: a CTA stages a tile of L lines
 // of that axis in shared memory (rows of L consecutive x values for the y
 // and z axes, so every row is one coalesced run; L whole x lines for the x
-// axis), transforms every line there by radix-8 Stockham stages (a 4 or a 2
-// last), each stage's butterflies in registers between two barriers, and
-// writes the tile back.  So each axis costs one read and one write of the
+// axis) and transforms every line by radix-8 Stockham stages (a 4 or a 2
+// last), each stage's butterflies in registers: the first stage reads its
+// points from the field, the last writes its outputs to the field, and the
+// stages between exchange through shared memory.  So each axis costs one read and one write of the
 // field.  The inverse transform's first axis (z) also does evolve: it reads
 // u0, multiplies each point by its twiddle factor (looked up by the point's
 // squared frequency in a table that stays in L2), writes the evolved u0
@@ -201,36 +202,85 @@ constexpr int smem_points()
     return N * P + N / 8;
 }
 
-// One Stockham stage over L lines of N points in s[sidx(n, l)]: butterfly j
-// of a line takes the points j + r N/R, twiddles them by
-// W^((j mod NS) r N/(NS R)), transforms them and puts them at
-// (j / NS) NS R + (j mod NS) + r NS.  T threads, each (N/R) L / T
-// butterflies; all reads before the barrier, all writes after it.
-template <int N, int L, int P, int NS, int R, int SIGN>
-__device__ __forceinline__ void stage(double2 *s, const double2 *__restrict__ W, int wscale)
+// Stockham stages over L lines of N points: a stage with sub-transforms of
+// NS points and radix R has N/R butterflies a line; butterfly j takes the
+// points j + r N/R, twiddles them by W^((j mod NS) r N/(NS R)), transforms
+// them and puts them at (j / NS) NS R + (j mod NS) + r NS.  The first stage
+// (NS = 1, R = 8) reads its points straight from the field and the last
+// (NS R = N, so its outputs land on j + r NS) writes straight to it: the
+// stages between exchange through shared memory, s[sidx(n, l)].
+
+// Butterfly b's line l and index j: in the first and the last stage x
+// lines take j fastest (a warp walks a line: coalesced), y and z lines l
+// fastest (a warp walks a row of x values).
+template <int AXIS, int L, int NB>
+__device__ __forceinline__ void bfly(int b, int &l, int &j)
 {
-    constexpr int T = N * L / 8, PER = (N / R) * L / T;
+    if constexpr (AXIS == 0) {
+        j = b % NB;
+        l = b / NB;
+    } else {
+        l = b % L;
+        j = b / L;
+    }
+}
+
+// The twiddles w^r, r < R, of butterfly j: w, w^2 and w^4 from the roots
+// table, the others their products (a few ulps; the transform's rounding is
+// of the same order), so a butterfly loads 3 roots instead of 7.
+template <int N, int NS, int R, int SIGN>
+__device__ __forceinline__ void twiddle_dft(double2 *v, int j, const double2 *__restrict__ W, int wscale)
+{
+    if constexpr (NS > 1) {
+        const int step = (j % NS) * (N / (NS * R)) * wscale;
+        auto root = [&](int r) {
+            double2 w = __ldg(W + step * r);
+            if constexpr (SIGN < 0) w.y = -w.y;
+            return w;
+        };
+        if constexpr (R == 8) {
+            const double2 w1 = root(1), w2 = root(2), w4 = root(4), w3 = cmul(w1, w2);
+            v[1] = cmul(v[1], w1);
+            v[2] = cmul(v[2], w2);
+            v[3] = cmul(v[3], w3);
+            v[4] = cmul(v[4], w4);
+            v[5] = cmul(v[5], cmul(w1, w4));
+            v[6] = cmul(v[6], cmul(w2, w4));
+            v[7] = cmul(v[7], cmul(w3, w4));
+        } else if constexpr (R == 4) {
+            const double2 w1 = root(1), w2 = root(2);
+            v[1] = cmul(v[1], w1);
+            v[2] = cmul(v[2], w2);
+            v[3] = cmul(v[3], cmul(w1, w2));
+        } else {
+            v[1] = cmul(v[1], root(1));
+        }
+    }
+    dft<R, SIGN>(v);
+}
+
+// A stage between the first and the last: shared to shared, all reads
+// before the barrier, all writes after it.  Lines fastest on every axis
+// here: the L lanes of a butterfly index share its twiddles (one load for
+// them all).
+template <int N, int L, int P, int NS, int R, int SIGN>
+__device__ __forceinline__ void stage_mid(double2 *s, const double2 *__restrict__ W, int wscale)
+{
+    constexpr int T = N * L / 8, NB = N / R, PER = NB * L / T;
     double2 v[PER][R];
 #pragma unroll
     for (int p = 0; p < PER; p++) {
-        const int b = threadIdx.x + p * T, l = b % L, j = b / L;
+        int l, j;
+        bfly<1, L, NB>(threadIdx.x + p * T, l, j);
 #pragma unroll
-        for (int r = 0; r < R; r++) v[p][r] = s[sidx<P>(j + r * (N / R), l)];
-        if constexpr (NS > 1) {
-            const int jm = j % NS;
-#pragma unroll
-            for (int r = 1; r < R; r++) {
-                double2 w = __ldg(W + jm * r * (N / (NS * R)) * wscale);
-                if constexpr (SIGN < 0) w.y = -w.y;
-                v[p][r] = cmul(v[p][r], w);
-            }
-        }
-        dft<R, SIGN>(v[p]);
+        for (int r = 0; r < R; r++) v[p][r] = s[sidx<P>(j + r * NB, l)];
+        twiddle_dft<N, NS, R, SIGN>(v[p], j, W, wscale);
     }
     __syncthreads();
 #pragma unroll
     for (int p = 0; p < PER; p++) {
-        const int b = threadIdx.x + p * T, l = b % L, j = b / L;
+        int l, j;
+        bfly<1, L, NB>(threadIdx.x + p * T, l, j);
         const int d = (j / NS) * NS * R + (j % NS);
 #pragma unroll
         for (int r = 0; r < R; r++) s[sidx<P>(d + r * NS, l)] = v[p][r];
@@ -238,13 +288,25 @@ __device__ __forceinline__ void stage(double2 *s, const double2 *__restrict__ W,
     __syncthreads();
 }
 
-template <int N, int L, int P, int NS, int SIGN>
-__device__ __forceinline__ void stages(double2 *s, const double2 *__restrict__ W, int wscale)
+// NS of the last stage: the stages' radices are 8 while 8 divides what is
+// left, then 4 or 2
+__host__ __device__ constexpr int last_ns(int n)
 {
-    if constexpr (NS < N) {
+    int ns = 1;
+    for (;;) {
+        const int r = (n / ns) % 8 == 0 ? 8 : ((n / ns) % 4 == 0 ? 4 : 2);
+        if (ns * r == n) return ns;
+        ns *= r;
+    }
+}
+
+template <int N, int L, int P, int NS, int SIGN>
+__device__ __forceinline__ void mid_stages(double2 *s, const double2 *__restrict__ W, int wscale)
+{
+    if constexpr (NS < last_ns(N)) {
         constexpr int R = StageRadix<N, NS>::value;
-        stage<N, L, P, NS, R, SIGN>(s, W, wscale);
-        stages<N, L, P, NS * R, SIGN>(s, W, wscale);
+        stage_mid<N, L, P, NS, R, SIGN>(s, W, wscale);
+        mid_stages<N, L, P, NS * R, SIGN>(s, W, wscale);
     }
 }
 
@@ -265,7 +327,8 @@ struct Tile {
 };
 
 // One axis of the transform: AXIS 0 (x), 1 (y), 2 (z).  in and out may be
-// the same array (a CTA reads its whole tile before writing it).  EVOLVE:
+// the same array (a CTA reads its whole tile, in the first stage, before it
+// writes any of it, in the last).  EVOLVE:
 // in is u0; each point is first multiplied by its twiddle factor and the
 // product written back to u0 (ft.cu:1245-1256), then transformed into out.
 template <int N, int AXIS, int SIGN, bool EVOLVE>
@@ -297,45 +360,58 @@ __global__ void __launch_bounds__(Tile<N, AXIS>::T, (1024 / Tile<N, AXIS>::T) < 
         const int jj = q < ny / 2 ? q : q - ny;
         jj2 = jj * jj;
     }
-    // every load of the tile before any store: the evolved points go back to
-    // u0, which is `in`, so a store between loads would order them
-    double2 v[8];
+    static_assert(last_ns(N) >= 8, "a first and a last stage");
+    // first stage (NS = 1, R = 8): butterfly j of line l reads its 8 points,
+    // rows j + r N/8, from the field -- every load before any store (the
+    // evolved points go back to u0, which is `in`)
+    {
+        constexpr int NB = N / 8;
+        int l, j;
+        bfly<AXIS, L, NB>(threadIdx.x, l, j);
+        double2 v[8];
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-        const int i = threadIdx.x + k * T;
-        const int n = AXIS == 0 ? i % N : i / L, l = AXIS == 0 ? i / N : i % L;
-        v[k] = in[base + n * sn + l * sl];
-    }
-    if constexpr (EVOLVE) {
-        double t[8];
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
+        for (int r = 0; r < 8; r++) v[r] = in[base + (j + r * NB) * sn + l * sl];
+        if constexpr (EVOLVE) {
             // the point is (x0 + l, q, n); its squared frequency, summed as
             // the reference sums it (integers: exact in any order)
-            const int i = threadIdx.x + k * T, n = i / L, l = i % L;
-            const int xi = x0 + l, ii = xi < nx / 2 ? xi : xi - nx, kk = n < nz / 2 ? n : n - nz;
-            t[k] = __ldg(twk2 + (ii * ii + (jj2 + kk * kk)));
+            const int xi = x0 + l, ii = xi < nx / 2 ? xi : xi - nx;
+            double t[8];
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                const int n = j + r * NB, kk = n < nz / 2 ? n : n - nz;
+                t[r] = __ldg(twk2 + (ii * ii + (jj2 + kk * kk)));
+            }
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                v[r] = make_double2(v[r].x * t[r], v[r].y * t[r]);
+                u0[base + (j + r * NB) * sn + l * sl] = v[r];
+            }
+        }
+        dft<8, SIGN>(v);
+#pragma unroll
+        for (int r = 0; r < 8; r++) sbuf[sidx<P>(8 * j + r, l)] = v[r];
+        __syncthreads();
+    }
+    mid_stages<N, L, P, 8, SIGN>(sbuf, W, wscale);
+    // last stage: its outputs are the rows j + r NS of the field
+    {
+        constexpr int NS = last_ns(N), R = N / NS, NB = N / R, PER = NB * L / T;
+        double2 v[PER][R];
+#pragma unroll
+        for (int p = 0; p < PER; p++) {
+            int l, j;
+            bfly<AXIS, L, NB>(threadIdx.x + p * T, l, j);
+#pragma unroll
+            for (int r = 0; r < R; r++) v[p][r] = sbuf[sidx<P>(j + r * NB, l)];
+            twiddle_dft<N, NS, R, SIGN>(v[p], j, W, wscale);
         }
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const int i = threadIdx.x + k * T, n = i / L, l = i % L;
-            v[k] = make_double2(v[k].x * t[k], v[k].y * t[k]);
-            u0[base + n * sn + l * sl] = v[k];
+        for (int p = 0; p < PER; p++) {
+            int l, j;
+            bfly<AXIS, L, NB>(threadIdx.x + p * T, l, j);
+#pragma unroll
+            for (int r = 0; r < R; r++) out[base + (j + r * NS) * sn + l * sl] = v[p][r];
         }
-    }
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-        const int i = threadIdx.x + k * T;
-        const int n = AXIS == 0 ? i % N : i / L, l = AXIS == 0 ? i / N : i % L;
-        sbuf[sidx<P>(n, l)] = v[k];
-    }
-    __syncthreads();
-    stages<N, L, P, 1, SIGN>(sbuf, W, wscale);
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-        const int i = threadIdx.x + k * T;
-        const int n = AXIS == 0 ? i % N : i / L, l = AXIS == 0 ? i / N : i % L;
-        out[base + n * sn + l * sl] = sbuf[sidx<P>(n, l)];
     }
 }
 
