@@ -12,10 +12,12 @@
 // points from the field, the last writes its outputs to the field, and the
 // stages between exchange through shared memory.  So each axis costs one read and one write of the
 // field.  The inverse transform's first axis (z) also does evolve: it reads
-// u0, multiplies each point by its twiddle factor (looked up by the point's
-// squared frequency in a table that stays in L2), writes the evolved u0
-// back and transforms that; the checksum reads its 1024 points in a fixed
-// order.
+// the forward transform (kept in u0), multiplies each point by its twiddle
+// factor (looked up by the point's squared frequency in a table that stays
+// in L2) once per iteration since u0 was last written back -- the
+// reference's u0 *= twiddle, product for product -- and transforms that,
+// writing u0 back every few iterations; the checksum reads its 1024 points
+// in a fixed order.
 //
 // Transform sign: sign +1 is sum x_j exp(+2 pi i jk / n), the reference's
 // is = 1 (its forward transform); sign -1 its is = -1.  Results agree with
@@ -44,6 +46,15 @@ constexpr int kPoints = 1024;                     // CHECKSUM_TASKS
 constexpr int kInitPer = 16;                      // elements a thread of the initial conditions
 constexpr int kMaxIter = 64;
 constexpr double kRoot2Half = 0.70710678118654752440;
+#ifndef FT_STORE_EVERY
+#define FT_STORE_EVERY 64
+#endif
+// the evolved field goes back to u0 every kStoreEvery iterations (and in the
+// last): an iteration multiplies each point by its factor at most that many
+// times.  Measured at classes B-D, storing every 2, 4 or 8 iterations is
+// slower than storing only in the last (64 >= any run's niter): the
+// products cost less than u0's writes.
+constexpr int kStoreEvery = FT_STORE_EVERY;
 
 __device__ __forceinline__ uint64_t lcg_mul(uint64_t a, uint64_t b) { return (a * b) & kMask46; }
 
@@ -328,13 +339,14 @@ struct Tile {
 
 // One axis of the transform: AXIS 0 (x), 1 (y), 2 (z).  in and out may be
 // the same array (a CTA reads its whole tile, in the first stage, before it
-// writes any of it, in the last).  EVOLVE:
-// in is u0; each point is first multiplied by its twiddle factor and the
-// product written back to u0 (ft.cu:1245-1256), then transformed into out.
+// writes any of it, in the last).  EVOLVE: in is u0 as the forward
+// transform left it; each point is multiplied `steps` times by its twiddle
+// factor (iteration `steps` of ft.cu:1245-1256), written back to u0 when
+// `store` is set (the last iteration), and transformed into out.
 template <int N, int AXIS, int SIGN, bool EVOLVE>
 __global__ void __launch_bounds__(Tile<N, AXIS>::T, (1024 / Tile<N, AXIS>::T) < 1 ? 1 : 1024 / Tile<N, AXIS>::T)
     k_fft(const double2 *in, double2 *out, double2 *u0, const double *__restrict__ twk2,
-          const double2 *__restrict__ W, int wscale, int nx, int ny, int nz)
+          const double2 *__restrict__ W, int wscale, int nx, int ny, int nz, int steps, int store)
 {
     static_assert(!EVOLVE || AXIS == 2, "evolve rides on the z lines");
     constexpr int L = Tile<N, AXIS>::L, P = AXIS == 0 ? L + 1 : L, T = Tile<N, AXIS>::T;
@@ -381,10 +393,16 @@ __global__ void __launch_bounds__(Tile<N, AXIS>::T, (1024 / Tile<N, AXIS>::T) < 
                 const int n = j + r * NB, kk = n < nz / 2 ? n : n - nz;
                 t[r] = __ldg(twk2 + (ii * ii + (jj2 + kk * kk)));
             }
+            // u0 after `steps` iterations: the forward transform's point
+            // multiplied `steps` times by its factor, each product rounded
+            // as the reference's u0 *= twiddle rounds it -- the same double
+            for (int k = 0; k < steps; k++) {
 #pragma unroll
-            for (int r = 0; r < 8; r++) {
-                v[r] = make_double2(v[r].x * t[r], v[r].y * t[r]);
-                u0[base + (j + r * NB) * sn + l * sl] = v[r];
+                for (int r = 0; r < 8; r++) v[r] = make_double2(v[r].x * t[r], v[r].y * t[r]);
+            }
+            if (store) {
+#pragma unroll
+                for (int r = 0; r < 8; r++) u0[base + (j + r * NB) * sn + l * sl] = v[r];
             }
         }
         dft<8, SIGN>(v);
@@ -435,7 +453,7 @@ __global__ void __launch_bounds__(kPoints) k_checksum(const double2 *u1, int nx,
 }
 
 using FftKernel = void (*)(const double2 *, double2 *, double2 *, const double *, const double2 *, int, int, int,
-                           int);
+                           int, int, int);
 
 struct Launch {
     FftKernel k = nullptr;
@@ -514,17 +532,21 @@ void ft_release(cgb_ft *f)
 
 bool pow2_in(int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; }
 
-void run_pass(cgb_ft *f, const Launch &a, int axis, const double2 *in, double2 *out)
+void run_pass(cgb_ft *f, const Launch &a, int axis, const double2 *in, double2 *out, int steps = 0, int store = 0)
 {
     const int dims[3] = {f->nx, f->ny, f->nz};
     const unsigned tiles = unsigned(f->nt / ((long long)dims[axis] * a.lines));
     a.k<<<tiles, a.threads, a.smem, f->stream>>>(in, out, f->u0, f->twk2, f->W, f->maxdim / dims[axis], f->nx, f->ny,
-                                                  f->nz);
+                                                  f->nz, steps, store);
 }
 
 // main's timed region (ft.cu:391-408): index map (as its table by k2),
 // initial conditions, the roots, the forward transform u1 -> u0, then
-// niter x (evolve, inverse transform, checksum)
+// niter x (evolve, inverse transform, checksum).  Iteration it forms the
+// evolved field from u0 as last stored and one product by the twiddle
+// factor per iteration since (the doubles the reference's u0 holds then),
+// so u0 is read every iteration but written back only every kStoreEvery
+// iterations and in the last.
 void enqueue_benchmark(cgb_ft *f, int niter)
 {
     const cudaStream_t st = f->stream;
@@ -535,8 +557,11 @@ void enqueue_benchmark(cgb_ft *f, int niter)
     run_pass(f, f->fwd[0], 0, f->u1, f->u1);
     run_pass(f, f->fwd[1], 1, f->u1, f->u1);
     run_pass(f, f->fwd[2], 2, f->u1, f->u0);
+    int stored = 0;  // the iteration whose evolved field u0 holds (0: the forward transform)
     for (int it = 1; it <= niter; it++) {
-        run_pass(f, f->inv[2], 2, f->u0, f->u1);
+        const int steps = it - stored, store = (steps == kStoreEvery || it == niter) ? 1 : 0;
+        run_pass(f, f->inv[2], 2, f->u0, f->u1, steps, store);
+        if (store) stored = it;
         run_pass(f, f->inv[1], 1, f->u1, f->u1);
         run_pass(f, f->inv[0], 0, f->u1, f->u1);
         k_checksum<<<1, kPoints, 0, st>>>(f->u1, f->nx, f->ny, f->nz, it, f->sums);
