@@ -685,8 +685,10 @@ def ft_section(npbcg, device, rank):
     nt = float(nx * ny * nz)
     # ft.cu:418-421
     mflops = 1.0e-6 * nt * (14.8157 + 7.19641 * np.log(nt) + (5.23518 + 7.21113 * np.log(nt)) * niter) / (ms / 1e3)
-    # per iteration: evolve + z (u0 read, u0 and u1 written), y and x (read + write): 112 B a point
-    algorithmic = nt * (16 * 3 + 4 * 16 + niter * 112)
+    # the initial conditions (16 B a point written), the forward transform
+    # (3 passes, 32 B each), per iteration 3 passes of 32 B (the first reads
+    # u0 and writes u1), and u0 written back once (16 B)
+    algorithmic = nt * (16 + 3 * 32 + niter * 3 * 32 + 16)
     out = {
         "what": f"NPB FT class {FT_CLASS}: {nx}x{ny}x{nz}, {niter} iterations (one shared-memory "
                 "Stockham pass an axis, evolve fused into the z pass), FP64",
