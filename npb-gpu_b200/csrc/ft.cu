@@ -322,8 +322,9 @@ __device__ __forceinline__ void mid_stages(double2 *s, const double2 *__restrict
 }
 
 // Lines a CTA: about FT_TILE_POINTS points a tile, 2 .. 16 lines (x
-// lines), 4 .. 32 lines (y and z: a row of L consecutive x values is the
-// run each strided row read fetches).
+// lines); y and z lines about FT_ROW_POINTS points a tile but at least 8
+// (a row of L consecutive x values is the run each strided row read
+// fetches: 128 bytes) and at most 32 lines, and at most 1024 threads.
 #ifndef FT_TILE_POINTS
 #define FT_TILE_POINTS 4096
 #endif
@@ -333,7 +334,8 @@ __device__ __forceinline__ void mid_stages(double2 *s, const double2 *__restrict
 constexpr int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 template <int N, int AXIS>
 struct Tile {
-    static constexpr int L = AXIS == 0 ? clampi(FT_TILE_POINTS / N, 2, 16) : clampi(FT_ROW_POINTS / N, 4, 32);
+    static constexpr int L = AXIS == 0 ? clampi(FT_TILE_POINTS / N, 2, 16)
+                                       : clampi(FT_ROW_POINTS / N, 8 < 8192 / N ? 8 : 8192 / N, 32);
     static constexpr int T = N * L / 8;  // threads: one radix-8 butterfly each a stage
 };
 
