@@ -67,3 +67,22 @@ def test_reference_gpu_is_agrees(cgb):
     assert ref["passed"] == cgb.IS_PASSED and ref["seconds"] > 0
     with cgb.IntSort("S") as s:
         assert s.run()["passed"] == cgb.IS_PASSED
+
+
+@pytest.mark.parametrize("total_log2,max_log2", [(12, 8), (12, 26), (16, 20), (20, 10), (14, 14)])
+def test_is_bucket_edges_count_exactly(cgb, total_log2, max_log2):
+    """Custom sizes at the bucket pass's edges: one bucket of 256 values
+    (2^8), thousands of nearly empty buckets (2^12 keys below 2^26), runs of
+    keys shorter than the grid (2^12 keys: CTAs with no keys), square sizes.
+    After a run the counts below each value and the sorted keys must equal
+    an independent count of the keys the run left."""
+    with cgb.IntSort("U", total_log2, max_log2) as s:
+        out = s.run()
+        keys, below, srt = s.read("keys"), s.read("below"), s.read("sorted")
+    maxk = 1 << max_log2
+    assert keys.min() >= 0 and keys.max() < maxk
+    counts = np.bincount(keys, minlength=maxk)
+    want = np.concatenate(([0], np.cumsum(counts)[:-1]))
+    assert np.array_equal(below.astype(np.int64), want)
+    assert np.array_equal(srt, np.sort(keys))
+    assert out["passed"] == 1
