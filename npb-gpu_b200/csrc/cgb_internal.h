@@ -1,6 +1,8 @@
 // cgb_internal.h -- shared host-side declarations of libcgb.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <vector>
 
 #include "../../include/cgb.h"
@@ -10,6 +12,19 @@ namespace cgb {
 // Records a formatted message as the calling thread's last error and returns
 // `status` unchanged, so call sites read `return set_error(...)`.
 int set_error(int status, const char *fmt, ...);
+
+// A kernel's dynamic shared memory limit is one per process, shared by
+// every session or instance that launches it: this only ever raises it, so
+// an object set up for a larger problem stays launchable after a smaller
+// one is set up.  `kernel` is the kernel function's address.
+inline cudaError_t raise_smem_limit(const void *kernel, size_t bytes)
+{
+    cudaFuncAttributes fa{};
+    const cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    if (size_t(fa.maxDynamicSharedSizeBytes) >= bytes) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+}
 
 // Odd integer in (1, 2^46): the LCG's admissible seeds (c_randdp.cpp:70-71).
 bool valid_seed(double seed);

@@ -651,8 +651,8 @@ int cgb_is_create(int device, char cls, int total_log2, int max_log2, cgb_is **o
     // same grid
     int optin = 0;
     if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess ||
-        cudaFuncSetAttribute(k_bucket_rank, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(sizeof(unsigned)) * s->width) != cudaSuccess) {
+        raise_smem_limit(reinterpret_cast<const void *>(k_bucket_rank), sizeof(unsigned) * s->width) !=
+            cudaSuccess) {
         is_release(s);
         return set_error(CGB_ERR_CUDA, "is: kernel attributes");
     }
@@ -661,17 +661,14 @@ int cgb_is_create(int device, char cls, int total_log2, int max_log2, cgb_is **o
     for (int k = 0; k < 2; k++) {
         const size_t bytes = scatter_smem(s->nb, rings[k]);
         if (bytes > size_t(optin) ||
-            cudaFuncSetAttribute(k_bucket_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)) !=
-                cudaSuccess ||
+            raise_smem_limit(reinterpret_cast<const void *>(k_bucket_scatter), bytes) != cudaSuccess ||
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[k], k_bucket_scatter, kWideThreads, bytes) !=
                 cudaSuccess)
             per_sm[k] = 0;
     }
     cudaGetLastError();  // a ring that did not fit is no error
     const int pick = per_sm[0] >= per_sm[1] ? 0 : 1;
-    if (per_sm[pick] < 1 ||
-        cudaFuncSetAttribute(k_bucket_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(scatter_smem(s->nb, rings[pick]))) != cudaSuccess) {
+    if (per_sm[pick] < 1) {
         is_release(s);
         return set_error(CGB_ERR_CUDA, "is: the bucket scatter does not fit an SM");
     }

@@ -760,11 +760,9 @@ bool make_plan(cgb_session *s, int kind, int lpr, Plan *pl, int prefetch = 0, in
         P.block_pcg = kSlicedPcgBlock;
         P.smem = sliced_smem_bytes(s->sliced_max_rows, s->sliced_nacc);
         for (OuterKernel k : {P.fp64, P.mixed, P.pcg})
-            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)))
-                return false;
+            if (raise_smem_limit(reinterpret_cast<const void *>(k), P.smem)) return false;
         for (SpmvKernel k : {P.spmv, P.spmv32})
-            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)))
-                return false;
+            if (raise_smem_limit(reinterpret_cast<const void *>(k), P.smem)) return false;
     } else {
         return false;
     }

@@ -523,3 +523,22 @@ def test_recycle_rejects_out_of_range(cgb):
         # the reference mode ignores it
         out = s.power_iterate(niter, shift, recycle=4)
     assert abs(out["zeta"][-1] - VERIFY["S"]) / VERIFY["S"] <= 1e-10
+
+
+def test_sessions_of_different_sizes_coexist(cgb):
+    """A class-C session on the sliced plan, then a class-B one beside it (a
+    smaller shared-memory need: fewer rows a CTA): the kernels' shared
+    memory limit is one per process, and setting up the smaller session must
+    not leave the larger one unable to launch.  Its results stay
+    bit-identical."""
+    n, nonzer, _, shift = PARAMS["C"]
+    rs, ci, a = cgb.makea(n, nonzer, 0.1, shift)
+    na, nza, _, sha = PARAMS["B"]
+    rsa, cia, aa = cgb.makea(na, nza, 0.1, sha)
+    with cgb.Session(rs, ci, a, spmv_kernel=2) as big:
+        first = big.power_iterate(2, shift)
+        with cgb.Session(rsa, cia, aa, spmv_kernel=2) as small:
+            small.power_iterate(2, sha)
+            again = big.power_iterate(2, shift)
+    assert np.array_equal(first["zeta"], again["zeta"])
+    assert np.array_equal(first["rnorm"], again["rnorm"])

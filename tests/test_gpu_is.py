@@ -86,3 +86,18 @@ def test_is_bucket_edges_count_exactly(cgb, total_log2, max_log2):
     assert np.array_equal(below.astype(np.int64), want)
     assert np.array_equal(srt, np.sort(keys))
     assert out["passed"] == 1
+
+
+def test_is_instances_of_different_sizes_coexist(cgb):
+    """Two live instances, the larger made first: the smaller one's set-up
+    must not leave the larger one unable to launch (the kernels' shared
+    memory limit is per process)."""
+    with cgb.IntSort("W") as big:
+        with cgb.IntSort("S") as small:
+            assert small.run()["passed"] == cgb.IS_PASSED
+            assert big.run()["passed"] == cgb.IS_PASSED
+        assert big.run()["passed"] == cgb.IS_PASSED
+    with cgb.IntSort("U", 16, 27) as wide:  # 4096 buckets: the largest scatter tables
+        with cgb.IntSort("U", 16, 10) as narrow:
+            assert narrow.run()["passed"] == 1
+            assert wide.run()["passed"] == 1
