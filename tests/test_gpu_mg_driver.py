@@ -186,3 +186,18 @@ def test_ft_driver_report_verifies():
     assert abs(mops - expect) <= expect * (1e-6 / t + 1e-6) + 0.01
     line = json.loads(run_ft("S", "--json").stdout.strip().splitlines()[-1])
     assert line["verified"] is True and line["niter"] == 6 and line["max_rel_err"] <= 1e-12
+
+
+@pytest.mark.parametrize("name,runner", [("ep", run_ep), ("is", run_is), ("ft", run_ft)])
+def test_npb_drivers_fail_loudly_without_a_gpu(name, runner):
+    """No CPU fallback: without a CUDA device each driver exits 1 with the
+    library's error and prints no verification."""
+    import npbcg
+    try:
+        npbcg.device_info(0)
+        pytest.skip("a CUDA device is present")
+    except npbcg.CgbError:
+        pass
+    r = runner("S", timeout=120)
+    assert r.returncode == 1 and f"{name}: run failed" in r.stderr
+    assert "SUCCESSFUL" not in r.stdout
