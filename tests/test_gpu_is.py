@@ -69,11 +69,14 @@ def test_reference_gpu_is_agrees(cgb):
         assert s.run()["passed"] == cgb.IS_PASSED
 
 
-@pytest.mark.parametrize("total_log2,max_log2", [(12, 8), (12, 26), (16, 20), (20, 10), (14, 14)])
+@pytest.mark.parametrize("total_log2,max_log2", [(12, 8), (12, 26), (16, 20), (20, 10), (14, 14), (22, 8),
+                                                 (24, 8)])
 def test_is_bucket_edges_count_exactly(cgb, total_log2, max_log2):
     """Custom sizes at the bucket pass's edges: one bucket of 256 values
     (2^8), thousands of nearly empty buckets (2^12 keys below 2^26), runs of
-    keys shorter than the grid (2^12 keys: CTAs with no keys), square sizes.
+    keys shorter than the grid (2^12 keys: CTAs with no keys), square sizes,
+    and values holding tens of thousands of keys each (2^22 and 2^24 keys
+    below 2^8).
     After a run the counts below each value and the sorted keys must equal
     an independent count of the keys the run left."""
     with cgb.IntSort("U", total_log2, max_log2) as s:
