@@ -43,7 +43,7 @@ constexpr double kAlpha = 1.0e-6;          // ALPHA (ft.cu:131)
 constexpr double kPi = 3.141592653589793238;
 constexpr double kAp = -4.0 * kAlpha * kPi * kPi;  // AP (ft.cu:132), the same order of operations
 constexpr int kPoints = 1024;                     // CHECKSUM_TASKS
-constexpr int kInitPer = 16;                      // elements a thread of the initial conditions
+constexpr int kInitPer = 64;                      // elements a lane of the initial conditions
 constexpr int kMaxIter = 64;
 constexpr double kRoot2Half = 0.70710678118654752440;
 #ifndef FT_STORE_EVERY
@@ -72,17 +72,24 @@ __device__ __forceinline__ uint64_t jump(uint64_t e)
 
 // Element e holds draws 2e+1 and 2e+2 after the seed (the planes' seeds of
 // ft.cu:1188-1213 and their rows' vranlc runs are one stream in that order).
+// A warp fills 32 kInitPer consecutive elements: lane l takes l, l + 32,
+// l + 64, ..., so every store is one coalesced run; it jumps to its first
+// element once and steps 32 elements (64 draws) at a time by A^64.
 __global__ void k_initial(double2 *u, long long nt)
 {
-    const long long e0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) * kInitPer;
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long e0 = warp * 32 * kInitPer + lane;
     if (e0 >= nt) return;
-    uint64_t x = jump(2 * uint64_t(e0));
-    const long long e1 = min(nt, e0 + kInitPer);
-    for (long long e = e0; e < e1; e++) {
-        x = lcg_mul(x, kMult);
-        const double re = double(x) * 0x1p-46;
-        x = lcg_mul(x, kMult);
-        u[e] = make_double2(re, double(x) * 0x1p-46);
+    uint64_t a64 = kMult;  // A^64
+#pragma unroll
+    for (int k = 0; k < 6; k++) a64 = lcg_mul(a64, a64);
+    uint64_t x = jump(2 * uint64_t(e0) + 1);  // draw 2 e0 + 1
+    const long long e1 = min(nt, warp * 32 * kInitPer + 32 * kInitPer);
+    for (long long e = e0; e < e1; e += 32) {
+        const uint64_t y = lcg_mul(x, kMult);
+        u[e] = make_double2(double(x) * 0x1p-46, double(y) * 0x1p-46);
+        x = lcg_mul(x, a64);
     }
 }
 
@@ -554,7 +561,7 @@ void enqueue_benchmark(cgb_ft *f, int niter)
     const cudaStream_t st = f->stream;
     k_roots<<<(f->maxdim + 255) / 256, 256, 0, st>>>(f->W, f->maxdim);
     k_twiddle_table<<<(f->k2max + 256) / 256, 256, 0, st>>>(f->twk2, f->k2max);
-    const long long init_threads = (f->nt + kInitPer - 1) / kInitPer;
+    const long long init_threads = 32 * ((f->nt + 32LL * kInitPer - 1) / (32LL * kInitPer));
     k_initial<<<unsigned((init_threads + 255) / 256), 256, 0, st>>>(f->u1, f->nt);
     run_pass(f, f->fwd[0], 0, f->u1, f->u1);
     run_pass(f, f->fwd[1], 1, f->u1, f->u1);
