@@ -78,7 +78,16 @@ __device__ __forceinline__ uint64_t jump(uint64_t e)
     return r;
 }
 
-__global__ void k_keys(int32_t *keys, long long n, double scale)
+// The bucket mirror: key >> shift for every key, one byte a key where the
+// buckets number at most 256 (classes S-C), else two -- all the bucket
+// count reads of a key.
+__device__ __forceinline__ void put_bucket(void *hi, int hi_bytes, long long i, int32_t key, int shift)
+{
+    if (hi_bytes == 1) static_cast<uint8_t *>(hi)[i] = uint8_t(key >> shift);
+    else static_cast<uint16_t *>(hi)[i] = uint16_t(key >> shift);
+}
+
+__global__ void k_keys(int32_t *keys, void *hi, int hi_bytes, int shift, long long n, double scale)
 {
     const long long i0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) * kKeysPerThread;
     if (i0 >= n) return;
@@ -91,17 +100,30 @@ __global__ void k_keys(int32_t *keys, long long n, double scale)
             s = d == 0 ? double(x) * 0x1p-46 : s + double(x) * 0x1p-46;
         }
         keys[i] = int32_t(scale * s);
+        put_bucket(hi, hi_bytes, i, keys[i], shift);
     }
 }
 
-// The iteration's two rewritten keys, then the five test keys (one thread,
-// in the reference's order).
-__global__ void k_prep(int32_t *keys, int it, Params P, long long *probe)
+// The iteration's two rewritten keys (and their buckets), then the five
+// test keys (one thread, in the reference's order).
+__global__ void k_prep(int32_t *keys, void *hi, int hi_bytes, int shift, int it, Params P, long long *probe)
 {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     keys[it] = it;
     keys[it + kIters] = P.maxk - it;
+    put_bucket(hi, hi_bytes, it, it, shift);
+    put_bucket(hi, hi_bytes, it + kIters, P.maxk - it, shift);
     for (int i = 0; i < kTests; i++) probe[i] = keys[P.index[i]];
+}
+
+// Puts keys[0 .. 2 kIters] back from the copy taken after generation, with
+// their buckets (a run rewrites keys 1 .. 20).
+__global__ void k_restore(int32_t *keys, void *hi, int hi_bytes, int shift, const int32_t *backup)
+{
+    const int i = threadIdx.x;
+    if (i > 2 * kIters) return;
+    keys[i] = backup[i];
+    put_bucket(hi, hi_bytes, i, backup[i], shift);
 }
 
 // A ranking pass counts keys by value in three steps, all in shared memory:
@@ -145,37 +167,46 @@ constexpr long long kWaitLimitNs = 2000000000LL;                 // a bulk copy'
 
 // (1) hist[b G + g] = CTA g's keys in bucket b; a warp adds into one of
 // `copies` private tables, so that few buckets do not mean many collisions.
-__global__ void __launch_bounds__(kWideThreads, 1024 / kWideThreads) k_bucket_count(const int32_t *__restrict__ keys, long long n,
-                                                               long long chunk4, int shift, int nb, int copies,
-                                                               unsigned *__restrict__ hist)
+// It reads the bucket mirror only (HiT: uint8_t or uint16_t a key): CTA g's
+// keys are [g 4 chunk4, (g + 1) 4 chunk4), chunk4 a multiple of 8, so its
+// run starts on a 16-byte word of the mirror.
+template <class HiT>
+__global__ void __launch_bounds__(kWideThreads, 1024 / kWideThreads) k_bucket_count(const HiT *__restrict__ hi,
+                                                                                   long long n, long long chunk4,
+                                                                                   int nb, int copies,
+                                                                                   unsigned *__restrict__ hist)
 {
+    constexpr int kPer = 16 / int(sizeof(HiT));  // keys a 16-byte word
     extern __shared__ unsigned tab[];
     for (int i = threadIdx.x; i < copies * nb; i += blockDim.x) tab[i] = 0u;
     __syncthreads();
     unsigned *mine = tab + ((threadIdx.x >> 5) % copies) * nb;
     const unsigned top = unsigned(nb - 1);
-    const int4 *k4 = reinterpret_cast<const int4 *>(keys);
-    const long long j0 = blockIdx.x * chunk4, j1 = min(n >> 2, j0 + chunk4), step = blockDim.x;
+    const uint4 *h16 = reinterpret_cast<const uint4 *>(hi);
+    const long long k0 = blockIdx.x * 4 * chunk4, k1 = min(n, k0 + 4 * chunk4);
+    const long long j0 = k0 / kPer, j1 = k1 > k0 ? k1 / kPer : j0, step = blockDim.x;
+    auto add16 = [&](uint4 w) {
+        const unsigned ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if constexpr (sizeof(HiT) == 1) {
+#pragma unroll
+                for (int b = 0; b < 4; b++) atomicAdd(&mine[((ws[q] >> (8 * b)) & 0xffu) & top], 1u);
+            } else {
+                atomicAdd(&mine[(ws[q] & 0xffffu) & top], 1u);
+                atomicAdd(&mine[(ws[q] >> 16) & top], 1u);
+            }
+        }
+    };
     long long j = j0 + threadIdx.x;
     for (; j + (kUnroll - 1) * step < j1; j += kUnroll * step) {
-        int4 v[kUnroll];
+        uint4 v[kUnroll];
 #pragma unroll
-        for (int u = 0; u < kUnroll; u++) v[u] = __ldcs(k4 + j + u * step);
+        for (int u = 0; u < kUnroll; u++) v[u] = __ldcs(h16 + j + u * step);
 #pragma unroll
-        for (int u = 0; u < kUnroll; u++) {
-            atomicAdd(&mine[unsigned(v[u].x >> shift) & top], 1u);
-            atomicAdd(&mine[unsigned(v[u].y >> shift) & top], 1u);
-            atomicAdd(&mine[unsigned(v[u].z >> shift) & top], 1u);
-            atomicAdd(&mine[unsigned(v[u].w >> shift) & top], 1u);
-        }
+        for (int u = 0; u < kUnroll; u++) add16(v[u]);
     }
-    for (; j < j1; j += step) {
-        const int4 v = __ldcs(k4 + j);
-        atomicAdd(&mine[unsigned(v.x >> shift) & top], 1u);
-        atomicAdd(&mine[unsigned(v.y >> shift) & top], 1u);
-        atomicAdd(&mine[unsigned(v.z >> shift) & top], 1u);
-        atomicAdd(&mine[unsigned(v.w >> shift) & top], 1u);
-    }
+    for (; j < j1; j += step) add16(__ldcs(h16 + j));
     __syncthreads();
     for (int b = threadIdx.x; b < nb; b += blockDim.x) {
         unsigned t = 0u;
@@ -538,6 +569,8 @@ struct cgb_is {
     int device = 0, sms = 148;
     Params P{};
     int32_t *keys = nullptr, *sorted = nullptr, *backup = nullptr;  // backup: keys[0 .. 2 kIters]
+    void *hi = nullptr;                                 // the bucket mirror
+    int hi_bytes = 1;                                   // 1 (at most 256 buckets) or 2
     unsigned *counts = nullptr, *totals = nullptr, *hist = nullptr;
     long long *probe = nullptr;
     unsigned long long *passed = nullptr, *bad = nullptr;
@@ -565,7 +598,7 @@ void is_release(cgb_is *s)
     if (!s) return;
     cudaSetDevice(s->device);
     if (s->exec) cudaGraphExecDestroy(s->exec);
-    for (void *p : {(void *)s->keys, (void *)s->sorted, (void *)s->backup, (void *)s->counts,
+    for (void *p : {(void *)s->keys, s->hi, (void *)s->sorted, (void *)s->backup, (void *)s->counts,
                     (void *)s->totals, (void *)s->hist, (void *)s->err, (void *)s->probe, (void *)s->passed, (void *)s->bad})
         if (p) cudaFree(p);
     if (s->ev0) cudaEventDestroy(s->ev0);
@@ -584,9 +617,14 @@ void enqueue_rank(cgb_is *s, int it)
 {
     const cudaStream_t st = s->stream;
     const int len = s->grid * s->nb;
-    k_prep<<<1, 32, 0, st>>>(s->keys, it, s->P, s->probe);
-    k_bucket_count<<<s->grid, kWideThreads, sizeof(unsigned) * s->copies * s->nb, st>>>(
-        s->keys, s->P.n, s->chunk4, s->shift, s->nb, s->copies, s->hist);
+    k_prep<<<1, 32, 0, st>>>(s->keys, s->hi, s->hi_bytes, s->shift, it, s->P, s->probe);
+    const size_t count_smem = sizeof(unsigned) * s->copies * s->nb;
+    if (s->hi_bytes == 1)
+        k_bucket_count<uint8_t><<<s->grid, kWideThreads, count_smem, st>>>(
+            static_cast<const uint8_t *>(s->hi), s->P.n, s->chunk4, s->nb, s->copies, s->hist);
+    else
+        k_bucket_count<uint16_t><<<s->grid, kWideThreads, count_smem, st>>>(
+            static_cast<const uint16_t *>(s->hi), s->P.n, s->chunk4, s->nb, s->copies, s->hist);
     k_scan_tiles<<<s->tiles, kThreads, 0, st>>>(s->hist, len, s->totals);
     k_scan_totals<<<1, kThreads, 0, st>>>(s->totals, s->tiles);
     k_scan_add<<<s->tiles, kThreads, 0, st>>>(s->hist, len, s->totals);
@@ -674,11 +712,15 @@ int cgb_is_create(int device, char cls, int total_log2, int max_log2, cgb_is **o
     }
     s->ring = rings[pick];
     s->grid = per_sm[pick] * s->sms;
-    s->chunk4 = ((P.n >> 2) + s->grid - 1) / s->grid;
+    s->hi_bytes = s->nb <= 256 ? 1 : 2;
+    // 16-byte words of keys a CTA of (1) and (2), a multiple of 8 (so a CTA's
+    // run of the bucket mirror starts on a 16-byte word)
+    s->chunk4 = ((((P.n >> 2) + s->grid - 1) / s->grid) + 7) / 8 * 8;
     s->tiles = (s->grid * s->nb + kTileVals - 1) / kTileVals;
     const bool ok = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
                     cudaEventCreate(&s->ev0) == cudaSuccess && cudaEventCreate(&s->ev1) == cudaSuccess &&
                     cudaMalloc(&s->keys, sizeof(int32_t) * size_t(P.n)) == cudaSuccess &&
+                    cudaMalloc(&s->hi, size_t(s->hi_bytes) * size_t(P.n)) == cudaSuccess &&
                     cudaMalloc(&s->sorted, sizeof(int32_t) * size_t(P.n)) == cudaSuccess &&
                     cudaMalloc(&s->backup, sizeof(int32_t) * (2 * kIters + 1)) == cudaSuccess &&
                     cudaMalloc(&s->counts, sizeof(unsigned) * size_t(P.maxk)) == cudaSuccess &&
@@ -695,7 +737,7 @@ int cgb_is_create(int device, char cls, int total_log2, int max_log2, cgb_is **o
     }
     const long long gen_threads = (P.n + kKeysPerThread - 1) / kKeysPerThread;
     k_keys<<<unsigned((gen_threads + kThreads - 1) / kThreads), kThreads, 0, s->stream>>>(
-        s->keys, P.n, double(P.maxk) / 4.0);
+        s->keys, s->hi, s->hi_bytes, s->shift, P.n, double(P.maxk) / 4.0);
     if (cudaGetLastError() != cudaSuccess ||
         cudaMemcpyAsync(s->backup, s->keys, sizeof(int32_t) * (2 * kIters + 1), cudaMemcpyDeviceToDevice,
                         s->stream) != cudaSuccess ||
@@ -738,7 +780,7 @@ int cgb_is_run(cgb_is *s, long long *passed, double *device_ms)
     }
     // the generated keys back (a run rewrites keys 1 .. 20), then main's
     // untimed pass rank(1) and the reset of the passed count
-    IS_TRY(cudaMemcpyAsync(s->keys, s->backup, sizeof(int32_t) * (2 * kIters + 1), cudaMemcpyDeviceToDevice, st));
+    k_restore<<<1, 32, 0, st>>>(s->keys, s->hi, s->hi_bytes, s->shift, s->backup);
     IS_TRY(cudaMemsetAsync(s->passed, 0, sizeof(unsigned long long), st));
     enqueue_rank(s, 1);
     IS_TRY(cudaGetLastError());
