@@ -79,3 +79,17 @@ def test_reference_gpu_ft_agrees(cgb):
         ours = f.run(6)["sums"]
     for a, b in zip(ours, ref["sums"]):
         assert abs(complex(*a) - complex(*b)) <= 1e-12 * abs(complex(*b))
+
+
+def test_ft_runs_of_different_lengths_agree(cgb):
+    """A run is main's whole timed region, so its checksums do not depend on
+    the runs before it: 6 iterations after a 2-iteration run (the region
+    captured again for the new length) equal a fresh instance's 6, and the
+    first 2 of them equal the 2-iteration run's."""
+    with cgb.Ft(64, 64, 64) as f:
+        two = f.run(2)["sums"]
+        six = f.run(6)["sums"]
+    with cgb.Ft(64, 64, 64) as g:
+        fresh = g.run(6)["sums"]
+    assert six == fresh
+    assert six[:2] == two
